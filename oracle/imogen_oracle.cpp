@@ -1,0 +1,775 @@
+// C++ FP64 restatement of Imogen's relaxing-TVD fluid + magnet update.
+//
+// TEST INFRASTRUCTURE ONLY: this is the oracle (the checker).  Only tests/, the smoke check and
+// the CPU-baseline / reference arm of bench.py load it; the product library never links it.
+//
+// Like oracle/np_oracle.py it restates the reference array-at-a-time, one full-array temporary per
+// MATLAB expression, so every statement can be read against the MATLAB line it follows (cited
+// inline).  The two oracles perform the same IEEE-754 operations in the same order and agree
+// bit for bit (checked by tests/test_oracle.py).  Built with -O2 -ffp-contract=off (no FMA
+// contraction, no fast-math).  Element-wise loops are OpenMP-parallel over cells; results do not
+// depend on the thread count (no reductions other than max, which is exact).
+//
+// Parity against the MATLAB reference itself is unpinned (MATLAB/Octave are not available); the
+// MATLAB builtins it depends on are pinned separately (pchip vs SciPy, perms order by its
+// documented reverse-lexicographic order).
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+enum Mode { CIRC = 0, CONST = 1, FADE = 2, MIRROR = 3, TRANS = 4, WALL = 5 };
+enum Lim { VANLEER = 0, SUPERBEE = 1, MINMOD = 2 };
+enum Cls { C_MASS = 0, C_MOM = 1, C_ENER = 2, C_MAG = 3 };
+
+using Vec = std::vector<double>;
+
+// flux.m:17-27 -- perms([1 2 3]) rows (reverse lexicographic) and the matching magnet indices.
+const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1, 2, 3}};
+const int FWD_MI[3][2] = {{2, 3}, {1, 3}, {1, 2}};
+const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
+
+double msign(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : (v == 0 ? 0.0 : v)); }
+
+// ------------------------------------------------------------------------------------------------
+// pchip (MATLAB pchip / Moler pchiptx): harmonic-mean interior slopes, one-sided end slopes.
+// ------------------------------------------------------------------------------------------------
+void pchip_col(const double* x, int n, const double* y, const double* xi, int m, double* out) {
+    std::vector<double> h(n - 1), del(n - 1), d(n);
+    for (int k = 0; k < n - 1; ++k) {
+        h[k] = x[k + 1] - x[k];
+        del[k] = (y[k + 1] - y[k]) / h[k];
+    }
+    for (int k = 1; k < n - 1; ++k) {
+        double w1 = 2 * h[k] + h[k - 1];
+        double w2 = h[k] + 2 * h[k - 1];
+        if (msign(del[k - 1]) * msign(del[k]) > 0)
+            d[k] = (w1 + w2) / (w1 / del[k - 1] + w2 / del[k]);
+        else
+            d[k] = 0.0;
+    }
+    auto endslope = [](double h0, double h1, double d0, double d1) {
+        double dd = ((2 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+        if (msign(dd) != msign(d0)) dd = 0.0;
+        else if (msign(d0) != msign(d1) && std::fabs(dd) > std::fabs(3 * d0)) dd = 3 * d0;
+        return dd;
+    };
+    d[0] = endslope(h[0], h[1], del[0], del[1]);
+    d[n - 1] = endslope(h[n - 2], h[n - 3], del[n - 2], del[n - 3]);
+    for (int j = 0; j < m; ++j) {
+        int k = int(std::upper_bound(x, x + n, xi[j]) - x) - 1;
+        k = std::min(std::max(k, 0), n - 2);
+        double s = xi[j] - x[k];
+        double c1 = (d[k] + d[k + 1] - 2 * del[k]) / (h[k] * h[k]);
+        double c2 = (3 * del[k] - 2 * d[k] - d[k + 1]) / h[k];
+        out[j] = ((c1 * s + c2) * s + d[k]) * s + y[k];
+    }
+}
+
+struct Sim;
+
+// ------------------------------------------------------------------------------------------------
+// Edges.m
+// ------------------------------------------------------------------------------------------------
+struct Edges {
+    bool active[2][3] = {{false, false, false}, {false, false, false}};
+    Vec store[2][3];
+    double tol = 0.005;
+};
+
+struct IArr {
+    Sim* sim = nullptr;
+    int component = 0;   // 0 scalar, 1..3
+    int cls = 0;         // BC class
+    Vec a;
+    bool uninit = true;
+    Edges edges;
+    void set(Vec v);
+    void cleanup() { a.clear(); a.shrink_to_fit(); }
+    Vec shift(int DIRECT, int n);
+    Vec transparent_edge(int dim, bool upper);
+};
+
+struct Sim {
+    int n[3];
+    long long N;
+    int ndims;
+    double dgrid[3];
+    double gamma, cfl, minmass;
+    int bc[4][2][3];
+    int bc_inf;
+    Vec fade_coeff;
+    int limiter[3];
+    bool fluid_active, magnet_active;
+    double time_max;
+    int iter_max;
+    int update_mode;
+    double time = 0, dt = 0;
+    int iteration = 1;
+    double last_cmax = 0;
+    int last_grid_index = 0;
+
+    struct FluidVar { IArr prim, store, store_fluxR, store_fluxL, fluxR, fluxL; };
+    struct MagComp {
+        IArr prim, cellMag;
+        IArr velGrid[4], store[4], store_fluxR[4], wMag[4], flux[4];   // indexed by X (1..3)
+        bool isZero = false;
+    };
+    FluidVar fv[5];   // mass, momx, momy, momz, ener
+    MagComp mg[3];
+
+    long long stride(int d) const { return d == 0 ? 1 : (d == 1 ? n[0] : (long long)n[0] * n[1]); }
+    long long face(int d) const { return N / n[d]; }
+
+    void init_arr(IArr& A, int comp, int cls) { A.sim = this; A.component = comp; A.cls = cls; }
+};
+
+// Extract the face of array a at index idx along dim d, in column-major order of the other dims.
+Vec take_face(const Sim& s, const Vec& a, int d, int idx) {
+    Vec out(s.face(d));
+    int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    long long sd = s.stride(d), s1 = s.stride(d1), s2 = s.stride(d2);
+    for (int j = 0; j < s.n[d2]; ++j)
+        for (int i = 0; i < s.n[d1]; ++i)
+            out[(long long)j * s.n[d1] + i] = a[idx * sd + i * s1 + j * s2];
+    return out;
+}
+
+void IArr::set(Vec v) {
+    a = std::move(v);
+    if (uninit) {   // Edges(bcModes, array, 0.005) at first assignment (Edges.m:37-110)
+        for (int side = 0; side < 2; ++side)
+            for (int d = 0; d < sim->ndims; ++d) {
+                int mode = sim->bc[cls][side][d];
+                if (mode == TRANS || mode == WALL) {
+                    edges.active[side][d] = true;
+                    edges.store[side][d] = take_face(*sim, a, d, side == 0 ? 0 : sim->n[d] - 1);
+                } else if (mode == FADE) {
+                    edges.active[side][d] = true;
+                }
+            }
+        uninit = false;
+    }
+}
+
+Vec IArr::transparent_edge(int dim, bool upper) {
+    // ImogenArray.transparentEdge -> Edges.getEdge (Edges.m:112-137)
+    int d = dim - 1, side = upper ? 1 : 0;
+    int mode = sim->bc[cls][side][d];
+    if (mode == TRANS) {
+        Vec ne = take_face(*sim, a, d, upper ? sim->n[d] - 1 : 0);
+        Vec& old = edges.store[side][d];
+        for (size_t k = 0; k < ne.size(); ++k) {
+            double delta = std::min(std::fabs(ne[k] - old[k]), edges.tol);
+            bool st = (ne[k] - old[k]) > 0;
+            old[k] = old[k] + ((st ? 1.0 : 0.0) - (st ? 0.0 : 1.0)) * delta;
+        }
+    }
+    return edges.store[side][d];
+}
+
+// 0-based constant-shift source index (constant_shift.m:21-29)
+inline int cidx(int i, int n, int N) { return std::min(std::max(i + n, 0), N - 1); }
+
+Vec IArr::shift(int DIRECT, int n) {
+    const Sim& s = *sim;
+    int d = DIRECT - 1;
+    if (d >= s.ndims) return a;   // ImogenArray.m:159-163 (pShiftEnabled false)
+    int mode = s.bc[cls][n > 0 ? 1 : 0][d];
+    int Nd = s.n[d];
+    int m = std::abs(n);
+    long long sd = s.stride(d);
+    long long nf = s.face(d);
+    int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    long long s1 = s.stride(d1), s2 = s.stride(d2);
+    auto base_of = [&](long long f) { return (f % s.n[d1]) * s1 + (f / s.n[d1]) * s2; };
+    Vec r(s.N);
+
+    if (mode == CIRC) {   // circ_shift.m:21-29
+#pragma omp parallel for schedule(static)
+        for (long long f = 0; f < nf; ++f) {
+            long long b = base_of(f);
+            for (int i = 0; i < Nd; ++i) r[b + i * sd] = a[b + (((i + n) % Nd + Nd) % Nd) * sd];
+        }
+        return r;
+    }
+    if (mode == MIRROR) {   // mirror_shift.m:23-39
+        bool flip = component == DIRECT;
+#pragma omp parallel for schedule(static)
+        for (long long f = 0; f < nf; ++f) {
+            long long b = base_of(f);
+            for (int i = 0; i < Nd; ++i) {
+                int src; bool g = false;
+                if (n < 0) {
+                    if (i >= m) src = i - m; else { src = m - i; g = true; }
+                } else {
+                    if (i < Nd - m) src = i + m; else { src = Nd - 2 - (i - (Nd - m)); g = true; }
+                }
+                double v = a[b + (long long)src * sd];
+                r[b + i * sd] = (g && flip) ? -v : v;
+            }
+        }
+        return r;
+    }
+    // constant shift underlies const / trans / wall / fade
+#pragma omp parallel for schedule(static)
+    for (long long f = 0; f < nf; ++f) {
+        long long b = base_of(f);
+        for (int i = 0; i < Nd; ++i) r[b + i * sd] = a[b + (long long)cidx(i, n, Nd) * sd];
+    }
+    if (mode == CONST) return r;
+
+    if (mode == WALL) {   // wall_shift.m:12-33
+        Vec e = transparent_edge(DIRECT, n > 0);
+        for (long long f = 0; f < nf; ++f) {
+            long long b = base_of(f);
+            for (int k = 0; k < m; ++k) {
+                int gi = n < 0 ? k : Nd - m + k;
+                r[b + (long long)gi * sd] = e[f];
+            }
+        }
+        return r;
+    }
+    if (mode == FADE) {   // fade_shift.m:21-45
+        int fs = s.bc_inf;
+        const Vec& c = s.fade_coeff;
+#pragma omp parallel for schedule(static)
+        for (long long f = 0; f < nf; ++f) {
+            long long b = base_of(f);
+            double anchor = r[b];
+            for (int i = 0; i < fs; ++i) {
+                double& v = r[b + (long long)i * sd];
+                v = (1 - c[i]) * v + c[i] * anchor;
+            }
+            anchor = r[b + (long long)(Nd - 1) * sd];
+            for (int k = 0; k < fs; ++k) {
+                int i = Nd - fs + k;
+                double ck = c[fs - 1 - k];
+                double& v = r[b + (long long)i * sd];
+                v = (1 - ck) * v + ck * anchor;
+            }
+        }
+        return r;
+    }
+    // TRANS: transparent_shift.m:23-99
+    bool act = edges.active[(DIRECT - 1) % 2][(DIRECT - 1) / 2];   // ACTIVE(DIRECT), linear index
+    Vec e;
+    if (act) e = transparent_edge(DIRECT, n > 0);
+    double xk[5] = {1, 2, 3, double(s.bc_inf), double(s.bc_inf + 1)};
+    double xe[2];
+    for (int k = 0; k < m; ++k) xe[k] = n < 0 ? 3 + (m - k) : 3 + (k + 1);
+    for (long long f = 0; f < nf; ++f) {
+        long long b = base_of(f);
+        double y[5];
+        for (int q = 0; q < 3; ++q) {
+            int pick = n < 0 ? std::min(3 - q + m, Nd) - 1 : std::max(Nd - (2 - q) - m, 1) - 1;
+            y[q] = r[b + (long long)pick * sd];
+        }
+        y[3] = act ? e[f] : 0.0;
+        y[4] = y[3];
+        double out[2];
+        pchip_col(xk, 5, y, xe, m, out);
+        for (int k = 0; k < m; ++k) {
+            int gi = n < 0 ? k : Nd - m + k;
+            double orig = a[b + (long long)gi * sd];
+            bool t = std::fabs(orig - out[k]) < 1e-4;
+            r[b + (long long)gi * sd] = (t ? 0.0 : 1.0) * out[k] + (t ? 1.0 : 0.0) * orig;
+        }
+    }
+    return r;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Limiters (flux/*Limiter.m): flux.array = flux.array + correction
+// ------------------------------------------------------------------------------------------------
+void apply_limiter(int lim, IArr& fl, const Vec& dL, const Vec& dR) {
+    Vec out(fl.a.size());
+    long long N = (long long)out.size();
+    if (lim == VANLEER) {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i) {
+            double p = dL[i] * dR[i];
+            double st = (p > 0 ? p : 0.0) / (dL[i] + dR[i]);
+            if (std::isnan(st)) st = 0.0;
+            out[i] = fl.a[i] + st;
+        }
+    } else {
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i) {
+            double l = dL[i], r = dR[i];
+            if (lim == SUPERBEE) {
+                double c = std::fabs(l) < std::fabs(r) ? 1.0 : 0.0;
+                l = (1 + c) * l;
+                r = (2 - c) * r;
+            }
+            double corr = 0.125 * (msign(l) + msign(r)) * std::fmin(std::fabs(l), std::fabs(r));
+            out[i] = fl.a[i] + corr;
+        }
+    }
+    fl.set(std::move(out));
+}
+
+// pressure.m:16-66 (modes used on the hot path: totsnd, sound)
+void pressure(Sim& s, bool sound_mode, const Vec& rho, const Vec& px, const Vec& py, const Vec& pz,
+              const Vec& E, Vec& result, Vec* aux) {
+    const double G = s.gamma;
+    long long N = s.N;
+    result.assign(N, 0.0);
+    if (aux) aux->assign(N, 0.0);
+    const Vec* cm[3] = {&s.mg[0].cellMag.a, &s.mg[1].cellMag.a, &s.mg[2].cellMag.a};
+    bool use[3] = {!s.mg[0].isZero, !s.mg[1].isZero, !s.mg[2].isZero};
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < N; ++i) {
+        double vsq = (px[i] * px[i] + py[i] * py[i] + pz[i] * pz[i]) / (rho[i] * rho[i]);
+        double msq = 0.0;
+        for (int c = 0; c < 3; ++c)
+            if (use[c]) msq = msq + (*cm[c])[i] * (*cm[c])[i];
+        double r = (G - 1.0) * (E[i] - 0.5 * rho[i] * vsq);
+        if (!sound_mode) {
+            (*aux)[i] = std::sqrt(std::fabs((G * (r - (G - 1.0) * 0.5 * msq) + 2.0 * msq) / rho[i]));
+            r = r + 0.5 * (2.0 - G) * msq;
+        } else {
+            r = r - (G - 1.0) * 0.5 * msq;
+            r = std::sqrt(std::fabs((G * r + 2.0 * msq) / rho[i]));
+        }
+        result[i] = r < 0 ? 0.0 : r;
+    }
+}
+
+// wFluidFlux.m:14-44
+void w_fluid_flux(Sim& s, const Vec* u[5], int X, Vec& freeze, Vec w[5]) {
+    int d = X - 1;
+    long long N = s.N;
+    Vec press, sound;
+    pressure(s, false, *u[0], *u[1], *u[2], *u[3], *u[4], press, &sound);
+    Vec spd_line(s.face(d));
+    long long sd = s.stride(d);
+    int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    long long s1 = s.stride(d1), s2 = s.stride(d2);
+    const Vec& mom_d = *u[1 + d];
+    const Vec& rho = *u[0];
+#pragma omp parallel for schedule(static)
+    for (long long f = 0; f < s.face(d); ++f) {
+        long long b = (f % s.n[d1]) * s1 + (f / s.n[d1]) * s2;
+        double mx = std::numeric_limits<double>::quiet_NaN();
+        for (int i = 0; i < s.n[d]; ++i) {
+            long long q = b + i * sd;
+            double v = std::fabs(mom_d[q] / rho[q]) + sound[q];
+            if (std::isnan(mx) || v > mx) mx = std::isnan(v) ? mx : v;
+        }
+        spd_line[f] = mx;
+    }
+    freeze.assign(N, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long long f = 0; f < s.face(d); ++f) {
+        long long b = (f % s.n[d1]) * s1 + (f / s.n[d1]) * s2;
+        for (int i = 0; i < s.n[d]; ++i) freeze[b + i * sd] = spd_line[f];
+    }
+    const Vec* cm[3] = {&s.mg[0].cellMag.a, &s.mg[1].cellMag.a, &s.mg[2].cellMag.a};
+    for (int k = 0; k < 5; ++k) w[k].assign(N, 0.0);
+#pragma omp parallel for schedule(static)
+    for (long long i = 0; i < N; ++i) {
+        double fz = freeze[i];
+        double velocity = mom_d[i] / rho[i];
+        double press_i = press[i] + 0.0;   // viscosity.solve -> 0 ('empty')
+        double cx = (*cm[d])[i];
+        w[0][i] = (*u[1 + d])[i] / fz;
+        double we = velocity * ((*u[4])[i] + press_i) -
+                    cx * ((*cm[0])[i] * (*u[1])[i] + (*cm[1])[i] * (*u[2])[i] + (*cm[2])[i] * (*u[3])[i]) / rho[i];
+        w[4][i] = we / fz;
+        for (int c = 0; c < 3; ++c) {
+            double dirv = c == d ? 1.0 : 0.0;
+            w[1 + c][i] = (velocity * (*u[1 + c])[i] + press_i * dirv - cx * (*cm[c])[i]) / fz;
+        }
+    }
+}
+
+// relaxingFluid.m:16-73
+void relaxing_fluid(Sim& s, int X) {
+    long long N = s.N;
+    double ff = s.dt / s.dgrid[X - 1];
+    Vec freeze, w[5];
+    const Vec* u[5] = {&s.fv[0].prim.a, &s.fv[1].prim.a, &s.fv[2].prim.a, &s.fv[3].prim.a, &s.fv[4].prim.a};
+    w_fluid_flux(s, u, X, freeze, w);
+    for (int k = 0; k < 5; ++k) {
+        auto& v = s.fv[k];
+        Vec R(N), L(N);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i) {
+            R[i] = 0.5 * (v.prim.a[i] + w[k][i]);
+            L[i] = 0.5 * (v.prim.a[i] - w[k][i]);
+        }
+        v.store_fluxR.set(std::move(R));
+        v.store_fluxL.set(std::move(L));
+        Vec Rm = v.store_fluxR.shift(X, -1);
+        Vec Lp = v.store_fluxL.shift(X, 1);
+        Vec st(N);
+        const Vec &Ra = v.store_fluxR.a, &La = v.store_fluxL.a;
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i)
+            st[i] = v.prim.a[i] - 0.5 * ff * freeze[i] * (Ra[i] - Rm[i] + La[i] - Lp[i]);
+        v.store.set(std::move(st));
+        v.store_fluxR.cleanup();
+        v.store_fluxL.cleanup();
+    }
+    {
+        Vec m(N);
+        for (long long i = 0; i < N; ++i) m[i] = std::max(s.fv[0].store.a[i], s.minmass);
+        s.fv[0].store.set(std::move(m));
+    }
+    const Vec* us[5] = {&s.fv[0].store.a, &s.fv[1].store.a, &s.fv[2].store.a, &s.fv[3].store.a, &s.fv[4].store.a};
+    w_fluid_flux(s, us, X, freeze, w);
+    int lim = s.limiter[X - 1];
+    for (int k = 0; k < 5; ++k) {
+        auto& v = s.fv[k];
+        Vec R(N), L(N);
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i) {
+            R[i] = 0.5 * (v.store.a[i] + w[k][i]);
+            L[i] = 0.5 * (v.store.a[i] - w[k][i]);
+        }
+        v.fluxR.set(std::move(R));
+        v.fluxL.set(std::move(L));
+        {
+            Vec m1 = v.fluxR.shift(X, -1);
+            Vec p1 = v.fluxR.shift(X, 1);
+            Vec dL(N), dR(N);
+            for (long long i = 0; i < N; ++i) { dL[i] = v.fluxR.a[i] - m1[i]; dR[i] = p1[i] - v.fluxR.a[i]; }
+            apply_limiter(lim, v.fluxR, dL, dR);
+        }
+        {
+            Vec m1 = v.fluxL.shift(X, -1);
+            Vec p1 = v.fluxL.shift(X, 1);
+            Vec dL(N), dR(N);
+            for (long long i = 0; i < N; ++i) { dL[i] = m1[i] - v.fluxL.a[i]; dR[i] = v.fluxL.a[i] - p1[i]; }
+            apply_limiter(lim, v.fluxL, dL, dR);
+        }
+        Vec Rm = v.fluxR.shift(X, -1);
+        Vec Lp = v.fluxL.shift(X, 1);
+        Vec nv(N);
+        const Vec &Ra = v.fluxR.a, &La = v.fluxL.a;
+#pragma omp parallel for schedule(static)
+        for (long long i = 0; i < N; ++i)
+            nv[i] = v.prim.a[i] - ff * freeze[i] * (Ra[i] - Rm[i] + La[i] - Lp[i]);
+        v.prim.set(std::move(nv));
+        v.fluxR.cleanup();
+        v.fluxL.cleanup();
+    }
+    {
+        Vec m(N);
+        for (long long i = 0; i < N; ++i) m[i] = std::max(s.fv[0].prim.a[i], s.minmass);
+        s.fv[0].prim.set(std::move(m));
+    }
+}
+
+// relaxingMagnet.m:15-60
+void relaxing_magnet(Sim& s, int X, int I, IArr& vg) {
+    long long N = s.N;
+    auto& m = s.mg[I - 1];
+    double ff = 0.5 * s.dt / s.dgrid[X - 1];
+    Vec vgp = vg.shift(X, 1);
+    Vec vf(N);
+    for (long long i = 0; i < N; ++i) vf[i] = (vg.a[i] + vgp[i]) < 0.0 ? 1.0 : 0.0;
+
+    IArr& sfr = m.store_fluxR[X];
+    {
+        Vec F(N);
+        for (long long i = 0; i < N; ++i) F[i] = m.prim.a[i] * vg.a[i];
+        sfr.set(std::move(F));
+        Vec Fp = sfr.shift(X, 1);
+        Vec G(N);
+        for (long long i = 0; i < N; ++i) G[i] = sfr.a[i] * (1 - vf[i]) + Fp[i] * vf[i];
+        sfr.set(std::move(G));
+        Vec Fm = sfr.shift(X, -1);
+        Vec st(N);
+        for (long long i = 0; i < N; ++i) st[i] = m.prim.a[i] - ff * (sfr.a[i] - Fm[i]);
+        m.store[X].set(std::move(st));
+    }
+    ff = 2 * ff;
+    IArr& wm = m.wMag[X];
+    {
+        Vec W(N);
+        for (long long i = 0; i < N; ++i) W[i] = m.store[X].a[i] * vg.a[i];
+        wm.set(std::move(W));
+    }
+    IArr& fx = m.flux[X];
+    Vec dFluxR(N), dFluxL(N);
+    {
+        Vec Wp = wm.shift(X, 1);
+        Vec F(N);
+        for (long long i = 0; i < N; ++i) F[i] = wm.a[i] * (1 - vf[i]) + Wp[i] * vf[i];
+        fx.set(std::move(F));
+        Vec Wp1 = wm.shift(X, 1);
+        Vec Wp2 = wm.shift(X, 2);
+        for (long long i = 0; i < N; ++i) dFluxR[i] = Wp1[i] - (vf[i] * Wp2[i] + (1 - vf[i]) * wm.a[i]);
+        Vec Wq1 = wm.shift(X, 1);
+        Vec Wm1 = wm.shift(X, -1);
+        for (long long i = 0; i < N; ++i) dFluxL[i] = wm.a[i] - (vf[i] * Wq1[i] + (1 - vf[i]) * Wm1[i]);
+    }
+    apply_limiter(s.limiter[X - 1], fx, dFluxL, dFluxR);
+    {
+        Vec Fm = fx.shift(X, -1);
+        Vec B(N);
+        for (long long i = 0; i < N; ++i) B[i] = m.prim.a[i] - ff * (fx.a[i] - Fm[i]);
+        m.prim.set(std::move(B));
+    }
+    ff = s.dt / s.dgrid[I - 1];
+    {
+        Vec Fp = fx.shift(I, 1);
+        Vec C(N);
+        for (long long i = 0; i < N; ++i) C[i] = fx.a[i] - Fp[i];
+        fx.set(std::move(C));
+        Vec Cm = fx.shift(X, -1);
+        fx.set(std::move(Cm));
+        IArr& bx = s.mg[X - 1].prim;
+        Vec B(N);
+        for (long long i = 0; i < N; ++i) B[i] = bx.a[i] - ff * fx.a[i];
+        bx.set(std::move(B));
+    }
+}
+
+void update_cell_centered(Sim& s, int c) {   // MagnetArray.m:36-38
+    auto& m = s.mg[c - 1];
+    Vec sh = m.prim.shift(c, 1);
+    Vec out(s.N);
+    for (long long i = 0; i < s.N; ++i) out[i] = 0.5 * (m.prim.a[i] + sh[i]);
+    m.cellMag.set(std::move(out));
+}
+
+// magnetFlux.m:14-31
+void magnet_flux(Sim& s, int X, int I1, int I2) {
+    long long N = s.N;
+    int I = I1;
+    for (int q = 0; q < 2; ++q) {
+        I = q == 0 ? I1 : I2;
+        auto& m = s.mg[I - 1];
+        IArr& vg = m.velGrid[X];
+        IArr& momX = s.fv[X].prim;
+        IArr& mass = s.fv[0].prim;
+        Vec pm = momX.shift(I, -1);
+        Vec rm = mass.shift(I, -1);
+        Vec v(N);
+        for (long long i = 0; i < N; ++i) v[i] = (pm[i] + momX.a[i]) / (rm[i] + mass.a[i]);
+        vg.set(std::move(v));
+        Vec a = vg.shift(X, -1);
+        Vec b = vg.shift(X, 1);
+        Vec sm(N);
+        for (long long i = 0; i < N; ++i) sm[i] = 0.25 * (a[i] + b[i] + 2 * vg.a[i]);
+        vg.set(std::move(sm));
+        relaxing_magnet(s, X, I, vg);
+        vg.cleanup(); m.store[X].cleanup(); m.store_fluxR[X].cleanup(); m.wMag[X].cleanup(); m.flux[X].cleanup();
+    }
+    update_cell_centered(s, I);
+    update_cell_centered(s, X);
+}
+
+// flux.m:17-62
+void flux(Sim& s, int order) {
+    int row = (s.iteration - 1) % 6;
+    for (int q = 0; q < 3; ++q) {
+        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        if (s.n[X - 1] < 3) continue;
+        if (order > 0) {
+            if (s.fluid_active) relaxing_fluid(s, X);
+            if (s.magnet_active) magnet_flux(s, X, FWD_MI[X - 1][0], FWD_MI[X - 1][1]);
+        } else {
+            if (s.magnet_active) magnet_flux(s, X, BWD_MI[X - 1][0], BWD_MI[X - 1][1]);
+            if (s.fluid_active) relaxing_fluid(s, X);
+        }
+    }
+}
+
+// TimeManager.update (TimeManager.m:55-99); returns 0 or -1 on a CFL error
+int time_update(Sim& s, int flux_direction) {
+    if (flux_direction > 1 && s.update_mode != 0) return 0;
+    double cmax = 1e-2;
+    int gi = 0;
+    Vec snd;
+    pressure(s, true, s.fv[0].prim.a, s.fv[1].prim.a, s.fv[2].prim.a, s.fv[3].prim.a, s.fv[4].prim.a, snd, nullptr);
+    for (int i = 0; i < 3; ++i) {
+        const Vec& p = s.fv[1 + i].prim.a;
+        const Vec& r = s.fv[0].prim.a;
+        double c = std::numeric_limits<double>::quiet_NaN();
+        for (long long k = 0; k < s.N; ++k) {
+            double v = std::fabs(p[k] / r[k]) + snd[k];
+            if (!std::isnan(v) && (std::isnan(c) || v > c)) c = v;
+        }
+        if (c > cmax) { cmax = c; gi = i + 1; }
+    }
+    s.last_cmax = cmax;
+    s.last_grid_index = gi;
+    if (gi < 1) return -1;
+    s.dt = s.cfl * s.dgrid[gi - 1] / cmax;
+    double nt = s.time + (s.update_mode + 1) * s.dt;
+    if (nt > s.time_max) {
+        s.dt = (s.time_max - s.time) / (s.update_mode + 1);
+        nt = s.time_max;
+    }
+    s.time = nt;
+    return 0;
+}
+
+bool running(const Sim& s) { return s.iteration <= s.iter_max && s.time < s.time_max; }
+
+int iterate(Sim& s) {
+    for (int i = 1; i <= 2; ++i) {
+        if (time_update(s, i) != 0) return -1;
+        flux(s, i == 1 ? 1 : -1);
+    }
+    s.iteration += 1;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* orc_create(const int grid[3], const double dgrid[3], double gamma, double cfl, double minmass,
+                 const int* bc /*[4][2][3]*/, int bc_infinity, const int limiter[3], int fluid_active,
+                 int magnet_active, double time_max, int iter_max, int update_mode) {
+    auto* s = new Sim();
+    for (int d = 0; d < 3; ++d) { s->n[d] = grid[d]; s->dgrid[d] = dgrid[d]; s->limiter[d] = limiter[d]; }
+    s->N = (long long)grid[0] * grid[1] * grid[2];
+    s->ndims = grid[2] > 1 ? 3 : 2;
+    s->gamma = gamma; s->cfl = cfl; s->minmass = minmass;
+    std::memcpy(s->bc, bc, sizeof(s->bc));
+    s->bc_inf = bc_infinity;
+    {
+        int f = bc_infinity;
+        double xk[5] = {0, std::ceil(f / 4.0), std::floor(f / 2.0 + 0.5), double(f - 1), double(f)};
+        double yk[5] = {1, 1, 0.01, 0, 0};
+        std::vector<double> xi(f);
+        for (int i = 0; i < f; ++i) xi[i] = i + 1;
+        s->fade_coeff.assign(f, 0.0);
+        pchip_col(xk, 5, yk, xi.data(), f, s->fade_coeff.data());
+    }
+    // mirror_shift.m:31-33 and fade_shift.m:34-44 / Edges.m:80-93 index outside short dimensions:
+    // the reference stops there, so such settings are rejected.
+    for (int c = 0; c < 4; ++c)
+        for (int side = 0; side < 2; ++side)
+            for (int d = 0; d < s->ndims; ++d) {
+                int mode = s->bc[c][side][d];
+                bool bad = mode < 0 || mode > 5 || (mode == MIRROR && grid[d] < 2) ||
+                           (mode == FADE && grid[d] < std::max(20, bc_infinity));
+                if (bad) { delete s; return nullptr; }
+            }
+    s->fluid_active = fluid_active != 0;
+    s->magnet_active = magnet_active != 0;
+    s->time_max = time_max; s->iter_max = iter_max; s->update_mode = update_mode;
+    const int cls[5] = {C_MASS, C_MOM, C_MOM, C_MOM, C_ENER};
+    const int comp[5] = {0, 1, 2, 3, 0};
+    for (int k = 0; k < 5; ++k) {
+        auto& v = s->fv[k];
+        for (IArr* A : {&v.prim, &v.store, &v.store_fluxR, &v.store_fluxL, &v.fluxR, &v.fluxL})
+            s->init_arr(*A, comp[k], cls[k]);
+    }
+    for (int c = 0; c < 3; ++c) {
+        auto& m = s->mg[c];
+        s->init_arr(m.prim, c + 1, C_MAG);
+        s->init_arr(m.cellMag, c + 1, C_MAG);
+        for (int X = 1; X <= 3; ++X)
+            for (IArr* A : {&m.velGrid[X], &m.store[X], &m.store_fluxR[X], &m.wMag[X], &m.flux[X]})
+                s->init_arr(*A, c + 1, C_MAG);
+    }
+    return s;
+}
+
+void orc_destroy(void* p) { delete static_cast<Sim*>(p); }
+
+int orc_set_state(void* p, const double* mass, const double* mom, const double* ener, const double* mag) {
+    Sim& s = *static_cast<Sim*>(p);
+    long long N = s.N;
+    s.fv[0].prim.set(Vec(mass, mass + N));
+    for (int c = 0; c < 3; ++c) s.fv[1 + c].prim.set(Vec(mom + c * N, mom + (c + 1) * N));
+    s.fv[4].prim.set(Vec(ener, ener + N));
+    for (int c = 0; c < 3; ++c) {
+        s.mg[c].prim.set(Vec(mag + c * N, mag + (c + 1) * N));
+        update_cell_centered(s, c + 1);
+    }
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0;
+        for (long long i = 0; i < N; ++i) sum += s.mg[c].prim.a[i];
+        s.mg[c].isZero = (sum == 0) && !s.magnet_active;
+    }
+    return 0;
+}
+
+int orc_get_state(void* p, double* mass, double* mom, double* ener, double* mag, double* cellmag) {
+    Sim& s = *static_cast<Sim*>(p);
+    long long N = s.N;
+    if (mass) std::copy(s.fv[0].prim.a.begin(), s.fv[0].prim.a.end(), mass);
+    if (ener) std::copy(s.fv[4].prim.a.begin(), s.fv[4].prim.a.end(), ener);
+    for (int c = 0; c < 3; ++c) {
+        if (mom) std::copy(s.fv[1 + c].prim.a.begin(), s.fv[1 + c].prim.a.end(), mom + c * N);
+        if (mag) std::copy(s.mg[c].prim.a.begin(), s.mg[c].prim.a.end(), mag + c * N);
+        if (cellmag) std::copy(s.mg[c].cellMag.a.begin(), s.mg[c].cellMag.a.end(), cellmag + c * N);
+    }
+    return 0;
+}
+
+int orc_time_update(void* p, int flux_direction) { return time_update(*static_cast<Sim*>(p), flux_direction); }
+int orc_flux(void* p, int order) { flux(*static_cast<Sim*>(p), order); return 0; }
+int orc_relaxing_fluid(void* p, int X) { relaxing_fluid(*static_cast<Sim*>(p), X); return 0; }
+int orc_magnet_flux(void* p, int X, int I1, int I2) { magnet_flux(*static_cast<Sim*>(p), X, I1, I2); return 0; }
+int orc_iterate(void* p) { return iterate(*static_cast<Sim*>(p)); }
+
+int orc_run(void* p, int max_iterations) {
+    Sim& s = *static_cast<Sim*>(p);
+    int n = 0;
+    while (running(s) && (max_iterations < 0 || n < max_iterations)) {
+        if (iterate(s) != 0) return -1 - n;
+        ++n;
+    }
+    return n;
+}
+
+void orc_get_time(void* p, double* time, double* dt, int* iteration) {
+    Sim& s = *static_cast<Sim*>(p);
+    if (time) *time = s.time;
+    if (dt) *dt = s.dt;
+    if (iteration) *iteration = s.iteration;
+}
+
+void orc_set_time(void* p, double time, double dt, int iteration) {
+    Sim& s = *static_cast<Sim*>(p);
+    s.time = time; s.dt = dt; s.iteration = iteration;
+}
+
+void orc_get_cfl(void* p, double* cmax, int* grid_index) {
+    Sim& s = *static_cast<Sim*>(p);
+    *cmax = s.last_cmax; *grid_index = s.last_grid_index;
+}
+
+int orc_pchip(const double* x, int n, const double* y, int ncols, const double* xi, int m, double* out) {
+    for (int c = 0; c < ncols; ++c) pchip_col(x, n, y + (long long)c * n, xi, m, out + (long long)c * m);
+    return 0;
+}
+
+void orc_set_threads(int t) {
+#ifdef _OPENMP
+    if (t > 0) omp_set_num_threads(t);
+#else
+    (void)t;
+#endif
+}
+
+int orc_max_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"
