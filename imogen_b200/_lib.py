@@ -1,0 +1,101 @@
+"""ctypes binding of libimogen_b200.so (the C ABI declared in include/imogen_b200.h).
+
+The library is built in-tree (imogen_b200/build.py).  There is no fallback: if the shared library
+is missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libimogen_b200.so")
+
+# status codes (include/imogen_b200.h)
+IMG_OK = 0
+STATUS = {
+    -1: "IMG_ERR_ARG", -2: "IMG_ERR_CUDA", -3: "IMG_ERR_NOMEM", -4: "IMG_ERR_UNSUPPORTED",
+    -5: "IMG_ERR_CFL", -6: "IMG_ERR_NONFINITE", -7: "IMG_ERR_STATE",
+}
+
+# exported symbols, in header order
+SYMBOLS = (
+    "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
+    "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
+    "img_get_time", "img_set_time", "img_totals", "img_sync", "img_last_error", "img_bytes_required",
+)
+
+
+class ImgConfig(ctypes.Structure):
+    _fields_ = [
+        ("grid", ctypes.c_int * 3),
+        ("dgrid", ctypes.c_double * 3),
+        ("gamma", ctypes.c_double),
+        ("cfl", ctypes.c_double),
+        ("minmass", ctypes.c_double),
+        ("bc_infinity", ctypes.c_int),
+        ("bc_modes", ((ctypes.c_int * 3) * 2) * 4),
+        ("limiter", ctypes.c_int * 3),
+        ("fluid_active", ctypes.c_int),
+        ("magnet_active", ctypes.c_int),
+        ("time_max", ctypes.c_double),
+        ("iter_max", ctypes.c_int),
+        ("update_mode", ctypes.c_int),
+        ("precision", ctypes.c_int),
+    ]
+
+
+class ImogenError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+
+def lib():
+    """Load libimogen_b200.so (building it first if it is absent and nvcc is available)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        from . import build
+        build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    cfgp = ctypes.POINTER(ImgConfig)
+    L.img_config_default.argtypes = [cfgp]
+    L.img_config_default.restype = None
+    L.img_create.argtypes = [ctypes.POINTER(vp), cfgp]
+    L.img_destroy.argtypes = [vp]
+    L.img_set_state.argtypes = [vp, dp, dp, dp, dp]
+    L.img_upload.argtypes = [vp, ctypes.c_int, dp, ctypes.c_size_t]
+    L.img_download.argtypes = [vp, ctypes.c_int, dp, ctypes.c_size_t]
+    L.img_time_update.argtypes = [vp, ctypes.c_int, dp, ip]
+    L.img_flux.argtypes = [vp, ctypes.c_int]
+    L.img_fluid_sweep.argtypes = [vp, ctypes.c_int]
+    L.img_magnet_sweep.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.img_step.argtypes = [vp]
+    L.img_run.argtypes = [vp, ctypes.c_int, ip]
+    L.img_get_time.argtypes = [vp, dp, dp, ip]
+    L.img_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+    L.img_totals.argtypes = [vp, dp]
+    L.img_sync.argtypes = [vp]
+    L.img_last_error.argtypes = [vp]
+    L.img_last_error.restype = ctypes.c_char_p
+    L.img_bytes_required.argtypes = [cfgp]
+    L.img_bytes_required.restype = ctypes.c_size_t
+    for name in ("img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
+                 "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step",
+                 "img_run", "img_get_time", "img_set_time", "img_totals", "img_sync"):
+        getattr(L, name).restype = ctypes.c_int
+    _LIB = L
+    return L
+
+
+def check(rc, ctx=None):
+    if rc != IMG_OK:
+        msg = lib().img_last_error(ctx)
+        raise ImogenError(rc, msg.decode() if msg else "")
+    return rc

@@ -1,0 +1,172 @@
+// Device-side TimeManager.update (time/TimeManager.m:55-99) and state construction helpers.
+//
+// The CFL maxima max_cells(|p_i/rho| + c_s) for i = 1..3 are accumulated into DevTime::maxbits,
+// either by the last fluid sweep of the previous step (fused epilogue) or by cfl_reduce_kernel.
+// cfl_finalize_kernel then applies the 1e-2 floor, the first-strictly-larger argmax, the CFL
+// formula with MINDGRID(gridIndex), and the TIMEMAX clamp, all on the device, so a step never
+// waits for the host.
+#pragma once
+
+#include "magnet_sweep.cuh"
+
+namespace img {
+
+struct CflArgs {
+    Geom g;
+    const void* q[NQ];
+    DevTime* tm;
+    double gamma;
+    int mhd;
+    int use_b[3];
+};
+
+template <typename T>
+__global__ void cfl_reduce_kernel(const CflArgs a) {
+    if (a.tm->done || a.tm->error) return;
+    const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
+    const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
+                     reinterpret_cast<const T*>(a.q[Q_PZ])};
+    const T* E = reinterpret_cast<const T*>(a.q[Q_E]);
+    const T* cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
+                      reinterpret_cast<const T*>(a.q[Q_CBZ])};
+    double m3[3] = {0.0, 0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
+         i += (long long)gridDim.x * blockDim.x) {
+        double r = rho[i], px = p[0][i], py = p[1][i], pz = p[2][i];
+        double msq = 0.0;
+        if (a.mhd) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (a.use_b[c]) { double b = cb[c][i]; msq = msq + b * b; }
+        }
+        double cs = sound_speed(a.gamma, r, px, py, pz, (double)E[i], msq);
+        m3[0] = fmax(m3[0], fabs(px / r) + cs);
+        m3[1] = fmax(m3[1], fabs(py / r) + cs);
+        m3[2] = fmax(m3[2], fabs(pz / r) + cs);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        for (int o = 16; o > 0; o >>= 1) m3[c] = fmax(m3[c], __shfl_xor_sync(0xffffffffu, m3[c], o));
+        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&a.tm->maxbits[c], m3[c]);
+    }
+}
+
+// check_running: evaluate TimeManager.running (time < TIMEMAX) first, as imogen.m:58 does at the
+// top of each iteration; the iteration limit is enforced by the host.
+__global__ void cfl_finalize_kernel(DevTime* tm, int check_running) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (tm->done || tm->error) return;
+    if (check_running && !(tm->time < tm->time_max)) {
+        tm->done = 1;
+        return;
+    }
+    double cmax = 1e-2;
+    int gi = 0;
+    for (int i = 0; i < 3; ++i) {
+        double c = __longlong_as_double((long long)tm->maxbits[i]);
+        tm->maxbits[i] = 0ull;
+        if (c > cmax) { cmax = c; gi = i + 1; }
+    }
+    tm->cmax = cmax;
+    tm->grid_index = gi;
+    if (gi < 1) {   // TimeManager.m:79-86 (fireCFLError)
+        tm->error |= DERR_CFL;
+        return;
+    }
+    double dt = tm->cfl * tm->dgrid[gi - 1] / cmax;
+    double nt = tm->time + (tm->update_mode + 1) * dt;
+    if (nt > tm->time_max) {
+        dt = (tm->time_max - tm->time) / (tm->update_mode + 1);
+        nt = tm->time_max;
+    }
+    if (!isfinite(dt)) {
+        tm->error |= DERR_NONFINITE_DT;
+        return;
+    }
+    tm->dt = dt;
+    tm->time = nt;
+}
+
+// MagnetArray construction: cellMag = 0.5*(B + B.shift(component, +1)) (MagnetArray.m:36-38,41-49).
+struct CellMagInitArgs {
+    Geom g;
+    void* q[NQ];
+    int mode_hi[3];      // mag-class upper BC along dim c for component c
+    int act[3];
+    const EdgeTable* edges;
+    const double* fade;
+    int fade_f;
+    double bc_inf;
+};
+
+template <typename T>
+__global__ void cellmag_init_kernel(const CellMagInitArgs a) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3 * a.g.ncell;
+         i += (long long)gridDim.x * blockDim.x) {
+        int cpt = (int)(i / a.g.ncell);
+        long long cell = i - cpt * a.g.ncell;
+        const T* B = reinterpret_cast<const T*>(a.q[Q_BX + cpt]);
+        T* CB = reinterpret_cast<T*>(a.q[Q_CBX + cpt]);
+        int x, y, z;
+        cell_coords(a.g, cell, x, y, z);
+        T sh;
+        if (cpt < a.g.ndims) {
+            bool own = sel3(cpt, x, y, z) == a.g.n[cpt] - 1;
+            sh = shift_along<T>(a.g, B, cell, x, y, z, cpt, +1, a.mode_hi[cpt], a.act[cpt], true,
+                                a.edges->p[OBJ_PRIM_MAG + cpt][cpt][1], a.fade, a.fade_f, a.bc_inf, own);
+        } else {
+            sh = B[cell];
+        }
+        CB[cell] = T(0.5) * (B[cell] + sh);
+    }
+}
+
+// Neumaier-compensated FP64 totals of the conserved variables (rho, px, py, pz, E, Bx, By, Bz):
+// one partial (sum, compensation) pair per block and variable; the host finishes the sum.
+template <typename T>
+__global__ void totals_kernel(Geom g, const void* const* qp, double* partial) {
+    __shared__ double ss[8][32], cc[8][32];
+    double s[8], c[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) { s[v] = 0.0; c[v] = 0.0; }
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < g.ncell;
+         i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+            double x = (double)reinterpret_cast<const T*>(qp[v])[i];
+            double t = s[v] + x;
+            c[v] += fabs(s[v]) >= fabs(x) ? (s[v] - t) + x : (x - t) + s[v];
+            s[v] = t;
+        }
+    }
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+        // warp: pairwise Neumaier combine
+        for (int o = 16; o > 0; o >>= 1) {
+            double so = __shfl_xor_sync(0xffffffffu, s[v], o);
+            double co = __shfl_xor_sync(0xffffffffu, c[v], o);
+            double t = s[v] + so;
+            double e = fabs(s[v]) >= fabs(so) ? (s[v] - t) + so : (so - t) + s[v];
+            s[v] = t;
+            c[v] = c[v] + co + e;
+        }
+        if (lane == 0) { ss[v][w] = s[v]; cc[v][w] = c[v]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 8) {
+        int v = threadIdx.x;
+        double S = 0.0, Cc = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            double x = ss[v][k];
+            double t = S + x;
+            Cc += fabs(S) >= fabs(x) ? (S - t) + x : (x - t) + S;
+            S = t;
+            Cc += cc[v][k];
+        }
+        partial[(blockIdx.x * 8 + v) * 2] = S;
+        partial[(blockIdx.x * 8 + v) * 2 + 1] = Cc;
+    }
+}
+
+}  // namespace img

@@ -1,0 +1,212 @@
+// Shared device-side definitions for the relaxing-TVD sweep kernels.
+//
+// State layout in HBM: structure of arrays, one array per variable, x fastest (the MATLAB
+// column-major order of the reference), each array 256-byte aligned.  The eleven arrays are
+// rho, px, py, pz, E, the face-centred B (Bx, By, Bz; B_i(i) lives on face i-1/2,
+// magnet/MagnetArray.m:36-38) and the cell-centred B used by the fluid (cBx, cBy, cBz).  The
+// cell-centred copy is state, not a derived quantity: magnet/magnetFlux.m:30-31 refreshes only
+// two of its three components per sweep, so one component is a step stale by design.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace img {
+
+namespace cg = cooperative_groups;
+
+// ---- enumerations shared with the host (values match include/imogen_b200.h) --------------------
+enum BcMode { BC_CIRC = 0, BC_CONST = 1, BC_FADE = 2, BC_MIRROR = 3, BC_TRANS = 4, BC_WALL = 5 };
+enum Limiter { LIM_VANLEER = 0, LIM_SUPERBEE = 1, LIM_MINMOD = 2 };
+enum BcClass { CLS_MASS = 0, CLS_MOM = 1, CLS_ENER = 2, CLS_MAG = 3 };
+enum Var { Q_RHO = 0, Q_PX, Q_PY, Q_PZ, Q_E, Q_BX, Q_BY, Q_BZ, Q_CBX, Q_CBY, Q_CBZ, NQ };
+
+// Error bits written by kernels into DevTime::error (host reads them after a step).
+enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2, DERR_GEOMETRY = 4 };
+
+// ---- stored-edge objects ------------------------------------------------------------------------
+// Every array object of the reference that can be shifted under a stateful BC (trans, wall) owns a
+// stored edge per (dim, side) (shifting/Edges.m).  Object ids:
+//   fluid var v (0..4: rho,px,py,pz,E) x {store.fluxR, store.fluxL, fluxR, fluxL}: v*4 + k
+//   primary mass, mom(1..3), mag(1..3):                                   20, 21+c, 24+c
+//   mag(c) scratch for sweep dim X (c != X) x {velGrid, store.fluxR, wMag, flux}:
+//                                                                   27 + (c*3+X)*4 + k
+constexpr int OBJ_FLUID = 0;
+constexpr int OBJ_PRIM_MASS = 20;
+constexpr int OBJ_PRIM_MOM = 21;
+constexpr int OBJ_PRIM_MAG = 24;
+constexpr int OBJ_MAG = 27;
+constexpr int NOBJ = 27 + 36;
+enum FluidObj { FO_STORE_R = 0, FO_STORE_L = 1, FO_R = 2, FO_L = 3 };
+enum MagObj { MO_VELGRID = 0, MO_STORE_R = 1, MO_WMAG = 2, MO_FLUX = 3 };
+__host__ __device__ constexpr int fluid_obj(int v, int k) { return OBJ_FLUID + v * 4 + k; }
+__host__ __device__ constexpr int mag_obj(int c, int X, int k) { return OBJ_MAG + (c * 3 + X) * 4 + k; }
+
+// Table of stored-edge slices: edge[obj][dim][side] -> face array (double) or nullptr.
+struct EdgeTable {
+    double* p[NOBJ][3][2];
+};
+
+// ---- device-resident time manager (time/TimeManager.m:55-99) ------------------------------------
+struct DevTime {
+    double time;
+    double dt;
+    double time_max;
+    double cfl;
+    double dgrid[3];
+    double cmax;            // last CFL max (after the 1e-2 floor)
+    int grid_index;         // 1-based argmax direction of the last CFL
+    int update_mode;        // 0 per step, 1 per iteration
+    int error;              // DevError bits
+    int done;               // TimeManager.running turned false (time >= TIMEMAX)
+    unsigned long long maxbits[3];   // per-direction max of |v_i| + c_s (bit pattern, >= 0)
+    unsigned int counter;            // CTAs finished in the current CFL reduction
+    unsigned int pad2;
+};
+
+// ---- grid geometry --------------------------------------------------------------------------------
+struct Geom {
+    int n[3];
+    int ndims;        // 3 if nz > 1 else 2 (MATLAB squeeze + ndims)
+    long long s[3];   // strides: 1, nx, nx*ny
+    long long ncell;
+};
+
+// Index of a cell inside the face orthogonal to dim e (column-major order of the other two dims).
+__host__ __device__ inline long long face_index(const Geom& g, int e, int x, int y, int z) {
+    if (e == 0) return (long long)z * g.n[1] + y;
+    if (e == 1) return (long long)z * g.n[0] + x;
+    return (long long)y * g.n[0] + x;
+}
+
+// Select one of three values by a runtime index without indexing a register array.
+template <typename T>
+__host__ __device__ __forceinline__ T sel3(int i, T a, T b, T c) { return i == 0 ? a : (i == 1 ? b : c); }
+
+// ---- small numeric helpers --------------------------------------------------------------------------
+template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b ? a : b; }
+__device__ __forceinline__ double msign(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : (v == 0 ? 0.0 : v)); }
+__device__ __forceinline__ float msign(float v) { return v > 0 ? 1.f : (v < 0 ? -1.f : (v == 0 ? 0.f : v)); }
+
+// TVD limiter correction (flux/vanleerLimiter.m:9-11, minmodLimiter.m:9, superbeeLimiter.m:9-10).
+// The reference adds it to the flux in place: flux.array = flux.array + correction.
+template <typename T>
+__device__ __forceinline__ T limiter_corr(int lim, T dL, T dR) {
+    if (lim == LIM_VANLEER) {
+        T p = dL * dR;
+        T st = (p > T(0) ? p : T(0)) / (dL + dR);
+        return isnan(st) ? T(0) : st;
+    }
+    if (lim == LIM_SUPERBEE) {
+        T c = fabs(dL) < fabs(dR) ? T(1) : T(0);
+        dL = (T(1) + c) * dL;
+        dR = (T(2) - c) * dR;
+    }
+    return T(0.125) * (msign(dL) + msign(dR)) * fmin(fabs(dL), fabs(dR));
+}
+
+// Stored-edge drift of a transparent edge (Edges.m:121-136): move toward the current edge value
+// by at most TOLERANCE = 0.005.
+__device__ __forceinline__ double edge_drift(double old_e, double cur) {
+    double delta = fmin(fabs(cur - old_e), 0.005);
+    bool st = (cur - old_e) > 0;
+    return old_e + ((st ? 1.0 : 0.0) - (st ? 0.0 : 1.0)) * delta;
+}
+
+// MATLAB pchip through x = [1 2 3 inf inf+1] with y[0..4], evaluated at xe (>= 3).
+// Interior slopes: Fritsch-Butland weighted harmonic mean; end slopes: one-sided,
+// shape-preserving (Moler, "Numerical Computing with MATLAB", pchiptx).
+__device__ __noinline__ double pchip5(const double y[5], double inf, double xe) {
+    const double x[5] = {1.0, 2.0, 3.0, inf, inf + 1.0};
+    double h[4], del[4], d[5];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        h[k] = x[k + 1] - x[k];
+        del[k] = (y[k + 1] - y[k]) / h[k];
+    }
+#pragma unroll
+    for (int k = 1; k < 4; ++k) {
+        double w1 = 2 * h[k] + h[k - 1];
+        double w2 = h[k] + 2 * h[k - 1];
+        d[k] = (msign(del[k - 1]) * msign(del[k]) > 0) ? (w1 + w2) / (w1 / del[k - 1] + w2 / del[k]) : 0.0;
+    }
+    {
+        double dd = ((2 * h[0] + h[1]) * del[0] - h[0] * del[1]) / (h[0] + h[1]);
+        if (msign(dd) != msign(del[0])) dd = 0.0;
+        else if (msign(del[0]) != msign(del[1]) && fabs(dd) > fabs(3 * del[0])) dd = 3 * del[0];
+        d[0] = dd;
+        dd = ((2 * h[3] + h[2]) * del[3] - h[3] * del[2]) / (h[3] + h[2]);
+        if (msign(dd) != msign(del[3])) dd = 0.0;
+        else if (msign(del[3]) != msign(del[2]) && fabs(dd) > fabs(3 * del[3])) dd = 3 * del[3];
+        d[4] = dd;
+    }
+    int k = 0;
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+        if (x[q] <= xe) k = q;
+    k = k > 3 ? 3 : k;
+    double s = xe - x[k];
+    double c1 = (d[k] + d[k + 1] - 2 * del[k]) / (h[k] * h[k]);
+    double c2 = (3 * del[k] - 2 * d[k] - d[k + 1]) / h[k];
+    return ((c1 * s + c2) * s + d[k]) * s + y[k];
+}
+
+// Rows that transparent_shift.m:36-39 / :68-71 feed to pchip at x = 1, 2, 3 for a shift by
+// n = -m (lower end) or n = +m (upper end): rows 2,1,0 / N-3,N-2,N-1, clamped for short lines.
+__host__ __device__ __forceinline__ int trans_pick_lower(int N, int m, int q) {
+    int p = 3 - q + m;
+    p = p > N ? N : p;
+    p = p - 1 - m;
+    return p < 0 ? 0 : p;
+}
+__host__ __device__ __forceinline__ int trans_pick_upper(int N, int m, int q) {
+    int p = N - (2 - q) - m;
+    p = p < 1 ? 1 : p;
+    p = p - 1 + m;
+    return p > N - 1 ? N - 1 : p;
+}
+
+// Transparent ghost value (shifting/transparent_shift.m:23-99).  y3 = the three array values that
+// the reference feeds at x = 1, 2, 3 (x = 3 is the edge cell), edge = the stored edge after its
+// drift (0 when the edge store is not ACTIVE(DIRECT)), xe = 4 or 5, orig = the unshifted array
+// value at the ghost position (kept when the extrapolation is within 1e-4 of it).
+__device__ __noinline__ double trans_ghost(double y0, double y1, double y2, double edge, double inf, double xe,
+                                           double orig) {
+    double y[5] = {y0, y1, y2, edge, edge};
+    double out = pchip5(y, inf, xe);
+    bool t = fabs(orig - out) < 1e-4;
+    return (t ? 0.0 : 1.0) * out + (t ? 1.0 : 0.0) * orig;
+}
+
+// Pressure recovery (pressure/pressure.m:23-64), always in FP64.  Returns P (clamped at 0).
+// sound_mode = false: 'totsnd' (P_tot and c_s with the 2B^2 term); true: 'sound' (c_s in P).
+struct PressOut {
+    double p;
+    double cs;
+};
+__device__ __forceinline__ PressOut pressure_totsnd(double G, double rho, double px, double py, double pz, double E,
+                                                    double msq) {
+    double vsq = (px * px + py * py + pz * pz) / (rho * rho);
+    double r = (G - 1.0) * (E - 0.5 * rho * vsq);
+    PressOut o;
+    o.cs = sqrt(fabs((G * (r - (G - 1.0) * 0.5 * msq) + 2.0 * msq) / rho));
+    r = r + 0.5 * (2.0 - G) * msq;
+    o.p = r < 0 ? 0.0 : r;
+    return o;
+}
+__device__ __forceinline__ double sound_speed(double G, double rho, double px, double py, double pz, double E,
+                                              double msq) {
+    double vsq = (px * px + py * py + pz * pz) / (rho * rho);
+    double r = (G - 1.0) * (E - 0.5 * rho * vsq);
+    r = r - (G - 1.0) * 0.5 * msq;
+    r = sqrt(fabs((G * r + 2.0 * msq) / rho));
+    return r < 0 ? 0.0 : r;
+}
+
+// Atomic max of a non-negative double through its bit pattern (NaN never reaches here).
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+    atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+}  // namespace img

@@ -1,0 +1,828 @@
+// Host side of the imogen_b200 C ABI: context, resident state, launch sequencing.
+//
+// A context owns one grid's state on the device (eleven SoA arrays), its stored edges, scratch for
+// the magnet passes and a device-resident TimeManager.  flux()/step() only enqueue kernels on the
+// context's stream; the timestep is computed and consumed on the device, so a whole iteration runs
+// without a host round trip (and is captured once into a CUDA graph per sweep-order row).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/imogen_b200.h"
+#include "cfl.cuh"
+
+using namespace img;
+
+namespace {
+
+// flux.m:17-27 -- perms([1 2 3]) in reverse-lexicographic order; backward rows are reversed.
+const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1, 2, 3}};
+const int FWD_MI[3][2] = {{2, 3}, {1, 3}, {1, 2}};
+const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
+
+struct PencilCfg {
+    int Wb = 1, G = 32, CL = 1, NT = 32;
+};
+
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int pow2ceil(long long v) {
+    int p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+}  // namespace
+
+struct img_ctx {
+    img_config cfg{};
+    std::string err;
+    int dev = 0;
+    size_t elem = 8;            // bytes per state value (8 FP64, 4 mixed)
+    Geom g{};
+    cudaStream_t stream = nullptr;
+    void* slab = nullptr;       // one allocation: state, scratch, edges, tables
+    size_t slab_bytes = 0;
+    void* q[NQ] = {};
+    void* scratch[5] = {};      // F0, F1, C0, C1, BXn
+    DevTime* tm = nullptr;
+    EdgeTable* edges_dev = nullptr;
+    EdgeTable edges_host{};
+    double* fade_dev = nullptr;
+    double* partial = nullptr;  // totals partials
+    std::vector<double> fade_host;
+    int use_b[3] = {1, 1, 1};
+    int mhd = 0;
+    bool state_set = false;
+    bool init_store = true, init_flux = true;   // fluid objects not yet assigned
+    bool init_mag[3][3] = {{true, true, true}, {true, true, true}, {true, true, true}};
+    bool cfl_valid = false;     // DevTime.maxbits hold the CFL maxima of the current state
+    int iteration = 1;
+    int iters_base = 0;
+    PencilCfg pcfg[3];
+    int cpt = 2;
+    cudaGraphExec_t graphs[6] = {};
+    DevTime* host_tm = nullptr;  // pinned mirror
+};
+
+namespace {
+
+thread_local std::string g_create_err;
+
+int fail(img_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    else g_create_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(ctx, IMG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+bool active_lin(const img_config& c, int ndims, int cls, int DIRECT) {
+    // Edges.ACTIVE(DIRECT) read with a linear index into the 2x3 (side x dim) matrix
+    // (transparent_shift.m:42,74): element (side, dim) = ((DIRECT-1) % 2, (DIRECT-1) / 2).
+    int side = (DIRECT - 1) % 2, dim = (DIRECT - 1) / 2;
+    if (dim >= ndims) return false;
+    int m = c.bc_modes[cls][side][dim];
+    return m == IMG_BC_TRANS || m == IMG_BC_WALL || m == IMG_BC_FADE;
+}
+
+bool stateful(int m) { return m == IMG_BC_TRANS || m == IMG_BC_WALL; }
+
+int obj_class(int o) {
+    if (o < OBJ_PRIM_MASS) {
+        const int cls_of[5] = {CLS_MASS, CLS_MOM, CLS_MOM, CLS_MOM, CLS_ENER};
+        return cls_of[(o - OBJ_FLUID) / 4];
+    }
+    if (o == OBJ_PRIM_MASS) return CLS_MASS;
+    if (o < OBJ_PRIM_MAG) return CLS_MOM;
+    return CLS_MAG;
+}
+
+bool obj_used(const img_config& c, int o) {
+    if (o < OBJ_PRIM_MASS) return c.fluid_active != 0;
+    if (o < OBJ_MAG) return true;
+    int r = (o - OBJ_MAG) / 4;
+    int comp = r / 3, X = r % 3;
+    return c.magnet_active && comp != X;
+}
+
+// MATLAB pchip on 5 knots (host copy for the fade coefficients of fade_shift.m:31).
+std::vector<double> fade_coefficients(int f) {
+    double xk[5] = {0, std::ceil(f / 4.0), std::floor(f / 2.0 + 0.5), double(f - 1), double(f)};
+    double yk[5] = {1, 1, 0.01, 0, 0};
+    double h[4], del[4], d[5];
+    auto sg = [](double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); };
+    for (int k = 0; k < 4; ++k) { h[k] = xk[k + 1] - xk[k]; del[k] = (yk[k + 1] - yk[k]) / h[k]; }
+    for (int k = 1; k < 4; ++k) {
+        double w1 = 2 * h[k] + h[k - 1], w2 = h[k] + 2 * h[k - 1];
+        d[k] = sg(del[k - 1]) * sg(del[k]) > 0 ? (w1 + w2) / (w1 / del[k - 1] + w2 / del[k]) : 0.0;
+    }
+    auto endslope = [&](double h0, double h1, double d0, double d1) {
+        double dd = ((2 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+        if (sg(dd) != sg(d0)) dd = 0.0;
+        else if (sg(d0) != sg(d1) && std::fabs(dd) > std::fabs(3 * d0)) dd = 3 * d0;
+        return dd;
+    };
+    d[0] = endslope(h[0], h[1], del[0], del[1]);
+    d[4] = endslope(h[3], h[2], del[3], del[2]);
+    std::vector<double> out(f);
+    for (int j = 0; j < f; ++j) {
+        double xv = j + 1;
+        int k = 0;
+        for (int q = 0; q < 5; ++q)
+            if (xk[q] <= xv) k = q;
+        k = std::min(k, 3);
+        double s = xv - xk[k];
+        double c1 = (d[k] + d[k + 1] - 2 * del[k]) / (h[k] * h[k]);
+        double c2 = (3 * del[k] - 2 * d[k] - d[k + 1]) / h[k];
+        out[j] = ((c1 * s + c2) * s + d[k]) * s + yk[k];
+    }
+    return out;
+}
+
+PencilCfg choose_pencil(const Geom& g, int d, size_t elem, int cpt) {
+    PencilCfg p;
+    int N = g.n[d];
+    long long ncol = g.ncell / N;
+    int G = pow2ceil((N + cpt - 1) / cpt);
+    int maxnt = 256;
+    int CL = 1;
+    if (d == 0) {
+        while (G > maxnt) { G >>= 1; CL <<= 1; }
+        if (CL > 8) { maxnt = 512; G <<= 1; CL >>= 1; }
+        int Wb = std::max(1, std::min(32, maxnt / G));
+        if (Wb * G < 32) Wb = 32 / G;
+        while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+        p.Wb = Wb;
+    } else {
+        int Wb = elem == 8 ? 4 : 8;
+        G = std::max(G, 32 / Wb);
+        while (Wb * G > maxnt) { G >>= 1; CL <<= 1; }
+        if (CL > 8) { maxnt = 512; G <<= 1; CL >>= 1; }
+        p.Wb = Wb;
+    }
+    p.G = G;
+    p.CL = CL;
+    p.NT = p.Wb * p.G;
+    return p;
+}
+
+int launch_blocks(long long work, int bs = 256) {
+    long long b = (work + bs - 1) / bs;
+    return (int)std::max(1LL, std::min(b, 148LL * 16));
+}
+
+template <typename T>
+int launch_fluid(img_ctx* ctx, int d, bool cfl) {
+    FluidArgs a{};
+    const img_config& c = ctx->cfg;
+    PencilCfg pcf = ctx->pcfg[d];
+    a.sg.g = ctx->g;
+    a.sg.d = d;
+    a.sg.d1 = d == 0 ? 1 : 0;
+    a.sg.d2 = d == 2 ? 1 : 2;
+    a.sg.N = ctx->g.n[d];
+    a.sg.ncol = ctx->g.ncell / a.sg.N;
+    a.sg.Wb = pcf.Wb;
+    a.sg.G = pcf.G;
+    a.sg.CL = pcf.CL;
+    a.sg.NT = pcf.NT;
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    a.tm = ctx->tm;
+    a.gamma = c.gamma;
+    a.minmass = c.minmass;
+    a.dx = c.dgrid[d];
+    a.limiter = c.limiter[d];
+    for (int k = 0; k < 4; ++k) {
+        a.mode[k][0] = c.bc_modes[k][0][d];
+        a.mode[k][1] = c.bc_modes[k][1][d];
+        a.act[k] = active_lin(c, ctx->g.ndims, k, d + 1);
+    }
+    a.fade = ctx->fade_dev;
+    a.fade_f = c.bc_infinity;
+    a.bc_inf = c.bc_infinity;
+    a.edges = ctx->edges_dev;
+    a.init_store = ctx->init_store;
+    a.init_flux = ctx->init_flux;
+    a.mhd = ctx->mhd;
+    for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
+    a.cfl = cfl;
+    long long nb = (a.sg.ncol + pcf.Wb - 1) / pcf.Wb;
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3((unsigned)(nb * pcf.CL));
+    lc.blockDim = dim3(pcf.NT);
+    using PC = Pencil<T, (sizeof(T) == 8 ? 2 : 4), FLUID_NSLOT, false>;
+    lc.dynamicSmemBytes = PC::smem_bytes(pcf.NT, pcf.Wb);
+    lc.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = pcf.CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    constexpr int CPT = sizeof(T) == 8 ? 2 : 4;
+    void (*kern)(const FluidArgs) = ctx->mhd ? fluid_sweep_kernel<T, true, CPT> : fluid_sweep_kernel<T, false, CPT>;
+    if (pcf.CL > 8) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    if (lc.dynamicSmemBytes > 48 * 1024)
+        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lc.dynamicSmemBytes));
+    CK(cudaLaunchKernelEx(&lc, kern, a));
+    ctx->init_store = false;
+    ctx->init_flux = false;
+    return IMG_OK;
+}
+
+template <typename T>
+void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
+    const img_config& c = ctx->cfg;
+    int d = X - 1;
+    PencilCfg pcf = ctx->pcfg[d];
+    a.sg.g = ctx->g;
+    a.sg.d = d;
+    a.sg.d1 = d == 0 ? 1 : 0;
+    a.sg.d2 = d == 2 ? 1 : 2;
+    a.sg.N = ctx->g.n[d];
+    a.sg.ncol = ctx->g.ncell / a.sg.N;
+    a.sg.Wb = pcf.Wb;
+    a.sg.G = pcf.G;
+    a.sg.CL = pcf.CL;
+    a.sg.NT = pcf.NT;
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    a.F[0] = ctx->scratch[0];
+    a.F[1] = ctx->scratch[1];
+    a.C[0] = ctx->scratch[2];
+    a.C[1] = ctx->scratch[3];
+    a.BXn = ctx->scratch[4];
+    a.tm = ctx->tm;
+    a.X = X;
+    a.I[0] = I1;
+    a.I[1] = I2;
+    a.dx = c.dgrid[d];
+    a.limiter = c.limiter[d];
+    a.modeX[0] = c.bc_modes[CLS_MAG][0][d];
+    a.modeX[1] = c.bc_modes[CLS_MAG][1][d];
+    a.modeX_magX[0] = a.modeX[0];
+    a.modeX_magX[1] = a.modeX[1];
+    a.actX = active_lin(c, ctx->g.ndims, CLS_MAG, X);
+    for (int q = 0; q < 2; ++q) {
+        int I = q == 0 ? I1 : I2, e = I - 1;
+        a.shiftI[q] = e < ctx->g.ndims;
+        a.dI[q] = c.dgrid[e];
+        for (int s = 0; s < 2; ++s) {
+            a.modeI_mass[q][s] = c.bc_modes[CLS_MASS][s][e];
+            a.modeI_mom[q][s] = c.bc_modes[CLS_MOM][s][e];
+            a.modeI_mag[q][s] = c.bc_modes[CLS_MAG][s][e];
+        }
+        a.actI_mass[q] = active_lin(c, ctx->g.ndims, CLS_MASS, I);
+        a.actI_mom[q] = active_lin(c, ctx->g.ndims, CLS_MOM, I);
+        a.actI_mag[q] = active_lin(c, ctx->g.ndims, CLS_MAG, I);
+        a.init_mag[q] = ctx->init_mag[I - 1][d];
+    }
+    a.fade = ctx->fade_dev;
+    a.fade_f = c.bc_infinity;
+    a.bc_inf = c.bc_infinity;
+    a.edges = ctx->edges_dev;
+}
+
+template <typename T>
+int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
+    MagArgs a{};
+    fill_mag_args<T>(ctx, X, I1, I2, a);
+    int d = X - 1;
+    PencilCfg pcf = ctx->pcfg[d];
+    constexpr int CPT = sizeof(T) == 8 ? 2 : 4;
+    using PC = Pencil<T, CPT, MAG_NSLOT, true>;
+    long long nb = (a.sg.ncol + pcf.Wb - 1) / pcf.Wb;
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3((unsigned)(nb * pcf.CL), 2);
+    lc.blockDim = dim3(pcf.NT);
+    lc.dynamicSmemBytes = PC::smem_bytes(pcf.NT, pcf.Wb);
+    lc.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = pcf.CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    void (*kern)(const MagArgs) = mag_chain_kernel<T, CPT>;
+    if (pcf.CL > 8) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    CK(cudaLaunchKernelEx(&lc, kern, a));
+    long long n = ctx->g.ncell;
+    mag_ct1_kernel<T><<<launch_blocks(2 * n), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    mag_ct2_kernel<T><<<launch_blocks(2 * n), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    mag_bx_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    mag_cell_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    ctx->init_mag[I1 - 1][d] = false;
+    ctx->init_mag[I2 - 1][d] = false;
+    return IMG_OK;
+}
+
+template <typename T>
+int launch_cfl_reduce(img_ctx* ctx) {
+    CflArgs a{};
+    a.g = ctx->g;
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    a.tm = ctx->tm;
+    a.gamma = ctx->cfg.gamma;
+    a.mhd = ctx->mhd;
+    for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
+    cfl_reduce_kernel<T><<<launch_blocks(ctx->g.ncell), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    return IMG_OK;
+}
+
+int fluid_sweep(img_ctx* ctx, int X, bool cfl) {
+    return ctx->elem == 8 ? launch_fluid<double>(ctx, X - 1, cfl) : launch_fluid<float>(ctx, X - 1, cfl);
+}
+int magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
+    return ctx->elem == 8 ? launch_magnet<double>(ctx, X, I1, I2) : launch_magnet<float>(ctx, X, I1, I2);
+}
+int cfl_reduce(img_ctx* ctx) { return ctx->elem == 8 ? launch_cfl_reduce<double>(ctx) : launch_cfl_reduce<float>(ctx); }
+
+// flux.m:17-62 for one half step.  `fuse_cfl`: the final fluid sweep accumulates the CFL maxima.
+int do_flux(img_ctx* ctx, int order, bool fuse_cfl) {
+    const img_config& c = ctx->cfg;
+    int row = (ctx->iteration - 1) % 6;
+    int last_fluid = -1;
+    for (int q = 0; q < 3; ++q) {
+        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        if (ctx->g.n[X - 1] >= 3) last_fluid = q;
+    }
+    for (int q = 0; q < 3; ++q) {
+        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        if (ctx->g.n[X - 1] < 3) continue;
+        bool cfl_here = fuse_cfl && order < 0 && q == last_fluid && c.fluid_active;
+        int rc;
+        if (order > 0) {
+            if (c.fluid_active && (rc = fluid_sweep(ctx, X, false)) != IMG_OK) return rc;
+            if (c.magnet_active && (rc = magnet_sweep(ctx, X, FWD_MI[X - 1][0], FWD_MI[X - 1][1])) != IMG_OK) return rc;
+        } else {
+            if (c.magnet_active && (rc = magnet_sweep(ctx, X, BWD_MI[X - 1][0], BWD_MI[X - 1][1])) != IMG_OK) return rc;
+            if (c.fluid_active && (rc = fluid_sweep(ctx, X, cfl_here)) != IMG_OK) return rc;
+        }
+    }
+    return IMG_OK;
+}
+
+int time_update_async(img_ctx* ctx, int flux_direction) {
+    if (flux_direction > 1 && ctx->cfg.update_mode != 0) return IMG_OK;   // TimeManager.m:61-63
+    if (!ctx->cfl_valid) {
+        int rc = cfl_reduce(ctx);
+        if (rc != IMG_OK) return rc;
+    }
+    cfl_finalize_kernel<<<1, 32, 0, ctx->stream>>>(ctx->tm, flux_direction == 1 ? 1 : 0);
+    CK(cudaGetLastError());
+    ctx->cfl_valid = false;
+    return IMG_OK;
+}
+
+// One iteration (imogen.m:60-66): time.update(1), flux(+1), time.update(2), flux(-1).
+int enqueue_iteration(img_ctx* ctx) {
+    int rc;
+    bool per_iter = ctx->cfg.update_mode != 0;
+    if ((rc = time_update_async(ctx, 1)) != IMG_OK) return rc;
+    if ((rc = do_flux(ctx, 1, false)) != IMG_OK) return rc;
+    if ((rc = time_update_async(ctx, 2)) != IMG_OK) return rc;
+    if ((rc = do_flux(ctx, -1, per_iter)) != IMG_OK) return rc;
+    ctx->cfl_valid = per_iter && ctx->cfg.fluid_active;
+    return IMG_OK;
+}
+
+int check_dev_error(img_ctx* ctx) {
+    CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    int e = ctx->host_tm->error;
+    if (e & DERR_CFL) return fail(ctx, IMG_ERR_CFL, "CFL error: no velocity exceeded the 1e-2 floor (cmax=%g)", ctx->host_tm->cmax);
+    if (e & DERR_NONFINITE_DT) return fail(ctx, IMG_ERR_NONFINITE, "non-finite timestep");
+    return IMG_OK;
+}
+
+int validate(const img_config& c, std::string& why) {
+    for (int d = 0; d < 3; ++d) {
+        if (c.grid[d] < 1) { why = "grid extents must be >= 1"; return IMG_ERR_ARG; }
+        if (!(c.dgrid[d] > 0)) { why = "dGrid must be > 0"; return IMG_ERR_ARG; }
+        if (c.limiter[d] < 0 || c.limiter[d] > 2) { why = "unknown flux limiter"; return IMG_ERR_ARG; }
+    }
+    if (c.precision != IMG_PREC_FP64 && c.precision != IMG_PREC_MIXED) { why = "unknown precision"; return IMG_ERR_ARG; }
+    if (c.bc_infinity < 4) { why = "bcInfinity must be >= 4"; return IMG_ERR_ARG; }
+    int ndims = c.grid[2] > 1 ? 3 : 2;
+    for (int k = 0; k < 4; ++k)
+        for (int s = 0; s < 2; ++s)
+            for (int d = 0; d < ndims; ++d) {
+                int m = c.bc_modes[k][s][d];
+                if (m < 0 || m > 5) { why = "unknown BC mode"; return IMG_ERR_ARG; }
+                // mirror_shift.m:31-33 / fade_shift.m:34-44 and Edges.m:80-93 index outside short
+                // dimensions: the reference stops with an index error there.
+                if (m == IMG_BC_MIRROR && c.grid[d] < 2) { why = "mirror BC on a dimension of extent 1"; return IMG_ERR_UNSUPPORTED; }
+                if (m == IMG_BC_FADE && c.grid[d] < std::max(20, c.bc_infinity)) {
+                    why = "fade BC on a dimension shorter than max(20, bcInfinity)";
+                    return IMG_ERR_UNSUPPORTED;
+                }
+            }
+    return IMG_OK;
+}
+
+// Device bytes: state + scratch + edges + tables.
+struct Layout {
+    size_t state, scratch, tm, table, fade, partial, edges, total;
+    size_t edge_off[NOBJ][3][2];
+};
+
+Layout plan(const img_config& c) {
+    Layout L{};
+    size_t elem = c.precision == IMG_PREC_FP64 ? 8 : 4;
+    long long n = (long long)c.grid[0] * c.grid[1] * c.grid[2];
+    size_t arr = align256(n * elem);
+    L.state = arr * NQ;
+    L.scratch = c.magnet_active ? arr * 5 : 0;
+    L.tm = align256(sizeof(DevTime));
+    L.table = align256(sizeof(EdgeTable));
+    L.fade = align256(sizeof(double) * std::max(1, c.bc_infinity));
+    L.partial = align256(sizeof(double) * 2 * 8 * 1024);
+    int ndims = c.grid[2] > 1 ? 3 : 2;
+    size_t off = 0;
+    for (int o = 0; o < NOBJ; ++o)
+        for (int e = 0; e < 3; ++e)
+            for (int s = 0; s < 2; ++s) {
+                L.edge_off[o][e][s] = (size_t)-1;
+                if (e >= ndims || !obj_used(c, o)) continue;
+                if (!stateful(c.bc_modes[obj_class(o)][s][e])) continue;
+                L.edge_off[o][e][s] = off;
+                off += align256(sizeof(double) * (n / c.grid[e]));
+            }
+    L.edges = off;
+    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.edges;
+    return L;
+}
+
+template <typename T>
+void to_dev_type(const double* src, T* dst, long long n) {
+    for (long long i = 0; i < n; ++i) dst[i] = (T)src[i];
+}
+
+// Face of a host FP64 array along dim e at index idx (column-major order of the other dims).
+void host_face(const Geom& g, const double* a, int e, int idx, std::vector<double>& out) {
+    out.resize(g.ncell / g.n[e]);
+    for (int z = 0; z < g.n[2]; ++z)
+        for (int y = 0; y < g.n[1]; ++y)
+            for (int x = 0; x < g.n[0]; ++x) {
+                int c[3] = {x, y, z};
+                if (c[e] != idx) continue;
+                out[face_index(g, e, x, y, z)] = a[x + (long long)g.n[0] * (y + (long long)g.n[1] * z)];
+            }
+}
+
+template <typename T>
+int cellmag_init(img_ctx* ctx) {
+    CellMagInitArgs a{};
+    a.g = ctx->g;
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    for (int c = 0; c < 3; ++c) {
+        a.mode_hi[c] = ctx->cfg.bc_modes[CLS_MAG][1][c];
+        a.act[c] = active_lin(ctx->cfg, ctx->g.ndims, CLS_MAG, c + 1);
+    }
+    a.edges = ctx->edges_dev;
+    a.fade = ctx->fade_dev;
+    a.fade_f = ctx->cfg.bc_infinity;
+    a.bc_inf = ctx->cfg.bc_infinity;
+    cellmag_init_kernel<T><<<launch_blocks(3 * ctx->g.ncell), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    return IMG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void img_config_default(img_config* c) {
+    std::memset(c, 0, sizeof *c);
+    for (int d = 0; d < 3; ++d) { c->grid[d] = 1; c->dgrid[d] = 1.0; c->limiter[d] = IMG_LIM_VANLEER; }
+    c->gamma = 5.0 / 3.0;
+    c->cfl = 0.7;
+    c->minmass = 1e-5;
+    c->bc_infinity = 20;
+    c->fluid_active = 1;
+    c->magnet_active = 0;
+    c->time_max = 1e5;
+    c->iter_max = 10;
+    c->update_mode = 1;
+    c->precision = IMG_PREC_FP64;
+}
+
+size_t img_bytes_required(const img_config* cfg) { return cfg ? plan(*cfg).total : 0; }
+
+int img_create(img_ctx** out, const img_config* cfg) {
+    img_ctx* ctx = nullptr;
+    if (!out || !cfg) return fail(nullptr, IMG_ERR_ARG, "null argument");
+    *out = nullptr;
+    std::string why;
+    int rc = validate(*cfg, why);
+    if (rc != IMG_OK) return fail(nullptr, rc, "%s", why.c_str());
+    ctx = new img_ctx();
+    ctx->cfg = *cfg;
+    ctx->elem = cfg->precision == IMG_PREC_FP64 ? 8 : 4;
+    ctx->cpt = ctx->elem == 8 ? 2 : 4;
+    Geom& g = ctx->g;
+    for (int d = 0; d < 3; ++d) g.n[d] = cfg->grid[d];
+    g.ndims = cfg->grid[2] > 1 ? 3 : 2;
+    g.s[0] = 1;
+    g.s[1] = g.n[0];
+    g.s[2] = (long long)g.n[0] * g.n[1];
+    g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (int d = 0; d < 3; ++d) ctx->pcfg[d] = choose_pencil(g, d, ctx->elem, ctx->cpt);
+
+    auto bail = [&](int code) {
+        if (ctx->slab) cudaFree(ctx->slab);
+        if (ctx->host_tm) cudaFreeHost(ctx->host_tm);
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        g_create_err = ctx->err;
+        delete ctx;
+        return code;
+    };
+    if (cudaGetDevice(&ctx->dev) != cudaSuccess) { fail(ctx, IMG_ERR_CUDA, "no CUDA device"); return bail(IMG_ERR_CUDA); }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        fail(ctx, IMG_ERR_CUDA, "stream creation failed");
+        return bail(IMG_ERR_CUDA);
+    }
+    Layout L = plan(*cfg);
+    ctx->slab_bytes = L.total;
+    if (cudaMalloc(&ctx->slab, L.total) != cudaSuccess) {
+        cudaGetLastError();
+        fail(ctx, IMG_ERR_NOMEM, "cudaMalloc of %zu bytes failed", L.total);
+        return bail(IMG_ERR_NOMEM);
+    }
+    if (cudaMallocHost(&ctx->host_tm, sizeof(DevTime)) != cudaSuccess) {
+        fail(ctx, IMG_ERR_NOMEM, "pinned allocation failed");
+        return bail(IMG_ERR_NOMEM);
+    }
+    char* p = static_cast<char*>(ctx->slab);
+    size_t arr = align256(g.ncell * ctx->elem);
+    for (int v = 0; v < NQ; ++v) ctx->q[v] = p + v * arr;
+    p += L.state;
+    if (cfg->magnet_active)
+        for (int k = 0; k < 5; ++k) ctx->scratch[k] = p + k * arr;
+    p += L.scratch;
+    ctx->tm = reinterpret_cast<DevTime*>(p);
+    p += L.tm;
+    ctx->edges_dev = reinterpret_cast<EdgeTable*>(p);
+    p += L.table;
+    ctx->fade_dev = reinterpret_cast<double*>(p);
+    p += L.fade;
+    ctx->partial = reinterpret_cast<double*>(p);
+    p += L.partial;
+    char* edge_base = p;
+    for (int o = 0; o < NOBJ; ++o)
+        for (int e = 0; e < 3; ++e)
+            for (int s = 0; s < 2; ++s)
+                ctx->edges_host.p[o][e][s] =
+                    L.edge_off[o][e][s] == (size_t)-1 ? nullptr : reinterpret_cast<double*>(edge_base + L.edge_off[o][e][s]);
+    if (cudaMemsetAsync(ctx->slab, 0, L.total, ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->edges_dev, &ctx->edges_host, sizeof(EdgeTable), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+        fail(ctx, IMG_ERR_CUDA, "device initialisation failed");
+        return bail(IMG_ERR_CUDA);
+    }
+    ctx->fade_host = fade_coefficients(std::max(1, cfg->bc_infinity));
+    DevTime t{};
+    t.time = 0;
+    t.dt = 0;
+    t.time_max = cfg->time_max;
+    t.cfl = cfg->cfl;
+    for (int d = 0; d < 3; ++d) t.dgrid[d] = cfg->dgrid[d];
+    t.update_mode = cfg->update_mode;
+    *ctx->host_tm = t;
+    if (cudaMemcpyAsync(ctx->fade_dev, ctx->fade_host.data(), sizeof(double) * ctx->fade_host.size(), cudaMemcpyHostToDevice,
+                        ctx->stream) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->tm, ctx->host_tm, sizeof(DevTime), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        fail(ctx, IMG_ERR_CUDA, "device initialisation failed");
+        return bail(IMG_ERR_CUDA);
+    }
+    *out = ctx;
+    return IMG_OK;
+}
+
+int img_destroy(img_ctx* ctx) {
+    if (!ctx) return IMG_OK;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& gx : ctx->graphs)
+        if (gx) cudaGraphExecDestroy(gx);
+    if (ctx->slab) cudaFree(ctx->slab);
+    if (ctx->host_tm) cudaFreeHost(ctx->host_tm);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return IMG_OK;
+}
+
+const char* img_last_error(const img_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
+
+int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
+    if (!ctx || !host || var < 0 || var > IMG_VAR_MAGZ) return fail(ctx, IMG_ERR_ARG, "bad upload argument");
+    if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "upload size %zu != %lld cells", n, ctx->g.ncell);
+    if (ctx->elem == 8) {
+        CK(cudaMemcpyAsync(ctx->q[var], host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::vector<float> tmp(n);
+        to_dev_type(host, tmp.data(), (long long)n);
+        CK(cudaMemcpyAsync(ctx->q[var], tmp.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->cfl_valid = false;
+    return IMG_OK;
+}
+
+int img_download(img_ctx* ctx, int var, double* host, size_t n) {
+    if (!ctx || !host || var < 0 || var >= NQ) return fail(ctx, IMG_ERR_ARG, "bad download argument");
+    if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "download size %zu != %lld cells", n, ctx->g.ncell);
+    if (ctx->elem == 8) {
+        CK(cudaMemcpyAsync(host, ctx->q[var], n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpyAsync(tmp.data(), ctx->q[var], n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (size_t i = 0; i < n; ++i) host[i] = tmp[i];
+    }
+    return IMG_OK;
+}
+
+int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const double* ener, const double* mag) {
+    if (!ctx || !mass || !mom || !ener || !mag) return fail(ctx, IMG_ERR_ARG, "null state array");
+    long long n = ctx->g.ncell;
+    int rc;
+    if ((rc = img_upload(ctx, IMG_VAR_MASS, mass, n)) != IMG_OK) return rc;
+    for (int c = 0; c < 3; ++c)
+        if ((rc = img_upload(ctx, IMG_VAR_MOMX + c, mom + c * n, n)) != IMG_OK) return rc;
+    if ((rc = img_upload(ctx, IMG_VAR_ENER, ener, n)) != IMG_OK) return rc;
+    for (int c = 0; c < 3; ++c)
+        if ((rc = img_upload(ctx, IMG_VAR_MAGX + c, mag + c * n, n)) != IMG_OK) return rc;
+    // primary stored edges from the initial condition (Edges.m:37-110 at FluidArray/MagnetArray creation)
+    std::vector<double> face;
+    const double* prim[7] = {mass, mom, mom + n, mom + 2 * n, mag, mag + n, mag + 2 * n};
+    const int pobj[7] = {OBJ_PRIM_MASS, OBJ_PRIM_MOM, OBJ_PRIM_MOM + 1, OBJ_PRIM_MOM + 2, OBJ_PRIM_MAG, OBJ_PRIM_MAG + 1,
+                         OBJ_PRIM_MAG + 2};
+    for (int k = 0; k < 7; ++k)
+        for (int e = 0; e < ctx->g.ndims; ++e)
+            for (int s = 0; s < 2; ++s) {
+                double* dst = ctx->edges_host.p[pobj[k]][e][s];
+                if (!dst) continue;
+                host_face(ctx->g, prim[k], e, s == 0 ? 0 : ctx->g.n[e] - 1, face);
+                CK(cudaMemcpyAsync(dst, face.data(), face.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+            }
+    // MagnetArray.isZero (MagnetArray.m:44): all-zero component while the magnet is inactive
+    ctx->mhd = ctx->cfg.magnet_active ? 1 : 0;
+    for (int c = 0; c < 3; ++c) {
+        double sum = 0.0;
+        for (long long i = 0; i < n; ++i) sum += mag[c * n + i];
+        bool isZero = (sum == 0.0) && !ctx->cfg.magnet_active;
+        ctx->use_b[c] = !isZero;
+        if (!isZero) ctx->mhd = 1;
+    }
+    if ((rc = ctx->elem == 8 ? cellmag_init<double>(ctx) : cellmag_init<float>(ctx)) != IMG_OK) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->state_set = true;
+    ctx->cfl_valid = false;
+    return IMG_OK;
+}
+
+int img_time_update(img_ctx* ctx, int flux_direction, double* dt_out, int* dir_out) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    int rc = time_update_async(ctx, flux_direction);
+    if (rc != IMG_OK) return rc;
+    if (dt_out || dir_out) {
+        if ((rc = check_dev_error(ctx)) != IMG_OK) return rc;
+        if (dt_out) *dt_out = ctx->host_tm->dt;
+        if (dir_out) *dir_out = ctx->host_tm->grid_index;
+    }
+    return IMG_OK;
+}
+
+int img_flux(img_ctx* ctx, int order) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (order != 1 && order != -1) return fail(ctx, IMG_ERR_ARG, "%d is not a recognized direction", order);
+    ctx->cfl_valid = false;
+    return do_flux(ctx, order, false);
+}
+
+int img_fluid_sweep(img_ctx* ctx, int X) {
+    if (!ctx || X < 1 || X > 3) return fail(ctx, IMG_ERR_ARG, "bad sweep direction");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (ctx->g.n[X - 1] < 3) return fail(ctx, IMG_ERR_ARG, "dimension %d has fewer than 3 cells", X);
+    ctx->cfl_valid = false;
+    return fluid_sweep(ctx, X, false);
+}
+
+int img_magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
+    if (!ctx || X < 1 || X > 3 || I1 < 1 || I1 > 3 || I2 < 1 || I2 > 3 || I1 == X || I2 == X || I1 == I2)
+        return fail(ctx, IMG_ERR_ARG, "bad magnet sweep indices");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (!ctx->cfg.magnet_active) return fail(ctx, IMG_ERR_STATE, "magnet is not active");
+    ctx->cfl_valid = false;
+    return magnet_sweep(ctx, X, I1, I2);
+}
+
+int img_step(img_ctx* ctx) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    int rc = enqueue_iteration(ctx);
+    if (rc != IMG_OK) return rc;
+    ctx->iteration += 1;
+    return IMG_OK;
+}
+
+int img_run(img_ctx* ctx, int max_iters, int* iters_done) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    int n = 0, rc;
+    while (ctx->iteration <= ctx->cfg.iter_max && (max_iters < 0 || n < max_iters)) {
+        // TimeManager.running: time < TIMEMAX (checked on the device copy every iteration)
+        if ((rc = check_dev_error(ctx)) != IMG_OK) return rc;
+        if (!(ctx->host_tm->time < ctx->host_tm->time_max)) break;
+        if ((rc = img_step(ctx)) != IMG_OK) return rc;
+        ++n;
+    }
+    if ((rc = check_dev_error(ctx)) != IMG_OK) return rc;
+    if (iters_done) *iters_done = n;
+    return IMG_OK;
+}
+
+int img_get_time(img_ctx* ctx, double* time, double* dt, int* iteration) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    int rc = check_dev_error(ctx);
+    if (time) *time = ctx->host_tm->time;
+    if (dt) *dt = ctx->host_tm->dt;
+    if (iteration) *iteration = ctx->iteration;
+    return rc;
+}
+
+int img_set_time(img_ctx* ctx, double time, double dt, int iteration) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->host_tm->time = time;
+    ctx->host_tm->dt = dt;
+    ctx->host_tm->done = 0;
+    ctx->host_tm->error = 0;
+    CK(cudaMemcpyAsync(ctx->tm, ctx->host_tm, sizeof(DevTime), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->iteration = iteration;
+    return IMG_OK;
+}
+
+int img_totals(img_ctx* ctx, double out[8]) {
+    if (!ctx || !out) return fail(ctx, IMG_ERR_ARG, "null argument");
+    const int nb = 1024;
+    void* qp_host[8];
+    for (int v = 0; v < 8; ++v) qp_host[v] = ctx->q[v];
+    // the pointer table lives in the partial buffer's tail
+    void** qp_dev = reinterpret_cast<void**>(ctx->partial + 2 * 8 * nb - 16);
+    CK(cudaMemcpyAsync(qp_dev, qp_host, sizeof qp_host, cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->elem == 8) totals_kernel<double><<<nb - 1, 256, 0, ctx->stream>>>(ctx->g, qp_dev, ctx->partial);
+    else totals_kernel<float><<<nb - 1, 256, 0, ctx->stream>>>(ctx->g, qp_dev, ctx->partial);
+    CK(cudaGetLastError());
+    std::vector<double> part(2 * 8 * (nb - 1));
+    CK(cudaMemcpyAsync(part.data(), ctx->partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int v = 0; v < 8; ++v) {
+        double S = 0.0, C = 0.0;
+        for (int b = 0; b < nb - 1; ++b) {
+            double x = part[(b * 8 + v) * 2];
+            double t = S + x;
+            C += std::fabs(S) >= std::fabs(x) ? (S - t) + x : (x - t) + S;
+            S = t;
+            C += part[(b * 8 + v) * 2 + 1];
+        }
+        out[v] = S + C;
+    }
+    return IMG_OK;
+}
+
+int img_sync(img_ctx* ctx) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    return check_dev_error(ctx);
+}
+
+}  // extern "C"

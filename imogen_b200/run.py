@@ -1,0 +1,249 @@
+"""Host-side mirror of the reference's call surface for the relaxing-TVD path.
+
+``ImogenRun`` stands in for the ImogenManager plus the FluidArray/MagnetArray objects of one run
+(classes/ImogenManager.m, imogen.m:34-45); its state is resident on the GPU.  The functions
+``flux``, ``relaxingFluid`` and ``magnetFlux`` keep the reference signatures (flux/flux.m:1,
+fluid/relaxingFluid.m:1, magnet/magnetFlux.m:1) so a driver written against the reference reads
+the same; the array arguments are accepted for signature compatibility and ignored, because the
+arrays live in the run.  ``run.time`` mirrors TimeManager (time/TimeManager.m).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import ImgConfig, check, lib
+
+BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall")      # enums/ENUM.m:22-31
+LIMITERS = {"vanleer": 0, "superbee": 1, "minmond": 2, "minmod": 2}   # FluxLimiterEnum.m:10-13
+BC_CLASSES = ("mass", "mom", "ener", "mag")
+PRECISIONS = {"fp64": 0, "mixed": 1}
+VAR = dict(mass=0, momx=1, momy=2, momz=3, ener=4, magx=5, magy=6, magz=7, cmagx=8, cmagy=9, cmagz=10)
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def bc_table(bc):
+    """bcMode as initialize.m:24-40 accepts it: one mode string for everything, a struct-like
+    dict {x, y, z} (each a mode or a (lower, upper) pair), or per-class {mass|mom|ener|mag: ...}.
+    Returns int[4][2][3]."""
+    def one(spec):
+        out = [[0, 0, 0], [0, 0, 0]]
+        if isinstance(spec, str):
+            spec = {"x": spec, "y": spec, "z": spec}
+        for d, f in enumerate("xyz"):
+            v = spec.get(f, "circ")
+            lo, hi = (v, v) if isinstance(v, str) else (v[0], v[-1])
+            out[0][d] = BC_MODES.index(lo)
+            out[1][d] = BC_MODES.index(hi)
+        return out
+    if bc is None:
+        bc = "circ"
+    if isinstance(bc, str) or any(k in bc for k in "xyz"):
+        t = one(bc)
+        return [t, t, t, t]
+    if isinstance(bc, dict) and all(k in bc for k in BC_CLASSES):
+        res = []
+        for k in BC_CLASSES:
+            v = bc[k]
+            if isinstance(v, (list, tuple)) and len(v) == 2 and not isinstance(v[0], str):
+                res.append([[BC_MODES.index(m) for m in v[0]], [BC_MODES.index(m) for m in v[1]]])
+            else:
+                res.append(one(v))
+        return res
+    raise ValueError(f"unrecognised bcMode {bc!r}")
+
+
+def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ", bc_infinity=20,
+                limiter="vanleer", fluid=True, magnet=False, time_max=1e5, iter_max=10,
+                update_mode=1, precision="fp64"):
+    """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults)."""
+    c = ImgConfig()
+    lib().img_config_default(ctypes.byref(c))
+    grid = tuple(int(g) for g in grid) + (1,) * (3 - len(grid))
+    if dgrid is None:
+        dgrid = (1.0, 1.0, 1.0)
+    if np.isscalar(dgrid):
+        dgrid = (float(dgrid),) * 3
+    for d in range(3):
+        c.grid[d] = grid[d]
+        c.dgrid[d] = float(dgrid[d])
+    c.gamma = float(gamma)
+    c.cfl = float(cfl if cfl is not None else (0.35 if magnet else 0.7))   # Initializer.m:143-150
+    c.minmass = float(minmass)
+    c.bc_infinity = int(bc_infinity)
+    t = bc_table(bc)
+    for k in range(4):
+        for s in range(2):
+            for d in range(3):
+                c.bc_modes[k][s][d] = t[k][s][d]
+    lims = (limiter,) * 3 if isinstance(limiter, str) else tuple(limiter)
+    for d in range(3):
+        c.limiter[d] = LIMITERS[lims[d]]
+    c.fluid_active = int(bool(fluid))
+    c.magnet_active = int(bool(magnet))
+    c.time_max = float(time_max)
+    c.iter_max = int(iter_max)
+    c.update_mode = int(update_mode)
+    c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    return c
+
+
+def bytes_required(**kw):
+    c = make_config(**kw)
+    return int(lib().img_bytes_required(ctypes.byref(c)))
+
+
+class TimeManager:
+    """run.time (time/TimeManager.m): update/running/step on the device-resident clock."""
+
+    def __init__(self, run):
+        self._run = run
+
+    def update(self, flux_direction, sync=False):
+        dt, gi = ctypes.c_double(), ctypes.c_int()
+        r = self._run
+        if sync:
+            check(lib().img_time_update(r._h, int(flux_direction), ctypes.byref(dt), ctypes.byref(gi)), r._h)
+            return dt.value, gi.value
+        check(lib().img_time_update(r._h, int(flux_direction), None, None), r._h)
+        return None
+
+    def _get(self):
+        t, dt, it = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        r = self._run
+        check(lib().img_get_time(r._h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it)), r._h)
+        return t.value, dt.value, it.value
+
+    @property
+    def time(self):
+        return self._get()[0]
+
+    @property
+    def dTime(self):
+        return self._get()[1]
+
+    @property
+    def iteration(self):
+        return self._get()[2]
+
+    @property
+    def running(self):
+        t, _, it = self._get()
+        return it <= self._run.config.iter_max and t < self._run.config.time_max
+
+    def set(self, time, dt, iteration):
+        r = self._run
+        check(lib().img_set_time(r._h, float(time), float(dt), int(iteration)), r._h)
+
+
+class ImogenRun:
+    """One run of the hot path with its state resident on the current CUDA device."""
+
+    def __init__(self, grid, **kw):
+        self.config = make_config(grid, **kw)
+        self.grid = tuple(self.config.grid)
+        self.ncell = int(np.prod(self.grid))
+        h = ctypes.c_void_p()
+        rc = lib().img_create(ctypes.byref(h), ctypes.byref(self.config))
+        check(rc, None)
+        self._h = h
+        self.time = TimeManager(self)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().img_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- arrays (x fastest; numpy arrays shaped (nx, ny, nz) or flat) -----------------------------
+    def _flat(self, a):
+        a = np.asarray(a, dtype=np.float64)
+        if a.ndim == 1:
+            return np.ascontiguousarray(a)
+        return np.ascontiguousarray(a.reshape(self.grid).ravel(order="F"))
+
+    def set_state(self, mass, mom, ener, mag):
+        """FluidArray/MagnetArray construction from the IC (imogen.m:34-42)."""
+        m = self._flat(mass)
+        e = self._flat(ener)
+        p = np.concatenate([self._flat(mom[i]) for i in range(3)])
+        b = np.concatenate([self._flat(mag[i]) for i in range(3)])
+        check(lib().img_set_state(self._h, _dp(m), _dp(p), _dp(e), _dp(b)), self._h)
+
+    def upload(self, name, arr):
+        a = self._flat(arr)
+        check(lib().img_upload(self._h, VAR[name], _dp(a), a.size), self._h)
+
+    def download(self, name):
+        out = np.empty(self.ncell)
+        check(lib().img_download(self._h, VAR[name], _dp(out), out.size), self._h)
+        return out.reshape(self.grid, order="F")
+
+    def state(self):
+        g = self.download
+        return dict(mass=g("mass"), ener=g("ener"),
+                    mom=np.stack([g("momx"), g("momy"), g("momz")]),
+                    mag=np.stack([g("magx"), g("magy"), g("magz")]),
+                    cellmag=np.stack([g("cmagx"), g("cmagy"), g("cmagz")]))
+
+    # ---- the hot path ------------------------------------------------------------------------------
+    def flux(self, order):
+        check(lib().img_flux(self._h, int(order)), self._h)
+
+    def relaxing_fluid(self, X):
+        check(lib().img_fluid_sweep(self._h, int(X)), self._h)
+
+    def magnet_flux(self, X, mag_indices):
+        check(lib().img_magnet_sweep(self._h, int(X), int(mag_indices[0]), int(mag_indices[1])), self._h)
+
+    def iterate(self):
+        """imogen.m:60-66 loop body: two timesteps, then iteration += 1 (asynchronous)."""
+        check(lib().img_step(self._h), self._h)
+
+    def run(self, max_iterations=None):
+        """while run.time.running: iterate (imogen.m:58-72).  Returns iterations executed."""
+        n = ctypes.c_int()
+        check(lib().img_run(self._h, -1 if max_iterations is None else int(max_iterations), ctypes.byref(n)),
+              self._h)
+        return n.value
+
+    def sync(self):
+        check(lib().img_sync(self._h), self._h)
+
+    def totals(self):
+        """Neumaier-compensated FP64 sums of rho, px, py, pz, E, Bx, By, Bz."""
+        out = np.zeros(8)
+        check(lib().img_totals(self._h, _dp(out)), self._h)
+        return out
+
+
+# ---- reference call surface ------------------------------------------------------------------------
+def flux(run, mass, mom, ener, mag, grav, order):
+    """flux(run, mass, mom, ener, mag, grav, order) -- flux/flux.m:1."""
+    run.flux(order)
+
+
+def relaxingFluid(run, mass, mom, ener, mag, grav, X):
+    """relaxingFluid(run, mass, mom, ener, mag, grav, X) -- fluid/relaxingFluid.m:1."""
+    run.relaxing_fluid(X)
+
+
+def magnetFlux(run, mass, mom, mag, X, magneticIndices):
+    """magnetFlux(run, mass, mom, mag, X, magneticIndices) -- magnet/magnetFlux.m:1."""
+    run.magnet_flux(X, magneticIndices)

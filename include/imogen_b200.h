@@ -1,0 +1,129 @@
+/*
+ * imogen_b200 -- C ABI of the B200 relaxing-TVD fluid + magnet update.
+ *
+ * Plain C: opaque context handles, host pointers and sizes, int status codes.  No exception or
+ * C++/torch type crosses this boundary.  Every entry point replaces one piece of the reference's
+ * MATLAB call surface (paths are relative to the reference project root); the MEX gateway that a
+ * MATLAB caller binds is shown in INTEGRATION.md.
+ *
+ * Threading: a context is used by one host thread at a time.  All work of a context is issued on
+ * its own CUDA stream; state stays resident on the device between calls.
+ */
+#ifndef IMOGEN_B200_H
+#define IMOGEN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------------------- */
+enum {
+    IMG_OK = 0,
+    IMG_ERR_ARG = -1,          /* invalid argument (message in img_last_error) */
+    IMG_ERR_CUDA = -2,         /* CUDA runtime error */
+    IMG_ERR_NOMEM = -3,        /* device allocation failed / over the HBM budget */
+    IMG_ERR_UNSUPPORTED = -4,  /* setting that the reference itself cannot run (index error) */
+    IMG_ERR_CFL = -5,          /* TimeManager.m:79-86: no direction exceeded the 1e-2 floor */
+    IMG_ERR_NONFINITE = -6,    /* the timestep became non-finite */
+    IMG_ERR_STATE = -7         /* call out of order (e.g. step before state was set) */
+};
+
+/* ---- enumerations (enums/ENUM.m, enums/FluxLimiterEnum.m) ----------------------------------- */
+enum { IMG_BC_CIRC = 0, IMG_BC_CONST = 1, IMG_BC_FADE = 2, IMG_BC_MIRROR = 3, IMG_BC_TRANS = 4, IMG_BC_WALL = 5 };
+enum { IMG_LIM_VANLEER = 0, IMG_LIM_SUPERBEE = 1, IMG_LIM_MINMOD = 2 };
+enum { IMG_CLS_MASS = 0, IMG_CLS_MOM = 1, IMG_CLS_ENER = 2, IMG_CLS_MAG = 3 };
+enum { IMG_PREC_FP64 = 0, IMG_PREC_MIXED = 1 };
+/* variable ids for upload/download: rho, momentum x/y/z, energy, face-centred B x/y/z, and the
+ * cell-centred B x/y/z (MagnetArray.cellMag, download only) */
+enum {
+    IMG_VAR_MASS = 0, IMG_VAR_MOMX = 1, IMG_VAR_MOMY = 2, IMG_VAR_MOMZ = 3, IMG_VAR_ENER = 4,
+    IMG_VAR_MAGX = 5, IMG_VAR_MAGY = 6, IMG_VAR_MAGZ = 7,
+    IMG_VAR_CMAGX = 8, IMG_VAR_CMAGY = 9, IMG_VAR_CMAGZ = 10
+};
+
+/* Run settings: the subset of the ini structure that initialize.m parses for this path
+ * (initialize.m:24-190; defaults of experiment/Initializer.m:73-184). */
+typedef struct img_config {
+    int grid[3];              /* ini.grid (nx, ny, nz); nz == 1 gives a 2-D run */
+    double dgrid[3];          /* ini.dGrid, uniform spacing per dimension (MINDGRID = dgrid) */
+    double gamma;             /* ini.gamma */
+    double cfl;               /* ini.cfl */
+    double minmass;           /* ini.minMass */
+    int bc_infinity;          /* ini.bcInfinity (trans extrapolation distance, fade width) */
+    int bc_modes[4][2][3];    /* [class: mass, mom, ener, mag][side: lower, upper][dim] */
+    int limiter[3];           /* ini.fluxLimiter.{x,y,z}; the magnet uses the same table */
+    int fluid_active;         /* ini.mode.fluid */
+    int magnet_active;        /* ini.mode.magnet */
+    double time_max;          /* ini.timeMax */
+    int iter_max;             /* ini.iterMax */
+    int update_mode;          /* ini.timeUpdateMode: 0 per step, 1 per iteration */
+    int precision;            /* IMG_PREC_FP64 (plain) or IMG_PREC_MIXED (FP32 state, FP64 pressure/CFL) */
+} img_config;
+
+typedef struct img_ctx img_ctx;
+
+/* Default config: Initializer.m defaults (gamma 5/3, cfl 0.7, minMass 1e-5, circ BCs,
+ * bcInfinity 20, vanleer, fluid on, magnet off, timeMax 1e5, iterMax 10, per-iteration dt). */
+void img_config_default(img_config* cfg);
+
+/* Create a context for one grid on the current CUDA device.  Replaces initialize.m:18-410 for
+ * the settings above plus the FluidArray/MagnetArray allocations of imogen.m:34-45. */
+int img_create(img_ctx** out, const img_config* cfg);
+int img_destroy(img_ctx* ctx);
+
+/* Construct the state from host FP64 arrays (x fastest, nx*ny*nz each; mom and mag hold the
+ * three components back to back): FluidArray(...)/MagnetArray(...) of imogen.m:34-42, including
+ * the initial stored edges of trans/wall boundaries and cellMag (MagnetArray.m:41-49). */
+int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const double* ener,
+                  const double* mag);
+
+/* X.array = value (ImogenArray.m:82-89) for one variable, and X.array reads (get.array). */
+int img_upload(img_ctx* ctx, int var_id, const double* host, size_t n);
+int img_download(img_ctx* ctx, int var_id, double* host, size_t n);
+
+/* TimeManager.update(mass, mom, ener, mag, fluxDirection) (time/TimeManager.m:55-99).  The new
+ * dt is computed and applied on the device; dt_out / dir_out may be NULL (no host sync then). */
+int img_time_update(img_ctx* ctx, int flux_direction, double* dt_out, int* dir_out);
+
+/* flux(run, mass, mom, ener, mag, grav, order) (flux/flux.m:1-64) at the current iteration. */
+int img_flux(img_ctx* ctx, int order);
+
+/* relaxingFluid(run, mass, mom, ener, mag, grav, X) (fluid/relaxingFluid.m:1) -- one sweep. */
+int img_fluid_sweep(img_ctx* ctx, int X);
+
+/* magnetFlux(run, mass, mom, mag, X, magneticIndices) (magnet/magnetFlux.m:1) -- one sweep. */
+int img_magnet_sweep(img_ctx* ctx, int X, int I1, int I2);
+
+/* One pass of the imogen.m:58-72 loop body: two timesteps (CFL, flux +1, flux -1), iteration+1.
+ * Asynchronous: returns after enqueueing. */
+int img_step(img_ctx* ctx);
+
+/* while run.time.running: img_step (imogen.m:58-72), at most max_iters iterations (-1: no cap).
+ * Returns after the device finished; *iters_done = iterations that advanced the state. */
+int img_run(img_ctx* ctx, int max_iters, int* iters_done);
+
+/* run.time.time, run.time.dTime, run.time.iteration (synchronises). */
+int img_get_time(img_ctx* ctx, double* time, double* dt, int* iteration);
+/* Overwrite the time manager state (time, dt, iteration). */
+int img_set_time(img_ctx* ctx, double time, double dt, int iteration);
+
+/* Compensated (Neumaier) FP64 totals of rho, px, py, pz, E, Bx, By, Bz over the grid. */
+int img_totals(img_ctx* ctx, double out[8]);
+
+/* Block until the context's stream is idle; returns a pending device error if any. */
+int img_sync(img_ctx* ctx);
+
+/* Message of the last failing call on this context (or of img_create when ctx is NULL). */
+const char* img_last_error(const img_ctx* ctx);
+
+/* Device bytes a context with this config allocates (for HBM-budget admission). */
+size_t img_bytes_required(const img_config* cfg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IMOGEN_B200_H */

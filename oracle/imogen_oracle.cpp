@@ -425,7 +425,7 @@ void relaxing_fluid(Sim& s, int X) {
     }
     {
         Vec m(N);
-        for (long long i = 0; i < N; ++i) m[i] = std::max(s.fv[0].store.a[i], s.minmass);
+        for (long long i = 0; i < N; ++i) m[i] = std::fmax(s.fv[0].store.a[i], s.minmass);   // max ignores NaN
         s.fv[0].store.set(std::move(m));
     }
     const Vec* us[5] = {&s.fv[0].store.a, &s.fv[1].store.a, &s.fv[2].store.a, &s.fv[3].store.a, &s.fv[4].store.a};
@@ -468,7 +468,7 @@ void relaxing_fluid(Sim& s, int X) {
     }
     {
         Vec m(N);
-        for (long long i = 0; i < N; ++i) m[i] = std::max(s.fv[0].prim.a[i], s.minmass);
+        for (long long i = 0; i < N; ++i) m[i] = std::fmax(s.fv[0].prim.a[i], s.minmass);
         s.fv[0].prim.set(std::move(m));
     }
 }

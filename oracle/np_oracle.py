@@ -497,7 +497,7 @@ class Sim:
                 + vi.store_fluxL.a - vi.store_fluxL.shift(X, 1)))
             vi.store_fluxR.cleanup()
             vi.store_fluxL.cleanup()
-        self.mass.store.set(np.maximum(self.mass.store.a, self.MINMASS))
+        self.mass.store.set(np.fmax(self.mass.store.a, self.MINMASS))   # MATLAB max ignores NaN
 
         freeze, w = self.w_fluid_flux(v[0].store.a, [v[1].store.a, v[2].store.a, v[3].store.a],
                                       v[4].store.a, X)
@@ -513,7 +513,7 @@ class Sim:
             vi.fluxR.cleanup()
             vi.fluxL.cleanup()
             vi.store.cleanup()
-        self.mass.prim.set(np.maximum(self.mass.prim.a, self.MINMASS))
+        self.mass.prim.set(np.fmax(self.mass.prim.a, self.MINMASS))
 
     # ---------------------------------------------------------------------------------------
     def magnet_flux(self, X, mag_indices):

@@ -1,0 +1,105 @@
+"""CUDA path vs the C++ oracle on identical seeded inputs (GPU required).
+
+Tolerances (relative L1 per variable, sum|gpu-oracle|/sum|oracle|):
+  * FP64 plain: 1e-10 after 100 iterations, 1e-12 for a single sweep.
+  * mixed (FP32 state, FP64 pressure/CFL): stated per test, against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from imogen_b200 import problems
+from tests.parity import errors, make_pair, smooth_state
+
+pytestmark = pytest.mark.gpu
+
+BCS = ["circ", "const", "mirror", "trans", "wall", "fade"]
+
+
+def _bc_settings(bc, grid):
+    # mirror/fade need extent >= 2 / >= 20 along every shift-enabled dimension
+    spec = {}
+    for d, f in enumerate("xyz"):
+        ok = not ((bc == "mirror" and grid[d] < 2) or (bc == "fade" and grid[d] < 20))
+        spec[f] = bc if ok else "circ"
+    return spec
+
+
+def _settings(grid, bc, magnet, limiter=("vanleer", "minmod", "superbee"), cfl=0.35):
+    return dict(grid=grid, dgrid=tuple(1.0 / g for g in grid), gamma=5 / 3, cfl=cfl, bc=_bc_settings(bc, grid),
+                limiter=limiter, magnet=magnet, time_max=1e5, iter_max=10 ** 6)
+
+
+def _assert_close(o, g, tol, what=""):
+    e = errors(g.state(), o.state())
+    bad = {k: v for k, v in e.items() if not (v <= tol)}
+    assert not bad, f"{what}: relative L1 above {tol}: {bad}"
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("grid", [(32, 1, 1), (24, 22, 1), (22, 21, 20)])
+def test_fluid_sweep_single(bc, grid):
+    if bc == "fade" and grid[0] < 20:
+        pytest.skip("fade needs >= 20 cells")
+    s = _settings(grid, bc, magnet=False)
+    o, g = make_pair(s, smooth_state(grid, seed=1, mhd=False))
+    for X in (1, 2, 3):
+        if grid[X - 1] < 3:
+            continue
+        o.set_time(0.0, 1e-3, 1)
+        g.time.set(0.0, 1e-3, 1)
+        o.relaxing_fluid(X)
+        g.relaxing_fluid(X)
+        _assert_close(o, g, 1e-12, f"fluid sweep X={X}")
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("grid", [(24, 22, 1), (22, 21, 20)])
+def test_mhd_sweeps_single(bc, grid):
+    s = _settings(grid, bc, magnet=True)
+    o, g = make_pair(s, smooth_state(grid, seed=2, mhd=True))
+    mi = {1: (2, 3), 2: (1, 3), 3: (1, 2)}
+    for X in (1, 2, 3):
+        if grid[X - 1] < 3:
+            continue
+        o.set_time(0.0, 1e-3, 1)
+        g.time.set(0.0, 1e-3, 1)
+        o.relaxing_fluid(X)
+        g.relaxing_fluid(X)
+        _assert_close(o, g, 1e-12, f"MHD fluid sweep X={X}")
+        o.magnet_flux(X, mi[X])
+        g.magnet_flux(X, mi[X])
+        _assert_close(o, g, 1e-12, f"magnet sweep X={X}")
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("grid,magnet", [((48, 1, 1), False), ((24, 22, 1), True), ((20, 20, 21), True)])
+def test_iterations_fp64(bc, grid, magnet):
+    s = _settings(grid, bc, magnet=magnet)
+    o, g = make_pair(s, smooth_state(grid, seed=3, mhd=magnet))
+    o.run(10)
+    g.run(10)
+    assert abs(g.time.time - o.time) <= 1e-12 * max(1.0, o.time)
+    _assert_close(o, g, 1e-11, f"10 iterations bc={bc}")
+
+
+@pytest.mark.parametrize("name", ["sod", "orszag_tang", "kelvin_helmholtz", "brio_wu", "sedov2d", "sedov3d"])
+def test_workload_100_iterations_fp64(name):
+    """plain FP64 within 1e-10 relative L1 of the oracle after 100 iterations."""
+    if name == "sod":
+        s, st = problems.sod(256)
+    elif name == "orszag_tang":
+        s, st = problems.orszag_tang(64)
+    elif name == "kelvin_helmholtz":
+        s, st = problems.kelvin_helmholtz(16)
+    elif name == "brio_wu":
+        s, st = problems.brio_wu_tube(256, 1.0, 0.125, 1.0, 0.1)
+    elif name == "sedov2d":
+        s, st = problems.sedov(48, dims=2)
+    else:
+        s, st = problems.sedov(24, dims=3)
+    s = dict(s, iter_max=100, time_max=1e5)
+    o, g = make_pair(s, st)
+    no = o.run()
+    ng = g.run()
+    assert no == ng == 100
+    _assert_close(o, g, 1e-10, name)
