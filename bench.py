@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 relaxing-TVD MHD path (one JSON line on stdout, rank 0).
+
+Workload (default): Orszag-Tang vortex, 2-D ideal MHD, 512 x 512 periodic, gamma 5/3, synthetic
+IC (imogen_b200.problems.orszag_tang).  One bench step = one iteration of the reference main loop
+(imogen.m:60-66) = two timesteps, each sweeping X and Y (fluid + magnet), with the CFL timestep
+computed on the device.  Metric: zone-updates/s = cells x timesteps / s.  The state (16.8 MB FP64)
+fits in the 126 MB L2, so L2 is flushed (a 512 MB write) before every timed step and each step is
+timed alone with CUDA events on the library's stream.
+
+Headline `value` is the mixed-precision form (FP32 state and fluxes, FP64 pressure recovery and
+CFL); the plain FP64 form is measured in the same run (`fp64`), with the relative L1 error of the
+mixed state against the FP64 state after the same iterations (`l1_mixed_vs_fp64`).
+
+--impl reference times the C++ FP64 restatement of the reference (oracle/) on all host threads
+(the MATLAB reference itself cannot run here).  With torchrun (N > 1) every rank advances its own
+replica (the path does not shard: replicas only) and the max time over ranks is used.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAK_FALLBACK_GBS = 6650.0
+
+
+def measured_hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(name):
+    from imogen_b200 import problems
+    if name == "ot512":
+        s, st = problems.orszag_tang(512)
+        return s, st, "orszag_tang_512x512_mhd", 2, 16   # dims swept, MHD words/dir
+    if name == "kh256":
+        s, st = problems.kelvin_helmholtz(256)
+        return s, st, "kelvin_helmholtz_256^3_mhd", 3, 16
+    if name == "ot64":
+        s, st = problems.orszag_tang(64)
+        return s, st, "orszag_tang_64x64_mhd", 2, 16
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---------------------------------------------------------------------------------------------------
+def run_reference(args):
+    """C++ FP64 restatement of the reference path, all host threads, bounded sample."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import cpp_oracle
+    from imogen_b200 import problems
+    s, st, wname, _, _ = workload(args.workload)
+    ncell = int(np.prod(s["grid"]))
+    cores = os.cpu_count() or 1
+    cpp_oracle.set_threads(cores)
+    o = cpp_oracle.Sim(**problems.oracle_kwargs(dict(s, iter_max=10 ** 7, time_max=1e5)))
+    o.set_state(*st)
+    for _ in range(args.warmup):
+        o.iterate()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.iterate()
+    el = time.perf_counter() - t0
+    v = ncell * 2 * args.steps / el
+    line = {
+        "impl": "reference", "metric": "MHD zone-updates/s", "value": v, "unit": "zone-updates/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Orszag-Tang IC)",
+        "config": {"workload": wname, "cells": ncell, "step": "1 iteration = 2 timesteps",
+                   "l2": "host run"},
+        "cpu_baseline": {"value": v, "unit": "zone-updates/s", "cores": cpp_oracle.max_threads(),
+                         "kind": "port", "sample": f"{args.steps} iterations of {wname} after {args.warmup} warm-up"},
+        "e2e": {"value": v, "unit": "zone-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(s, st, wname, budget_s=20.0):
+    """The C++ oracle on all host threads, timed on a bounded number of iterations."""
+    from oracle import cpp_oracle
+    from imogen_b200 import problems
+    cores = os.cpu_count() or 1
+    cpp_oracle.set_threads(cores)
+    ncell = int(np.prod(s["grid"]))
+    o = cpp_oracle.Sim(**problems.oracle_kwargs(dict(s, iter_max=10 ** 7, time_max=1e5)))
+    o.set_state(*st)
+    o.iterate()   # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.iterate()
+        n += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or n >= 200:
+            break
+    return {"value": ncell * 2 * n / el, "unit": "zone-updates/s", "cores": cpp_oracle.max_threads(),
+            "kind": "port", "sample": f"{n} iterations of {wname} (C++ FP64 oracle, OpenMP)"}
+
+
+def run_ours(args):
+    import torch
+    import imogen_b200
+    from imogen_b200 import ImogenRun
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    s, st, wname, ndir, words = workload(args.workload)
+    ncell = int(np.prod(s["grid"]))
+    s = dict(s, iter_max=10 ** 7, time_max=1e5)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # 512 MB > 126 MB L2
+
+    def barrier():
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    def timed_steps(run, k, per_launch=None):
+        """k iterations, each after an L2 flush, each timed alone on the run's stream."""
+        ext = torch.cuda.ExternalStream(run.stream)
+        tot = 0.0
+        evs = []
+        for _ in range(k):
+            with torch.cuda.stream(ext):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+            (per_launch or run.iterate)()
+            with torch.cuda.stream(ext):
+                e1.record(ext)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            tot += e0.elapsed_time(e1) * 1e-3
+        return tot
+
+    results = {}
+    runs = {}
+    for prec in ("fp64", "mixed"):
+        r = ImogenRun(precision=prec, **s)
+        r.set_state(*st)
+        for _ in range(args.warmup):
+            r.iterate()
+        r.sync()
+        runs[prec] = r
+    clocks = ClockSampler(local)
+    launches = {}
+    with clocks:
+        for prec in ("fp64", "mixed"):
+            r = runs[prec]
+            barrier()
+            l0 = r.launches
+            el = timed_steps(r, args.steps)
+            launches[prec] = r.launches - l0
+            if ws > 1:
+                t = torch.tensor([el], device=dev, dtype=torch.float64)
+                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+                el = float(t.item())
+            results[prec] = el
+    clk = clocks.summary()
+
+    # relative L1 of mixed vs FP64 after the same iterations
+    sf, sm = runs["fp64"].state(), runs["mixed"].state()
+    l1 = {}
+    for k in ("mass", "ener"):
+        l1[k] = float(np.abs(sm[k] - sf[k]).sum() / np.abs(sf[k]).sum())
+    for k in ("mom", "mag"):
+        for c in range(3):
+            den = np.abs(sf[k][c]).sum()
+            if den > 0:
+                l1[f"{k}{'xyz'[c]}"] = float(np.abs(sm[k][c] - sf[k][c]).sum() / den)
+
+    # per-kernel roofline: the fused fluid sweep timed alone, L2 flushed before each launch
+    peak, peak_kind = measured_hbm_peak()
+    roof = {}
+    for prec in ("mixed", "fp64"):
+        r = runs[prec]
+        w = 4 if prec == "mixed" else 8
+        r.time.set(r.time.time, 1e-4, r.time.iteration)
+        el = timed_steps(r, max(5, args.steps), per_launch=lambda r=r: r.relaxing_fluid(1))
+        per = el / max(5, args.steps)
+        alg = ncell * (8 + 5) * w     # reads rho,p,E,cellB (8 words), writes rho,p,E (5 words)
+        roof[prec] = {"bound": "hbm", "achieved": alg / per / 1e9, "peak": peak, "unit": "GB/s",
+                      "frac": alg / per / 1e9 / peak, "traffic": None, "kernel": "fluid_sweep_kernel X",
+                      "launch_us": per * 1e6, "alg_bytes": alg, "peak_kind": peak_kind}
+
+    # end to end through the C ABI: the step's state comes from pinned host memory (X.array = ...
+    # for the 8 conserved arrays), one iteration runs, and the 8 arrays are read back to pinned host
+    # memory (get.array), every step.
+    e2e = None
+    r = runs["mixed"]
+    names = ("mass", "momx", "momy", "momz", "ener", "magx", "magy", "magz")
+    src = [st[0], st[1][0], st[1][1], st[1][2], st[2], st[3][0], st[3][1], st[3][2]]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F"))
+                                     ).pin_memory().numpy()
+    ins = [pin(a) for a in src]
+    outs = [pin(np.zeros(ncell)) for _ in range(8)]
+    ke = max(3, args.steps // 2)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        for nm, a in zip(names, ins):
+            r.upload(nm, a)
+        r.iterate()
+        for nm, o in zip(names, outs):
+            r.download(nm, out=o)
+    r.sync()
+    el = time.perf_counter() - t0
+    e2e = {"value": ncell * 2 * ke / el, "unit": "zone-updates/s",
+           "h2d_bytes_per_step": 8 * ncell * 8, "d2h_bytes_per_step": 8 * ncell * 8,
+           "form": "mixed", "steps": ke}
+
+    if rank == 0:
+        v = ncell * 2 * args.steps * ws / results["mixed"]
+        v64 = ncell * 2 * args.steps * ws / results["fp64"]
+        line = {
+            "metric": "MHD zone-updates/s", "value": v, "unit": "zone-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * results["mixed"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded Orszag-Tang IC, no dataset)",
+            "config": {"workload": wname, "cells": ncell, "form": "mixed (FP32 state/fluxes, FP64 pressure+CFL)",
+                       "step": "1 iteration = 2 timesteps (X,Y fluid+magnet each)",
+                       "l2": "flushed (512 MB write) before every timed step", "parallelism": f"replicas x{ws}"},
+            "fp64": {"value": v64, "unit": "zone-updates/s", "ms_per_step": 1e3 * results["fp64"] / args.steps},
+            "mixed_over_fp64": v / v64,
+            "l1_mixed_vs_fp64": l1,
+            "l1_mixed_vs_fp64_max": max(l1.values()),
+            "roofline": roof["mixed"],
+            "roofline_fp64": roof["fp64"],
+            "gpu_launches": launches["mixed"],
+            "clocks": clk,
+            "e2e": e2e,
+            "p50_p99_job_latency": None,
+        }
+        if not args.no_cpu_baseline and ws == 1:
+            line["cpu_baseline"] = cpu_baseline(s, st, wname, budget_s=args.cpu_budget)
+        print(json.dumps(line), flush=True)
+    for r in runs.values():
+        r.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ot512")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -23,6 +23,7 @@ SYMBOLS = (
     "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
     "img_get_time", "img_set_time", "img_totals", "img_sync", "img_last_error", "img_bytes_required",
+    "img_get_stream", "img_launch_count",
 )
 
 
@@ -59,9 +60,8 @@ def lib():
     global _LIB
     if _LIB is not None:
         return _LIB
-    if not os.path.exists(LIB_PATH):
-        from . import build
-        build.build()
+    from . import build
+    build.build()   # no-op when libimogen_b200.so is newer than its sources
     L = ctypes.CDLL(LIB_PATH)
     vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
     cfgp = ctypes.POINTER(ImgConfig)
@@ -86,6 +86,10 @@ def lib():
     L.img_last_error.restype = ctypes.c_char_p
     L.img_bytes_required.argtypes = [cfgp]
     L.img_bytes_required.restype = ctypes.c_size_t
+    L.img_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.img_get_stream.restype = ctypes.c_int
+    L.img_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.img_launch_count.restype = ctypes.c_int
     for name in ("img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
                  "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step",
                  "img_run", "img_get_time", "img_set_time", "img_totals", "img_sync"):

@@ -31,7 +31,13 @@ def up_to_date(out=OUT, deps=DEPS):
 
 
 def build(force=False, verbose=False, extra=()):
-    """Compile csrc/imogen_b200.cu into libimogen_b200.so (static cudart, -fPIC)."""
+    """Compile csrc/imogen_b200.cu into libimogen_b200.so (static cudart, -fPIC).
+
+    IMOGEN_CHECKED=1 in the environment adds -DIMG_CHECKED (access checks that record instead of
+    faulting), for diagnosing a kernel on a small case."""
+    if os.environ.get("IMOGEN_CHECKED") == "1":
+        extra = tuple(extra) + ("-DIMG_CHECKED",)
+        force = True
     if not force and up_to_date():
         return OUT
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",

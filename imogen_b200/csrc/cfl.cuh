@@ -21,7 +21,7 @@ struct CflArgs {
 };
 
 template <typename T>
-__global__ void cfl_reduce_kernel(const CflArgs a) {
+__global__ void __launch_bounds__(256) cfl_reduce_kernel(const __grid_constant__ CflArgs a) {
     if (a.tm->done || a.tm->error) return;
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
@@ -44,10 +44,18 @@ __global__ void cfl_reduce_kernel(const CflArgs a) {
         m3[1] = fmax(m3[1], fabs(py / r) + cs);
         m3[2] = fmax(m3[2], fabs(pz / r) + cs);
     }
+    __shared__ double wp[3][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         for (int o = 16; o > 0; o >>= 1) m3[c] = fmax(m3[c], __shfl_xor_sync(0xffffffffu, m3[c], o));
-        if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&a.tm->maxbits[c], m3[c]);
+        if (lane == 0) wp[c][warp] = m3[c];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {   // one global atomic per block and direction
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, wp[threadIdx.x][w]);
+        atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
     }
 }
 
@@ -100,7 +108,7 @@ struct CellMagInitArgs {
 };
 
 template <typename T>
-__global__ void cellmag_init_kernel(const CellMagInitArgs a) {
+__global__ void cellmag_init_kernel(const __grid_constant__ CellMagInitArgs a) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3 * a.g.ncell;
          i += (long long)gridDim.x * blockDim.x) {
         int cpt = (int)(i / a.g.ncell);

@@ -23,7 +23,21 @@ enum BcClass { CLS_MASS = 0, CLS_MOM = 1, CLS_ENER = 2, CLS_MAG = 3 };
 enum Var { Q_RHO = 0, Q_PX, Q_PY, Q_PZ, Q_E, Q_BX, Q_BY, Q_BZ, Q_CBX, Q_CBY, Q_CBZ, NQ };
 
 // Error bits written by kernels into DevTime::error (host reads them after a step).
-enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2, DERR_GEOMETRY = 4 };
+enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2, DERR_GEOMETRY = 4, DERR_CHECK = 8 };
+
+// Checked builds (-DIMG_CHECKED) verify pointer alignment and index ranges before selected accesses,
+// record the first failure in a global word, and skip the access instead of faulting.
+#ifdef IMG_CHECKED
+__device__ int g_check_site;
+__device__ int g_check_val;
+__device__ __forceinline__ bool img_check(bool ok, int site, long long val) {
+    if (!ok && atomicCAS(&g_check_site, 0, site) == 0) g_check_val = (int)val;
+    return ok;
+}
+#define IMG_CHECK(cond, site, val) img_check((cond), (site), (long long)(val))
+#else
+#define IMG_CHECK(cond, site, val) true
+#endif
 
 // ---- stored-edge objects ------------------------------------------------------------------------
 // Every array object of the reference that can be shifted under a stateful BC (trans, wall) owns a
@@ -60,6 +74,8 @@ struct DevTime {
     int update_mode;        // 0 per step, 1 per iteration
     int error;              // DevError bits
     int done;               // TimeManager.running turned false (time >= TIMEMAX)
+    int dbg_site;           // checked builds: first failing access check (site id) ...
+    int dbg_val;            // ... and the offending index
     unsigned long long maxbits[3];   // per-direction max of |v_i| + c_s (bit pattern, >= 0)
     unsigned int counter;            // CTAs finished in the current CFL reduction
     unsigned int pad2;
@@ -95,7 +111,10 @@ template <typename T>
 __device__ __forceinline__ T limiter_corr(int lim, T dL, T dR) {
     if (lim == LIM_VANLEER) {
         T p = dL * dR;
-        T st = (p > T(0) ? p : T(0)) / (dL + dR);
+        T num = p > T(0) ? p : T(0);
+        T st;
+        if constexpr (sizeof(T) == 4) st = __fdividef(num, dL + dR);   // mixed form: fast divide
+        else st = num / (dL + dR);
         return isnan(st) ? T(0) : st;
     }
     if (lim == LIM_SUPERBEE) {
@@ -114,42 +133,42 @@ __device__ __forceinline__ double edge_drift(double old_e, double cur) {
     return old_e + ((st ? 1.0 : 0.0) - (st ? 0.0 : 1.0)) * delta;
 }
 
-// MATLAB pchip through x = [1 2 3 inf inf+1] with y[0..4], evaluated at xe (>= 3).
-// Interior slopes: Fritsch-Butland weighted harmonic mean; end slopes: one-sided,
-// shape-preserving (Moler, "Numerical Computing with MATLAB", pchiptx).
-__device__ __noinline__ double pchip5(const double y[5], double inf, double xe) {
-    const double x[5] = {1.0, 2.0, 3.0, inf, inf + 1.0};
-    double h[4], del[4], d[5];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        h[k] = x[k + 1] - x[k];
-        del[k] = (y[k + 1] - y[k]) / h[k];
-    }
-#pragma unroll
-    for (int k = 1; k < 4; ++k) {
-        double w1 = 2 * h[k] + h[k - 1];
-        double w2 = h[k] + 2 * h[k - 1];
-        d[k] = (msign(del[k - 1]) * msign(del[k]) > 0) ? (w1 + w2) / (w1 / del[k - 1] + w2 / del[k]) : 0.0;
-    }
-    {
-        double dd = ((2 * h[0] + h[1]) * del[0] - h[0] * del[1]) / (h[0] + h[1]);
-        if (msign(dd) != msign(del[0])) dd = 0.0;
-        else if (msign(del[0]) != msign(del[1]) && fabs(dd) > fabs(3 * del[0])) dd = 3 * del[0];
-        d[0] = dd;
-        dd = ((2 * h[3] + h[2]) * del[3] - h[3] * del[2]) / (h[3] + h[2]);
-        if (msign(dd) != msign(del[3])) dd = 0.0;
-        else if (msign(del[3]) != msign(del[2]) && fabs(dd) > fabs(3 * del[3])) dd = 3 * del[3];
-        d[4] = dd;
-    }
-    int k = 0;
-#pragma unroll
-    for (int q = 0; q < 5; ++q)
-        if (x[q] <= xe) k = q;
-    k = k > 3 ? 3 : k;
-    double s = xe - x[k];
-    double c1 = (d[k] + d[k + 1] - 2 * del[k]) / (h[k] * h[k]);
-    double c2 = (3 * del[k] - 2 * d[k] - d[k + 1]) / h[k];
-    return ((c1 * s + c2) * s + d[k]) * s + y[k];
+// One-sided shape-preserving end slope of MATLAB pchip (pchipslopes end formula).
+__device__ __forceinline__ double pchip_end_slope(double h0, double h1, double d0, double d1) {
+    double dd = ((2 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+    if (msign(dd) != msign(d0)) dd = 0.0;
+    else if (msign(d0) != msign(d1) && fabs(dd) > fabs(3 * d0)) dd = 3 * d0;
+    return dd;
+}
+// Interior slope: Fritsch-Butland weighted harmonic mean, 0 at sign changes.
+__device__ __forceinline__ double pchip_mid_slope(double hl, double hr, double dl, double dr) {
+    double w1 = 2 * hr + hl;
+    double w2 = hr + 2 * hl;
+    return (msign(dl) * msign(dr) > 0) ? (w1 + w2) / (w1 / dl + w2 / dr) : 0.0;
+}
+
+// MATLAB pchip through x = [1 2 3 inf inf+1] with values y0..y4, evaluated at xe >= 3 (Moler,
+// "Numerical Computing with MATLAB", pchiptx; the interval is the last breakpoint <= xe, clamped
+// to the last interval as ppval does).  Scalars only: no local-memory arrays.
+__device__ __forceinline__ double pchip5(double y0, double y1, double y2, double y3, double y4, double inf,
+                                         double xe) {
+    const double x3 = inf, x4 = inf + 1.0;
+    const double h0 = 1.0, h1 = 1.0, h2 = x3 - 3.0, h3 = x4 - x3;
+    const double e0 = (y1 - y0) / h0, e1 = (y2 - y1) / h1, e2 = (y3 - y2) / h2, e3 = (y4 - y3) / h3;
+    const double s0 = pchip_end_slope(h0, h1, e0, e1);
+    const double s1 = pchip_mid_slope(h0, h1, e0, e1);
+    const double s2 = pchip_mid_slope(h1, h2, e1, e2);
+    const double s3 = pchip_mid_slope(h2, h3, e2, e3);
+    const double s4 = pchip_end_slope(h3, h2, e3, e2);
+    double xk, yk, hk, ek, dk, dk1;
+    if (xe >= x3) { xk = x3; yk = y3; hk = h3; ek = e3; dk = s3; dk1 = s4; }
+    else if (xe >= 3.0) { xk = 3.0; yk = y2; hk = h2; ek = e2; dk = s2; dk1 = s3; }
+    else if (xe >= 2.0) { xk = 2.0; yk = y1; hk = h1; ek = e1; dk = s1; dk1 = s2; }
+    else { xk = 1.0; yk = y0; hk = h0; ek = e0; dk = s0; dk1 = s1; }
+    const double s = xe - xk;
+    const double c1 = (dk + dk1 - 2 * ek) / (hk * hk);
+    const double c2 = (3 * ek - 2 * dk - dk1) / hk;
+    return ((c1 * s + c2) * s + dk) * s + yk;
 }
 
 // Rows that transparent_shift.m:36-39 / :68-71 feed to pchip at x = 1, 2, 3 for a shift by
@@ -171,10 +190,9 @@ __host__ __device__ __forceinline__ int trans_pick_upper(int N, int m, int q) {
 // the reference feeds at x = 1, 2, 3 (x = 3 is the edge cell), edge = the stored edge after its
 // drift (0 when the edge store is not ACTIVE(DIRECT)), xe = 4 or 5, orig = the unshifted array
 // value at the ghost position (kept when the extrapolation is within 1e-4 of it).
-__device__ __noinline__ double trans_ghost(double y0, double y1, double y2, double edge, double inf, double xe,
-                                           double orig) {
-    double y[5] = {y0, y1, y2, edge, edge};
-    double out = pchip5(y, inf, xe);
+__device__ __forceinline__ double trans_ghost(double y0, double y1, double y2, double edge, double inf, double xe,
+                                              double orig) {
+    double out = pchip5(y0, y1, y2, edge, edge, inf, xe);
     bool t = fabs(orig - out) < 1e-4;
     return (t ? 0.0 : 1.0) * out + (t ? 1.0 : 0.0) * orig;
 }
@@ -195,6 +213,28 @@ __device__ __forceinline__ PressOut pressure_totsnd(double G, double rho, double
     o.p = r < 0 ? 0.0 : r;
     return o;
 }
+// Mixed form of 'totsnd' for FP32 state: the pressure recovery P0 = (G-1)(E - rho v^2/2) and the
+// magnetic terms are evaluated in FP64 (the reciprocal of rho is an FP32 estimate refined by one
+// FP64 Newton step, exact to ~1e-15), the sound speed is taken in FP32.
+struct PressOutF {
+    float p;
+    float cs;
+};
+__device__ __forceinline__ PressOutF pressure_totsnd_mixed(double G, float rho, float px, float py, float pz, float E,
+                                                          double msq) {
+    double r = rho;
+    double inv = (double)__frcp_rn(rho);
+    inv = inv * (2.0 - r * inv);
+    double psq = (double)px * px + (double)py * py + (double)pz * pz;
+    double p0 = (G - 1.0) * ((double)E - 0.5 * psq * inv);
+    double pg = p0 - (G - 1.0) * 0.5 * msq;
+    PressOutF o;
+    o.cs = sqrtf((float)fabs((G * pg + 2.0 * msq) * inv));
+    double pt = p0 + 0.5 * (2.0 - G) * msq;
+    o.p = pt < 0 ? 0.f : (float)pt;
+    return o;
+}
+
 __device__ __forceinline__ double sound_speed(double G, double rho, double px, double py, double pz, double E,
                                               double msq) {
     double vsq = (px * px + py * py + pz * pz) / (rho * rho);

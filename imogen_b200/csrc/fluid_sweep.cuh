@@ -1,11 +1,15 @@
 // Fused relaxing-TVD fluid sweep along one dimension (fluid/relaxingFluid.m:16-73,
 // fluid/wFluidFlux.m:14-44, pressure/pressure.m:23-64, flux/*Limiter.m).
 //
-// One launch updates rho, p and E for every cell: per pencil it computes the freezing speed
-// (pencil max of |v| + c_s, a column reduction), the predictor half step, the second freezing
-// speed on the half-step state, and the TVD-limited corrector, with the boundary ghosts of the
-// four flux arrays of each variable synthesised in the same pass.  State is read once and written
-// once; nothing else touches HBM except the stored edges of stateful boundaries (trans, wall).
+// One launch updates rho, p and E of every cell: per pencil it computes the freezing speed (the
+// pencil max of |v| + c_s, a column reduction), the predictor half step, the second freezing speed
+// on the half-step state, and the TVD-limited corrector; the boundary ghosts of the four flux
+// arrays of each variable are synthesised in the same pass.  The state is read once and written
+// once; the only other HBM traffic is the stored edges of stateful boundaries (trans, wall).
+//
+// Shared memory: two sets of ten flux arrays (R and L of the five variables) -- set A holds the
+// predictor fluxes and then the corrector fluxes, set B the half-step state and then the limited
+// corrector fluxes -- plus the ghost slots of the ten arrays of the current stage.
 #pragma once
 
 #include "pencil.cuh"
@@ -33,353 +37,342 @@ struct FluidArgs {
     int cfl;               // accumulate the CFL maxima of the new state (fused TimeManager pass)
 };
 
-constexpr int FLUID_NSLOT = 10;
+constexpr int FLUID_NARR = 20;
+constexpr int MAX_WARPS = 16;
+
+// Dynamic shared memory of the fluid kernel: 20 arrays of RC*Wb values + ghost slots of 10 arrays.
+template <typename T>
+__host__ __device__ inline size_t fluid_smem_bytes(int RC, int Wb) {
+    return sizeof(T) * (size_t)FLUID_NARR * RC * Wb + sizeof(Ghost<T>) * 10 * 2 * (size_t)Wb;
+}
 
 template <typename T>
 __device__ __forceinline__ T ldq(const void* p, long long i) { return reinterpret_cast<const T*>(p)[i]; }
 template <typename T>
 __device__ __forceinline__ void stq(void* p, long long i, T v) { reinterpret_cast<T*>(p)[i] = v; }
 
+// BC class of fluid variable v (rho -> mass, p_i -> mom, E -> ener).
+__device__ __forceinline__ int fluid_class(int v) { return v == 0 ? CLS_MASS : (v == 4 ? CLS_ENER : CLS_MOM); }
+
 // w arrays of wFluidFlux.m:31-44 for one cell (X = sweep dim d).
 template <typename T>
 __device__ __forceinline__ void wflux(int d, const T u[5], const T bb[3], T press, T cf, T w[5]) {
     const T pX = sel3(d, u[1], u[2], u[3]);
-    T velocity = pX / u[0];
-    w[0] = pX / cf;
     T bX = sel3(d, bb[0], bb[1], bb[2]);
-    T we = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) / u[0];
-    w[4] = we / cf;
+    if constexpr (sizeof(T) == 4) {   // mixed form: one reciprocal each for rho and c_f
+        const T ir = __frcp_rn(u[0]), ic = __frcp_rn(cf);
+        const T velocity = pX * ir;
+        w[0] = pX * ic;
+        w[4] = (velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir) * ic;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        T dirv = c == d ? T(1) : T(0);
-        w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) / cf;
+        for (int c = 0; c < 3; ++c) {
+            T dirv = c == d ? T(1) : T(0);
+            w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) * ic;
+        }
+    } else {   // plain FP64: the operation order of wFluidFlux.m
+        T velocity = pX / u[0];
+        w[0] = pX / cf;
+        T we = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) / u[0];
+        w[4] = we / cf;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            T dirv = c == d ? T(1) : T(0);
+            w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) / cf;
+        }
     }
 }
 
-// Column max over the pencil (and over the cluster): returns the max for this thread's column.
-template <typename T, int CPT, int NSLOT, bool H2>
-__device__ double column_max(Pencil<T, CPT, NSLOT, H2>& pc, unsigned long long* red, double local) {
-    const SweepGeom& s = *pc.sg;
-    // lanes that share a column: d == 0 -> consecutive groups of min(G,32); else stride Wb
-    unsigned mask = 0xffffffffu;
-    if (s.d == 0) {
-        int w = s.G < 32 ? s.G : 32;
-        for (int o = w / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+// 'totsnd' pressure and the freezing-speed candidate |p_X / rho| + c_s of one cell.
+template <typename T>
+__device__ __forceinline__ T press_speed(double G, int d, const T u[5], double msq, T& p) {
+    const T pX = sel3(d, u[1], u[2], u[3]);
+    if constexpr (sizeof(T) == 4) {
+        PressOutF o = pressure_totsnd_mixed(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p;
+        return fabsf(pX * __frcp_rn(u[0])) + o.cs;
     } else {
-        for (int o = 16; o >= s.Wb; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        PressOut o = pressure_totsnd(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p + 0.0;   // + viscosity.solve ('empty' -> 0)
+        return fabs(pX / u[0]) + o.cs;
     }
-    if (pc.colok) atomic_max_nonneg(&red[pc.b], local);
-    pc.csync();
-    double m = __longlong_as_double((long long)red[pc.b]);
-    for (int r = 0; r < s.CL; ++r) {
-        if (r == pc.rank) continue;
-        unsigned long long* rp = pc.remote(red, r);
-        m = fmax(m, __longlong_as_double((long long)rp[pc.b]));
+}
+
+// Column max over the pencil (and the cluster); also a full stage barrier (tl.csync).  Lanes of a
+// column reduce with warp shuffles; where a pencil spans several warps one lane per (warp, column)
+// writes part[warp][b] and every thread then takes the max over the warps of all CTAs of its
+// cluster.  No atomics: every slot has exactly one writer, and part is zero beforehand.
+template <typename T, int CPT>
+__device__ __forceinline__ double column_max(const Tile<T, CPT>& tl, int NT, double (*part)[32], double local) {
+    const unsigned mask = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (tl.d == 0 && tl.G <= 32 && tl.CL == 1) {   // each pencil lies inside one warp
+        for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        tl.csync();
+        return local;
+    }
+    bool leader;
+    if (tl.d == 0) {   // G is a multiple of 32: one column per warp
+        for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        leader = lane == 0;
+    } else {           // lanes b, b + Wb, ... belong to column b
+        for (int o = 16; o >= tl.Wb; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        leader = lane < tl.Wb;
+    }
+    if (leader) part[warp][tl.b] = local;
+    tl.csync();
+    const int nw = NT >> 5;
+    double m = 0.0;
+    for (int r = 0; r < tl.CL; ++r) {
+        double (*rp)[32] = tl.remote(part, r);
+        for (int w = 0; w < nw; ++w) m = fmax(m, rp[w][tl.b]);
     }
     return m;
 }
 
-// Ghost value at the pencil end for A.shift(d, -1)[0] (lower) or A.shift(d, +1)[N-1] (upper),
-// for the modes without fade damping (fade uses the const ghost, damping applied by the caller).
-// edge_ptr: stored edge slice of this object for (d, side) or nullptr.
-template <typename T, int CPT, int NSLOT, bool H2>
-__device__ T end_ghost(const Pencil<T, CPT, NSLOT, H2>& pc, int slot, bool upper, int mode, int act, bool flip,
-                       double* edge_ptr, double bc_inf) {
-    int N = pc.sg->N;
-    switch (mode) {
-        case BC_CIRC: return upper ? pc.endv(slot, 0) : pc.endv(slot, N - 1);
-        case BC_MIRROR: { T v = upper ? pc.endv(slot, N - 2) : pc.endv(slot, 1); return flip ? -v : v; }
-        case BC_WALL: return (T)edge_ptr[pc.col];
-        case BC_TRANS: {
-            double e = 0.0;
-            T a0, a1, a2;   // array values at x = 1, 2, 3 (x = 3 is the edge cell)
-            if (!upper) {
-                a0 = pc.endv(slot, trans_pick_lower(N, 1, 0));
-                a1 = pc.endv(slot, trans_pick_lower(N, 1, 1));
-                a2 = pc.endv(slot, 0);
-            } else {
-                a0 = pc.endv(slot, trans_pick_upper(N, 1, 0));
-                a1 = pc.endv(slot, trans_pick_upper(N, 1, 1));
-                a2 = pc.endv(slot, N - 1);
-            }
-            if (act) {
-                e = edge_drift(edge_ptr[pc.col], (double)a2);
-                edge_ptr[pc.col] = e;
-            }
-            return (T)trans_ghost((double)a0, (double)a1, (double)a2, e, bc_inf, 4.0, (double)a2);
-        }
-        default:   // const and fade (const ghost)
-            return upper ? pc.endv(slot, N - 1) : pc.endv(slot, 0);
-    }
-}
-
-// A.shift(d, -1) (sm) and A.shift(d, +1) (sp) at this thread's rows for array A published in `slot`.
-template <typename T, int CPT, int NSLOT, bool H2>
-__device__ void shifted(const Pencil<T, CPT, NSLOT, H2>& pc, const FluidArgs& a, int slot, const T (&A)[CPT], int cls,
-                        bool flip, bool need_m, bool need_p, double* e_lo, double* e_hi, T (&sm)[CPT], T (&sp)[CPT]) {
-    const int N = pc.sg->N;
-    const int mlo = a.mode[cls][0], mhi = a.mode[cls][1];
-    T glo = T(0), ghi = T(0);
-    bool own0 = pc.nv > 0 && pc.r0 == 0;
-    bool ownN = pc.nv > 0 && pc.r0 + pc.nv - 1 == N - 1;
-    if (need_m && own0) glo = end_ghost(pc, slot, false, mlo, a.act[cls], flip, e_lo, a.bc_inf);
-    if (need_p && ownN) ghi = end_ghost(pc, slot, true, mhi, a.act[cls], flip, e_hi, a.bc_inf);
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        if (k >= pc.nv) { sm[k] = T(0); sp[k] = T(0); continue; }
-        int r = pc.r0 + k;
-        if (need_m) {
-            T v = r == 0 ? glo : pc.prev(slot, A, k);
-            if (mlo == BC_FADE) v = fade_apply(v, r, N, a.fade, a.fade_f, pc.endv(slot, 0), pc.endv(slot, N - 2));
-            sm[k] = v;
-        }
-        if (need_p) {
-            T v = r == N - 1 ? ghi : pc.next(slot, A, k);
-            if (mhi == BC_FADE) v = fade_apply(v, r, N, a.fade, a.fade_f, pc.endv(slot, 1), pc.endv(slot, N - 1));
-            sp[k] = v;
-        }
-    }
-}
-
 // First assignment of an InitializedArray takes its stored edges on every face it lies on
 // (classes/InitializedArray.m:43-47 -> Edges.m:37-110).
-template <typename T, int CPT, int NSLOT, bool H2>
-__device__ void init_edges(const Pencil<T, CPT, NSLOT, H2>& pc, const EdgeTable* et, int obj, const T (&A)[CPT]) {
-    const Geom& g = pc.sg->g;
+__device__ __forceinline__ void init_edges_cell(const Geom& g, const EdgeTable* et, int obj, int x, int y, int z,
+                                                double v) {
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        if (k >= pc.nv) continue;
-        int x, y, z;
-        pc.coords(k, x, y, z);
-#pragma unroll
-        for (int e = 0; e < 3; ++e) {
-            if (e >= g.ndims) continue;
-            double* lo = et->p[obj][e][0];
-            double* hi = et->p[obj][e][1];
-            int ce = sel3(e, x, y, z);
-            long long fi = face_index(g, e, x, y, z);
-            if (lo && ce == 0) lo[fi] = (double)A[k];
-            if (hi && ce == g.n[e] - 1) hi[fi] = (double)A[k];
-        }
+    for (int e = 0; e < 3; ++e) {
+        if (e >= g.ndims) continue;
+        const int ce = sel3(e, x, y, z);
+        const int ne = sel3(e, g.n[0], g.n[1], g.n[2]);
+        if (ce != 0 && ce != ne - 1) continue;
+        double* lo = et->p[obj][e][0];
+        double* hi = et->p[obj][e][1];
+        const long long fi = face_index(g, e, x, y, z);
+        if (lo && ce == 0) lo[fi] = v;
+        if (hi && ce == ne - 1) hi[fi] = v;
+    }
+}
+
+__device__ __forceinline__ bool on_face(const Geom& g, int x, int y, int z) {
+    return x == 0 || x == g.n[0] - 1 || y == 0 || y == g.n[1] - 1 || (g.ndims > 2 && (z == 0 || z == g.n[2] - 1));
+}
+
+// Ghost jobs of one stage for the ten arrays R_v (= base + v*AS) and L_v (= base + (5+v)*AS):
+// `lo_mask`/`hi_mask` (bit 0: R, bit 1: L) select which sides this stage shifts.  Lower ghosts are
+// computed on cluster rank 0, upper ghosts on the rank holding the last row, by the threads of each
+// column in turn; `kindR/kindL` name the fluid objects whose stored edges are used.  Each job is one
+// shift call of the reference, so a trans edge drifts exactly once per job.
+template <typename T, int CPT>
+__device__ __forceinline__ void fluid_ghost_jobs(const Tile<T, CPT>& tl, const FluidArgs& a, const T* base, size_t AS,
+                                                 Ghost<T>* GS, int lo_mask, int hi_mask, int kindR, int kindL) {
+    if (!tl.colok) return;
+    const int d = tl.d;
+    const bool do_lo = tl.rank == 0, do_hi = tl.rank == tl.rank_hi();
+    if (!do_lo && !do_hi) return;
+    for (int j = tl.g; j < 20; j += tl.G) {   // job j: array j % 10 (R0..R4, L0..L4), side j / 10
+        const int arr = j % 10, side = j / 10;
+        const int isL = arr >= 5, v = arr - 5 * isL;
+        if (side == 0 && !(do_lo && (lo_mask >> isL & 1))) continue;
+        if (side == 1 && !(do_hi && (hi_mask >> isL & 1))) continue;
+        const int cls = fluid_class(v);
+        double* edge = a.edges->p[fluid_obj(v, isL ? kindL : kindR)][d][side];
+        fill_ghost(tl, base + arr * AS, GS + arr * 2 * tl.Wb, side ? +1 : -1, a.mode[cls][side], a.act[cls],
+                   v == 1 + d, edge, a.bc_inf);
     }
 }
 
 template <typename T, bool MHD, int CPT>
-__global__ void __launch_bounds__(512) fluid_sweep_kernel(const FluidArgs a) {
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
-    __shared__ unsigned long long red[2][32];
-    using PC = Pencil<T, CPT, FLUID_NSLOT>;
-    PC pc;
-    pc.init(a.sg, smem);
+    __shared__ double part[2][MAX_WARPS][32];   // per-warp column maxima (two freezing speeds)
+    __shared__ double cflp[3][MAX_WARPS];       // per-warp CFL maxima
+    Tile<T, CPT> tl;
+    tl.init(a.sg);
     const int d = a.sg.d;
-    for (int i = threadIdx.x; i < 64; i += blockDim.x) (&red[0][0])[i] = 0ull;
+    const int NT = a.sg.NT;
+    const size_t AS = (size_t)tl.RC * tl.Wb;
+    T* SA = reinterpret_cast<T*>(smem);   // set A: R[v] at SA + v*AS, L[v] at SA + (5+v)*AS
+    T* SB = SA + 10 * AS;                 // set B
+    Ghost<T>* GS = reinterpret_cast<Ghost<T>*>(SA + 20 * AS);   // [array][side][column]
+    for (int i = threadIdx.x; i < 2 * MAX_WARPS * 32; i += blockDim.x) (&part[0][0][0])[i] = 0.0;
     __syncthreads();
 
     const double G = a.gamma;
     const double dt = a.tm->dt;
     const T ff = (T)(dt / a.dx);
     const T half_ffx = (T)(0.5 * (dt / a.dx));
+    const double* fc = a.fade;
+    const int fw = a.fade_f;
 
-    // ---- load u (rho, px, py, pz, E) and cell-centred B --------------------------------------------
-    T u[5][CPT], bb[3][CPT];
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        if (pc.valid(k)) {
-            long long o = pc.off(k);
-#pragma unroll
-            for (int v = 0; v < 5; ++v) u[v][k] = ldq<T>(a.q[v], o);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) bb[c][k] = MHD ? ldq<T>(a.q[Q_CBX + c], o) : T(0);
-        } else {
-#pragma unroll
-            for (int v = 0; v < 5; ++v) u[v][k] = v == 0 ? T(1) : T(0);
-#pragma unroll
-            for (int c = 0; c < 3; ++c) bb[c][k] = T(0);
-        }
-    }
-
-    auto msq_of = [&](int k) -> double {
-        double m = 0.0;
-        if (MHD) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (a.use_b[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
-        }
-        return m;
-    };
-
-    // ---- freezing speed #1 (wFluidFlux.m:18-22) ----------------------------------------------------
-    T press[CPT];
+    // ---- load u (rho, px, py, pz, E) and cell-centred B; freezing speed #1 (wFluidFlux.m:18-22) --
+    T u[5][CPT], bb[3][CPT], press[CPT];
+    double msq[CPT];
     double lmax = 0.0;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        PressOut po = pressure_totsnd(G, u[0][k], u[1][k], u[2][k], u[3][k], u[4][k], msq_of(k));
-        press[k] = (T)(po.p + 0.0);
-        T cs = (T)po.cs;
-        T spd = fabs(sel3(d, u[1][k], u[2][k], u[3][k]) / u[0][k]) + cs;
-        if (pc.valid(k)) lmax = fmax(lmax, (double)spd);
+        const bool ok = tl.ok(k);
+        const long long o = tl.off(k);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) u[v][k] = ok ? ldq<T>(a.q[v], o) : (v == 0 ? T(1) : T(0));
+        double m = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            bb[c][k] = (MHD && ok) ? ldq<T>(a.q[Q_CBX + c], o) : T(0);
+            if (MHD && a.use_b[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+        }
+        msq[k] = m;
+        T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+        T spd = press_speed<T>(G, d, uu, m, press[k]);
+        if (ok) lmax = fmax(lmax, (double)spd);
     }
-    const T cf = (T)column_max(pc, red[0], lmax);
+    const T cf = (T)column_max(tl, NT, part[0], lmax);
 
-    // ---- predictor (relaxingFluid.m:30-39) ----------------------------------------------------------
-    T R[5][CPT], L[5][CPT];
+    // ---- predictor fluxes R = (u+w)/2, L = (u-w)/2 -> set A (relaxingFluid.m:30-31) ---------------
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
         T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
         T w[5];
         wflux<T>(d, uu, b3, press[k], cf, w);
+        const int ix = tl.idx(k);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            R[v][k] = T(0.5) * (uu[v] + w[v]);
-            L[v][k] = T(0.5) * (uu[v] - w[v]);
+            SA[v * AS + ix] = T(0.5) * (uu[v] + w[v]);
+            SA[(5 + v) * AS + ix] = T(0.5) * (uu[v] - w[v]);
+        }
+        if (a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(a.sg.g, x, y, z)) {
+#pragma unroll 1
+                for (int arr = 0; arr < 10; ++arr)
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(arr % 5, arr < 5 ? FO_STORE_R : FO_STORE_L), x, y,
+                                    z, (double)SA[arr * AS + ix]);
+            }
         }
     }
-    const EdgeTable* et = a.edges;
-    const int cls_of[5] = {CLS_MASS, CLS_MOM, CLS_MOM, CLS_MOM, CLS_ENER};
-    if (a.init_store) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            init_edges(pc, et, fluid_obj(v, FO_STORE_R), R[v]);
-            init_edges(pc, et, fluid_obj(v, FO_STORE_L), L[v]);
-        }
-    }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        pc.publish(v, R[v]);
-        pc.publish(5 + v, L[v]);
-    }
-    pc.csync();
-    T us[5][CPT];
-    {
-        T sm[CPT], sp[CPT], dummy[CPT];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            bool flip = (v == 1 + d);
-            int cls = cls_of[v];
-            shifted(pc, a, v, R[v], cls, flip, true, false, et->p[fluid_obj(v, FO_STORE_R)][d][0], nullptr, sm, dummy);
-            shifted(pc, a, 5 + v, L[v], cls, flip, false, true, nullptr, et->p[fluid_obj(v, FO_STORE_L)][d][1], dummy,
-                    sp);
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) us[v][k] = u[v][k] - half_ffx * cf * (R[v][k] - sm[k] + L[v][k] - sp[k]);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) us[0][k] = us[0][k] > (T)a.minmass ? us[0][k] : (T)a.minmass;
+    tl.csync();
+    fluid_ghost_jobs(tl, a, SA, AS, GS, /*lower: R*/ 1, /*upper: L*/ 2, FO_STORE_R, FO_STORE_L);
+    __syncthreads();
 
-    // ---- freezing speed #2 on the half-step state (relaxingFluid.m:47-50) --------------------------
-    lmax = 0.0;
+    // ---- predictor (relaxingFluid.m:32-39): half-step state -> set B; freezing speed #2 -----------
+    double lmax2 = 0.0;
+    T press2[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        if (!pc.valid(k)) { us[0][k] = T(1); us[1][k] = us[2][k] = us[3][k] = us[4][k] = T(0); }
-        PressOut po = pressure_totsnd(G, us[0][k], us[1][k], us[2][k], us[3][k], us[4][k], msq_of(k));
-        press[k] = (T)(po.p + 0.0);
-        T spd = fabs(sel3(d, us[1][k], us[2][k], us[3][k]) / us[0][k]) + (T)po.cs;
-        if (pc.valid(k)) lmax = fmax(lmax, (double)spd);
+        const int ix = tl.idx(k);
+        T us[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const int cls = fluid_class(v);
+            const T* R = SA + v * AS;
+            const T* L = SA + (5 + v) * AS;
+            const T Rm = shifted(tl, R, GS + v * 2 * tl.Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted(tl, L, GS + (5 + v) * 2 * tl.Wb, k, +1, a.mode[cls][1], fc, fw);
+            us[v] = u[v][k] - half_ffx * cf * (R[ix] - Rm + L[ix] - Lp);
+        }
+        us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
+        if (!tl.ok(k)) { us[0] = T(1); us[1] = us[2] = us[3] = us[4] = T(0); }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) SB[v * AS + ix] = us[v];
+        T spd = press_speed<T>(G, d, us, msq[k], press2[k]);   // relaxingFluid.m:47-50
+        if (tl.ok(k)) lmax2 = fmax(lmax2, (double)spd);
     }
-    const T cfs = (T)column_max(pc, red[1], lmax);
+    const T cfs = (T)column_max(tl, NT, part[1], lmax2);   // its barrier also ends the predictor reads of set A
 
-    // ---- corrector fluxes and limiter (relaxingFluid.m:52-62) ---------------------------------------
+    // ---- corrector fluxes (relaxingFluid.m:52-56) from the half-step state -> set A --------------
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        T uu[5] = {us[0][k], us[1][k], us[2][k], us[3][k], us[4][k]};
+        const int ix = tl.idx(k);
+        T uu[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) uu[v] = SB[v * AS + ix];
         T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
         T w[5];
-        wflux<T>(d, uu, b3, press[k], cfs, w);
+        wflux<T>(d, uu, b3, press2[k], cfs, w);
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            R[v][k] = T(0.5) * (uu[v] + w[v]);
-            L[v][k] = T(0.5) * (uu[v] - w[v]);
+            SA[v * AS + ix] = T(0.5) * (uu[v] + w[v]);
+            SA[(5 + v) * AS + ix] = T(0.5) * (uu[v] - w[v]);
         }
-    }
-    if (a.init_flux) {
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            init_edges(pc, et, fluid_obj(v, FO_R), R[v]);
-            init_edges(pc, et, fluid_obj(v, FO_L), L[v]);
-        }
-    }
-    // the column_max sync above guarantees every thread is done reading the predictor slots
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        pc.publish(v, R[v]);
-        pc.publish(5 + v, L[v]);
-    }
-    pc.csync();
-    {
-        T sm[CPT], sp[CPT];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            bool flip = (v == 1 + d);
-            int cls = cls_of[v];
-            // fluxR: dL = R - R.shift(-1), dR = R.shift(+1) - R
-            shifted(pc, a, v, R[v], cls, flip, true, true, et->p[fluid_obj(v, FO_R)][d][0],
-                    et->p[fluid_obj(v, FO_R)][d][1], sm, sp);
-            T Rn[CPT];
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) Rn[k] = R[v][k] + limiter_corr<T>(a.limiter, R[v][k] - sm[k], sp[k] - R[v][k]);
-            // fluxL: dL = L.shift(-1) - L, dR = L - L.shift(+1)
-            shifted(pc, a, 5 + v, L[v], cls, flip, true, true, et->p[fluid_obj(v, FO_L)][d][0],
-                    et->p[fluid_obj(v, FO_L)][d][1], sm, sp);
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) {
-                L[v][k] = L[v][k] + limiter_corr<T>(a.limiter, sm[k] - L[v][k], L[v][k] - sp[k]);
-                R[v][k] = Rn[k];
+        if (a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(a.sg.g, x, y, z)) {
+#pragma unroll 1
+                for (int arr = 0; arr < 10; ++arr)
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(arr % 5, arr < 5 ? FO_R : FO_L), x, y, z,
+                                    (double)SA[arr * AS + ix]);
             }
         }
     }
-    pc.csync();   // all reads of the limiter-stage slots are done
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        pc.publish(v, R[v]);
-        pc.publish(5 + v, L[v]);
-    }
-    pc.csync();
+    tl.csync();
+    fluid_ghost_jobs(tl, a, SA, AS, GS, 3, 3, FO_R, FO_L);
+    __syncthreads();
 
-    // ---- corrector update (relaxingFluid.m:64-71) ---------------------------------------------------
-    T unew[5][CPT];
-    {
-        T sm[CPT], sp[CPT], dummy[CPT];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            bool flip = (v == 1 + d);
-            int cls = cls_of[v];
-            shifted(pc, a, v, R[v], cls, flip, true, false, et->p[fluid_obj(v, FO_R)][d][0], nullptr, sm, dummy);
-            shifted(pc, a, 5 + v, L[v], cls, flip, false, true, nullptr, et->p[fluid_obj(v, FO_L)][d][1], dummy, sp);
-#pragma unroll
-            for (int k = 0; k < CPT; ++k) unew[v][k] = u[v][k] - ff * cfs * (R[v][k] - sm[k] + L[v][k] - sp[k]);
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < CPT; ++k) unew[0][k] = unew[0][k] > (T)a.minmass ? unew[0][k] : (T)a.minmass;
-
+    // ---- TVD limiter (relaxingFluid.m:57-62): corrected R and L -> set B --------------------------
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        if (!pc.valid(k)) continue;
-        long long o = pc.off(k);
+        const int ix = tl.idx(k);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) stq<T>(a.q[v], o, unew[v][k]);
+        for (int v = 0; v < 5; ++v) {
+            const int cls = fluid_class(v);
+            const T* R = SA + v * AS;
+            const T* L = SA + (5 + v) * AS;
+            const Ghost<T>* gR = GS + v * 2 * tl.Wb;
+            const Ghost<T>* gL = GS + (5 + v) * 2 * tl.Wb;
+            const int mlo = a.mode[cls][0], mhi = a.mode[cls][1];
+            const T r = R[ix], l = L[ix];
+            const T Rm = shifted(tl, R, gR, k, -1, mlo, fc, fw);
+            const T Rp = shifted(tl, R, gR, k, +1, mhi, fc, fw);
+            const T Lm = shifted(tl, L, gL, k, -1, mlo, fc, fw);
+            const T Lp = shifted(tl, L, gL, k, +1, mhi, fc, fw);
+            SB[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
+            SB[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
+        }
+    }
+    tl.csync();
+    fluid_ghost_jobs(tl, a, SB, AS, GS, 1, 2, FO_R, FO_L);
+    __syncthreads();
+
+    // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
+    double m3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int ix = tl.idx(k);
+        T unew[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const int cls = fluid_class(v);
+            const T* R = SB + v * AS;
+            const T* L = SB + (5 + v) * AS;
+            const T Rm = shifted(tl, R, GS + v * 2 * tl.Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted(tl, L, GS + (5 + v) * 2 * tl.Wb, k, +1, a.mode[cls][1], fc, fw);
+            unew[v] = u[v][k] - ff * cfs * (R[ix] - Rm + L[ix] - Lp);
+        }
+        unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
+        if (!tl.ok(k)) continue;
+        const long long o = tl.off(k);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) stq<T>(a.q[v], o, unew[v]);
+        if (a.cfl) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
+            double cs = sound_speed(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3],
+                                    (double)unew[4], msq[k]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], fabs((double)unew[1 + c] / (double)unew[0]) + cs);
+        }
     }
 
-    // ---- fused CFL maxima of the new state (TimeManager.m:65-77) -----------------------------------
+    // peers of a cluster read this CTA's shared memory through DSMEM until their last stage ends
+    if (tl.CL > 1) cg::this_cluster().sync();
+
     if (a.cfl) {
-        double m3[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) continue;
-            double cs = sound_speed(G, (double)unew[0][k], (double)unew[1][k], (double)unew[2][k], (double)unew[3][k],
-                                    (double)unew[4][k], msq_of(k));
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                double v = fabs((double)unew[1 + c][k] / (double)unew[0][k]) + cs;
-                m3[c] = fmax(m3[c], v);
-            }
-        }
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             for (int o = 16; o > 0; o >>= 1) m3[c] = fmax(m3[c], __shfl_xor_sync(0xffffffffu, m3[c], o));
-            if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&a.tm->maxbits[c], m3[c]);
+            if (lane == 0) cflp[c][warp] = m3[c];
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {   // one global atomic per CTA and direction
+            double m = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, cflp[threadIdx.x][w]);
+            atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
         }
     }
 }

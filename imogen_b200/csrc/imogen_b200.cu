@@ -26,8 +26,10 @@ const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1
 const int FWD_MI[3][2] = {{2, 3}, {1, 3}, {1, 2}};
 const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
 
+// Launch shape of the pencil kernels for one sweep direction: Wb pencils per CTA, G threads per
+// pencil, CPT cells per thread (2, or 4 for long pencils), CL CTAs per cluster.
 struct PencilCfg {
-    int Wb = 1, G = 32, CL = 1, NT = 32;
+    int Wb = 1, G = 32, CL = 1, NT = 32, cpt = 2;
 };
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -66,9 +68,12 @@ struct img_ctx {
     int iteration = 1;
     int iters_base = 0;
     PencilCfg pcfg[3];
-    int cpt = 2;
-    cudaGraphExec_t graphs[6] = {};
+    // one captured iteration per (cfl_valid at its start, sweep-order row (iteration-1) % 6)
+    cudaGraphExec_t graphs[2][6] = {};
+    uint64_t graph_launches[2][6] = {};
+    bool use_graphs = true;
     DevTime* host_tm = nullptr;  // pinned mirror
+    uint64_t launches = 0;       // kernels launched by this context
 };
 
 namespace {
@@ -155,30 +160,35 @@ std::vector<double> fade_coefficients(int f) {
     return out;
 }
 
-PencilCfg choose_pencil(const Geom& g, int d, size_t elem, int cpt) {
+// Pencil tiling of one sweep direction: one cell per thread where the pencil fits a cluster of at
+// most 4 CTAs of 512 threads (2 or 4 cells per thread otherwise).  Along x a CTA holds whole pencil
+// segments of up to 512 rows; along y and z it holds 32 contiguous bytes of x (one DRAM sector) per
+// pencil row, so both directions load and store full sectors.
+PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
+    const int N = g.n[d];
+    const long long ncol = g.ncell / N;
+    const int maxnt = 512;
     PencilCfg p;
-    int N = g.n[d];
-    long long ncol = g.ncell / N;
-    int G = pow2ceil((N + cpt - 1) / cpt);
-    int maxnt = 256;
-    int CL = 1;
-    if (d == 0) {
-        while (G > maxnt) { G >>= 1; CL <<= 1; }
-        if (CL > 8) { maxnt = 512; G <<= 1; CL >>= 1; }
-        int Wb = std::max(1, std::min(32, maxnt / G));
-        if (Wb * G < 32) Wb = 32 / G;
-        while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+    for (int cpt : {1, 2, 4}) {
+        int G = std::max(2, pow2ceil((N + cpt - 1) / cpt));
+        int CL = 1, Wb;
+        if (d == 0) {
+            while (G > maxnt) { G >>= 1; CL <<= 1; }
+            Wb = std::max(1, 256 / G);
+            if (Wb * G < 32) Wb = 32 / G;
+            while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+        } else {
+            Wb = elem == 8 ? 4 : 8;
+            G = std::max(G, 32 / Wb);
+            while (Wb * G > maxnt) { G >>= 1; CL <<= 1; }
+        }
         p.Wb = Wb;
-    } else {
-        int Wb = elem == 8 ? 4 : 8;
-        G = std::max(G, 32 / Wb);
-        while (Wb * G > maxnt) { G >>= 1; CL <<= 1; }
-        if (CL > 8) { maxnt = 512; G <<= 1; CL >>= 1; }
-        p.Wb = Wb;
+        p.G = G;
+        p.CL = CL;
+        p.NT = Wb * G;
+        p.cpt = cpt;
+        if (CL <= 4) break;   // clusters of 8 CTAs of these kernels do not schedule: more cells per thread
     }
-    p.G = G;
-    p.CL = CL;
-    p.NT = p.Wb * p.G;
     return p;
 }
 
@@ -187,8 +197,8 @@ int launch_blocks(long long work, int bs = 256) {
     return (int)std::max(1LL, std::min(b, 148LL * 16));
 }
 
-template <typename T>
-int launch_fluid(img_ctx* ctx, int d, bool cfl) {
+template <typename T, int CPT>
+int launch_fluid_cpt(img_ctx* ctx, int d, bool cfl) {
     FluidArgs a{};
     const img_config& c = ctx->cfg;
     PencilCfg pcf = ctx->pcfg[d];
@@ -226,8 +236,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3((unsigned)(nb * pcf.CL));
     lc.blockDim = dim3(pcf.NT);
-    using PC = Pencil<T, (sizeof(T) == 8 ? 2 : 4), FLUID_NSLOT, false>;
-    lc.dynamicSmemBytes = PC::smem_bytes(pcf.NT, pcf.Wb);
+    lc.dynamicSmemBytes = fluid_smem_bytes<T>(pcf.G * CPT, pcf.Wb);
     lc.stream = ctx->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -236,15 +245,24 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     attr[0].val.clusterDim.z = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    constexpr int CPT = sizeof(T) == 8 ? 2 : 4;
     void (*kern)(const FluidArgs) = ctx->mhd ? fluid_sweep_kernel<T, true, CPT> : fluid_sweep_kernel<T, false, CPT>;
-    if (pcf.CL > 8) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    if (lc.dynamicSmemBytes > 48 * 1024)
-        CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lc.dynamicSmemBytes));
-    CK(cudaLaunchKernelEx(&lc, kern, a));
+    cudaError_t le = cudaLaunchKernelEx(&lc, kern, a);
+    if (le != cudaSuccess)
+        return fail(ctx, IMG_ERR_CUDA, "fluid sweep launch (dim %d, grid %u, block %u, smem %zu, cluster %d): %s", d,
+                    lc.gridDim.x, lc.blockDim.x, lc.dynamicSmemBytes, pcf.CL, cudaGetErrorString(le));
+    ctx->launches += 1;
     ctx->init_store = false;
     ctx->init_flux = false;
     return IMG_OK;
+}
+
+template <typename T>
+int launch_fluid(img_ctx* ctx, int d, bool cfl) {
+    switch (ctx->pcfg[d].cpt) {
+        case 1: return launch_fluid_cpt<T, 1>(ctx, d, cfl);
+        case 2: return launch_fluid_cpt<T, 2>(ctx, d, cfl);
+        default: return launch_fluid_cpt<T, 4>(ctx, d, cfl);
+    }
 }
 
 template <typename T>
@@ -299,19 +317,17 @@ void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     a.edges = ctx->edges_dev;
 }
 
-template <typename T>
-int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
+template <typename T, int CPT>
+int launch_magnet_cpt(img_ctx* ctx, int X, int I1, int I2) {
     MagArgs a{};
     fill_mag_args<T>(ctx, X, I1, I2, a);
     int d = X - 1;
     PencilCfg pcf = ctx->pcfg[d];
-    constexpr int CPT = sizeof(T) == 8 ? 2 : 4;
-    using PC = Pencil<T, CPT, MAG_NSLOT, true>;
     long long nb = (a.sg.ncol + pcf.Wb - 1) / pcf.Wb;
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3((unsigned)(nb * pcf.CL), 2);
     lc.blockDim = dim3(pcf.NT);
-    lc.dynamicSmemBytes = PC::smem_bytes(pcf.NT, pcf.Wb);
+    lc.dynamicSmemBytes = mag_smem_bytes<T>(pcf.G * CPT, pcf.Wb);
     lc.stream = ctx->stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -321,8 +337,10 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     lc.attrs = attr;
     lc.numAttrs = 1;
     void (*kern)(const MagArgs) = mag_chain_kernel<T, CPT>;
-    if (pcf.CL > 8) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    CK(cudaLaunchKernelEx(&lc, kern, a));
+    cudaError_t le = cudaLaunchKernelEx(&lc, kern, a);
+    if (le != cudaSuccess)
+        return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
+                    lc.gridDim.x, lc.blockDim.x, lc.dynamicSmemBytes, pcf.CL, cudaGetErrorString(le));
     long long n = ctx->g.ncell;
     mag_ct1_kernel<T><<<launch_blocks(2 * n), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
@@ -332,9 +350,19 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     CK(cudaGetLastError());
     mag_cell_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    ctx->launches += 5;
     ctx->init_mag[I1 - 1][d] = false;
     ctx->init_mag[I2 - 1][d] = false;
     return IMG_OK;
+}
+
+template <typename T>
+int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
+    switch (ctx->pcfg[X - 1].cpt) {
+        case 1: return launch_magnet_cpt<T, 1>(ctx, X, I1, I2);
+        case 2: return launch_magnet_cpt<T, 2>(ctx, X, I1, I2);
+        default: return launch_magnet_cpt<T, 4>(ctx, X, I1, I2);
+    }
 }
 
 template <typename T>
@@ -348,7 +376,65 @@ int launch_cfl_reduce(img_ctx* ctx) {
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     cfl_reduce_kernel<T><<<launch_blocks(ctx->g.ncell), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
+    ctx->launches += 1;
     return IMG_OK;
+}
+
+// Kernel attributes (shared memory above 48 KB, clusters above 8 CTAs), set once per context so
+// that no attribute call happens inside a stream capture, and a schedulability check of every
+// pencil configuration.
+template <typename T, int CPT>
+int set_kernel_attributes_cpt(img_ctx* ctx) {
+    size_t smem = 0;
+    int cl = 1;
+    bool used = false;
+    for (int d = 0; d < 3; ++d) {
+        const PencilCfg& p = ctx->pcfg[d];
+        if (p.cpt != CPT) continue;
+        used = true;
+        smem = std::max(smem, fluid_smem_bytes<T>(p.G * CPT, p.Wb));
+        smem = std::max(smem, mag_smem_bytes<T>(p.G * CPT, p.Wb));
+        cl = std::max(cl, p.CL);
+    }
+    if (!used) return IMG_OK;
+    void (*fk[2])(const FluidArgs) = {fluid_sweep_kernel<T, false, CPT>, fluid_sweep_kernel<T, true, CPT>};
+    void (*mk)(const MagArgs) = mag_chain_kernel<T, CPT>;
+    // the default dynamic limit is 48 KB minus the static shared memory: always raise it
+    for (auto k : fk) {
+        CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (cl > 8) CK(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    CK(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (cl > 8) CK(cudaFuncSetAttribute(mk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for (int d = 0; d < 3; ++d) {
+        const PencilCfg& p = ctx->pcfg[d];
+        if (ctx->g.n[d] < 3 || p.cpt != CPT) continue;
+        cudaLaunchConfig_t lc{};
+        lc.gridDim = dim3((unsigned)p.CL);
+        lc.blockDim = dim3(p.NT);
+        lc.dynamicSmemBytes = fluid_smem_bytes<T>(p.G * CPT, p.Wb);
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = p.CL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        lc.attrs = attr;
+        lc.numAttrs = 1;
+        int nclusters = 0;
+        cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, fk[1], &lc);
+        if (e != cudaSuccess || nclusters < 1)
+            return fail(ctx, IMG_ERR_UNSUPPORTED, "pencil configuration for dim %d (block %d, cluster %d, smem %zu) "
+                        "cannot be scheduled: %s", d, p.NT, p.CL, lc.dynamicSmemBytes,
+                        e != cudaSuccess ? cudaGetErrorString(e) : "0 active clusters");
+    }
+    return IMG_OK;
+}
+
+template <typename T>
+int set_kernel_attributes(img_ctx* ctx) {
+    int rc = set_kernel_attributes_cpt<T, 1>(ctx);
+    if (rc == IMG_OK) rc = set_kernel_attributes_cpt<T, 2>(ctx);
+    return rc != IMG_OK ? rc : set_kernel_attributes_cpt<T, 4>(ctx);
 }
 
 int fluid_sweep(img_ctx* ctx, int X, bool cfl) {
@@ -392,6 +478,7 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
     }
     cfl_finalize_kernel<<<1, 32, 0, ctx->stream>>>(ctx->tm, flux_direction == 1 ? 1 : 0);
     CK(cudaGetLastError());
+    ctx->launches += 1;
     ctx->cfl_valid = false;
     return IMG_OK;
 }
@@ -411,6 +498,12 @@ int enqueue_iteration(img_ctx* ctx) {
 int check_dev_error(img_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+#ifdef IMG_CHECKED
+    int site = 0, val = 0;
+    CK(cudaMemcpyFromSymbol(&site, g_check_site, sizeof(int)));
+    CK(cudaMemcpyFromSymbol(&val, g_check_val, sizeof(int)));
+    if (site) return fail(ctx, IMG_ERR_CUDA, "checked build: access check %d failed (value %d)", site, val);
+#endif
     int e = ctx->host_tm->error;
     if (e & DERR_CFL) return fail(ctx, IMG_ERR_CFL, "CFL error: no velocity exceeded the 1e-2 floor (cmax=%g)", ctx->host_tm->cmax);
     if (e & DERR_NONFINITE_DT) return fail(ctx, IMG_ERR_NONFINITE, "non-finite timestep");
@@ -424,6 +517,7 @@ int validate(const img_config& c, std::string& why) {
         if (c.limiter[d] < 0 || c.limiter[d] > 2) { why = "unknown flux limiter"; return IMG_ERR_ARG; }
     }
     if (c.precision != IMG_PREC_FP64 && c.precision != IMG_PREC_MIXED) { why = "unknown precision"; return IMG_ERR_ARG; }
+    if ((long long)c.grid[0] * c.grid[1] * c.grid[2] >= (1LL << 31)) { why = "grids are limited to < 2^31 cells"; return IMG_ERR_ARG; }
     if (c.bc_infinity < 4) { why = "bcInfinity must be >= 4"; return IMG_ERR_ARG; }
     int ndims = c.grid[2] > 1 ? 3 : 2;
     for (int k = 0; k < 4; ++k)
@@ -541,7 +635,6 @@ int img_create(img_ctx** out, const img_config* cfg) {
     ctx = new img_ctx();
     ctx->cfg = *cfg;
     ctx->elem = cfg->precision == IMG_PREC_FP64 ? 8 : 4;
-    ctx->cpt = ctx->elem == 8 ? 2 : 4;
     Geom& g = ctx->g;
     for (int d = 0; d < 3; ++d) g.n[d] = cfg->grid[d];
     g.ndims = cfg->grid[2] > 1 ? 3 : 2;
@@ -549,7 +642,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     g.s[1] = g.n[0];
     g.s[2] = (long long)g.n[0] * g.n[1];
     g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (int d = 0; d < 3; ++d) ctx->pcfg[d] = choose_pencil(g, d, ctx->elem, ctx->cpt);
+    for (int d = 0; d < 3; ++d) ctx->pcfg[d] = choose_pencil(g, d, ctx->elem);
 
     auto bail = [&](int code) {
         if (ctx->slab) cudaFree(ctx->slab);
@@ -617,6 +710,8 @@ int img_create(img_ctx** out, const img_config* cfg) {
         fail(ctx, IMG_ERR_CUDA, "device initialisation failed");
         return bail(IMG_ERR_CUDA);
     }
+    if ((ctx->elem == 8 ? set_kernel_attributes<double>(ctx) : set_kernel_attributes<float>(ctx)) != IMG_OK)
+        return bail(IMG_ERR_CUDA);
     *out = ctx;
     return IMG_OK;
 }
@@ -624,8 +719,9 @@ int img_create(img_ctx** out, const img_config* cfg) {
 int img_destroy(img_ctx* ctx) {
     if (!ctx) return IMG_OK;
     cudaStreamSynchronize(ctx->stream);
-    for (auto& gx : ctx->graphs)
-        if (gx) cudaGraphExecDestroy(gx);
+    for (auto& row : ctx->graphs)
+        for (auto& gx : row)
+            if (gx) cudaGraphExecDestroy(gx);
     if (ctx->slab) cudaFree(ctx->slab);
     if (ctx->host_tm) cudaFreeHost(ctx->host_tm);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -703,6 +799,10 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->state_set = true;
     ctx->cfl_valid = false;
+    // new FluidArray/MagnetArray objects: their InitializedArrays take edges at first assignment
+    ctx->init_store = ctx->init_flux = true;
+    for (auto& r : ctx->init_mag)
+        for (auto& v : r) v = true;
     return IMG_OK;
 }
 
@@ -744,9 +844,47 @@ int img_magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
     return magnet_sweep(ctx, X, I1, I2);
 }
 
+// Whether the next iteration's launch sequence is the steady one a graph can replay: every
+// InitializedArray has had its first assignment (no edge-capture flags left in the arguments).
+static bool steady(const img_ctx* ctx) {
+    if (ctx->init_store || ctx->init_flux) return !ctx->cfg.fluid_active;
+    for (int c = 0; c < 3; ++c)
+        for (int X = 0; X < 3; ++X)
+            if (c != X && ctx->cfg.magnet_active && ctx->init_mag[c][X] && ctx->g.n[X] >= 3) return false;
+    return true;
+}
+
 int img_step(img_ctx* ctx) {
     if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
     if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    int row = (ctx->iteration - 1) % 6;
+    if (ctx->use_graphs && steady(ctx)) {
+        const int cv = ctx->cfl_valid ? 1 : 0;
+        if (!ctx->graphs[cv][row]) {
+            uint64_t l0 = ctx->launches;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = enqueue_iteration(ctx);
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+            if (rc != IMG_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            if (ce != cudaSuccess) return fail(ctx, IMG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+            cudaGraphExec_t exec = nullptr;
+            ce = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ce != cudaSuccess) return fail(ctx, IMG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+            ctx->graphs[cv][row] = exec;
+            ctx->graph_launches[cv][row] = ctx->launches - l0;
+            ctx->launches = l0;   // counted when replayed
+        }
+        CK(cudaGraphLaunch(ctx->graphs[cv][row], ctx->stream));
+        ctx->launches += ctx->graph_launches[cv][row];
+        ctx->cfl_valid = ctx->cfg.update_mode != 0 && ctx->cfg.fluid_active;
+        ctx->iteration += 1;
+        return IMG_OK;
+    }
     int rc = enqueue_iteration(ctx);
     if (rc != IMG_OK) return rc;
     ctx->iteration += 1;
@@ -817,6 +955,18 @@ int img_totals(img_ctx* ctx, double out[8]) {
         }
         out[v] = S + C;
     }
+    return IMG_OK;
+}
+
+int img_get_stream(img_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return fail(ctx, IMG_ERR_ARG, "null argument");
+    *stream = (void*)ctx->stream;
+    return IMG_OK;
+}
+
+int img_launch_count(const img_ctx* ctx, uint64_t* count) {
+    if (!ctx || !count) return IMG_ERR_ARG;
+    *count = ctx->launches;
     return IMG_OK;
 }
 

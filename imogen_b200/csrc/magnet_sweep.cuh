@@ -49,7 +49,7 @@ struct MagArgs {
 // mode/act/flip/edge describe the array object; the edge state of a trans edge is drifted and
 // written back when `own_update` (exactly one thread per face cell calls with own_update = true).
 template <typename T>
-__device__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y, int z, int e, int n, int mode,
+__device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y, int z, int e, int n, int mode,
                          int act, bool flip, double* edge, const double* fc, int f, double bc_inf, bool own_update) {
     const int Ne = sel3(e, g.n[0], g.n[1], g.n[2]);
     const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
@@ -94,122 +94,67 @@ __device__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y
 }
 
 // ---- the X-chain ------------------------------------------------------------------------------------
-constexpr int MAG_NSLOT = 2;
+constexpr int MAG_NARR = 4;
+constexpr int MAG_NSLOT = 6;   // ghost slots per column: lower, upper +1 (x3), upper +2 (two rows)
+
+// Dynamic shared memory of the chain kernel: 4 arrays of RC*Wb values + 6 ghost slots per column.
+template <typename T>
+__host__ __device__ inline size_t mag_smem_bytes(int RC, int Wb) {
+    return sizeof(T) * (size_t)MAG_NARR * RC * Wb + sizeof(Ghost<T>) * MAG_NSLOT * (size_t)Wb;
+}
+
+// A.shift(X, +2) at row k, fade damping included: ghosts of rows N and N+1 in slots s3, s4 (the
+// anchors of the constant shift by 2 -- rows min(2, N-1) and N-1 -- ride in s3).
+template <typename T, int CPT>
+__device__ __forceinline__ T shifted2(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* s3, const Ghost<T>* s4, int k,
+                                      int mode, const double* fc, int f) {
+    const T g2[2] = {s3[tl.b].g, s4[tl.b].g};
+    T v = tl.above2(A, g2, k);
+    if (mode == BC_FADE) v = fade_apply(v, tl.grow(k), tl.N, fc, f, s3[tl.b].s0, s3[tl.b].sN1);
+    return v;
+}
 
 template <typename T, int CPT>
-struct MagChain {
-    using PC = Pencil<T, CPT, MAG_NSLOT, true>;
-    const MagArgs& a;
-    PC& pc;
-    int N;
-    __device__ MagChain(const MagArgs& aa, PC& p) : a(aa), pc(p), N(p.sg->N) {}
-
-    // Ghost of a mag-class array at the pencil's lower end for shift(X,-1) (trans: one drift).
-    __device__ T ghost_lo(int slot, double* edge, bool own) {
-        int mode = a.modeX[0];
-        switch (mode) {
-            case BC_CIRC: return pc.endv(slot, N - 1);
-            case BC_MIRROR: return pc.endv(slot, 1);
-            case BC_WALL: return (T)edge[pc.col];
-            case BC_TRANS: {
-                double ev = 0.0;
-                T y0 = pc.endv(slot, trans_pick_lower(N, 1, 0)), y1 = pc.endv(slot, trans_pick_lower(N, 1, 1));
-                T y2 = pc.endv(slot, 0);
-                if (a.actX) {
-                    ev = edge_drift(edge[pc.col], (double)y2);
-                    if (own) edge[pc.col] = ev;
-                }
-                return (T)trans_ghost((double)y0, (double)y1, (double)y2, ev, a.bc_inf, 4.0, (double)y2);
-            }
-            default: return pc.endv(slot, 0);
-        }
-    }
-    // A.shift(X,-1) at row r (k = segment index) including fade damping.
-    __device__ T sm(int slot, const T (&A)[CPT], int k, T glo) {
-        int r = pc.r0 + k;
-        T v = r == 0 ? glo : pc.prev(slot, A, k);
-        if (a.modeX[0] == BC_FADE) v = fade_apply(v, r, N, a.fade, a.fade_f, pc.endv(slot, 0), pc.endv(slot, N - 2));
-        return v;
-    }
-    // Upper ghosts for one shift(X,+m) call given the stored edge value after its drift (ev).
-    // Returns the ghost for row N-1 (m=1) or rows N-2, N-1 (m=2) in g[0], g[1].
-    __device__ void ghost_hi(int slot, int m, double ev, T g[2]) {
-        int mode = a.modeX[1];
-        switch (mode) {
-            case BC_CIRC:   // rows N, N+1 wrap to 0, 1
-                g[0] = pc.endv(slot, 0);
-                g[1] = m == 2 ? pc.endv(slot, 1) : g[0];
-                return;
-            case BC_MIRROR:
-                if (m == 1) g[0] = pc.endv(slot, N - 2);
-                else { g[0] = pc.endv(slot, N - 2); g[1] = pc.endv(slot, N - 3); }
-                return;
-            case BC_WALL: g[0] = g[1] = (T)ev; return;
-            case BC_TRANS: {
-                double y0 = pc.endv(slot, trans_pick_upper(N, m, 0));
-                double y1 = pc.endv(slot, trans_pick_upper(N, m, 1));
-                double y2 = pc.endv(slot, trans_pick_upper(N, m, 2));
-                if (m == 1) {
-                    g[0] = (T)trans_ghost(y0, y1, y2, ev, a.bc_inf, 4.0, (double)pc.endv(slot, N - 1));
-                } else {
-                    g[0] = (T)trans_ghost(y0, y1, y2, ev, a.bc_inf, 4.0, (double)pc.endv(slot, N - 2));
-                    g[1] = (T)trans_ghost(y0, y1, y2, ev, a.bc_inf, 5.0, (double)pc.endv(slot, N - 1));
-                }
-                return;
-            }
-            default: g[0] = g[1] = pc.endv(slot, N - 1); return;   // const, fade
-        }
-    }
-    // A.shift(X,+m)[r] for this thread's row k given the upper ghosts g of this call.
-    __device__ T sp(int slot, const T (&A)[CPT], int k, int m, const T g[2]) {
-        int r = pc.r0 + k;
-        T v;
-        if (r + m <= N - 1) v = m == 1 ? pc.next(slot, A, k) : pc.next2(slot, A, k);
-        else v = (m == 1) ? g[0] : g[(r + m) - N];   // m=2: r=N-2 -> g[0], r=N-1 -> g[1]
-        if (a.modeX[1] == BC_FADE) {
-            T s0 = pc.endv(slot, m < N ? m : N - 1);
-            v = fade_apply(v, r, N, a.fade, a.fade_f, s0, pc.endv(slot, N - 1));
-        }
-        return v;
-    }
-};
-
-template <typename T, int CPT>
-__global__ void __launch_bounds__(512) mag_chain_kernel(const MagArgs a) {
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
-    using PC = Pencil<T, CPT, MAG_NSLOT, true>;
-    PC pc;
-    pc.init(a.sg, smem);
+    Tile<T, CPT> tl;
+    tl.init(a.sg);
     const int q = blockIdx.y;          // which transverse component
-    const int X = a.X, I = q ? a.I[1] : a.I[0];
+    const int I = q ? a.I[1] : a.I[0];
     const int shiftI = q ? a.shiftI[1] : a.shiftI[0];
     const int mode_mom_lo = q ? a.modeI_mom[1][0] : a.modeI_mom[0][0];
     const int mode_mass_lo = q ? a.modeI_mass[1][0] : a.modeI_mass[0][0];
     const int act_mom = q ? a.actI_mom[1] : a.actI_mom[0];
     const int act_mass = q ? a.actI_mass[1] : a.actI_mass[0];
     const int init_mag = q ? a.init_mag[1] : a.init_mag[0];
-    const int d = X - 1, e = I - 1;
-    const int N = a.sg.N;
+    const int d = a.X - 1, e = I - 1, c = I - 1;
+    const int N = a.sg.N, Wb = tl.Wb, b = tl.b;
     const Geom& g = a.sg.g;
     const double dt = a.tm->dt;
     const T ff = (T)(0.5 * dt / a.dx);
     const T ff2 = T(2) * ff;
     const EdgeTable* et = a.edges;
-    MagChain<T, CPT> mc(a, pc);
-    const int c = I - 1;   // component index of mag(I)
-    double* e_vg_lo = et->p[mag_obj(c, d, MO_VELGRID)][d][0];
-    double* e_vg_hi = et->p[mag_obj(c, d, MO_VELGRID)][d][1];
-    double* e_sf_lo = et->p[mag_obj(c, d, MO_STORE_R)][d][0];
-    double* e_sf_hi = et->p[mag_obj(c, d, MO_STORE_R)][d][1];
-    double* e_wm_lo = et->p[mag_obj(c, d, MO_WMAG)][d][0];
-    double* e_wm_hi = et->p[mag_obj(c, d, MO_WMAG)][d][1];
-    double* e_fx_lo = et->p[mag_obj(c, d, MO_FLUX)][d][0];
-    const bool own0 = pc.nv > 0 && pc.r0 == 0;
-    const bool ownN = pc.nv > 0 && pc.r0 + pc.nv - 1 == N - 1;
-    const bool ownN2 = pc.nv > 0 && pc.r0 <= N - 2 && pc.r0 + pc.nv - 1 >= N - 2;
+    const size_t AS = (size_t)tl.RC * Wb;
+    T* S0 = reinterpret_cast<T*>(smem);
+    T* S1 = S0 + AS;
+    T* S2 = S1 + AS;
+    T* S3 = S2 + AS;
+    Ghost<T>* GS = reinterpret_cast<Ghost<T>*>(S0 + MAG_NARR * AS);   // [slot][column]
+    // upper slot s is read by shifted(.., +1) through GS + (s-1)*Wb (it reads gs[Wb + b])
+    const Ghost<T>* GL = GS;
+    const double* fc = a.fade;
+    const int f = a.fade_f;
+    const double binf = a.bc_inf;
+    const int mlo = a.modeX[0], mhi = a.modeX[1];
+    // the scratch objects of mag(I) for this sweep (mag-class BC along X, no mirror flip)
+    auto edge_of = [&](int kind, int side) -> double* { return et->p[mag_obj(c, d, kind)][d][side]; };
+    // ghost job helpers: lower ghosts on cluster rank 0 (thread g == 0 of the column), upper ghosts
+    // on the rank holding row N-1 (thread g == 1, or 0 when the column has one thread)
+    const bool job_lo = tl.colok && tl.rank == 0 && tl.g == 0;
+    const bool job_hi = tl.colok && tl.rank == tl.rank_hi() && tl.g == (tl.G > 1 ? 1 : 0);
 
-    // ---- corner velocity (magnetFlux.m:18-19) --------------------------------------------------
+    // ---- corner velocity (magnetFlux.m:18-19): transverse average with mass/mom BCs along I ------
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* pX = reinterpret_cast<const T*>(a.q[Q_PX + d]);
     T* BI = reinterpret_cast<T*>(a.q[Q_BX + c]);
@@ -218,172 +163,163 @@ __global__ void __launch_bounds__(512) mag_chain_kernel(const MagArgs a) {
     for (int k = 0; k < CPT; ++k) {
         vgr[k] = T(0);
         bI[k] = T(0);
-        if (!pc.valid(k)) continue;
-        long long o = pc.off(k);
-        int x, y, z;
-        pc.coords(k, x, y, z);
-        T pm, rm;
-        if (shiftI) {
-            pm = shift_along<T>(g, pX, o, x, y, z, e, -1, mode_mom_lo, act_mom, false,
-                                et->p[OBJ_PRIM_MOM + d][e][0], a.fade, a.fade_f, a.bc_inf, true);
-            rm = shift_along<T>(g, rho, o, x, y, z, e, -1, mode_mass_lo, act_mass, false,
-                                et->p[OBJ_PRIM_MASS][e][0], a.fade, a.fade_f, a.bc_inf, true);
-        } else {
-            pm = pX[o];
-            rm = rho[o];
-        }
-        vgr[k] = (pm + pX[o]) / (rm + rho[o]);
-        bI[k] = BI[o];
-    }
-    if (init_mag) init_edges(pc, et, mag_obj(c, d, MO_VELGRID), vgr);
-
-    // vg = 0.25*(vg.shift(X,-1) + vg.shift(X,1) + 2*vg)   (magnetFlux.m:21-23)
-    double s_vg_hi = 0.0;
-    if (ownN && e_vg_hi) s_vg_hi = e_vg_hi[pc.col];
-    pc.publish(0, vgr);
-    pc.csync();
-    T vg[CPT];
-    {
-        T glo = own0 ? mc.ghost_lo(0, e_vg_lo, true) : T(0);
-        T gh[2] = {T(0), T(0)};
-        if (ownN) {
-            double ev = s_vg_hi;
-            if (a.modeX[1] == BC_TRANS && a.actX) ev = edge_drift(ev, (double)pc.endv(0, N - 1));
-            mc.ghost_hi(0, 1, ev, gh);
-            s_vg_hi = ev;
-        }
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) { vg[k] = T(0); continue; }
-            T m1 = mc.sm(0, vgr, k, glo);
-            T p1 = mc.sp(0, vgr, k, 1, gh);
-            vg[k] = T(0.25) * (m1 + p1 + T(2) * vgr[k]);
-        }
-    }
-    // velocityFlow = (vg + vg.shift(X,1)) < 0   (relaxingMagnet.m:17)
-    pc.publish(1, vg);
-    pc.csync();
-    T vf[CPT], F[CPT];
-    {
-        T gh[2] = {T(0), T(0)};
-        if (ownN) {
-            double ev = s_vg_hi;
-            if (a.modeX[1] == BC_TRANS && a.actX) ev = edge_drift(ev, (double)pc.endv(1, N - 1));
-            mc.ghost_hi(1, 1, ev, gh);
-            if (e_vg_hi && a.modeX[1] == BC_TRANS && a.actX) e_vg_hi[pc.col] = ev;
-        }
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) { vf[k] = T(0); F[k] = T(0); continue; }
-            T p1 = mc.sp(1, vg, k, 1, gh);
-            vf[k] = (vg[k] + p1) < T(0) ? T(1) : T(0);
-            F[k] = bI[k] * vg[k];
-        }
-    }
-    if (init_mag) init_edges(pc, et, mag_obj(c, d, MO_STORE_R), F);
-    // store.fluxR = F.*(1-vf) + F.shift(X,1).*vf   (relaxingMagnet.m:22-24)
-    double s_sf_hi = (ownN && e_sf_hi) ? e_sf_hi[pc.col] : 0.0;
-    pc.csync();
-    pc.publish(0, F);
-    pc.csync();
-    T Fu[CPT];
-    {
-        T gh[2] = {T(0), T(0)};
-        if (ownN) {
-            double ev = s_sf_hi;
-            if (a.modeX[1] == BC_TRANS && a.actX) {
-                ev = edge_drift(ev, (double)pc.endv(0, N - 1));
-                if (e_sf_hi) e_sf_hi[pc.col] = ev;
+        if (tl.ok(k)) {
+            const long long o = tl.off(k);
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            T pm, rm;
+            if (shiftI) {
+                pm = shift_along<T>(g, pX, o, x, y, z, e, -1, mode_mom_lo, act_mom, false,
+                                    et->p[OBJ_PRIM_MOM + d][e][0], fc, f, binf, true);
+                rm = shift_along<T>(g, rho, o, x, y, z, e, -1, mode_mass_lo, act_mass, false,
+                                    et->p[OBJ_PRIM_MASS][e][0], fc, f, binf, true);
+            } else {
+                pm = pX[o];
+                rm = rho[o];
             }
-            mc.ghost_hi(0, 1, ev, gh);
+            vgr[k] = (pm + pX[o]) / (rm + rho[o]);
+            bI[k] = BI[o];
+            if (init_mag && on_face(g, x, y, z))
+                init_edges_cell(g, et, mag_obj(c, d, MO_VELGRID), x, y, z, (double)vgr[k]);
         }
+        S0[tl.idx(k)] = vgr[k];
+    }
+    tl.csync();
+    if (job_lo) fill_ghost(tl, S0, GS, -1, mlo, a.actX, 0, edge_of(MO_VELGRID, 0), binf);
+    if (job_hi) fill_ghost(tl, S0, GS, +1, mhi, a.actX, 0, edge_of(MO_VELGRID, 1), binf);
+    __syncthreads();
+    // vg = 0.25*(vg.shift(X,-1) + vg.shift(X,1) + 2*vg)   (magnetFlux.m:21-23)
+    T vg[CPT];
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) { Fu[k] = T(0); continue; }
-            Fu[k] = F[k] * (T(1) - vf[k]) + mc.sp(0, F, k, 1, gh) * vf[k];
+    for (int k = 0; k < CPT; ++k) {
+        const T m1 = shifted(tl, (const T*)S0, GL, k, -1, mlo, fc, f);
+        const T p1 = shifted(tl, (const T*)S0, GS, k, +1, mhi, fc, f);
+        vg[k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[k]) : T(0);
+        S1[tl.idx(k)] = vg[k];
+    }
+    tl.csync();
+    if (job_hi) fill_ghost(tl, S1, GS, +1, mhi, a.actX, 0, edge_of(MO_VELGRID, 1), binf);
+    __syncthreads();
+    // velocityFlow = (vg + vg.shift(X,1)) < 0; store.fluxR = B_I.*vg   (relaxingMagnet.m:17,22)
+    T vf[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const T p1 = shifted(tl, (const T*)S1, GS, k, +1, mhi, fc, f);
+        vf[k] = (vg[k] + p1) < T(0) ? T(1) : T(0);
+        const T F = bI[k] * vg[k];
+        S2[tl.idx(k)] = F;
+        if (init_mag && tl.ok(k)) {
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_STORE_R), x, y, z, (double)F);
         }
     }
-    // store = B_I - ff*(fluxR - fluxR.shift(X,-1))   (relaxingMagnet.m:26-27)
-    pc.csync();
-    pc.publish(1, Fu);
-    pc.csync();
+    tl.csync();
+    if (job_hi) fill_ghost(tl, S2, GS, +1, mhi, a.actX, 0, edge_of(MO_STORE_R, 1), binf);
+    __syncthreads();
+    // store.fluxR = F.*(1-vf) + F.shift(X,1).*vf   (relaxingMagnet.m:23-24)
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const T F = S2[tl.idx(k)];
+        const T Fp = shifted(tl, (const T*)S2, GS, k, +1, mhi, fc, f);
+        S3[tl.idx(k)] = F * (T(1) - vf[k]) + Fp * vf[k];
+    }
+    tl.csync();
+    if (job_lo) fill_ghost(tl, S3, GS, -1, mlo, a.actX, 0, edge_of(MO_STORE_R, 0), binf);
+    __syncthreads();
+    // store = B_I - ff*(fluxR - fluxR.shift(X,-1)); wMag = store.*velGrid   (relaxingMagnet.m:26-33)
     T W[CPT];
-    {
-        T glo = own0 ? mc.ghost_lo(1, e_sf_lo, true) : T(0);
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) { W[k] = T(0); continue; }
-            T st = bI[k] - ff * (Fu[k] - mc.sm(1, Fu, k, glo));
-            W[k] = st * vg[k];   // wMag = store .* velGrid   (relaxingMagnet.m:33)
+    for (int k = 0; k < CPT; ++k) {
+        const T Fu = S3[tl.idx(k)];
+        const T st = bI[k] - ff * (Fu - shifted(tl, (const T*)S3, GL, k, -1, mlo, fc, f));
+        W[k] = st * vg[k];
+        S0[tl.idx(k)] = W[k];
+        if (init_mag && tl.ok(k)) {
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_WMAG), x, y, z, (double)W[k]);
         }
     }
-    if (init_mag) init_edges(pc, et, mag_obj(c, d, MO_WMAG), W);
-
-    // flux, dFluxR, dFluxL from wMag shifts (relaxingMagnet.m:34-45): upper edge drifts 4 times
-    // (shift +1, +1, +2, +1 in evaluation order), the lower edge once.
-    double s_wm_hi = ((ownN || ownN2) && e_wm_hi) ? e_wm_hi[pc.col] : 0.0;
-    pc.csync();
-    pc.publish(0, W);
-    pc.csync();
+    tl.csync();
+    // wMag is shifted +1, +1, +2, +1 (upper edge drifts four times, in that order) and -1: one job
+    // computes the four upper ghosts from the successive edge states and stores the last state.
+    if (job_lo) fill_ghost(tl, S0, GS, -1, mlo, a.actX, 0, edge_of(MO_WMAG, 0), binf);
+    if (job_hi) {
+        double* eh = edge_of(MO_WMAG, 1);
+        const bool stateful = (mhi == BC_TRANS || mhi == BC_WALL) && eh != nullptr;
+        const bool drift = mhi == BC_TRANS && a.actX && eh != nullptr;
+        const double s0 = stateful ? eh[tl.col] : 0.0;
+        const double cur = (double)tl.row((const T*)S0, N - 1);
+        const double e1 = drift ? edge_drift(s0, cur) : s0;
+        const double e2 = drift ? edge_drift(e1, cur) : s0;
+        const double e3 = drift ? edge_drift(e2, cur) : s0;
+        const double e4 = drift ? edge_drift(e3, cur) : s0;
+        Ghost<T> u;
+        u.s0 = tl.row((const T*)S0, N > 1 ? 1 : 0);
+        u.sN1 = tl.row((const T*)S0, N - 1);
+        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e1);
+        GS[1 * Wb + b] = u;
+        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e2);
+        GS[2 * Wb + b] = u;
+        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e4);
+        GS[5 * Wb + b] = u;
+        Ghost<T> w2;
+        w2.s0 = tl.row((const T*)S0, N > 2 ? 2 : N - 1);
+        w2.sN1 = tl.row((const T*)S0, N - 1);
+        w2.g = bc_ghost(tl, (const T*)S0, +2, 1, mhi, a.actX, 0, eh, binf, e3);
+        GS[3 * Wb + b] = w2;
+        w2.g = bc_ghost(tl, (const T*)S0, +2, 2, mhi, a.actX, 0, eh, binf, e3);
+        GS[4 * Wb + b] = w2;
+        if (drift) eh[tl.col] = e4;
+    }
+    __syncthreads();
     T Fl[CPT];
-    {
-        T g1[2] = {T(0), T(0)}, g2[2] = {T(0), T(0)}, g3[2] = {T(0), T(0)}, g4[2] = {T(0), T(0)};
-        if (ownN || ownN2) {
-            bool tr = a.modeX[1] == BC_TRANS && a.actX;
-            double cur = (double)pc.endv(0, N - 1);
-            double e1 = tr ? edge_drift(s_wm_hi, cur) : s_wm_hi;
-            double e2 = tr ? edge_drift(e1, cur) : e1;
-            double e3 = tr ? edge_drift(e2, cur) : e2;
-            double e4 = tr ? edge_drift(e3, cur) : e3;
-            mc.ghost_hi(0, 1, e1, g1);
-            mc.ghost_hi(0, 1, e2, g2);
-            mc.ghost_hi(0, 2, e3, g3);
-            mc.ghost_hi(0, 1, e4, g4);
-            s_wm_hi = e4;
-        }
-        T glo = own0 ? mc.ghost_lo(0, e_wm_lo, true) : T(0);
-        T fx[CPT];
 #pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) { fx[k] = T(0); Fl[k] = T(0); continue; }
-            T w = W[k];
-            T v = vf[k];
-            fx[k] = w * (T(1) - v) + mc.sp(0, W, k, 1, g1) * v;
-            T dFluxR = mc.sp(0, W, k, 1, g2) - (v * mc.sp(0, W, k, 2, g3) + (T(1) - v) * w);
-            T dFluxL = w - (v * mc.sp(0, W, k, 1, g4) + (T(1) - v) * mc.sm(0, W, k, glo));
-            Fl[k] = fx[k] + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
-        }
-        if (init_mag) init_edges(pc, et, mag_obj(c, d, MO_FLUX), fx);
-    }
-    // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49)
-    pc.csync();   // every thread has read the wMag slot (and the wMag upper state) by now
-    if (ownN && e_wm_hi && a.modeX[1] == BC_TRANS && a.actX) e_wm_hi[pc.col] = s_wm_hi;
-    pc.publish(1, Fl);
-    pc.csync();
-    {
-        T glo = own0 ? mc.ghost_lo(1, e_fx_lo, true) : T(0);
-        T* Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (!pc.valid(k)) continue;
-            long long o = pc.off(k);
-            BI[o] = bI[k] - ff2 * (Fl[k] - mc.sm(1, Fl, k, glo));
-            Fout[o] = Fl[k];
+    for (int k = 0; k < CPT; ++k) {
+        const T w = W[k], v = vf[k];
+        const T* A = S0;
+        const T fx = w * (T(1) - v) + shifted(tl, A, GS + 0 * Wb, k, +1, mhi, fc, f) * v;
+        const T dFluxR = shifted(tl, A, GS + 1 * Wb, k, +1, mhi, fc, f) -
+                         (v * shifted2(tl, A, GS + 3 * Wb, GS + 4 * Wb, k, mhi, fc, f) + (T(1) - v) * w);
+        const T dFluxL = w - (v * shifted(tl, A, GS + 4 * Wb, k, +1, mhi, fc, f) +
+                              (T(1) - v) * shifted(tl, A, GL, k, -1, mlo, fc, f));
+        Fl[k] = fx + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
+        S1[tl.idx(k)] = Fl[k];
+        if (init_mag && tl.ok(k)) {
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_FLUX), x, y, z, (double)fx);
         }
     }
+    tl.csync();
+    if (job_lo) fill_ghost(tl, S1, GS, -1, mlo, a.actX, 0, edge_of(MO_FLUX, 0), binf);
+    __syncthreads();
+    // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49); F_I -> scratch for CT
+    T* Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const T fm = shifted(tl, (const T*)S1, GL, k, -1, mlo, fc, f);
+        if (!tl.ok(k)) continue;
+        const long long o = tl.off(k);
+        BI[o] = bI[k] - ff2 * (Fl[k] - fm);
+        Fout[o] = Fl[k];
+    }
+    if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
 }
 
 // ---- pointwise passes ---------------------------------------------------------------------------------
 __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, int& y, int& z) {
-    x = (int)(i % g.n[0]);
-    long long r = i / g.n[0];
-    y = (int)(r % g.n[1]);
-    z = (int)(r / g.n[1]);
+    unsigned u = (unsigned)i, n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
+    unsigned r = u / n0;
+    x = (int)(u - r * n0);
+    z = (int)(r / n1);
+    y = (int)(r - (unsigned)z * n1);
 }
 
 // C_I = F_I - F_I.shift(I, +1)   (flux(X) object of mag(I): mag-class BC along I, component I)
 template <typename T>
-__global__ void mag_ct1_kernel(const MagArgs a) {
+__global__ void mag_ct1_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const int d = a.X - 1;
@@ -411,7 +347,7 @@ __global__ void mag_ct1_kernel(const MagArgs a) {
 
 // D_I = C_I.shift(X, -1)   (flux(X) object of mag(I), lower X edge) -> written over F_I
 template <typename T>
-__global__ void mag_ct2_kernel(const MagArgs a) {
+__global__ void mag_ct2_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const int d = a.X - 1;
@@ -432,7 +368,7 @@ __global__ void mag_ct2_kernel(const MagArgs a) {
 
 // B_X' = (B_X - dt/dI1 * D_I1) - dt/dI2 * D_I2 -> scratch; cell-centred B of I2 (the last component).
 template <typename T>
-__global__ void mag_bx_kernel(const MagArgs a) {
+__global__ void mag_bx_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const double dt = a.tm->dt;
@@ -464,7 +400,7 @@ __global__ void mag_bx_kernel(const MagArgs a) {
 
 // B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1))
 template <typename T>
-__global__ void mag_cell_kernel(const MagArgs a) {
+__global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const int X = a.X, d = X - 1;

@@ -1,12 +1,16 @@
-// Pencil machinery shared by the sweep kernels.
+// Pencil tiles shared by the sweep kernels.
 //
-// A pencil is one line of cells along the sweep dimension d.  A CTA holds a bundle of Wb
-// pencils ("columns"); a thread-block cluster of CL CTAs splits long pencils into CL row ranges,
-// so a pencil of any length stays on chip (rank r owns rows [r*RC, (r+1)*RC), RC = G*CPT).
-// Each thread owns CPT consecutive cells of one column; values live in registers.  Stencil
-// neighbours across thread boundaries and the pencil-end windows that the boundary conditions
-// need (rows 0,1,2 and N-3,N-2,N-1) are exchanged through shared memory, and through
-// distributed shared memory (map_shared_rank) across the CTAs of a cluster.
+// A pencil is one line of cells along the sweep dimension d.  A CTA holds a bundle of Wb pencils
+// ("columns") and G rows of each (one cell per thread); a thread-block cluster of CL CTAs covers
+// pencils longer than G (rank r holds rows [r*G, (r+1)*G)), so every pencil stays on chip whatever
+// its length.  Thread (b, g) owns row g of column b; consecutive threads touch consecutive cells,
+// so global loads/stores are coalesced along x for every sweep direction.
+//
+// Stencil operands live in shared-memory arrays A[row][b] (one per flux array).  A neighbour read
+// is one shared load; the row across a CTA boundary is read from the neighbouring cluster rank
+// through DSMEM; the rows beyond the pencil ends are boundary-condition ghosts that a few threads
+// compute once per stage into ghost slots (shifting/*_shift.m), including the drift of stateful
+// edges.  Boundary predicates are per-thread constants, so the common path has no extra work.
 #pragma once
 
 #include "common.cuh"
@@ -21,131 +25,105 @@ struct SweepGeom {
     int N;            // pencil length g.n[d]
     long long ncol;   // number of pencils = ncell / N
     int Wb;           // pencils per CTA
-    int G;            // thread groups per pencil per CTA
+    int G;            // rows (threads) per pencil per CTA
     int CL;           // CTAs per cluster along the pencil
     int NT;           // threads per CTA = Wb * G
 };
 
-// Per-thread pencil context.
-template <typename T, int CPT, int NSLOT, bool HAS2 = false>
-struct Pencil {
-    const SweepGeom* sg;
-    int t, b, g, rank, RC;
-    long long col;     // global pencil index (may be >= ncol for idle threads)
-    bool colok;
-    int r0;            // first row of this thread's segment
-    int nv;            // valid rows in the segment (0..CPT)
-    long long base;    // linear offset of row 0 of this pencil
-    int coord1, coord2;// coordinates of the pencil along d1, d2
-    // shared buffers
-    T* xf;   // [NSLOT][NT] first value of each thread segment
-    T* xs;   // [NSLOT][NT] second value (for shifts by +2)
-    T* xl;   // [NSLOT][NT] last valid value
-    T* ends; // [NSLOT][Wb][6]
+// Ghost slot of one (array, side, column): the ghost value beyond the pencil end and the two fade
+// anchors (constant-shifted values at rows 0 and N-1 before damping).
+template <typename T>
+struct Ghost {
+    T g, s0, sN1;
+};
 
-    __device__ void init(const SweepGeom& s, unsigned char* smem_base) {
-        sg = &s;
-        t = threadIdx.x;
+template <typename T, int CPT>
+struct Tile {
+    int b, g, rank, N, Wb, G, CL, d, RC;
+    long long col;        // global pencil index
+    bool colok;
+    long long base;       // linear offset of row 0 of this pencil
+    long long sd;         // stride along the sweep
+    int coord1, coord2;
+    // rows owned by this thread: local row g + k*G, global row rank*RC + g + k*G
+
+    __device__ __forceinline__ void init(const SweepGeom& s) {
+        const int t = threadIdx.x;
         if (s.d == 0) { g = t % s.G; b = t / s.G; }
         else { b = t % s.Wb; g = t / s.Wb; }
         rank = (int)(blockIdx.x % (unsigned)s.CL);
         long long bundle = blockIdx.x / (unsigned)s.CL;
-        RC = s.G * CPT;
+        N = s.N;
+        Wb = s.Wb;
+        G = s.G;
+        CL = s.CL;
+        d = s.d;
+        RC = G * CPT;
         col = bundle * s.Wb + b;
         colok = col < s.ncol;
-        r0 = rank * RC + g * CPT;
-        int rem = s.N - r0;
-        nv = colok ? (rem < 0 ? 0 : (rem > CPT ? CPT : rem)) : 0;
         long long c = colok ? col : 0;
         coord1 = (int)(c % s.g.n[s.d1]);
         coord2 = (int)(c / s.g.n[s.d1]);
-        base = coord1 * s.g.s[s.d1] + (long long)coord2 * s.g.s[s.d2];
-        T* p = reinterpret_cast<T*>(smem_base);
-        xf = p; p += NSLOT * s.NT;
-        xs = p; if (HAS2) p += NSLOT * s.NT;
-        xl = p; p += NSLOT * s.NT;
-        ends = p;
+        base = coord1 * sel3(s.d1, s.g.s[0], s.g.s[1], s.g.s[2]) +
+               (long long)coord2 * sel3(s.d2, s.g.s[0], s.g.s[1], s.g.s[2]);
+        sd = sel3(s.d, s.g.s[0], s.g.s[1], s.g.s[2]);
     }
-    static __host__ __device__ size_t smem_bytes(int NT, int Wb) {
-        return sizeof(T) * ((size_t)(HAS2 ? 3 : 2) * NSLOT * NT + (size_t)NSLOT * Wb * 6);
-    }
-    __device__ __forceinline__ long long off(int k) const { return base + (long long)(r0 + k) * sg->g.s[sg->d]; }
-    __device__ __forceinline__ bool valid(int k) const { return k < nv; }
-    __device__ __forceinline__ int row(int k) const { return r0 + k; }
-    // cell coordinates (x, y, z) of segment row k
+    __device__ __forceinline__ int lrow(int k) const { return g + k * G; }
+    __device__ __forceinline__ int grow(int k) const { return rank * RC + g + k * G; }
+    __device__ __forceinline__ bool ok(int k) const { return colok && grow(k) < N; }
+    __device__ __forceinline__ long long off(int k) const { return base + (long long)grow(k) * sd; }
+    __device__ __forceinline__ int idx(int k) const { return lrow(k) * Wb + b; }
     __device__ __forceinline__ void coords(int k, int& x, int& y, int& z) const {
-        int r = r0 + k;
-        if (sg->d == 0) { x = r; y = coord1; z = coord2; }
-        else if (sg->d == 1) { x = coord1; y = r; z = coord2; }
+        int r = grow(k);
+        if (d == 0) { x = r; y = coord1; z = coord2; }
+        else if (d == 1) { x = coord1; y = r; z = coord2; }
         else { x = coord1; y = coord2; z = r; }
     }
-
     __device__ __forceinline__ void csync() const {
-        if (sg->CL > 1) cg::this_cluster().sync();
+        if (CL > 1) cg::this_cluster().sync();
         else __syncthreads();
     }
-    __device__ __forceinline__ int tid_of(int bb, int gg) const { return sg->d == 0 ? bb * sg->G + gg : gg * sg->Wb + bb; }
     template <typename U>
     __device__ __forceinline__ U* remote(U* p, int r) const {
-        if (sg->CL == 1) return p;
+        if (CL == 1 || r == rank) return p;
         return cg::this_cluster().map_shared_rank(p, r);
     }
-
-    // Publish array A (this thread's CPT values) into slot s.
-    __device__ void publish(int s, const T (&A)[CPT]) {
-        int NT = sg->NT;
-        xf[s * NT + t] = A[0];
-        if (HAS2) xs[s * NT + t] = A[CPT > 1 ? 1 : 0];
-        if (nv > 0) xl[s * NT + t] = A[nv - 1];
-#pragma unroll
-        for (int k = 0; k < CPT; ++k) {
-            if (k < nv) {
-                int r = r0 + k;
-                if (r < 3) ends[(s * sg->Wb + b) * 6 + r] = A[k];
-                int u = r - (sg->N - 3);
-                if (u >= 0) ends[(s * sg->Wb + b) * 6 + 3 + u] = A[k];
-            }
-        }
-    }
-    // Value of the array at global row r of this column (r in 0..2 or N-3..N-1), from the ends buffer.
-    __device__ T endv(int s, int r) const {
-        int slot = r < 3 ? r : 3 + (r - (sg->N - 3));
+    // Value of array A at global row r of this column (any cluster rank).
+    template <typename U>
+    __device__ __forceinline__ U row(const U* A, int r) const {
         int rk = r / RC;
-        T* p = remote(ends, rk);
-        return p[(s * sg->Wb + b) * 6 + slot];
+        const U* p = remote(const_cast<U*>(A), rk);
+        return p[(r - rk * RC) * Wb + b];
     }
-    // A at row (r0 + k - 1); requires that row to exist (>= 0).
-    __device__ T prev(int s, const T (&A)[CPT], int k) const {
-        if (k > 0) return A[k - 1];
-        int NT = sg->NT;
-        if (g > 0) return xl[s * NT + tid_of(b, g - 1)];
-        T* p = remote(xl, rank - 1);
-        return p[s * NT + tid_of(b, sg->G - 1)];
+    // A.shift(d, -1) and A.shift(d, +1) at row k before fade damping (gs: the array's ghost slots,
+    // [side][column]).  The rare cases (pencil end, other cluster rank) are per-row constants.
+    template <typename U>
+    __device__ __forceinline__ U below(const U* A, const Ghost<U>* gs, int k) const {
+        if (grow(k) == 0) return gs[b].g;
+        if (lrow(k) == 0) return remote(const_cast<U*>(A), rank - 1)[(RC - 1) * Wb + b];
+        return A[idx(k) - Wb];
     }
-    // A at row (r0 + k + 1); requires that row to exist (<= N-1).
-    __device__ T next(int s, const T (&A)[CPT], int k) const {
-        if (k + 1 < CPT) return A[k + 1];
-        int NT = sg->NT;
-        if (g + 1 < sg->G) return xf[s * NT + tid_of(b, g + 1)];
-        T* p = remote(xf, rank + 1);
-        return p[s * NT + tid_of(b, 0)];
+    template <typename U>
+    __device__ __forceinline__ U above(const U* A, const Ghost<U>* gs, int k) const {
+        if (grow(k) >= N - 1) return gs[Wb + b].g;   // also rows past the pencil end (idle cells)
+        if (lrow(k) == RC - 1) return remote(const_cast<U*>(A), rank + 1)[b];
+        return A[idx(k) + Wb];
     }
-    // A at row (r0 + k + 2); requires that row to exist.  Needs CPT >= 2.
-    __device__ T next2(int s, const T (&A)[CPT], int k) const {
-        if (k + 2 < CPT) return A[k + 2];
-        int NT = sg->NT;
-        int gg = g + 1, rr = rank;
-        if (gg >= sg->G) { gg = 0; rr = rank + 1; }
-        int sel = (k + 2) - CPT;   // 0: first of next segment, 1: second
-        T* pf = rr == rank ? xf : remote(xf, rr);
-        T* ps = rr == rank ? xs : remote(xs, rr);
-        return sel == 0 ? pf[s * NT + tid_of(b, gg)] : ps[s * NT + tid_of(b, gg)];
+    // A.shift(d, +2) at row k before fade damping; ghosts at rows N and N+1 in g2[0], g2[1].
+    template <typename U>
+    __device__ __forceinline__ U above2(const U* A, const U g2[2], int k) const {
+        const int r = grow(k) + 2;
+        if (r >= N) return r == N ? g2[0] : g2[1];
+        const int lr = lrow(k) + 2;
+        if (lr >= RC) return remote(const_cast<U*>(A), rank + 1)[(lr - RC) * Wb + b];
+        return A[idx(k) + 2 * Wb];
     }
+    // Cluster rank that holds the pencil's last row (where its upper ghosts are consumed).
+    __device__ __forceinline__ int rank_hi() const { return (N - 1) / RC; }
 };
 
-// Value of A.shift(d, n)[r] for n = -1 (from_prev) or +1 computed from the const-shifted value
-// sv (A[r-1] or A[r+1] with the end row repeated) and the fade damping of fade_shift.m:31-44.
-// a0/an1 are the const-shifted values at rows 0 and N-1 (the two fade anchors before damping).
+// Fade damping of fade_shift.m:31-44 applied to the constant-shifted value sv at row r of a line of
+// N cells: s0 and sN1 are the constant-shifted values at rows 0 and N-1 (the two anchors).
 template <typename T>
 __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, int f, T s0, T sN1) {
     T lf = sv;
@@ -157,6 +135,80 @@ __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, in
         lf = (T(1) - c) * lf + c * lfN1;
     }
     return lf;
+}
+
+// A.shift(d, n) at row k for n = -1 / +1, fade damping included.
+template <typename T, int CPT>
+__device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* gs, int k, int n, int mode,
+                                     const double* fc, int f) {
+    T v = n < 0 ? tl.below(A, gs, k) : tl.above(A, gs, k);
+    if (mode == BC_FADE) {
+        const Ghost<T>& q = gs[(n < 0 ? 0 : tl.Wb) + tl.b];
+        v = fade_apply(v, tl.grow(k), tl.N, fc, f, q.s0, q.sN1);
+    }
+    return v;
+}
+
+// "No stored-edge value supplied" marker (stored edges are finite physical values).
+constexpr double NO_EV = -1.0e300;
+
+// Ghost of array A beyond the pencil end for one shift call A.shift(d, n): n = -1 (row -1),
+// n = +1 (row N) or n = +2 (rows N and N+1, mp = 1 or 2 selects which).  Stateful edges (trans,
+// wall) use `ev` when given; otherwise a trans edge is drifted here and written back (the caller is
+// the one thread per pencil end and shift call).  Rows are read through tl.row (any cluster rank).
+template <typename T, int CPT>
+__device__ __forceinline__ T bc_ghost(const Tile<T, CPT>& tl, const T* A, int n, int mp, int mode, int act, int flip,
+                                      double* edge, double bc_inf, double ev) {
+    const int N = tl.N;
+    const bool upper = n > 0;
+    const int m = n < 0 ? -n : n;
+    switch (mode) {
+        case BC_CIRC: return upper ? tl.row(A, mp - 1) : tl.row(A, N - 1);
+        case BC_MIRROR: {
+            T x = upper ? tl.row(A, N - 1 - mp) : tl.row(A, mp);
+            return flip ? -x : x;
+        }
+        case BC_WALL: return (T)(ev != NO_EV ? ev : edge[tl.col]);
+        case BC_TRANS: {
+            double y0, y1, y2, cur;
+            if (upper) {
+                y0 = (double)tl.row(A, trans_pick_upper(N, m, 0));
+                y1 = (double)tl.row(A, trans_pick_upper(N, m, 1));
+                y2 = (double)tl.row(A, trans_pick_upper(N, m, 2));
+                cur = (double)tl.row(A, N - 1);
+            } else {
+                y0 = (double)tl.row(A, trans_pick_lower(N, m, 0));
+                y1 = (double)tl.row(A, trans_pick_lower(N, m, 1));
+                y2 = (double)tl.row(A, trans_pick_lower(N, m, 2));
+                cur = (double)tl.row(A, 0);
+            }
+            double e = 0.0;
+            if (act) {
+                if (ev != NO_EV) e = ev;
+                else {
+                    e = edge_drift(edge[tl.col], cur);
+                    edge[tl.col] = e;
+                }
+            }
+            // the 1e-4 keep test compares with the unshifted array at the ghost's position
+            const int gpos = upper ? N - 1 - (m - mp) : 0;
+            return (T)trans_ghost(y0, y1, y2, e, bc_inf, 3.0 + mp, (double)tl.row(A, gpos));
+        }
+        default: return upper ? tl.row(A, N - 1) : tl.row(A, 0);   // const and fade: constant shift
+    }
+}
+
+// Fill the ghost slot of array A for one side (n = -1 or +1) of this thread's column: ghost value
+// and fade anchors.  Called by exactly one thread per (array, side, column) and stage.
+template <typename T, int CPT>
+__device__ __forceinline__ void fill_ghost(const Tile<T, CPT>& tl, const T* A, Ghost<T>* gs, int n, int mode, int act,
+                                           int flip, double* edge, double bc_inf) {
+    Ghost<T> q;
+    q.g = bc_ghost(tl, A, n, 1, mode, act, flip, edge, bc_inf, NO_EV);
+    const int N = tl.N;
+    if (n < 0) { q.s0 = tl.row(A, 0); q.sN1 = tl.row(A, N - 2 < 0 ? 0 : N - 2); }
+    else { q.s0 = tl.row(A, N > 1 ? 1 : 0); q.sN1 = tl.row(A, N - 1); }
+    gs[(n < 0 ? 0 : tl.Wb) + tl.b] = q;
 }
 
 }  // namespace img

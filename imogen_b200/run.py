@@ -187,13 +187,21 @@ class ImogenRun:
         check(lib().img_set_state(self._h, _dp(m), _dp(p), _dp(e), _dp(b)), self._h)
 
     def upload(self, name, arr):
+        """X.array = value for one variable (ImogenArray.m:82-89); no copy when `arr` is already a
+        flat C-contiguous float64 buffer (e.g. pinned host memory)."""
         a = self._flat(arr)
         check(lib().img_upload(self._h, VAR[name], _dp(a), a.size), self._h)
 
-    def download(self, name):
-        out = np.empty(self.ncell)
+    def download(self, name, out=None):
+        """get.array of one variable; `out` (a C-contiguous float64 buffer of ncell values, e.g.
+        pinned host memory) is filled in place when given."""
+        if out is None:
+            out = np.empty(self.ncell)
+            check(lib().img_download(self._h, VAR[name], _dp(out), out.size), self._h)
+            return out.reshape(self.grid, order="F")
+        assert out.dtype == np.float64 and out.flags.c_contiguous and out.size == self.ncell
         check(lib().img_download(self._h, VAR[name], _dp(out), out.size), self._h)
-        return out.reshape(self.grid, order="F")
+        return out
 
     def state(self):
         g = self.download
@@ -225,6 +233,19 @@ class ImogenRun:
 
     def sync(self):
         check(lib().img_sync(self._h), self._h)
+
+    @property
+    def stream(self):
+        """cudaStream_t (as an int) that all of this run's kernels are launched on."""
+        s = ctypes.c_void_p()
+        check(lib().img_get_stream(self._h, ctypes.byref(s)), self._h)
+        return s.value or 0
+
+    @property
+    def launches(self):
+        n = ctypes.c_uint64()
+        check(lib().img_launch_count(self._h, ctypes.byref(n)), self._h)
+        return n.value
 
     def totals(self):
         """Neumaier-compensated FP64 sums of rho, px, py, pz, E, Bx, By, Bz."""

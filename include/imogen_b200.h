@@ -122,6 +122,13 @@ const char* img_last_error(const img_ctx* ctx);
 /* Device bytes a context with this config allocates (for HBM-budget admission). */
 size_t img_bytes_required(const img_config* cfg);
 
+/* The CUDA stream (cudaStream_t) all work of the context is issued on, for callers that record
+ * CUDA events around calls or order their own work after it.  No reference counterpart. */
+int img_get_stream(img_ctx* ctx, void** stream);
+
+/* Number of kernels the context has launched so far.  No reference counterpart. */
+int img_launch_count(const img_ctx* ctx, uint64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,17 @@ def errors(sa, sb):
     return out
 
 
+def errors_vector(sa, sb):
+    """rho and E per variable; momentum and B as vectors: sum|a-b| / sum|b| over all components
+    (components that start at zero, like vz in a 2-D-seeded KH layer, are mostly round-off)."""
+    out = {}
+    for k in ("mass", "ener"):
+        out[k] = rel_l1(np.asarray(sa[k]), np.asarray(sb[k]))
+    for k in ("mom", "mag"):
+        out[k] = rel_l1(np.asarray(sa[k]), np.asarray(sb[k]))
+    return out
+
+
 def smooth_state(grid, seed=0, mhd=True, gamma=5 / 3, amp=0.2):
     """A smooth, well-resolved random-phase state (positive density and pressure)."""
     rng = np.random.default_rng(seed)

@@ -1,0 +1,60 @@
+"""The C ABI library: loads, exports every symbol include/imogen_b200.h declares, and rejects
+invalid settings before touching a GPU (CPU only)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+import imogen_b200
+from imogen_b200 import _lib
+from imogen_b200.run import bc_table, make_config
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "imogen_b200.h")).read()
+    return sorted(set(re.findall(r"\b(img_[a-z_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    syms = header_symbols()
+    assert len(syms) >= 18
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(_lib.SYMBOLS)
+
+
+def test_create_rejects_settings_the_reference_cannot_run():
+    L = _lib.lib()
+    for kw, code in [(dict(grid=(32, 1, 1), bc="mirror"), -4), (dict(grid=(19, 32, 1), bc="fade"), -4)]:
+        c = make_config(**kw)
+        h = ctypes.c_void_p()
+        assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == code
+        assert b"BC" in L.img_last_error(None)
+    c = make_config(grid=(32, 32, 1), precision=7)
+    h = ctypes.c_void_p()
+    assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -1
+
+
+def test_bytes_required_counts_state_scratch_and_edges():
+    n = 64 * 48
+    b64 = imogen_b200.bytes_required(grid=(64, 48, 1), magnet=True, precision="fp64")
+    b32 = imogen_b200.bytes_required(grid=(64, 48, 1), magnet=True, precision="mixed")
+    assert b64 >= 16 * n * 8 and b32 >= 16 * n * 4 and b64 > b32
+    bt = imogen_b200.bytes_required(grid=(64, 48, 1), magnet=True, bc="trans")
+    assert bt > b64          # stored edges of the trans objects
+
+
+def test_bc_table_forms():
+    assert bc_table("trans") == [[[4] * 3, [4] * 3]] * 4
+    t = bc_table({"x": ("const", "wall"), "y": "circ", "z": "circ"})
+    assert t[0] == [[1, 0, 0], [5, 0, 0]]
+
+
+def test_null_context_is_an_error_not_a_crash():
+    L = _lib.lib()
+    assert L.img_step(None) == -1
+    assert L.img_sync(None) == -1

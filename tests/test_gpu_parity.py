@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from imogen_b200 import problems
-from tests.parity import errors, make_pair, smooth_state
+from tests.parity import errors, errors_vector, make_pair, smooth_state
 
 pytestmark = pytest.mark.gpu
 
@@ -97,9 +97,42 @@ def test_workload_100_iterations_fp64(name):
         s, st = problems.sedov(48, dims=2)
     else:
         s, st = problems.sedov(24, dims=3)
-    s = dict(s, iter_max=100, time_max=1e5)
+    # Sedov runs to its own end time (t = 0.05): past it the fade BCs damp every speed below the
+    # 1e-2 CFL floor and TimeManager.m:79-86 raises, in the reference as in the oracle.
+    s = dict(s, iter_max=100, time_max=s["time_max"] if name.startswith("sedov") else 1e5)
     o, g = make_pair(s, st)
     no = o.run()
     ng = g.run()
-    assert no == ng == 100
+    assert no == ng and (no == 100 or name.startswith("sedov"))
+    assert abs(g.time.time - o.time) <= 1e-12 * max(1.0, o.time)
     _assert_close(o, g, 1e-10, name)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_long_pencils_use_clusters(precision):
+    """Pencils longer than one CTA's cells are split over a thread-block cluster (DSMEM exchange)."""
+    tol = 1e-11 if precision == "fp64" else 2e-5
+    s, st = problems.sod(3000)
+    s = dict(s, iter_max=10, time_max=1e5)
+    o, g = make_pair(s, st, precision=precision)
+    o.run()
+    g.run()
+    _assert_close(o, g, tol, f"sod 3000 {precision}")
+    s, st = problems.brio_wu_tube(2500, 1.0, 0.125, 1.0, 0.1)
+    s = dict(s, iter_max=5, time_max=1e5)
+    o, g = make_pair(s, st, precision=precision)
+    o.run()
+    g.run()
+    _assert_close(o, g, tol, f"brio-wu 2500x3x3 {precision}")
+
+
+@pytest.mark.parametrize("name", ["orszag_tang", "kelvin_helmholtz"])
+def test_mixed_precision_error_is_bounded(name):
+    """Mixed form (FP32 state/fluxes, FP64 pressure/CFL) against the FP64 oracle, 20 iterations."""
+    s, st = problems.orszag_tang(64) if name == "orszag_tang" else problems.kelvin_helmholtz(16)
+    s = dict(s, iter_max=20, time_max=1e5)
+    o, g = make_pair(s, st, precision="mixed")
+    o.run()
+    g.run()
+    e = errors_vector(g.state(), o.state())
+    assert max(e.values()) < 1e-5, e
