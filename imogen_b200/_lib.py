@@ -22,7 +22,7 @@ STATUS = {
 SYMBOLS = (
     "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
-    "img_get_time", "img_set_time", "img_totals", "img_sync", "img_last_error", "img_bytes_required",
+    "img_get_time", "img_set_time", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_launch_count",
 )
 
@@ -81,6 +81,7 @@ def lib():
     L.img_get_time.argtypes = [vp, dp, dp, ip]
     L.img_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
     L.img_totals.argtypes = [vp, dp]
+    L.img_totals_static.argtypes = [vp, dp]
     L.img_sync.argtypes = [vp]
     L.img_last_error.argtypes = [vp]
     L.img_last_error.restype = ctypes.c_char_p
@@ -92,7 +93,7 @@ def lib():
     L.img_launch_count.restype = ctypes.c_int
     for name in ("img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
                  "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step",
-                 "img_run", "img_get_time", "img_set_time", "img_totals", "img_sync"):
+                 "img_run", "img_get_time", "img_set_time", "img_totals", "img_totals_static", "img_sync"):
         getattr(L, name).restype = ctypes.c_int
     _LIB = L
     return L

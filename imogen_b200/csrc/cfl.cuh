@@ -177,4 +177,20 @@ __global__ void totals_kernel(Geom g, const void* const* qp, double* partial) {
     }
 }
 
+// Final Neumaier combine of the per-block totals partials, in block order (the same operations, in
+// the same order, as the host combine of img_totals): one thread per variable.
+__global__ void totals_finalize_kernel(const double* partial, int nblocks, double* out) {
+    const int v = threadIdx.x;
+    if (v >= 8) return;
+    double S = 0.0, C = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        const double x = partial[(b * 8 + v) * 2];
+        const double t = S + x;
+        C += fabs(S) >= fabs(x) ? (S - t) + x : (x - t) + S;
+        S = t;
+        C += partial[(b * 8 + v) * 2 + 1];
+    }
+    out[v] = S + C;
+}
+
 }  // namespace img

@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -955,6 +956,66 @@ int img_totals(img_ctx* ctx, double out[8]) {
         }
         out[v] = S + C;
     }
+    return IMG_OK;
+}
+
+// ---- totals with static scratch -------------------------------------------------------------------
+// img_totals_static works in a file-scope device array instead of the context's slab: the 1023
+// per-block partial pairs (sum, compensation) of 8 variables, the 8 results and the 8-entry pointer
+// table, 128.2 KiB in all, whatever the grid size (the reduction is a grid-stride loop over a fixed
+// 1023 blocks).  Every call overwrites every slot it later reads, so nothing must start at zero.
+// All contexts of a device share the one array: calls that overlap in time (other threads, other
+// streams) race on it and must be serialised by the caller.
+namespace {
+constexpr int kStaticTotalsBlocks = 1023;
+constexpr size_t kStaticTotalsPartial = 2 * 8 * kStaticTotalsBlocks;
+constexpr size_t kStaticTotalsDoubles = kStaticTotalsPartial + 8 + 8;
+constexpr int kMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) double g_static_totals[kStaticTotalsDoubles];
+
+// Address of g_static_totals on device `dev` (the current device), looked up once per device.  The
+// first call on a device must come before any stream capture that includes this entry point: the
+// lookup may load the module.
+static int static_totals_scratch(img_ctx* ctx, double** out) {
+    static std::mutex mu;
+    static double* addr[kMaxDevices] = {};
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) return fail(ctx, IMG_ERR_CUDA, "cudaGetDevice failed");
+    if (cur != ctx->dev)
+        return fail(ctx, IMG_ERR_ARG, "current device %d is not the context's device %d", cur, ctx->dev);
+    if (cur < 0 || cur >= kMaxDevices) return fail(ctx, IMG_ERR_UNSUPPORTED, "device ordinal %d >= %d", cur, kMaxDevices);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[cur]) {
+        void* a = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&a, g_static_totals);
+        if (e != cudaSuccess || !a)
+            return fail(ctx, IMG_ERR_CUDA, "cudaGetSymbolAddress(static totals scratch): %s", cudaGetErrorString(e));
+        addr[cur] = static_cast<double*>(a);
+    }
+    *out = addr[cur];
+    return IMG_OK;
+}
+
+int img_totals_static(img_ctx* ctx, double out[8]) {
+    if (!ctx || !out) return fail(ctx, IMG_ERR_ARG, "null argument");
+    double* scratch = nullptr;
+    int rc = static_totals_scratch(ctx, &scratch);
+    if (rc != IMG_OK) return rc;
+    double* partial = scratch;
+    double* result = scratch + kStaticTotalsPartial;
+    void** table = reinterpret_cast<void**>(result + 8);
+    void* qp_host[8];
+    for (int v = 0; v < 8; ++v) qp_host[v] = ctx->q[v];
+    CK(cudaMemcpyAsync(table, qp_host, sizeof qp_host, cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->elem == 8) totals_kernel<double><<<kStaticTotalsBlocks, 256, 0, ctx->stream>>>(ctx->g, table, partial);
+    else totals_kernel<float><<<kStaticTotalsBlocks, 256, 0, ctx->stream>>>(ctx->g, table, partial);
+    CK(cudaGetLastError());
+    totals_finalize_kernel<<<1, 32, 0, ctx->stream>>>(partial, kStaticTotalsBlocks, result);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, result, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
 }
 

@@ -253,6 +253,12 @@ class ImogenRun:
         check(lib().img_totals(self._h, _dp(out)), self._h)
         return out
 
+    def totals_static(self):
+        """The same sums as totals(), computed in the library's static device scratch (no allocation)."""
+        out = np.zeros(8)
+        check(lib().img_totals_static(self._h, _dp(out)), self._h)
+        return out
+
 
 # ---- reference call surface ------------------------------------------------------------------------
 def flux(run, mass, mom, ener, mag, grav, order):

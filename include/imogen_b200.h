@@ -113,6 +113,15 @@ int img_set_time(img_ctx* ctx, double time, double dt, int iteration);
 /* Compensated (Neumaier) FP64 totals of rho, px, py, pz, E, Bx, By, Bz over the grid. */
 int img_totals(img_ctx* ctx, double out[8]);
 
+/* The same totals as img_totals, bit for bit, computed without allocating anything: the scratch is a
+ * file-scope device array of 128.2 KiB (1023 per-block partial pairs of 8 variables, the 8 results and
+ * an 8-entry pointer table), looked up once per device with cudaGetSymbolAddress; grids of any size.
+ * The first call on a device should come before any stream capture.  Every call overwrites all the
+ * scratch it reads, so nothing needs to start at zero.  All contexts of a device share that scratch:
+ * calls that overlap in time race on it and must be serialised by the caller.  The context's device
+ * must be current.  No counterpart in the reference. */
+int img_totals_static(img_ctx* ctx, double out[8]);
+
 /* Block until the context's stream is idle; returns a pending device error if any. */
 int img_sync(img_ctx* ctx);
 
