@@ -147,24 +147,18 @@ __device__ __forceinline__ double pchip_mid_slope(double hl, double hr, double d
     return (msign(dl) * msign(dr) > 0) ? (w1 + w2) / (w1 / dl + w2 / dr) : 0.0;
 }
 
-// MATLAB pchip through x = [1 2 3 inf inf+1] with values y0..y4, evaluated at xe >= 3 (Moler,
+// MATLAB pchip through x = [1 2 3 inf inf+1] with values y0..y4, evaluated at xe >= 4 (Moler,
 // "Numerical Computing with MATLAB", pchiptx; the interval is the last breakpoint <= xe, clamped
-// to the last interval as ppval does).  Scalars only: no local-memory arrays.
-__device__ __forceinline__ double pchip5(double y0, double y1, double y2, double y3, double y4, double inf,
-                                         double xe) {
+// to the last interval as ppval does).  For xe >= 4 the interval is [3, inf) or [inf, inf+1], so
+// only the slopes at x = 3, inf and inf+1 are formed (y0 enters none of them).  Scalars only.
+__device__ __forceinline__ double pchip5(double y1, double y2, double y3, double y4, double inf, double xe) {
     const double x3 = inf, x4 = inf + 1.0;
-    const double h0 = 1.0, h1 = 1.0, h2 = x3 - 3.0, h3 = x4 - x3;
-    const double e0 = (y1 - y0) / h0, e1 = (y2 - y1) / h1, e2 = (y3 - y2) / h2, e3 = (y4 - y3) / h3;
-    const double s0 = pchip_end_slope(h0, h1, e0, e1);
-    const double s1 = pchip_mid_slope(h0, h1, e0, e1);
-    const double s2 = pchip_mid_slope(h1, h2, e1, e2);
+    const double h1 = 1.0, h2 = x3 - 3.0, h3 = x4 - x3;
+    const double e1 = (y2 - y1) / h1, e2 = (y3 - y2) / h2, e3 = (y4 - y3) / h3;
     const double s3 = pchip_mid_slope(h2, h3, e2, e3);
-    const double s4 = pchip_end_slope(h3, h2, e3, e2);
     double xk, yk, hk, ek, dk, dk1;
-    if (xe >= x3) { xk = x3; yk = y3; hk = h3; ek = e3; dk = s3; dk1 = s4; }
-    else if (xe >= 3.0) { xk = 3.0; yk = y2; hk = h2; ek = e2; dk = s2; dk1 = s3; }
-    else if (xe >= 2.0) { xk = 2.0; yk = y1; hk = h1; ek = e1; dk = s1; dk1 = s2; }
-    else { xk = 1.0; yk = y0; hk = h0; ek = e0; dk = s0; dk1 = s1; }
+    if (xe >= x3) { xk = x3; yk = y3; hk = h3; ek = e3; dk = s3; dk1 = pchip_end_slope(h3, h2, e3, e2); }
+    else { xk = 3.0; yk = y2; hk = h2; ek = e2; dk = pchip_mid_slope(h1, h2, e1, e2); dk1 = s3; }
     const double s = xe - xk;
     const double c1 = (dk + dk1 - 2 * ek) / (hk * hk);
     const double c2 = (3 * ek - 2 * dk - dk1) / hk;
@@ -186,13 +180,13 @@ __host__ __device__ __forceinline__ int trans_pick_upper(int N, int m, int q) {
     return p > N - 1 ? N - 1 : p;
 }
 
-// Transparent ghost value (shifting/transparent_shift.m:23-99).  y3 = the three array values that
-// the reference feeds at x = 1, 2, 3 (x = 3 is the edge cell), edge = the stored edge after its
-// drift (0 when the edge store is not ACTIVE(DIRECT)), xe = 4 or 5, orig = the unshifted array
-// value at the ghost position (kept when the extrapolation is within 1e-4 of it).
-__device__ __forceinline__ double trans_ghost(double y0, double y1, double y2, double edge, double inf, double xe,
-                                              double orig) {
-    double out = pchip5(y0, y1, y2, edge, edge, inf, xe);
+// Transparent ghost value (shifting/transparent_shift.m:23-99).  y1, y2 = the array values that
+// the reference feeds at x = 2, 3 (x = 3 is the edge cell; the value at x = 1 does not affect the
+// result at xe >= 4), edge = the stored edge after its drift (0 when the edge store is not
+// ACTIVE(DIRECT)), xe = 4 or 5, orig = the unshifted array value at the ghost position (kept when
+// the extrapolation is within 1e-4 of it).
+__device__ __forceinline__ double trans_ghost(double y1, double y2, double edge, double inf, double xe, double orig) {
+    double out = pchip5(y1, y2, edge, edge, inf, xe);
     bool t = fabs(orig - out) < 1e-4;
     return (t ? 0.0 : 1.0) * out + (t ? 1.0 : 0.0) * orig;
 }

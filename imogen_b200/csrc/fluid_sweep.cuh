@@ -7,9 +7,9 @@
 // arrays of each variable are synthesised in the same pass.  The state is read once and written
 // once; the only other HBM traffic is the stored edges of stateful boundaries (trans, wall).
 //
-// Shared memory: two sets of ten flux arrays (R and L of the five variables) -- set A holds the
-// predictor fluxes and then the corrector fluxes, set B the half-step state and then the limited
-// corrector fluxes -- plus the ghost slots of the ten arrays of the current stage.
+// Shared memory: two sets of ten halo'd flux arrays (R and L of the five variables) -- set A holds
+// the predictor fluxes and then the corrector fluxes, set B the half-step state and then the limited
+// corrector fluxes -- plus the fade anchors of the ten arrays of the current stage.
 #pragma once
 
 #include "pencil.cuh"
@@ -40,10 +40,10 @@ struct FluidArgs {
 constexpr int FLUID_NARR = 20;
 constexpr int MAX_WARPS = 16;
 
-// Dynamic shared memory of the fluid kernel: 20 arrays of RC*Wb values + ghost slots of 10 arrays.
+// Dynamic shared memory of the fluid kernel: 20 halo'd arrays + fade anchors of 10 arrays x 2 sides.
 template <typename T>
 __host__ __device__ inline size_t fluid_smem_bytes(int RC, int Wb) {
-    return sizeof(T) * (size_t)FLUID_NARR * RC * Wb + sizeof(Ghost<T>) * 10 * 2 * (size_t)Wb;
+    return sizeof(T) * (size_t)FLUID_NARR * tile_rows(RC) * Wb + sizeof(Ghost<T>) * 10 * 2 * (size_t)Wb;
 }
 
 template <typename T>
@@ -99,32 +99,45 @@ __device__ __forceinline__ T press_speed(double G, int d, const T u[5], double m
 
 // Column max over the pencil (and the cluster); also a full stage barrier (tl.csync).  Lanes of a
 // column reduce with warp shuffles; where a pencil spans several warps one lane per (warp, column)
-// writes part[warp][b] and every thread then takes the max over the warps of all CTAs of its
-// cluster.  No atomics: every slot has exactly one writer, and part is zero beforehand.
+// writes part[warp][b], and after the barrier the lanes of each column share the reads of those
+// slots over all cluster ranks and reduce again.  No atomics: every slot has exactly one writer.
 template <typename T, int CPT>
-__device__ __forceinline__ double column_max(const Tile<T, CPT>& tl, int NT, double (*part)[32], double local) {
+__device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part)[32], T local) {
     const unsigned mask = 0xffffffffu;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (tl.d == 0 && tl.G <= 32 && tl.CL == 1) {   // each pencil lies inside one warp
         for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
         tl.csync();
         return local;
     }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int grp, lig, w0, nwc;   // lanes of the column in a warp, this lane's index among them, its warps
     bool leader;
-    if (tl.d == 0) {   // G is a multiple of 32: one column per warp
+    if (tl.d == 0) {   // G is a multiple of 32: whole warps per column
         for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
         leader = lane == 0;
+        grp = 32;
+        lig = lane;
+        w0 = (tl.b * tl.G) >> 5;
+        nwc = tl.G >> 5;
     } else {           // lanes b, b + Wb, ... belong to column b
         for (int o = 16; o >= tl.Wb; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
         leader = lane < tl.Wb;
+        grp = 32 / tl.Wb;
+        lig = lane / tl.Wb;
+        w0 = 0;
+        nwc = NT >> 5;
     }
     if (leader) part[warp][tl.b] = local;
     tl.csync();
-    const int nw = NT >> 5;
-    double m = 0.0;
-    for (int r = 0; r < tl.CL; ++r) {
-        double (*rp)[32] = tl.remote(part, r);
-        for (int w = 0; w < nw; ++w) m = fmax(m, rp[w][tl.b]);
+    T m = T(0);
+    for (int j = lig; j < tl.CL * nwc; j += grp) {
+        const int r = j / nwc, w = w0 + j - r * nwc;
+        m = fmax(m, tl.remote(part, r)[w][tl.b]);
+    }
+    if (tl.d == 0) {
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
+    } else {
+        for (int o = 16; o >= tl.Wb; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
     }
     return m;
 }
@@ -151,27 +164,22 @@ __device__ __forceinline__ bool on_face(const Geom& g, int x, int y, int z) {
     return x == 0 || x == g.n[0] - 1 || y == 0 || y == g.n[1] - 1 || (g.ndims > 2 && (z == 0 || z == g.n[2] - 1));
 }
 
-// Ghost jobs of one stage for the ten arrays R_v (= base + v*AS) and L_v (= base + (5+v)*AS):
-// `lo_mask`/`hi_mask` (bit 0: R, bit 1: L) select which sides this stage shifts.  Lower ghosts are
-// computed on cluster rank 0, upper ghosts on the rank holding the last row, by the threads of each
-// column in turn; `kindR/kindL` name the fluid objects whose stored edges are used.  Each job is one
-// shift call of the reference, so a trans edge drifts exactly once per job.
+// Halo jobs of one stage for the ten arrays R_v (= base + v*AS) and L_v (= base + (5+v)*AS):
+// `lo_mask`/`hi_mask` (bit 0: R, bit 1: L) say which sides the reference shifts in the coming stage
+// (a pencil-end ghost is computed only for those); `kindR/kindL` name the fluid objects whose stored
+// edges are used.  The 20 (array, side) jobs of a column are shared by its threads.
 template <typename T, int CPT>
-__device__ __forceinline__ void fluid_ghost_jobs(const Tile<T, CPT>& tl, const FluidArgs& a, const T* base, size_t AS,
-                                                 Ghost<T>* GS, int lo_mask, int hi_mask, int kindR, int kindL) {
+__device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const FluidArgs& a, T* base, size_t AS,
+                                                Ghost<T>* an, int lo_mask, int hi_mask, int kindR, int kindL) {
     if (!tl.colok) return;
-    const int d = tl.d;
-    const bool do_lo = tl.rank == 0, do_hi = tl.rank == tl.rank_hi();
-    if (!do_lo && !do_hi) return;
     for (int j = tl.g; j < 20; j += tl.G) {   // job j: array j % 10 (R0..R4, L0..L4), side j / 10
         const int arr = j % 10, side = j / 10;
         const int isL = arr >= 5, v = arr - 5 * isL;
-        if (side == 0 && !(do_lo && (lo_mask >> isL & 1))) continue;
-        if (side == 1 && !(do_hi && (hi_mask >> isL & 1))) continue;
+        const bool shift = ((side ? hi_mask : lo_mask) >> isL) & 1;
         const int cls = fluid_class(v);
-        double* edge = a.edges->p[fluid_obj(v, isL ? kindL : kindR)][d][side];
-        fill_ghost(tl, base + arr * AS, GS + arr * 2 * tl.Wb, side ? +1 : -1, a.mode[cls][side], a.act[cls],
-                   v == 1 + d, edge, a.bc_inf);
+        double* edge = a.edges->p[fluid_obj(v, isL ? kindL : kindR)][tl.d][side];
+        halo_job(tl, base + arr * AS, an + (arr * 2 + side) * tl.Wb, side, shift, a.mode[cls][side], a.act[cls],
+                 v == 1 + tl.d, edge, a.bc_inf, 1);
     }
 }
 
@@ -179,18 +187,17 @@ template <typename T, bool MHD, int CPT>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
-    __shared__ double part[2][MAX_WARPS][32];   // per-warp column maxima (two freezing speeds)
-    __shared__ double cflp[3][MAX_WARPS];       // per-warp CFL maxima
+    __shared__ T part[2][MAX_WARPS][32];   // per-warp column maxima (two freezing speeds)
+    __shared__ double cflp[3][MAX_WARPS];  // per-warp CFL maxima
     Tile<T, CPT> tl;
     tl.init(a.sg);
     const int d = a.sg.d;
     const int NT = a.sg.NT;
-    const size_t AS = (size_t)tl.RC * tl.Wb;
+    const int Wb = tl.Wb;
+    const size_t AS = (size_t)tile_rows(tl.RC) * Wb;
     T* SA = reinterpret_cast<T*>(smem);   // set A: R[v] at SA + v*AS, L[v] at SA + (5+v)*AS
     T* SB = SA + 10 * AS;                 // set B
-    Ghost<T>* GS = reinterpret_cast<Ghost<T>*>(SA + 20 * AS);   // [array][side][column]
-    for (int i = threadIdx.x; i < 2 * MAX_WARPS * 32; i += blockDim.x) (&part[0][0][0])[i] = 0.0;
-    __syncthreads();
+    Ghost<T>* AN = reinterpret_cast<Ghost<T>*>(SA + 20 * AS);   // fade anchors [array][side][column]
 
     const double G = a.gamma;
     const double dt = a.tm->dt;
@@ -202,7 +209,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
     // ---- load u (rho, px, py, pz, E) and cell-centred B; freezing speed #1 (wFluidFlux.m:18-22) --
     T u[5][CPT], bb[3][CPT], press[CPT];
     double msq[CPT];
-    double lmax = 0.0;
+    T lmax = T(0);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const bool ok = tl.ok(k);
@@ -218,9 +225,9 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
         msq[k] = m;
         T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
         T spd = press_speed<T>(G, d, uu, m, press[k]);
-        if (ok) lmax = fmax(lmax, (double)spd);
+        if (ok) lmax = fmax(lmax, spd);
     }
-    const T cf = (T)column_max(tl, NT, part[0], lmax);
+    const T cf = column_max(tl, NT, part[0], lmax);
 
     // ---- predictor fluxes R = (u+w)/2, L = (u-w)/2 -> set A (relaxingFluid.m:30-31) ---------------
 #pragma unroll
@@ -247,11 +254,11 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
         }
     }
     tl.csync();
-    fluid_ghost_jobs(tl, a, SA, AS, GS, /*lower: R*/ 1, /*upper: L*/ 2, FO_STORE_R, FO_STORE_L);
+    fluid_halo_jobs(tl, a, SA, AS, AN, /*lower: R*/ 1, /*upper: L*/ 2, FO_STORE_R, FO_STORE_L);
     __syncthreads();
 
     // ---- predictor (relaxingFluid.m:32-39): half-step state -> set B; freezing speed #2 -----------
-    double lmax2 = 0.0;
+    T lmax2 = T(0);
     T press2[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
@@ -262,8 +269,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const int cls = fluid_class(v);
             const T* R = SA + v * AS;
             const T* L = SA + (5 + v) * AS;
-            const T Rm = shifted(tl, R, GS + v * 2 * tl.Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted(tl, L, GS + (5 + v) * 2 * tl.Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = shifted(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
             us[v] = u[v][k] - half_ffx * cf * (R[ix] - Rm + L[ix] - Lp);
         }
         us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
@@ -271,9 +278,9 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
 #pragma unroll
         for (int v = 0; v < 5; ++v) SB[v * AS + ix] = us[v];
         T spd = press_speed<T>(G, d, us, msq[k], press2[k]);   // relaxingFluid.m:47-50
-        if (tl.ok(k)) lmax2 = fmax(lmax2, (double)spd);
+        if (tl.ok(k)) lmax2 = fmax(lmax2, spd);
     }
-    const T cfs = (T)column_max(tl, NT, part[1], lmax2);   // its barrier also ends the predictor reads of set A
+    const T cfs = column_max(tl, NT, part[1], lmax2);   // its barrier also ends the predictor reads of set A
 
     // ---- corrector fluxes (relaxingFluid.m:52-56) from the half-step state -> set A --------------
 #pragma unroll
@@ -302,7 +309,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
         }
     }
     tl.csync();
-    fluid_ghost_jobs(tl, a, SA, AS, GS, 3, 3, FO_R, FO_L);
+    fluid_halo_jobs(tl, a, SA, AS, AN, 3, 3, FO_R, FO_L);
     __syncthreads();
 
     // ---- TVD limiter (relaxingFluid.m:57-62): corrected R and L -> set B --------------------------
@@ -314,20 +321,20 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const int cls = fluid_class(v);
             const T* R = SA + v * AS;
             const T* L = SA + (5 + v) * AS;
-            const Ghost<T>* gR = GS + v * 2 * tl.Wb;
-            const Ghost<T>* gL = GS + (5 + v) * 2 * tl.Wb;
+            const Ghost<T>* aR = AN + (2 * v) * Wb;
+            const Ghost<T>* aL = AN + (2 * (5 + v)) * Wb;
             const int mlo = a.mode[cls][0], mhi = a.mode[cls][1];
             const T r = R[ix], l = L[ix];
-            const T Rm = shifted(tl, R, gR, k, -1, mlo, fc, fw);
-            const T Rp = shifted(tl, R, gR, k, +1, mhi, fc, fw);
-            const T Lm = shifted(tl, L, gL, k, -1, mlo, fc, fw);
-            const T Lp = shifted(tl, L, gL, k, +1, mhi, fc, fw);
+            const T Rm = shifted(tl, R, aR, k, -1, mlo, fc, fw);
+            const T Rp = shifted(tl, R, aR + Wb, k, +1, mhi, fc, fw);
+            const T Lm = shifted(tl, L, aL, k, -1, mlo, fc, fw);
+            const T Lp = shifted(tl, L, aL + Wb, k, +1, mhi, fc, fw);
             SB[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
             SB[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
         }
     }
     tl.csync();
-    fluid_ghost_jobs(tl, a, SB, AS, GS, 1, 2, FO_R, FO_L);
+    fluid_halo_jobs(tl, a, SB, AS, AN, 1, 2, FO_R, FO_L);
     __syncthreads();
 
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
@@ -341,8 +348,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const int cls = fluid_class(v);
             const T* R = SB + v * AS;
             const T* L = SB + (5 + v) * AS;
-            const T Rm = shifted(tl, R, GS + v * 2 * tl.Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted(tl, L, GS + (5 + v) * 2 * tl.Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = shifted(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
             unew[v] = u[v][k] - ff * cfs * (R[ix] - Rm + L[ix] - Lp);
         }
         unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;

@@ -73,15 +73,15 @@ __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long ce
         case BC_MIRROR: { T v = upper ? at(Ne - 2) : at(1); return flip ? -v : v; }
         case BC_WALL: return (T)edge[fi];
         case BC_TRANS: {
-            T a0, a1, a2;
-            if (!upper) { a0 = at(trans_pick_lower(Ne, 1, 0)); a1 = at(trans_pick_lower(Ne, 1, 1)); a2 = at(0); }
-            else { a0 = at(trans_pick_upper(Ne, 1, 0)); a1 = at(trans_pick_upper(Ne, 1, 1)); a2 = at(Ne - 1); }
+            T a1, a2;
+            if (!upper) { a1 = at(trans_pick_lower(Ne, 1, 1)); a2 = at(0); }
+            else { a1 = at(trans_pick_upper(Ne, 1, 1)); a2 = at(Ne - 1); }
             double ev = 0.0;
             if (act) {
                 ev = edge_drift(edge[fi], (double)a2);
                 if (own_update) edge[fi] = ev;
             }
-            return (T)trans_ghost((double)a0, (double)a1, (double)a2, ev, bc_inf, 4.0, (double)a2);
+            return (T)trans_ghost((double)a1, (double)a2, ev, bc_inf, 4.0, (double)a2);
         }
         case BC_FADE: {
             T v = upper ? at(Ne - 1) : at(0);
@@ -95,23 +95,44 @@ __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long ce
 
 // ---- the X-chain ------------------------------------------------------------------------------------
 constexpr int MAG_NARR = 4;
-constexpr int MAG_NSLOT = 6;   // ghost slots per column: lower, upper +1 (x3), upper +2 (two rows)
+constexpr int MAG_NSLOT = 6;   // per column: lower anchors, upper +1 (e1), +1 (e2), +2 row N, +2 row N+1, +1 (e4)
 
-// Dynamic shared memory of the chain kernel: 4 arrays of RC*Wb values + 6 ghost slots per column.
+// Dynamic shared memory of the chain kernel: 4 halo'd arrays + 6 ghost/anchor slots per column.
 template <typename T>
 __host__ __device__ inline size_t mag_smem_bytes(int RC, int Wb) {
-    return sizeof(T) * (size_t)MAG_NARR * RC * Wb + sizeof(Ghost<T>) * MAG_NSLOT * (size_t)Wb;
+    return sizeof(T) * (size_t)MAG_NARR * tile_rows(RC) * Wb + sizeof(Ghost<T>) * MAG_NSLOT * (size_t)Wb;
 }
 
-// A.shift(X, +2) at row k, fade damping included: ghosts of rows N and N+1 in slots s3, s4 (the
-// anchors of the constant shift by 2 -- rows min(2, N-1) and N-1 -- ride in s3).
+// The four upper shift calls of wMag in relaxingMagnet.m:37-45 (+1, +1, +2, +1, in that order; a
+// trans edge drifts once per call): their ghosts from the successive edge states e1..e4 go to slots
+// 1, 2, (3, 4), 5, with the fade anchors of the +1 and +2 shifts.  Returns e4, the edge's new state.
 template <typename T, int CPT>
-__device__ __forceinline__ T shifted2(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* s3, const Ghost<T>* s4, int k,
-                                      int mode, const double* fc, int f) {
-    const T g2[2] = {s3[tl.b].g, s4[tl.b].g};
-    T v = tl.above2(A, g2, k);
-    if (mode == BC_FADE) v = fade_apply(v, tl.grow(k), tl.N, fc, f, s3[tl.b].s0, s3[tl.b].sN1);
-    return v;
+__device__ __forceinline__ double wmag_upper_ghosts(const Tile<T, CPT>& tl, const T* A, Ghost<T>* GS, int mode,
+                                                    int act, double* eh, double binf) {
+    const int N = tl.N, Wb = tl.Wb, b = tl.b;
+    const bool stateful = (mode == BC_TRANS || mode == BC_WALL) && eh != nullptr;
+    const bool drift = mode == BC_TRANS && act && eh != nullptr;
+    const double s0 = stateful ? eh[tl.col] : 0.0;
+    const double cur = (double)tl.row(A, N - 1);
+    const double e1 = drift ? edge_drift(s0, cur) : s0;
+    const double e2 = drift ? edge_drift(e1, cur) : s0;
+    const double e3 = drift ? edge_drift(e2, cur) : s0;
+    const double e4 = drift ? edge_drift(e3, cur) : s0;
+    Ghost<T> u = fade_anchors(tl, A, +1);
+    u.g = bc_ghost(tl, A, +1, 1, mode, act, 0, eh, binf, e1);
+    GS[1 * Wb + b] = u;
+    u.g = bc_ghost(tl, A, +1, 1, mode, act, 0, eh, binf, e2);
+    GS[2 * Wb + b] = u;
+    u.g = bc_ghost(tl, A, +1, 1, mode, act, 0, eh, binf, e4);
+    GS[5 * Wb + b] = u;
+    Ghost<T> w2;
+    w2.s0 = tl.row(A, N > 2 ? 2 : N - 1);
+    w2.sN1 = tl.row(A, N - 1);
+    w2.g = bc_ghost(tl, A, +2, 1, mode, act, 0, eh, binf, e3);
+    GS[3 * Wb + b] = w2;
+    w2.g = bc_ghost(tl, A, +2, 2, mode, act, 0, eh, binf, e3);
+    GS[4 * Wb + b] = w2;
+    return e4;
 }
 
 template <typename T, int CPT>
@@ -135,24 +156,26 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
     const T ff = (T)(0.5 * dt / a.dx);
     const T ff2 = T(2) * ff;
     const EdgeTable* et = a.edges;
-    const size_t AS = (size_t)tl.RC * Wb;
+    const size_t AS = (size_t)tile_rows(tl.RC) * Wb;
     T* S0 = reinterpret_cast<T*>(smem);
     T* S1 = S0 + AS;
     T* S2 = S1 + AS;
     T* S3 = S2 + AS;
     Ghost<T>* GS = reinterpret_cast<Ghost<T>*>(S0 + MAG_NARR * AS);   // [slot][column]
-    // upper slot s is read by shifted(.., +1) through GS + (s-1)*Wb (it reads gs[Wb + b])
-    const Ghost<T>* GL = GS;
+    Ghost<T>* const ANL = GS;            // lower-side fade anchors
+    Ghost<T>* const ANU = GS + Wb;       // upper-side fade anchors (+1 shifts of stages 2-4)
     const double* fc = a.fade;
     const int f = a.fade_f;
     const double binf = a.bc_inf;
     const int mlo = a.modeX[0], mhi = a.modeX[1];
     // the scratch objects of mag(I) for this sweep (mag-class BC along X, no mirror flip)
     auto edge_of = [&](int kind, int side) -> double* { return et->p[mag_obj(c, d, kind)][d][side]; };
-    // ghost job helpers: lower ghosts on cluster rank 0 (thread g == 0 of the column), upper ghosts
-    // on the rank holding row N-1 (thread g == 1, or 0 when the column has one thread)
-    const bool job_lo = tl.colok && tl.rank == 0 && tl.g == 0;
-    const bool job_hi = tl.colok && tl.rank == tl.rank_hi() && tl.g == (tl.G > 1 ? 1 : 0);
+    // halo jobs: thread g == 0 of a column does the lower side, thread g == 1 the upper side
+    const int job_side = tl.colok && tl.g < 2 ? tl.g : -1;
+    auto halo = [&](T* A, int kind, bool lo_shift, bool hi_shift, int hi_rows) {
+        if (job_side == 0) halo_job(tl, A, ANL, 0, lo_shift, mlo, a.actX, 0, edge_of(kind, 0), binf, hi_rows);
+        if (job_side == 1) halo_job(tl, A, ANU, 1, hi_shift, mhi, a.actX, 0, edge_of(kind, 1), binf, hi_rows);
+    };
 
     // ---- corner velocity (magnetFlux.m:18-19): transverse average with mass/mom BCs along I ------
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
@@ -185,26 +208,25 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
         S0[tl.idx(k)] = vgr[k];
     }
     tl.csync();
-    if (job_lo) fill_ghost(tl, S0, GS, -1, mlo, a.actX, 0, edge_of(MO_VELGRID, 0), binf);
-    if (job_hi) fill_ghost(tl, S0, GS, +1, mhi, a.actX, 0, edge_of(MO_VELGRID, 1), binf);
+    halo(S0, MO_VELGRID, true, true, 1);
     __syncthreads();
     // vg = 0.25*(vg.shift(X,-1) + vg.shift(X,1) + 2*vg)   (magnetFlux.m:21-23)
     T vg[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T m1 = shifted(tl, (const T*)S0, GL, k, -1, mlo, fc, f);
-        const T p1 = shifted(tl, (const T*)S0, GS, k, +1, mhi, fc, f);
+        const T m1 = shifted(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
+        const T p1 = shifted(tl, (const T*)S0, ANU, k, +1, mhi, fc, f);
         vg[k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[k]) : T(0);
         S1[tl.idx(k)] = vg[k];
     }
     tl.csync();
-    if (job_hi) fill_ghost(tl, S1, GS, +1, mhi, a.actX, 0, edge_of(MO_VELGRID, 1), binf);
+    halo(S1, MO_VELGRID, false, true, 1);
     __syncthreads();
     // velocityFlow = (vg + vg.shift(X,1)) < 0; store.fluxR = B_I.*vg   (relaxingMagnet.m:17,22)
     T vf[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T p1 = shifted(tl, (const T*)S1, GS, k, +1, mhi, fc, f);
+        const T p1 = shifted(tl, (const T*)S1, ANU, k, +1, mhi, fc, f);
         vf[k] = (vg[k] + p1) < T(0) ? T(1) : T(0);
         const T F = bI[k] * vg[k];
         S2[tl.idx(k)] = F;
@@ -215,24 +237,24 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
         }
     }
     tl.csync();
-    if (job_hi) fill_ghost(tl, S2, GS, +1, mhi, a.actX, 0, edge_of(MO_STORE_R, 1), binf);
+    halo(S2, MO_STORE_R, false, true, 1);
     __syncthreads();
     // store.fluxR = F.*(1-vf) + F.shift(X,1).*vf   (relaxingMagnet.m:23-24)
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T F = S2[tl.idx(k)];
-        const T Fp = shifted(tl, (const T*)S2, GS, k, +1, mhi, fc, f);
+        const T Fp = shifted(tl, (const T*)S2, ANU, k, +1, mhi, fc, f);
         S3[tl.idx(k)] = F * (T(1) - vf[k]) + Fp * vf[k];
     }
     tl.csync();
-    if (job_lo) fill_ghost(tl, S3, GS, -1, mlo, a.actX, 0, edge_of(MO_STORE_R, 0), binf);
+    halo(S3, MO_STORE_R, true, false, 1);
     __syncthreads();
     // store = B_I - ff*(fluxR - fluxR.shift(X,-1)); wMag = store.*velGrid   (relaxingMagnet.m:26-33)
     T W[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T Fu = S3[tl.idx(k)];
-        const T st = bI[k] - ff * (Fu - shifted(tl, (const T*)S3, GL, k, -1, mlo, fc, f));
+        const T st = bI[k] - ff * (Fu - shifted(tl, (const T*)S3, ANL, k, -1, mlo, fc, f));
         W[k] = st * vg[k];
         S0[tl.idx(k)] = W[k];
         if (init_mag && tl.ok(k)) {
@@ -242,50 +264,54 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
         }
     }
     tl.csync();
-    // wMag is shifted +1, +1, +2, +1 (upper edge drifts four times, in that order) and -1: one job
-    // computes the four upper ghosts from the successive edge states and stores the last state.
-    if (job_lo) fill_ghost(tl, S0, GS, -1, mlo, a.actX, 0, edge_of(MO_WMAG, 0), binf);
-    if (job_hi) {
-        double* eh = edge_of(MO_WMAG, 1);
-        const bool stateful = (mhi == BC_TRANS || mhi == BC_WALL) && eh != nullptr;
-        const bool drift = mhi == BC_TRANS && a.actX && eh != nullptr;
-        const double s0 = stateful ? eh[tl.col] : 0.0;
-        const double cur = (double)tl.row((const T*)S0, N - 1);
-        const double e1 = drift ? edge_drift(s0, cur) : s0;
-        const double e2 = drift ? edge_drift(e1, cur) : s0;
-        const double e3 = drift ? edge_drift(e2, cur) : s0;
-        const double e4 = drift ? edge_drift(e3, cur) : s0;
-        Ghost<T> u;
-        u.s0 = tl.row((const T*)S0, N > 1 ? 1 : 0);
-        u.sN1 = tl.row((const T*)S0, N - 1);
-        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e1);
-        GS[1 * Wb + b] = u;
-        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e2);
-        GS[2 * Wb + b] = u;
-        u.g = bc_ghost(tl, (const T*)S0, +1, 1, mhi, a.actX, 0, eh, binf, e4);
-        GS[5 * Wb + b] = u;
+    // wMag: one lower shift (an ordinary halo job; the upper side only copies the next rank's two
+    // rows) and four upper shift calls whose ghosts differ, kept in slots by every rank that owns
+    // row N-1 or N-2.  The edge's new state is stored after the next cluster barrier, once every
+    // rank has read the old one.
+    double e4 = 0.0;
+    halo(S0, MO_WMAG, true, false, 2);
+    const bool own_end = tl.rank == tl.rank_hi || (tl.rank + 1 == tl.rank_hi && tl.N - 1 == tl.rank_hi * tl.RC);
+    if (job_side == 1 && own_end) e4 = wmag_upper_ghosts(tl, (const T*)S0, GS, mhi, a.actX, edge_of(MO_WMAG, 1), binf);
+    else if (job_side == 1 && mhi == BC_FADE) {   // fade anchors of the +1 and +2 shifts on the other ranks
+        GS[1 * Wb + b] = GS[2 * Wb + b] = GS[5 * Wb + b] = fade_anchors(tl, (const T*)S0, +1);
         Ghost<T> w2;
+        w2.g = T(0);
         w2.s0 = tl.row((const T*)S0, N > 2 ? 2 : N - 1);
         w2.sN1 = tl.row((const T*)S0, N - 1);
-        w2.g = bc_ghost(tl, (const T*)S0, +2, 1, mhi, a.actX, 0, eh, binf, e3);
         GS[3 * Wb + b] = w2;
-        w2.g = bc_ghost(tl, (const T*)S0, +2, 2, mhi, a.actX, 0, eh, binf, e3);
-        GS[4 * Wb + b] = w2;
-        if (drift) eh[tl.col] = e4;
     }
     __syncthreads();
     T Fl[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T w = W[k], v = vf[k];
-        const T* A = S0;
-        const T fx = w * (T(1) - v) + shifted(tl, A, GS + 0 * Wb, k, +1, mhi, fc, f) * v;
-        const T dFluxR = shifted(tl, A, GS + 1 * Wb, k, +1, mhi, fc, f) -
-                         (v * shifted2(tl, A, GS + 3 * Wb, GS + 4 * Wb, k, mhi, fc, f) + (T(1) - v) * w);
-        const T dFluxL = w - (v * shifted(tl, A, GS + 4 * Wb, k, +1, mhi, fc, f) +
-                              (T(1) - v) * shifted(tl, A, GL, k, -1, mlo, fc, f));
+        const int ix = tl.idx(k);
+        const int r = tl.grow(k);
+        T p1a = S0[ix + Wb], p1b = p1a, p1d = p1a, p2 = S0[ix + 2 * Wb];
+        if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
+            if (r == N - 1) {
+                p1a = GS[1 * Wb + b].g;
+                p1b = GS[2 * Wb + b].g;
+                p1d = GS[5 * Wb + b].g;
+                p2 = GS[4 * Wb + b].g;
+            } else {
+                p2 = GS[3 * Wb + b].g;
+            }
+        }
+        if (mhi == BC_FADE) {
+            const Ghost<T>& u1 = GS[1 * Wb + b];
+            const Ghost<T>& u2 = GS[3 * Wb + b];
+            p1a = fade_apply(p1a, r, N, fc, f, u1.s0, u1.sN1);
+            p1b = fade_apply(p1b, r, N, fc, f, u1.s0, u1.sN1);
+            p1d = fade_apply(p1d, r, N, fc, f, u1.s0, u1.sN1);
+            p2 = fade_apply(p2, r, N, fc, f, u2.s0, u2.sN1);
+        }
+        const T m1 = shifted(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
+        const T fx = w * (T(1) - v) + p1a * v;
+        const T dFluxR = p1b - (v * p2 + (T(1) - v) * w);
+        const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
         Fl[k] = fx + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
-        S1[tl.idx(k)] = Fl[k];
+        S1[ix] = Fl[k];
         if (init_mag && tl.ok(k)) {
             int x, y, z;
             tl.coords(k, x, y, z);
@@ -293,13 +319,17 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
         }
     }
     tl.csync();
-    if (job_lo) fill_ghost(tl, S1, GS, -1, mlo, a.actX, 0, edge_of(MO_FLUX, 0), binf);
+    if (job_side == 1 && tl.rank == tl.rank_hi && mhi == BC_TRANS && a.actX) {
+        double* eh = edge_of(MO_WMAG, 1);
+        if (eh) eh[tl.col] = e4;
+    }
+    halo(S1, MO_FLUX, true, false, 1);
     __syncthreads();
     // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49); F_I -> scratch for CT
     T* Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T fm = shifted(tl, (const T*)S1, GL, k, -1, mlo, fc, f);
+        const T fm = shifted(tl, (const T*)S1, ANL, k, -1, mlo, fc, f);
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
         BI[o] = bI[k] - ff2 * (Fl[k] - fm);

@@ -1,16 +1,16 @@
 // Pencil tiles shared by the sweep kernels.
 //
 // A pencil is one line of cells along the sweep dimension d.  A CTA holds a bundle of Wb pencils
-// ("columns") and G rows of each (one cell per thread); a thread-block cluster of CL CTAs covers
-// pencils longer than G (rank r holds rows [r*G, (r+1)*G)), so every pencil stays on chip whatever
-// its length.  Thread (b, g) owns row g of column b; consecutive threads touch consecutive cells,
+// ("columns") and RC = G*CPT rows of each (thread (b, g) owns rows g, g+G, ... of column b); a
+// thread-block cluster of CL CTAs covers pencils longer than RC (rank r holds rows [r*RC, (r+1)*RC)),
+// so every pencil stays on chip whatever its length.  Consecutive threads touch consecutive cells,
 // so global loads/stores are coalesced along x for every sweep direction.
 //
-// Stencil operands live in shared-memory arrays A[row][b] (one per flux array).  A neighbour read
-// is one shared load; the row across a CTA boundary is read from the neighbouring cluster rank
-// through DSMEM; the rows beyond the pencil ends are boundary-condition ghosts that a few threads
-// compute once per stage into ghost slots (shifting/*_shift.m), including the drift of stateful
-// edges.  Boundary predicates are per-thread constants, so the common path has no extra work.
+// Stencil operands live in shared-memory arrays with HALO rows: local row 0 is the row below the
+// CTA's first row, local rows RC+1 and RC+2 the two rows above its last row.  Between stages a few
+// threads fill the halos -- the neighbouring cluster rank's edge rows (read through DSMEM), or, at
+// the pencil ends, the boundary-condition ghost of the reference's shift (shifting/*_shift.m),
+// stateful edge drift included -- so every stencil read is one unconditional shared load.
 #pragma once
 
 #include "common.cuh"
@@ -25,13 +25,19 @@ struct SweepGeom {
     int N;            // pencil length g.n[d]
     long long ncol;   // number of pencils = ncell / N
     int Wb;           // pencils per CTA
-    int G;            // rows (threads) per pencil per CTA
+    int G;            // threads per pencil per CTA
     int CL;           // CTAs per cluster along the pencil
     int NT;           // threads per CTA = Wb * G
 };
 
-// Ghost slot of one (array, side, column): the ghost value beyond the pencil end and the two fade
-// anchors (constant-shifted values at rows 0 and N-1 before damping).
+constexpr int HALO_LO = 1;   // halo rows below the CTA's rows
+constexpr int HALO_HI = 2;   // halo rows above (two: the magnet's shift by +2)
+
+// Rows of one shared array (own rows plus halos).
+__host__ __device__ inline int tile_rows(int RC) { return RC + HALO_LO + HALO_HI; }
+
+// Fade anchors of one (array, side): the constant-shifted values at rows 0 and N-1 (fade_shift.m
+// damps toward them); `g` holds a ghost value where a stage needs more than one per side.
 template <typename T>
 struct Ghost {
     T g, s0, sN1;
@@ -39,13 +45,12 @@ struct Ghost {
 
 template <typename T, int CPT>
 struct Tile {
-    int b, g, rank, N, Wb, G, CL, d, RC;
+    int b, g, rank, N, Wb, G, CL, d, RC, rank_hi;
     long long col;        // global pencil index
     bool colok;
     long long base;       // linear offset of row 0 of this pencil
     long long sd;         // stride along the sweep
     int coord1, coord2;
-    // rows owned by this thread: local row g + k*G, global row rank*RC + g + k*G
 
     __device__ __forceinline__ void init(const SweepGeom& s) {
         const int t = threadIdx.x;
@@ -59,6 +64,7 @@ struct Tile {
         CL = s.CL;
         d = s.d;
         RC = G * CPT;
+        rank_hi = (N - 1) / RC;
         col = bundle * s.Wb + b;
         colok = col < s.ncol;
         long long c = colok ? col : 0;
@@ -68,11 +74,12 @@ struct Tile {
                (long long)coord2 * sel3(s.d2, s.g.s[0], s.g.s[1], s.g.s[2]);
         sd = sel3(s.d, s.g.s[0], s.g.s[1], s.g.s[2]);
     }
-    __device__ __forceinline__ int lrow(int k) const { return g + k * G; }
     __device__ __forceinline__ int grow(int k) const { return rank * RC + g + k * G; }
     __device__ __forceinline__ bool ok(int k) const { return colok && grow(k) < N; }
     __device__ __forceinline__ long long off(int k) const { return base + (long long)grow(k) * sd; }
-    __device__ __forceinline__ int idx(int k) const { return lrow(k) * Wb + b; }
+    // shared index of own row k, and of local row l (0 = lower halo)
+    __device__ __forceinline__ int idx(int k) const { return (g + k * G + HALO_LO) * Wb + b; }
+    __device__ __forceinline__ int lidx(int l) const { return l * Wb + b; }
     __device__ __forceinline__ void coords(int k, int& x, int& y, int& z) const {
         int r = grow(k);
         if (d == 0) { x = r; y = coord1; z = coord2; }
@@ -88,38 +95,15 @@ struct Tile {
         if (CL == 1 || r == rank) return p;
         return cg::this_cluster().map_shared_rank(p, r);
     }
-    // Value of array A at global row r of this column (any cluster rank).
+    // Value of array A at global row r (0 <= r < N) of this column, on any cluster rank.
     template <typename U>
     __device__ __forceinline__ U row(const U* A, int r) const {
         int rk = r / RC;
         const U* p = remote(const_cast<U*>(A), rk);
-        return p[(r - rk * RC) * Wb + b];
+        return p[(r - rk * RC + HALO_LO) * Wb + b];
     }
-    // A.shift(d, -1) and A.shift(d, +1) at row k before fade damping (gs: the array's ghost slots,
-    // [side][column]).  The rare cases (pencil end, other cluster rank) are per-row constants.
-    template <typename U>
-    __device__ __forceinline__ U below(const U* A, const Ghost<U>* gs, int k) const {
-        if (grow(k) == 0) return gs[b].g;
-        if (lrow(k) == 0) return remote(const_cast<U*>(A), rank - 1)[(RC - 1) * Wb + b];
-        return A[idx(k) - Wb];
-    }
-    template <typename U>
-    __device__ __forceinline__ U above(const U* A, const Ghost<U>* gs, int k) const {
-        if (grow(k) >= N - 1) return gs[Wb + b].g;   // also rows past the pencil end (idle cells)
-        if (lrow(k) == RC - 1) return remote(const_cast<U*>(A), rank + 1)[b];
-        return A[idx(k) + Wb];
-    }
-    // A.shift(d, +2) at row k before fade damping; ghosts at rows N and N+1 in g2[0], g2[1].
-    template <typename U>
-    __device__ __forceinline__ U above2(const U* A, const U g2[2], int k) const {
-        const int r = grow(k) + 2;
-        if (r >= N) return r == N ? g2[0] : g2[1];
-        const int lr = lrow(k) + 2;
-        if (lr >= RC) return remote(const_cast<U*>(A), rank + 1)[(lr - RC) * Wb + b];
-        return A[idx(k) + 2 * Wb];
-    }
-    // Cluster rank that holds the pencil's last row (where its upper ghosts are consumed).
-    __device__ __forceinline__ int rank_hi() const { return (N - 1) / RC; }
+    // Local shared index of global row r (r may be N or N+1 on rank_hi: an idle row or a halo row).
+    __device__ __forceinline__ int ridx(int r) const { return (r - rank * RC + HALO_LO) * Wb + b; }
 };
 
 // Fade damping of fade_shift.m:31-44 applied to the constant-shifted value sv at row r of a line of
@@ -137,13 +121,14 @@ __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, in
     return lf;
 }
 
-// A.shift(d, n) at row k for n = -1 / +1, fade damping included.
+// A.shift(d, n) at own row k for n = -1 / +1 (one shared load), fade damping included.  `an` is the
+// array's anchor pair for that side (read only under fade, a uniform branch).
 template <typename T, int CPT>
-__device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* gs, int k, int n, int mode,
+__device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* an, int k, int n, int mode,
                                      const double* fc, int f) {
-    T v = n < 0 ? tl.below(A, gs, k) : tl.above(A, gs, k);
+    T v = A[tl.idx(k) + n * tl.Wb];
     if (mode == BC_FADE) {
-        const Ghost<T>& q = gs[(n < 0 ? 0 : tl.Wb) + tl.b];
+        const Ghost<T>& q = an[tl.b];
         v = fade_apply(v, tl.grow(k), tl.N, fc, f, q.s0, q.sN1);
     }
     return v;
@@ -151,6 +136,38 @@ __device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const G
 
 // "No stored-edge value supplied" marker (stored edges are finite physical values).
 constexpr double NO_EV = -1.0e300;
+
+// Transparent ghost of one shift call (shifting/transparent_shift.m:23-99), out of line: it runs
+// for a few threads per stage only, and keeping its FP64 interpolation out of the stencil code keeps
+// the register allocation of the sweep kernels at the stencil's needs.
+template <typename T, int CPT>
+__device__ __noinline__ double trans_bc_ghost(const Tile<T, CPT> tl, const T* A, int n, int mp, int act, double* edge,
+                                              double bc_inf, double ev) {
+    const int N = tl.N;
+    const bool upper = n > 0;
+    const int m = n < 0 ? -n : n;
+    double y1, y2, cur;
+    if (upper) {
+        y1 = (double)tl.row(A, trans_pick_upper(N, m, 1));
+        y2 = (double)tl.row(A, trans_pick_upper(N, m, 2));
+        cur = (double)tl.row(A, N - 1);
+    } else {
+        y1 = (double)tl.row(A, trans_pick_lower(N, m, 1));
+        y2 = (double)tl.row(A, trans_pick_lower(N, m, 2));
+        cur = (double)tl.row(A, 0);
+    }
+    double e = 0.0;
+    if (act) {
+        if (ev != NO_EV) e = ev;
+        else {
+            e = edge_drift(edge[tl.col], cur);
+            edge[tl.col] = e;
+        }
+    }
+    // the 1e-4 keep test compares with the unshifted array at the ghost's position
+    const int gpos = upper ? N - 1 - (m - mp) : 0;
+    return trans_ghost(y1, y2, e, bc_inf, 3.0 + mp, (double)tl.row(A, gpos));
+}
 
 // Ghost of array A beyond the pencil end for one shift call A.shift(d, n): n = -1 (row -1),
 // n = +1 (row N) or n = +2 (rows N and N+1, mp = 1 or 2 selects which).  Stateful edges (trans,
@@ -161,7 +178,6 @@ __device__ __forceinline__ T bc_ghost(const Tile<T, CPT>& tl, const T* A, int n,
                                       double* edge, double bc_inf, double ev) {
     const int N = tl.N;
     const bool upper = n > 0;
-    const int m = n < 0 ? -n : n;
     switch (mode) {
         case BC_CIRC: return upper ? tl.row(A, mp - 1) : tl.row(A, N - 1);
         case BC_MIRROR: {
@@ -169,46 +185,47 @@ __device__ __forceinline__ T bc_ghost(const Tile<T, CPT>& tl, const T* A, int n,
             return flip ? -x : x;
         }
         case BC_WALL: return (T)(ev != NO_EV ? ev : edge[tl.col]);
-        case BC_TRANS: {
-            double y0, y1, y2, cur;
-            if (upper) {
-                y0 = (double)tl.row(A, trans_pick_upper(N, m, 0));
-                y1 = (double)tl.row(A, trans_pick_upper(N, m, 1));
-                y2 = (double)tl.row(A, trans_pick_upper(N, m, 2));
-                cur = (double)tl.row(A, N - 1);
-            } else {
-                y0 = (double)tl.row(A, trans_pick_lower(N, m, 0));
-                y1 = (double)tl.row(A, trans_pick_lower(N, m, 1));
-                y2 = (double)tl.row(A, trans_pick_lower(N, m, 2));
-                cur = (double)tl.row(A, 0);
-            }
-            double e = 0.0;
-            if (act) {
-                if (ev != NO_EV) e = ev;
-                else {
-                    e = edge_drift(edge[tl.col], cur);
-                    edge[tl.col] = e;
-                }
-            }
-            // the 1e-4 keep test compares with the unshifted array at the ghost's position
-            const int gpos = upper ? N - 1 - (m - mp) : 0;
-            return (T)trans_ghost(y0, y1, y2, e, bc_inf, 3.0 + mp, (double)tl.row(A, gpos));
-        }
+        case BC_TRANS: return (T)trans_bc_ghost<T, CPT>(tl, A, n, mp, act, edge, bc_inf, ev);
         default: return upper ? tl.row(A, N - 1) : tl.row(A, 0);   // const and fade: constant shift
     }
 }
 
-// Fill the ghost slot of array A for one side (n = -1 or +1) of this thread's column: ghost value
-// and fade anchors.  Called by exactly one thread per (array, side, column) and stage.
+// Fade anchors of A for a shift by n = -1 or +1 (constant-shifted rows 0 and N-1).
 template <typename T, int CPT>
-__device__ __forceinline__ void fill_ghost(const Tile<T, CPT>& tl, const T* A, Ghost<T>* gs, int n, int mode, int act,
-                                           int flip, double* edge, double bc_inf) {
-    Ghost<T> q;
-    q.g = bc_ghost(tl, A, n, 1, mode, act, flip, edge, bc_inf, NO_EV);
+__device__ __forceinline__ Ghost<T> fade_anchors(const Tile<T, CPT>& tl, const T* A, int n) {
     const int N = tl.N;
+    Ghost<T> q;
+    q.g = T(0);
     if (n < 0) { q.s0 = tl.row(A, 0); q.sN1 = tl.row(A, N - 2 < 0 ? 0 : N - 2); }
     else { q.s0 = tl.row(A, N > 1 ? 1 : 0); q.sN1 = tl.row(A, N - 1); }
-    gs[(n < 0 ? 0 : tl.Wb) + tl.b] = q;
+    return q;
+}
+
+// Halo job for one (array, side) of this thread's column.  At the pencil end (rank 0 below, the
+// rank holding row N-1 above) it writes the boundary ghost of one shift call -- only when `shift`
+// says the reference shifts that side in the coming stage, since a trans edge drifts once per call;
+// elsewhere it copies the neighbouring rank's edge rows (`hi_rows` of them above).  Under fade every
+// rank keeps the side's anchors (the damping reaches up to bc_infinity rows from each end).  Called
+// by exactly one thread per (array, side, column) and stage, after a cluster barrier; the values it
+// writes are read by its own CTA only.
+template <typename T, int CPT>
+__device__ __forceinline__ void halo_job(const Tile<T, CPT>& tl, T* A, Ghost<T>* an, int side, bool shift, int mode,
+                                         int act, int flip, double* edge, double bc_inf, int hi_rows) {
+    if (shift && mode == BC_FADE) an[tl.b] = fade_anchors(tl, (const T*)A, side ? +1 : -1);
+    if (side == 0) {
+        if (tl.rank == 0) {
+            if (shift) A[tl.lidx(0)] = bc_ghost(tl, (const T*)A, -1, 1, mode, act, flip, edge, bc_inf, NO_EV);
+        } else {
+            A[tl.lidx(0)] = tl.remote(A, tl.rank - 1)[tl.lidx(tl.RC)];
+        }
+    } else {
+        if (tl.rank == tl.rank_hi) {
+            if (shift) A[tl.ridx(tl.N)] = bc_ghost(tl, (const T*)A, +1, 1, mode, act, flip, edge, bc_inf, NO_EV);
+        } else if (tl.rank < tl.rank_hi) {
+            const T* up = tl.remote(A, tl.rank + 1);
+            for (int h = 1; h <= hi_rows; ++h) A[tl.lidx(tl.RC + h)] = up[tl.lidx(h)];
+        }
+    }
 }
 
 }  // namespace img

@@ -131,3 +131,42 @@ def oracle_kwargs(settings):
                 limiter=lim, fluid_active=s.get("fluid", True), magnet_active=s.get("magnet", False),
                 time_max=s.get("time_max", 1e5), iter_max=s.get("iter_max", 10),
                 update_mode=s.get("update_mode", 1))
+
+
+WORKLOADS = {
+    "ot512": lambda: orszag_tang(512),
+    "ot64": lambda: orszag_tang(64),
+    "kh256": lambda: kelvin_helmholtz(256),
+    "kh128": lambda: kelvin_helmholtz(128),
+    "sod": lambda: sod(4096),
+}
+
+
+def main(argv=None):
+    """Run a workload for a few iterations on the current CUDA device (e.g. under a profiler):
+    python -m imogen_b200.problems ot512 --precision mixed --iters 3"""
+    import argparse
+    import time
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("workload", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--iters", type=int, default=3)
+    a = ap.parse_args(argv)
+    from imogen_b200 import ImogenRun
+
+    s, st = WORKLOADS[a.workload]()
+    run = ImogenRun(precision=a.precision, **dict(s, iter_max=10 ** 7, time_max=1e5))
+    run.set_state(*st)
+    t0 = time.perf_counter()
+    for _ in range(a.iters):
+        run.iterate()
+    run.sync()
+    el = time.perf_counter() - t0
+    tot = run.totals()
+    run.close()
+    print(f"{a.workload} {a.precision}: {a.iters} iterations in {el * 1e3:.2f} ms, mass {tot[0]:.12e}")
+
+
+if __name__ == "__main__":
+    main()
