@@ -193,4 +193,30 @@ __global__ void totals_finalize_kernel(const double* partial, int nblocks, doubl
     out[v] = S + C;
 }
 
+// Host-transfer conversions of the mixed form (FP64 staging <-> FP32 state), 4 values per thread
+// where the array's 16-byte alignment allows (arrays start 256-byte aligned).
+__global__ void f64_to_f32_kernel(const double* __restrict__ src, float* __restrict__ dst, long long n) {
+    const long long n4 = n / 4;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        const double2 a = reinterpret_cast<const double2*>(src)[2 * i];
+        const double2 b = reinterpret_cast<const double2*>(src)[2 * i + 1];
+        reinterpret_cast<float4*>(dst)[i] = make_float4((float)a.x, (float)a.y, (float)b.x, (float)b.y);
+    }
+    for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+
+__global__ void f32_to_f64_kernel(const float* __restrict__ src, double* __restrict__ dst, long long n) {
+    const long long n4 = n / 4;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4; i += (long long)gridDim.x * blockDim.x) {
+        const float4 a = reinterpret_cast<const float4*>(src)[i];
+        reinterpret_cast<double2*>(dst)[2 * i] = make_double2(a.x, a.y);
+        reinterpret_cast<double2*>(dst)[2 * i + 1] = make_double2(a.z, a.w);
+    }
+    for (long long i = 4 * n4 + blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
+
 }  // namespace img

@@ -53,12 +53,13 @@ struct img_ctx {
     void* slab = nullptr;       // one allocation: state, scratch, edges, tables
     size_t slab_bytes = 0;
     void* q[NQ] = {};
-    void* scratch[5] = {};      // F0, F1, C0, C1, BXn
+    void* scratch[3] = {};      // F0, F1, BXn
     DevTime* tm = nullptr;
     EdgeTable* edges_dev = nullptr;
     EdgeTable edges_host{};
     double* fade_dev = nullptr;
     double* partial = nullptr;  // totals partials
+    double* stage = nullptr;    // mixed form: FP64 staging buffer of one array for host transfers
     std::vector<double> fade_host;
     int use_b[3] = {1, 1, 1};
     int mhd = 0;
@@ -284,9 +285,7 @@ void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.F[0] = ctx->scratch[0];
     a.F[1] = ctx->scratch[1];
-    a.C[0] = ctx->scratch[2];
-    a.C[1] = ctx->scratch[3];
-    a.BXn = ctx->scratch[4];
+    a.BXn = ctx->scratch[2];
     a.tm = ctx->tm;
     a.X = X;
     a.I[0] = I1;
@@ -343,15 +342,11 @@ int launch_magnet_cpt(img_ctx* ctx, int X, int I1, int I2) {
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
                     lc.gridDim.x, lc.blockDim.x, lc.dynamicSmemBytes, pcf.CL, cudaGetErrorString(le));
     long long n = ctx->g.ncell;
-    mag_ct1_kernel<T><<<launch_blocks(2 * n), 256, 0, ctx->stream>>>(a);
-    CK(cudaGetLastError());
-    mag_ct2_kernel<T><<<launch_blocks(2 * n), 256, 0, ctx->stream>>>(a);
-    CK(cudaGetLastError());
-    mag_bx_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
+    mag_ct_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
     mag_cell_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
-    ctx->launches += 5;
+    ctx->launches += 3;
     ctx->init_mag[I1 - 1][d] = false;
     ctx->init_mag[I2 - 1][d] = false;
     return IMG_OK;
@@ -539,7 +534,7 @@ int validate(const img_config& c, std::string& why) {
 
 // Device bytes: state + scratch + edges + tables.
 struct Layout {
-    size_t state, scratch, tm, table, fade, partial, edges, total;
+    size_t state, scratch, tm, table, fade, partial, stage, edges, total;
     size_t edge_off[NOBJ][3][2];
 };
 
@@ -549,11 +544,12 @@ Layout plan(const img_config& c) {
     long long n = (long long)c.grid[0] * c.grid[1] * c.grid[2];
     size_t arr = align256(n * elem);
     L.state = arr * NQ;
-    L.scratch = c.magnet_active ? arr * 5 : 0;
+    L.scratch = c.magnet_active ? arr * 3 : 0;
     L.tm = align256(sizeof(DevTime));
     L.table = align256(sizeof(EdgeTable));
     L.fade = align256(sizeof(double) * std::max(1, c.bc_infinity));
     L.partial = align256(sizeof(double) * 2 * 8 * 1024);
+    L.stage = elem == 4 ? align256(n * sizeof(double)) : 0;   // FP64 staging of host transfers (mixed)
     int ndims = c.grid[2] > 1 ? 3 : 2;
     size_t off = 0;
     for (int o = 0; o < NOBJ; ++o)
@@ -566,13 +562,8 @@ Layout plan(const img_config& c) {
                 off += align256(sizeof(double) * (n / c.grid[e]));
             }
     L.edges = off;
-    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.edges;
+    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.edges;
     return L;
-}
-
-template <typename T>
-void to_dev_type(const double* src, T* dst, long long n) {
-    for (long long i = 0; i < n; ++i) dst[i] = (T)src[i];
 }
 
 // Face of a host FP64 array along dim e at index idx (column-major order of the other dims).
@@ -674,7 +665,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     for (int v = 0; v < NQ; ++v) ctx->q[v] = p + v * arr;
     p += L.state;
     if (cfg->magnet_active)
-        for (int k = 0; k < 5; ++k) ctx->scratch[k] = p + k * arr;
+        for (int k = 0; k < 3; ++k) ctx->scratch[k] = p + k * arr;
     p += L.scratch;
     ctx->tm = reinterpret_cast<DevTime*>(p);
     p += L.tm;
@@ -684,6 +675,8 @@ int img_create(img_ctx** out, const img_config* cfg) {
     p += L.fade;
     ctx->partial = reinterpret_cast<double*>(p);
     p += L.partial;
+    ctx->stage = L.stage ? reinterpret_cast<double*>(p) : nullptr;
+    p += L.stage;
     char* edge_base = p;
     for (int o = 0; o < NOBJ; ++o)
         for (int e = 0; e < 3; ++e)
@@ -737,13 +730,14 @@ int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
     if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "upload size %zu != %lld cells", n, ctx->g.ncell);
     if (ctx->elem == 8) {
         CK(cudaMemcpyAsync(ctx->q[var], host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-    } else {
-        std::vector<float> tmp(n);
-        to_dev_type(host, tmp.data(), (long long)n);
-        CK(cudaMemcpyAsync(ctx->q[var], tmp.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
+    } else {   // FP64 values to the staging buffer, rounded to FP32 on the device
+        CK(cudaMemcpyAsync(ctx->stage, host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+        f64_to_f32_kernel<<<launch_blocks((long long)(n + 3) / 4), 256, 0, ctx->stream>>>(
+            ctx->stage, static_cast<float*>(ctx->q[var]), (long long)n);
+        CK(cudaGetLastError());
+        ctx->launches += 1;
     }
+    CK(cudaStreamSynchronize(ctx->stream));
     ctx->cfl_valid = false;
     return IMG_OK;
 }
@@ -753,13 +747,14 @@ int img_download(img_ctx* ctx, int var, double* host, size_t n) {
     if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "download size %zu != %lld cells", n, ctx->g.ncell);
     if (ctx->elem == 8) {
         CK(cudaMemcpyAsync(host, ctx->q[var], n * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-    } else {
-        std::vector<float> tmp(n);
-        CK(cudaMemcpyAsync(tmp.data(), ctx->q[var], n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaStreamSynchronize(ctx->stream));
-        for (size_t i = 0; i < n; ++i) host[i] = tmp[i];
+    } else {   // widened to FP64 on the device, then one copy
+        f32_to_f64_kernel<<<launch_blocks((long long)(n + 3) / 4), 256, 0, ctx->stream>>>(
+            static_cast<const float*>(ctx->q[var]), ctx->stage, (long long)n);
+        CK(cudaGetLastError());
+        ctx->launches += 1;
+        CK(cudaMemcpyAsync(host, ctx->stage, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     }
+    CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
 }
 

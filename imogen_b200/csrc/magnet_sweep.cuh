@@ -1,16 +1,16 @@
 // Magnet sweep along X for the two transverse components (magnet/magnetFlux.m:14-31,
 // magnet/relaxingMagnet.m:15-60, magnet/MagnetArray.m:36-38).
 //
-// The general path is five launches:
+// Three launches per sweep:
 //   mag_chain  -- per X-pencil and component I: corner velocity (transverse average, then the
 //                 1-2-1 smoothing along X), upwind predictor, TVD corrector, B_I update.  Writes
 //                 B_I in place and the limited flux F_I to scratch.  Both components in one launch.
-//   mag_ct1    -- C_I = F_I - F_I.shift(I,+1)                     (relaxingMagnet.m:56)
-//   mag_ct2    -- D_I = C_I.shift(X,-1)                           (relaxingMagnet.m:57)
-//   mag_bx     -- B_X' = (B_X - dt/dI1 D_I1) - dt/dI2 D_I2 to scratch; cell-centred B_I2
-//   mag_cell   -- B_X = B_X'; cell-centred B_X                    (MagnetArray.m:36-38)
-// Each pointwise pass reads neighbours of the previous pass's output, so no pass overwrites an
-// array that another thread of the same pass still reads.
+//   mag_ct     -- D_I = (F_I - F_I.shift(I,+1)).shift(X,-1) for both components, evaluated from F
+//                 (relaxingMagnet.m:56-57), B_X' = (B_X - dt/dI1 D_I1) - dt/dI2 D_I2 to scratch,
+//                 cell-centred B_I2
+//   mag_cell   -- B_X = B_X'; cell-centred B_X (MagnetArray.m:36-38); the drift of the flux
+//                 objects' stored edges along I, which mag_ct only reads
+// Each pass reads only arrays that no thread of the same pass writes.
 #pragma once
 
 #include "fluid_sweep.cuh"
@@ -21,7 +21,6 @@ struct MagArgs {
     SweepGeom sg;              // sweep along d = X-1
     void* q[NQ];
     void* F[2];                // limited flux per component (scratch)
-    void* C[2];                // CT differences per component (scratch)
     void* BXn;                 // new B_X (scratch)
     DevTime* tm;
     int X;                     // 1-based sweep dimension
@@ -45,17 +44,13 @@ struct MagArgs {
 };
 
 // ---- transverse (non-pencil) shifts used by the pointwise passes ----------------------------------
-// Value of A.shift(dim e, n)[cell] for n = -1 or +1, computed from global memory along e.
+// Value of A.shift(dim e, n) at index i of a line of Ne values along e, for n = -1 or +1, where
+// at(j) returns A at index j of that line and fi is the line's index in the face orthogonal to e.
 // mode/act/flip/edge describe the array object; the edge state of a trans edge is drifted and
 // written back when `own_update` (exactly one thread per face cell calls with own_update = true).
-template <typename T>
-__device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y, int z, int e, int n, int mode,
-                         int act, bool flip, double* edge, const double* fc, int f, double bc_inf, bool own_update) {
-    const int Ne = sel3(e, g.n[0], g.n[1], g.n[2]);
-    const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
-    const int i = sel3(e, x, y, z);
-    const long long b = cell - (long long)i * se;   // row 0 of this line along e
-    auto at = [&](int j) -> T { return A[b + (long long)j * se]; };
+template <typename T, typename At>
+__device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long fi, int n, int mode, int act, bool flip,
+                                        double* edge, const double* fc, int f, double bc_inf, bool own_update) {
     const bool upper = n > 0;
     const bool is_ghost = upper ? (i == Ne - 1) : (i == 0);
     if (mode == BC_CIRC) return at(((i + n) % Ne + Ne) % Ne);
@@ -68,7 +63,6 @@ __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long ce
         }
         return v;
     }
-    long long fi = face_index(g, e, x, y, z);
     switch (mode) {
         case BC_MIRROR: { T v = upper ? at(Ne - 2) : at(1); return flip ? -v : v; }
         case BC_WALL: return (T)edge[fi];
@@ -91,6 +85,19 @@ __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long ce
         }
         default: return upper ? at(Ne - 1) : at(0);   // const
     }
+}
+
+// A.shift(dim e, n)[cell] for an array A in global memory.
+template <typename T>
+__device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y, int z, int e, int n,
+                                         int mode, int act, bool flip, double* edge, const double* fc, int f,
+                                         double bc_inf, bool own_update) {
+    const int Ne = sel3(e, g.n[0], g.n[1], g.n[2]);
+    const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
+    const int i = sel3(e, x, y, z);
+    const long long b = cell - (long long)i * se;   // row 0 of this line along e
+    auto at = [&](int j) -> T { return A[b + (long long)j * se]; };
+    return shift_line<T>(at, i, Ne, face_index(g, e, x, y, z), n, mode, act, flip, edge, fc, f, bc_inf, own_update);
 }
 
 // ---- the X-chain ------------------------------------------------------------------------------------
@@ -347,75 +354,57 @@ __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, 
     y = (int)(r - (unsigned)z * n1);
 }
 
-// C_I = F_I - F_I.shift(I, +1)   (flux(X) object of mag(I): mag-class BC along I, component I)
+// D_q = (F_q - F_q.shift(I_q, +1)).shift(X, -1) at one cell, from the limited flux F_q (the flux(X)
+// object of mag(I_q): mag-class BC along I_q with the mirror flip of component I_q, along X the
+// mag-class BC without it).  The I-shift's trans edge is only read here (mag_cell stores its drift);
+// the X-shift's lower edge is drifted and stored by the thread of the face cell (x == 0).
 template <typename T>
-__global__ void mag_ct1_kernel(const __grid_constant__ MagArgs a) {
-    if (a.tm->done || a.tm->error) return;
+__device__ __forceinline__ T ct_difference(const MagArgs& a, int q, long long cell, int x, int y, int z) {
     const Geom& g = a.sg.g;
     const int d = a.X - 1;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * g.ncell;
-         i += (long long)gridDim.x * blockDim.x) {
-        int q = i >= g.ncell;
-        long long cell = i - q * g.ncell;
-        int x, y, z;
-        cell_coords(g, cell, x, y, z);
-        const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
-        T* C = reinterpret_cast<T*>(q ? a.C[1] : a.C[0]);
-        int I = q ? a.I[1] : a.I[0], e = I - 1;
-        T fs;
-        if (q ? a.shiftI[1] : a.shiftI[0]) {
-            bool own = sel3(e, x, y, z) == sel3(e, g.n[0], g.n[1], g.n[2]) - 1;
-            fs = shift_along<T>(g, F, cell, x, y, z, e, +1, q ? a.modeI_mag[1][1] : a.modeI_mag[0][1],
-                                q ? a.actI_mag[1] : a.actI_mag[0], true,
-                                a.edges->p[mag_obj(I - 1, d, MO_FLUX)][e][1], a.fade, a.fade_f, a.bc_inf, own);
-        } else {
-            fs = F[cell];
-        }
-        C[cell] = F[cell] - fs;
-    }
-}
-
-// D_I = C_I.shift(X, -1)   (flux(X) object of mag(I), lower X edge) -> written over F_I
-template <typename T>
-__global__ void mag_ct2_kernel(const __grid_constant__ MagArgs a) {
-    if (a.tm->done || a.tm->error) return;
-    const Geom& g = a.sg.g;
-    const int d = a.X - 1;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * g.ncell;
-         i += (long long)gridDim.x * blockDim.x) {
-        int q = i >= g.ncell;
-        long long cell = i - q * g.ncell;
-        int x, y, z;
-        cell_coords(g, cell, x, y, z);
-        const T* C = reinterpret_cast<const T*>(q ? a.C[1] : a.C[0]);
-        T* D = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
-        int I = q ? a.I[1] : a.I[0];
-        bool own = sel3(d, x, y, z) == 0;
-        D[cell] = shift_along<T>(g, C, cell, x, y, z, d, -1, a.modeX[0], a.actX, I - 1 == d,
-                                 a.edges->p[mag_obj(I - 1, d, MO_FLUX)][d][0], a.fade, a.fade_f, a.bc_inf, own);
-    }
+    const int I = q ? a.I[1] : a.I[0], e = I - 1;
+    const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
+    const bool shI = q ? a.shiftI[1] : a.shiftI[0];
+    const int modeI = q ? a.modeI_mag[1][1] : a.modeI_mag[0][1];
+    const int actI = q ? a.actI_mag[1] : a.actI_mag[0];
+    double* edgeI = a.edges->p[mag_obj(e, d, MO_FLUX)][e][1];
+    const int Nd = sel3(d, g.n[0], g.n[1], g.n[2]);
+    const long long sdx = sel3(d, g.s[0], g.s[1], g.s[2]);
+    const int xd = sel3(d, x, y, z);
+    const long long row0 = cell - (long long)xd * sdx;   // X-index 0 of this cell's X-line
+    // C_q at X-index j of this line
+    auto C = [&](int j) -> T {
+        const long long c2 = row0 + (long long)j * sdx;
+        const T fv = F[c2];
+        if (!shI) return fv - fv;
+        const int x2 = d == 0 ? j : x, y2 = d == 1 ? j : y, z2 = d == 2 ? j : z;
+        return fv - shift_along<T>(g, F, c2, x2, y2, z2, e, +1, modeI, actI, true, edgeI, a.fade, a.fade_f, a.bc_inf,
+                                   false);
+    };
+    return shift_line<T>(C, xd, Nd, face_index(g, d, x, y, z), -1, a.modeX[0], a.actX, e == d,
+                         a.edges->p[mag_obj(e, d, MO_FLUX)][d][0], a.fade, a.fade_f, a.bc_inf, xd == 0);
 }
 
 // B_X' = (B_X - dt/dI1 * D_I1) - dt/dI2 * D_I2 -> scratch; cell-centred B of I2 (the last component).
 template <typename T>
-__global__ void mag_bx_kernel(const __grid_constant__ MagArgs a) {
+__global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const double dt = a.tm->dt;
     const T f0 = (T)(dt / a.dI[0]), f1 = (T)(dt / a.dI[1]);
     const int X = a.X;
     const T* BX = reinterpret_cast<const T*>(a.q[Q_BX + X - 1]);
-    const T* D0 = reinterpret_cast<const T*>(a.F[0]);
-    const T* D1 = reinterpret_cast<const T*>(a.F[1]);
     T* BXn = reinterpret_cast<T*>(a.BXn);
     const int I2 = a.I[1], e2 = I2 - 1;
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
     T* CB2 = reinterpret_cast<T*>(a.q[Q_CBX + e2]);
     for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
          cell += (long long)gridDim.x * blockDim.x) {
-        BXn[cell] = (BX[cell] - f0 * D0[cell]) - f1 * D1[cell];
         int x, y, z;
         cell_coords(g, cell, x, y, z);
+        const T D0 = ct_difference<T>(a, 0, cell, x, y, z);
+        const T D1 = ct_difference<T>(a, 1, cell, x, y, z);
+        BXn[cell] = (BX[cell] - f0 * D0) - f1 * D1;
         T sh;
         if (e2 < g.ndims) {
             bool own = sel3(e2, x, y, z) == sel3(e2, g.n[0], g.n[1], g.n[2]) - 1;
@@ -428,7 +417,9 @@ __global__ void mag_bx_kernel(const __grid_constant__ MagArgs a) {
     }
 }
 
-// B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1))
+// B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1)); and the drift of the I-direction
+// trans edges of both flux objects (the C_I = F_I - F_I.shift(I,+1) calls of mag_ct), stored by
+// the thread of each upper face cell.
 template <typename T>
 __global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
     if (a.tm->done || a.tm->error) return;
@@ -446,6 +437,18 @@ __global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
                               a.fade, a.fade_f, a.bc_inf, own);
         BX[cell] = BXn[cell];
         CBX[cell] = T(0.5) * (BXn[cell] + sh);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const int e = (q ? a.I[1] : a.I[0]) - 1;
+            if (!(q ? a.shiftI[1] : a.shiftI[0]) || (q ? a.modeI_mag[1][1] : a.modeI_mag[0][1]) != BC_TRANS ||
+                !(q ? a.actI_mag[1] : a.actI_mag[0]))
+                continue;
+            if (sel3(e, x, y, z) != sel3(e, g.n[0], g.n[1], g.n[2]) - 1) continue;
+            double* edge = a.edges->p[mag_obj(e, d, MO_FLUX)][e][1];
+            const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
+            const long long fi = face_index(g, e, x, y, z);
+            edge[fi] = edge_drift(edge[fi], (double)F[cell]);
+        }
     }
 }
 
