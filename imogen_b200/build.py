@@ -1,19 +1,26 @@
-"""Build the in-tree CUDA library libimogen_b200.so for sm_100a (nvcc, no JIT cache)."""
+"""Build the in-tree CUDA library libimogen_b200.so for sm_100a (nvcc, no JIT cache).
+
+The kernels are split over several translation units (host code; fluid and magnet sweeps per
+precision) that compile in parallel and link into one shared library with the CUDA runtime
+linked statically."""
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
 import sys
+import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "imogen_b200.cu")
+CSRC = os.path.join(HERE, "csrc")
+UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu"]
 OUT = os.path.join(HERE, "libimogen_b200.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))]
-DEPS.append(os.path.join(ROOT, "include", "imogen_b200.h"))
+HEADER = os.path.join(ROOT, "include", "imogen_b200.h")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 
 
 def nvcc():
@@ -23,34 +30,48 @@ def nvcc():
     raise RuntimeError("nvcc not found")
 
 
-def up_to_date(out=OUT, deps=DEPS):
+def sources():
+    return [os.path.join(CSRC, f) for f in sorted(os.listdir(CSRC))] + [HEADER]
+
+
+def up_to_date(out=OUT):
     if not os.path.exists(out):
         return False
     t = os.path.getmtime(out)
-    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+    return all(os.path.getmtime(d) <= t for d in sources() if os.path.exists(d))
 
 
 def build(force=False, verbose=False, extra=()):
-    """Compile csrc/imogen_b200.cu into libimogen_b200.so (static cudart, -fPIC).
-
-    IMOGEN_CHECKED=1 in the environment adds -DIMG_CHECKED (access checks that record instead of
-    faulting), for diagnosing a kernel on a small case."""
-    if os.environ.get("IMOGEN_CHECKED") == "1":
-        extra = tuple(extra) + ("-DIMG_CHECKED",)
-        force = True
+    """Compile csrc/*.cu (one process per translation unit) and link libimogen_b200.so."""
     if not force and up_to_date():
         return OUT
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "-cudart", "static", "-I", os.path.join(ROOT, "include"), SRC, "-o", OUT + ".tmp", *extra]
-    if verbose:
-        cmd += ["-Xptxas", "-v"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed for libimogen_b200.so")
-    if verbose:
-        sys.stderr.write(r.stderr)
-    os.replace(OUT + ".tmp", OUT)
+    cc = nvcc()
+    tmp = tempfile.mkdtemp(prefix="imogen_b200_build_")
+    try:
+        def compile_unit(unit):
+            obj = os.path.join(tmp, unit.replace(".cu", ".o"))
+            cmd = [cc, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, unit),
+                   "-o", obj, *extra]
+            if verbose:
+                cmd += ["-Xptxas", "-v"]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            return unit, obj, r
+
+        with concurrent.futures.ThreadPoolExecutor(len(UNITS)) as ex:
+            results = list(ex.map(compile_unit, UNITS))
+        for unit, _, r in results:
+            if verbose or r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {unit}")
+        link = [cc, *ARCH, "-shared", "-cudart", "static", *[o for _, o, _ in results], "-o", OUT + ".tmp"]
+        r = subprocess.run(link, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError("link of libimogen_b200.so failed")
+        os.replace(OUT + ".tmp", OUT)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
     return OUT
 
 

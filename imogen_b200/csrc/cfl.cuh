@@ -7,7 +7,7 @@
 // waits for the host.
 #pragma once
 
-#include "magnet_sweep.cuh"
+#include "sweeps.cuh"
 
 namespace img {
 

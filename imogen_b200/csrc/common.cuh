@@ -23,21 +23,7 @@ enum BcClass { CLS_MASS = 0, CLS_MOM = 1, CLS_ENER = 2, CLS_MAG = 3 };
 enum Var { Q_RHO = 0, Q_PX, Q_PY, Q_PZ, Q_E, Q_BX, Q_BY, Q_BZ, Q_CBX, Q_CBY, Q_CBZ, NQ };
 
 // Error bits written by kernels into DevTime::error (host reads them after a step).
-enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2, DERR_GEOMETRY = 4, DERR_CHECK = 8 };
-
-// Checked builds (-DIMG_CHECKED) verify pointer alignment and index ranges before selected accesses,
-// record the first failure in a global word, and skip the access instead of faulting.
-#ifdef IMG_CHECKED
-__device__ int g_check_site;
-__device__ int g_check_val;
-__device__ __forceinline__ bool img_check(bool ok, int site, long long val) {
-    if (!ok && atomicCAS(&g_check_site, 0, site) == 0) g_check_val = (int)val;
-    return ok;
-}
-#define IMG_CHECK(cond, site, val) img_check((cond), (site), (long long)(val))
-#else
-#define IMG_CHECK(cond, site, val) true
-#endif
+enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2 };
 
 // ---- stored-edge objects ------------------------------------------------------------------------
 // Every array object of the reference that can be shifted under a stateful BC (trans, wall) owns a
@@ -74,8 +60,8 @@ struct DevTime {
     int update_mode;        // 0 per step, 1 per iteration
     int error;              // DevError bits
     int done;               // TimeManager.running turned false (time >= TIMEMAX)
-    int dbg_site;           // checked builds: first failing access check (site id) ...
-    int dbg_val;            // ... and the offending index
+    int reserved0;
+    int reserved1;
     unsigned long long maxbits[3];   // per-direction max of |v_i| + c_s (bit pattern, >= 0)
     unsigned int counter;            // CTAs finished in the current CFL reduction
     unsigned int pad2;

@@ -1,0 +1,8 @@
+// Fluid sweep kernels in double: the launch entry points of sweeps.cuh for this precision.
+#include "sweeps_impl.cuh"
+
+namespace img {
+template cudaError_t launch_fluid_sweep<double>(const FluidArgs&, const PencilLaunch&, bool);
+template cudaError_t fluid_attributes<double>(int, size_t);
+template cudaError_t fluid_max_clusters<double>(const PencilLaunch&, int*);
+}  // namespace img

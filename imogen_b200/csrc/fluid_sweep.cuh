@@ -97,49 +97,49 @@ __device__ __forceinline__ T press_speed(double G, int d, const T u[5], double m
     }
 }
 
-// Column max over the pencil (and the cluster); also a full stage barrier (tl.csync).  Lanes of a
-// column reduce with warp shuffles; where a pencil spans several warps one lane per (warp, column)
-// writes part[warp][b], and after the barrier the lanes of each column share the reads of those
-// slots over all cluster ranks and reduce again.  No atomics: every slot has exactly one writer.
+// Column max over the pencil (and the cluster); also a stage barrier that orders this CTA's shared
+// reads before its next writes and, with a cluster, every rank's remote reads before them.  Lanes of
+// a column reduce with warp shuffles; one lane per (warp, column) writes part[warp][b]; after a CTA
+// barrier the lanes of each column share the reads of those local slots and reduce again.  With a
+// cluster one thread per column then publishes the CTA's maximum in cpart[b], and after the cluster
+// barrier each rank's value is read once (DSMEM) and reduced.  No atomics: every slot has one writer.
 template <typename T, int CPT>
-__device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part)[32], T local) {
+__device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part)[33], T* cpart, T local) {
     const unsigned mask = 0xffffffffu;
     if (tl.d == 0 && tl.G <= 32 && tl.CL == 1) {   // each pencil lies inside one warp
         for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
-        tl.csync();
+        __syncthreads();
         return local;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int grp, lig, w0, nwc;   // lanes of the column in a warp, this lane's index among them, its warps
-    bool leader;
     if (tl.d == 0) {   // G is a multiple of 32: whole warps per column
         for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
-        leader = lane == 0;
         grp = 32;
         lig = lane;
         w0 = (tl.b * tl.G) >> 5;
         nwc = tl.G >> 5;
     } else {           // lanes b, b + Wb, ... belong to column b
         for (int o = 16; o >= tl.Wb; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
-        leader = lane < tl.Wb;
         grp = 32 / tl.Wb;
         lig = lane / tl.Wb;
         w0 = 0;
         nwc = NT >> 5;
     }
-    if (leader) part[warp][tl.b] = local;
-    tl.csync();
+    if (lig == 0) part[warp][tl.b] = local;
+    __syncthreads();
     T m = T(0);
-    for (int j = lig; j < tl.CL * nwc; j += grp) {
-        const int r = j / nwc, w = w0 + j - r * nwc;
-        m = fmax(m, tl.remote(part, r)[w][tl.b]);
-    }
-    if (tl.d == 0) {
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
-    } else {
-        for (int o = 16; o >= tl.Wb; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
-    }
-    return m;
+    if (lig < nwc) m = part[w0 + lig][tl.b];
+    if (lig + grp < nwc) m = fmax(m, part[w0 + lig + grp][tl.b]);   // nwc <= 16 <= 2 * grp
+    const int olo = tl.d == 0 ? 1 : tl.Wb;
+    for (int o = 16; o >= olo; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
+    if (tl.CL == 1) return m;
+    if (tl.g == 0) cpart[tl.b] = m;
+    cg::this_cluster().sync();
+    T c = T(0);
+    if (lig < tl.CL) c = tl.remote(cpart, lig)[tl.b];
+    for (int o = 16; o >= olo; o >>= 1) c = fmax(c, __shfl_xor_sync(mask, c, o));
+    return c;
 }
 
 // First assignment of an InitializedArray takes its stored edges on every face it lies on
@@ -183,11 +183,14 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
     }
 }
 
-template <typename T, bool MHD, int CPT>
+// FADE: some BC of this sweep direction is fade (compiles the damping in).
+template <typename T, bool MHD, int CPT, bool FADE>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
-    __shared__ T part[2][MAX_WARPS][32];   // per-warp column maxima (two freezing speeds)
+    __shared__ T part[2][MAX_WARPS][33];   // per-warp column maxima (two freezing speeds; rows padded
+                                           // so the lanes reading one column's warps hit distinct banks)
+    __shared__ T cpart[2][32];             // per-CTA column maxima, read by the other cluster ranks
     __shared__ double cflp[3][MAX_WARPS];  // per-warp CFL maxima
     Tile<T, CPT> tl;
     tl.init(a.sg);
@@ -227,7 +230,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
         T spd = press_speed<T>(G, d, uu, m, press[k]);
         if (ok) lmax = fmax(lmax, spd);
     }
-    const T cf = column_max(tl, NT, part[0], lmax);
+    const T cf = column_max(tl, NT, part[0], cpart[0], lmax);
 
     // ---- predictor fluxes R = (u+w)/2, L = (u-w)/2 -> set A (relaxingFluid.m:30-31) ---------------
 #pragma unroll
@@ -269,8 +272,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const int cls = fluid_class(v);
             const T* R = SA + v * AS;
             const T* L = SA + (5 + v) * AS;
-            const T Rm = shifted(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = shifted<FADE>(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted<FADE>(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
             us[v] = u[v][k] - half_ffx * cf * (R[ix] - Rm + L[ix] - Lp);
         }
         us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
@@ -280,7 +283,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
         T spd = press_speed<T>(G, d, us, msq[k], press2[k]);   // relaxingFluid.m:47-50
         if (tl.ok(k)) lmax2 = fmax(lmax2, spd);
     }
-    const T cfs = column_max(tl, NT, part[1], lmax2);   // its barrier also ends the predictor reads of set A
+    const T cfs = column_max(tl, NT, part[1], cpart[1], lmax2);   // its barrier also ends the predictor reads of set A
 
     // ---- corrector fluxes (relaxingFluid.m:52-56) from the half-step state -> set A --------------
 #pragma unroll
@@ -325,10 +328,10 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const Ghost<T>* aL = AN + (2 * (5 + v)) * Wb;
             const int mlo = a.mode[cls][0], mhi = a.mode[cls][1];
             const T r = R[ix], l = L[ix];
-            const T Rm = shifted(tl, R, aR, k, -1, mlo, fc, fw);
-            const T Rp = shifted(tl, R, aR + Wb, k, +1, mhi, fc, fw);
-            const T Lm = shifted(tl, L, aL, k, -1, mlo, fc, fw);
-            const T Lp = shifted(tl, L, aL + Wb, k, +1, mhi, fc, fw);
+            const T Rm = shifted<FADE>(tl, R, aR, k, -1, mlo, fc, fw);
+            const T Rp = shifted<FADE>(tl, R, aR + Wb, k, +1, mhi, fc, fw);
+            const T Lm = shifted<FADE>(tl, L, aL, k, -1, mlo, fc, fw);
+            const T Lp = shifted<FADE>(tl, L, aL + Wb, k, +1, mhi, fc, fw);
             SB[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
             SB[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
         }
@@ -348,8 +351,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             const int cls = fluid_class(v);
             const T* R = SB + v * AS;
             const T* L = SB + (5 + v) * AS;
-            const T Rm = shifted(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = shifted<FADE>(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
+            const T Lp = shifted<FADE>(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
             unew[v] = u[v][k] - ff * cfs * (R[ix] - Rm + L[ix] - Lp);
         }
         unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;

@@ -199,21 +199,59 @@ int launch_blocks(long long work, int bs = 256) {
     return (int)std::max(1LL, std::min(b, 148LL * 16));
 }
 
-template <typename T, int CPT>
-int launch_fluid_cpt(img_ctx* ctx, int d, bool cfl) {
+// Sweep geometry of direction d with the context's pencil tiling (cells per thread CPT).
+SweepGeom sweep_geom(const img_ctx* ctx, int d, int cpt) {
+    const PencilCfg& pcf = ctx->pcfg[d];
+    SweepGeom s{};
+    s.g = ctx->g;
+    s.d = d;
+    s.d1 = d == 0 ? 1 : 0;
+    s.d2 = d == 2 ? 1 : 2;
+    s.N = ctx->g.n[d];
+    s.ncol = ctx->g.ncell / s.N;
+    s.Wb = pcf.Wb;
+    s.G = pcf.G;
+    s.CL = pcf.CL;
+    s.NT = pcf.NT;
+    s.RC = pcf.G * cpt;
+    s.rank_hi = (s.N - 1) / s.RC;
+    s.n1 = ctx->g.n[s.d1];
+    s.sd = ctx->g.s[d];
+    s.s1 = ctx->g.s[s.d1];
+    s.s2 = ctx->g.s[s.d2];
+    return s;
+}
+
+// A fade BC on sweep direction d for any of the given classes (compiles the fade damping in).
+bool fade_on(const img_config& c, int d, int cls_lo, int cls_hi) {
+    for (int k = cls_lo; k <= cls_hi; ++k)
+        if (c.bc_modes[k][0][d] == IMG_BC_FADE || c.bc_modes[k][1][d] == IMG_BC_FADE) return true;
+    return false;
+}
+
+template <typename T>
+PencilLaunch pencil_launch(const img_ctx* ctx, int d, size_t smem, unsigned grid_y, bool fade) {
+    const PencilCfg& pcf = ctx->pcfg[d];
+    const long long ncol = ctx->g.ncell / ctx->g.n[d];
+    const long long nb = (ncol + pcf.Wb - 1) / pcf.Wb;
+    PencilLaunch L{};
+    L.grid_x = (unsigned)(nb * pcf.CL);
+    L.grid_y = grid_y;
+    L.block = pcf.NT;
+    L.smem = smem;
+    L.cluster = pcf.CL;
+    L.cpt = pcf.cpt;
+    L.fade = fade;
+    L.stream = ctx->stream;
+    return L;
+}
+
+template <typename T>
+int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     FluidArgs a{};
     const img_config& c = ctx->cfg;
-    PencilCfg pcf = ctx->pcfg[d];
-    a.sg.g = ctx->g;
-    a.sg.d = d;
-    a.sg.d1 = d == 0 ? 1 : 0;
-    a.sg.d2 = d == 2 ? 1 : 2;
-    a.sg.N = ctx->g.n[d];
-    a.sg.ncol = ctx->g.ncell / a.sg.N;
-    a.sg.Wb = pcf.Wb;
-    a.sg.G = pcf.G;
-    a.sg.CL = pcf.CL;
-    a.sg.NT = pcf.NT;
+    const PencilCfg& pcf = ctx->pcfg[d];
+    a.sg = sweep_geom(ctx, d, pcf.cpt);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.tm = ctx->tm;
     a.gamma = c.gamma;
@@ -234,24 +272,12 @@ int launch_fluid_cpt(img_ctx* ctx, int d, bool cfl) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.cfl = cfl;
-    long long nb = (a.sg.ncol + pcf.Wb - 1) / pcf.Wb;
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3((unsigned)(nb * pcf.CL));
-    lc.blockDim = dim3(pcf.NT);
-    lc.dynamicSmemBytes = fluid_smem_bytes<T>(pcf.G * CPT, pcf.Wb);
-    lc.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = pcf.CL;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    lc.attrs = attr;
-    lc.numAttrs = 1;
-    void (*kern)(const FluidArgs) = ctx->mhd ? fluid_sweep_kernel<T, true, CPT> : fluid_sweep_kernel<T, false, CPT>;
-    cudaError_t le = cudaLaunchKernelEx(&lc, kern, a);
+    const PencilLaunch L = pencil_launch<T>(ctx, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+                                            fade_on(c, d, CLS_MASS, CLS_ENER));
+    cudaError_t le = launch_fluid_sweep<T>(a, L, ctx->mhd != 0);
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "fluid sweep launch (dim %d, grid %u, block %u, smem %zu, cluster %d): %s", d,
-                    lc.gridDim.x, lc.blockDim.x, lc.dynamicSmemBytes, pcf.CL, cudaGetErrorString(le));
+                    L.grid_x, L.block, L.smem, L.cluster, cudaGetErrorString(le));
     ctx->launches += 1;
     ctx->init_store = false;
     ctx->init_flux = false;
@@ -259,29 +285,11 @@ int launch_fluid_cpt(img_ctx* ctx, int d, bool cfl) {
 }
 
 template <typename T>
-int launch_fluid(img_ctx* ctx, int d, bool cfl) {
-    switch (ctx->pcfg[d].cpt) {
-        case 1: return launch_fluid_cpt<T, 1>(ctx, d, cfl);
-        case 2: return launch_fluid_cpt<T, 2>(ctx, d, cfl);
-        default: return launch_fluid_cpt<T, 4>(ctx, d, cfl);
-    }
-}
-
-template <typename T>
 void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     const img_config& c = ctx->cfg;
     int d = X - 1;
     PencilCfg pcf = ctx->pcfg[d];
-    a.sg.g = ctx->g;
-    a.sg.d = d;
-    a.sg.d1 = d == 0 ? 1 : 0;
-    a.sg.d2 = d == 2 ? 1 : 2;
-    a.sg.N = ctx->g.n[d];
-    a.sg.ncol = ctx->g.ncell / a.sg.N;
-    a.sg.Wb = pcf.Wb;
-    a.sg.G = pcf.G;
-    a.sg.CL = pcf.CL;
-    a.sg.NT = pcf.NT;
+    a.sg = sweep_geom(ctx, d, pcf.cpt);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.F[0] = ctx->scratch[0];
     a.F[1] = ctx->scratch[1];
@@ -317,48 +325,25 @@ void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     a.edges = ctx->edges_dev;
 }
 
-template <typename T, int CPT>
-int launch_magnet_cpt(img_ctx* ctx, int X, int I1, int I2) {
+template <typename T>
+int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     MagArgs a{};
     fill_mag_args<T>(ctx, X, I1, I2, a);
-    int d = X - 1;
-    PencilCfg pcf = ctx->pcfg[d];
-    long long nb = (a.sg.ncol + pcf.Wb - 1) / pcf.Wb;
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3((unsigned)(nb * pcf.CL), 2);
-    lc.blockDim = dim3(pcf.NT);
-    lc.dynamicSmemBytes = mag_smem_bytes<T>(pcf.G * CPT, pcf.Wb);
-    lc.stream = ctx->stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = pcf.CL;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    lc.attrs = attr;
-    lc.numAttrs = 1;
-    void (*kern)(const MagArgs) = mag_chain_kernel<T, CPT>;
-    cudaError_t le = cudaLaunchKernelEx(&lc, kern, a);
+    const int d = X - 1;
+    const PencilCfg& pcf = ctx->pcfg[d];
+    const PencilLaunch L = pencil_launch<T>(ctx, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 2,
+                                            fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    cudaError_t le = launch_mag_chain<T>(a, L);
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
-                    lc.gridDim.x, lc.blockDim.x, lc.dynamicSmemBytes, pcf.CL, cudaGetErrorString(le));
-    long long n = ctx->g.ncell;
-    mag_ct_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
-    CK(cudaGetLastError());
-    mag_cell_kernel<T><<<launch_blocks(n), 256, 0, ctx->stream>>>(a);
-    CK(cudaGetLastError());
+                    L.grid_x, L.block, L.smem, L.cluster, cudaGetErrorString(le));
+    const long long n = ctx->g.ncell;
+    CK(launch_mag_ct<T>(a, launch_blocks(n), ctx->stream));
+    CK(launch_mag_cell<T>(a, launch_blocks(n), ctx->stream));
     ctx->launches += 3;
     ctx->init_mag[I1 - 1][d] = false;
     ctx->init_mag[I2 - 1][d] = false;
     return IMG_OK;
-}
-
-template <typename T>
-int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
-    switch (ctx->pcfg[X - 1].cpt) {
-        case 1: return launch_magnet_cpt<T, 1>(ctx, X, I1, I2);
-        case 2: return launch_magnet_cpt<T, 2>(ctx, X, I1, I2);
-        default: return launch_magnet_cpt<T, 4>(ctx, X, I1, I2);
-    }
 }
 
 template <typename T>
@@ -376,61 +361,34 @@ int launch_cfl_reduce(img_ctx* ctx) {
     return IMG_OK;
 }
 
-// Kernel attributes (shared memory above 48 KB, clusters above 8 CTAs), set once per context so
-// that no attribute call happens inside a stream capture, and a schedulability check of every
-// pencil configuration.
-template <typename T, int CPT>
-int set_kernel_attributes_cpt(img_ctx* ctx) {
-    size_t smem = 0;
-    int cl = 1;
-    bool used = false;
+// Kernel attributes (dynamic shared memory limits), set once per context so that no attribute call
+// happens inside a stream capture, and a schedulability check of every pencil configuration.
+template <typename T>
+int set_kernel_attributes(img_ctx* ctx) {
+    for (int cpt : {1, 2, 4}) {
+        size_t fs = 0, ms = 0;
+        for (int d = 0; d < 3; ++d) {
+            const PencilCfg& p = ctx->pcfg[d];
+            if (p.cpt != cpt) continue;
+            fs = std::max(fs, fluid_smem_bytes<T>(p.G * cpt, p.Wb));
+            ms = std::max(ms, mag_smem_bytes<T>(p.G * cpt, p.Wb));
+        }
+        // the default dynamic limit is 48 KB minus the static shared memory: always raise it
+        if (fs) CK(fluid_attributes<T>(cpt, fs));
+        if (ms) CK(chain_attributes<T>(cpt, ms));
+    }
     for (int d = 0; d < 3; ++d) {
         const PencilCfg& p = ctx->pcfg[d];
-        if (p.cpt != CPT) continue;
-        used = true;
-        smem = std::max(smem, fluid_smem_bytes<T>(p.G * CPT, p.Wb));
-        smem = std::max(smem, mag_smem_bytes<T>(p.G * CPT, p.Wb));
-        cl = std::max(cl, p.CL);
-    }
-    if (!used) return IMG_OK;
-    void (*fk[2])(const FluidArgs) = {fluid_sweep_kernel<T, false, CPT>, fluid_sweep_kernel<T, true, CPT>};
-    void (*mk)(const MagArgs) = mag_chain_kernel<T, CPT>;
-    // the default dynamic limit is 48 KB minus the static shared memory: always raise it
-    for (auto k : fk) {
-        CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        if (cl > 8) CK(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    }
-    CK(cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    if (cl > 8) CK(cudaFuncSetAttribute(mk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    for (int d = 0; d < 3; ++d) {
-        const PencilCfg& p = ctx->pcfg[d];
-        if (ctx->g.n[d] < 3 || p.cpt != CPT) continue;
-        cudaLaunchConfig_t lc{};
-        lc.gridDim = dim3((unsigned)p.CL);
-        lc.blockDim = dim3(p.NT);
-        lc.dynamicSmemBytes = fluid_smem_bytes<T>(p.G * CPT, p.Wb);
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = p.CL;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        lc.attrs = attr;
-        lc.numAttrs = 1;
+        if (ctx->g.n[d] < 3) continue;
+        PencilLaunch L = pencil_launch<T>(ctx, d, fluid_smem_bytes<T>(p.G * p.cpt, p.Wb), 1, false);
         int nclusters = 0;
-        cudaError_t e = cudaOccupancyMaxActiveClusters(&nclusters, fk[1], &lc);
+        cudaError_t e = fluid_max_clusters<T>(L, &nclusters);
         if (e != cudaSuccess || nclusters < 1)
             return fail(ctx, IMG_ERR_UNSUPPORTED, "pencil configuration for dim %d (block %d, cluster %d, smem %zu) "
-                        "cannot be scheduled: %s", d, p.NT, p.CL, lc.dynamicSmemBytes,
+                        "cannot be scheduled: %s", d, p.NT, p.CL, L.smem,
                         e != cudaSuccess ? cudaGetErrorString(e) : "0 active clusters");
     }
     return IMG_OK;
-}
-
-template <typename T>
-int set_kernel_attributes(img_ctx* ctx) {
-    int rc = set_kernel_attributes_cpt<T, 1>(ctx);
-    if (rc == IMG_OK) rc = set_kernel_attributes_cpt<T, 2>(ctx);
-    return rc != IMG_OK ? rc : set_kernel_attributes_cpt<T, 4>(ctx);
 }
 
 int fluid_sweep(img_ctx* ctx, int X, bool cfl) {
@@ -494,12 +452,6 @@ int enqueue_iteration(img_ctx* ctx) {
 int check_dev_error(img_ctx* ctx) {
     CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-#ifdef IMG_CHECKED
-    int site = 0, val = 0;
-    CK(cudaMemcpyFromSymbol(&site, g_check_site, sizeof(int)));
-    CK(cudaMemcpyFromSymbol(&val, g_check_val, sizeof(int)));
-    if (site) return fail(ctx, IMG_ERR_CUDA, "checked build: access check %d failed (value %d)", site, val);
-#endif
     int e = ctx->host_tm->error;
     if (e & DERR_CFL) return fail(ctx, IMG_ERR_CFL, "CFL error: no velocity exceeded the 1e-2 floor (cmax=%g)", ctx->host_tm->cmax);
     if (e & DERR_NONFINITE_DT) return fail(ctx, IMG_ERR_NONFINITE, "non-finite timestep");

@@ -1,0 +1,9 @@
+// Magnet sweep kernels in float: the launch entry points of sweeps.cuh for this precision.
+#include "sweeps_impl.cuh"
+
+namespace img {
+template cudaError_t launch_mag_chain<float>(const MagArgs&, const PencilLaunch&);
+template cudaError_t launch_mag_ct<float>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t launch_mag_cell<float>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t chain_attributes<float>(int, size_t);
+}  // namespace img

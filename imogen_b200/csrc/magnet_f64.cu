@@ -1,0 +1,9 @@
+// Magnet sweep kernels in double: the launch entry points of sweeps.cuh for this precision.
+#include "sweeps_impl.cuh"
+
+namespace img {
+template cudaError_t launch_mag_chain<double>(const MagArgs&, const PencilLaunch&);
+template cudaError_t launch_mag_ct<double>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t launch_mag_cell<double>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t chain_attributes<double>(int, size_t);
+}  // namespace img

@@ -142,7 +142,8 @@ __device__ __forceinline__ double wmag_upper_ghosts(const Tile<T, CPT>& tl, cons
     return e4;
 }
 
-template <typename T, int CPT>
+// FADE: a mag-class BC along X is fade (compiles the damping in).
+template <typename T, int CPT, bool FADE>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
@@ -221,8 +222,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
     T vg[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T m1 = shifted(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
-        const T p1 = shifted(tl, (const T*)S0, ANU, k, +1, mhi, fc, f);
+        const T m1 = shifted<FADE>(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
+        const T p1 = shifted<FADE>(tl, (const T*)S0, ANU, k, +1, mhi, fc, f);
         vg[k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[k]) : T(0);
         S1[tl.idx(k)] = vg[k];
     }
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
     T vf[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T p1 = shifted(tl, (const T*)S1, ANU, k, +1, mhi, fc, f);
+        const T p1 = shifted<FADE>(tl, (const T*)S1, ANU, k, +1, mhi, fc, f);
         vf[k] = (vg[k] + p1) < T(0) ? T(1) : T(0);
         const T F = bI[k] * vg[k];
         S2[tl.idx(k)] = F;
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T F = S2[tl.idx(k)];
-        const T Fp = shifted(tl, (const T*)S2, ANU, k, +1, mhi, fc, f);
+        const T Fp = shifted<FADE>(tl, (const T*)S2, ANU, k, +1, mhi, fc, f);
         S3[tl.idx(k)] = F * (T(1) - vf[k]) + Fp * vf[k];
     }
     tl.csync();
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T Fu = S3[tl.idx(k)];
-        const T st = bI[k] - ff * (Fu - shifted(tl, (const T*)S3, ANL, k, -1, mlo, fc, f));
+        const T st = bI[k] - ff * (Fu - shifted<FADE>(tl, (const T*)S3, ANL, k, -1, mlo, fc, f));
         W[k] = st * vg[k];
         S0[tl.idx(k)] = W[k];
         if (init_mag && tl.ok(k)) {
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
                 p2 = GS[3 * Wb + b].g;
             }
         }
-        if (mhi == BC_FADE) {
+        if (FADE && mhi == BC_FADE) {
             const Ghost<T>& u1 = GS[1 * Wb + b];
             const Ghost<T>& u2 = GS[3 * Wb + b];
             p1a = fade_apply(p1a, r, N, fc, f, u1.s0, u1.sN1);
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
             p1d = fade_apply(p1d, r, N, fc, f, u1.s0, u1.sN1);
             p2 = fade_apply(p2, r, N, fc, f, u2.s0, u2.sN1);
         }
-        const T m1 = shifted(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
+        const T m1 = shifted<FADE>(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
         const T fx = w * (T(1) - v) + p1a * v;
         const T dFluxR = p1b - (v * p2 + (T(1) - v) * w);
         const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
@@ -336,7 +337,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
     T* Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T fm = shifted(tl, (const T*)S1, ANL, k, -1, mlo, fc, f);
+        const T fm = shifted<FADE>(tl, (const T*)S1, ANL, k, -1, mlo, fc, f);
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
         BI[o] = bI[k] - ff2 * (Fl[k] - fm);

@@ -17,7 +17,8 @@
 
 namespace img {
 
-// Geometry of one directional sweep (host-filled).
+// Geometry of one directional sweep (host-filled; kernels read it from their grid-constant
+// parameter, so the uniform values cost no registers).
 struct SweepGeom {
     Geom g;
     int d;            // sweep dimension 0..2
@@ -26,8 +27,12 @@ struct SweepGeom {
     long long ncol;   // number of pencils = ncell / N
     int Wb;           // pencils per CTA
     int G;            // threads per pencil per CTA
-    int CL;           // CTAs per cluster along the pencil
+    int CL;           // CTAs per cluster along the pencil (1, 2 or 4)
     int NT;           // threads per CTA = Wb * G
+    int RC;           // rows per CTA = G * cells per thread
+    int rank_hi;      // cluster rank holding row N-1 = (N-1) / RC
+    int n1;           // g.n[d1]
+    long long sd, s1, s2;   // strides along d, d1, d2
 };
 
 constexpr int HALO_LO = 1;   // halo rows below the CTA's rows
@@ -45,46 +50,54 @@ struct Ghost {
 
 template <typename T, int CPT>
 struct Tile {
-    int b, g, rank, N, Wb, G, CL, d, RC, rank_hi;
+    // uniform (copies of parameter values)
+    int N, Wb, G, CL, d, RC, rank_hi;
+    // per thread
+    int b, g, rank;
+    int row0;             // global row of own cell k = 0
+    int ix0;              // shared index of own cell k = 0
     long long col;        // global pencil index
     bool colok;
     long long base;       // linear offset of row 0 of this pencil
     long long sd;         // stride along the sweep
-    int coord1, coord2;
+    int n1;
 
     __device__ __forceinline__ void init(const SweepGeom& s) {
         const int t = threadIdx.x;
-        if (s.d == 0) { g = t % s.G; b = t / s.G; }
-        else { b = t % s.Wb; g = t / s.Wb; }
-        rank = (int)(blockIdx.x % (unsigned)s.CL);
-        long long bundle = blockIdx.x / (unsigned)s.CL;
         N = s.N;
         Wb = s.Wb;
         G = s.G;
         CL = s.CL;
         d = s.d;
-        RC = G * CPT;
-        rank_hi = (N - 1) / RC;
+        RC = s.RC;
+        rank_hi = s.rank_hi;
+        sd = s.sd;
+        n1 = s.n1;
+        if (s.d == 0) { g = t % s.G; b = t / s.G; }
+        else { b = t % s.Wb; g = t / s.Wb; }
+        rank = (int)(blockIdx.x & (unsigned)(s.CL - 1));   // CL is a power of two
+        const long long bundle = blockIdx.x / (unsigned)s.CL;
+        row0 = rank * s.RC + g;
+        ix0 = (g + HALO_LO) * s.Wb + b;
         col = bundle * s.Wb + b;
         colok = col < s.ncol;
-        long long c = colok ? col : 0;
-        coord1 = (int)(c % s.g.n[s.d1]);
-        coord2 = (int)(c / s.g.n[s.d1]);
-        base = coord1 * sel3(s.d1, s.g.s[0], s.g.s[1], s.g.s[2]) +
-               (long long)coord2 * sel3(s.d2, s.g.s[0], s.g.s[1], s.g.s[2]);
-        sd = sel3(s.d, s.g.s[0], s.g.s[1], s.g.s[2]);
+        const long long c = colok ? col : 0;
+        const int c1 = (int)(c % s.n1), c2 = (int)(c / s.n1);
+        base = c1 * s.s1 + (long long)c2 * s.s2;
     }
-    __device__ __forceinline__ int grow(int k) const { return rank * RC + g + k * G; }
+    __device__ __forceinline__ int grow(int k) const { return row0 + k * G; }
     __device__ __forceinline__ bool ok(int k) const { return colok && grow(k) < N; }
     __device__ __forceinline__ long long off(int k) const { return base + (long long)grow(k) * sd; }
     // shared index of own row k, and of local row l (0 = lower halo)
-    __device__ __forceinline__ int idx(int k) const { return (g + k * G + HALO_LO) * Wb + b; }
+    __device__ __forceinline__ int idx(int k) const { return ix0 + k * G * Wb; }
     __device__ __forceinline__ int lidx(int l) const { return l * Wb + b; }
     __device__ __forceinline__ void coords(int k, int& x, int& y, int& z) const {
-        int r = grow(k);
-        if (d == 0) { x = r; y = coord1; z = coord2; }
-        else if (d == 1) { x = coord1; y = r; z = coord2; }
-        else { x = coord1; y = coord2; z = r; }
+        const int r = grow(k);
+        const long long c = colok ? col : 0;
+        const int c1 = (int)(c % n1), c2 = (int)(c / n1);
+        if (d == 0) { x = r; y = c1; z = c2; }
+        else if (d == 1) { x = c1; y = r; z = c2; }
+        else { x = c1; y = c2; z = r; }
     }
     __device__ __forceinline__ void csync() const {
         if (CL > 1) cg::this_cluster().sync();
@@ -122,12 +135,13 @@ __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, in
 }
 
 // A.shift(d, n) at own row k for n = -1 / +1 (one shared load), fade damping included.  `an` is the
-// array's anchor pair for that side (read only under fade, a uniform branch).
-template <typename T, int CPT>
+// array's anchor pair for that side, read only under fade; FADE = false (no fade BC on this sweep
+// direction, known at launch) compiles the damping out.
+template <bool FADE, typename T, int CPT>
 __device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* an, int k, int n, int mode,
                                      const double* fc, int f) {
     T v = A[tl.idx(k) + n * tl.Wb];
-    if (mode == BC_FADE) {
+    if (FADE && mode == BC_FADE) {
         const Ghost<T>& q = an[tl.b];
         v = fade_apply(v, tl.grow(k), tl.N, fc, f, q.s0, q.sN1);
     }

@@ -1,0 +1,31 @@
+// Launch entry points of the pencil kernels, compiled in their own translation units (one per
+// kernel family and precision, built in parallel) and called by the host code.
+#pragma once
+
+#include "magnet_sweep.cuh"
+
+namespace img {
+
+// Launch shape of one pencil-kernel launch.
+struct PencilLaunch {
+    unsigned grid_x, grid_y;   // CTAs (grid_x = bundles x cluster size)
+    unsigned block;            // threads per CTA
+    size_t smem;               // dynamic shared memory per CTA
+    int cluster;               // CTAs per cluster along the pencil
+    int cpt;                   // cells per thread (1, 2 or 4)
+    bool fade;                 // a fade BC on this sweep direction
+    cudaStream_t stream;
+};
+
+template <typename T> cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd);
+template <typename T> cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L);
+template <typename T> cudaError_t launch_mag_ct(const MagArgs& a, unsigned blocks, cudaStream_t stream);
+template <typename T> cudaError_t launch_mag_cell(const MagArgs& a, unsigned blocks, cudaStream_t stream);
+// Raise the dynamic shared memory limit of every fluid (resp. chain) kernel variant with `cpt` cells
+// per thread to `smem` bytes.
+template <typename T> cudaError_t fluid_attributes(int cpt, size_t smem);
+template <typename T> cudaError_t chain_attributes(int cpt, size_t smem);
+// Clusters of the MHD fluid kernel that can be co-resident for launch shape L (0: not schedulable).
+template <typename T> cudaError_t fluid_max_clusters(const PencilLaunch& L, int* n);
+
+}  // namespace img
