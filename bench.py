@@ -88,6 +88,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def profiled_traffic(key):
+    """DRAM bytes (read + write) per launch of a kernel, from the committed ncu summary."""
+    import re
+    try:
+        with open(os.path.join(ROOT, "profiles", "pencil_kernels_orszag_tang_512_mixed.md")) as f:
+            m = re.search(r"traffic_bytes %s = (\d+)" % re.escape(key), f.read())
+        return int(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -245,6 +256,7 @@ def run_ours(args):
 
     # per-kernel roofline: the fused fluid sweep timed alone, L2 flushed before each launch
     peak, peak_kind = measured_hbm_peak()
+    traffic = profiled_traffic("fluid_sweep_x_mixed") if args.workload == "ot512" else None
     roof = {}
     for prec in ("mixed", "fp64"):
         r = runs[prec]
@@ -254,7 +266,9 @@ def run_ours(args):
         per = el / max(5, args.steps)
         alg = ncell * (8 + 5) * w     # reads rho,p,E,cellB (8 words), writes rho,p,E (5 words)
         roof[prec] = {"bound": "hbm", "achieved": alg / per / 1e9, "peak": peak, "unit": "GB/s",
-                      "frac": alg / per / 1e9 / peak, "traffic": None, "kernel": "fluid_sweep_kernel X",
+                      "frac": alg / per / 1e9 / peak, "traffic": traffic if prec == "mixed" else None,
+                      "traffic_source": "profiles/pencil_kernels_orszag_tang_512_mixed.md (ncu capture)"
+                      if prec == "mixed" and traffic else None, "kernel": "fluid_sweep_kernel X",
                       "launch_us": per * 1e6, "alg_bytes": alg, "peak_kind": peak_kind}
 
     # end to end through the C ABI: the step's state comes from pinned host memory (X.array = ...

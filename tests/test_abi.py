@@ -59,3 +59,24 @@ def test_null_context_is_an_error_not_a_crash():
     L = _lib.lib()
     assert L.img_step(None) == -1
     assert L.img_sync(None) == -1
+
+
+def test_mex_gateway_compiles_against_the_abi():
+    """The MEX gateway (imogen_b200/mex) compiles with the C ABI header and a declarations-only
+    mex.h, and every img_* function it calls is exported by the library."""
+    import re
+    import shutil
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = os.path.join(root, "imogen_b200", "mex", "imogen_b200_mex.c")
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    with tempfile.TemporaryDirectory() as d:
+        r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-c", src, "-I", os.path.join(root, "tests", "mexstub"),
+                            "-I", os.path.join(root, "include"), "-o", os.path.join(d, "mex.o")],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    called = set(re.findall(r"\b(img_[a-z_]+)\(", open(src).read()))
+    assert called <= set(_lib.SYMBOLS), called - set(_lib.SYMBOLS)
