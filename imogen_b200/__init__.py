@@ -6,7 +6,7 @@ surface.  There is no CPU fallback: without the CUDA library every call raises.
 """
 from . import _lib
 from ._lib import ImogenError, lib
-from .run import ImogenRun, TimeManager, bytes_required, flux, magnetFlux, make_config, relaxingFluid
+from .run import ImogenBatch, ImogenRun, TimeManager, bytes_required, flux, magnetFlux, make_config, relaxingFluid
 
-__all__ = ["ImogenRun", "TimeManager", "ImogenError", "flux", "relaxingFluid", "magnetFlux",
+__all__ = ["ImogenBatch", "ImogenRun", "TimeManager", "ImogenError", "flux", "relaxingFluid", "magnetFlux",
            "make_config", "bytes_required", "lib"]

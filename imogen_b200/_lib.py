@@ -24,6 +24,8 @@ SYMBOLS = (
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
     "img_get_time", "img_set_time", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_launch_count",
+    "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
+    "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
 
 
@@ -91,6 +93,22 @@ def lib():
     L.img_get_stream.restype = ctypes.c_int
     L.img_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     L.img_launch_count.restype = ctypes.c_int
+    L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
+    L.img_batch_destroy.argtypes = [vp]
+    L.img_batch_add.argtypes = [vp, vp]
+    L.img_batch_remove.argtypes = [vp, vp]
+    L.img_batch_size.argtypes = [vp, ip]
+    L.img_batch_step.argtypes = [vp]
+    L.img_batch_run.argtypes = [vp, ctypes.c_int, ctypes.c_int, ip]
+    L.img_batch_status.argtypes = [vp, ip, ctypes.c_int]
+    L.img_batch_get_stream.argtypes = [vp, ctypes.POINTER(ctypes.c_void_p)]
+    L.img_batch_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.img_batch_last_error.argtypes = [vp]
+    L.img_batch_last_error.restype = ctypes.c_char_p
+    for name in ("img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size",
+                 "img_batch_step", "img_batch_run", "img_batch_status", "img_batch_get_stream",
+                 "img_batch_launch_count"):
+        getattr(L, name).restype = ctypes.c_int
     for name in ("img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
                  "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step",
                  "img_run", "img_get_time", "img_set_time", "img_totals", "img_totals_static", "img_sync"):

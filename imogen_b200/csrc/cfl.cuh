@@ -20,8 +20,9 @@ struct CflArgs {
     int use_b[3];
 };
 
+// CFL maxima of one grid, run by block vblock of vgrid blocks of that grid's launch.
 template <typename T>
-__global__ void __launch_bounds__(256) cfl_reduce_kernel(const __grid_constant__ CflArgs a) {
+__device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vblock, unsigned vgrid) {
     if (a.tm->done || a.tm->error) return;
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
@@ -30,8 +31,8 @@ __global__ void __launch_bounds__(256) cfl_reduce_kernel(const __grid_constant__
     const T* cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
                       reinterpret_cast<const T*>(a.q[Q_CBZ])};
     double m3[3] = {0.0, 0.0, 0.0};
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
-         i += (long long)gridDim.x * blockDim.x) {
+    for (long long i = vblock * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
+         i += (long long)vgrid * blockDim.x) {
         double r = rho[i], px = p[0][i], py = p[1][i], pz = p[2][i];
         double msq = 0.0;
         if (a.mhd) {
@@ -59,10 +60,24 @@ __global__ void __launch_bounds__(256) cfl_reduce_kernel(const __grid_constant__
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) cfl_reduce_kernel(const __grid_constant__ CflArgs a) {
+    cfl_reduce_body<T>(a, blockIdx.x, gridDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) cfl_reduce_batch_kernel(const CflArgs* __restrict__ args,
+                                                               const BlockMap* __restrict__ map) {
+    __shared__ CflArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    cfl_reduce_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
+}
+
 // check_running: evaluate TimeManager.running (time < TIMEMAX) first, as imogen.m:58 does at the
 // top of each iteration; the iteration limit is enforced by the host.
-__global__ void cfl_finalize_kernel(DevTime* tm, int check_running) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void cfl_finalize_body(DevTime* tm, int check_running) {
     if (tm->done || tm->error) return;
     if (check_running && !(tm->time < tm->time_max)) {
         tm->done = 1;
@@ -93,6 +108,17 @@ __global__ void cfl_finalize_kernel(DevTime* tm, int check_running) {
     }
     tm->dt = dt;
     tm->time = nt;
+}
+
+__global__ void cfl_finalize_kernel(DevTime* tm, int check_running) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    cfl_finalize_body(tm, check_running);
+}
+
+// The finalisation for many grids: thread i handles member i.
+__global__ void cfl_finalize_batch_kernel(DevTime* const* __restrict__ tms, int n, int check_running) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cfl_finalize_body(tms[i], check_running);
 }
 
 // MagnetArray construction: cellMag = 0.5*(B + B.shift(component, +1)) (MagnetArray.m:36-38,41-49).

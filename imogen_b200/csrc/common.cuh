@@ -67,6 +67,25 @@ struct DevTime {
     unsigned int pad2;
 };
 
+// ---- batched launches -----------------------------------------------------------------------------
+// A batched launch runs one kernel over the CTAs of many grids ("members"): CTA b of the launch
+// works on block `block` of member `member`, whose own launch would have `nblocks` CTAs.  A
+// member's CTAs are contiguous and start at a multiple of the cluster size.
+struct BlockMap {
+    int member;
+    int block;
+    int nblocks;
+};
+
+// Copy one member's kernel arguments into shared memory (all threads; a barrier follows).
+template <typename Args>
+__device__ __forceinline__ void load_member_args(Args& dst, const Args* src) {
+    static_assert(sizeof(Args) % 4 == 0, "argument blocks are word multiples");
+    const int* s = reinterpret_cast<const int*>(src);
+    int* d = reinterpret_cast<int*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(Args) / 4); i += blockDim.x) d[i] = s[i];
+}
+
 // ---- grid geometry --------------------------------------------------------------------------------
 struct Geom {
     int n[3];

@@ -3,6 +3,7 @@
 
 namespace img {
 template cudaError_t launch_fluid_sweep<float>(const FluidArgs&, const PencilLaunch&, bool);
-template cudaError_t fluid_attributes<float>(int, size_t);
+template cudaError_t launch_fluid_sweep_batch<float>(const FluidArgs*, const BlockMap*, const PencilLaunch&, bool);
+template cudaError_t fluid_attributes<float>(int, int);
 template cudaError_t fluid_max_clusters<float>(const PencilLaunch&, int*);
 }  // namespace img

@@ -3,6 +3,7 @@
 
 namespace img {
 template cudaError_t launch_fluid_sweep<double>(const FluidArgs&, const PencilLaunch&, bool);
-template cudaError_t fluid_attributes<double>(int, size_t);
+template cudaError_t launch_fluid_sweep_batch<double>(const FluidArgs*, const BlockMap*, const PencilLaunch&, bool);
+template cudaError_t fluid_attributes<double>(int, int);
 template cudaError_t fluid_max_clusters<double>(const PencilLaunch&, int*);
 }  // namespace img

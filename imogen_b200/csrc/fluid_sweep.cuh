@@ -183,9 +183,10 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
     }
 }
 
+// One fluid sweep of one grid, run by CTA `vblock` of that grid's launch.
 // FADE: some BC of this sweep direction is fade (compiles the damping in).
 template <typename T, bool MHD, int CPT, bool FADE>
-__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
+__device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
     __shared__ T part[2][MAX_WARPS][33];   // per-warp column maxima (two freezing speeds; rows padded
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
     __shared__ T cpart[2][32];             // per-CTA column maxima, read by the other cluster ranks
     __shared__ double cflp[3][MAX_WARPS];  // per-warp CFL maxima
     Tile<T, CPT> tl;
-    tl.init(a.sg);
+    tl.init(a.sg, vblock);
     const int d = a.sg.d;
     const int NT = a.sg.NT;
     const int Wb = tl.Wb;
@@ -385,6 +386,22 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(cons
             atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
         }
     }
+}
+
+template <typename T, bool MHD, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
+    fluid_sweep_body<T, MHD, CPT, FADE>(a, blockIdx.x);
+}
+
+// The same sweep over many grids in one launch (BlockMap per CTA, arguments per member).
+template <typename T, bool MHD, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_batch_kernel(const FluidArgs* __restrict__ args,
+                                                                                  const BlockMap* __restrict__ map) {
+    __shared__ FluidArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    fluid_sweep_body<T, MHD, CPT, FADE>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

@@ -43,6 +43,24 @@ int pow2ceil(long long v) {
 
 }  // namespace
 
+// One kernel launch of a context, recorded instead of issued while the context steps as a member of
+// a batch (img_batch_*): the batch replays the records of all members as batched launches.
+enum OpKind { OP_FLUID, OP_CHAIN, OP_CT, OP_CELL, OP_CFL_REDUCE, OP_CFL_FINALIZE };
+struct OpRec {
+    int kind;
+    int elem;                 // 4 (mixed) or 8 (FP64)
+    bool mhd;                 // fluid: MHD variant
+    PencilLaunch L;           // pencil kernels: this member's launch shape
+    unsigned blocks;          // pointwise kernels: this member's block count
+    FluidArgs fa;
+    MagArgs ma;
+    CflArgs ca;
+    DevTime* tm;              // cfl finalize
+    int check_running;
+};
+
+struct img_batch;
+
 struct img_ctx {
     img_config cfg{};
     std::string err;
@@ -76,6 +94,9 @@ struct img_ctx {
     bool use_graphs = true;
     DevTime* host_tm = nullptr;  // pinned mirror
     uint64_t launches = 0;       // kernels launched by this context
+    cudaStream_t own_stream = nullptr;   // the context's stream (stream is the batch's while a member)
+    img_batch* batch = nullptr;          // batch this context is a member of
+    std::vector<OpRec>* rec = nullptr;   // set while the batch records this member's launches
 };
 
 namespace {
@@ -274,6 +295,18 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.cfl = cfl;
     const PencilLaunch L = pencil_launch<T>(ctx, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
                                             fade_on(c, d, CLS_MASS, CLS_ENER));
+    if (ctx->rec) {
+        OpRec r{};
+        r.kind = OP_FLUID;
+        r.elem = sizeof(T);
+        r.mhd = ctx->mhd != 0;
+        r.L = L;
+        r.fa = a;
+        ctx->rec->push_back(r);
+        ctx->init_store = false;
+        ctx->init_flux = false;
+        return IMG_OK;
+    }
     cudaError_t le = launch_fluid_sweep<T>(a, L, ctx->mhd != 0);
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "fluid sweep launch (dim %d, grid %u, block %u, smem %zu, cluster %d): %s", d,
@@ -333,6 +366,22 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     const PencilCfg& pcf = ctx->pcfg[d];
     const PencilLaunch L = pencil_launch<T>(ctx, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 2,
                                             fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    if (ctx->rec) {
+        OpRec r{};
+        r.elem = sizeof(T);
+        r.ma = a;
+        r.kind = OP_CHAIN;
+        r.L = L;
+        ctx->rec->push_back(r);
+        r.kind = OP_CT;
+        r.blocks = launch_blocks(ctx->g.ncell);
+        ctx->rec->push_back(r);
+        r.kind = OP_CELL;
+        ctx->rec->push_back(r);
+        ctx->init_mag[I1 - 1][d] = false;
+        ctx->init_mag[I2 - 1][d] = false;
+        return IMG_OK;
+    }
     cudaError_t le = launch_mag_chain<T>(a, L);
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
@@ -355,6 +404,15 @@ int launch_cfl_reduce(img_ctx* ctx) {
     a.gamma = ctx->cfg.gamma;
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
+    if (ctx->rec) {
+        OpRec r{};
+        r.kind = OP_CFL_REDUCE;
+        r.elem = sizeof(T);
+        r.ca = a;
+        r.blocks = launch_blocks(ctx->g.ncell);
+        ctx->rec->push_back(r);
+        return IMG_OK;
+    }
     cfl_reduce_kernel<T><<<launch_blocks(ctx->g.ncell), 256, 0, ctx->stream>>>(a);
     CK(cudaGetLastError());
     ctx->launches += 1;
@@ -365,17 +423,22 @@ int launch_cfl_reduce(img_ctx* ctx) {
 // happens inside a stream capture, and a schedulability check of every pencil configuration.
 template <typename T>
 int set_kernel_attributes(img_ctx* ctx) {
-    for (int cpt : {1, 2, 4}) {
-        size_t fs = 0, ms = 0;
-        for (int d = 0; d < 3; ++d) {
-            const PencilCfg& p = ctx->pcfg[d];
-            if (p.cpt != cpt) continue;
-            fs = std::max(fs, fluid_smem_bytes<T>(p.G * cpt, p.Wb));
-            ms = std::max(ms, mag_smem_bytes<T>(p.G * cpt, p.Wb));
+    // once per device and precision: every pencil kernel may use the opt-in shared memory maximum
+    static std::mutex mu;
+    static bool done[64][2] = {};
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (ctx->dev < 0 || ctx->dev >= 64) return fail(ctx, IMG_ERR_UNSUPPORTED, "device ordinal %d", ctx->dev);
+        bool& dn = done[ctx->dev][sizeof(T) == 8 ? 1 : 0];
+        if (!dn) {
+            int optin = 0;
+            CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->dev));
+            for (int cpt : {1, 2, 4}) {
+                CK(fluid_attributes<T>(cpt, optin));
+                CK(chain_attributes<T>(cpt, optin));
+            }
+            dn = true;
         }
-        // the default dynamic limit is 48 KB minus the static shared memory: always raise it
-        if (fs) CK(fluid_attributes<T>(cpt, fs));
-        if (ms) CK(chain_attributes<T>(cpt, ms));
     }
     for (int d = 0; d < 3; ++d) {
         const PencilCfg& p = ctx->pcfg[d];
@@ -429,6 +492,16 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
     if (!ctx->cfl_valid) {
         int rc = cfl_reduce(ctx);
         if (rc != IMG_OK) return rc;
+    }
+    if (ctx->rec) {
+        OpRec r{};
+        r.kind = OP_CFL_FINALIZE;
+        r.elem = (int)ctx->elem;
+        r.tm = ctx->tm;
+        r.check_running = flux_direction == 1 ? 1 : 0;
+        ctx->rec->push_back(r);
+        ctx->cfl_valid = false;
+        return IMG_OK;
     }
     cfl_finalize_kernel<<<1, 32, 0, ctx->stream>>>(ctx->tm, flux_direction == 1 ? 1 : 0);
     CK(cudaGetLastError());
@@ -601,6 +674,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
         fail(ctx, IMG_ERR_CUDA, "stream creation failed");
         return bail(IMG_ERR_CUDA);
     }
+    ctx->own_stream = ctx->stream;
     Layout L = plan(*cfg);
     ctx->slab_bytes = L.total;
     if (cudaMalloc(&ctx->slab, L.total) != cudaSuccess) {
@@ -664,13 +738,14 @@ int img_create(img_ctx** out, const img_config* cfg) {
 
 int img_destroy(img_ctx* ctx) {
     if (!ctx) return IMG_OK;
+    if (ctx->batch) img_batch_remove(ctx->batch, ctx);
     cudaStreamSynchronize(ctx->stream);
     for (auto& row : ctx->graphs)
         for (auto& gx : row)
             if (gx) cudaGraphExecDestroy(gx);
     if (ctx->slab) cudaFree(ctx->slab);
     if (ctx->host_tm) cudaFreeHost(ctx->host_tm);
-    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return IMG_OK;
 }
@@ -903,6 +978,427 @@ int img_totals(img_ctx* ctx, double out[8]) {
         }
         out[v] = S + C;
     }
+    return IMG_OK;
+}
+
+}  // extern "C"
+
+// ---- batches: many grids advanced by batched launches ------------------------------------------------
+// A batch advances all its member contexts by one iteration per img_batch_step.  The members' own
+// launch sequences are recorded (the same host code as img_step, so every member's kernel
+// arguments are exactly those of its own launches), and launch k of every member becomes part of
+// ONE batched launch (one per group of members that share a launch shape), driven by per-CTA block
+// maps and per-member argument blocks in a device arena.  Steady iterations are captured once per
+// (CFL-valid, sweep-order row) into a CUDA graph and replayed.  Every member keeps its own time
+// step on the device.
+
+struct BatchItem {            // one batched launch
+    int kind = 0, elem = 0;
+    bool mhd = false;
+    PencilLaunch L{};         // pencil kernels: the shared shape; grid_x = CTAs of all members
+    unsigned blocks = 0;      // pointwise kernels: blocks of all members
+    size_t args_off = 0, map_off = 0;
+    int nmembers = 0;
+    int check_running = 0;
+};
+
+struct BatchPlan {            // one recorded iteration of all members
+    std::vector<BatchItem> items;
+    std::vector<unsigned char> host;
+    void* dev = nullptr;
+    size_t cap = 0;
+    cudaGraphExec_t graph = nullptr;
+    void release() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (dev) cudaFree(dev);
+        graph = nullptr;
+        dev = nullptr;
+        cap = 0;
+        items.clear();
+        host.clear();
+    }
+};
+
+struct img_batch {
+    std::string err;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<img_ctx*> members;
+    BatchPlan cached[2][6];
+    BatchPlan transient;
+    uint64_t launches = 0;
+    uint64_t graph_items[2][6] = {};
+    int* status_dev = nullptr;      // gathered done/error flags
+    DevTime** tms_dev = nullptr;
+    size_t status_cap = 0;
+};
+
+namespace {
+
+int bfail(img_batch* b, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (b) b->err = buf;
+    return code;
+}
+
+#define BCK(call)                                                                                  \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return bfail(b, IMG_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+void clear_plans(img_batch* b) {
+    for (auto& row : b->cached)
+        for (auto& p : row) p.release();
+    for (auto& row : b->graph_items)
+        for (auto& n : row) n = 0;
+}
+
+// Members must take the same launch sequence: same precision, physics, swept dimensions, time
+// update mode and iteration.
+bool same_signature(const img_ctx* a, const img_ctx* c) {
+    if (a->elem != c->elem || a->cfg.fluid_active != c->cfg.fluid_active ||
+        a->cfg.magnet_active != c->cfg.magnet_active || a->cfg.update_mode != c->cfg.update_mode ||
+        a->iteration != c->iteration || a->cfl_valid != c->cfl_valid || a->dev != c->dev)
+        return false;
+    for (int d = 0; d < 3; ++d)
+        if ((a->g.n[d] >= 3) != (c->g.n[d] >= 3)) return false;
+    return true;
+}
+
+size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+template <typename V>
+size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
+    size_t off = align16(h.size());
+    h.resize(off + n * sizeof(V));
+    std::memcpy(h.data() + off, v, n * sizeof(V));
+    return off;
+}
+
+bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
+    return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
+           x.cpt == y.cpt && x.fade == y.fade;
+}
+
+// Turn the members' records into batched launch items and the arena image.
+int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchPlan& plan) {
+    plan.items.clear();
+    plan.host.clear();
+    const size_t nops = recs[0].size();
+    const int n = (int)recs.size();
+    for (int m = 1; m < n; ++m)
+        if (recs[m].size() != nops) return bfail(b, IMG_ERR_STATE, "members recorded different launch sequences");
+    std::vector<int> group(n);
+    for (size_t k = 0; k < nops; ++k) {
+        const int kind = recs[0][k].kind;
+        for (int m = 1; m < n; ++m)
+            if (recs[m][k].kind != kind) return bfail(b, IMG_ERR_STATE, "members recorded different launch sequences");
+        // group members by launch shape (pencil kernels) -- first-appearance order
+        std::vector<int> heads;
+        for (int m = 0; m < n; ++m) {
+            int gi = -1;
+            for (int h = 0; h < (int)heads.size() && gi < 0; ++h) {
+                const OpRec& a = recs[heads[h]][k];
+                const OpRec& c = recs[m][k];
+                bool same = a.elem == c.elem && a.mhd == c.mhd;
+                if (kind == OP_FLUID || kind == OP_CHAIN) same = same && same_shape(a.L, c.L);
+                if (kind == OP_CFL_FINALIZE) same = same && a.check_running == c.check_running;
+                if (same) gi = h;
+            }
+            if (gi < 0) {
+                gi = (int)heads.size();
+                heads.push_back(m);
+            }
+            group[m] = gi;
+        }
+        for (int h = 0; h < (int)heads.size(); ++h) {
+            BatchItem it;
+            const OpRec& r0 = recs[heads[h]][k];
+            it.kind = kind;
+            it.elem = r0.elem;
+            it.mhd = r0.mhd;
+            it.L = r0.L;
+            it.check_running = r0.check_running;
+            std::vector<int> mem;
+            for (int m = 0; m < n; ++m)
+                if (group[m] == h) mem.push_back(m);
+            it.nmembers = (int)mem.size();
+            std::vector<BlockMap> map;
+            if (kind == OP_CFL_FINALIZE) {
+                std::vector<DevTime*> tms;
+                for (int m : mem) tms.push_back(recs[m][k].tm);
+                it.args_off = put(plan.host, tms.data(), tms.size());
+            } else {
+                for (int j = 0; j < (int)mem.size(); ++j) {
+                    const OpRec& r = recs[mem[j]][k];
+                    const int nb = (kind == OP_FLUID || kind == OP_CHAIN) ? (int)r.L.grid_x : (int)r.blocks;
+                    for (int blk = 0; blk < nb; ++blk) map.push_back(BlockMap{j, blk, nb});
+                }
+                if (kind == OP_FLUID) {
+                    std::vector<FluidArgs> v;
+                    for (int m : mem) v.push_back(recs[m][k].fa);
+                    it.args_off = put(plan.host, v.data(), v.size());
+                } else if (kind == OP_CFL_REDUCE) {
+                    std::vector<CflArgs> v;
+                    for (int m : mem) v.push_back(recs[m][k].ca);
+                    it.args_off = put(plan.host, v.data(), v.size());
+                } else {
+                    std::vector<MagArgs> v;
+                    for (int m : mem) v.push_back(recs[m][k].ma);
+                    it.args_off = put(plan.host, v.data(), v.size());
+                }
+                it.map_off = put(plan.host, map.data(), map.size());
+                if (kind == OP_FLUID || kind == OP_CHAIN) it.L.grid_x = (unsigned)map.size();
+                else it.blocks = (unsigned)map.size();
+            }
+            it.L.stream = b->stream;
+            plan.items.push_back(it);
+        }
+    }
+    if (plan.host.size() > plan.cap) {
+        if (plan.dev) BCK(cudaFree(plan.dev));
+        plan.dev = nullptr;
+        plan.cap = 0;
+        BCK(cudaMalloc(&plan.dev, plan.host.size()));
+        plan.cap = plan.host.size();
+    }
+    BCK(cudaMemcpyAsync(plan.dev, plan.host.data(), plan.host.size(), cudaMemcpyHostToDevice, b->stream));
+    return IMG_OK;
+}
+
+template <typename T>
+cudaError_t launch_item(const BatchItem& it, const unsigned char* base, cudaStream_t st) {
+    switch (it.kind) {
+        case OP_FLUID:
+            return launch_fluid_sweep_batch<T>(reinterpret_cast<const FluidArgs*>(base + it.args_off),
+                                               reinterpret_cast<const BlockMap*>(base + it.map_off), it.L, it.mhd);
+        case OP_CHAIN:
+            return launch_mag_chain_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
+                                             reinterpret_cast<const BlockMap*>(base + it.map_off), it.L);
+        case OP_CT:
+            return launch_mag_ct_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
+                                          reinterpret_cast<const BlockMap*>(base + it.map_off), it.blocks, st);
+        case OP_CELL:
+            return launch_mag_cell_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
+                                            reinterpret_cast<const BlockMap*>(base + it.map_off), it.blocks, st);
+        case OP_CFL_REDUCE:
+            cfl_reduce_batch_kernel<T><<<it.blocks, 256, 0, st>>>(reinterpret_cast<const CflArgs*>(base + it.args_off),
+                                                                 reinterpret_cast<const BlockMap*>(base + it.map_off));
+            return cudaGetLastError();
+        default:
+            cfl_finalize_batch_kernel<<<(it.nmembers + 127) / 128, 128, 0, st>>>(
+                reinterpret_cast<DevTime* const*>(base + it.args_off), it.nmembers, it.check_running);
+            return cudaGetLastError();
+    }
+}
+
+int launch_plan(img_batch* b, const BatchPlan& plan) {
+    const unsigned char* base = static_cast<const unsigned char*>(plan.dev);
+    for (const BatchItem& it : plan.items) {
+        cudaError_t e = it.elem == 8 ? launch_item<double>(it, base, b->stream) : launch_item<float>(it, base, b->stream);
+        if (e != cudaSuccess)
+            return bfail(b, IMG_ERR_CUDA, "batched launch (kind %d, %d members, grid %u): %s", it.kind, it.nmembers,
+                         it.kind == OP_FLUID || it.kind == OP_CHAIN ? it.L.grid_x : it.blocks, cudaGetErrorString(e));
+    }
+    return IMG_OK;
+}
+
+__global__ void batch_status_kernel(DevTime* const* __restrict__ tms, int n, int* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (tms[i]->done ? 1 : 0) | (tms[i]->error ? 2 : 0);
+}
+
+}  // namespace
+
+extern "C" {
+
+int img_batch_create(img_batch** out) {
+    if (!out) return IMG_ERR_ARG;
+    *out = nullptr;
+    img_batch* b = new img_batch();
+    if (cudaGetDevice(&b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return IMG_ERR_CUDA;
+    }
+    *out = b;
+    return IMG_OK;
+}
+
+static void batch_detach(img_batch* b, img_ctx* m) {
+    cudaStreamSynchronize(b->stream);
+    m->stream = m->own_stream;
+    m->batch = nullptr;
+}
+
+int img_batch_destroy(img_batch* b) {
+    if (!b) return IMG_OK;
+    cudaStreamSynchronize(b->stream);
+    for (img_ctx* m : b->members) batch_detach(b, m);
+    clear_plans(b);
+    b->transient.release();
+    if (b->status_dev) cudaFree(b->status_dev);
+    if (b->tms_dev) cudaFree(b->tms_dev);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return IMG_OK;
+}
+
+const char* img_batch_last_error(const img_batch* b) { return b ? b->err.c_str() : ""; }
+
+int img_batch_add(img_batch* b, img_ctx* ctx) {
+    if (!b || !ctx) return bfail(b, IMG_ERR_ARG, "null argument");
+    if (!ctx->state_set) return bfail(b, IMG_ERR_STATE, "member state not set");
+    if (ctx->batch) return bfail(b, IMG_ERR_STATE, "context is already a batch member");
+    if (ctx->dev != b->dev) return bfail(b, IMG_ERR_ARG, "member is on device %d, batch on %d", ctx->dev, b->dev);
+    if (!b->members.empty() && !same_signature(b->members[0], ctx))
+        return bfail(b, IMG_ERR_ARG, "member differs from the batch in precision, physics, swept dimensions, "
+                     "time update mode or iteration");
+    BCK(cudaStreamSynchronize(ctx->own_stream));
+    ctx->stream = b->stream;
+    ctx->batch = b;
+    b->members.push_back(ctx);
+    clear_plans(b);
+    return IMG_OK;
+}
+
+int img_batch_remove(img_batch* b, img_ctx* ctx) {
+    if (!b || !ctx || ctx->batch != b) return bfail(b, IMG_ERR_ARG, "not a member of this batch");
+    batch_detach(b, ctx);
+    b->members.erase(std::find(b->members.begin(), b->members.end(), ctx));
+    clear_plans(b);
+    return IMG_OK;
+}
+
+int img_batch_size(const img_batch* b, int* n) {
+    if (!b || !n) return IMG_ERR_ARG;
+    *n = (int)b->members.size();
+    return IMG_OK;
+}
+
+int img_batch_step(img_batch* b) {
+    if (!b) return IMG_ERR_ARG;
+    if (b->members.empty()) return bfail(b, IMG_ERR_STATE, "empty batch");
+    img_ctx* m0 = b->members[0];
+    for (img_ctx* m : b->members)
+        if (m->iteration != m0->iteration || m->cfl_valid != m0->cfl_valid)
+            return bfail(b, IMG_ERR_STATE, "members out of step (a member was advanced on its own)");
+    // members past ITERMAX stop (imogen.m:58): their kernels return at once from now on
+    static const int one = 1;
+    for (img_ctx* m : b->members)
+        if (m->iteration > m->cfg.iter_max)
+            BCK(cudaMemcpyAsync(&m->tm->done, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    const int row = (m0->iteration - 1) % 6;
+    const int cv = m0->cfl_valid ? 1 : 0;
+    bool st = true;
+    for (img_ctx* m : b->members) st = st && steady(m);
+    BatchPlan& cp = b->cached[cv][row];
+    if (st && cp.graph) {
+        BCK(cudaGraphLaunch(cp.graph, b->stream));
+        b->launches += b->graph_items[cv][row];
+        for (img_ctx* m : b->members) {
+            m->cfl_valid = m->cfg.update_mode != 0 && m->cfg.fluid_active;
+            m->iteration += 1;
+        }
+        return IMG_OK;
+    }
+    std::vector<std::vector<OpRec>> recs(b->members.size());
+    for (size_t i = 0; i < b->members.size(); ++i) {
+        img_ctx* m = b->members[i];
+        m->rec = &recs[i];
+        int rc = enqueue_iteration(m);
+        m->rec = nullptr;
+        if (rc != IMG_OK) return bfail(b, rc, "member %zu: %s", i, m->err.c_str());
+    }
+    BatchPlan& plan = st ? cp : b->transient;
+    if (!st) BCK(cudaStreamSynchronize(b->stream));   // the transient arena may still be in use
+    int rc = build_plan(b, recs, plan);
+    if (rc != IMG_OK) return rc;
+    if (st) {
+        BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        rc = launch_plan(b, plan);
+        cudaGraph_t graph = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(b->stream, &graph);
+        if (rc != IMG_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return bfail(b, IMG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&plan.graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return bfail(b, IMG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+        b->graph_items[cv][row] = plan.items.size();
+        BCK(cudaGraphLaunch(plan.graph, b->stream));
+    } else {
+        rc = launch_plan(b, plan);
+        if (rc != IMG_OK) return rc;
+    }
+    b->launches += plan.items.size();
+    for (img_ctx* m : b->members) m->iteration += 1;
+    return IMG_OK;
+}
+
+// Done/error flags of every member (bit 0: stopped, bit 1: error), after a stream sync.
+int img_batch_status(img_batch* b, int* flags, int n) {
+    if (!b || !flags || n != (int)b->members.size()) return bfail(b, IMG_ERR_ARG, "bad status buffer");
+    if (n == 0) return IMG_OK;
+    if ((size_t)n > b->status_cap) {
+        if (b->status_dev) cudaFree(b->status_dev);
+        if (b->tms_dev) cudaFree(b->tms_dev);
+        b->status_dev = nullptr;
+        b->tms_dev = nullptr;
+        b->status_cap = 0;
+        BCK(cudaMalloc(&b->status_dev, sizeof(int) * n));
+        BCK(cudaMalloc(&b->tms_dev, sizeof(DevTime*) * n));
+        b->status_cap = n;
+    }
+    std::vector<DevTime*> tms;
+    for (img_ctx* m : b->members) tms.push_back(m->tm);
+    BCK(cudaMemcpyAsync(b->tms_dev, tms.data(), sizeof(DevTime*) * n, cudaMemcpyHostToDevice, b->stream));
+    batch_status_kernel<<<(n + 127) / 128, 128, 0, b->stream>>>(b->tms_dev, n, b->status_dev);
+    BCK(cudaGetLastError());
+    BCK(cudaMemcpyAsync(flags, b->status_dev, sizeof(int) * n, cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; ++i)
+        if (b->members[i]->iteration > b->members[i]->cfg.iter_max) flags[i] |= 1;
+    return IMG_OK;
+}
+
+int img_batch_run(img_batch* b, int max_iters, int check_every, int* iters_done) {
+    if (!b) return IMG_ERR_ARG;
+    if (check_every < 1) check_every = 1;
+    std::vector<int> flags(b->members.size());
+    int n = 0, rc;
+    while (max_iters < 0 || n < max_iters) {
+        if (n % check_every == 0) {
+            if ((rc = img_batch_status(b, flags.data(), (int)flags.size())) != IMG_OK) return rc;
+            bool all = true;
+            for (int f : flags) all = all && (f & 1 || f & 2);
+            if (all) break;
+        }
+        if ((rc = img_batch_step(b)) != IMG_OK) return rc;
+        ++n;
+    }
+    if ((rc = img_batch_status(b, flags.data(), (int)flags.size())) != IMG_OK) return rc;
+    if (iters_done) *iters_done = n;
+    for (size_t i = 0; i < flags.size(); ++i)
+        if (flags[i] & 2) return bfail(b, IMG_ERR_CFL, "member %zu stopped with a time-step error", i);
+    return IMG_OK;
+}
+
+int img_batch_get_stream(img_batch* b, void** stream) {
+    if (!b || !stream) return IMG_ERR_ARG;
+    *stream = (void*)b->stream;
+    return IMG_OK;
+}
+
+int img_batch_launch_count(const img_batch* b, uint64_t* count) {
+    if (!b || !count) return IMG_ERR_ARG;
+    *count = b->launches;
     return IMG_OK;
 }
 

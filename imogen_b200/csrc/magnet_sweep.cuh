@@ -142,13 +142,14 @@ __device__ __forceinline__ double wmag_upper_ghosts(const Tile<T, CPT>& tl, cons
     return e4;
 }
 
+// The chain of one grid, run by CTA (vblock, blockIdx.y) of that grid's launch.
 // FADE: a mag-class BC along X is fade (compiles the damping in).
 template <typename T, int CPT, bool FADE>
-__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
+__device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
     Tile<T, CPT> tl;
-    tl.init(a.sg);
+    tl.init(a.sg, vblock);
     const int q = blockIdx.y;          // which transverse component
     const int I = q ? a.I[1] : a.I[0];
     const int shiftI = q ? a.shiftI[1] : a.shiftI[0];
@@ -387,8 +388,9 @@ __device__ __forceinline__ T ct_difference(const MagArgs& a, int q, long long ce
 }
 
 // B_X' = (B_X - dt/dI1 * D_I1) - dt/dI2 * D_I2 -> scratch; cell-centred B of I2 (the last component).
+// Run by block vblock of vgrid blocks of one grid's launch.
 template <typename T>
-__global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
+__device__ __forceinline__ void mag_ct_body(const MagArgs& a, unsigned vblock, unsigned vgrid) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const double dt = a.tm->dt;
@@ -399,8 +401,8 @@ __global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
     const int I2 = a.I[1], e2 = I2 - 1;
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
     T* CB2 = reinterpret_cast<T*>(a.q[Q_CBX + e2]);
-    for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
-         cell += (long long)gridDim.x * blockDim.x) {
+    for (long long cell = vblock * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
+         cell += (long long)vgrid * blockDim.x) {
         int x, y, z;
         cell_coords(g, cell, x, y, z);
         const T D0 = ct_difference<T>(a, 0, cell, x, y, z);
@@ -420,17 +422,17 @@ __global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
 
 // B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1)); and the drift of the I-direction
 // trans edges of both flux objects (the C_I = F_I - F_I.shift(I,+1) calls of mag_ct), stored by
-// the thread of each upper face cell.
+// the thread of each upper face cell.  Run by block vblock of vgrid blocks of one grid's launch.
 template <typename T>
-__global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
+__device__ __forceinline__ void mag_cell_body(const MagArgs& a, unsigned vblock, unsigned vgrid) {
     if (a.tm->done || a.tm->error) return;
     const Geom& g = a.sg.g;
     const int X = a.X, d = X - 1;
     const T* BXn = reinterpret_cast<const T*>(a.BXn);
     T* BX = reinterpret_cast<T*>(a.q[Q_BX + d]);
     T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
-    for (long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
-         cell += (long long)gridDim.x * blockDim.x) {
+    for (long long cell = vblock * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
+         cell += (long long)vgrid * blockDim.x) {
         int x, y, z;
         cell_coords(g, cell, x, y, z);
         bool own = sel3(d, x, y, z) == sel3(d, g.n[0], g.n[1], g.n[2]) - 1;
@@ -451,6 +453,50 @@ __global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
             edge[fi] = edge_drift(edge[fi], (double)F[cell]);
         }
     }
+}
+
+template <typename T, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
+    mag_chain_body<T, CPT, FADE>(a, blockIdx.x);
+}
+
+template <typename T>
+__global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
+    mag_ct_body<T>(a, blockIdx.x, gridDim.x);
+}
+
+template <typename T>
+__global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
+    mag_cell_body<T>(a, blockIdx.x, gridDim.x);
+}
+
+// The same passes over many grids in one launch (BlockMap per CTA, arguments per member).
+template <typename T, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_batch_kernel(const MagArgs* __restrict__ args,
+                                                                                const BlockMap* __restrict__ map) {
+    __shared__ MagArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    mag_chain_body<T, CPT, FADE>(sa, (unsigned)bm.block);
+}
+
+template <typename T>
+__global__ void mag_ct_batch_kernel(const MagArgs* __restrict__ args, const BlockMap* __restrict__ map) {
+    __shared__ MagArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    mag_ct_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
+}
+
+template <typename T>
+__global__ void mag_cell_batch_kernel(const MagArgs* __restrict__ args, const BlockMap* __restrict__ map) {
+    __shared__ MagArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    mag_cell_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
 }
 
 }  // namespace img

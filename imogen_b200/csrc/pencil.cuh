@@ -62,7 +62,8 @@ struct Tile {
     long long sd;         // stride along the sweep
     int n1;
 
-    __device__ __forceinline__ void init(const SweepGeom& s) {
+    // vblock: this CTA's block index within its grid's launch (blockIdx.x for a single launch)
+    __device__ __forceinline__ void init(const SweepGeom& s, unsigned vblock) {
         const int t = threadIdx.x;
         N = s.N;
         Wb = s.Wb;
@@ -75,8 +76,8 @@ struct Tile {
         n1 = s.n1;
         if (s.d == 0) { g = t % s.G; b = t / s.G; }
         else { b = t % s.Wb; g = t / s.Wb; }
-        rank = (int)(blockIdx.x & (unsigned)(s.CL - 1));   // CL is a power of two
-        const long long bundle = blockIdx.x / (unsigned)s.CL;
+        rank = (int)(vblock & (unsigned)(s.CL - 1));   // CL is a power of two
+        const long long bundle = vblock / (unsigned)s.CL;
         row0 = rank * s.RC + g;
         ix0 = (g + HALO_LO) * s.Wb + b;
         col = bundle * s.Wb + b;

@@ -6,6 +6,29 @@
 
 namespace img {
 
+inline cudaLaunchConfig_t pencil_config(const PencilLaunch& L, cudaLaunchAttribute* attr) {
+    cudaLaunchConfig_t lc{};
+    lc.gridDim = dim3(L.grid_x, L.grid_y);
+    lc.blockDim = dim3(L.block);
+    lc.dynamicSmemBytes = L.smem;
+    lc.stream = L.stream;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    lc.attrs = attr;
+    lc.numAttrs = 1;
+    return lc;
+}
+
+template <typename Args>
+cudaError_t launch_pencil_batch(void (*kern)(const Args*, const BlockMap*), const Args* args, const BlockMap* map,
+                                const PencilLaunch& L) {
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t lc = pencil_config(L, attr);
+    return cudaLaunchKernelEx(&lc, kern, args, map);
+}
+
 template <typename Args>
 cudaError_t launch_pencil(void (*kern)(const Args), const Args& a, const PencilLaunch& L) {
     cudaLaunchConfig_t lc{};
@@ -41,6 +64,53 @@ void (*chain_kernel(int cpt))(const MagArgs) {
     }
 }
 
+template <typename T, bool MHD, bool FADE>
+void (*fluid_batch_kernel(int cpt))(const FluidArgs*, const BlockMap*) {
+    switch (cpt) {
+        case 1: return fluid_sweep_batch_kernel<T, MHD, 1, FADE>;
+        case 2: return fluid_sweep_batch_kernel<T, MHD, 2, FADE>;
+        default: return fluid_sweep_batch_kernel<T, MHD, 4, FADE>;
+    }
+}
+
+template <typename T, bool FADE>
+void (*chain_batch_kernel(int cpt))(const MagArgs*, const BlockMap*) {
+    switch (cpt) {
+        case 1: return mag_chain_batch_kernel<T, 1, FADE>;
+        case 2: return mag_chain_batch_kernel<T, 2, FADE>;
+        default: return mag_chain_batch_kernel<T, 4, FADE>;
+    }
+}
+
+template <typename T>
+void (*fluid_batch_kernel(int cpt, bool mhd, bool fade))(const FluidArgs*, const BlockMap*) {
+    if (mhd) return fade ? fluid_batch_kernel<T, true, true>(cpt) : fluid_batch_kernel<T, true, false>(cpt);
+    return fade ? fluid_batch_kernel<T, false, true>(cpt) : fluid_batch_kernel<T, false, false>(cpt);
+}
+
+template <typename T>
+cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
+    return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, L.fade), args, map, L);
+}
+
+template <typename T>
+cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
+    return launch_pencil_batch(L.fade ? chain_batch_kernel<T, true>(L.cpt) : chain_batch_kernel<T, false>(L.cpt), args,
+                               map, L);
+}
+
+template <typename T>
+cudaError_t launch_mag_ct_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream) {
+    mag_ct_batch_kernel<T><<<blocks, 256, 0, stream>>>(args, map);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_mag_cell_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream) {
+    mag_cell_batch_kernel<T><<<blocks, 256, 0, stream>>>(args, map);
+    return cudaGetLastError();
+}
+
 template <typename T>
 void (*fluid_kernel(int cpt, bool mhd, bool fade))(const FluidArgs) {
     if (mhd) return fade ? fluid_kernel<T, true, true>(cpt) : fluid_kernel<T, true, false>(cpt);
@@ -69,21 +139,32 @@ cudaError_t launch_mag_cell(const MagArgs& a, unsigned blocks, cudaStream_t stre
     return cudaGetLastError();
 }
 
+// Allow a kernel the device's whole opt-in shared memory per block (minus its static shared
+// memory).  The attribute belongs to the kernel, not to a launch, so it is raised to the maximum
+// once instead of to one context's need (a smaller later value would break earlier contexts).
+template <typename K>
+cudaError_t allow_max_smem(K kern, int optin) {
+    cudaFuncAttributes fa{};
+    cudaError_t e = cudaFuncGetAttributes(&fa, kern);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+}
+
 template <typename T>
-cudaError_t fluid_attributes(int cpt, size_t smem) {
+cudaError_t fluid_attributes(int cpt, int optin) {
     for (int v = 0; v < 4; ++v) {
-        cudaError_t e = cudaFuncSetAttribute(fluid_kernel<T>(cpt, v & 1, v >> 1),
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_max_smem(fluid_kernel<T>(cpt, v & 1, v >> 1), optin);
+        if (e == cudaSuccess) e = allow_max_smem(fluid_batch_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
 template <typename T>
-cudaError_t chain_attributes(int cpt, size_t smem) {
+cudaError_t chain_attributes(int cpt, int optin) {
     for (int v = 0; v < 2; ++v) {
-        cudaError_t e = cudaFuncSetAttribute(v ? chain_kernel<T, true>(cpt) : chain_kernel<T, false>(cpt),
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = allow_max_smem(v ? chain_kernel<T, true>(cpt) : chain_kernel<T, false>(cpt), optin);
+        if (e == cudaSuccess) e = allow_max_smem(v ? chain_batch_kernel<T, true>(cpt) : chain_batch_kernel<T, false>(cpt), optin);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ImgConfig, check, lib
+from ._lib import ImgConfig, ImogenError, check, lib
 
 BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall")      # enums/ENUM.m:22-31
 LIMITERS = {"vanleer": 0, "superbee": 1, "minmond": 2, "minmod": 2}   # FluxLimiterEnum.m:10-13
@@ -258,6 +258,80 @@ class ImogenRun:
         out = np.zeros(8)
         check(lib().img_totals_static(self._h, _dp(out)), self._h)
         return out
+
+
+class ImogenBatch:
+    """Many runs advanced together by batched launches (img_batch_*): one iteration of every member
+    per step, each member with its own time step; members stay ImogenRun objects (upload,
+    download, totals work on them as usual)."""
+
+    def __init__(self, members=()):
+        h = ctypes.c_void_p()
+        rc = lib().img_batch_create(ctypes.byref(h))
+        if rc != 0:
+            raise ImogenError(rc, "batch creation failed")
+        self._h = h
+        self.members = []
+        for m in members:
+            self.add(m)
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().img_batch_last_error(self._h)
+            raise ImogenError(rc, msg.decode() if msg else "")
+
+    def add(self, run):
+        self._check(lib().img_batch_add(self._h, run._h))
+        self.members.append(run)
+
+    def remove(self, run):
+        self._check(lib().img_batch_remove(self._h, run._h))
+        self.members.remove(run)
+
+    def step(self):
+        self._check(lib().img_batch_step(self._h))
+
+    def run(self, max_iterations=None, check_every=8):
+        n = ctypes.c_int()
+        self._check(lib().img_batch_run(self._h, -1 if max_iterations is None else int(max_iterations),
+                                        int(check_every), ctypes.byref(n)))
+        return n.value
+
+    def status(self):
+        """Per member: bit 0 stopped (TIMEMAX/ITERMAX), bit 1 error."""
+        f = (ctypes.c_int * len(self.members))()
+        self._check(lib().img_batch_status(self._h, f, len(self.members)))
+        return list(f)
+
+    @property
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._check(lib().img_batch_get_stream(self._h, ctypes.byref(s)))
+        return s.value or 0
+
+    @property
+    def launches(self):
+        n = ctypes.c_uint64()
+        self._check(lib().img_batch_launch_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().img_batch_destroy(self._h)
+            self._h = None
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 # ---- reference call surface ------------------------------------------------------------------------

@@ -138,6 +138,30 @@ int img_get_stream(img_ctx* ctx, void** stream);
 /* Number of kernels the context has launched so far.  No reference counterpart. */
 int img_launch_count(const img_ctx* ctx, uint64_t* count);
 
+/* ---- batches: many grids, one batched launch per kernel --------------------------------------- */
+/* A batch advances member contexts together: img_batch_step runs one iteration (imogen.m:58-72) of
+ * every member, each with its own time step, issuing each kernel of the iteration as ONE launch
+ * over all members that share its launch shape; steady iterations are replayed from a CUDA graph.
+ * Members keep their state and stay usable on their own (upload/download/totals); while in a batch
+ * their work runs on the batch's stream.  Members must agree in precision, physics (fluid/magnet),
+ * the dimensions that are swept (extent >= 3), the time update mode and the current iteration.
+ * No reference counterpart: the reference advances one grid per MATLAB session. */
+typedef struct img_batch img_batch;
+int img_batch_create(img_batch** out);
+int img_batch_destroy(img_batch* b);                  /* members leave the batch; they are not destroyed */
+int img_batch_add(img_batch* b, img_ctx* member);
+int img_batch_remove(img_batch* b, img_ctx* member);  /* also done by img_destroy(member) */
+int img_batch_size(const img_batch* b, int* n);
+int img_batch_step(img_batch* b);                     /* asynchronous */
+/* Step until every member has stopped (TIMEMAX reached, ITERMAX passed, or an error), checking the
+ * members' flags every check_every iterations; at most max_iters iterations (-1: no cap). */
+int img_batch_run(img_batch* b, int max_iters, int check_every, int* iters_done);
+/* flags[i] of member i (in order of addition): bit 0 stopped, bit 1 error.  Synchronises. */
+int img_batch_status(img_batch* b, int* flags, int n);
+int img_batch_get_stream(img_batch* b, void** stream);
+int img_batch_launch_count(const img_batch* b, uint64_t* count);
+const char* img_batch_last_error(const img_batch* b);
+
 #ifdef __cplusplus
 }
 #endif
