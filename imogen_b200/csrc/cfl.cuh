@@ -83,6 +83,7 @@ __device__ __forceinline__ void cfl_finalize_body(DevTime* tm, int check_running
         tm->done = 1;
         return;
     }
+    if (check_running) tm->iters_run += 1;
     double cmax = 1e-2;
     int gi = 0;
     for (int i = 0; i < 3; ++i) {

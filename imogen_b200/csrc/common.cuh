@@ -60,7 +60,7 @@ struct DevTime {
     int update_mode;        // 0 per step, 1 per iteration
     int error;              // DevError bits
     int done;               // TimeManager.running turned false (time >= TIMEMAX)
-    int reserved0;
+    int iters_run;          // iterations that started (TimeManager.running was true at their top)
     int reserved1;
     unsigned long long maxbits[3];   // per-direction max of |v_i| + c_s (bit pattern, >= 0)
     unsigned int counter;            // CTAs finished in the current CFL reduction

@@ -947,10 +947,20 @@ int img_set_time(img_ctx* ctx, double time, double dt, int iteration) {
     ctx->host_tm->dt = dt;
     ctx->host_tm->done = 0;
     ctx->host_tm->error = 0;
+    ctx->host_tm->iters_run = iteration - 1;
     CK(cudaMemcpyAsync(ctx->tm, ctx->host_tm, sizeof(DevTime), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->iteration = iteration;
     return IMG_OK;
+}
+
+int img_progress(img_ctx* ctx, double* time, int* iterations_run, int* stopped) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    int rc = check_dev_error(ctx);
+    if (time) *time = ctx->host_tm->time;
+    if (iterations_run) *iterations_run = ctx->host_tm->iters_run;
+    if (stopped) *stopped = ctx->host_tm->done || ctx->iteration > ctx->cfg.iter_max;
+    return rc;
 }
 
 int img_totals(img_ctx* ctx, double out[8]) {
@@ -1024,10 +1034,14 @@ struct img_batch {
     int dev = 0;
     cudaStream_t stream = nullptr;
     std::vector<img_ctx*> members;
-    BatchPlan cached[2][6];
-    BatchPlan transient;
+    // Steady plans by phase: every member's sweep-order row advances by one per step, so with fixed
+    // membership the batch's launch sequence repeats every 6 steps.  Membership changes clear them.
+    BatchPlan cached[6];
+    BatchPlan transient[4];          // ring of arenas for plans launched once
+    cudaEvent_t transient_done[4] = {};
+    int next_transient = 0;
+    uint64_t steps = 0;             // steps since the membership last changed
     uint64_t launches = 0;
-    uint64_t graph_items[2][6] = {};
     int* status_dev = nullptr;      // gathered done/error flags
     DevTime** tms_dev = nullptr;
     size_t status_cap = 0;
@@ -1052,18 +1066,17 @@ int bfail(img_batch* b, int code, const char* fmt, ...) {
     } while (0)
 
 void clear_plans(img_batch* b) {
-    for (auto& row : b->cached)
-        for (auto& p : row) p.release();
-    for (auto& row : b->graph_items)
-        for (auto& n : row) n = 0;
+    for (auto& p : b->cached) p.release();
+    b->steps = 0;
 }
 
-// Members must take the same launch sequence: same precision, physics, swept dimensions, time
-// update mode and iteration.
+// Members must issue the same kinds of launches in the same order: same precision, physics, swept
+// dimensions and time update mode (their sweep directions may differ: members that joined at
+// other iterations sit at other rows of the sweep-order table, and go to other launch groups).
 bool same_signature(const img_ctx* a, const img_ctx* c) {
     if (a->elem != c->elem || a->cfg.fluid_active != c->cfg.fluid_active ||
         a->cfg.magnet_active != c->cfg.magnet_active || a->cfg.update_mode != c->cfg.update_mode ||
-        a->iteration != c->iteration || a->cfl_valid != c->cfl_valid || a->dev != c->dev)
+        a->dev != c->dev)
         return false;
     for (int d = 0; d < 3; ++d)
         if ((a->g.n[d] >= 3) != (c->g.n[d] >= 3)) return false;
@@ -1240,7 +1253,10 @@ int img_batch_destroy(img_batch* b) {
     cudaStreamSynchronize(b->stream);
     for (img_ctx* m : b->members) batch_detach(b, m);
     clear_plans(b);
-    b->transient.release();
+    for (int i = 0; i < 4; ++i) {
+        b->transient[i].release();
+        if (b->transient_done[i]) cudaEventDestroy(b->transient_done[i]);
+    }
     if (b->status_dev) cudaFree(b->status_dev);
     if (b->tms_dev) cudaFree(b->tms_dev);
     cudaStreamDestroy(b->stream);
@@ -1283,27 +1299,23 @@ int img_batch_size(const img_batch* b, int* n) {
 int img_batch_step(img_batch* b) {
     if (!b) return IMG_ERR_ARG;
     if (b->members.empty()) return bfail(b, IMG_ERR_STATE, "empty batch");
-    img_ctx* m0 = b->members[0];
-    for (img_ctx* m : b->members)
-        if (m->iteration != m0->iteration || m->cfl_valid != m0->cfl_valid)
-            return bfail(b, IMG_ERR_STATE, "members out of step (a member was advanced on its own)");
     // members past ITERMAX stop (imogen.m:58): their kernels return at once from now on
     static const int one = 1;
     for (img_ctx* m : b->members)
         if (m->iteration > m->cfg.iter_max)
             BCK(cudaMemcpyAsync(&m->tm->done, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    const int row = (m0->iteration - 1) % 6;
-    const int cv = m0->cfl_valid ? 1 : 0;
     bool st = true;
-    for (img_ctx* m : b->members) st = st && steady(m);
-    BatchPlan& cp = b->cached[cv][row];
+    for (img_ctx* m : b->members) st = st && steady(m) && m->cfl_valid == b->members[0]->cfl_valid;
+    const int phase = (int)(b->steps % 6);
+    BatchPlan& cp = b->cached[phase];
     if (st && cp.graph) {
         BCK(cudaGraphLaunch(cp.graph, b->stream));
-        b->launches += b->graph_items[cv][row];
+        b->launches += cp.items.size();
         for (img_ctx* m : b->members) {
             m->cfl_valid = m->cfg.update_mode != 0 && m->cfg.fluid_active;
             m->iteration += 1;
         }
+        b->steps += 1;
         return IMG_OK;
     }
     std::vector<std::vector<OpRec>> recs(b->members.size());
@@ -1314,11 +1326,19 @@ int img_batch_step(img_batch* b) {
         m->rec = nullptr;
         if (rc != IMG_OK) return bfail(b, rc, "member %zu: %s", i, m->err.c_str());
     }
-    BatchPlan& plan = st ? cp : b->transient;
-    if (!st) BCK(cudaStreamSynchronize(b->stream));   // the transient arena may still be in use
+    // a steady plan is kept (and captured as a graph) from the second cycle of a membership on,
+    // so that a batch whose members change often does not pay for captures it never replays
+    const bool keep = st && b->steps >= 6;
+    const int tr = b->next_transient;
+    BatchPlan& plan = keep ? cp : b->transient[tr];
+    if (!keep) {   // wait until this arena's previous launches have finished with it
+        if (!b->transient_done[tr]) BCK(cudaEventCreateWithFlags(&b->transient_done[tr], cudaEventDisableTiming));
+        else BCK(cudaEventSynchronize(b->transient_done[tr]));
+        b->next_transient = (tr + 1) % 4;
+    }
     int rc = build_plan(b, recs, plan);
     if (rc != IMG_OK) return rc;
-    if (st) {
+    if (keep) {
         BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
         rc = launch_plan(b, plan);
         cudaGraph_t graph = nullptr;
@@ -1331,14 +1351,15 @@ int img_batch_step(img_batch* b) {
         ce = cudaGraphInstantiate(&plan.graph, graph, 0);
         cudaGraphDestroy(graph);
         if (ce != cudaSuccess) return bfail(b, IMG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-        b->graph_items[cv][row] = plan.items.size();
         BCK(cudaGraphLaunch(plan.graph, b->stream));
     } else {
         rc = launch_plan(b, plan);
         if (rc != IMG_OK) return rc;
+        BCK(cudaEventRecord(b->transient_done[tr], b->stream));
     }
     b->launches += plan.items.size();
     for (img_ctx* m : b->members) m->iteration += 1;
+    b->steps += 1;
     return IMG_OK;
 }
 

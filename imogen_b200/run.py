@@ -247,6 +247,12 @@ class ImogenRun:
         check(lib().img_launch_count(self._h, ctypes.byref(n)), self._h)
         return n.value
 
+    def progress(self):
+        """(simulated time, iterations run, stopped) from the device clock (synchronises)."""
+        t, n, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        check(lib().img_progress(self._h, ctypes.byref(t), ctypes.byref(n), ctypes.byref(st)), self._h)
+        return t.value, n.value, bool(st.value)
+
     def totals(self):
         """Neumaier-compensated FP64 sums of rho, px, py, pz, E, Bx, By, Bz."""
         out = np.zeros(8)

@@ -110,6 +110,11 @@ int img_get_time(img_ctx* ctx, double* time, double* dt, int* iteration);
 /* Overwrite the time manager state (time, dt, iteration). */
 int img_set_time(img_ctx* ctx, double time, double dt, int iteration);
 
+/* Simulated time, iterations that have run (TimeManager.running was true at their top), and whether
+ * the run has stopped (TIMEMAX reached or ITERMAX passed).  Synchronises.  No reference counterpart
+ * (the reference reads run.time and run.time.iteration). */
+int img_progress(img_ctx* ctx, double* time, int* iterations_run, int* stopped);
+
 /* Compensated (Neumaier) FP64 totals of rho, px, py, pz, E, Bx, By, Bz over the grid. */
 int img_totals(img_ctx* ctx, double out[8]);
 
@@ -144,7 +149,9 @@ int img_launch_count(const img_ctx* ctx, uint64_t* count);
  * over all members that share its launch shape; steady iterations are replayed from a CUDA graph.
  * Members keep their state and stay usable on their own (upload/download/totals); while in a batch
  * their work runs on the batch's stream.  Members must agree in precision, physics (fluid/magnet),
- * the dimensions that are swept (extent >= 3), the time update mode and the current iteration.
+ * the dimensions that are swept (extent >= 3) and the time update mode; they may sit at different
+ * iterations, but must issue the same kinds of launches: a member joins after its first iteration
+ * (which captures its stored edges) or all members start together.
  * No reference counterpart: the reference advances one grid per MATLAB session. */
 typedef struct img_batch img_batch;
 int img_batch_create(img_batch** out);
