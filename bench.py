@@ -297,6 +297,9 @@ def run_ours(args):
            "h2d_bytes_per_step": 8 * ncell * 8, "d2h_bytes_per_step": 8 * ncell * 8,
            "form": "mixed", "steps": ke}
 
+    serving = run_serving(args) if args.serve_jobs > 0 else None
+    ensemble = run_ensemble(args, timed_steps) if args.ensemble > 0 else None
+
     if rank == 0:
         v = ncell * 2 * args.steps * ws / results["mixed"]
         v64 = ncell * 2 * args.steps * ws / results["fp64"]
@@ -317,7 +320,11 @@ def run_ours(args):
             "gpu_launches": launches["mixed"],
             "clocks": clk,
             "e2e": e2e,
-            "p50_p99_job_latency": None,
+            "p50_p99_job_latency": None if serving is None else
+            {"p50_s": serving["served_mixed"]["p50_s"], "p99_s": serving["served_mixed"]["p99_s"],
+             "unit": "s", "workload": serving["workload"]},
+            "serving": serving,
+            "ensemble": ensemble,
         }
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(s, st, wname, budget_s=args.cpu_budget)
@@ -326,6 +333,65 @@ def run_ours(args):
         r.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_serving(args):
+    """Poisson stream of Sedov-Taylor jobs: the continuous-batching server (mixed form) against the
+    same jobs one at a time in plain FP64.  Latency = completion - arrival, wall clock."""
+    from imogen_b200 import serve
+    jobs = serve.sedov_stream(args.serve_jobs, rate=50.0, seed=0, precision="mixed")
+    t0 = time.perf_counter()
+    done = serve.Server(hbm_budget=args.serve_budget_gb << 30, check_every=4, keep="totals").serve(jobs)
+    el = time.perf_counter() - t0
+    a = serve.latency_summary(done)
+    a.update(wall_s=el, zone_updates_per_s=a["zone_updates"] / el)
+    t0 = time.perf_counter()
+    base = serve.one_at_a_time(serve.sedov_stream(args.serve_jobs, rate=50.0, seed=0, precision="fp64"), precision="fp64")
+    el = time.perf_counter() - t0
+    b = serve.latency_summary(base)
+    b.update(wall_s=el, zone_updates_per_s=b["zone_updates"] / el)
+    return {"workload": f"{args.serve_jobs} Sedov-Taylor jobs, Poisson arrivals 50/s (seed 0), 2-D 64^2..512^2 / "
+                        f"3-D 32^3..192^3 log-uniform, t=0.05, HBM budget {args.serve_budget_gb} GB",
+            "served_mixed": a, "one_at_a_time_fp64": b}
+
+
+def run_ensemble(args, timed_steps):
+    """Brio-Wu ensemble (N x 3 x 3 MHD tubes, N log-uniform in [256, 8192], seeded, mixed form): all
+    members advanced by batched launches, against the same members stepped one at a time."""
+    import torch
+    from imogen_b200 import ImogenBatch, ImogenRun, problems
+    tubes = problems.brio_wu_ensemble(count=args.ensemble, seed=0)
+    cells = sum(int(np.prod(s["grid"])) for s, _ in tubes)
+    members = []
+    for s, st in tubes:
+        r = ImogenRun(precision="mixed", **dict(s, time_max=1e5))
+        r.set_state(*st)
+        members.append(r)
+    k = 20
+    # one at a time: each member advances k iterations on its own stream, in turn
+    for r in members:
+        r.iterate()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for r in members:
+        for _ in range(k):
+            r.iterate()
+    for r in members:
+        r.sync()
+    seq = time.perf_counter() - t0
+    b = ImogenBatch(members)
+    for _ in range(8):                         # into the graph-replay regime
+        b.step()
+    l0 = b.launches
+    el = timed_steps(b, k, per_launch=b.step)
+    out = {"members": len(members), "cells": cells, "form": "mixed", "steps": k,
+           "batched_zone_updates_per_s": cells * 2 * k / el, "batched_ms_per_step": 1e3 * el / k,
+           "batched_launches_per_step": (b.launches - l0) / k,
+           "one_at_a_time_zone_updates_per_s": cells * 2 * k / seq}
+    b.close()
+    for r in members:
+        r.close()
+    return out
 
 
 def main():
@@ -337,6 +403,9 @@ def main():
     ap.add_argument("--workload", default="ot512")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving leg (0: skip)")
+    ap.add_argument("--serve-budget-gb", type=int, default=64)
+    ap.add_argument("--ensemble", type=int, default=512, help="members of the batched-ensemble leg (0: skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

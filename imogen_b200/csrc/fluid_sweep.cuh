@@ -111,6 +111,14 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
         __syncthreads();
         return local;
     }
+    if (tl.d != 0 && tl.Wb >= 32) {   // short pencils, one CTA: G rows of Wb columns, one value each
+        T* flat = &part[0][0];          // G * Wb = blockDim.x <= 512 slots
+        flat[tl.g * tl.Wb + tl.b] = local;
+        __syncthreads();
+        T m = T(0);
+        for (int r = 0; r < tl.G; ++r) m = fmax(m, flat[r * tl.Wb + tl.b]);
+        return m;
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int grp, lig, w0, nwc;   // lanes of the column in a warp, this lane's index among them, its warps
     if (tl.d == 0) {   // G is a multiple of 32: whole warps per column

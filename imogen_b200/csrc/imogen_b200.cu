@@ -186,7 +186,8 @@ std::vector<double> fade_coefficients(int f) {
 // Pencil tiling of one sweep direction: one cell per thread where the pencil fits a cluster of at
 // most 4 CTAs of 512 threads (2 or 4 cells per thread otherwise).  Along x a CTA holds whole pencil
 // segments of up to 512 rows; along y and z it holds 4 adjacent pencils, so each row of the tile is
-// 4 contiguous values of x (one 32-byte sector in FP64, half of one in FP32).
+// 4 contiguous values of x (one 32-byte sector in FP64, half of one in FP32), or, for pencils of at
+// most 16 cells, 32 to 256 adjacent pencils.
 PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
@@ -200,6 +201,11 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
             Wb = std::max(1, 256 / G);
             if (Wb * G < 32) Wb = 32 / G;
             while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+        } else if (cpt == 1 && G <= 16) {
+            // short pencils: many of them side by side, at least a warp of x per row (one CTA
+            // holds whole pencils, so the column maximum stays inside the CTA)
+            Wb = maxnt / G;
+            while (Wb > 32 && (long long)Wb / 2 >= ncol) Wb >>= 1;
         } else {
             Wb = 4;   // 4 pencils: 32 contiguous bytes of x per row in FP64 (16 in FP32)
             G = std::max(G, 32 / Wb);

@@ -36,7 +36,7 @@ def _assert_close(o, g, tol, what=""):
 
 
 @pytest.mark.parametrize("bc", BCS)
-@pytest.mark.parametrize("grid", [(32, 1, 1), (24, 22, 1), (22, 21, 20)])
+@pytest.mark.parametrize("grid", [(32, 1, 1), (24, 22, 1), (22, 21, 20), (26, 7, 5)])
 def test_fluid_sweep_single(bc, grid):
     if bc == "fade" and grid[0] < 20:
         pytest.skip("fade needs >= 20 cells")
@@ -53,7 +53,7 @@ def test_fluid_sweep_single(bc, grid):
 
 
 @pytest.mark.parametrize("bc", BCS)
-@pytest.mark.parametrize("grid", [(24, 22, 1), (22, 21, 20)])
+@pytest.mark.parametrize("grid", [(24, 22, 1), (22, 21, 20), (26, 7, 5)])
 def test_mhd_sweeps_single(bc, grid):
     s = _settings(grid, bc, magnet=True)
     o, g = make_pair(s, smooth_state(grid, seed=2, mhd=True))
