@@ -221,6 +221,12 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
     return p;
 }
 
+// Blocks of a pointwise pass (for_cells): units of one 256-cell chunk of an x-row.
+int pointwise_blocks(const Geom& g) {
+    const long long units = (long long)g.n[1] * g.n[2] * ((g.n[0] + 255) / 256);
+    return (int)std::max(1LL, std::min(units, 148LL * 16));
+}
+
 int launch_blocks(long long work, int bs = 256) {
     long long b = (work + bs - 1) / bs;
     return (int)std::max(1LL, std::min(b, 148LL * 16));
@@ -380,7 +386,7 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
         r.L = L;
         ctx->rec->push_back(r);
         r.kind = OP_CT;
-        r.blocks = launch_blocks(ctx->g.ncell);
+        r.blocks = pointwise_blocks(ctx->g);
         ctx->rec->push_back(r);
         r.kind = OP_CELL;
         ctx->rec->push_back(r);
@@ -392,9 +398,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
                     L.grid_x, L.block, L.smem, L.cluster, cudaGetErrorString(le));
-    const long long n = ctx->g.ncell;
-    CK(launch_mag_ct<T>(a, launch_blocks(n), ctx->stream));
-    CK(launch_mag_cell<T>(a, launch_blocks(n), ctx->stream));
+    CK(launch_mag_ct<T>(a, pointwise_blocks(ctx->g), ctx->stream));
+    CK(launch_mag_cell<T>(a, pointwise_blocks(ctx->g), ctx->stream));
     ctx->launches += 3;
     ctx->init_mag[I1 - 1][d] = false;
     ctx->init_mag[I2 - 1][d] = false;

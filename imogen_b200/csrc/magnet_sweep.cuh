@@ -53,7 +53,11 @@ __device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long f
                                         double* edge, const double* fc, int f, double bc_inf, bool own_update) {
     const bool upper = n > 0;
     const bool is_ghost = upper ? (i == Ne - 1) : (i == 0);
-    if (mode == BC_CIRC) return at(((i + n) % Ne + Ne) % Ne);
+    if (mode == BC_CIRC) {   // |n| = 1 <= Ne: one wrap at most
+        int j = i + n;
+        j = j < 0 ? j + Ne : (j >= Ne ? j - Ne : j);
+        return at(j);
+    }
     if (!is_ghost) {
         T v = at(i + n);
         if (mode == BC_FADE) {
@@ -348,6 +352,22 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
 }
 
 // ---- pointwise passes ---------------------------------------------------------------------------------
+// Pointwise passes walk the grid in units of one chunk of blockDim.x cells of an x-row: the
+// coordinates cost one 32-bit division pair per unit instead of per cell (ncell < 2^31).
+template <typename F>
+__device__ __forceinline__ void for_cells(const Geom& g, unsigned vblock, unsigned vgrid, F&& f) {
+    const unsigned nx = (unsigned)g.n[0], ny = (unsigned)g.n[1];
+    const unsigned chunks = (nx + blockDim.x - 1) / blockDim.x;
+    const unsigned units = ny * (unsigned)g.n[2] * chunks;
+    for (unsigned u = vblock; u < units; u += vgrid) {
+        const unsigned r = u / chunks;
+        const unsigned x = (u - r * chunks) * blockDim.x + threadIdx.x;
+        if (x >= nx) continue;
+        const unsigned z = r / ny;
+        f((long long)r * nx + x, (int)x, (int)(r - z * ny), (int)z);
+    }
+}
+
 __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, int& y, int& z) {
     unsigned u = (unsigned)i, n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
     unsigned r = u / n0;
@@ -401,10 +421,7 @@ __device__ __forceinline__ void mag_ct_body(const MagArgs& a, unsigned vblock, u
     const int I2 = a.I[1], e2 = I2 - 1;
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
     T* CB2 = reinterpret_cast<T*>(a.q[Q_CBX + e2]);
-    for (long long cell = vblock * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
-         cell += (long long)vgrid * blockDim.x) {
-        int x, y, z;
-        cell_coords(g, cell, x, y, z);
+    for_cells(g, vblock, vgrid, [&](long long cell, int x, int y, int z) {
         const T D0 = ct_difference<T>(a, 0, cell, x, y, z);
         const T D1 = ct_difference<T>(a, 1, cell, x, y, z);
         BXn[cell] = (BX[cell] - f0 * D0) - f1 * D1;
@@ -417,7 +434,7 @@ __device__ __forceinline__ void mag_ct_body(const MagArgs& a, unsigned vblock, u
             sh = BI2[cell];
         }
         CB2[cell] = T(0.5) * (BI2[cell] + sh);
-    }
+    });
 }
 
 // B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1)); and the drift of the I-direction
@@ -431,10 +448,7 @@ __device__ __forceinline__ void mag_cell_body(const MagArgs& a, unsigned vblock,
     const T* BXn = reinterpret_cast<const T*>(a.BXn);
     T* BX = reinterpret_cast<T*>(a.q[Q_BX + d]);
     T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
-    for (long long cell = vblock * (long long)blockDim.x + threadIdx.x; cell < g.ncell;
-         cell += (long long)vgrid * blockDim.x) {
-        int x, y, z;
-        cell_coords(g, cell, x, y, z);
+    for_cells(g, vblock, vgrid, [&](long long cell, int x, int y, int z) {
         bool own = sel3(d, x, y, z) == sel3(d, g.n[0], g.n[1], g.n[2]) - 1;
         T sh = shift_along<T>(g, BXn, cell, x, y, z, d, +1, a.modeX[1], a.actX, true, a.edges->p[OBJ_PRIM_MAG + d][d][1],
                               a.fade, a.fade_f, a.bc_inf, own);
@@ -452,7 +466,7 @@ __device__ __forceinline__ void mag_cell_body(const MagArgs& a, unsigned vblock,
             const long long fi = face_index(g, e, x, y, z);
             edge[fi] = edge_drift(edge[fi], (double)F[cell]);
         }
-    }
+    });
 }
 
 template <typename T, int CPT, bool FADE>

@@ -136,3 +136,27 @@ def test_mixed_precision_error_is_bounded(name):
     g.run()
     e = errors_vector(g.state(), o.state())
     assert max(e.values()) < 1e-5, e
+
+
+def test_reference_jump_state_fp64():
+    """A stationary MHD shock from the reference's own jump-solver data (Mach 2, 45 degrees): the GPU
+    path agrees with the oracle after 40 iterations."""
+    import json
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "corrugation_jumps.json")
+    j = next(x for x in json.load(open(path)) if x["file"].endswith("ics-t45-ms2-ma0_5.mat"))
+    gamma, n = j["gamma"], 64
+    rho, P = np.array(j["mass"][0]), np.array(j["pressure"][0])
+    v, B = np.array(j["velocity"]), np.array(j["magnet"])
+    grid = (n, 3, 3)
+    side = (np.arange(n) >= n // 2).astype(int)[:, None, None] * np.ones(grid, dtype=int)
+    r = rho[side]
+    mom = np.stack([r * v[c][side] for c in range(3)])
+    mag = np.stack([B[c][side] for c in range(3)])
+    ener = P[side] / (gamma - 1) + 0.5 * r * (v[:, side] ** 2).sum(0) + 0.5 * (mag ** 2).sum(0)
+    s = dict(grid=grid, dgrid=(1.0 / n,) * 3, gamma=gamma, cfl=0.35, bc={"x": "const", "y": "circ", "z": "circ"},
+             limiter="vanleer", magnet=True, time_max=1e5, iter_max=40)
+    o, g = make_pair(s, (r, mom, ener, mag))
+    o.run()
+    g.run()
+    _assert_close(o, g, 1e-10, "reference jump state, 40 iterations")
