@@ -220,9 +220,13 @@ def run_ours(args):
 
     results = {}
     runs = {}
+    tilings = {}
     for prec in ("fp64", "mixed"):
         r = ImogenRun(precision=prec, **s)
         r.set_state(*st)
+        r.iterate()
+        if args.autotune:
+            tilings[prec] = {"xyz"[d - 1]: t for d, t in r.autotune(trials=3).items() if s["grid"][d - 1] >= 3}
         for _ in range(args.warmup):
             r.iterate()
         r.sync()
@@ -310,7 +314,9 @@ def run_ours(args):
             "data": "synthetic (seeded Orszag-Tang IC, no dataset)",
             "config": {"workload": wname, "cells": ncell, "form": "mixed (FP32 state/fluxes, FP64 pressure+CFL)",
                        "step": "1 iteration = 2 timesteps (X,Y fluid+magnet each)",
-                       "l2": "flushed (512 MB write) before every timed step", "parallelism": f"replicas x{ws}"},
+                       "l2": "flushed (512 MB write) before every timed step", "parallelism": f"replicas x{ws}",
+                       "tiling": tilings or None,
+                       "tiling_fields": "pencils/CTA, threads/pencil, CTAs/cluster, threads/CTA, cells/thread"},
             "fp64": {"value": v64, "unit": "zone-updates/s", "ms_per_step": 1e3 * results["fp64"] / args.steps},
             "mixed_over_fp64": v / v64,
             "l1_mixed_vs_fp64": l1,
@@ -404,6 +410,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving leg (0: skip)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false", help="keep the default tilings")
     ap.add_argument("--serve-budget-gb", type=int, default=64)
     ap.add_argument("--ensemble", type=int, default=512, help="members of the batched-ensemble leg (0: skip)")
     args = ap.parse_args()

@@ -137,8 +137,7 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
     if (lig == 0) part[warp][tl.b] = local;
     __syncthreads();
     T m = T(0);
-    if (lig < nwc) m = part[w0 + lig][tl.b];
-    if (lig + grp < nwc) m = fmax(m, part[w0 + lig + grp][tl.b]);   // nwc <= 16 <= 2 * grp
+    for (int j = lig; j < nwc; j += grp) m = fmax(m, part[w0 + j][tl.b]);
     const int olo = tl.d == 0 ? 1 : tl.Wb;
     for (int o = 16; o >= olo; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
     if (tl.CL == 1) return m;

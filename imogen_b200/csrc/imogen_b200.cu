@@ -11,7 +11,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -219,6 +221,67 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
         if (CL <= 4) break;   // clusters of 8 CTAs of these kernels do not schedule: more cells per thread
     }
     return p;
+}
+
+// Process-wide cache of autotuned tilings, keyed by what decides them: sweep direction, pencil
+// length, number of pencils (rounded up to a power of two), precision and physics.  Contexts
+// created later with the same key start from the tuned tiling.
+using TuneKey = std::tuple<int, int, int, int, int, int>;
+std::mutex g_tune_mu;
+std::map<TuneKey, PencilCfg> g_tuned;
+
+TuneKey tune_key(const Geom& g, int d, size_t elem, const img_config& c) {
+    const long long ncol = g.ncell / g.n[d];
+    return TuneKey(d, g.n[d], pow2ceil((int)std::min<long long>(ncol, 1 << 30)), (int)elem, c.fluid_active,
+                   c.magnet_active);
+}
+
+// Every pencil tiling the kernels accept for direction d (the autotuner's search space): one, two
+// or four cells per thread; along x whole-pencil CTAs of up to 256 or 512 threads; along y and z
+// 2, 4 or 8 pencils per CTA, or for pencils of at most 16 cells 32..512/G pencils; at most 4 CTAs
+// per cluster, and one CTA when pencils sit 32 or more side by side.
+std::vector<PencilCfg> pencil_candidates(const Geom& g, int d) {
+    const int N = g.n[d];
+    const long long ncol = g.ncell / N;
+    std::vector<PencilCfg> out;
+    auto add = [&](int Wb, int G, int CL, int cpt) {
+        PencilCfg p;
+        p.Wb = Wb;
+        p.G = G;
+        p.CL = CL;
+        p.NT = Wb * G;
+        p.cpt = cpt;
+        if (CL > 4 || p.NT < 32 || p.NT > 512 || p.NT % 32 || G < 2) return;
+        if ((long long)G * cpt * CL < N) return;
+        for (const PencilCfg& q : out)
+            if (q.Wb == Wb && q.G == G && q.CL == CL && q.cpt == cpt) return;
+        out.push_back(p);
+    };
+    for (int cpt : {1, 2, 4}) {
+        const int G0 = std::max(2, pow2ceil((N + cpt - 1) / cpt));
+        if (d == 0) {
+            for (int maxnt : {256, 512}) {
+                int G = G0, CL = 1;
+                while (G > maxnt) { G >>= 1; CL <<= 1; }
+                int Wb = std::max(1, maxnt / G);
+                while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+                if (G > 32 && Wb > 8) continue;   // pencils spanning warps: at most 8 per CTA
+                add(Wb, G, CL, cpt);
+            }
+        } else {
+            for (int Wb : {2, 4, 8}) {
+                int G = std::max(G0, 32 / Wb), CL = 1;
+                while (Wb * G > 512) { G >>= 1; CL <<= 1; }
+                add(Wb, G, CL, cpt);
+            }
+            if (cpt == 1 && G0 <= 16)
+                for (int Wb = 32; Wb * G0 <= 512; Wb <<= 1) {
+                    if ((long long)Wb / 2 >= ncol && Wb > 32) break;
+                    add(Wb, G0, 1, cpt);
+                }
+        }
+    }
+    return out;
 }
 
 // Blocks of a pointwise pass (for_cells): units of one 256-cell chunk of an x-row.
@@ -670,7 +733,12 @@ int img_create(img_ctx** out, const img_config* cfg) {
     g.s[1] = g.n[0];
     g.s[2] = (long long)g.n[0] * g.n[1];
     g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (int d = 0; d < 3; ++d) ctx->pcfg[d] = choose_pencil(g, d, ctx->elem);
+    for (int d = 0; d < 3; ++d) {
+        ctx->pcfg[d] = choose_pencil(g, d, ctx->elem);
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(tune_key(g, d, ctx->elem, *cfg));
+        if (it != g_tuned.end()) ctx->pcfg[d] = it->second;
+    }
 
     auto bail = [&](int code) {
         if (ctx->slab) cudaFree(ctx->slab);
@@ -1497,6 +1565,103 @@ int img_totals_static(img_ctx* ctx, double out[8]) {
 int img_get_stream(img_ctx* ctx, void** stream) {
     if (!ctx || !stream) return fail(ctx, IMG_ERR_ARG, "null argument");
     *stream = (void*)ctx->stream;
+    return IMG_OK;
+}
+
+static void drop_graphs(img_ctx* ctx) {
+    for (auto& row : ctx->graphs)
+        for (auto& gx : row)
+            if (gx) {
+                cudaGraphExecDestroy(gx);
+                gx = nullptr;
+            }
+}
+
+int img_autotune(img_ctx* ctx, int trials) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot tune a batch member");
+    if (trials < 1) trials = 3;
+    CK(cudaStreamSynchronize(ctx->stream));
+    void* backup = nullptr;
+    if (cudaMalloc(&backup, ctx->slab_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, IMG_ERR_NOMEM, "autotune needs a %zu-byte copy of the context", ctx->slab_bytes);
+    }
+    const bool s_store = ctx->init_store, s_flux = ctx->init_flux, s_cfl = ctx->cfl_valid;
+    bool s_mag[3][3];
+    std::memcpy(s_mag, ctx->init_mag, sizeof s_mag);
+    const uint64_t s_launches = ctx->launches;
+    auto restore = [&]() {
+        cudaMemcpyAsync(ctx->slab, backup, ctx->slab_bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+        ctx->init_store = s_store;
+        ctx->init_flux = s_flux;
+        ctx->cfl_valid = s_cfl;
+        std::memcpy(ctx->init_mag, s_mag, sizeof s_mag);
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = IMG_OK;
+    if (cudaMemcpyAsync(backup, ctx->slab, ctx->slab_bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        rc = fail(ctx, IMG_ERR_CUDA, "autotune setup failed");
+    for (int d = 0; d < 3 && rc == IMG_OK; ++d) {
+        if (ctx->g.n[d] < 3) continue;
+        PencilCfg best = ctx->pcfg[d];
+        float best_ms = 1e30f;
+        for (const PencilCfg& cand : pencil_candidates(ctx->g, d)) {
+            ctx->pcfg[d] = cand;
+            int ncl = 0;
+            const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
+                                             : fluid_smem_bytes<float>(cand.G * cand.cpt, cand.Wb);
+            PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, d, fs, 1, false) : pencil_launch<float>(ctx, d, fs, 1, false);
+            cudaError_t ce = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
+            if (ce != cudaSuccess || ncl < 1) {
+                cudaGetLastError();
+                continue;
+            }
+            auto sweep = [&]() {
+                int r = ctx->cfg.fluid_active ? fluid_sweep(ctx, d + 1, false) : IMG_OK;
+                if (r == IMG_OK && ctx->cfg.magnet_active) r = magnet_sweep(ctx, d + 1, FWD_MI[d][0], FWD_MI[d][1]);
+                return r;
+            };
+            bool ok = sweep() == IMG_OK;                                   // warm-up
+            ok = ok && cudaEventRecord(e0, ctx->stream) == cudaSuccess;
+            for (int t = 0; ok && t < trials; ++t) ok = sweep() == IMG_OK;
+            ok = ok && cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+            float ms = 0.f;
+            ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            restore();
+            if (!ok) {
+                cudaGetLastError();
+                continue;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = cand;
+            }
+        }
+        ctx->pcfg[d] = best;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[tune_key(ctx->g, d, ctx->elem, ctx->cfg)] = best;
+    }
+    restore();
+    cudaStreamSynchronize(ctx->stream);
+    ctx->launches = s_launches;
+    drop_graphs(ctx);   // captured with the old tilings
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(backup);
+    return rc != IMG_OK ? rc : check_dev_error(ctx);
+}
+
+int img_get_tiling(const img_ctx* ctx, int dim, int out[5]) {
+    if (!ctx || !out || dim < 1 || dim > 3) return IMG_ERR_ARG;
+    const PencilCfg& p = ctx->pcfg[dim - 1];
+    out[0] = p.Wb;
+    out[1] = p.G;
+    out[2] = p.CL;
+    out[3] = p.NT;
+    out[4] = p.cpt;
     return IMG_OK;
 }
 

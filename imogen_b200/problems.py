@@ -152,12 +152,16 @@ def main(argv=None):
     ap.add_argument("workload", choices=sorted(WORKLOADS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--autotune", action="store_true", help="tune the pencil tilings first (as bench.py does)")
     a = ap.parse_args(argv)
     from imogen_b200 import ImogenRun
 
     s, st = WORKLOADS[a.workload]()
     run = ImogenRun(precision=a.precision, **dict(s, iter_max=10 ** 7, time_max=1e5))
     run.set_state(*st)
+    if a.autotune:
+        run.iterate()
+        print("tiling", run.autotune(trials=3))
     t0 = time.perf_counter()
     for _ in range(a.iters):
         run.iterate()

@@ -247,6 +247,20 @@ class ImogenRun:
         check(lib().img_launch_count(self._h, ctypes.byref(n)), self._h)
         return n.value
 
+    def autotune(self, trials=3):
+        """Pick the fastest pencil tiling per swept direction (img_autotune); returns tiling()."""
+        check(lib().img_autotune(self._h, int(trials)), self._h)
+        return self.tiling()
+
+    def tiling(self):
+        """{dim: (pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread)}"""
+        out = {}
+        for d in (1, 2, 3):
+            t = (ctypes.c_int * 5)()
+            check(lib().img_get_tiling(self._h, d, t), self._h)
+            out[d] = tuple(t)
+        return out
+
     def progress(self):
         """(simulated time, iterations run, stopped) from the device clock (synchronises)."""
         t, n, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()

@@ -140,6 +140,16 @@ size_t img_bytes_required(const img_config* cfg);
  * CUDA events around calls or order their own work after it.  No reference counterpart. */
 int img_get_stream(img_ctx* ctx, void** stream);
 
+/* Autotuner: time every pencil tiling the kernels accept (cells per thread, CTA shape, cluster
+ * size) for each swept direction on this context's own state, `trials` sweeps each, keep the
+ * fastest, and remember it for later contexts of the same shape.  The state, stored edges and
+ * clock are restored afterwards.  Needs a temporary device copy of the context.  No reference
+ * counterpart. */
+int img_autotune(img_ctx* ctx, int trials);
+/* Tiling of direction dim (1..3): {pencils per CTA, threads per pencil, CTAs per cluster,
+ * threads per CTA, cells per thread}. */
+int img_get_tiling(const img_ctx* ctx, int dim, int out[5]);
+
 /* Number of kernels the context has launched so far.  No reference counterpart. */
 int img_launch_count(const img_ctx* ctx, uint64_t* count);
 

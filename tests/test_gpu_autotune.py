@@ -1,0 +1,46 @@
+"""Autotuner (img_autotune): it leaves the state untouched, every tiling it may pick gives the same
+results, and later contexts of the same shape start from the tuned tiling (GPU required)."""
+import numpy as np
+import pytest
+
+from imogen_b200 import ImogenRun, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(s, st, precision):
+    r = ImogenRun(precision=precision, **s)
+    r.set_state(*st)
+    return r
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", ["ot", "kh", "tube"])
+def test_autotune_keeps_state_and_results(precision, case):
+    if case == "ot":
+        s, st = problems.orszag_tang(96)
+    elif case == "kh":
+        s, st = problems.kelvin_helmholtz(24)
+    else:
+        s, st = problems.brio_wu_tube(1500, 1.0, 0.125, 1.0, 0.1)
+    s = dict(s, time_max=1e5, iter_max=10 ** 6)
+    tuned, plain = _run(s, st, precision), _run(s, st, precision)
+    for r in (tuned, plain):                     # past the first (edge-capture) iteration
+        r.iterate()
+    before = tuned.state()
+    t0 = tuned.time.time
+    tuned.autotune(trials=2)
+    after = tuned.state()
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k
+    assert tuned.time.time == t0
+    for _ in range(4):
+        tuned.iterate()
+        plain.iterate()
+    a, b = tuned.state(), plain.state()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), (k, tuned.tiling(), plain.tiling())
+    again = _run(s, st, precision)
+    assert again.tiling() == tuned.tiling()
+    for r in (tuned, plain, again):
+        r.close()
