@@ -301,6 +301,7 @@ def run_ours(args):
            "h2d_bytes_per_step": 8 * ncell * 8, "d2h_bytes_per_step": 8 * ncell * 8,
            "form": "mixed", "steps": ke}
 
+    kh = run_kh(args, timed_steps, measured_hbm_peak()[0]) if args.kh > 0 else None
     serving = run_serving(args) if args.serve_jobs > 0 else None
     ensemble = run_ensemble(args, timed_steps) if args.ensemble > 0 else None
 
@@ -331,6 +332,7 @@ def run_ours(args):
              "unit": "s", "workload": serving["workload"]},
             "serving": serving,
             "ensemble": ensemble,
+            "kh3d": kh,
         }
         if not args.no_cpu_baseline and ws == 1:
             line["cpu_baseline"] = cpu_baseline(s, st, wname, budget_s=args.cpu_budget)
@@ -339,6 +341,36 @@ def run_ours(args):
         r.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_kh(args, timed_steps, peak):
+    """3-D MHD Kelvin-Helmholtz at n^3 (default 256^3, 16.8 M cells: the state exceeds L2, so this is
+    the HBM-bound configuration): iteration throughput of both forms and the x fluid sweep against
+    the measured HBM bandwidth."""
+    from imogen_b200 import ImogenRun, problems
+    n = args.kh
+    s, st = problems.kelvin_helmholtz(n)
+    s = dict(s, iter_max=10 ** 7, time_max=1e5)
+    cells = n ** 3
+    out = {"workload": f"kelvin_helmholtz_{n}^3_mhd", "cells": cells}
+    for prec, w in (("mixed", 4), ("fp64", 8)):
+        r = ImogenRun(precision=prec, **s)
+        r.set_state(*st)
+        r.iterate()
+        tiling = r.autotune(trials=2) if args.autotune else r.tiling()
+        for _ in range(2):
+            r.iterate()
+        k = 5
+        el = timed_steps(r, k)
+        r.time.set(r.time.time, 1e-5, r.time.iteration)
+        per = timed_steps(r, k, per_launch=lambda r=r: r.relaxing_fluid(1)) / k
+        alg = cells * (8 + 5) * w
+        out[prec] = {"zone_updates_per_s": cells * 2 * k / el, "ms_per_step": 1e3 * el / k,
+                     "fluid_x": {"launch_us": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
+                                 "frac_of_measured_hbm": alg / per / 1e9 / peak},
+                     "tiling": {"xyz"[d - 1]: t for d, t in tiling.items()}}
+        r.close()
+    return out
 
 
 def run_serving(args):
@@ -411,6 +443,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--serve-jobs", type=int, default=16, help="jobs of the serving leg (0: skip)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false", help="keep the default tilings")
+    ap.add_argument("--kh", type=int, default=256, help="edge of the 3-D Kelvin-Helmholtz leg (0: skip)")
     ap.add_argument("--serve-budget-gb", type=int, default=64)
     ap.add_argument("--ensemble", type=int, default=512, help="members of the batched-ensemble leg (0: skip)")
     args = ap.parse_args()

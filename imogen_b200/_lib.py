@@ -23,7 +23,7 @@ SYMBOLS = (
     "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
     "img_get_time", "img_set_time", "img_progress", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
-    "img_get_stream", "img_autotune", "img_get_tiling", "img_launch_count",
+    "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -98,6 +98,8 @@ def lib():
     L.img_autotune.restype = ctypes.c_int
     L.img_get_tiling.argtypes = [vp, ctypes.c_int, ip]
     L.img_get_tiling.restype = ctypes.c_int
+    L.img_set_tiling.argtypes = [vp, ctypes.c_int, ip]
+    L.img_set_tiling.restype = ctypes.c_int
     L.img_launch_count.restype = ctypes.c_int
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]

@@ -203,6 +203,10 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
             Wb = std::max(1, 256 / G);
             if (Wb * G < 32) Wb = 32 / G;
             while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+            if (G > 32) {   // whole warps per pencil, without padding to a power of two
+                const int rows = (N + cpt - 1) / cpt;
+                G = ((rows + CL - 1) / CL + 31) / 32 * 32;
+            }
         } else if (cpt == 1 && G <= 16) {
             // short pencils: many of them side by side, at least a warp of x per row (one CTA
             // holds whole pencils, so the column maximum stays inside the CTA)
@@ -257,8 +261,10 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d) {
             if (q.Wb == Wb && q.G == G && q.CL == CL && q.cpt == cpt) return;
         out.push_back(p);
     };
+    auto up = [](int v, int m) { return (v + m - 1) / m * m; };
     for (int cpt : {1, 2, 4}) {
-        const int G0 = std::max(2, pow2ceil((N + cpt - 1) / cpt));
+        const int rows = (N + cpt - 1) / cpt;
+        const int G0 = std::max(2, pow2ceil(rows));
         if (d == 0) {
             for (int maxnt : {256, 512}) {
                 int G = G0, CL = 1;
@@ -267,12 +273,19 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d) {
                 while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
                 if (G > 32 && Wb > 8) continue;   // pencils spanning warps: at most 8 per CTA
                 add(Wb, G, CL, cpt);
+                // whole warps per pencil without the power-of-two padding (G a multiple of 32)
+                if (G > 32) {
+                    const int Gt = up((rows + CL - 1) / CL, 32);
+                    if (Gt < G) add(Wb, Gt, CL, cpt);
+                }
             }
         } else {
             for (int Wb : {2, 4, 8}) {
                 int G = std::max(G0, 32 / Wb), CL = 1;
                 while (Wb * G > 512) { G >>= 1; CL <<= 1; }
                 add(Wb, G, CL, cpt);
+                const int Gt = std::max(up((rows + CL - 1) / CL, 32 / Wb), 32 / Wb);
+                if (Gt < G) add(Wb, Gt, CL, cpt);
             }
             if (cpt == 1 && G0 <= 16)
                 for (int Wb = 32; Wb * G0 <= 512; Wb <<= 1) {
@@ -1652,6 +1665,29 @@ int img_autotune(img_ctx* ctx, int trials) {
     if (e1) cudaEventDestroy(e1);
     cudaFree(backup);
     return rc != IMG_OK ? rc : check_dev_error(ctx);
+}
+
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
+    if (!ctx || !cfg || dim < 1 || dim > 3) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
+    if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot retile a batch member");
+    const int d = dim - 1;
+    for (const PencilCfg& c : pencil_candidates(ctx->g, d)) {
+        if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4]) continue;
+        int ncl = 0;
+        const PencilCfg old = ctx->pcfg[d];
+        ctx->pcfg[d] = c;
+        const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(c.G * c.cpt, c.Wb) : fluid_smem_bytes<float>(c.G * c.cpt, c.Wb);
+        PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, d, fs, 1, false) : pencil_launch<float>(ctx, d, fs, 1, false);
+        cudaError_t e = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
+        if (e != cudaSuccess || ncl < 1) {
+            cudaGetLastError();
+            ctx->pcfg[d] = old;
+            return fail(ctx, IMG_ERR_UNSUPPORTED, "tiling cannot be scheduled on this device");
+        }
+        drop_graphs(ctx);
+        return IMG_OK;
+    }
+    return fail(ctx, IMG_ERR_UNSUPPORTED, "not a tiling the kernels accept for this direction");
 }
 
 int img_get_tiling(const img_ctx* ctx, int dim, int out[5]) {

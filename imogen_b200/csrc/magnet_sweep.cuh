@@ -53,12 +53,7 @@ __device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long f
                                         double* edge, const double* fc, int f, double bc_inf, bool own_update) {
     const bool upper = n > 0;
     const bool is_ghost = upper ? (i == Ne - 1) : (i == 0);
-    if (mode == BC_CIRC) {   // |n| = 1 <= Ne: one wrap at most
-        int j = i + n;
-        j = j < 0 ? j + Ne : (j >= Ne ? j - Ne : j);
-        return at(j);
-    }
-    if (!is_ghost) {
+    if (!is_ghost) {   // interior: the neighbour, damped under fade
         T v = at(i + n);
         if (mode == BC_FADE) {
             T s0 = upper ? at(Ne > 1 ? 1 : 0) : at(0);
@@ -68,6 +63,7 @@ __device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long f
         return v;
     }
     switch (mode) {
+        case BC_CIRC: return at(upper ? 0 : Ne - 1);
         case BC_MIRROR: { T v = upper ? at(Ne - 2) : at(1); return flip ? -v : v; }
         case BC_WALL: return (T)edge[fi];
         case BC_TRANS: {
@@ -300,7 +296,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
         const T w = W[k], v = vf[k];
         const int ix = tl.idx(k);
         const int r = tl.grow(k);
-        T p1a = S0[ix + Wb], p1b = p1a, p1d = p1a, p2 = S0[ix + 2 * Wb];
+        T p1a = S0[ix + tl.rs], p1b = p1a, p1d = p1a, p2 = S0[ix + 2 * tl.rs];
         if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
             if (r == N - 1) {
                 p1a = GS[1 * Wb + b].g;

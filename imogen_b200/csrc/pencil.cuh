@@ -7,7 +7,7 @@
 // so global loads/stores are coalesced along x for every sweep direction.
 //
 // Stencil operands live in shared-memory arrays with HALO rows: local row 0 is the row below the
-// CTA's first row, local rows RC+1 and RC+2 the two rows above its last row.  Between stages a few
+// CTA's first row, local rows RC+1 and RC+2 the two rows above its last row (layout: Tile::rs/cs).  Between stages a few
 // threads fill the halos -- the neighbouring cluster rank's edge rows (read through DSMEM), or, at
 // the pencil ends, the boundary-condition ghost of the reference's shift (shifting/*_shift.m),
 // stateful edge drift included -- so every stencil read is one unconditional shared load.
@@ -52,6 +52,10 @@ template <typename T, int CPT>
 struct Tile {
     // uniform (copies of parameter values)
     int N, Wb, G, CL, d, RC, rank_hi;
+    // shared layout: element (local row l, column b) at l * rs + b * cs.  Along x a warp's lanes
+    // walk the rows of one pencil, so rows are contiguous (rs = 1); along y/z the lanes walk the
+    // columns, so columns are (cs = 1).  Either way consecutive lanes hit consecutive banks.
+    int rs, cs;
     // per thread
     int b, g, rank;
     int row0;             // global row of own cell k = 0
@@ -76,10 +80,12 @@ struct Tile {
         n1 = s.n1;
         if (s.d == 0) { g = t % s.G; b = t / s.G; }
         else { b = t % s.Wb; g = t / s.Wb; }
+        rs = s.d == 0 ? 1 : s.Wb;
+        cs = s.d == 0 ? tile_rows(s.RC) : 1;
         rank = (int)(vblock & (unsigned)(s.CL - 1));   // CL is a power of two
         const long long bundle = vblock / (unsigned)s.CL;
         row0 = rank * s.RC + g;
-        ix0 = (g + HALO_LO) * s.Wb + b;
+        ix0 = (g + HALO_LO) * rs + b * cs;
         col = bundle * s.Wb + b;
         colok = col < s.ncol;
         const long long c = colok ? col : 0;
@@ -90,8 +96,8 @@ struct Tile {
     __device__ __forceinline__ bool ok(int k) const { return colok && grow(k) < N; }
     __device__ __forceinline__ long long off(int k) const { return base + (long long)grow(k) * sd; }
     // shared index of own row k, and of local row l (0 = lower halo)
-    __device__ __forceinline__ int idx(int k) const { return ix0 + k * G * Wb; }
-    __device__ __forceinline__ int lidx(int l) const { return l * Wb + b; }
+    __device__ __forceinline__ int idx(int k) const { return ix0 + k * G * rs; }
+    __device__ __forceinline__ int lidx(int l) const { return l * rs + b * cs; }
     __device__ __forceinline__ void coords(int k, int& x, int& y, int& z) const {
         const int r = grow(k);
         const long long c = colok ? col : 0;
@@ -114,10 +120,10 @@ struct Tile {
     __device__ __forceinline__ U row(const U* A, int r) const {
         int rk = r / RC;
         const U* p = remote(const_cast<U*>(A), rk);
-        return p[(r - rk * RC + HALO_LO) * Wb + b];
+        return p[(r - rk * RC + HALO_LO) * rs + b * cs];
     }
     // Local shared index of global row r (r may be N or N+1 on rank_hi: an idle row or a halo row).
-    __device__ __forceinline__ int ridx(int r) const { return (r - rank * RC + HALO_LO) * Wb + b; }
+    __device__ __forceinline__ int ridx(int r) const { return (r - rank * RC + HALO_LO) * rs + b * cs; }
 };
 
 // Fade damping of fade_shift.m:31-44 applied to the constant-shifted value sv at row r of a line of
@@ -141,7 +147,7 @@ __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, in
 template <bool FADE, typename T, int CPT>
 __device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const Ghost<T>* an, int k, int n, int mode,
                                      const double* fc, int f) {
-    T v = A[tl.idx(k) + n * tl.Wb];
+    T v = A[tl.idx(k) + n * tl.rs];
     if (FADE && mode == BC_FADE) {
         const Ghost<T>& q = an[tl.b];
         v = fade_apply(v, tl.grow(k), tl.N, fc, f, q.s0, q.sN1);

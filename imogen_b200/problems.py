@@ -138,6 +138,7 @@ WORKLOADS = {
     "ot64": lambda: orszag_tang(64),
     "kh256": lambda: kelvin_helmholtz(256),
     "kh128": lambda: kelvin_helmholtz(128),
+    "kh160": lambda: kelvin_helmholtz(160),
     "sod": lambda: sod(4096),
 }
 
@@ -153,12 +154,17 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--autotune", action="store_true", help="tune the pencil tilings first (as bench.py does)")
+    ap.add_argument("--tiling", action="append", default=[],
+                    help="dim=Wb,G,CL,NT,cpt for one direction, e.g. x=2,128,1,256,4 (repeatable)")
     a = ap.parse_args(argv)
     from imogen_b200 import ImogenRun
 
     s, st = WORKLOADS[a.workload]()
     run = ImogenRun(precision=a.precision, **dict(s, iter_max=10 ** 7, time_max=1e5))
     run.set_state(*st)
+    for spec in a.tiling:
+        dim, vals = spec.split("=")
+        run.set_tiling("xyz".index(dim) + 1, [int(v) for v in vals.split(",")])
     if a.autotune:
         run.iterate()
         print("tiling", run.autotune(trials=3))

@@ -261,6 +261,11 @@ class ImogenRun:
             out[d] = tuple(t)
         return out
 
+    def set_tiling(self, dim, tiling):
+        """Use one of the accepted tilings for direction dim (1..3); see tiling()."""
+        t = (ctypes.c_int * 5)(*[int(v) for v in tiling])
+        check(lib().img_set_tiling(self._h, int(dim), t), self._h)
+
     def progress(self):
         """(simulated time, iterations run, stopped) from the device clock (synchronises)."""
         t, n, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()

@@ -149,6 +149,8 @@ int img_autotune(img_ctx* ctx, int trials);
 /* Tiling of direction dim (1..3): {pencils per CTA, threads per pencil, CTAs per cluster,
  * threads per CTA, cells per thread}. */
 int img_get_tiling(const img_ctx* ctx, int dim, int out[5]);
+/* Set the tiling of direction dim to one of those the autotuner may pick (same field order). */
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]);
 
 /* Number of kernels the context has launched so far.  No reference counterpart. */
 int img_launch_count(const img_ctx* ctx, uint64_t* count);
