@@ -191,6 +191,11 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     const T* pX = reinterpret_cast<const T*>(a.q[Q_PX + d]);
     T* BI = reinterpret_cast<T*>(a.q[Q_BX + c]);
     T vgr[CPT], bI[CPT];
+    // the transverse coordinate is the pencil's own (e != d): interior pencils read their lower
+    // neighbour directly; the boundary and fade cases go through the reference's shift
+    const int ie = e == a.sg.d1 ? tl.c1 : tl.c2;
+    const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
+    const bool direct = shiftI && ie > 0 && mode_mom_lo != BC_FADE && mode_mass_lo != BC_FADE;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         vgr[k] = T(0);
@@ -200,7 +205,10 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             int x, y, z;
             tl.coords(k, x, y, z);
             T pm, rm;
-            if (shiftI) {
+            if (direct) {
+                pm = pX[o - se];
+                rm = rho[o - se];
+            } else if (shiftI) {
                 pm = shift_along<T>(g, pX, o, x, y, z, e, -1, mode_mom_lo, act_mom, false,
                                     et->p[OBJ_PRIM_MOM + d][e][0], fc, f, binf, true);
                 rm = shift_along<T>(g, rho, o, x, y, z, e, -1, mode_mass_lo, act_mass, false,
@@ -390,15 +398,21 @@ __device__ __forceinline__ T ct_difference(const MagArgs& a, int q, long long ce
     const long long sdx = sel3(d, g.s[0], g.s[1], g.s[2]);
     const int xd = sel3(d, x, y, z);
     const long long row0 = cell - (long long)xd * sdx;   // X-index 0 of this cell's X-line
+    // the I coordinate is the same at every X-index of this line: away from the upper I face (and
+    // without fade) the I-shift is the next cell along I
+    const bool directI = shI && sel3(e, x, y, z) < sel3(e, g.n[0], g.n[1], g.n[2]) - 1 && modeI != BC_FADE;
+    const long long sI = sel3(e, g.s[0], g.s[1], g.s[2]);
     // C_q at X-index j of this line
     auto C = [&](int j) -> T {
         const long long c2 = row0 + (long long)j * sdx;
         const T fv = F[c2];
         if (!shI) return fv - fv;
+        if (directI) return fv - F[c2 + sI];
         const int x2 = d == 0 ? j : x, y2 = d == 1 ? j : y, z2 = d == 2 ? j : z;
         return fv - shift_along<T>(g, F, c2, x2, y2, z2, e, +1, modeI, actI, true, edgeI, a.fade, a.fade_f, a.bc_inf,
                                    false);
     };
+    if (xd >= 1 && a.modeX[0] != BC_FADE) return C(xd - 1);   // interior along X
     return shift_line<T>(C, xd, Nd, face_index(g, d, x, y, z), -1, a.modeX[0], a.actX, e == d,
                          a.edges->p[mag_obj(e, d, MO_FLUX)][d][0], a.fade, a.fade_f, a.bc_inf, xd == 0);
 }

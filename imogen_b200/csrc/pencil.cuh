@@ -60,11 +60,11 @@ struct Tile {
     int b, g, rank;
     int row0;             // global row of own cell k = 0
     int ix0;              // shared index of own cell k = 0
-    long long col;        // global pencil index
+    int col;              // global pencil index (ncell < 2^31)
     bool colok;
     long long base;       // linear offset of row 0 of this pencil
     long long sd;         // stride along the sweep
-    int n1;
+    int c1, c2;           // the pencil's coordinates along d1 and d2
 
     // vblock: this CTA's block index within its grid's launch (blockIdx.x for a single launch)
     __device__ __forceinline__ void init(const SweepGeom& s, unsigned vblock) {
@@ -77,19 +77,19 @@ struct Tile {
         RC = s.RC;
         rank_hi = s.rank_hi;
         sd = s.sd;
-        n1 = s.n1;
         if (s.d == 0) { g = t % s.G; b = t / s.G; }
         else { b = t % s.Wb; g = t / s.Wb; }
         rs = s.d == 0 ? 1 : s.Wb;
         cs = s.d == 0 ? tile_rows(s.RC) : 1;
         rank = (int)(vblock & (unsigned)(s.CL - 1));   // CL is a power of two
-        const long long bundle = vblock / (unsigned)s.CL;
+        const unsigned bundle = vblock / (unsigned)s.CL;
         row0 = rank * s.RC + g;
         ix0 = (g + HALO_LO) * rs + b * cs;
-        col = bundle * s.Wb + b;
+        col = (int)(bundle * (unsigned)s.Wb + (unsigned)b);
         colok = col < s.ncol;
-        const long long c = colok ? col : 0;
-        const int c1 = (int)(c % s.n1), c2 = (int)(c / s.n1);
+        const unsigned c = colok ? (unsigned)col : 0u;
+        c2 = (int)(c / (unsigned)s.n1);
+        c1 = (int)(c - (unsigned)c2 * (unsigned)s.n1);
         base = c1 * s.s1 + (long long)c2 * s.s2;
     }
     __device__ __forceinline__ int grow(int k) const { return row0 + k * G; }
@@ -100,8 +100,6 @@ struct Tile {
     __device__ __forceinline__ int lidx(int l) const { return l * rs + b * cs; }
     __device__ __forceinline__ void coords(int k, int& x, int& y, int& z) const {
         const int r = grow(k);
-        const long long c = colok ? col : 0;
-        const int c1 = (int)(c % n1), c2 = (int)(c / n1);
         if (d == 0) { x = r; y = c1; z = c2; }
         else if (d == 1) { x = c1; y = r; z = c2; }
         else { x = c1; y = c2; z = r; }
