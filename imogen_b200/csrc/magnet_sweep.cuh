@@ -484,8 +484,9 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const 
     mag_chain_body<T, CPT, FADE>(a, blockIdx.x);
 }
 
+// CT and cell passes are latency-bound: at most 64 registers so that 4 CTAs of 256 threads share an SM.
 template <typename T>
-__global__ void mag_ct_kernel(const __grid_constant__ MagArgs a) {
+__global__ void __launch_bounds__(256, 4) mag_ct_kernel(const __grid_constant__ MagArgs a) {
     mag_ct_body<T>(a, blockIdx.x, gridDim.x);
 }
 
@@ -506,7 +507,8 @@ __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_batch_kernel(
 }
 
 template <typename T>
-__global__ void mag_ct_batch_kernel(const MagArgs* __restrict__ args, const BlockMap* __restrict__ map) {
+__global__ void __launch_bounds__(256, 4) mag_ct_batch_kernel(const MagArgs* __restrict__ args,
+                                                              const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
