@@ -226,7 +226,8 @@ def run_ours(args):
         r.set_state(*st)
         r.iterate()
         if args.autotune:
-            tilings[prec] = {"xyz"[d - 1]: t for d, t in r.autotune(trials=3).items() if s["grid"][d - 1] >= 3}
+            tilings[prec] = {kind: {"xyz"[d - 1]: t for d, t in tl.items() if s["grid"][d - 1] >= 3}
+                             for kind, tl in r.autotune(trials=3).items()}
         for _ in range(args.warmup):
             r.iterate()
         r.sync()
@@ -357,7 +358,7 @@ def run_kh(args, timed_steps, peak):
         r = ImogenRun(precision=prec, **s)
         r.set_state(*st)
         r.iterate()
-        tiling = r.autotune(trials=2) if args.autotune else r.tiling()
+        tiling = r.autotune(trials=2) if args.autotune else {"fluid": r.tiling("fluid"), "magnet": r.tiling("magnet")}
         for _ in range(2):
             r.iterate()
         k = 5
@@ -368,7 +369,7 @@ def run_kh(args, timed_steps, peak):
         out[prec] = {"zone_updates_per_s": cells * 2 * k / el, "ms_per_step": 1e3 * el / k,
                      "fluid_x": {"launch_us": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
                                  "frac_of_measured_hbm": alg / per / 1e9 / peak},
-                     "tiling": {"xyz"[d - 1]: t for d, t in tiling.items()}}
+                     "tiling": {kind: {"xyz"[d - 1]: t for d, t in tl.items()} for kind, tl in tiling.items()}}
         r.close()
     return out
 

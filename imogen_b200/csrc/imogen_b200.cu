@@ -89,7 +89,7 @@ struct img_ctx {
     bool cfl_valid = false;     // DevTime.maxbits hold the CFL maxima of the current state
     int iteration = 1;
     int iters_base = 0;
-    PencilCfg pcfg[3];
+    PencilCfg pcfg[2][3];        // pencil tiling per kernel family (0 fluid, 1 magnet) and direction
     // one captured iteration per (cfl_valid at its start, sweep-order row (iteration-1) % 6)
     cudaGraphExec_t graphs[2][6] = {};
     uint64_t graph_launches[2][6] = {};
@@ -230,13 +230,13 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
 // Process-wide cache of autotuned tilings, keyed by what decides them: sweep direction, pencil
 // length, number of pencils (rounded up to a power of two), precision and physics.  Contexts
 // created later with the same key start from the tuned tiling.
-using TuneKey = std::tuple<int, int, int, int, int, int>;
+using TuneKey = std::tuple<int, int, int, int, int, int, int>;
 std::mutex g_tune_mu;
 std::map<TuneKey, PencilCfg> g_tuned;
 
-TuneKey tune_key(const Geom& g, int d, size_t elem, const img_config& c) {
+TuneKey tune_key(int kind, const Geom& g, int d, size_t elem, const img_config& c) {
     const long long ncol = g.ncell / g.n[d];
-    return TuneKey(d, g.n[d], pow2ceil((int)std::min<long long>(ncol, 1 << 30)), (int)elem, c.fluid_active,
+    return TuneKey(kind, d, g.n[d], pow2ceil((int)std::min<long long>(ncol, 1 << 30)), (int)elem, c.fluid_active,
                    c.magnet_active);
 }
 
@@ -309,8 +309,8 @@ int launch_blocks(long long work, int bs = 256) {
 }
 
 // Sweep geometry of direction d with the context's pencil tiling (cells per thread CPT).
-SweepGeom sweep_geom(const img_ctx* ctx, int d, int cpt) {
-    const PencilCfg& pcf = ctx->pcfg[d];
+SweepGeom sweep_geom(const img_ctx* ctx, int d, const PencilCfg& pcf) {
+    const int cpt = pcf.cpt;
     SweepGeom s{};
     s.g = ctx->g;
     s.d = d;
@@ -339,8 +339,7 @@ bool fade_on(const img_config& c, int d, int cls_lo, int cls_hi) {
 }
 
 template <typename T>
-PencilLaunch pencil_launch(const img_ctx* ctx, int d, size_t smem, unsigned grid_y, bool fade) {
-    const PencilCfg& pcf = ctx->pcfg[d];
+PencilLaunch pencil_launch(const img_ctx* ctx, const PencilCfg& pcf, int d, size_t smem, unsigned grid_y, bool fade) {
     const long long ncol = ctx->g.ncell / ctx->g.n[d];
     const long long nb = (ncol + pcf.Wb - 1) / pcf.Wb;
     PencilLaunch L{};
@@ -359,8 +358,8 @@ template <typename T>
 int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     FluidArgs a{};
     const img_config& c = ctx->cfg;
-    const PencilCfg& pcf = ctx->pcfg[d];
-    a.sg = sweep_geom(ctx, d, pcf.cpt);
+    const PencilCfg& pcf = ctx->pcfg[0][d];
+    a.sg = sweep_geom(ctx, d, pcf);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.tm = ctx->tm;
     a.gamma = c.gamma;
@@ -381,7 +380,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.cfl = cfl;
-    const PencilLaunch L = pencil_launch<T>(ctx, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
                                             fade_on(c, d, CLS_MASS, CLS_ENER));
     if (ctx->rec) {
         OpRec r{};
@@ -409,8 +408,8 @@ template <typename T>
 void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     const img_config& c = ctx->cfg;
     int d = X - 1;
-    PencilCfg pcf = ctx->pcfg[d];
-    a.sg = sweep_geom(ctx, d, pcf.cpt);
+    const PencilCfg& pcf = ctx->pcfg[1][d];
+    a.sg = sweep_geom(ctx, d, pcf);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.F[0] = ctx->scratch[0];
     a.F[1] = ctx->scratch[1];
@@ -451,8 +450,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     MagArgs a{};
     fill_mag_args<T>(ctx, X, I1, I2, a);
     const int d = X - 1;
-    const PencilCfg& pcf = ctx->pcfg[d];
-    const PencilLaunch L = pencil_launch<T>(ctx, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 2,
+    const PencilCfg& pcf = ctx->pcfg[1][d];
+    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 2,
                                             fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
     if (ctx->rec) {
         OpRec r{};
@@ -527,17 +526,18 @@ int set_kernel_attributes(img_ctx* ctx) {
             dn = true;
         }
     }
-    for (int d = 0; d < 3; ++d) {
-        const PencilCfg& p = ctx->pcfg[d];
-        if (ctx->g.n[d] < 3) continue;
-        PencilLaunch L = pencil_launch<T>(ctx, d, fluid_smem_bytes<T>(p.G * p.cpt, p.Wb), 1, false);
-        int nclusters = 0;
-        cudaError_t e = fluid_max_clusters<T>(L, &nclusters);
-        if (e != cudaSuccess || nclusters < 1)
-            return fail(ctx, IMG_ERR_UNSUPPORTED, "pencil configuration for dim %d (block %d, cluster %d, smem %zu) "
-                        "cannot be scheduled: %s", d, p.NT, p.CL, L.smem,
-                        e != cudaSuccess ? cudaGetErrorString(e) : "0 active clusters");
-    }
+    for (int kind = 0; kind < 2; ++kind)
+        for (int d = 0; d < 3; ++d) {
+            const PencilCfg& p = ctx->pcfg[kind][d];
+            if (ctx->g.n[d] < 3) continue;
+            PencilLaunch L = pencil_launch<T>(ctx, p, d, fluid_smem_bytes<T>(p.G * p.cpt, p.Wb), 1, false);
+            int nclusters = 0;
+            cudaError_t e = fluid_max_clusters<T>(L, &nclusters);
+            if (e != cudaSuccess || nclusters < 1)
+                return fail(ctx, IMG_ERR_UNSUPPORTED, "pencil configuration for dim %d (block %d, cluster %d, smem %zu) "
+                            "cannot be scheduled: %s", d, p.NT, p.CL, L.smem,
+                            e != cudaSuccess ? cudaGetErrorString(e) : "0 active clusters");
+        }
     return IMG_OK;
 }
 
@@ -746,12 +746,13 @@ int img_create(img_ctx** out, const img_config* cfg) {
     g.s[1] = g.n[0];
     g.s[2] = (long long)g.n[0] * g.n[1];
     g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (int d = 0; d < 3; ++d) {
-        ctx->pcfg[d] = choose_pencil(g, d, ctx->elem);
-        std::lock_guard<std::mutex> lock(g_tune_mu);
-        auto it = g_tuned.find(tune_key(g, d, ctx->elem, *cfg));
-        if (it != g_tuned.end()) ctx->pcfg[d] = it->second;
-    }
+    for (int kind = 0; kind < 2; ++kind)
+        for (int d = 0; d < 3; ++d) {
+            ctx->pcfg[kind][d] = choose_pencil(g, d, ctx->elem);
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            auto it = g_tuned.find(tune_key(kind, g, d, ctx->elem, *cfg));
+            if (it != g_tuned.end()) ctx->pcfg[kind][d] = it->second;
+        }
 
     auto bail = [&](int code) {
         if (ctx->slab) cudaFree(ctx->slab);
@@ -1617,45 +1618,50 @@ int img_autotune(img_ctx* ctx, int trials) {
     if (cudaMemcpyAsync(backup, ctx->slab, ctx->slab_bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
         rc = fail(ctx, IMG_ERR_CUDA, "autotune setup failed");
-    for (int d = 0; d < 3 && rc == IMG_OK; ++d) {
-        if (ctx->g.n[d] < 3) continue;
-        PencilCfg best = ctx->pcfg[d];
-        float best_ms = 1e30f;
-        for (const PencilCfg& cand : pencil_candidates(ctx->g, d)) {
-            ctx->pcfg[d] = cand;
-            int ncl = 0;
-            const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
-                                             : fluid_smem_bytes<float>(cand.G * cand.cpt, cand.Wb);
-            PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, d, fs, 1, false) : pencil_launch<float>(ctx, d, fs, 1, false);
-            cudaError_t ce = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
-            if (ce != cudaSuccess || ncl < 1) {
-                cudaGetLastError();
-                continue;
+    // each kernel family is tuned on its own sweeps: the fluid sweep for the fluid tiling, the
+    // magnet sweep (chain + CT) for the magnet tiling
+    for (int kind = 0; kind < 2 && rc == IMG_OK; ++kind) {
+        if (kind == 0 ? !ctx->cfg.fluid_active : !ctx->cfg.magnet_active) continue;
+        for (int d = 0; d < 3 && rc == IMG_OK; ++d) {
+            if (ctx->g.n[d] < 3) continue;
+            PencilCfg best = ctx->pcfg[kind][d];
+            float best_ms = 1e30f;
+            for (const PencilCfg& cand : pencil_candidates(ctx->g, d)) {
+                ctx->pcfg[kind][d] = cand;
+                int ncl = 0;
+                const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
+                                                 : fluid_smem_bytes<float>(cand.G * cand.cpt, cand.Wb);
+                PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, cand, d, fs, 1, false)
+                                                : pencil_launch<float>(ctx, cand, d, fs, 1, false);
+                cudaError_t ce = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
+                if (ce != cudaSuccess || ncl < 1) {
+                    cudaGetLastError();
+                    continue;
+                }
+                auto sweep = [&]() {
+                    return kind == 0 ? fluid_sweep(ctx, d + 1, false)
+                                     : magnet_sweep(ctx, d + 1, FWD_MI[d][0], FWD_MI[d][1]);
+                };
+                bool ok = sweep() == IMG_OK;                                   // warm-up
+                ok = ok && cudaEventRecord(e0, ctx->stream) == cudaSuccess;
+                for (int t = 0; ok && t < trials; ++t) ok = sweep() == IMG_OK;
+                ok = ok && cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+                float ms = 0.f;
+                ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+                restore();
+                if (!ok) {
+                    cudaGetLastError();
+                    continue;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = cand;
+                }
             }
-            auto sweep = [&]() {
-                int r = ctx->cfg.fluid_active ? fluid_sweep(ctx, d + 1, false) : IMG_OK;
-                if (r == IMG_OK && ctx->cfg.magnet_active) r = magnet_sweep(ctx, d + 1, FWD_MI[d][0], FWD_MI[d][1]);
-                return r;
-            };
-            bool ok = sweep() == IMG_OK;                                   // warm-up
-            ok = ok && cudaEventRecord(e0, ctx->stream) == cudaSuccess;
-            for (int t = 0; ok && t < trials; ++t) ok = sweep() == IMG_OK;
-            ok = ok && cudaEventRecord(e1, ctx->stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
-            float ms = 0.f;
-            ok = ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
-            restore();
-            if (!ok) {
-                cudaGetLastError();
-                continue;
-            }
-            if (ms < best_ms) {
-                best_ms = ms;
-                best = cand;
-            }
+            ctx->pcfg[kind][d] = best;
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            g_tuned[tune_key(kind, ctx->g, d, ctx->elem, ctx->cfg)] = best;
         }
-        ctx->pcfg[d] = best;
-        std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tuned[tune_key(ctx->g, d, ctx->elem, ctx->cfg)] = best;
     }
     restore();
     cudaStreamSynchronize(ctx->stream);
@@ -1668,22 +1674,20 @@ int img_autotune(img_ctx* ctx, int trials) {
 }
 
 int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
-    if (!ctx || !cfg || dim < 1 || dim > 3) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
+    if (!ctx || !cfg || dim < 1 || dim > 6) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
     if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot retile a batch member");
-    const int d = dim - 1;
+    const int kind = (dim - 1) / 3, d = (dim - 1) % 3;
     for (const PencilCfg& c : pencil_candidates(ctx->g, d)) {
         if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4]) continue;
         int ncl = 0;
-        const PencilCfg old = ctx->pcfg[d];
-        ctx->pcfg[d] = c;
         const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(c.G * c.cpt, c.Wb) : fluid_smem_bytes<float>(c.G * c.cpt, c.Wb);
-        PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, d, fs, 1, false) : pencil_launch<float>(ctx, d, fs, 1, false);
+        PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, c, d, fs, 1, false) : pencil_launch<float>(ctx, c, d, fs, 1, false);
         cudaError_t e = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
         if (e != cudaSuccess || ncl < 1) {
             cudaGetLastError();
-            ctx->pcfg[d] = old;
             return fail(ctx, IMG_ERR_UNSUPPORTED, "tiling cannot be scheduled on this device");
         }
+        ctx->pcfg[kind][d] = c;
         drop_graphs(ctx);
         return IMG_OK;
     }
@@ -1691,8 +1695,8 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
 }
 
 int img_get_tiling(const img_ctx* ctx, int dim, int out[5]) {
-    if (!ctx || !out || dim < 1 || dim > 3) return IMG_ERR_ARG;
-    const PencilCfg& p = ctx->pcfg[dim - 1];
+    if (!ctx || !out || dim < 1 || dim > 6) return IMG_ERR_ARG;
+    const PencilCfg& p = ctx->pcfg[(dim - 1) / 3][(dim - 1) % 3];
     out[0] = p.Wb;
     out[1] = p.G;
     out[2] = p.CL;

@@ -155,7 +155,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--autotune", action="store_true", help="tune the pencil tilings first (as bench.py does)")
     ap.add_argument("--tiling", action="append", default=[],
-                    help="dim=Wb,G,CL,NT,cpt for one direction, e.g. x=2,128,1,256,4 (repeatable)")
+                    help="dim=Wb,G,CL,NT,cpt for the fluid sweeps along one direction, e.g. x=2,128,1,256,4, or "
+                         "mx=... for the magnet sweeps (repeatable)")
     a = ap.parse_args(argv)
     from imogen_b200 import ImogenRun
 
@@ -164,7 +165,8 @@ def main(argv=None):
     run.set_state(*st)
     for spec in a.tiling:
         dim, vals = spec.split("=")
-        run.set_tiling("xyz".index(dim) + 1, [int(v) for v in vals.split(",")])
+        kind = "magnet" if dim.startswith("m") else "fluid"
+        run.set_tiling("xyz".index(dim[-1]) + 1, [int(v) for v in vals.split(",")], kind=kind)
     if a.autotune:
         run.iterate()
         print("tiling", run.autotune(trials=3))

@@ -248,23 +248,26 @@ class ImogenRun:
         return n.value
 
     def autotune(self, trials=3):
-        """Pick the fastest pencil tiling per swept direction (img_autotune); returns tiling()."""
+        """Pick the fastest pencil tiling per swept direction and kernel family (img_autotune);
+        returns {"fluid": tiling("fluid"), "magnet": tiling("magnet")}."""
         check(lib().img_autotune(self._h, int(trials)), self._h)
-        return self.tiling()
+        return {"fluid": self.tiling("fluid"), "magnet": self.tiling("magnet")}
 
-    def tiling(self):
-        """{dim: (pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread)}"""
+    def tiling(self, kind="fluid"):
+        """{dim: (pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread)}
+        of the fluid or the magnet sweeps."""
         out = {}
+        base = 0 if kind == "fluid" else 3
         for d in (1, 2, 3):
             t = (ctypes.c_int * 5)()
-            check(lib().img_get_tiling(self._h, d, t), self._h)
+            check(lib().img_get_tiling(self._h, base + d, t), self._h)
             out[d] = tuple(t)
         return out
 
-    def set_tiling(self, dim, tiling):
-        """Use one of the accepted tilings for direction dim (1..3); see tiling()."""
+    def set_tiling(self, dim, tiling, kind="fluid"):
+        """Use one of the accepted tilings for direction dim (1..3) of the fluid or magnet sweeps."""
         t = (ctypes.c_int * 5)(*[int(v) for v in tiling])
-        check(lib().img_set_tiling(self._h, int(dim), t), self._h)
+        check(lib().img_set_tiling(self._h, int(dim) + (0 if kind == "fluid" else 3), t), self._h)
 
     def progress(self):
         """(simulated time, iterations run, stopped) from the device clock (synchronises)."""
