@@ -57,6 +57,24 @@ class ClockSampler:
         self._t = None
 
     def _run(self):
+        # NVML when available: a sample every 2 ms, so that even a timed region of a few
+        # milliseconds is covered; otherwise nvidia-smi every 200 ms
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            mx = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+            get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+            bits = (0x8, 0x40, 0x20, 0x4)   # hw slowdown, hw thermal, sw thermal, sw power cap
+            while not self._stop.is_set():
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                r = get_reasons(h)
+                self.samples.append([str(sm), str(mx), ""] + ["Active" if r & b else "Not Active" for b in bits])
+                self._stop.wait(0.002)
+            return
+        except Exception:
+            pass
         while not self._stop.is_set():
             try:
                 out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
