@@ -203,9 +203,11 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
             Wb = std::max(1, 256 / G);
             if (Wb * G < 32) Wb = 32 / G;
             while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
-            if (G > 32) {   // whole warps per pencil, without padding to a power of two
+            if (G > 32) {   // whole warps per pencil, padded to a quarter of the power of two only,
+                            // so that pencils of similar length share a launch shape (batching)
                 const int rows = (N + cpt - 1) / cpt;
-                G = ((rows + CL - 1) / CL + 31) / 32 * 32;
+                const int q = std::max(32, G / 4);
+                G = ((rows + CL - 1) / CL + q - 1) / q * q;
             }
         } else if (cpt == 1 && G <= 16) {
             // short pencils: many of them side by side, at least a warp of x per row (one CTA
