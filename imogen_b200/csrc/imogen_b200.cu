@@ -185,6 +185,84 @@ std::vector<double> fade_coefficients(int f) {
     return out;
 }
 
+// Dynamic shared memory per CTA the pencil kernels may use (the opt-in 227 KB, less a margin for
+// their static shared memory).
+constexpr size_t kPencilSmemLimit = 210 * 1024;
+
+bool tiling_fits(const PencilCfg& p, size_t elem) {
+    return (elem == 8 ? fluid_smem_bytes<double>(p.G * p.cpt, p.Wb) : fluid_smem_bytes<float>(p.G * p.cpt, p.Wb)) <=
+           kPencilSmemLimit;
+}
+
+// Every pencil tiling the kernels accept for direction d (the autotuner's search space): one, two
+// or four cells per thread; along x whole-pencil CTAs of up to 256 or 512 threads; along y and z
+// 2, 4 or 8 pencils per CTA, or for pencils of at most 16 cells 32..512/G pencils; at most 4 CTAs
+// per cluster, and one CTA when pencils sit 32 or more side by side.
+std::vector<PencilCfg> pencil_candidates(const Geom& g, int d, size_t elem) {
+    const int N = g.n[d];
+    const long long ncol = g.ncell / N;
+    std::vector<PencilCfg> out;
+    auto add1 = [&](int Wb, int G, int CL, int cpt) {
+        PencilCfg p;
+        p.Wb = Wb;
+        p.G = G;
+        p.CL = CL;
+        p.NT = Wb * G;
+        p.cpt = cpt;
+        if (CL > 4 || p.NT < 32 || p.NT > 512 || p.NT % 32 || G < 2) return;
+        if ((long long)G * cpt * CL < N) return;
+        if (d != 0 && Wb >= 32 && CL > 1) return;                 // side-by-side pencils: one CTA
+        if (d == 0 && G <= 32 && CL > 1) return;                  // in-warp pencils: one CTA
+        if (!tiling_fits(p, elem)) return;
+        for (const PencilCfg& q : out)
+            if (q.Wb == Wb && q.G == G && q.CL == CL && q.cpt == cpt) return;
+        out.push_back(p);
+    };
+    // each shape also with its pencil spread over twice and four times as many CTAs (less shared
+    // memory per CTA, for long FP64 pencils)
+    auto add = [&](int Wb, int G, int CL, int cpt) {
+        for (; CL <= 4; CL *= 2, G /= 2) {
+            add1(Wb, G, CL, cpt);
+            const int h = G / 2;
+            if (G % 2 || h < 2 || (d == 0 && (h % 32 || h <= 32)) || (d != 0 && (Wb * h) % 32)) break;
+        }
+    };
+    auto up = [](int v, int m) { return (v + m - 1) / m * m; };
+    for (int cpt : {1, 2, 4}) {
+        const int rows = (N + cpt - 1) / cpt;
+        const int G0 = std::max(2, pow2ceil(rows));
+        if (d == 0) {
+            for (int maxnt : {256, 512}) {
+                int G = G0, CL = 1;
+                while (G > maxnt) { G >>= 1; CL <<= 1; }
+                int Wb = std::max(1, maxnt / G);
+                while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
+                if (G > 32 && Wb > 8) continue;   // pencils spanning warps: at most 8 per CTA
+                add(Wb, G, CL, cpt);
+                // whole warps per pencil without the power-of-two padding (G a multiple of 32)
+                if (G > 32) {
+                    const int Gt = up((rows + CL - 1) / CL, 32);
+                    if (Gt < G) add(Wb, Gt, CL, cpt);
+                }
+            }
+        } else {
+            for (int Wb : {2, 4, 8}) {
+                int G = std::max(G0, 32 / Wb), CL = 1;
+                while (Wb * G > 512) { G >>= 1; CL <<= 1; }
+                add(Wb, G, CL, cpt);
+                const int Gt = std::max(up((rows + CL - 1) / CL, 32 / Wb), 32 / Wb);
+                if (Gt < G) add(Wb, Gt, CL, cpt);
+            }
+            if (cpt == 1 && G0 <= 16)
+                for (int Wb = 32; Wb * G0 <= 512; Wb <<= 1) {
+                    if ((long long)Wb / 2 >= ncol && Wb > 32) break;
+                    add(Wb, G0, 1, cpt);
+                }
+        }
+    }
+    return out;
+}
+
 // Pencil tiling of one sweep direction: one cell per thread where the pencil fits a cluster of at
 // most 4 CTAs of 512 threads (2 or 4 cells per thread otherwise).  Along x a CTA holds whole pencil
 // segments of up to 512 rows; along y and z it holds 4 adjacent pencils, so each row of the tile is
@@ -226,7 +304,18 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
         p.cpt = cpt;
         if (CL <= 4) break;   // clusters of 8 CTAs of these kernels do not schedule: more cells per thread
     }
-    return p;
+    if (p.CL <= 4 && tiling_fits(p, elem)) return p;
+    // too much shared memory per CTA (long FP64 pencils): the accepted tiling with the fewest
+    // CTAs per cluster, then the fewest cells per thread, then the most threads
+    PencilCfg best = p;
+    bool found = false;
+    for (const PencilCfg& c : pencil_candidates(g, d, elem)) {
+        if (!found || std::make_tuple(c.CL, c.cpt, -c.NT) < std::make_tuple(best.CL, best.cpt, -best.NT)) {
+            best = c;
+            found = true;
+        }
+    }
+    return best;
 }
 
 // Process-wide cache of autotuned tilings, keyed by what decides them: sweep direction, pencil
@@ -240,63 +329,6 @@ TuneKey tune_key(int kind, const Geom& g, int d, size_t elem, const img_config& 
     const long long ncol = g.ncell / g.n[d];
     return TuneKey(kind, d, g.n[d], pow2ceil((int)std::min<long long>(ncol, 1 << 30)), (int)elem, c.fluid_active,
                    c.magnet_active);
-}
-
-// Every pencil tiling the kernels accept for direction d (the autotuner's search space): one, two
-// or four cells per thread; along x whole-pencil CTAs of up to 256 or 512 threads; along y and z
-// 2, 4 or 8 pencils per CTA, or for pencils of at most 16 cells 32..512/G pencils; at most 4 CTAs
-// per cluster, and one CTA when pencils sit 32 or more side by side.
-std::vector<PencilCfg> pencil_candidates(const Geom& g, int d) {
-    const int N = g.n[d];
-    const long long ncol = g.ncell / N;
-    std::vector<PencilCfg> out;
-    auto add = [&](int Wb, int G, int CL, int cpt) {
-        PencilCfg p;
-        p.Wb = Wb;
-        p.G = G;
-        p.CL = CL;
-        p.NT = Wb * G;
-        p.cpt = cpt;
-        if (CL > 4 || p.NT < 32 || p.NT > 512 || p.NT % 32 || G < 2) return;
-        if ((long long)G * cpt * CL < N) return;
-        for (const PencilCfg& q : out)
-            if (q.Wb == Wb && q.G == G && q.CL == CL && q.cpt == cpt) return;
-        out.push_back(p);
-    };
-    auto up = [](int v, int m) { return (v + m - 1) / m * m; };
-    for (int cpt : {1, 2, 4}) {
-        const int rows = (N + cpt - 1) / cpt;
-        const int G0 = std::max(2, pow2ceil(rows));
-        if (d == 0) {
-            for (int maxnt : {256, 512}) {
-                int G = G0, CL = 1;
-                while (G > maxnt) { G >>= 1; CL <<= 1; }
-                int Wb = std::max(1, maxnt / G);
-                while (Wb > 1 && (long long)Wb / 2 >= ncol && Wb * G > 32) Wb >>= 1;
-                if (G > 32 && Wb > 8) continue;   // pencils spanning warps: at most 8 per CTA
-                add(Wb, G, CL, cpt);
-                // whole warps per pencil without the power-of-two padding (G a multiple of 32)
-                if (G > 32) {
-                    const int Gt = up((rows + CL - 1) / CL, 32);
-                    if (Gt < G) add(Wb, Gt, CL, cpt);
-                }
-            }
-        } else {
-            for (int Wb : {2, 4, 8}) {
-                int G = std::max(G0, 32 / Wb), CL = 1;
-                while (Wb * G > 512) { G >>= 1; CL <<= 1; }
-                add(Wb, G, CL, cpt);
-                const int Gt = std::max(up((rows + CL - 1) / CL, 32 / Wb), 32 / Wb);
-                if (Gt < G) add(Wb, Gt, CL, cpt);
-            }
-            if (cpt == 1 && G0 <= 16)
-                for (int Wb = 32; Wb * G0 <= 512; Wb <<= 1) {
-                    if ((long long)Wb / 2 >= ncol && Wb > 32) break;
-                    add(Wb, G0, 1, cpt);
-                }
-        }
-    }
-    return out;
 }
 
 // Blocks of a pointwise pass (for_cells): units of one 256-cell chunk of an x-row.
@@ -1628,7 +1660,7 @@ int img_autotune(img_ctx* ctx, int trials) {
             if (ctx->g.n[d] < 3) continue;
             PencilCfg best = ctx->pcfg[kind][d];
             float best_ms = 1e30f;
-            for (const PencilCfg& cand : pencil_candidates(ctx->g, d)) {
+            for (const PencilCfg& cand : pencil_candidates(ctx->g, d, ctx->elem)) {
                 ctx->pcfg[kind][d] = cand;
                 int ncl = 0;
                 const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
@@ -1679,7 +1711,7 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
     if (!ctx || !cfg || dim < 1 || dim > 6) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
     if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot retile a batch member");
     const int kind = (dim - 1) / 3, d = (dim - 1) % 3;
-    for (const PencilCfg& c : pencil_candidates(ctx->g, d)) {
+    for (const PencilCfg& c : pencil_candidates(ctx->g, d, ctx->elem)) {
         if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4]) continue;
         int ncl = 0;
         const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(c.G * c.cpt, c.Wb) : fluid_smem_bytes<float>(c.G * c.cpt, c.Wb);

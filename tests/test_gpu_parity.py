@@ -160,3 +160,19 @@ def test_reference_jump_state_fp64():
     o.run()
     g.run()
     _assert_close(o, g, 1e-10, "reference jump state, 40 iterations")
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("grid,magnet", [((4, 2000, 1), False), ((3, 1300, 3), True), ((3, 3, 1100), True)])
+def test_long_pencils_along_y_and_z(grid, magnet, precision):
+    """y and z pencils longer than one CTA (clusters and several cells per thread in those layouts),
+    with transparent ends along the long dimension."""
+    tol = 1e-11 if precision == "fp64" else 2e-5
+    long_dim = "xyz"[int(np.argmax(grid))]
+    bc = {f: ("trans" if f == long_dim else "circ") for f in "xyz"}
+    s = dict(grid=grid, dgrid=tuple(1.0 / max(grid) for _ in grid), gamma=5 / 3, cfl=0.35, bc=bc,
+             limiter="vanleer", magnet=magnet, time_max=1e5, iter_max=6)
+    o, g = make_pair(s, smooth_state(grid, seed=11, mhd=magnet), precision=precision)
+    o.run()
+    g.run()
+    _assert_close(o, g, tol, f"{grid} {precision}")
