@@ -308,12 +308,12 @@ def run_ours(args):
     ke = max(3, args.steps // 2)
     barrier()
     t0 = time.perf_counter()
+    up = dict(zip(names, ins))
+    down = dict(zip(names, outs))
     for _ in range(ke):
-        for nm, a in zip(names, ins):
-            r.upload(nm, a)
+        r.upload_many(up)
         r.iterate()
-        for nm, o in zip(names, outs):
-            r.download(nm, out=o)
+        r.download_many(down)
     r.sync()
     el = time.perf_counter() - t0
     e2e = {"value": ncell * 2 * ke / el, "unit": "zone-updates/s",

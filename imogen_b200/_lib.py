@@ -21,6 +21,7 @@ STATUS = {
 # exported symbols, in header order
 SYMBOLS = (
     "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
+    "img_upload_many", "img_download_many",
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
     "img_get_time", "img_set_time", "img_progress", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count",
@@ -74,6 +75,10 @@ def lib():
     L.img_set_state.argtypes = [vp, dp, dp, dp, dp]
     L.img_upload.argtypes = [vp, ctypes.c_int, dp, ctypes.c_size_t]
     L.img_download.argtypes = [vp, ctypes.c_int, dp, ctypes.c_size_t]
+    L.img_upload_many.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(dp), ctypes.c_size_t]
+    L.img_upload_many.restype = ctypes.c_int
+    L.img_download_many.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(dp), ctypes.c_size_t]
+    L.img_download_many.restype = ctypes.c_int
     L.img_time_update.argtypes = [vp, ctypes.c_int, dp, ip]
     L.img_flux.argtypes = [vp, ctypes.c_int]
     L.img_fluid_sweep.argtypes = [vp, ctypes.c_int]

@@ -567,6 +567,7 @@ int set_kernel_attributes(img_ctx* ctx) {
             PencilLaunch L = pencil_launch<T>(ctx, p, d, fluid_smem_bytes<T>(p.G * p.cpt, p.Wb), 1, false);
             int nclusters = 0;
             cudaError_t e = fluid_max_clusters<T>(L, &nclusters);
+            if (e != cudaSuccess) cudaGetLastError();   // leave no launch error behind for the next call
             if (e != cudaSuccess || nclusters < 1)
                 return fail(ctx, IMG_ERR_UNSUPPORTED, "pencil configuration for dim %d (block %d, cluster %d, smem %zu) "
                             "cannot be scheduled: %s", d, p.NT, p.CL, L.smem,
@@ -879,8 +880,9 @@ int img_destroy(img_ctx* ctx) {
 
 const char* img_last_error(const img_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_err.c_str(); }
 
-int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
-    if (!ctx || !host || var < 0 || var > IMG_VAR_MAGZ) return fail(ctx, IMG_ERR_ARG, "bad upload argument");
+// Enqueue one host -> device array transfer (no synchronisation).
+static int enqueue_upload(img_ctx* ctx, int var, const double* host, size_t n) {
+    if (!host || var < 0 || var > IMG_VAR_MAGZ) return fail(ctx, IMG_ERR_ARG, "bad upload argument");
     if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "upload size %zu != %lld cells", n, ctx->g.ncell);
     if (ctx->elem == 8) {
         CK(cudaMemcpyAsync(ctx->q[var], host, n * 8, cudaMemcpyHostToDevice, ctx->stream));
@@ -891,13 +893,13 @@ int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
         CK(cudaGetLastError());
         ctx->launches += 1;
     }
-    CK(cudaStreamSynchronize(ctx->stream));
     ctx->cfl_valid = false;
     return IMG_OK;
 }
 
-int img_download(img_ctx* ctx, int var, double* host, size_t n) {
-    if (!ctx || !host || var < 0 || var >= NQ) return fail(ctx, IMG_ERR_ARG, "bad download argument");
+// Enqueue one device -> host array transfer (no synchronisation).
+static int enqueue_download(img_ctx* ctx, int var, double* host, size_t n) {
+    if (!host || var < 0 || var >= NQ) return fail(ctx, IMG_ERR_ARG, "bad download argument");
     if (n != (size_t)ctx->g.ncell) return fail(ctx, IMG_ERR_ARG, "download size %zu != %lld cells", n, ctx->g.ncell);
     if (ctx->elem == 8) {
         CK(cudaMemcpyAsync(host, ctx->q[var], n * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -908,6 +910,41 @@ int img_download(img_ctx* ctx, int var, double* host, size_t n) {
         ctx->launches += 1;
         CK(cudaMemcpyAsync(host, ctx->stage, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     }
+    return IMG_OK;
+}
+
+int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    int rc = enqueue_upload(ctx, var, host, n);
+    if (rc != IMG_OK) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return IMG_OK;
+}
+
+int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* const* hosts, size_t n) {
+    if (!ctx || count < 0 || (count && (!var_ids || !hosts))) return fail(ctx, IMG_ERR_ARG, "bad upload argument");
+    for (int i = 0; i < count; ++i) {
+        int rc = enqueue_upload(ctx, var_ids[i], hosts[i], n);
+        if (rc != IMG_OK) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return IMG_OK;
+}
+
+int img_download_many(img_ctx* ctx, int count, const int* var_ids, double* const* hosts, size_t n) {
+    if (!ctx || count < 0 || (count && (!var_ids || !hosts))) return fail(ctx, IMG_ERR_ARG, "bad download argument");
+    for (int i = 0; i < count; ++i) {
+        int rc = enqueue_download(ctx, var_ids[i], hosts[i], n);
+        if (rc != IMG_OK) return rc;
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return IMG_OK;
+}
+
+int img_download(img_ctx* ctx, int var, double* host, size_t n) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    int rc = enqueue_download(ctx, var, host, n);
+    if (rc != IMG_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
 }

@@ -203,6 +203,27 @@ class ImogenRun:
         check(lib().img_download(self._h, VAR[name], _dp(out), out.size), self._h)
         return out
 
+    def upload_many(self, arrays):
+        """{name: array} -> X.array = value for each, one synchronisation (flat C-contiguous float64
+        buffers, e.g. pinned host memory, are used without a copy)."""
+        names = list(arrays)
+        flat = [self._flat(arrays[k]) for k in names]
+        ids = (ctypes.c_int * len(names))(*[VAR[k] for k in names])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(names))(*[_dp(a) for a in flat])
+        check(lib().img_upload_many(self._h, len(names), ids, ptrs, self.ncell), self._h)
+
+    def download_many(self, outs):
+        """{name: out} with out a C-contiguous float64 buffer of ncell values: filled in place, one
+        synchronisation."""
+        names = list(outs)
+        for k in names:
+            o = outs[k]
+            assert o.dtype == np.float64 and o.flags.c_contiguous and o.size == self.ncell
+        ids = (ctypes.c_int * len(names))(*[VAR[k] for k in names])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(names))(*[_dp(outs[k]) for k in names])
+        check(lib().img_download_many(self._h, len(names), ids, ptrs, self.ncell), self._h)
+        return outs
+
     def state(self):
         g = self.download
         return dict(mass=g("mass"), ener=g("ener"),

@@ -83,6 +83,10 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
 /* X.array = value (ImogenArray.m:82-89) for one variable, and X.array reads (get.array). */
 int img_upload(img_ctx* ctx, int var_id, const double* host, size_t n);
 int img_download(img_ctx* ctx, int var_id, double* host, size_t n);
+/* The same for several variables with one synchronisation at the end (hosts[i] holds n values of
+ * variable var_ids[i]); the transfers are queued back to back on the context's stream. */
+int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* const* hosts, size_t n);
+int img_download_many(img_ctx* ctx, int count, const int* var_ids, double* const* hosts, size_t n);
 
 /* TimeManager.update(mass, mom, ener, mag, fluxDirection) (time/TimeManager.m:55-99).  The new
  * dt is computed and applied on the device; dt_out / dir_out may be NULL (no host sync then). */
