@@ -336,7 +336,7 @@ def run_ours(args):
                        "step": "1 iteration = 2 timesteps (X,Y fluid+magnet each)",
                        "l2": "flushed (512 MB write) before every timed step", "parallelism": f"replicas x{ws}",
                        "tiling": tilings or None,
-                       "tiling_fields": "pencils/CTA, threads/pencil, CTAs/cluster, threads/CTA, cells/thread"},
+                       "tiling_fields": "pencils/CTA, threads/pencil, CTAs/cluster, threads/CTA, cells/thread, components/CTA"},
             "fp64": {"value": v64, "unit": "zone-updates/s", "ms_per_step": 1e3 * results["fp64"] / args.steps},
             "mixed_over_fp64": v / v64,
             "l1_mixed_vs_fp64": l1,

@@ -33,6 +33,7 @@ const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
 // pencil, CPT cells per thread (2, or 4 for long pencils), CL CTAs per cluster.
 struct PencilCfg {
     int Wb = 1, G = 32, CL = 1, NT = 32, cpt = 2;
+    int nqc = 1;   // magnet chain: transverse components per CTA
 };
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -383,6 +384,7 @@ PencilLaunch pencil_launch(const img_ctx* ctx, const PencilCfg& pcf, int d, size
     L.smem = smem;
     L.cluster = pcf.CL;
     L.cpt = pcf.cpt;
+    L.nqc = pcf.nqc;
     L.fade = fade;
     L.stream = ctx->stream;
     return L;
@@ -485,8 +487,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     fill_mag_args<T>(ctx, X, I1, I2, a);
     const int d = X - 1;
     const PencilCfg& pcf = ctx->pcfg[1][d];
-    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 2,
-                                            fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
+                                            2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
     if (ctx->rec) {
         OpRec r{};
         r.elem = sizeof(T);
@@ -1259,7 +1261,7 @@ size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
 
 bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
     return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
-           x.cpt == y.cpt && x.fade == y.fade;
+           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade;
 }
 
 // Turn the members' records into batched launch items and the arena image.
@@ -1697,7 +1699,17 @@ int img_autotune(img_ctx* ctx, int trials) {
             if (ctx->g.n[d] < 3) continue;
             PencilCfg best = ctx->pcfg[kind][d];
             float best_ms = 1e30f;
-            for (const PencilCfg& cand : pencil_candidates(ctx->g, d, ctx->elem)) {
+            std::vector<PencilCfg> cands = pencil_candidates(ctx->g, d, ctx->elem);
+            if (kind == 1) {   // the chain may also take both transverse components per CTA
+                const size_t n0 = cands.size();
+                for (size_t i = 0; i < n0; ++i)
+                    if (cands[i].cpt <= 2) {
+                        PencilCfg c2 = cands[i];
+                        c2.nqc = 2;
+                        cands.push_back(c2);
+                    }
+            }
+            for (const PencilCfg& cand : cands) {
                 ctx->pcfg[kind][d] = cand;
                 int ncl = 0;
                 const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
@@ -1744,12 +1756,16 @@ int img_autotune(img_ctx* ctx, int trials) {
     return rc != IMG_OK ? rc : check_dev_error(ctx);
 }
 
-int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]) {
     if (!ctx || !cfg || dim < 1 || dim > 6) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
     if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot retile a batch member");
     const int kind = (dim - 1) / 3, d = (dim - 1) % 3;
-    for (const PencilCfg& c : pencil_candidates(ctx->g, d, ctx->elem)) {
+    const int nqc = cfg[5];
+    if (nqc != 1 && !(nqc == 2 && kind == 1 && cfg[4] <= 2))
+        return fail(ctx, IMG_ERR_UNSUPPORTED, "two components per CTA: magnet sweeps with at most 2 cells per thread");
+    for (PencilCfg c : pencil_candidates(ctx->g, d, ctx->elem)) {
         if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4]) continue;
+        c.nqc = nqc;
         int ncl = 0;
         const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(c.G * c.cpt, c.Wb) : fluid_smem_bytes<float>(c.G * c.cpt, c.Wb);
         PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, c, d, fs, 1, false) : pencil_launch<float>(ctx, c, d, fs, 1, false);
@@ -1765,7 +1781,7 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]) {
     return fail(ctx, IMG_ERR_UNSUPPORTED, "not a tiling the kernels accept for this direction");
 }
 
-int img_get_tiling(const img_ctx* ctx, int dim, int out[5]) {
+int img_get_tiling(const img_ctx* ctx, int dim, int out[6]) {
     if (!ctx || !out || dim < 1 || dim > 6) return IMG_ERR_ARG;
     const PencilCfg& p = ctx->pcfg[(dim - 1) / 3][(dim - 1) % 3];
     out[0] = p.Wb;
@@ -1773,6 +1789,7 @@ int img_get_tiling(const img_ctx* ctx, int dim, int out[5]) {
     out[2] = p.CL;
     out[3] = p.NT;
     out[4] = p.cpt;
+    out[5] = p.nqc;
     return IMG_OK;
 }
 

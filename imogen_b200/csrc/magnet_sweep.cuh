@@ -104,10 +104,11 @@ __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long ce
 constexpr int MAG_NARR = 4;
 constexpr int MAG_NSLOT = 6;   // per column: lower anchors, upper +1 (e1), +1 (e2), +2 row N, +2 row N+1, +1 (e4)
 
-// Dynamic shared memory of the chain kernel: 4 halo'd arrays + 6 ghost/anchor slots per column.
+// Dynamic shared memory of the chain kernel for NQC components per CTA: 4 halo'd arrays + 6
+// ghost/anchor slots per column, per component.
 template <typename T>
-__host__ __device__ inline size_t mag_smem_bytes(int RC, int Wb) {
-    return sizeof(T) * (size_t)MAG_NARR * tile_rows(RC) * Wb + sizeof(Ghost<T>) * MAG_NSLOT * (size_t)Wb;
+__host__ __device__ inline size_t mag_smem_bytes(int RC, int Wb, int NQC = 1) {
+    return NQC * (sizeof(T) * (size_t)MAG_NARR * tile_rows(RC) * Wb + sizeof(Ghost<T>) * MAG_NSLOT * (size_t)Wb);
 }
 
 // The four upper shift calls of wMag in relaxingMagnet.m:37-45 (+1, +1, +2, +1, in that order; a
@@ -142,23 +143,42 @@ __device__ __forceinline__ double wmag_upper_ghosts(const Tile<T, CPT>& tl, cons
     return e4;
 }
 
-// The chain of one grid, run by CTA (vblock, blockIdx.y) of that grid's launch.
+// Per-component constants of the chain: component I (1-based) of the transverse pair, its BC
+// settings along I and its pointers.
+template <typename T>
+struct ChainComp {
+    int I, e, shiftI, mode_mom_lo, mode_mass_lo, act_mom, act_mass, init_mag;
+    T* BI;
+    T* Fout;
+    __device__ __forceinline__ void init(const MagArgs& a, int q) {
+        I = q ? a.I[1] : a.I[0];
+        e = I - 1;
+        shiftI = q ? a.shiftI[1] : a.shiftI[0];
+        mode_mom_lo = q ? a.modeI_mom[1][0] : a.modeI_mom[0][0];
+        mode_mass_lo = q ? a.modeI_mass[1][0] : a.modeI_mass[0][0];
+        act_mom = q ? a.actI_mom[1] : a.actI_mom[0];
+        act_mass = q ? a.actI_mass[1] : a.actI_mass[0];
+        init_mag = q ? a.init_mag[1] : a.init_mag[0];
+        BI = reinterpret_cast<T*>(a.q[Q_BX + e]);
+        Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
+    }
+};
+
+// The chain of one grid, run by CTA (vblock, blockIdx.y) of that grid's launch: NQC = 1 handles
+// component blockIdx.y, NQC = 2 both transverse components, interleaved stage by stage so that
+// every barrier serves twice the work.
 // FADE: a mag-class BC along X is fade (compiles the damping in).
-template <typename T, int CPT, bool FADE>
+template <typename T, int CPT, bool FADE, int NQC>
 __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
     Tile<T, CPT> tl;
     tl.init(a.sg, vblock);
-    const int q = blockIdx.y;          // which transverse component
-    const int I = q ? a.I[1] : a.I[0];
-    const int shiftI = q ? a.shiftI[1] : a.shiftI[0];
-    const int mode_mom_lo = q ? a.modeI_mom[1][0] : a.modeI_mom[0][0];
-    const int mode_mass_lo = q ? a.modeI_mass[1][0] : a.modeI_mass[0][0];
-    const int act_mom = q ? a.actI_mom[1] : a.actI_mom[0];
-    const int act_mass = q ? a.actI_mass[1] : a.actI_mass[0];
-    const int init_mag = q ? a.init_mag[1] : a.init_mag[0];
-    const int d = a.X - 1, e = I - 1, c = I - 1;
+    const int q0 = NQC == 2 ? 0 : (int)blockIdx.y;
+    ChainComp<T> cp[NQC];
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) cp[q].init(a, q0 + q);
+    const int d = a.X - 1;
     const int N = a.sg.N, Wb = tl.Wb, b = tl.b;
     const Geom& g = a.sg.g;
     const double dt = a.tm->dt;
@@ -166,192 +186,220 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     const T ff2 = T(2) * ff;
     const EdgeTable* et = a.edges;
     const size_t AS = (size_t)tile_rows(tl.RC) * Wb;
-    T* S0 = reinterpret_cast<T*>(smem);
-    T* S1 = S0 + AS;
-    T* S2 = S1 + AS;
-    T* S3 = S2 + AS;
-    Ghost<T>* GS = reinterpret_cast<Ghost<T>*>(S0 + MAG_NARR * AS);   // [slot][column]
-    Ghost<T>* const ANL = GS;            // lower-side fade anchors
-    Ghost<T>* const ANU = GS + Wb;       // upper-side fade anchors (+1 shifts of stages 2-4)
+    // component q: arrays S[q][0..3] at smem + (4q + i) * AS, ghost slots after all arrays
+    T* const SB = reinterpret_cast<T*>(smem);
+    Ghost<T>* const GSB = reinterpret_cast<Ghost<T>*>(SB + NQC * MAG_NARR * AS);
+    auto S = [&](int q, int i) -> T* { return SB + (q * MAG_NARR + i) * AS; };
+    auto GS = [&](int q) -> Ghost<T>* { return GSB + q * MAG_NSLOT * Wb; };
     const double* fc = a.fade;
     const int f = a.fade_f;
     const double binf = a.bc_inf;
     const int mlo = a.modeX[0], mhi = a.modeX[1];
     // the scratch objects of mag(I) for this sweep (mag-class BC along X, no mirror flip)
-    auto edge_of = [&](int kind, int side) -> double* { return et->p[mag_obj(c, d, kind)][d][side]; };
-    // halo jobs: thread g == 0 of a column does the lower side, thread g == 1 the upper side
-    const int job_side = tl.colok && tl.g < 2 ? tl.g : -1;
-    auto halo = [&](T* A, int kind, bool lo_shift, bool hi_shift, int hi_rows) {
-        if (job_side == 0) halo_job(tl, A, ANL, 0, lo_shift, mlo, a.actX, 0, edge_of(kind, 0), binf, hi_rows);
-        if (job_side == 1) halo_job(tl, A, ANU, 1, hi_shift, mhi, a.actX, 0, edge_of(kind, 1), binf, hi_rows);
+    auto edge_of = [&](int q, int kind, int side) -> double* { return et->p[mag_obj(cp[q].e, d, kind)][d][side]; };
+    // halo jobs: (component q, side) is done by thread g == (2q + side) mod G of the column
+    auto job = [&](int q, int side) { return tl.colok && tl.g == (2 * q + side) % tl.G; };
+    auto halo = [&](int q, T* A, int kind, bool lo_shift, bool hi_shift, int hi_rows) {
+        if (job(q, 0)) halo_job(tl, A, GS(q), 0, lo_shift, mlo, a.actX, 0, edge_of(q, kind, 0), binf, hi_rows);
+        if (job(q, 1)) halo_job(tl, A, GS(q) + Wb, 1, hi_shift, mhi, a.actX, 0, edge_of(q, kind, 1), binf, hi_rows);
     };
 
     // ---- corner velocity (magnetFlux.m:18-19): transverse average with mass/mom BCs along I ------
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* pX = reinterpret_cast<const T*>(a.q[Q_PX + d]);
-    T* BI = reinterpret_cast<T*>(a.q[Q_BX + c]);
-    T vgr[CPT], bI[CPT];
-    // the transverse coordinate is the pencil's own (e != d): interior pencils read their lower
-    // neighbour directly; the boundary and fade cases go through the reference's shift
-    const int ie = e == a.sg.d1 ? tl.c1 : tl.c2;
-    const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
-    const bool direct = shiftI && ie > 0 && mode_mom_lo != BC_FADE && mode_mass_lo != BC_FADE;
+    T vgr[NQC][CPT], bI[NQC][CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        vgr[k] = T(0);
-        bI[k] = T(0);
-        if (tl.ok(k)) {
-            const long long o = tl.off(k);
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            T pm, rm;
-            if (direct) {
-                pm = pX[o - se];
-                rm = rho[o - se];
-            } else if (shiftI) {
-                pm = shift_along<T>(g, pX, o, x, y, z, e, -1, mode_mom_lo, act_mom, false,
-                                    et->p[OBJ_PRIM_MOM + d][e][0], fc, f, binf, true);
-                rm = shift_along<T>(g, rho, o, x, y, z, e, -1, mode_mass_lo, act_mass, false,
-                                    et->p[OBJ_PRIM_MASS][e][0], fc, f, binf, true);
-            } else {
-                pm = pX[o];
-                rm = rho[o];
+    for (int q = 0; q < NQC; ++q) {
+        const ChainComp<T>& c = cp[q];
+        // the transverse coordinate is the pencil's own (e != d): interior pencils read their lower
+        // neighbour directly; the boundary and fade cases go through the reference's shift
+        const int ie = c.e == a.sg.d1 ? tl.c1 : tl.c2;
+        const long long se = sel3(c.e, g.s[0], g.s[1], g.s[2]);
+        const bool direct = c.shiftI && ie > 0 && c.mode_mom_lo != BC_FADE && c.mode_mass_lo != BC_FADE;
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            vgr[q][k] = T(0);
+            bI[q][k] = T(0);
+            if (tl.ok(k)) {
+                const long long o = tl.off(k);
+                int x, y, z;
+                tl.coords(k, x, y, z);
+                T pm, rm;
+                if (direct) {
+                    pm = pX[o - se];
+                    rm = rho[o - se];
+                } else if (c.shiftI) {
+                    pm = shift_along<T>(g, pX, o, x, y, z, c.e, -1, c.mode_mom_lo, c.act_mom, false,
+                                        et->p[OBJ_PRIM_MOM + d][c.e][0], fc, f, binf, true);
+                    rm = shift_along<T>(g, rho, o, x, y, z, c.e, -1, c.mode_mass_lo, c.act_mass, false,
+                                        et->p[OBJ_PRIM_MASS][c.e][0], fc, f, binf, true);
+                } else {
+                    pm = pX[o];
+                    rm = rho[o];
+                }
+                vgr[q][k] = (pm + pX[o]) / (rm + rho[o]);
+                bI[q][k] = c.BI[o];
+                if (c.init_mag && on_face(g, x, y, z))
+                    init_edges_cell(g, et, mag_obj(c.e, d, MO_VELGRID), x, y, z, (double)vgr[q][k]);
             }
-            vgr[k] = (pm + pX[o]) / (rm + rho[o]);
-            bI[k] = BI[o];
-            if (init_mag && on_face(g, x, y, z))
-                init_edges_cell(g, et, mag_obj(c, d, MO_VELGRID), x, y, z, (double)vgr[k]);
+            S(q, 0)[tl.idx(k)] = vgr[q][k];
         }
-        S0[tl.idx(k)] = vgr[k];
     }
     tl.csync();
-    halo(S0, MO_VELGRID, true, true, 1);
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) halo(q, S(q, 0), MO_VELGRID, true, true, 1);
     __syncthreads();
     // vg = 0.25*(vg.shift(X,-1) + vg.shift(X,1) + 2*vg)   (magnetFlux.m:21-23)
-    T vg[CPT];
+    T vg[NQC][CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T m1 = shifted<FADE>(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
-        const T p1 = shifted<FADE>(tl, (const T*)S0, ANU, k, +1, mhi, fc, f);
-        vg[k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[k]) : T(0);
-        S1[tl.idx(k)] = vg[k];
-    }
+    for (int q = 0; q < NQC; ++q)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T m1 = shifted<FADE>(tl, (const T*)S(q, 0), GS(q), k, -1, mlo, fc, f);
+            const T p1 = shifted<FADE>(tl, (const T*)S(q, 0), GS(q) + Wb, k, +1, mhi, fc, f);
+            vg[q][k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[q][k]) : T(0);
+            S(q, 1)[tl.idx(k)] = vg[q][k];
+        }
     tl.csync();
-    halo(S1, MO_VELGRID, false, true, 1);
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) halo(q, S(q, 1), MO_VELGRID, false, true, 1);
     __syncthreads();
     // velocityFlow = (vg + vg.shift(X,1)) < 0; store.fluxR = B_I.*vg   (relaxingMagnet.m:17,22)
-    T vf[CPT];
+    T vf[NQC][CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T p1 = shifted<FADE>(tl, (const T*)S1, ANU, k, +1, mhi, fc, f);
-        vf[k] = (vg[k] + p1) < T(0) ? T(1) : T(0);
-        const T F = bI[k] * vg[k];
-        S2[tl.idx(k)] = F;
-        if (init_mag && tl.ok(k)) {
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_STORE_R), x, y, z, (double)F);
+    for (int q = 0; q < NQC; ++q)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T p1 = shifted<FADE>(tl, (const T*)S(q, 1), GS(q) + Wb, k, +1, mhi, fc, f);
+            vf[q][k] = (vg[q][k] + p1) < T(0) ? T(1) : T(0);
+            const T F = bI[q][k] * vg[q][k];
+            S(q, 2)[tl.idx(k)] = F;
+            if (cp[q].init_mag && tl.ok(k)) {
+                int x, y, z;
+                tl.coords(k, x, y, z);
+                if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_STORE_R), x, y, z, (double)F);
+            }
         }
-    }
     tl.csync();
-    halo(S2, MO_STORE_R, false, true, 1);
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) halo(q, S(q, 2), MO_STORE_R, false, true, 1);
     __syncthreads();
     // store.fluxR = F.*(1-vf) + F.shift(X,1).*vf   (relaxingMagnet.m:23-24)
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T F = S2[tl.idx(k)];
-        const T Fp = shifted<FADE>(tl, (const T*)S2, ANU, k, +1, mhi, fc, f);
-        S3[tl.idx(k)] = F * (T(1) - vf[k]) + Fp * vf[k];
-    }
+    for (int q = 0; q < NQC; ++q)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T F = S(q, 2)[tl.idx(k)];
+            const T Fp = shifted<FADE>(tl, (const T*)S(q, 2), GS(q) + Wb, k, +1, mhi, fc, f);
+            S(q, 3)[tl.idx(k)] = F * (T(1) - vf[q][k]) + Fp * vf[q][k];
+        }
     tl.csync();
-    halo(S3, MO_STORE_R, true, false, 1);
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) halo(q, S(q, 3), MO_STORE_R, true, false, 1);
     __syncthreads();
     // store = B_I - ff*(fluxR - fluxR.shift(X,-1)); wMag = store.*velGrid   (relaxingMagnet.m:26-33)
-    T W[CPT];
+    T W[NQC][CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T Fu = S3[tl.idx(k)];
-        const T st = bI[k] - ff * (Fu - shifted<FADE>(tl, (const T*)S3, ANL, k, -1, mlo, fc, f));
-        W[k] = st * vg[k];
-        S0[tl.idx(k)] = W[k];
-        if (init_mag && tl.ok(k)) {
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_WMAG), x, y, z, (double)W[k]);
+    for (int q = 0; q < NQC; ++q)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T Fu = S(q, 3)[tl.idx(k)];
+            const T st = bI[q][k] - ff * (Fu - shifted<FADE>(tl, (const T*)S(q, 3), GS(q), k, -1, mlo, fc, f));
+            W[q][k] = st * vg[q][k];
+            S(q, 0)[tl.idx(k)] = W[q][k];
+            if (cp[q].init_mag && tl.ok(k)) {
+                int x, y, z;
+                tl.coords(k, x, y, z);
+                if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_WMAG), x, y, z, (double)W[q][k]);
+            }
         }
-    }
     tl.csync();
     // wMag: one lower shift (an ordinary halo job; the upper side only copies the next rank's two
     // rows) and four upper shift calls whose ghosts differ, kept in slots by every rank that owns
     // row N-1 or N-2.  The edge's new state is stored after the next cluster barrier, once every
     // rank has read the old one.
-    double e4 = 0.0;
-    halo(S0, MO_WMAG, true, false, 2);
+    double e4[NQC];
     const bool own_end = tl.rank == tl.rank_hi || (tl.rank + 1 == tl.rank_hi && tl.N - 1 == tl.rank_hi * tl.RC);
-    if (job_side == 1 && own_end) e4 = wmag_upper_ghosts(tl, (const T*)S0, GS, mhi, a.actX, edge_of(MO_WMAG, 1), binf);
-    else if (job_side == 1 && mhi == BC_FADE) {   // fade anchors of the +1 and +2 shifts on the other ranks
-        GS[1 * Wb + b] = GS[2 * Wb + b] = GS[5 * Wb + b] = fade_anchors(tl, (const T*)S0, +1);
-        Ghost<T> w2;
-        w2.g = T(0);
-        w2.s0 = tl.row((const T*)S0, N > 2 ? 2 : N - 1);
-        w2.sN1 = tl.row((const T*)S0, N - 1);
-        GS[3 * Wb + b] = w2;
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) {
+        e4[q] = 0.0;
+        halo(q, S(q, 0), MO_WMAG, true, false, 2);
+        Ghost<T>* gs = GS(q);
+        if (job(q, 1) && own_end)
+            e4[q] = wmag_upper_ghosts(tl, (const T*)S(q, 0), gs, mhi, a.actX, edge_of(q, MO_WMAG, 1), binf);
+        else if (job(q, 1) && mhi == BC_FADE) {   // fade anchors of the +1 and +2 shifts on the other ranks
+            gs[1 * Wb + b] = gs[2 * Wb + b] = gs[5 * Wb + b] = fade_anchors(tl, (const T*)S(q, 0), +1);
+            Ghost<T> w2;
+            w2.g = T(0);
+            w2.s0 = tl.row((const T*)S(q, 0), N > 2 ? 2 : N - 1);
+            w2.sN1 = tl.row((const T*)S(q, 0), N - 1);
+            gs[3 * Wb + b] = w2;
+        }
     }
     __syncthreads();
-    T Fl[CPT];
+    T Fl[NQC][CPT];
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T w = W[k], v = vf[k];
-        const int ix = tl.idx(k);
-        const int r = tl.grow(k);
-        T p1a = S0[ix + tl.rs], p1b = p1a, p1d = p1a, p2 = S0[ix + 2 * tl.rs];
-        if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
-            if (r == N - 1) {
-                p1a = GS[1 * Wb + b].g;
-                p1b = GS[2 * Wb + b].g;
-                p1d = GS[5 * Wb + b].g;
-                p2 = GS[4 * Wb + b].g;
-            } else {
-                p2 = GS[3 * Wb + b].g;
+    for (int q = 0; q < NQC; ++q) {
+        const T* A = S(q, 0);
+        const Ghost<T>* gs = GS(q);
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T w = W[q][k], v = vf[q][k];
+            const int ix = tl.idx(k);
+            const int r = tl.grow(k);
+            T p1a = A[ix + tl.rs], p1b = p1a, p1d = p1a, p2 = A[ix + 2 * tl.rs];
+            if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
+                if (r == N - 1) {
+                    p1a = gs[1 * Wb + b].g;
+                    p1b = gs[2 * Wb + b].g;
+                    p1d = gs[5 * Wb + b].g;
+                    p2 = gs[4 * Wb + b].g;
+                } else {
+                    p2 = gs[3 * Wb + b].g;
+                }
             }
-        }
-        if (FADE && mhi == BC_FADE) {
-            const Ghost<T>& u1 = GS[1 * Wb + b];
-            const Ghost<T>& u2 = GS[3 * Wb + b];
-            p1a = fade_apply(p1a, r, N, fc, f, u1.s0, u1.sN1);
-            p1b = fade_apply(p1b, r, N, fc, f, u1.s0, u1.sN1);
-            p1d = fade_apply(p1d, r, N, fc, f, u1.s0, u1.sN1);
-            p2 = fade_apply(p2, r, N, fc, f, u2.s0, u2.sN1);
-        }
-        const T m1 = shifted<FADE>(tl, (const T*)S0, ANL, k, -1, mlo, fc, f);
-        const T fx = w * (T(1) - v) + p1a * v;
-        const T dFluxR = p1b - (v * p2 + (T(1) - v) * w);
-        const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
-        Fl[k] = fx + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
-        S1[ix] = Fl[k];
-        if (init_mag && tl.ok(k)) {
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(c, d, MO_FLUX), x, y, z, (double)fx);
+            if (FADE && mhi == BC_FADE) {
+                const Ghost<T>& u1 = gs[1 * Wb + b];
+                const Ghost<T>& u2 = gs[3 * Wb + b];
+                p1a = fade_apply(p1a, r, N, fc, f, u1.s0, u1.sN1);
+                p1b = fade_apply(p1b, r, N, fc, f, u1.s0, u1.sN1);
+                p1d = fade_apply(p1d, r, N, fc, f, u1.s0, u1.sN1);
+                p2 = fade_apply(p2, r, N, fc, f, u2.s0, u2.sN1);
+            }
+            const T m1 = shifted<FADE>(tl, A, gs, k, -1, mlo, fc, f);
+            const T fx = w * (T(1) - v) + p1a * v;
+            const T dFluxR = p1b - (v * p2 + (T(1) - v) * w);
+            const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
+            Fl[q][k] = fx + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
+            S(q, 1)[ix] = Fl[q][k];
+            if (cp[q].init_mag && tl.ok(k)) {
+                int x, y, z;
+                tl.coords(k, x, y, z);
+                if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_FLUX), x, y, z, (double)fx);
+            }
         }
     }
     tl.csync();
-    if (job_side == 1 && tl.rank == tl.rank_hi && mhi == BC_TRANS && a.actX) {
-        double* eh = edge_of(MO_WMAG, 1);
-        if (eh) eh[tl.col] = e4;
+#pragma unroll
+    for (int q = 0; q < NQC; ++q) {
+        if (job(q, 1) && tl.rank == tl.rank_hi && mhi == BC_TRANS && a.actX) {
+            double* eh = edge_of(q, MO_WMAG, 1);
+            if (eh) eh[tl.col] = e4[q];
+        }
+        halo(q, S(q, 1), MO_FLUX, true, false, 1);
     }
-    halo(S1, MO_FLUX, true, false, 1);
     __syncthreads();
     // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49); F_I -> scratch for CT
-    T* Fout = reinterpret_cast<T*>(q ? a.F[1] : a.F[0]);
 #pragma unroll
-    for (int k = 0; k < CPT; ++k) {
-        const T fm = shifted<FADE>(tl, (const T*)S1, ANL, k, -1, mlo, fc, f);
-        if (!tl.ok(k)) continue;
-        const long long o = tl.off(k);
-        BI[o] = bI[k] - ff2 * (Fl[k] - fm);
-        Fout[o] = Fl[k];
-    }
+    for (int q = 0; q < NQC; ++q)
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const T fm = shifted<FADE>(tl, (const T*)S(q, 1), GS(q), k, -1, mlo, fc, f);
+            if (!tl.ok(k)) continue;
+            const long long o = tl.off(k);
+            cp[q].BI[o] = bI[q][k] - ff2 * (Fl[q][k] - fm);
+            cp[q].Fout[o] = Fl[q][k];
+        }
     if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
 }
 
@@ -479,9 +527,9 @@ __device__ __forceinline__ void mag_cell_body(const MagArgs& a, unsigned vblock,
     });
 }
 
-template <typename T, int CPT, bool FADE>
-__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
-    mag_chain_body<T, CPT, FADE>(a, blockIdx.x);
+template <typename T, int CPT, bool FADE, int NQC>
+__global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
+    mag_chain_body<T, CPT, FADE, NQC>(a, blockIdx.x);
 }
 
 // CT and cell passes are latency-bound: at most 64 registers so that 4 CTAs of 256 threads share an SM.
@@ -496,14 +544,14 @@ __global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
 }
 
 // The same passes over many grids in one launch (BlockMap per CTA, arguments per member).
-template <typename T, int CPT, bool FADE>
-__global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) mag_chain_batch_kernel(const MagArgs* __restrict__ args,
+template <typename T, int CPT, bool FADE, int NQC>
+__global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_batch_kernel(const MagArgs* __restrict__ args,
                                                                                 const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    mag_chain_body<T, CPT, FADE>(sa, (unsigned)bm.block);
+    mag_chain_body<T, CPT, FADE, NQC>(sa, (unsigned)bm.block);
 }
 
 template <typename T>

@@ -13,6 +13,7 @@ struct PencilLaunch {
     size_t smem;               // dynamic shared memory per CTA
     int cluster;               // CTAs per cluster along the pencil
     int cpt;                   // cells per thread (1, 2 or 4)
+    int nqc;                   // magnet chain: transverse components per CTA (1, or 2 with cpt <= 2)
     bool fade;                 // a fade BC on this sweep direction
     cudaStream_t stream;
 };

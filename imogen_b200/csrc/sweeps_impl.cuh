@@ -56,11 +56,12 @@ void (*fluid_kernel(int cpt))(const FluidArgs) {
 }
 
 template <typename T, bool FADE>
-void (*chain_kernel(int cpt))(const MagArgs) {
+void (*chain_kernel(int cpt, int nqc))(const MagArgs) {
+    if (nqc == 2) return cpt == 1 ? mag_chain_kernel<T, 1, FADE, 2> : mag_chain_kernel<T, 2, FADE, 2>;
     switch (cpt) {
-        case 1: return mag_chain_kernel<T, 1, FADE>;
-        case 2: return mag_chain_kernel<T, 2, FADE>;
-        default: return mag_chain_kernel<T, 4, FADE>;
+        case 1: return mag_chain_kernel<T, 1, FADE, 1>;
+        case 2: return mag_chain_kernel<T, 2, FADE, 1>;
+        default: return mag_chain_kernel<T, 4, FADE, 1>;
     }
 }
 
@@ -74,11 +75,12 @@ void (*fluid_batch_kernel(int cpt))(const FluidArgs*, const BlockMap*) {
 }
 
 template <typename T, bool FADE>
-void (*chain_batch_kernel(int cpt))(const MagArgs*, const BlockMap*) {
+void (*chain_batch_kernel(int cpt, int nqc))(const MagArgs*, const BlockMap*) {
+    if (nqc == 2) return cpt == 1 ? mag_chain_batch_kernel<T, 1, FADE, 2> : mag_chain_batch_kernel<T, 2, FADE, 2>;
     switch (cpt) {
-        case 1: return mag_chain_batch_kernel<T, 1, FADE>;
-        case 2: return mag_chain_batch_kernel<T, 2, FADE>;
-        default: return mag_chain_batch_kernel<T, 4, FADE>;
+        case 1: return mag_chain_batch_kernel<T, 1, FADE, 1>;
+        case 2: return mag_chain_batch_kernel<T, 2, FADE, 1>;
+        default: return mag_chain_batch_kernel<T, 4, FADE, 1>;
     }
 }
 
@@ -95,8 +97,8 @@ cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map,
 
 template <typename T>
 cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
-    return launch_pencil_batch(L.fade ? chain_batch_kernel<T, true>(L.cpt) : chain_batch_kernel<T, false>(L.cpt), args,
-                               map, L);
+    return launch_pencil_batch(L.fade ? chain_batch_kernel<T, true>(L.cpt, L.nqc) : chain_batch_kernel<T, false>(L.cpt, L.nqc),
+                               args, map, L);
 }
 
 template <typename T>
@@ -124,7 +126,7 @@ cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool m
 
 template <typename T>
 cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L) {
-    return launch_pencil(L.fade ? chain_kernel<T, true>(L.cpt) : chain_kernel<T, false>(L.cpt), a, L);
+    return launch_pencil(L.fade ? chain_kernel<T, true>(L.cpt, L.nqc) : chain_kernel<T, false>(L.cpt, L.nqc), a, L);
 }
 
 template <typename T>
@@ -162,11 +164,13 @@ cudaError_t fluid_attributes(int cpt, int optin) {
 
 template <typename T>
 cudaError_t chain_attributes(int cpt, int optin) {
-    for (int v = 0; v < 2; ++v) {
-        cudaError_t e = allow_max_smem(v ? chain_kernel<T, true>(cpt) : chain_kernel<T, false>(cpt), optin);
-        if (e == cudaSuccess) e = allow_max_smem(v ? chain_batch_kernel<T, true>(cpt) : chain_batch_kernel<T, false>(cpt), optin);
-        if (e != cudaSuccess) return e;
-    }
+    for (int v = 0; v < 2; ++v)
+        for (int nqc = 1; nqc <= (cpt <= 2 ? 2 : 1); ++nqc) {
+            cudaError_t e = allow_max_smem(v ? chain_kernel<T, true>(cpt, nqc) : chain_kernel<T, false>(cpt, nqc), optin);
+            if (e == cudaSuccess)
+                e = allow_max_smem(v ? chain_batch_kernel<T, true>(cpt, nqc) : chain_batch_kernel<T, false>(cpt, nqc), optin);
+            if (e != cudaSuccess) return e;
+        }
     return cudaSuccess;
 }
 

@@ -151,10 +151,11 @@ int img_get_stream(img_ctx* ctx, void** stream);
  * device copy of the context.  No reference counterpart. */
 int img_autotune(img_ctx* ctx, int trials);
 /* Tiling of slot dim: 1..3 the fluid sweeps along x, y, z, 4..6 the magnet sweeps along x, y, z;
- * out = {pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread}. */
-int img_get_tiling(const img_ctx* ctx, int dim, int out[5]);
+ * out = {pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread,
+ * transverse components per CTA (magnet: 1 or 2; fluid: 1)}. */
+int img_get_tiling(const img_ctx* ctx, int dim, int out[6]);
 /* Set the tiling of slot dim to one of those the autotuner may pick (same field order). */
-int img_set_tiling(img_ctx* ctx, int dim, const int cfg[5]);
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]);
 
 /* Number of kernels the context has launched so far.  No reference counterpart. */
 int img_launch_count(const img_ctx* ctx, uint64_t* count);

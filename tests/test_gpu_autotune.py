@@ -44,3 +44,26 @@ def test_autotune_keeps_state_and_results(precision, case):
     assert again.tiling("fluid") == tuned.tiling("fluid") and again.tiling("magnet") == tuned.tiling("magnet")
     for r in (tuned, plain, again):
         r.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_chain_with_both_components_per_cta_matches(precision):
+    """The magnet chain tiling that carries both transverse components in one CTA (a choice the
+    autotuner may make) gives bitwise the same results as one component per CTA."""
+    for case in ("ot", "kh"):
+        s, st = problems.orszag_tang(64) if case == "ot" else problems.kelvin_helmholtz(20)
+        s = dict(s, time_max=1e5, iter_max=10 ** 6)
+        a, b = _run(s, st, precision), _run(s, st, precision)
+        for dim, t in a.tiling("magnet").items():
+            if s["grid"][dim - 1] < 3 or t[4] > 2:
+                continue
+            a.set_tiling(dim, tuple(t[:5]) + (2,), kind="magnet")
+            assert a.tiling("magnet")[dim][5] == 2
+        for _ in range(4):
+            a.iterate()
+            b.iterate()
+        x, y = a.state(), b.state()
+        for k in x:
+            assert np.array_equal(x[k], y[k]), (case, k)
+        a.close()
+        b.close()
