@@ -23,7 +23,8 @@ SYMBOLS = (
     "img_config_default", "img_create", "img_destroy", "img_set_state", "img_upload", "img_download",
     "img_upload_many", "img_download_many",
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
-    "img_get_time", "img_set_time", "img_progress", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
+    "img_get_time", "img_set_time", "img_progress", "img_checkpoint_bytes", "img_checkpoint_save",
+    "img_checkpoint_load", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
@@ -89,6 +90,12 @@ def lib():
     L.img_set_time.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
     L.img_totals.argtypes = [vp, dp]
     L.img_progress.argtypes = [vp, dp, ip, ip]
+    L.img_checkpoint_bytes.argtypes = [vp]
+    L.img_checkpoint_bytes.restype = ctypes.c_size_t
+    L.img_checkpoint_save.argtypes = [vp, vp, ctypes.c_size_t]
+    L.img_checkpoint_save.restype = ctypes.c_int
+    L.img_checkpoint_load.argtypes = [vp, vp, ctypes.c_size_t]
+    L.img_checkpoint_load.restype = ctypes.c_int
     L.img_progress.restype = ctypes.c_int
     L.img_totals_static.argtypes = [vp, dp]
     L.img_sync.argtypes = [vp]

@@ -1129,6 +1129,83 @@ int img_progress(img_ctx* ctx, double* time, int* iterations_run, int* stopped) 
     return rc;
 }
 
+// ---- checkpoint / resume ------------------------------------------------------------------------
+// A checkpoint is the context's whole device slab (state, stored edges, device clock, scratch) plus
+// the host-side bookkeeping that decides the next launches (first-assignment flags, CFL validity,
+// iteration), behind a header that carries the configuration; it resumes bit for bit in a
+// context created with the same configuration.
+namespace {
+struct CheckpointHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t header_bytes;
+    uint64_t slab_bytes;
+    img_config cfg;
+    int state_set, init_store, init_flux, cfl_valid, iteration, mhd;
+    int init_mag[3][3];
+    int use_b[3];
+};
+const char kCheckpointMagic[8] = {'I', 'M', 'G', 'B', '2', '0', '0', 'C'};
+}  // namespace
+
+size_t img_checkpoint_bytes(const img_ctx* ctx) { return ctx ? sizeof(CheckpointHeader) + ctx->slab_bytes : 0; }
+
+int img_checkpoint_save(img_ctx* ctx, void* host, size_t bytes) {
+    if (!ctx || !host) return fail(ctx, IMG_ERR_ARG, "null argument");
+    if (bytes < img_checkpoint_bytes(ctx)) return fail(ctx, IMG_ERR_ARG, "checkpoint buffer too small");
+    CheckpointHeader h{};
+    std::memcpy(h.magic, kCheckpointMagic, 8);
+    h.version = 1;
+    h.header_bytes = sizeof h;
+    h.slab_bytes = ctx->slab_bytes;
+    h.cfg = ctx->cfg;
+    h.state_set = ctx->state_set;
+    h.init_store = ctx->init_store;
+    h.init_flux = ctx->init_flux;
+    h.cfl_valid = ctx->cfl_valid;
+    h.iteration = ctx->iteration;
+    h.mhd = ctx->mhd;
+    for (int i = 0; i < 3; ++i) {
+        h.use_b[i] = ctx->use_b[i];
+        for (int j = 0; j < 3; ++j) h.init_mag[i][j] = ctx->init_mag[i][j];
+    }
+    std::memcpy(host, &h, sizeof h);
+    CK(cudaMemcpyAsync(static_cast<char*>(host) + sizeof h, ctx->slab, ctx->slab_bytes, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return IMG_OK;
+}
+
+int img_checkpoint_load(img_ctx* ctx, const void* host, size_t bytes) {
+    if (!ctx || !host) return fail(ctx, IMG_ERR_ARG, "null argument");
+    if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot load a checkpoint into a batch member");
+    CheckpointHeader h;
+    if (bytes < sizeof h) return fail(ctx, IMG_ERR_ARG, "checkpoint too short");
+    std::memcpy(&h, host, sizeof h);
+    if (std::memcmp(h.magic, kCheckpointMagic, 8) || h.version != 1 || h.header_bytes != sizeof h)
+        return fail(ctx, IMG_ERR_ARG, "not an imogen_b200 checkpoint of this version");
+    if (h.slab_bytes != ctx->slab_bytes || bytes < sizeof h + h.slab_bytes ||
+        std::memcmp(&h.cfg, &ctx->cfg, sizeof(img_config)) != 0)
+        return fail(ctx, IMG_ERR_ARG, "checkpoint was written by a context with another configuration");
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaMemcpyAsync(ctx->slab, static_cast<const char*>(host) + sizeof h, ctx->slab_bytes, cudaMemcpyHostToDevice,
+                       ctx->stream));
+    // the stored-edge table holds device addresses: this context's own, not the writer's
+    CK(cudaMemcpyAsync(ctx->edges_dev, &ctx->edges_host, sizeof(EdgeTable), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->state_set = h.state_set != 0;
+    ctx->init_store = h.init_store != 0;
+    ctx->init_flux = h.init_flux != 0;
+    ctx->cfl_valid = h.cfl_valid != 0;
+    ctx->iteration = h.iteration;
+    ctx->mhd = h.mhd;
+    for (int i = 0; i < 3; ++i) {
+        ctx->use_b[i] = h.use_b[i];
+        for (int j = 0; j < 3; ++j) ctx->init_mag[i][j] = h.init_mag[i][j] != 0;
+    }
+    return check_dev_error(ctx);
+}
+
 int img_totals(img_ctx* ctx, double out[8]) {
     if (!ctx || !out) return fail(ctx, IMG_ERR_ARG, "null argument");
     const int nb = 1024;

@@ -291,6 +291,18 @@ class ImogenRun:
         t = (ctypes.c_int * 6)(*vals)
         check(lib().img_set_tiling(self._h, int(dim) + (0 if kind == "fluid" else 3), t), self._h)
 
+    def checkpoint(self):
+        """The run's complete resumable state as bytes (img_checkpoint_save)."""
+        n = int(lib().img_checkpoint_bytes(self._h))
+        buf = ctypes.create_string_buffer(n)
+        check(lib().img_checkpoint_save(self._h, ctypes.cast(buf, ctypes.c_void_p), n), self._h)
+        return buf.raw
+
+    def restore(self, data):
+        """Resume from checkpoint() bytes of a run with the same settings (img_checkpoint_load)."""
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        check(lib().img_checkpoint_load(self._h, ctypes.cast(buf, ctypes.c_void_p), len(data)), self._h)
+
     def progress(self):
         """(simulated time, iterations run, stopped) from the device clock (synchronises)."""
         t, n, st = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()

@@ -72,6 +72,7 @@ class Server:
         self.batches: Dict[tuple, ImogenBatch] = {}
         self.running: Dict[int, tuple] = {}     # job id -> (job, run, bytes)
         self.t0 = None
+        self._n = 0
 
     def now(self) -> float:
         return self.clock() - self.t0
@@ -102,6 +103,7 @@ class Server:
             if b is None:
                 b = self.batches[key] = ImogenBatch()
             b.add(run)                                   # waits for the run's own stream
+            run.batch_ref = b
             self.running[job.id] = (job, run, need)
             self.used += need
 
@@ -124,28 +126,79 @@ class Server:
             self.used -= need
             self.done.append(job)
 
-    def serve(self, jobs: List[Job], idle_sleep: float = 2e-4) -> List[Job]:
-        """Run until every job has completed; returns them in completion order."""
-        for j in jobs:
-            self.submit(j)
+    def start(self):
+        """Start the clock (arrival times are measured from here)."""
         self.t0 = self.clock()
-        n = 0
-        while self.queue or self.running:
-            self._admit()
-            active = [b for b in self.batches.values() if b.members]
-            if not active:
-                if self.queue:
-                    time.sleep(min(idle_sleep, max(0.0, self.queue[0].arrival - self.now())))
-                continue
+        self._n = 0
+
+    def tick(self, idle_sleep: float = 2e-4) -> bool:
+        """One scheduling round: admit what fits, advance every running batch one iteration, and
+        every check_every rounds retire the finished jobs.  Returns False once nothing is queued or
+        running.  Jobs may be submitted, polled and cancelled between rounds."""
+        if self.t0 is None:
+            self.start()
+        if not (self.queue or self.running):
+            return False
+        self._admit()
+        active = [b for b in self.batches.values() if b.members]
+        if not active:
+            if self.queue:
+                time.sleep(min(idle_sleep, max(0.0, self.queue[0].arrival - self.now())))
+            return True
+        for b in active:
+            b.step()
+        self._n += 1
+        if self._n % self.check_every == 0:
             for b in active:
-                b.step()
-            n += 1
-            if n % self.check_every == 0:
-                for b in active:
-                    self._retire(b)
+                self._retire(b)
+        return True
+
+    def poll(self, job_id: int) -> dict:
+        """State of a job: queued, running (with simulated time and iterations), done or cancelled."""
+        for j in self.queue:
+            if j.id == job_id:
+                return {"state": "queued"}
+        if job_id in self.running:
+            job, run, _ = self.running[job_id]
+            t, n, _ = run.progress()
+            return {"state": "running", "time": t, "iterations": n}
+        for j in self.done:
+            if j.id == job_id:
+                return {"state": "cancelled" if j.result and j.result.get("cancelled") else "done",
+                        "latency_s": j.latency}
+        raise KeyError(job_id)
+
+    def cancel(self, job_id: int) -> bool:
+        """Drop a queued job, or stop a running one and free its memory.  False if it already ended."""
+        for i, j in enumerate(self.queue):
+            if j.id == job_id:
+                self.queue.pop(i)
+                j.result = {"cancelled": True}
+                self.done.append(j)
+                return True
+        if job_id in self.running:
+            job, run, need = self.running.pop(job_id)
+            run.batch_ref.remove(run)
+            run.close()
+            self.used -= need
+            job.result = {"cancelled": True}
+            self.done.append(job)
+            return True
+        return False
+
+    def close(self):
         for b in self.batches.values():
             b.close()
         self.batches = {}
+
+    def serve(self, jobs: List[Job]) -> List[Job]:
+        """Run until every job has completed; returns them in completion order."""
+        for j in jobs:
+            self.submit(j)
+        self.start()
+        while self.tick():
+            pass
+        self.close()
         return self.done
 
 

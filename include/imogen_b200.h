@@ -119,6 +119,14 @@ int img_set_time(img_ctx* ctx, double time, double dt, int iteration);
  * (the reference reads run.time and run.time.iteration). */
 int img_progress(img_ctx* ctx, double* time, int* iterations_run, int* stopped);
 
+/* Checkpoint / resume: the context's complete device state (arrays, stored edges, device clock)
+ * and the host bookkeeping of its next launches, copied to a host buffer of img_checkpoint_bytes;
+ * loading it into a context created with the same configuration resumes bit for bit.  The
+ * reference's save/resume writes .mat slices (resultsHandler.m), which this does not replace. */
+size_t img_checkpoint_bytes(const img_ctx* ctx);
+int img_checkpoint_save(img_ctx* ctx, void* host, size_t bytes);
+int img_checkpoint_load(img_ctx* ctx, const void* host, size_t bytes);
+
 /* Compensated (Neumaier) FP64 totals of rho, px, py, pz, E, Bx, By, Bz over the grid. */
 int img_totals(img_ctx* ctx, double out[8]);
 

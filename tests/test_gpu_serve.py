@@ -61,3 +61,50 @@ def test_mixed_form_within_tolerance_of_fp64():
     for i, j in mixed.items():
         for k in ("mass", "ener"):
             assert _rel_l1(j.result[k], fp64[i].result[k]) < 1e-5, (i, k)
+
+
+def test_poll_and_cancel():
+    jobs = serve.sedov_stream(6, rate=400.0, seed=13, sizes2=(48, 64), sizes3=(24, 32), precision="mixed",
+                              time_max=0.05)
+    srv = serve.Server(hbm_budget=1 << 34, check_every=1, keep="totals")
+    for j in jobs:
+        srv.submit(j)
+    srv.start()
+    while not srv.running and srv.tick():                # until a job is on the device
+        pass
+    running = list(srv.running)
+    assert running, "nothing running to cancel"
+    victim = running[0]
+    assert srv.poll(victim)["state"] == "running"
+    assert srv.cancel(victim) and not srv.cancel(victim)
+    assert srv.poll(victim)["state"] == "cancelled"
+    while srv.tick():
+        pass
+    srv.close()
+    states = {j.id: srv.poll(j.id)["state"] for j in jobs}
+    assert states[victim] == "cancelled" and sum(s == "done" for s in states.values()) == len(jobs) - 1
+    assert srv.used == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_checkpoint_resumes_bit_for_bit(precision):
+    from imogen_b200 import ImogenRun, problems
+    for s, st in (problems.orszag_tang(48), problems.sedov(40, dims=2, bc="trans")):
+        s = dict(s, time_max=1e5, iter_max=10 ** 6)
+        a = ImogenRun(precision=precision, **s)
+        a.set_state(*st)
+        for _ in range(3):
+            a.iterate()
+        ck = a.checkpoint()
+        for _ in range(4):
+            a.iterate()
+        b = ImogenRun(precision=precision, **s)
+        b.restore(ck)
+        for _ in range(4):
+            b.iterate()
+        x, y = a.state(), b.state()
+        for k in x:
+            assert np.array_equal(x[k], y[k]), k
+        assert a.time.time == b.time.time and a.time.iteration == b.time.iteration
+        a.close()
+        b.close()
