@@ -48,7 +48,8 @@ int pow2ceil(long long v) {
 
 // One kernel launch of a context, recorded instead of issued while the context steps as a member of
 // a batch (img_batch_*): the batch replays the records of all members as batched launches.
-enum OpKind { OP_FLUID, OP_CHAIN, OP_CT, OP_CELL, OP_CFL_REDUCE, OP_CFL_FINALIZE };
+enum OpKind { OP_FLUID, OP_CHAIN, OP_CTCELL, OP_CFL_REDUCE, OP_CFL_FINALIZE };
+inline bool pencil_kind(int kind) { return kind == OP_FLUID || kind == OP_CHAIN || kind == OP_CTCELL; }
 struct OpRec {
     int kind;
     int elem;                 // 4 (mixed) or 8 (FP64)
@@ -74,7 +75,7 @@ struct img_ctx {
     void* slab = nullptr;       // one allocation: state, scratch, edges, tables
     size_t slab_bytes = 0;
     void* q[NQ] = {};
-    void* scratch[3] = {};      // F0, F1, BXn
+    void* scratch[2] = {};      // F0, F1 (limited fluxes of the magnet chain)
     DevTime* tm = nullptr;
     EdgeTable* edges_dev = nullptr;
     EdgeTable edges_host{};
@@ -332,12 +333,6 @@ TuneKey tune_key(int kind, const Geom& g, int d, size_t elem, const img_config& 
                    c.magnet_active);
 }
 
-// Blocks of a pointwise pass (for_cells): units of one 256-cell chunk of an x-row.
-int pointwise_blocks(const Geom& g) {
-    const long long units = (long long)g.n[1] * g.n[2] * ((g.n[0] + 255) / 256);
-    return (int)std::max(1LL, std::min(units, 148LL * 16));
-}
-
 int launch_blocks(long long work, int bs = 256) {
     long long b = (work + bs - 1) / bs;
     return (int)std::max(1LL, std::min(b, 148LL * 16));
@@ -449,7 +444,6 @@ void fill_mag_args(img_ctx* ctx, int X, int I1, int I2, MagArgs& a) {
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.F[0] = ctx->scratch[0];
     a.F[1] = ctx->scratch[1];
-    a.BXn = ctx->scratch[2];
     a.tm = ctx->tm;
     a.X = X;
     a.I[0] = I1;
@@ -489,6 +483,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     const PencilCfg& pcf = ctx->pcfg[1][d];
     const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
                                             2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    const PencilLaunch Lc = pencil_launch<T>(ctx, pcf, d, ctcell_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+                                             fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
     if (ctx->rec) {
         OpRec r{};
         r.elem = sizeof(T);
@@ -496,10 +492,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
         r.kind = OP_CHAIN;
         r.L = L;
         ctx->rec->push_back(r);
-        r.kind = OP_CT;
-        r.blocks = pointwise_blocks(ctx->g);
-        ctx->rec->push_back(r);
-        r.kind = OP_CELL;
+        r.kind = OP_CTCELL;
+        r.L = Lc;
         ctx->rec->push_back(r);
         ctx->init_mag[I1 - 1][d] = false;
         ctx->init_mag[I2 - 1][d] = false;
@@ -509,9 +503,11 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
                     L.grid_x, L.block, L.smem, L.cluster, cudaGetErrorString(le));
-    CK(launch_mag_ct<T>(a, pointwise_blocks(ctx->g), ctx->stream));
-    CK(launch_mag_cell<T>(a, pointwise_blocks(ctx->g), ctx->stream));
-    ctx->launches += 3;
+    le = launch_mag_ctcell<T>(a, Lc);
+    if (le != cudaSuccess)
+        return fail(ctx, IMG_ERR_CUDA, "magnet CT launch (dim %d, grid %u, block %u, smem %zu, cluster %d): %s", d,
+                    Lc.grid_x, Lc.block, Lc.smem, Lc.cluster, cudaGetErrorString(le));
+    ctx->launches += 2;
     ctx->init_mag[I1 - 1][d] = false;
     ctx->init_mag[I2 - 1][d] = false;
     return IMG_OK;
@@ -693,7 +689,7 @@ Layout plan(const img_config& c) {
     long long n = (long long)c.grid[0] * c.grid[1] * c.grid[2];
     size_t arr = align256(n * elem);
     L.state = arr * NQ;
-    L.scratch = c.magnet_active ? arr * 3 : 0;
+    L.scratch = c.magnet_active ? arr * 2 : 0;
     L.tm = align256(sizeof(DevTime));
     L.table = align256(sizeof(EdgeTable));
     L.fade = align256(sizeof(double) * std::max(1, c.bc_infinity));
@@ -821,7 +817,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     for (int v = 0; v < NQ; ++v) ctx->q[v] = p + v * arr;
     p += L.state;
     if (cfg->magnet_active)
-        for (int k = 0; k < 3; ++k) ctx->scratch[k] = p + k * arr;
+        for (int k = 0; k < 2; ++k) ctx->scratch[k] = p + k * arr;
     p += L.scratch;
     ctx->tm = reinterpret_cast<DevTime*>(p);
     p += L.tm;
@@ -1362,7 +1358,7 @@ int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchP
                 const OpRec& a = recs[heads[h]][k];
                 const OpRec& c = recs[m][k];
                 bool same = a.elem == c.elem && a.mhd == c.mhd;
-                if (kind == OP_FLUID || kind == OP_CHAIN) same = same && same_shape(a.L, c.L);
+                if (pencil_kind(kind)) same = same && same_shape(a.L, c.L);
                 if (kind == OP_CFL_FINALIZE) same = same && a.check_running == c.check_running;
                 if (same) gi = h;
             }
@@ -1392,7 +1388,7 @@ int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchP
             } else {
                 for (int j = 0; j < (int)mem.size(); ++j) {
                     const OpRec& r = recs[mem[j]][k];
-                    const int nb = (kind == OP_FLUID || kind == OP_CHAIN) ? (int)r.L.grid_x : (int)r.blocks;
+                    const int nb = pencil_kind(kind) ? (int)r.L.grid_x : (int)r.blocks;
                     for (int blk = 0; blk < nb; ++blk) map.push_back(BlockMap{j, blk, nb});
                 }
                 if (kind == OP_FLUID) {
@@ -1409,7 +1405,7 @@ int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchP
                     it.args_off = put(plan.host, v.data(), v.size());
                 }
                 it.map_off = put(plan.host, map.data(), map.size());
-                if (kind == OP_FLUID || kind == OP_CHAIN) it.L.grid_x = (unsigned)map.size();
+                if (pencil_kind(kind)) it.L.grid_x = (unsigned)map.size();
                 else it.blocks = (unsigned)map.size();
             }
             it.L.stream = b->stream;
@@ -1436,12 +1432,9 @@ cudaError_t launch_item(const BatchItem& it, const unsigned char* base, cudaStre
         case OP_CHAIN:
             return launch_mag_chain_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
                                              reinterpret_cast<const BlockMap*>(base + it.map_off), it.L);
-        case OP_CT:
-            return launch_mag_ct_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
-                                          reinterpret_cast<const BlockMap*>(base + it.map_off), it.blocks, st);
-        case OP_CELL:
-            return launch_mag_cell_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
-                                            reinterpret_cast<const BlockMap*>(base + it.map_off), it.blocks, st);
+        case OP_CTCELL:
+            return launch_mag_ctcell_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
+                                              reinterpret_cast<const BlockMap*>(base + it.map_off), it.L);
         case OP_CFL_REDUCE:
             cfl_reduce_batch_kernel<T><<<it.blocks, 256, 0, st>>>(reinterpret_cast<const CflArgs*>(base + it.args_off),
                                                                  reinterpret_cast<const BlockMap*>(base + it.map_off));
@@ -1459,7 +1452,7 @@ int launch_plan(img_batch* b, const BatchPlan& plan) {
         cudaError_t e = it.elem == 8 ? launch_item<double>(it, base, b->stream) : launch_item<float>(it, base, b->stream);
         if (e != cudaSuccess)
             return bfail(b, IMG_ERR_CUDA, "batched launch (kind %d, %d members, grid %u): %s", it.kind, it.nmembers,
-                         it.kind == OP_FLUID || it.kind == OP_CHAIN ? it.L.grid_x : it.blocks, cudaGetErrorString(e));
+                         pencil_kind(it.kind) ? it.L.grid_x : it.blocks, cudaGetErrorString(e));
     }
     return IMG_OK;
 }

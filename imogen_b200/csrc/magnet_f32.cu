@@ -4,9 +4,7 @@
 namespace img {
 template cudaError_t launch_mag_chain<float>(const MagArgs&, const PencilLaunch&);
 template cudaError_t launch_mag_chain_batch<float>(const MagArgs*, const BlockMap*, const PencilLaunch&);
-template cudaError_t launch_mag_ct_batch<float>(const MagArgs*, const BlockMap*, unsigned, cudaStream_t);
-template cudaError_t launch_mag_cell_batch<float>(const MagArgs*, const BlockMap*, unsigned, cudaStream_t);
-template cudaError_t launch_mag_ct<float>(const MagArgs&, unsigned, cudaStream_t);
-template cudaError_t launch_mag_cell<float>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t launch_mag_ctcell_batch<float>(const MagArgs*, const BlockMap*, const PencilLaunch&);
+template cudaError_t launch_mag_ctcell<float>(const MagArgs&, const PencilLaunch&);
 template cudaError_t chain_attributes<float>(int, int);
 }  // namespace img

@@ -4,9 +4,7 @@
 namespace img {
 template cudaError_t launch_mag_chain<double>(const MagArgs&, const PencilLaunch&);
 template cudaError_t launch_mag_chain_batch<double>(const MagArgs*, const BlockMap*, const PencilLaunch&);
-template cudaError_t launch_mag_ct_batch<double>(const MagArgs*, const BlockMap*, unsigned, cudaStream_t);
-template cudaError_t launch_mag_cell_batch<double>(const MagArgs*, const BlockMap*, unsigned, cudaStream_t);
-template cudaError_t launch_mag_ct<double>(const MagArgs&, unsigned, cudaStream_t);
-template cudaError_t launch_mag_cell<double>(const MagArgs&, unsigned, cudaStream_t);
+template cudaError_t launch_mag_ctcell_batch<double>(const MagArgs*, const BlockMap*, const PencilLaunch&);
+template cudaError_t launch_mag_ctcell<double>(const MagArgs&, const PencilLaunch&);
 template cudaError_t chain_attributes<double>(int, int);
 }  // namespace img

@@ -1,16 +1,14 @@
 // Magnet sweep along X for the two transverse components (magnet/magnetFlux.m:14-31,
 // magnet/relaxingMagnet.m:15-60, magnet/MagnetArray.m:36-38).
 //
-// Three launches per sweep:
-//   mag_chain  -- per X-pencil and component I: corner velocity (transverse average, then the
-//                 1-2-1 smoothing along X), upwind predictor, TVD corrector, B_I update.  Writes
-//                 B_I in place and the limited flux F_I to scratch.  Both components in one launch.
-//   mag_ct     -- D_I = (F_I - F_I.shift(I,+1)).shift(X,-1) for both components, evaluated from F
-//                 (relaxingMagnet.m:56-57), B_X' = (B_X - dt/dI1 D_I1) - dt/dI2 D_I2 to scratch,
-//                 cell-centred B_I2
-//   mag_cell   -- B_X = B_X'; cell-centred B_X (MagnetArray.m:36-38); the drift of the flux
-//                 objects' stored edges along I, which mag_ct only reads
-// Each pass reads only arrays that no thread of the same pass writes.
+// Two launches per sweep, both on the same X-pencil tiling:
+//   mag_chain   -- per X-pencil and component I: corner velocity (transverse average, then the
+//                  1-2-1 smoothing along X), upwind predictor, TVD corrector, B_I update.  Writes
+//                  B_I in place and the limited flux F_I to scratch.  Both components in one launch.
+//   mag_ctcell  -- C_I = F_I - F_I.shift(I,+1) at own cells, D_I = C_I.shift(X,-1) through shared
+//                  memory, B_X = (B_X - dt/dI1 D_I1) - dt/dI2 D_I2 in place, cell-centred B_I2 and
+//                  B_X (relaxingMagnet.m:54-58, MagnetArray.m:36-38).
+// The second launch needs the first's F_I at the neighbouring pencils along I, hence two launches.
 #pragma once
 
 #include "fluid_sweep.cuh"
@@ -21,7 +19,6 @@ struct MagArgs {
     SweepGeom sg;              // sweep along d = X-1
     void* q[NQ];
     void* F[2];                // limited flux per component (scratch)
-    void* BXn;                 // new B_X (scratch)
     DevTime* tm;
     int X;                     // 1-based sweep dimension
     int I[2];                  // 1-based transverse components, in the reference's order
@@ -403,21 +400,121 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
 }
 
-// ---- pointwise passes ---------------------------------------------------------------------------------
-// Pointwise passes walk the grid in units of one chunk of blockDim.x cells of an x-row: the
-// coordinates cost one 32-bit division pair per unit instead of per cell (ncell < 2^31).
-template <typename F>
-__device__ __forceinline__ void for_cells(const Geom& g, unsigned vblock, unsigned vgrid, F&& f) {
-    const unsigned nx = (unsigned)g.n[0], ny = (unsigned)g.n[1];
-    const unsigned chunks = (nx + blockDim.x - 1) / blockDim.x;
-    const unsigned units = ny * (unsigned)g.n[2] * chunks;
-    for (unsigned u = vblock; u < units; u += vgrid) {
-        const unsigned r = u / chunks;
-        const unsigned x = (u - r * chunks) * blockDim.x + threadIdx.x;
-        if (x >= nx) continue;
-        const unsigned z = r / ny;
-        f((long long)r * nx + x, (int)x, (int)(r - z * ny), (int)z);
+// ---- CT and cell-centring, fused along X-pencils --------------------------------------------------------
+// Per X-pencil, on the chain's tiling:
+//   C_q  = F_q - F_q.shift(I_q, +1) at the thread's own cells        (relaxingMagnet.m:56)
+//   D_q  = C_q.shift(X, -1), through shared memory                   (relaxingMagnet.m:57)
+//   B_X  = (B_X - dt/dI_1 * D_1) - dt/dI_2 * D_2                      (relaxingMagnet.m:58, both calls)
+//   cell-centred B_I2 along I2 and B_X along X, the latter from the new B_X in shared memory
+//                                                                    (magnetFlux.m:30-31, MagnetArray.m:36-38)
+// Every thread reads B_X only at its own cells, so B_X is updated in place.  Each flux object's
+// shift(I, +1) call drifts its trans edge in the thread of the upper I face cell, which is also the
+// only thread that reads that edge.
+template <typename T>
+__host__ __device__ inline size_t ctcell_smem_bytes(int RC, int Wb) {
+    return 3 * (sizeof(T) * (size_t)tile_rows(RC) * Wb + sizeof(Ghost<T>) * (size_t)Wb);
+}
+
+template <typename T, int CPT, bool FADE>
+__device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vblock) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (a.tm->done || a.tm->error) return;
+    Tile<T, CPT> tl;
+    tl.init(a.sg, vblock);
+    const int d = a.X - 1;
+    const Geom& g = a.sg.g;
+    const int Wb = tl.Wb;
+    const double dt = a.tm->dt;
+    const EdgeTable* et = a.edges;
+    const double* fc = a.fade;
+    const int f = a.fade_f;
+    const double binf = a.bc_inf;
+    const int mlo = a.modeX[0], mhi = a.modeX[1];
+    const size_t AS = (size_t)tile_rows(tl.RC) * Wb;
+    // shared: C_1, C_2, new B_X; then their ghost/anchor slots (C lower sides, B_X upper side)
+    T* const S = reinterpret_cast<T*>(smem);
+    Ghost<T>* const GS = reinterpret_cast<Ghost<T>*>(S + 3 * AS);
+
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int e = (q ? a.I[1] : a.I[0]) - 1;
+        const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
+        const bool shI = q ? a.shiftI[1] : a.shiftI[0];
+        const int modeI = q ? a.modeI_mag[1][1] : a.modeI_mag[0][1];
+        const int actI = q ? a.actI_mag[1] : a.actI_mag[0];
+        const int ie = e == a.sg.d1 ? tl.c1 : tl.c2;   // the pencil's coordinate along I (I != X)
+        const bool directI = shI && ie < sel3(e, g.n[0], g.n[1], g.n[2]) - 1 && modeI != BC_FADE;
+        const long long sI = sel3(e, g.s[0], g.s[1], g.s[2]);
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            T c = T(0);
+            if (tl.ok(k)) {
+                const long long o = tl.off(k);
+                const T fv = F[o];
+                if (!shI) c = fv - fv;
+                else if (directI) c = fv - F[o + sI];
+                else {
+                    int x, y, z;
+                    tl.coords(k, x, y, z);
+                    c = fv - shift_along<T>(g, F, o, x, y, z, e, +1, modeI, actI, true,
+                                            et->p[mag_obj(e, d, MO_FLUX)][e][1], fc, f, binf, true);
+                }
+            }
+            S[q * AS + tl.idx(k)] = c;
+        }
     }
+    tl.csync();
+    // lower ghosts of C_q along X: the flux object's mag-class BC, no mirror flip (I != X)
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+        if (tl.colok && tl.g == q % tl.G)
+            halo_job(tl, S + q * AS, GS + q * Wb, 0, true, mlo, a.actX, 0,
+                     et->p[mag_obj((q ? a.I[1] : a.I[0]) - 1, d, MO_FLUX)][d][0], binf, 1);
+    __syncthreads();
+    T* BX = reinterpret_cast<T*>(a.q[Q_BX + d]);
+    const T f0 = (T)(dt / a.dI[0]), f1 = (T)(dt / a.dI[1]);
+    T bx[CPT];
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const T D0 = shifted<FADE>(tl, (const T*)S, GS, k, -1, mlo, fc, f);
+        const T D1 = shifted<FADE>(tl, (const T*)(S + AS), GS + Wb, k, -1, mlo, fc, f);
+        bx[k] = T(0);
+        if (tl.ok(k)) bx[k] = (BX[tl.off(k)] - f0 * D0) - f1 * D1;
+        S[2 * AS + tl.idx(k)] = bx[k];
+    }
+    tl.csync();
+    // upper ghost of the new B_X along X: mag(X).shift(X, +1) of the primary array (mirror flips B_X)
+    if (tl.colok && tl.g == 2 % tl.G)
+        halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, 1, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
+    __syncthreads();
+    T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
+    const int e2 = a.I[1] - 1;
+    const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
+    T* CB2 = reinterpret_cast<T*>(a.q[Q_CBX + e2]);
+    const int i2 = e2 == a.sg.d1 ? tl.c1 : tl.c2;
+    const int N2 = sel3(e2, g.n[0], g.n[1], g.n[2]);
+    const int mode2 = a.modeI_mag[1][1];
+    const bool direct2 = a.shiftI[1] && i2 < N2 - 1 && mode2 != BC_FADE;
+    const long long s2 = sel3(e2, g.s[0], g.s[1], g.s[2]);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const T up = shifted<FADE>(tl, (const T*)(S + 2 * AS), GS + 2 * Wb, k, +1, mhi, fc, f);
+        if (!tl.ok(k)) continue;
+        const long long o = tl.off(k);
+        BX[o] = bx[k];
+        CBX[o] = T(0.5) * (bx[k] + up);
+        const T b2 = BI2[o];
+        T sh;
+        if (direct2) sh = BI2[o + s2];
+        else if (a.shiftI[1]) {
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            sh = shift_along<T>(g, BI2, o, x, y, z, e2, +1, mode2, a.actI_mag[1], true,
+                                et->p[OBJ_PRIM_MAG + e2][e2][1], fc, f, binf, i2 == N2 - 1);
+        } else sh = b2;
+        CB2[o] = T(0.5) * (b2 + sh);
+    }
+    if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
 }
 
 __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, int& y, int& z) {
@@ -428,119 +525,14 @@ __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, 
     y = (int)(r - (unsigned)z * n1);
 }
 
-// D_q = (F_q - F_q.shift(I_q, +1)).shift(X, -1) at one cell, from the limited flux F_q (the flux(X)
-// object of mag(I_q): mag-class BC along I_q with the mirror flip of component I_q, along X the
-// mag-class BC without it).  The I-shift's trans edge is only read here (mag_cell stores its drift);
-// the X-shift's lower edge is drifted and stored by the thread of the face cell (x == 0).
-template <typename T>
-__device__ __forceinline__ T ct_difference(const MagArgs& a, int q, long long cell, int x, int y, int z) {
-    const Geom& g = a.sg.g;
-    const int d = a.X - 1;
-    const int I = q ? a.I[1] : a.I[0], e = I - 1;
-    const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
-    const bool shI = q ? a.shiftI[1] : a.shiftI[0];
-    const int modeI = q ? a.modeI_mag[1][1] : a.modeI_mag[0][1];
-    const int actI = q ? a.actI_mag[1] : a.actI_mag[0];
-    double* edgeI = a.edges->p[mag_obj(e, d, MO_FLUX)][e][1];
-    const int Nd = sel3(d, g.n[0], g.n[1], g.n[2]);
-    const long long sdx = sel3(d, g.s[0], g.s[1], g.s[2]);
-    const int xd = sel3(d, x, y, z);
-    const long long row0 = cell - (long long)xd * sdx;   // X-index 0 of this cell's X-line
-    // the I coordinate is the same at every X-index of this line: away from the upper I face (and
-    // without fade) the I-shift is the next cell along I
-    const bool directI = shI && sel3(e, x, y, z) < sel3(e, g.n[0], g.n[1], g.n[2]) - 1 && modeI != BC_FADE;
-    const long long sI = sel3(e, g.s[0], g.s[1], g.s[2]);
-    // C_q at X-index j of this line
-    auto C = [&](int j) -> T {
-        const long long c2 = row0 + (long long)j * sdx;
-        const T fv = F[c2];
-        if (!shI) return fv - fv;
-        if (directI) return fv - F[c2 + sI];
-        const int x2 = d == 0 ? j : x, y2 = d == 1 ? j : y, z2 = d == 2 ? j : z;
-        return fv - shift_along<T>(g, F, c2, x2, y2, z2, e, +1, modeI, actI, true, edgeI, a.fade, a.fade_f, a.bc_inf,
-                                   false);
-    };
-    if (xd >= 1 && a.modeX[0] != BC_FADE) return C(xd - 1);   // interior along X
-    return shift_line<T>(C, xd, Nd, face_index(g, d, x, y, z), -1, a.modeX[0], a.actX, e == d,
-                         a.edges->p[mag_obj(e, d, MO_FLUX)][d][0], a.fade, a.fade_f, a.bc_inf, xd == 0);
-}
-
-// B_X' = (B_X - dt/dI1 * D_I1) - dt/dI2 * D_I2 -> scratch; cell-centred B of I2 (the last component).
-// Run by block vblock of vgrid blocks of one grid's launch.
-template <typename T>
-__device__ __forceinline__ void mag_ct_body(const MagArgs& a, unsigned vblock, unsigned vgrid) {
-    if (a.tm->done || a.tm->error) return;
-    const Geom& g = a.sg.g;
-    const double dt = a.tm->dt;
-    const T f0 = (T)(dt / a.dI[0]), f1 = (T)(dt / a.dI[1]);
-    const int X = a.X;
-    const T* BX = reinterpret_cast<const T*>(a.q[Q_BX + X - 1]);
-    T* BXn = reinterpret_cast<T*>(a.BXn);
-    const int I2 = a.I[1], e2 = I2 - 1;
-    const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
-    T* CB2 = reinterpret_cast<T*>(a.q[Q_CBX + e2]);
-    for_cells(g, vblock, vgrid, [&](long long cell, int x, int y, int z) {
-        const T D0 = ct_difference<T>(a, 0, cell, x, y, z);
-        const T D1 = ct_difference<T>(a, 1, cell, x, y, z);
-        BXn[cell] = (BX[cell] - f0 * D0) - f1 * D1;
-        T sh;
-        if (e2 < g.ndims) {
-            bool own = sel3(e2, x, y, z) == sel3(e2, g.n[0], g.n[1], g.n[2]) - 1;
-            sh = shift_along<T>(g, BI2, cell, x, y, z, e2, +1, a.modeI_mag[1][1], a.actI_mag[1], true,
-                                a.edges->p[OBJ_PRIM_MAG + e2][e2][1], a.fade, a.fade_f, a.bc_inf, own);
-        } else {
-            sh = BI2[cell];
-        }
-        CB2[cell] = T(0.5) * (BI2[cell] + sh);
-    });
-}
-
-// B_X = B_X'; cell-centred B_X = 0.5*(B_X + B_X.shift(X, +1)); and the drift of the I-direction
-// trans edges of both flux objects (the C_I = F_I - F_I.shift(I,+1) calls of mag_ct), stored by
-// the thread of each upper face cell.  Run by block vblock of vgrid blocks of one grid's launch.
-template <typename T>
-__device__ __forceinline__ void mag_cell_body(const MagArgs& a, unsigned vblock, unsigned vgrid) {
-    if (a.tm->done || a.tm->error) return;
-    const Geom& g = a.sg.g;
-    const int X = a.X, d = X - 1;
-    const T* BXn = reinterpret_cast<const T*>(a.BXn);
-    T* BX = reinterpret_cast<T*>(a.q[Q_BX + d]);
-    T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
-    for_cells(g, vblock, vgrid, [&](long long cell, int x, int y, int z) {
-        bool own = sel3(d, x, y, z) == sel3(d, g.n[0], g.n[1], g.n[2]) - 1;
-        T sh = shift_along<T>(g, BXn, cell, x, y, z, d, +1, a.modeX[1], a.actX, true, a.edges->p[OBJ_PRIM_MAG + d][d][1],
-                              a.fade, a.fade_f, a.bc_inf, own);
-        BX[cell] = BXn[cell];
-        CBX[cell] = T(0.5) * (BXn[cell] + sh);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const int e = (q ? a.I[1] : a.I[0]) - 1;
-            if (!(q ? a.shiftI[1] : a.shiftI[0]) || (q ? a.modeI_mag[1][1] : a.modeI_mag[0][1]) != BC_TRANS ||
-                !(q ? a.actI_mag[1] : a.actI_mag[0]))
-                continue;
-            if (sel3(e, x, y, z) != sel3(e, g.n[0], g.n[1], g.n[2]) - 1) continue;
-            double* edge = a.edges->p[mag_obj(e, d, MO_FLUX)][e][1];
-            const T* F = reinterpret_cast<const T*>(q ? a.F[1] : a.F[0]);
-            const long long fi = face_index(g, e, x, y, z);
-            edge[fi] = edge_drift(edge[fi], (double)F[cell]);
-        }
-    });
-}
-
 template <typename T, int CPT, bool FADE, int NQC>
 __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
     mag_chain_body<T, CPT, FADE, NQC>(a, blockIdx.x);
 }
 
-// CT and cell passes are latency-bound: at most 64 registers so that 4 CTAs of 256 threads share an SM.
-template <typename T>
-__global__ void __launch_bounds__(256, 4) mag_ct_kernel(const __grid_constant__ MagArgs a) {
-    mag_ct_body<T>(a, blockIdx.x, gridDim.x);
-}
-
-template <typename T>
-__global__ void mag_cell_kernel(const __grid_constant__ MagArgs a) {
-    mag_cell_body<T>(a, blockIdx.x, gridDim.x);
+template <typename T, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, 2) mag_ctcell_kernel(const __grid_constant__ MagArgs a) {
+    mag_ctcell_body<T, CPT, FADE>(a, blockIdx.x);
 }
 
 // The same passes over many grids in one launch (BlockMap per CTA, arguments per member).
@@ -554,23 +546,14 @@ __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_b
     mag_chain_body<T, CPT, FADE, NQC>(sa, (unsigned)bm.block);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256, 4) mag_ct_batch_kernel(const MagArgs* __restrict__ args,
-                                                              const BlockMap* __restrict__ map) {
+template <typename T, int CPT, bool FADE>
+__global__ void __launch_bounds__(512, 2) mag_ctcell_batch_kernel(const MagArgs* __restrict__ args,
+                                                                  const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    mag_ct_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
-}
-
-template <typename T>
-__global__ void mag_cell_batch_kernel(const MagArgs* __restrict__ args, const BlockMap* __restrict__ map) {
-    __shared__ MagArgs sa;
-    const BlockMap bm = map[blockIdx.x];
-    load_member_args(sa, args + bm.member);
-    __syncthreads();
-    mag_cell_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
+    mag_ctcell_body<T, CPT, FADE>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

@@ -20,19 +20,16 @@ struct PencilLaunch {
 
 template <typename T> cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd);
 template <typename T> cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L);
-template <typename T> cudaError_t launch_mag_ct(const MagArgs& a, unsigned blocks, cudaStream_t stream);
-template <typename T> cudaError_t launch_mag_cell(const MagArgs& a, unsigned blocks, cudaStream_t stream);
+template <typename T> cudaError_t launch_mag_ctcell(const MagArgs& a, const PencilLaunch& L);
 // Batched forms: one launch over the CTAs of many grids; `args` and `map` are device arrays (one
 // argument block per member, one BlockMap per CTA of the launch, L.grid_x CTAs).
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd);
 template <typename T> cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L);
 template <typename T>
-cudaError_t launch_mag_ct_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream);
-template <typename T>
-cudaError_t launch_mag_cell_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream);
-// Let every fluid (resp. chain) kernel variant with `cpt` cells per thread, single and batched,
-// use up to `optin` bytes of shared memory per block (the device's opt-in maximum).
+cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L);
+// Let every fluid (resp. chain and CT) kernel variant with `cpt` cells per thread, single and
+// batched, use up to `optin` bytes of shared memory per block (the device's opt-in maximum).
 template <typename T> cudaError_t fluid_attributes(int cpt, int optin);
 template <typename T> cudaError_t chain_attributes(int cpt, int optin);
 // Clusters of the MHD fluid kernel that can be co-resident for launch shape L (0: not schedulable).

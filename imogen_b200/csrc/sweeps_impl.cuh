@@ -101,16 +101,28 @@ cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, con
                                args, map, L);
 }
 
-template <typename T>
-cudaError_t launch_mag_ct_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream) {
-    mag_ct_batch_kernel<T><<<blocks, 256, 0, stream>>>(args, map);
-    return cudaGetLastError();
+template <typename T, bool FADE>
+void (*ctcell_kernel(int cpt))(const MagArgs) {
+    switch (cpt) {
+        case 1: return mag_ctcell_kernel<T, 1, FADE>;
+        case 2: return mag_ctcell_kernel<T, 2, FADE>;
+        default: return mag_ctcell_kernel<T, 4, FADE>;
+    }
+}
+
+template <typename T, bool FADE>
+void (*ctcell_batch_kernel(int cpt))(const MagArgs*, const BlockMap*) {
+    switch (cpt) {
+        case 1: return mag_ctcell_batch_kernel<T, 1, FADE>;
+        case 2: return mag_ctcell_batch_kernel<T, 2, FADE>;
+        default: return mag_ctcell_batch_kernel<T, 4, FADE>;
+    }
 }
 
 template <typename T>
-cudaError_t launch_mag_cell_batch(const MagArgs* args, const BlockMap* map, unsigned blocks, cudaStream_t stream) {
-    mag_cell_batch_kernel<T><<<blocks, 256, 0, stream>>>(args, map);
-    return cudaGetLastError();
+cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
+    return launch_pencil_batch(L.fade ? ctcell_batch_kernel<T, true>(L.cpt) : ctcell_batch_kernel<T, false>(L.cpt),
+                               args, map, L);
 }
 
 template <typename T>
@@ -130,15 +142,8 @@ cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L) {
 }
 
 template <typename T>
-cudaError_t launch_mag_ct(const MagArgs& a, unsigned blocks, cudaStream_t stream) {
-    mag_ct_kernel<T><<<blocks, 256, 0, stream>>>(a);
-    return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_mag_cell(const MagArgs& a, unsigned blocks, cudaStream_t stream) {
-    mag_cell_kernel<T><<<blocks, 256, 0, stream>>>(a);
-    return cudaGetLastError();
+cudaError_t launch_mag_ctcell(const MagArgs& a, const PencilLaunch& L) {
+    return launch_pencil(L.fade ? ctcell_kernel<T, true>(L.cpt) : ctcell_kernel<T, false>(L.cpt), a, L);
 }
 
 // Allow a kernel the device's whole opt-in shared memory per block (minus its static shared
@@ -171,6 +176,11 @@ cudaError_t chain_attributes(int cpt, int optin) {
                 e = allow_max_smem(v ? chain_batch_kernel<T, true>(cpt, nqc) : chain_batch_kernel<T, false>(cpt, nqc), optin);
             if (e != cudaSuccess) return e;
         }
+    for (int v = 0; v < 2; ++v) {
+        cudaError_t e = allow_max_smem(v ? ctcell_kernel<T, true>(cpt) : ctcell_kernel<T, false>(cpt), optin);
+        if (e == cudaSuccess) e = allow_max_smem(v ? ctcell_batch_kernel<T, true>(cpt) : ctcell_batch_kernel<T, false>(cpt), optin);
+        if (e != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 
