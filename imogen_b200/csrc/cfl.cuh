@@ -40,10 +40,11 @@ __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vbloc
             for (int c = 0; c < 3; ++c)
                 if (a.use_b[c]) { double b = cb[c][i]; msq = msq + b * b; }
         }
-        double cs = sound_speed(a.gamma, r, px, py, pz, (double)E[i], msq);
-        m3[0] = fmax(m3[0], fabs(px / r) + cs);
-        m3[1] = fmax(m3[1], fabs(py / r) + cs);
-        m3[2] = fmax(m3[2], fabs(pz / r) + cs);
+        double sp[3];
+        cfl_speeds(a.gamma, r, px, py, pz, (double)E[i], msq, sp);
+        m3[0] = fmax(m3[0], sp[0]);
+        m3[1] = fmax(m3[1], sp[1]);
+        m3[2] = fmax(m3[2], sp[2]);
     }
     __shared__ double wp[3][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -234,13 +234,18 @@ __device__ __forceinline__ PressOutF pressure_totsnd_mixed(double G, float rho, 
     return o;
 }
 
-__device__ __forceinline__ double sound_speed(double G, double rho, double px, double py, double pz, double E,
-                                              double msq) {
-    double vsq = (px * px + py * py + pz * pz) / (rho * rho);
+// CFL speed candidates |p_c / rho| + c_s of one cell, c = x, y, z (TimeManager.m:65-77 with the
+// 'sound' speed of pressure.m): one FP64 reciprocal of rho serves the four quotients.
+__device__ __forceinline__ void cfl_speeds(double G, double rho, double px, double py, double pz, double E,
+                                           double msq, double s[3]) {
+    const double inv = 1.0 / rho;
+    const double vsq = (px * px + py * py + pz * pz) * (inv * inv);
     double r = (G - 1.0) * (E - 0.5 * rho * vsq);
     r = r - (G - 1.0) * 0.5 * msq;
-    r = sqrt(fabs((G * r + 2.0 * msq) / rho));
-    return r < 0 ? 0.0 : r;
+    const double cs = sqrt(fabs((G * r + 2.0 * msq) * inv));
+    s[0] = fabs(px * inv) + cs;
+    s[1] = fabs(py * inv) + cs;
+    s[2] = fabs(pz * inv) + cs;
 }
 
 // Atomic max of a non-negative double through its bit pattern (NaN never reaches here).

@@ -192,7 +192,10 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
 
 // One fluid sweep of one grid, run by CTA `vblock` of that grid's launch.
 // FADE: some BC of this sweep direction is fade (compiles the damping in).
-template <typename T, bool MHD, int CPT, bool FADE>
+// CG (copy ghosts): single-CTA pencils whose three fluid classes share one circ or const mode per
+// side.  Those ghosts copy an own row (circ: the far end, const: the near end), so the reader of
+// row 0 or N-1 indexes that row directly: no halo jobs and no barrier after them.
+template <typename T, bool MHD, int CPT, bool FADE, bool CG>
 __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
@@ -210,12 +213,24 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
     T* SB = SA + 10 * AS;                 // set B
     Ghost<T>* AN = reinterpret_cast<Ghost<T>*>(SA + 20 * AS);   // fade anchors [array][side][column]
 
+    // copy ghosts: shared index of the row that row -1 (dn_src) and row N (up_src) copy
+    const int N = tl.N;
+    const int dn_src = tl.ridx(a.mode[CLS_MASS][0] == BC_CIRC ? N - 1 : 0);
+    const int up_src = tl.ridx(a.mode[CLS_MASS][1] == BC_CIRC ? 0 : N - 1);
+    // A.shift(d, n) at own row k, n = -1 or +1 (the anchors `an` are read under fade only)
+    auto sh = [&](const T* A, const Ghost<T>* an, int k, int n, int mode) -> T {
+        if constexpr (CG) {
+            const int r = tl.grow(k);
+            const int ix = n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs);
+            return A[ix];
+        } else {
+            return shifted<FADE>(tl, A, an, k, n, mode, a.fade, a.fade_f);
+        }
+    };
     const double G = a.gamma;
     const double dt = a.tm->dt;
     const T ff = (T)(dt / a.dx);
     const T half_ffx = (T)(0.5 * (dt / a.dx));
-    const double* fc = a.fade;
-    const int fw = a.fade_f;
 
     // ---- load u (rho, px, py, pz, E) and cell-centred B; freezing speed #1 (wFluidFlux.m:18-22) --
     T u[5][CPT], bb[3][CPT], press[CPT];
@@ -265,8 +280,10 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
         }
     }
     tl.csync();
-    fluid_halo_jobs(tl, a, SA, AS, AN, /*lower: R*/ 1, /*upper: L*/ 2, FO_STORE_R, FO_STORE_L);
-    __syncthreads();
+    if constexpr (!CG) {
+        fluid_halo_jobs(tl, a, SA, AS, AN, /*lower: R*/ 1, /*upper: L*/ 2, FO_STORE_R, FO_STORE_L);
+        __syncthreads();
+    }
 
     // ---- predictor (relaxingFluid.m:32-39): half-step state -> set B; freezing speed #2 -----------
     T lmax2 = T(0);
@@ -280,8 +297,8 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
             const int cls = fluid_class(v);
             const T* R = SA + v * AS;
             const T* L = SA + (5 + v) * AS;
-            const T Rm = shifted<FADE>(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted<FADE>(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = sh(R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0]);
+            const T Lp = sh(L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1]);
             us[v] = u[v][k] - half_ffx * cf * (R[ix] - Rm + L[ix] - Lp);
         }
         us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
@@ -320,8 +337,10 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
         }
     }
     tl.csync();
-    fluid_halo_jobs(tl, a, SA, AS, AN, 3, 3, FO_R, FO_L);
-    __syncthreads();
+    if constexpr (!CG) {
+        fluid_halo_jobs(tl, a, SA, AS, AN, 3, 3, FO_R, FO_L);
+        __syncthreads();
+    }
 
     // ---- TVD limiter (relaxingFluid.m:57-62): corrected R and L -> set B --------------------------
 #pragma unroll
@@ -336,17 +355,19 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
             const Ghost<T>* aL = AN + (2 * (5 + v)) * Wb;
             const int mlo = a.mode[cls][0], mhi = a.mode[cls][1];
             const T r = R[ix], l = L[ix];
-            const T Rm = shifted<FADE>(tl, R, aR, k, -1, mlo, fc, fw);
-            const T Rp = shifted<FADE>(tl, R, aR + Wb, k, +1, mhi, fc, fw);
-            const T Lm = shifted<FADE>(tl, L, aL, k, -1, mlo, fc, fw);
-            const T Lp = shifted<FADE>(tl, L, aL + Wb, k, +1, mhi, fc, fw);
+            const T Rm = sh(R, aR, k, -1, mlo);
+            const T Rp = sh(R, aR + Wb, k, +1, mhi);
+            const T Lm = sh(L, aL, k, -1, mlo);
+            const T Lp = sh(L, aL + Wb, k, +1, mhi);
             SB[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
             SB[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
         }
     }
     tl.csync();
-    fluid_halo_jobs(tl, a, SB, AS, AN, 1, 2, FO_R, FO_L);
-    __syncthreads();
+    if constexpr (!CG) {
+        fluid_halo_jobs(tl, a, SB, AS, AN, 1, 2, FO_R, FO_L);
+        __syncthreads();
+    }
 
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
     double m3[3] = {0.0, 0.0, 0.0};
@@ -359,8 +380,8 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
             const int cls = fluid_class(v);
             const T* R = SB + v * AS;
             const T* L = SB + (5 + v) * AS;
-            const T Rm = shifted<FADE>(tl, R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0], fc, fw);
-            const T Lp = shifted<FADE>(tl, L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1], fc, fw);
+            const T Rm = sh(R, AN + (2 * v) * Wb, k, -1, a.mode[cls][0]);
+            const T Lp = sh(L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1]);
             unew[v] = u[v][k] - ff * cfs * (R[ix] - Rm + L[ix] - Lp);
         }
         unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
@@ -369,10 +390,11 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
 #pragma unroll
         for (int v = 0; v < 5; ++v) stq<T>(a.q[v], o, unew[v]);
         if (a.cfl) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
-            double cs = sound_speed(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3],
-                                    (double)unew[4], msq[k]);
+            double sp[3];
+            cfl_speeds(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3], (double)unew[4], msq[k],
+                       sp);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], fabs((double)unew[1 + c] / (double)unew[0]) + cs);
+            for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp[c]);
         }
     }
 
@@ -395,20 +417,20 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
     }
 }
 
-template <typename T, bool MHD, int CPT, bool FADE>
+template <typename T, bool MHD, int CPT, bool FADE, bool CG>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
-    fluid_sweep_body<T, MHD, CPT, FADE>(a, blockIdx.x);
+    fluid_sweep_body<T, MHD, CPT, FADE, CG>(a, blockIdx.x);
 }
 
 // The same sweep over many grids in one launch (BlockMap per CTA, arguments per member).
-template <typename T, bool MHD, int CPT, bool FADE>
+template <typename T, bool MHD, int CPT, bool FADE, bool CG>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_batch_kernel(const FluidArgs* __restrict__ args,
                                                                                   const BlockMap* __restrict__ map) {
     __shared__ FluidArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    fluid_sweep_body<T, MHD, CPT, FADE>(sa, (unsigned)bm.block);
+    fluid_sweep_body<T, MHD, CPT, FADE, CG>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

@@ -411,8 +411,15 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.cfl = cfl;
-    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
-                                            fade_on(c, d, CLS_MASS, CLS_ENER));
+    PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+                                      fade_on(c, d, CLS_MASS, CLS_ENER));
+    // copy ghosts: single-CTA pencils, one circ or const mode per side shared by the fluid classes
+    L.cg = pcf.CL == 1;
+    for (int k = 0; k < 3; ++k)
+        for (int side = 0; side < 2; ++side) {
+            const int m = a.mode[k][side];
+            if ((m != IMG_BC_CIRC && m != IMG_BC_CONST) || m != a.mode[CLS_MASS][side]) L.cg = false;
+        }
     if (ctx->rec) {
         OpRec r{};
         r.kind = OP_FLUID;
@@ -1334,7 +1341,7 @@ size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
 
 bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
     return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
-           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade;
+           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg;
 }
 
 // Turn the members' records into batched launch items and the arena image.

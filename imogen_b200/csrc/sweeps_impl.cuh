@@ -46,12 +46,12 @@ cudaError_t launch_pencil(void (*kern)(const Args), const Args& a, const PencilL
     return cudaLaunchKernelEx(&lc, kern, a);
 }
 
-template <typename T, bool MHD, bool FADE>
+template <typename T, bool MHD, bool FADE, bool CG>
 void (*fluid_kernel(int cpt))(const FluidArgs) {
     switch (cpt) {
-        case 1: return fluid_sweep_kernel<T, MHD, 1, FADE>;
-        case 2: return fluid_sweep_kernel<T, MHD, 2, FADE>;
-        default: return fluid_sweep_kernel<T, MHD, 4, FADE>;
+        case 1: return fluid_sweep_kernel<T, MHD, 1, FADE, CG>;
+        case 2: return fluid_sweep_kernel<T, MHD, 2, FADE, CG>;
+        default: return fluid_sweep_kernel<T, MHD, 4, FADE, CG>;
     }
 }
 
@@ -65,12 +65,12 @@ void (*chain_kernel(int cpt, int nqc))(const MagArgs) {
     }
 }
 
-template <typename T, bool MHD, bool FADE>
+template <typename T, bool MHD, bool FADE, bool CG>
 void (*fluid_batch_kernel(int cpt))(const FluidArgs*, const BlockMap*) {
     switch (cpt) {
-        case 1: return fluid_sweep_batch_kernel<T, MHD, 1, FADE>;
-        case 2: return fluid_sweep_batch_kernel<T, MHD, 2, FADE>;
-        default: return fluid_sweep_batch_kernel<T, MHD, 4, FADE>;
+        case 1: return fluid_sweep_batch_kernel<T, MHD, 1, FADE, CG>;
+        case 2: return fluid_sweep_batch_kernel<T, MHD, 2, FADE, CG>;
+        default: return fluid_sweep_batch_kernel<T, MHD, 4, FADE, CG>;
     }
 }
 
@@ -84,15 +84,21 @@ void (*chain_batch_kernel(int cpt, int nqc))(const MagArgs*, const BlockMap*) {
     }
 }
 
+// Ghost variant: 0 halo jobs, 1 halo jobs with fade damping, 2 copy ghosts.
+inline int ghost_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
+
 template <typename T>
-void (*fluid_batch_kernel(int cpt, bool mhd, bool fade))(const FluidArgs*, const BlockMap*) {
-    if (mhd) return fade ? fluid_batch_kernel<T, true, true>(cpt) : fluid_batch_kernel<T, true, false>(cpt);
-    return fade ? fluid_batch_kernel<T, false, true>(cpt) : fluid_batch_kernel<T, false, false>(cpt);
+void (*fluid_batch_kernel(int cpt, bool mhd, int gv))(const FluidArgs*, const BlockMap*) {
+    if (mhd)
+        return gv == 1 ? fluid_batch_kernel<T, true, true, false>(cpt)
+                       : (gv == 2 ? fluid_batch_kernel<T, true, false, true>(cpt) : fluid_batch_kernel<T, true, false, false>(cpt));
+    return gv == 1 ? fluid_batch_kernel<T, false, true, false>(cpt)
+                   : (gv == 2 ? fluid_batch_kernel<T, false, false, true>(cpt) : fluid_batch_kernel<T, false, false, false>(cpt));
 }
 
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
-    return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, L.fade), args, map, L);
+    return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, ghost_variant(L.fade, L.cg)), args, map, L);
 }
 
 template <typename T>
@@ -126,14 +132,17 @@ cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, co
 }
 
 template <typename T>
-void (*fluid_kernel(int cpt, bool mhd, bool fade))(const FluidArgs) {
-    if (mhd) return fade ? fluid_kernel<T, true, true>(cpt) : fluid_kernel<T, true, false>(cpt);
-    return fade ? fluid_kernel<T, false, true>(cpt) : fluid_kernel<T, false, false>(cpt);
+void (*fluid_kernel(int cpt, bool mhd, int gv))(const FluidArgs) {
+    if (mhd)
+        return gv == 1 ? fluid_kernel<T, true, true, false>(cpt)
+                       : (gv == 2 ? fluid_kernel<T, true, false, true>(cpt) : fluid_kernel<T, true, false, false>(cpt));
+    return gv == 1 ? fluid_kernel<T, false, true, false>(cpt)
+                   : (gv == 2 ? fluid_kernel<T, false, false, true>(cpt) : fluid_kernel<T, false, false, false>(cpt));
 }
 
 template <typename T>
 cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd) {
-    return launch_pencil(fluid_kernel<T>(L.cpt, mhd, L.fade), a, L);
+    return launch_pencil(fluid_kernel<T>(L.cpt, mhd, ghost_variant(L.fade, L.cg)), a, L);
 }
 
 template <typename T>
@@ -159,7 +168,7 @@ cudaError_t allow_max_smem(K kern, int optin) {
 
 template <typename T>
 cudaError_t fluid_attributes(int cpt, int optin) {
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 6; ++v) {
         cudaError_t e = allow_max_smem(fluid_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e == cudaSuccess) e = allow_max_smem(fluid_batch_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e != cudaSuccess) return e;
@@ -197,7 +206,7 @@ cudaError_t fluid_max_clusters(const PencilLaunch& L, int* n) {
     attr[0].val.clusterDim.z = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(n, fluid_kernel<T>(L.cpt, true, L.fade), &lc);
+    return cudaOccupancyMaxActiveClusters(n, fluid_kernel<T>(L.cpt, true, ghost_variant(L.fade, L.cg)), &lc);
 }
 
 }  // namespace img
