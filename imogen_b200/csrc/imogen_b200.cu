@@ -488,10 +488,13 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     fill_mag_args<T>(ctx, X, I1, I2, a);
     const int d = X - 1;
     const PencilCfg& pcf = ctx->pcfg[1][d];
-    const PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
-                                            2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
-    const PencilLaunch Lc = pencil_launch<T>(ctx, pcf, d, ctcell_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
-                                             fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
+                                      2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    PencilLaunch Lc = pencil_launch<T>(ctx, pcf, d, ctcell_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+                                       fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    // copy ghosts: single-CTA pencils with circ or const mag-class shifts along X
+    L.cg = Lc.cg = pcf.CL == 1 && (a.modeX[0] == IMG_BC_CIRC || a.modeX[0] == IMG_BC_CONST) &&
+                   (a.modeX[1] == IMG_BC_CIRC || a.modeX[1] == IMG_BC_CONST);
     if (ctx->rec) {
         OpRec r{};
         r.elem = sizeof(T);

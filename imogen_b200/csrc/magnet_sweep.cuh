@@ -164,8 +164,10 @@ struct ChainComp {
 // The chain of one grid, run by CTA (vblock, blockIdx.y) of that grid's launch: NQC = 1 handles
 // component blockIdx.y, NQC = 2 both transverse components, interleaved stage by stage so that
 // every barrier serves twice the work.
-// FADE: a mag-class BC along X is fade (compiles the damping in).
-template <typename T, int CPT, bool FADE, int NQC>
+// FADE: a mag-class BC along X is fade (compiles the damping in).  CG (copy ghosts): single-CTA
+// pencils with circ or const mag-class shifts along X; the reader of a row next to a pencil end
+// indexes the row its ghost copies, so no stage needs halo jobs or the barrier after them.
+template <typename T, int CPT, bool FADE, int NQC, bool CG>
 __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
@@ -192,6 +194,19 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     const int f = a.fade_f;
     const double binf = a.bc_inf;
     const int mlo = a.modeX[0], mhi = a.modeX[1];
+    // copy ghosts: shared index of the row that row -1, row N and row N+1 copy
+    const int dn_src = tl.ridx(mlo == BC_CIRC ? N - 1 : 0);
+    const int up_src = tl.ridx(mhi == BC_CIRC ? 0 : N - 1);
+    const int up2_src = tl.ridx(mhi == BC_CIRC ? 1 : N - 1);
+    // A.shift(X, n) at own row k for n = -1 or +1 (anchors `an` read under fade only)
+    auto sh = [&](const T* A, const Ghost<T>* an, int k, int n, int mode) -> T {
+        if constexpr (CG) {
+            const int r = tl.grow(k);
+            return A[n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs)];
+        } else {
+            return shifted<FADE>(tl, A, an, k, n, mode, fc, f);
+        }
+    };
     // the scratch objects of mag(I) for this sweep (mag-class BC along X, no mirror flip)
     auto edge_of = [&](int q, int kind, int side) -> double* { return et->p[mag_obj(cp[q].e, d, kind)][d][side]; };
     // halo jobs: (component q, side) is done by thread g == (2q + side) mod G of the column
@@ -243,31 +258,35 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
         }
     }
     tl.csync();
+    if constexpr (!CG) {
 #pragma unroll
-    for (int q = 0; q < NQC; ++q) halo(q, S(q, 0), MO_VELGRID, true, true, 1);
-    __syncthreads();
+        for (int q = 0; q < NQC; ++q) halo(q, S(q, 0), MO_VELGRID, true, true, 1);
+        __syncthreads();
+    }
     // vg = 0.25*(vg.shift(X,-1) + vg.shift(X,1) + 2*vg)   (magnetFlux.m:21-23)
     T vg[NQC][CPT];
 #pragma unroll
     for (int q = 0; q < NQC; ++q)
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const T m1 = shifted<FADE>(tl, (const T*)S(q, 0), GS(q), k, -1, mlo, fc, f);
-            const T p1 = shifted<FADE>(tl, (const T*)S(q, 0), GS(q) + Wb, k, +1, mhi, fc, f);
+            const T m1 = sh((const T*)S(q, 0), GS(q), k, -1, mlo);
+            const T p1 = sh((const T*)S(q, 0), GS(q) + Wb, k, +1, mhi);
             vg[q][k] = tl.ok(k) ? T(0.25) * (m1 + p1 + T(2) * vgr[q][k]) : T(0);
             S(q, 1)[tl.idx(k)] = vg[q][k];
         }
     tl.csync();
+    if constexpr (!CG) {
 #pragma unroll
-    for (int q = 0; q < NQC; ++q) halo(q, S(q, 1), MO_VELGRID, false, true, 1);
-    __syncthreads();
+        for (int q = 0; q < NQC; ++q) halo(q, S(q, 1), MO_VELGRID, false, true, 1);
+        __syncthreads();
+    }
     // velocityFlow = (vg + vg.shift(X,1)) < 0; store.fluxR = B_I.*vg   (relaxingMagnet.m:17,22)
     T vf[NQC][CPT];
 #pragma unroll
     for (int q = 0; q < NQC; ++q)
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const T p1 = shifted<FADE>(tl, (const T*)S(q, 1), GS(q) + Wb, k, +1, mhi, fc, f);
+            const T p1 = sh((const T*)S(q, 1), GS(q) + Wb, k, +1, mhi);
             vf[q][k] = (vg[q][k] + p1) < T(0) ? T(1) : T(0);
             const T F = bI[q][k] * vg[q][k];
             S(q, 2)[tl.idx(k)] = F;
@@ -278,22 +297,26 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             }
         }
     tl.csync();
+    if constexpr (!CG) {
 #pragma unroll
-    for (int q = 0; q < NQC; ++q) halo(q, S(q, 2), MO_STORE_R, false, true, 1);
-    __syncthreads();
+        for (int q = 0; q < NQC; ++q) halo(q, S(q, 2), MO_STORE_R, false, true, 1);
+        __syncthreads();
+    }
     // store.fluxR = F.*(1-vf) + F.shift(X,1).*vf   (relaxingMagnet.m:23-24)
 #pragma unroll
     for (int q = 0; q < NQC; ++q)
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const T F = S(q, 2)[tl.idx(k)];
-            const T Fp = shifted<FADE>(tl, (const T*)S(q, 2), GS(q) + Wb, k, +1, mhi, fc, f);
+            const T Fp = sh((const T*)S(q, 2), GS(q) + Wb, k, +1, mhi);
             S(q, 3)[tl.idx(k)] = F * (T(1) - vf[q][k]) + Fp * vf[q][k];
         }
     tl.csync();
+    if constexpr (!CG) {
 #pragma unroll
-    for (int q = 0; q < NQC; ++q) halo(q, S(q, 3), MO_STORE_R, true, false, 1);
-    __syncthreads();
+        for (int q = 0; q < NQC; ++q) halo(q, S(q, 3), MO_STORE_R, true, false, 1);
+        __syncthreads();
+    }
     // store = B_I - ff*(fluxR - fluxR.shift(X,-1)); wMag = store.*velGrid   (relaxingMagnet.m:26-33)
     T W[NQC][CPT];
 #pragma unroll
@@ -301,7 +324,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
             const T Fu = S(q, 3)[tl.idx(k)];
-            const T st = bI[q][k] - ff * (Fu - shifted<FADE>(tl, (const T*)S(q, 3), GS(q), k, -1, mlo, fc, f));
+            const T st = bI[q][k] - ff * (Fu - sh((const T*)S(q, 3), GS(q), k, -1, mlo));
             W[q][k] = st * vg[q][k];
             S(q, 0)[tl.idx(k)] = W[q][k];
             if (cp[q].init_mag && tl.ok(k)) {
@@ -320,6 +343,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
 #pragma unroll
     for (int q = 0; q < NQC; ++q) {
         e4[q] = 0.0;
+        if constexpr (CG) continue;
         halo(q, S(q, 0), MO_WMAG, true, false, 2);
         Ghost<T>* gs = GS(q);
         if (job(q, 1) && own_end)
@@ -333,7 +357,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             gs[3 * Wb + b] = w2;
         }
     }
-    __syncthreads();
+    if constexpr (!CG) __syncthreads();
     T Fl[NQC][CPT];
 #pragma unroll
     for (int q = 0; q < NQC; ++q) {
@@ -345,7 +369,10 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             const int ix = tl.idx(k);
             const int r = tl.grow(k);
             T p1a = A[ix + tl.rs], p1b = p1a, p1d = p1a, p2 = A[ix + 2 * tl.rs];
-            if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
+            if constexpr (CG) {   // the four upper calls share their ghosts
+                p1a = p1b = p1d = A[r == N - 1 ? up_src : ix + tl.rs];
+                p2 = A[r == N - 2 ? up_src : (r == N - 1 ? up2_src : ix + 2 * tl.rs)];
+            } else if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
                 if (r == N - 1) {
                     p1a = gs[1 * Wb + b].g;
                     p1b = gs[2 * Wb + b].g;
@@ -363,7 +390,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
                 p1d = fade_apply(p1d, r, N, fc, f, u1.s0, u1.sN1);
                 p2 = fade_apply(p2, r, N, fc, f, u2.s0, u2.sN1);
             }
-            const T m1 = shifted<FADE>(tl, A, gs, k, -1, mlo, fc, f);
+            const T m1 = sh(A, gs, k, -1, mlo);
             const T fx = w * (T(1) - v) + p1a * v;
             const T dFluxR = p1b - (v * p2 + (T(1) - v) * w);
             const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
@@ -377,21 +404,23 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
         }
     }
     tl.csync();
+    if constexpr (!CG) {
 #pragma unroll
-    for (int q = 0; q < NQC; ++q) {
-        if (job(q, 1) && tl.rank == tl.rank_hi && mhi == BC_TRANS && a.actX) {
-            double* eh = edge_of(q, MO_WMAG, 1);
-            if (eh) eh[tl.col] = e4[q];
+        for (int q = 0; q < NQC; ++q) {
+            if (job(q, 1) && tl.rank == tl.rank_hi && mhi == BC_TRANS && a.actX) {
+                double* eh = edge_of(q, MO_WMAG, 1);
+                if (eh) eh[tl.col] = e4[q];
+            }
+            halo(q, S(q, 1), MO_FLUX, true, false, 1);
         }
-        halo(q, S(q, 1), MO_FLUX, true, false, 1);
+        __syncthreads();
     }
-    __syncthreads();
     // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49); F_I -> scratch for CT
 #pragma unroll
     for (int q = 0; q < NQC; ++q)
 #pragma unroll
         for (int k = 0; k < CPT; ++k) {
-            const T fm = shifted<FADE>(tl, (const T*)S(q, 1), GS(q), k, -1, mlo, fc, f);
+            const T fm = sh((const T*)S(q, 1), GS(q), k, -1, mlo);
             if (!tl.ok(k)) continue;
             const long long o = tl.off(k);
             cp[q].BI[o] = bI[q][k] - ff2 * (Fl[q][k] - fm);
@@ -415,7 +444,7 @@ __host__ __device__ inline size_t ctcell_smem_bytes(int RC, int Wb) {
     return 3 * (sizeof(T) * (size_t)tile_rows(RC) * Wb + sizeof(Ghost<T>) * (size_t)Wb);
 }
 
-template <typename T, int CPT, bool FADE>
+template <typename T, int CPT, bool FADE, bool CG>
 __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
@@ -430,6 +459,10 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
     const int f = a.fade_f;
     const double binf = a.bc_inf;
     const int mlo = a.modeX[0], mhi = a.modeX[1];
+    const int N = tl.N;
+    // copy ghosts (see mag_chain_body): the rows that row -1 and row N copy
+    const int dn_src = tl.ridx(mlo == BC_CIRC ? N - 1 : 0);
+    const int up_src = tl.ridx(mhi == BC_CIRC ? 0 : N - 1);
     const size_t AS = (size_t)tile_rows(tl.RC) * Wb;
     // shared: C_1, C_2, new B_X; then their ghost/anchor slots (C lower sides, B_X upper side)
     T* const S = reinterpret_cast<T*>(smem);
@@ -464,29 +497,40 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
         }
     }
     tl.csync();
-    // lower ghosts of C_q along X: the flux object's mag-class BC, no mirror flip (I != X)
+    if constexpr (!CG) {
+        // lower ghosts of C_q along X: the flux object's mag-class BC, no mirror flip (I != X)
 #pragma unroll
-    for (int q = 0; q < 2; ++q)
-        if (tl.colok && tl.g == q % tl.G)
-            halo_job(tl, S + q * AS, GS + q * Wb, 0, true, mlo, a.actX, 0,
-                     et->p[mag_obj((q ? a.I[1] : a.I[0]) - 1, d, MO_FLUX)][d][0], binf, 1);
-    __syncthreads();
+        for (int q = 0; q < 2; ++q)
+            if (tl.colok && tl.g == q % tl.G)
+                halo_job(tl, S + q * AS, GS + q * Wb, 0, true, mlo, a.actX, 0,
+                         et->p[mag_obj((q ? a.I[1] : a.I[0]) - 1, d, MO_FLUX)][d][0], binf, 1);
+        __syncthreads();
+    }
     T* BX = reinterpret_cast<T*>(a.q[Q_BX + d]);
     const T f0 = (T)(dt / a.dI[0]), f1 = (T)(dt / a.dI[1]);
     T bx[CPT];
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T D0 = shifted<FADE>(tl, (const T*)S, GS, k, -1, mlo, fc, f);
-        const T D1 = shifted<FADE>(tl, (const T*)(S + AS), GS + Wb, k, -1, mlo, fc, f);
+        T D0, D1;
+        if constexpr (CG) {
+            const int ix = tl.grow(k) == 0 ? dn_src : tl.idx(k) - tl.rs;
+            D0 = S[ix];
+            D1 = S[AS + ix];
+        } else {
+            D0 = shifted<FADE>(tl, (const T*)S, GS, k, -1, mlo, fc, f);
+            D1 = shifted<FADE>(tl, (const T*)(S + AS), GS + Wb, k, -1, mlo, fc, f);
+        }
         bx[k] = T(0);
         if (tl.ok(k)) bx[k] = (BX[tl.off(k)] - f0 * D0) - f1 * D1;
         S[2 * AS + tl.idx(k)] = bx[k];
     }
     tl.csync();
-    // upper ghost of the new B_X along X: mag(X).shift(X, +1) of the primary array (mirror flips B_X)
-    if (tl.colok && tl.g == 2 % tl.G)
-        halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, 1, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
-    __syncthreads();
+    if constexpr (!CG) {
+        // upper ghost of the new B_X along X: mag(X).shift(X, +1) of the primary array (mirror flips B_X)
+        if (tl.colok && tl.g == 2 % tl.G)
+            halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, 1, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
+        __syncthreads();
+    }
     T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
     const int e2 = a.I[1] - 1;
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
@@ -498,7 +542,9 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
     const long long s2 = sel3(e2, g.s[0], g.s[1], g.s[2]);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const T up = shifted<FADE>(tl, (const T*)(S + 2 * AS), GS + 2 * Wb, k, +1, mhi, fc, f);
+        T up;
+        if constexpr (CG) up = S[2 * AS + (tl.grow(k) == N - 1 ? up_src : tl.idx(k) + tl.rs)];
+        else up = shifted<FADE>(tl, (const T*)(S + 2 * AS), GS + 2 * Wb, k, +1, mhi, fc, f);
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
         BX[o] = bx[k];
@@ -525,35 +571,35 @@ __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, 
     y = (int)(r - (unsigned)z * n1);
 }
 
-template <typename T, int CPT, bool FADE, int NQC>
+template <typename T, int CPT, bool FADE, int NQC, bool CG>
 __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
-    mag_chain_body<T, CPT, FADE, NQC>(a, blockIdx.x);
+    mag_chain_body<T, CPT, FADE, NQC, CG>(a, blockIdx.x);
 }
 
-template <typename T, int CPT, bool FADE>
+template <typename T, int CPT, bool FADE, bool CG>
 __global__ void __launch_bounds__(512, 2) mag_ctcell_kernel(const __grid_constant__ MagArgs a) {
-    mag_ctcell_body<T, CPT, FADE>(a, blockIdx.x);
+    mag_ctcell_body<T, CPT, FADE, CG>(a, blockIdx.x);
 }
 
 // The same passes over many grids in one launch (BlockMap per CTA, arguments per member).
-template <typename T, int CPT, bool FADE, int NQC>
+template <typename T, int CPT, bool FADE, int NQC, bool CG>
 __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_batch_kernel(const MagArgs* __restrict__ args,
                                                                                 const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    mag_chain_body<T, CPT, FADE, NQC>(sa, (unsigned)bm.block);
+    mag_chain_body<T, CPT, FADE, NQC, CG>(sa, (unsigned)bm.block);
 }
 
-template <typename T, int CPT, bool FADE>
+template <typename T, int CPT, bool FADE, bool CG>
 __global__ void __launch_bounds__(512, 2) mag_ctcell_batch_kernel(const MagArgs* __restrict__ args,
                                                                   const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    mag_ctcell_body<T, CPT, FADE>(sa, (unsigned)bm.block);
+    mag_ctcell_body<T, CPT, FADE, CG>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

@@ -55,14 +55,23 @@ void (*fluid_kernel(int cpt))(const FluidArgs) {
     }
 }
 
-template <typename T, bool FADE>
+template <typename T, bool FADE, bool CG>
 void (*chain_kernel(int cpt, int nqc))(const MagArgs) {
-    if (nqc == 2) return cpt == 1 ? mag_chain_kernel<T, 1, FADE, 2> : mag_chain_kernel<T, 2, FADE, 2>;
+    if (nqc == 2) return cpt == 1 ? mag_chain_kernel<T, 1, FADE, 2, CG> : mag_chain_kernel<T, 2, FADE, 2, CG>;
     switch (cpt) {
-        case 1: return mag_chain_kernel<T, 1, FADE, 1>;
-        case 2: return mag_chain_kernel<T, 2, FADE, 1>;
-        default: return mag_chain_kernel<T, 4, FADE, 1>;
+        case 1: return mag_chain_kernel<T, 1, FADE, 1, CG>;
+        case 2: return mag_chain_kernel<T, 2, FADE, 1, CG>;
+        default: return mag_chain_kernel<T, 4, FADE, 1, CG>;
     }
+}
+
+// Ghost variant: 0 halo jobs, 1 halo jobs with fade damping, 2 copy ghosts.
+inline int ghost_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
+
+template <typename T>
+void (*chain_kernel(int cpt, int nqc, int gv))(const MagArgs) {
+    return gv == 1 ? chain_kernel<T, true, false>(cpt, nqc)
+                   : (gv == 2 ? chain_kernel<T, false, true>(cpt, nqc) : chain_kernel<T, false, false>(cpt, nqc));
 }
 
 template <typename T, bool MHD, bool FADE, bool CG>
@@ -74,18 +83,21 @@ void (*fluid_batch_kernel(int cpt))(const FluidArgs*, const BlockMap*) {
     }
 }
 
-template <typename T, bool FADE>
+template <typename T, bool FADE, bool CG>
 void (*chain_batch_kernel(int cpt, int nqc))(const MagArgs*, const BlockMap*) {
-    if (nqc == 2) return cpt == 1 ? mag_chain_batch_kernel<T, 1, FADE, 2> : mag_chain_batch_kernel<T, 2, FADE, 2>;
+    if (nqc == 2) return cpt == 1 ? mag_chain_batch_kernel<T, 1, FADE, 2, CG> : mag_chain_batch_kernel<T, 2, FADE, 2, CG>;
     switch (cpt) {
-        case 1: return mag_chain_batch_kernel<T, 1, FADE, 1>;
-        case 2: return mag_chain_batch_kernel<T, 2, FADE, 1>;
-        default: return mag_chain_batch_kernel<T, 4, FADE, 1>;
+        case 1: return mag_chain_batch_kernel<T, 1, FADE, 1, CG>;
+        case 2: return mag_chain_batch_kernel<T, 2, FADE, 1, CG>;
+        default: return mag_chain_batch_kernel<T, 4, FADE, 1, CG>;
     }
 }
 
-// Ghost variant: 0 halo jobs, 1 halo jobs with fade damping, 2 copy ghosts.
-inline int ghost_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
+template <typename T>
+void (*chain_batch_kernel(int cpt, int nqc, int gv))(const MagArgs*, const BlockMap*) {
+    return gv == 1 ? chain_batch_kernel<T, true, false>(cpt, nqc)
+                   : (gv == 2 ? chain_batch_kernel<T, false, true>(cpt, nqc) : chain_batch_kernel<T, false, false>(cpt, nqc));
+}
 
 template <typename T>
 void (*fluid_batch_kernel(int cpt, bool mhd, int gv))(const FluidArgs*, const BlockMap*) {
@@ -103,32 +115,42 @@ cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map,
 
 template <typename T>
 cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
-    return launch_pencil_batch(L.fade ? chain_batch_kernel<T, true>(L.cpt, L.nqc) : chain_batch_kernel<T, false>(L.cpt, L.nqc),
-                               args, map, L);
+    return launch_pencil_batch(chain_batch_kernel<T>(L.cpt, L.nqc, ghost_variant(L.fade, L.cg)), args, map, L);
 }
 
-template <typename T, bool FADE>
+template <typename T, bool FADE, bool CG>
 void (*ctcell_kernel(int cpt))(const MagArgs) {
     switch (cpt) {
-        case 1: return mag_ctcell_kernel<T, 1, FADE>;
-        case 2: return mag_ctcell_kernel<T, 2, FADE>;
-        default: return mag_ctcell_kernel<T, 4, FADE>;
+        case 1: return mag_ctcell_kernel<T, 1, FADE, CG>;
+        case 2: return mag_ctcell_kernel<T, 2, FADE, CG>;
+        default: return mag_ctcell_kernel<T, 4, FADE, CG>;
     }
 }
 
-template <typename T, bool FADE>
+template <typename T, bool FADE, bool CG>
 void (*ctcell_batch_kernel(int cpt))(const MagArgs*, const BlockMap*) {
     switch (cpt) {
-        case 1: return mag_ctcell_batch_kernel<T, 1, FADE>;
-        case 2: return mag_ctcell_batch_kernel<T, 2, FADE>;
-        default: return mag_ctcell_batch_kernel<T, 4, FADE>;
+        case 1: return mag_ctcell_batch_kernel<T, 1, FADE, CG>;
+        case 2: return mag_ctcell_batch_kernel<T, 2, FADE, CG>;
+        default: return mag_ctcell_batch_kernel<T, 4, FADE, CG>;
     }
 }
 
 template <typename T>
+void (*ctcell_kernel(int cpt, int gv))(const MagArgs) {
+    return gv == 1 ? ctcell_kernel<T, true, false>(cpt)
+                   : (gv == 2 ? ctcell_kernel<T, false, true>(cpt) : ctcell_kernel<T, false, false>(cpt));
+}
+
+template <typename T>
+void (*ctcell_batch_kernel(int cpt, int gv))(const MagArgs*, const BlockMap*) {
+    return gv == 1 ? ctcell_batch_kernel<T, true, false>(cpt)
+                   : (gv == 2 ? ctcell_batch_kernel<T, false, true>(cpt) : ctcell_batch_kernel<T, false, false>(cpt));
+}
+
+template <typename T>
 cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
-    return launch_pencil_batch(L.fade ? ctcell_batch_kernel<T, true>(L.cpt) : ctcell_batch_kernel<T, false>(L.cpt),
-                               args, map, L);
+    return launch_pencil_batch(ctcell_batch_kernel<T>(L.cpt, ghost_variant(L.fade, L.cg)), args, map, L);
 }
 
 template <typename T>
@@ -147,12 +169,12 @@ cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool m
 
 template <typename T>
 cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L) {
-    return launch_pencil(L.fade ? chain_kernel<T, true>(L.cpt, L.nqc) : chain_kernel<T, false>(L.cpt, L.nqc), a, L);
+    return launch_pencil(chain_kernel<T>(L.cpt, L.nqc, ghost_variant(L.fade, L.cg)), a, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_ctcell(const MagArgs& a, const PencilLaunch& L) {
-    return launch_pencil(L.fade ? ctcell_kernel<T, true>(L.cpt) : ctcell_kernel<T, false>(L.cpt), a, L);
+    return launch_pencil(ctcell_kernel<T>(L.cpt, ghost_variant(L.fade, L.cg)), a, L);
 }
 
 // Allow a kernel the device's whole opt-in shared memory per block (minus its static shared
@@ -178,16 +200,14 @@ cudaError_t fluid_attributes(int cpt, int optin) {
 
 template <typename T>
 cudaError_t chain_attributes(int cpt, int optin) {
-    for (int v = 0; v < 2; ++v)
+    for (int gv = 0; gv < 3; ++gv) {
         for (int nqc = 1; nqc <= (cpt <= 2 ? 2 : 1); ++nqc) {
-            cudaError_t e = allow_max_smem(v ? chain_kernel<T, true>(cpt, nqc) : chain_kernel<T, false>(cpt, nqc), optin);
-            if (e == cudaSuccess)
-                e = allow_max_smem(v ? chain_batch_kernel<T, true>(cpt, nqc) : chain_batch_kernel<T, false>(cpt, nqc), optin);
+            cudaError_t e = allow_max_smem(chain_kernel<T>(cpt, nqc, gv), optin);
+            if (e == cudaSuccess) e = allow_max_smem(chain_batch_kernel<T>(cpt, nqc, gv), optin);
             if (e != cudaSuccess) return e;
         }
-    for (int v = 0; v < 2; ++v) {
-        cudaError_t e = allow_max_smem(v ? ctcell_kernel<T, true>(cpt) : ctcell_kernel<T, false>(cpt), optin);
-        if (e == cudaSuccess) e = allow_max_smem(v ? ctcell_batch_kernel<T, true>(cpt) : ctcell_batch_kernel<T, false>(cpt), optin);
+        cudaError_t e = allow_max_smem(ctcell_kernel<T>(cpt, gv), optin);
+        if (e == cudaSuccess) e = allow_max_smem(ctcell_batch_kernel<T>(cpt, gv), optin);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
