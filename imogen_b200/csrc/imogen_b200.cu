@@ -274,7 +274,8 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
     const int maxnt = 512;
-    PencilCfg p;
+    PencilCfg p, first;
+    bool have_first = false;
     for (int cpt : {1, 2, 4}) {
         int G = std::max(2, pow2ceil((N + cpt - 1) / cpt));
         int CL = 1, Wb;
@@ -304,8 +305,16 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
         p.CL = CL;
         p.NT = Wb * G;
         p.cpt = cpt;
-        if (CL <= 4) break;   // clusters of 8 CTAs of these kernels do not schedule: more cells per thread
+        // a pencil inside one CTA takes the copy-ghost kernels (no halo jobs) where its BCs allow:
+        // the fewest cells per thread that achieve it; otherwise the fewest with a cluster of at
+        // most 4 CTAs (clusters of 8 CTAs of these kernels do not schedule)
+        if (CL == 1 && tiling_fits(p, elem)) return p;
+        if (CL <= 4 && !have_first) {
+            first = p;
+            have_first = true;
+        }
     }
+    if (have_first) p = first;
     if (p.CL <= 4 && tiling_fits(p, elem)) return p;
     // too much shared memory per CTA (long FP64 pencils): the accepted tiling with the fewest
     // CTAs per cluster, then the fewest cells per thread, then the most threads
