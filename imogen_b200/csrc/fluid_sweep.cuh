@@ -97,6 +97,23 @@ __device__ __forceinline__ T press_speed(double G, int d, const T u[5], double m
     }
 }
 
+// Maximum over the full warp of non-negative, non-NaN values (speeds): the bit patterns of such
+// values order like unsigned integers, so one hardware reduction (two for FP64: high words, then
+// the low words of the lanes holding the largest high word) replaces a shuffle tree, exactly.
+template <typename T>
+__device__ __forceinline__ T warp_max_nonneg(T v) {
+    const unsigned full = 0xffffffffu;
+    if constexpr (sizeof(T) == 4) {
+        return __uint_as_float(__reduce_max_sync(full, __float_as_uint(v + 0.0f)));   // + 0: no -0
+    } else {
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(v + 0.0);
+        const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
+        const unsigned mh = __reduce_max_sync(full, hi);
+        const unsigned ml = __reduce_max_sync(full, hi == mh ? lo : 0u);
+        return __longlong_as_double((long long)(((unsigned long long)mh << 32) | ml));
+    }
+}
+
 // Column max over the pencil (and the cluster); also a stage barrier that orders this CTA's shared
 // reads before its next writes and, with a cluster, every rank's remote reads before them.  Lanes of
 // a column reduce with warp shuffles; one lane per (warp, column) writes part[warp][b]; after a CTA
@@ -107,7 +124,9 @@ template <typename T, int CPT>
 __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part)[33], T* cpart, T local) {
     const unsigned mask = 0xffffffffu;
     if (tl.d == 0 && tl.G <= 32 && tl.CL == 1) {   // each pencil lies inside one warp
-        for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        if (tl.G == 32) local = warp_max_nonneg(local);
+        else
+            for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
         __syncthreads();
         return local;
     }
@@ -122,7 +141,7 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int grp, lig, w0, nwc;   // lanes of the column in a warp, this lane's index among them, its warps
     if (tl.d == 0) {   // G is a multiple of 32: whole warps per column
-        for (int o = 16; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        local = warp_max_nonneg(local);
         grp = 32;
         lig = lane;
         w0 = (tl.b * tl.G) >> 5;
@@ -139,13 +158,17 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
     T m = T(0);
     for (int j = lig; j < nwc; j += grp) m = fmax(m, part[w0 + j][tl.b]);
     const int olo = tl.d == 0 ? 1 : tl.Wb;
-    for (int o = 16; o >= olo; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
+    if (tl.d == 0) m = warp_max_nonneg(m);
+    else
+        for (int o = 16; o >= olo; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
     if (tl.CL == 1) return m;
     if (tl.g == 0) cpart[tl.b] = m;
     cg::this_cluster().sync();
     T c = T(0);
     if (lig < tl.CL) c = tl.remote(cpart, lig)[tl.b];
-    for (int o = 16; o >= olo; o >>= 1) c = fmax(c, __shfl_xor_sync(mask, c, o));
+    if (tl.d == 0) c = warp_max_nonneg(c);
+    else
+        for (int o = 16; o >= olo; o >>= 1) c = fmax(c, __shfl_xor_sync(mask, c, o));
     return c;
 }
 
@@ -405,7 +428,7 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            for (int o = 16; o > 0; o >>= 1) m3[c] = fmax(m3[c], __shfl_xor_sync(0xffffffffu, m3[c], o));
+            m3[c] = warp_max_nonneg(m3[c]);
             if (lane == 0) cflp[c][warp] = m3[c];
         }
         __syncthreads();
