@@ -54,21 +54,29 @@ __device__ __forceinline__ void stq(void* p, long long i, T v) { reinterpret_cas
 // BC class of fluid variable v (rho -> mass, p_i -> mom, E -> ener).
 __device__ __forceinline__ int fluid_class(int v) { return v == 0 ? CLS_MASS : (v == 4 ? CLS_ENER : CLS_MOM); }
 
+// Mixed form: the numerators F of the w arrays of wFluidFlux.m:31-44 (w = F / c_f) for one cell,
+// with one reciprocal of rho.
+__device__ __forceinline__ void flux_num(int d, const float u[5], const float bb[3], float press, float F[5]) {
+    const float pX = sel3(d, u[1], u[2], u[3]);
+    const float bX = sel3(d, bb[0], bb[1], bb[2]);
+    const float ir = __frcp_rn(u[0]);
+    const float velocity = pX * ir;
+    F[0] = pX;
+    F[4] = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) F[1 + c] = velocity * u[1 + c] + press * (c == d ? 1.f : 0.f) - bX * bb[c];
+}
+
 // w arrays of wFluidFlux.m:31-44 for one cell (X = sweep dim d).
 template <typename T>
 __device__ __forceinline__ void wflux(int d, const T u[5], const T bb[3], T press, T cf, T w[5]) {
     const T pX = sel3(d, u[1], u[2], u[3]);
     T bX = sel3(d, bb[0], bb[1], bb[2]);
-    if constexpr (sizeof(T) == 4) {   // mixed form: one reciprocal each for rho and c_f
-        const T ir = __frcp_rn(u[0]), ic = __frcp_rn(cf);
-        const T velocity = pX * ir;
-        w[0] = pX * ic;
-        w[4] = (velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir) * ic;
+    if constexpr (sizeof(T) == 4) {   // mixed form: w = F * (1 / c_f)
+        const T ic = __frcp_rn(cf);
+        flux_num(d, u, bb, press, w);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            T dirv = c == d ? T(1) : T(0);
-            w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) * ic;
-        }
+        for (int v = 0; v < 5; ++v) w[v] = w[v] * ic;
     } else {   // plain FP64: the operation order of wFluidFlux.m
         T velocity = pX / u[0];
         w[0] = pX / cf;
@@ -172,6 +180,53 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
     return c;
 }
 
+// The two halves of column_max for single-CTA pencils, placed around a barrier the caller has anyway:
+// colmax_publish reduces within the warp and leaves the warp's value in `part` where a column spans
+// several warps; colmax_collect, after the barrier, reduces the column's warp values.
+template <typename T, int CPT>
+__device__ __forceinline__ T colmax_publish(const Tile<T, CPT>& tl, T (*part)[33], T local) {
+    const unsigned mask = 0xffffffffu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (tl.d == 0) {
+        if (tl.G >= 32) {   // whole warps per column
+            local = warp_max_nonneg(local);
+            if (lane == 0) part[warp][tl.b] = local;
+        } else {
+            for (int o = tl.G / 2; o > 0; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+        }
+        return local;
+    }
+    if (tl.Wb >= 32) {   // short pencils: one value per (row, column)
+        (&part[0][0])[tl.g * tl.Wb + tl.b] = local;
+        return local;
+    }
+    for (int o = 16; o >= tl.Wb; o >>= 1) local = fmax(local, __shfl_xor_sync(mask, local, o));
+    if (lane < tl.Wb) part[warp][tl.b] = local;
+    return local;
+}
+
+template <typename T, int CPT>
+__device__ __forceinline__ T colmax_collect(const Tile<T, CPT>& tl, int NT, const T (*part)[33], T wv) {
+    const unsigned mask = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    if (tl.d == 0) {
+        if (tl.G <= 32) return wv;
+        const int w0 = (tl.b * tl.G) >> 5, nwc = tl.G >> 5;
+        return warp_max_nonneg(lane < nwc ? part[w0 + lane][tl.b] : T(0));
+    }
+    if (tl.Wb >= 32) {
+        const T* flat = &part[0][0];
+        T m = T(0);
+        for (int r = 0; r < tl.G; ++r) m = fmax(m, flat[r * tl.Wb + tl.b]);
+        return m;
+    }
+    const int grp = 32 / tl.Wb, lig = lane / tl.Wb, nwc = NT >> 5;
+    T m = T(0);
+    for (int j = lig; j < nwc; j += grp) m = fmax(m, part[j][tl.b]);
+    for (int o = 16; o >= tl.Wb; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
+    return m;
+}
+
 // First assignment of an InitializedArray takes its stored edges on every face it lies on
 // (classes/InitializedArray.m:43-47 -> Edges.m:37-110).
 __device__ __forceinline__ void init_edges_cell(const Geom& g, const EdgeTable* et, int obj, int x, int y, int z,
@@ -213,13 +268,198 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
     }
 }
 
+// Mixed form with copy ghosts (single-CTA pencils, circ/const shifts): the predictor and corrector
+// stages store the flux numerators F beside the state they come from, so a stage is written before
+// the pencil's freezing speed c_f is known and the two pencil maxima share the stage barriers.
+// Readers form R = (u + F/c_f)/2 and L = (u - F/c_f)/2 (relaxingFluid.m:30-31, 52-56) at the rows
+// they need, with the reciprocal of c_f the flux stage itself would use.  Three barriers per sweep.
+template <bool MHD, int CPT>
+__device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, unsigned vblock) {
+    using T = float;
+    extern __shared__ __align__(16) unsigned char smem[];
+    if (a.tm->done || a.tm->error) return;
+    __shared__ T part[2][MAX_WARPS][33];
+    __shared__ double cflp[3][MAX_WARPS];
+    Tile<T, CPT> tl;
+    tl.init(a.sg, vblock);
+    const int d = a.sg.d;
+    const int NT = a.sg.NT;
+    const int N = tl.N;
+    const size_t AS = (size_t)tile_rows(tl.RC) * tl.Wb;
+    T* SA = reinterpret_cast<T*>(smem);   // u[v] at SA + v*AS, F[v] at SA + (5+v)*AS; later limited R, L
+    T* SB = SA + 10 * AS;                 // half-step state and its F
+    const int dn_src = tl.ridx(a.mode[CLS_MASS][0] == BC_CIRC ? N - 1 : 0);
+    const int up_src = tl.ridx(a.mode[CLS_MASS][1] == BC_CIRC ? 0 : N - 1);
+    // shared index of own row k shifted by n = -1 / +1 (copy ghosts at the pencil ends)
+    auto nix = [&](int k, int n) -> int {
+        const int r = tl.grow(k);
+        return n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs);
+    };
+    const double G = a.gamma;
+    const double dt = a.tm->dt;
+    const T ff = (T)(dt / a.dx);
+    const T half_ffx = (T)(0.5 * (dt / a.dx));
+
+    // ---- load u and cell-centred B; pressure, speed and F of the state -> set A ------------------
+    T u[5][CPT], bb[3][CPT];
+    double msq[CPT];
+    T lmax = T(0);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const bool ok = tl.ok(k);
+        const long long o = tl.off(k);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) u[v][k] = ok ? ldq<T>(a.q[v], o) : (v == 0 ? T(1) : T(0));
+        double m = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            bb[c][k] = (MHD && ok) ? ldq<T>(a.q[Q_CBX + c], o) : T(0);
+            if (MHD && a.use_b[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+        }
+        msq[k] = m;
+        T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+        T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+        T p;
+        const T spd = press_speed<T>(G, d, uu, m, p);
+        if (ok) lmax = fmax(lmax, spd);
+        T F[5];
+        flux_num(d, uu, b3, p, F);
+        const int ix = tl.idx(k);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            SA[v * AS + ix] = uu[v];
+            SA[(5 + v) * AS + ix] = F[v];
+        }
+    }
+    const T wv1 = colmax_publish(tl, part[0], lmax);
+    __syncthreads();
+    const T cf = colmax_collect(tl, NT, part[0], wv1);   // freezing speed (wFluidFlux.m:18-22)
+    const T ic = __frcp_rn(cf);
+
+    // ---- predictor (relaxingFluid.m:30-39); pressure, speed and F of the half-step state -> set B --
+    T lmax2 = T(0);
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+        T us[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const T* U = SA + v * AS;
+            const T* Fv = SA + (5 + v) * AS;
+            const T w = Fv[ix] * ic;
+            const T Rm = T(0.5) * (U[im] + Fv[im] * ic);
+            const T Lp = T(0.5) * (U[ip] - Fv[ip] * ic);
+            us[v] = u[v][k] - half_ffx * cf * (T(0.5) * (u[v][k] + w) - Rm + T(0.5) * (u[v][k] - w) - Lp);
+        }
+        us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
+        if (!tl.ok(k)) { us[0] = T(1); us[1] = us[2] = us[3] = us[4] = T(0); }
+        T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+        T p2;
+        const T spd = press_speed<T>(G, d, us, msq[k], p2);   // relaxingFluid.m:47-50
+        if (tl.ok(k)) lmax2 = fmax(lmax2, spd);
+        T F[5];
+        flux_num(d, us, b3, p2, F);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            SB[v * AS + ix] = us[v];
+            SB[(5 + v) * AS + ix] = F[v];
+        }
+        if (a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(a.sg.g, x, y, z)) {
+#pragma unroll 1
+                for (int v = 0; v < 5; ++v) {   // R and L of the state, formed again from set A
+                    const T w = SA[(5 + v) * AS + ix] * ic, uv = SA[v * AS + ix];
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_R), x, y, z, (double)(T(0.5) * (uv + w)));
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_L), x, y, z, (double)(T(0.5) * (uv - w)));
+                }
+            }
+        }
+    }
+    const T wv2 = colmax_publish(tl, part[1], lmax2);
+    __syncthreads();   // also orders the predictor's reads of set A before the limiter's writes
+    const T cfs = colmax_collect(tl, NT, part[1], wv2);   // freezing speed of the half step
+    const T ics = __frcp_rn(cfs);
+
+    // ---- corrector fluxes and TVD limiter (relaxingFluid.m:52-62): limited R and L -> set A -------
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const T* U = SB + v * AS;
+            const T* Fv = SB + (5 + v) * AS;
+            const T wm = Fv[im] * ics, w0 = Fv[ix] * ics, wp = Fv[ip] * ics;
+            const T um = U[im], u0 = U[ix], up = U[ip];
+            const T Rm = T(0.5) * (um + wm), r = T(0.5) * (u0 + w0), Rp = T(0.5) * (up + wp);
+            const T Lm = T(0.5) * (um - wm), l = T(0.5) * (u0 - w0), Lp = T(0.5) * (up - wp);
+            SA[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
+            SA[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
+        }
+        if (a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
+            int x, y, z;
+            tl.coords(k, x, y, z);
+            if (on_face(a.sg.g, x, y, z)) {
+#pragma unroll 1
+                for (int v = 0; v < 5; ++v) {   // corrector R and L, formed again from set B
+                    const T w = SB[(5 + v) * AS + ix] * ics, uv = SB[v * AS + ix];
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_R), x, y, z, (double)(T(0.5) * (uv + w)));
+                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_L), x, y, z, (double)(T(0.5) * (uv - w)));
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
+    double m3[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < CPT; ++k) {
+        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+        T unew[5];
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            const T* R = SA + v * AS;
+            const T* L = SA + (5 + v) * AS;
+            unew[v] = u[v][k] - ff * cfs * (R[ix] - R[im] + L[ix] - L[ip]);
+        }
+        unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
+        if (!tl.ok(k)) continue;
+        const long long o = tl.off(k);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) stq<T>(a.q[v], o, unew[v]);
+        if (a.cfl) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
+            double sp[3];
+            cfl_speeds(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3], (double)unew[4], msq[k],
+                       sp);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp[c]);
+        }
+    }
+    if (a.cfl) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            m3[c] = warp_max_nonneg(m3[c]);
+            if (lane == 0) cflp[c][warp] = m3[c];
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {   // one global atomic per CTA and direction
+            double m = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, cflp[threadIdx.x][w]);
+            atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
+        }
+    }
+}
+
 // One fluid sweep of one grid, run by CTA `vblock` of that grid's launch.
 // FADE: some BC of this sweep direction is fade (compiles the damping in).
 // CG (copy ghosts): single-CTA pencils whose three fluid classes share one circ or const mode per
 // side.  Those ghosts copy an own row (circ: the far end, const: the near end), so the reader of
 // row 0 or N-1 indexes that row directly: no halo jobs and no barrier after them.
 template <typename T, bool MHD, int CPT, bool FADE, bool CG>
-__device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
+__device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
     __shared__ T part[2][MAX_WARPS][33];   // per-warp column maxima (two freezing speeds; rows padded
@@ -438,6 +678,12 @@ __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vb
             atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
         }
     }
+}
+
+template <typename T, bool MHD, int CPT, bool FADE, bool CG>
+__device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
+    if constexpr (CG && sizeof(T) == 4) fluid_sweep_body_mixed_cg<MHD, CPT>(a, vblock);
+    else fluid_sweep_body_general<T, MHD, CPT, FADE, CG>(a, vblock);
 }
 
 template <typename T, bool MHD, int CPT, bool FADE, bool CG>
