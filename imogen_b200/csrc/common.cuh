@@ -215,6 +215,20 @@ __device__ __forceinline__ PressOut pressure_totsnd(double G, double rho, double
 // Mixed form of 'totsnd' for FP32 state: the pressure recovery P0 = (G-1)(E - rho v^2/2) and the
 // magnetic terms are evaluated in FP64 (the reciprocal of rho is an FP32 estimate refined by one
 // FP64 Newton step, exact to ~1e-15), the sound speed is taken in FP32.
+// Hardware approximations for the FP32 arithmetic of the mixed form: the reciprocal within 1 ulp and
+// the square root within 2^-23 relative (PTX rcp.approx.f32 / sqrt.approx.f32), one instruction
+// each instead of the correctly rounded sequences.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 struct PressOutF {
     float p;
     float cs;
@@ -222,13 +236,13 @@ struct PressOutF {
 __device__ __forceinline__ PressOutF pressure_totsnd_mixed(double G, float rho, float px, float py, float pz, float E,
                                                           double msq) {
     double r = rho;
-    double inv = (double)__frcp_rn(rho);
+    double inv = (double)rcp_approx(rho);   // FP32 seed, one FP64 Newton step
     inv = inv * (2.0 - r * inv);
     double psq = (double)px * px + (double)py * py + (double)pz * pz;
     double p0 = (G - 1.0) * ((double)E - 0.5 * psq * inv);
     double pg = p0 - (G - 1.0) * 0.5 * msq;
     PressOutF o;
-    o.cs = sqrtf((float)fabs((G * pg + 2.0 * msq) * inv));
+    o.cs = sqrt_approx((float)fabs((G * pg + 2.0 * msq) * inv));
     double pt = p0 + 0.5 * (2.0 - G) * msq;
     o.p = pt < 0 ? 0.f : (float)pt;
     return o;

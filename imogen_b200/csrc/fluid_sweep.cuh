@@ -59,7 +59,7 @@ __device__ __forceinline__ int fluid_class(int v) { return v == 0 ? CLS_MASS : (
 __device__ __forceinline__ void flux_num(int d, const float u[5], const float bb[3], float press, float F[5]) {
     const float pX = sel3(d, u[1], u[2], u[3]);
     const float bX = sel3(d, bb[0], bb[1], bb[2]);
-    const float ir = __frcp_rn(u[0]);
+    const float ir = rcp_approx(u[0]);
     const float velocity = pX * ir;
     F[0] = pX;
     F[4] = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
@@ -97,7 +97,7 @@ __device__ __forceinline__ T press_speed(double G, int d, const T u[5], double m
     if constexpr (sizeof(T) == 4) {
         PressOutF o = pressure_totsnd_mixed(G, u[0], u[1], u[2], u[3], u[4], msq);
         p = o.p;
-        return fabsf(pX * __frcp_rn(u[0])) + o.cs;
+        return fabsf(pX * rcp_approx(u[0])) + o.cs;
     } else {
         PressOut o = pressure_totsnd(G, u[0], u[1], u[2], u[3], u[4], msq);
         p = o.p + 0.0;   // + viscosity.solve ('empty' -> 0)

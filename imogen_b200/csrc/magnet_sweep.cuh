@@ -249,7 +249,8 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
                     pm = pX[o];
                     rm = rho[o];
                 }
-                vgr[q][k] = (pm + pX[o]) / (rm + rho[o]);
+                if constexpr (sizeof(T) == 4) vgr[q][k] = (pm + pX[o]) * rcp_approx(rm + rho[o]);
+                else vgr[q][k] = (pm + pX[o]) / (rm + rho[o]);
                 bI[q][k] = c.BI[o];
                 if (c.init_mag && on_face(g, x, y, z))
                     init_edges_cell(g, et, mag_obj(c.e, d, MO_VELGRID), x, y, z, (double)vgr[q][k]);
