@@ -39,11 +39,14 @@ struct FluidArgs {
 
 constexpr int FLUID_NARR = 20;
 constexpr int MAX_WARPS = 16;
+constexpr int MIXED_CELL_WORDS = 11;   // mixed copy-ghost kernel: words per cell of a shared set
 
-// Dynamic shared memory of the fluid kernel: 20 halo'd arrays + fade anchors of 10 arrays x 2 sides.
+// Dynamic shared memory of the fluid kernel: 20 halo'd arrays + fade anchors of 10 arrays x 2 sides
+// (FP32: room for the mixed copy-ghost kernel's two cell-major sets of 11 words per cell).
 template <typename T>
 __host__ __device__ inline size_t fluid_smem_bytes(int RC, int Wb) {
-    return sizeof(T) * (size_t)FLUID_NARR * tile_rows(RC) * Wb + sizeof(Ghost<T>) * 10 * 2 * (size_t)Wb;
+    const int words = sizeof(T) == 4 ? 2 * MIXED_CELL_WORDS : FLUID_NARR;
+    return sizeof(T) * (size_t)words * tile_rows(RC) * Wb + sizeof(Ghost<T>) * 10 * 2 * (size_t)Wb;
 }
 
 template <typename T>
@@ -285,9 +288,13 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     const int d = a.sg.d;
     const int NT = a.sg.NT;
     const int N = tl.N;
+    // cell-major shared layout: cell i holds u[0..4] at S + i*CS and F[0..4] at S + i*CS + 5 (later the
+    // limited R and L); a stride of 11 words keeps consecutive cells on distinct banks, and every
+    // access is an immediate offset from one address per cell
+    constexpr int CS = MIXED_CELL_WORDS;
     const size_t AS = (size_t)tile_rows(tl.RC) * tl.Wb;
-    T* SA = reinterpret_cast<T*>(smem);   // u[v] at SA + v*AS, F[v] at SA + (5+v)*AS; later limited R, L
-    T* SB = SA + 10 * AS;                 // half-step state and its F
+    T* SA = reinterpret_cast<T*>(smem);   // the state and its F; later the limited R, L
+    T* SB = SA + CS * AS;                 // half-step state and its F
     const int dn_src = tl.ridx(a.mode[CLS_MASS][0] == BC_CIRC ? N - 1 : 0);
     const int up_src = tl.ridx(a.mode[CLS_MASS][1] == BC_CIRC ? 0 : N - 1);
     // shared index of own row k shifted by n = -1 / +1 (copy ghosts at the pencil ends)
@@ -324,11 +331,11 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
         if (ok) lmax = fmax(lmax, spd);
         T F[5];
         flux_num(d, uu, b3, p, F);
-        const int ix = tl.idx(k);
+        T* c0 = SA + tl.idx(k) * CS;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            SA[v * AS + ix] = uu[v];
-            SA[(5 + v) * AS + ix] = F[v];
+            c0[v] = uu[v];
+            c0[5 + v] = F[v];
         }
     }
     const T wv1 = colmax_publish(tl, part[0], lmax);
@@ -340,15 +347,16 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     T lmax2 = T(0);
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+        const int ix = tl.idx(k);
+        const T* cm = SA + nix(k, -1) * CS;
+        const T* c0 = SA + ix * CS;
+        const T* cp = SA + nix(k, +1) * CS;
         T us[5];
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            const T* U = SA + v * AS;
-            const T* Fv = SA + (5 + v) * AS;
-            const T w = Fv[ix] * ic;
-            const T Rm = T(0.5) * (U[im] + Fv[im] * ic);
-            const T Lp = T(0.5) * (U[ip] - Fv[ip] * ic);
+            const T w = c0[5 + v] * ic;
+            const T Rm = T(0.5) * (cm[v] + cm[5 + v] * ic);
+            const T Lp = T(0.5) * (cp[v] - cp[5 + v] * ic);
             us[v] = u[v][k] - half_ffx * cf * (T(0.5) * (u[v][k] + w) - Rm + T(0.5) * (u[v][k] - w) - Lp);
         }
         us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
@@ -359,10 +367,11 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
         if (tl.ok(k)) lmax2 = fmax(lmax2, spd);
         T F[5];
         flux_num(d, us, b3, p2, F);
+        T* b0 = SB + ix * CS;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            SB[v * AS + ix] = us[v];
-            SB[(5 + v) * AS + ix] = F[v];
+            b0[v] = us[v];
+            b0[5 + v] = F[v];
         }
         if (a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
             int x, y, z;
@@ -370,7 +379,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             if (on_face(a.sg.g, x, y, z)) {
 #pragma unroll 1
                 for (int v = 0; v < 5; ++v) {   // R and L of the state, formed again from set A
-                    const T w = SA[(5 + v) * AS + ix] * ic, uv = SA[v * AS + ix];
+                    const T w = c0[5 + v] * ic, uv = c0[v];
                     init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_R), x, y, z, (double)(T(0.5) * (uv + w)));
                     init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_L), x, y, z, (double)(T(0.5) * (uv - w)));
                 }
@@ -385,17 +394,19 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     // ---- corrector fluxes and TVD limiter (relaxingFluid.m:52-62): limited R and L -> set A -------
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+        const int ix = tl.idx(k);
+        const T* bm = SB + nix(k, -1) * CS;
+        const T* b0 = SB + ix * CS;
+        const T* bp = SB + nix(k, +1) * CS;
+        T* a0 = SA + ix * CS;
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
-            const T* U = SB + v * AS;
-            const T* Fv = SB + (5 + v) * AS;
-            const T wm = Fv[im] * ics, w0 = Fv[ix] * ics, wp = Fv[ip] * ics;
-            const T um = U[im], u0 = U[ix], up = U[ip];
+            const T wm = bm[5 + v] * ics, w0 = b0[5 + v] * ics, wp = bp[5 + v] * ics;
+            const T um = bm[v], u0 = b0[v], up = bp[v];
             const T Rm = T(0.5) * (um + wm), r = T(0.5) * (u0 + w0), Rp = T(0.5) * (up + wp);
             const T Lm = T(0.5) * (um - wm), l = T(0.5) * (u0 - w0), Lp = T(0.5) * (up - wp);
-            SA[v * AS + ix] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
-            SA[(5 + v) * AS + ix] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
+            a0[v] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
+            a0[5 + v] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
         }
         if (a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
             int x, y, z;
@@ -403,7 +414,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             if (on_face(a.sg.g, x, y, z)) {
 #pragma unroll 1
                 for (int v = 0; v < 5; ++v) {   // corrector R and L, formed again from set B
-                    const T w = SB[(5 + v) * AS + ix] * ics, uv = SB[v * AS + ix];
+                    const T w = b0[5 + v] * ics, uv = b0[v];
                     init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_R), x, y, z, (double)(T(0.5) * (uv + w)));
                     init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_L), x, y, z, (double)(T(0.5) * (uv - w)));
                 }
@@ -416,14 +427,12 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     double m3[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
-        const int ix = tl.idx(k), im = nix(k, -1), ip = nix(k, +1);
+        const T* am = SA + nix(k, -1) * CS;
+        const T* a0 = SA + tl.idx(k) * CS;
+        const T* ap = SA + nix(k, +1) * CS;
         T unew[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) {
-            const T* R = SA + v * AS;
-            const T* L = SA + (5 + v) * AS;
-            unew[v] = u[v][k] - ff * cfs * (R[ix] - R[im] + L[ix] - L[ip]);
-        }
+        for (int v = 0; v < 5; ++v) unew[v] = u[v][k] - ff * cfs * (a0[v] - am[v] + a0[5 + v] - ap[5 + v]);
         unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
