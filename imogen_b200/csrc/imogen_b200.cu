@@ -367,6 +367,9 @@ SweepGeom sweep_geom(const img_ctx* ctx, int d, const PencilCfg& pcf) {
     s.sd = ctx->g.s[d];
     s.s1 = ctx->g.s[s.d1];
     s.s2 = ctx->g.s[s.d2];
+    s.div_lanes = make_fastdiv((unsigned)(d == 0 ? s.G : s.Wb));
+    s.div_cl = make_fastdiv((unsigned)s.CL);
+    s.div_n1 = make_fastdiv((unsigned)s.n1);
     return s;
 }
 

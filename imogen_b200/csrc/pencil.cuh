@@ -17,6 +17,25 @@
 
 namespace img {
 
+// Division by a launch-invariant divisor D >= 1 for dividends n < 2^31 by one 64-bit multiply and a
+// shift (Granlund and Montgomery, "Division by invariant integers using multiplication", 1994,
+// round-up method): with l = ceil(log2 D), s = 31 + l and M = floor(2^s / D) + 1, M*D lies in
+// (2^s, 2^s + 2^l], so floor(n / D) = floor(n * M / 2^s) for every n < 2^31.
+struct FastDiv {
+    unsigned long long mul;
+    int shift;
+    __host__ __device__ unsigned div(unsigned n) const { return (unsigned)(((unsigned long long)n * mul) >> shift); }
+};
+
+inline FastDiv make_fastdiv(unsigned D) {
+    int l = 0;
+    while ((1ull << l) < D) ++l;
+    FastDiv f;
+    f.shift = 31 + l;
+    f.mul = (1ull << f.shift) / D + 1;
+    return f;
+}
+
 // Geometry of one directional sweep (host-filled; kernels read it from their grid-constant
 // parameter, so the uniform values cost no registers).
 struct SweepGeom {
@@ -33,6 +52,9 @@ struct SweepGeom {
     int rank_hi;      // cluster rank holding row N-1 = (N-1) / RC
     int n1;           // g.n[d1]
     long long sd, s1, s2;   // strides along d, d1, d2
+    FastDiv div_lanes;      // by G (d == 0: threads of a pencil are consecutive) or Wb (d >= 1)
+    FastDiv div_cl;         // by CL
+    FastDiv div_n1;         // by n1
 };
 
 constexpr int HALO_LO = 1;   // halo rows below the CTA's rows
@@ -77,18 +99,19 @@ struct Tile {
         RC = s.RC;
         rank_hi = s.rank_hi;
         sd = s.sd;
-        if (s.d == 0) { g = t % s.G; b = t / s.G; }
-        else { b = t % s.Wb; g = t / s.Wb; }
+        const unsigned tq = s.div_lanes.div((unsigned)t);   // t / G (x) or t / Wb (y, z)
+        if (s.d == 0) { b = (int)tq; g = t - b * s.G; }
+        else { g = (int)tq; b = t - g * s.Wb; }
         rs = s.d == 0 ? 1 : s.Wb;
         cs = s.d == 0 ? tile_rows(s.RC) : 1;
         rank = (int)(vblock & (unsigned)(s.CL - 1));   // CL is a power of two
-        const unsigned bundle = vblock / (unsigned)s.CL;
+        const unsigned bundle = s.div_cl.div(vblock);
         row0 = rank * s.RC + g;
         ix0 = (g + HALO_LO) * rs + b * cs;
         col = (int)(bundle * (unsigned)s.Wb + (unsigned)b);
         colok = col < s.ncol;
         const unsigned c = colok ? (unsigned)col : 0u;
-        c2 = (int)(c / (unsigned)s.n1);
+        c2 = (int)s.div_n1.div(c);
         c1 = (int)(c - (unsigned)c2 * (unsigned)s.n1);
         base = c1 * s.s1 + (long long)c2 * s.s2;
     }
