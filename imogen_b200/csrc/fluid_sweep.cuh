@@ -373,18 +373,6 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             b0[v] = us[v];
             b0[5 + v] = F[v];
         }
-        if (a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            if (on_face(a.sg.g, x, y, z)) {
-#pragma unroll 1
-                for (int v = 0; v < 5; ++v) {   // R and L of the state, formed again from set A
-                    const T w = c0[5 + v] * ic, uv = c0[v];
-                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_R), x, y, z, (double)(T(0.5) * (uv + w)));
-                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_STORE_L), x, y, z, (double)(T(0.5) * (uv - w)));
-                }
-            }
-        }
     }
     const T wv2 = colmax_publish(tl, part[1], lmax2);
     __syncthreads();   // also orders the predictor's reads of set A before the limiter's writes
@@ -407,18 +395,6 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             const T Lm = T(0.5) * (um - wm), l = T(0.5) * (u0 - w0), Lp = T(0.5) * (up - wp);
             a0[v] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
             a0[5 + v] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
-        }
-        if (a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
-            int x, y, z;
-            tl.coords(k, x, y, z);
-            if (on_face(a.sg.g, x, y, z)) {
-#pragma unroll 1
-                for (int v = 0; v < 5; ++v) {   // corrector R and L, formed again from set B
-                    const T w = b0[5 + v] * ics, uv = b0[v];
-                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_R), x, y, z, (double)(T(0.5) * (uv + w)));
-                    init_edges_cell(a.sg.g, a.edges, fluid_obj(v, FO_L), x, y, z, (double)(T(0.5) * (uv - w)));
-                }
-            }
         }
     }
     __syncthreads();
@@ -467,7 +443,8 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
 // CG (copy ghosts): single-CTA pencils whose three fluid classes share one circ or const mode per
 // side.  Those ghosts copy an own row (circ: the far end, const: the near end), so the reader of
 // row 0 or N-1 indexes that row directly: no halo jobs and no barrier after them.
-template <typename T, bool MHD, int CPT, bool FADE, bool CG>
+// INIT: this launch may capture stored edges of first-assigned objects (compiled out otherwise).
+template <typename T, bool MHD, int CPT, bool FADE, bool CG, bool INIT>
 __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
@@ -540,7 +517,7 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
             SA[v * AS + ix] = T(0.5) * (uu[v] + w[v]);
             SA[(5 + v) * AS + ix] = T(0.5) * (uu[v] - w[v]);
         }
-        if (a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
+        if (INIT && a.init_store && tl.ok(k)) {   // first assignment of store.fluxR/L (InitializedArray.m:43-47)
             int x, y, z;
             tl.coords(k, x, y, z);
             if (on_face(a.sg.g, x, y, z)) {
@@ -597,7 +574,7 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
             SA[v * AS + ix] = T(0.5) * (uu[v] + w[v]);
             SA[(5 + v) * AS + ix] = T(0.5) * (uu[v] - w[v]);
         }
-        if (a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
+        if (INIT && a.init_flux && tl.ok(k)) {   // first assignment of fluxR/L
             int x, y, z;
             tl.coords(k, x, y, z);
             if (on_face(a.sg.g, x, y, z)) {
@@ -689,26 +666,32 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
     }
 }
 
-template <typename T, bool MHD, int CPT, bool FADE, bool CG>
+// Kernel variant V: 0 halo jobs, 1 halo jobs with fade, 2 copy ghosts, 3 and 4 as 0 and 1 with the
+// capture of stored edges (a run's first sweeps).
+template <int V> constexpr bool kv_fade = V == 1 || V == 4;
+template <int V> constexpr bool kv_cg = V == 2;
+template <int V> constexpr bool kv_init = V >= 3;
+
+template <typename T, bool MHD, int CPT, int V>
 __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
-    if constexpr (CG && sizeof(T) == 4) fluid_sweep_body_mixed_cg<MHD, CPT>(a, vblock);
-    else fluid_sweep_body_general<T, MHD, CPT, FADE, CG>(a, vblock);
+    if constexpr (kv_cg<V> && sizeof(T) == 4) fluid_sweep_body_mixed_cg<MHD, CPT>(a, vblock);
+    else fluid_sweep_body_general<T, MHD, CPT, kv_fade<V>, kv_cg<V>, kv_init<V>>(a, vblock);
 }
 
-template <typename T, bool MHD, int CPT, bool FADE, bool CG>
+template <typename T, bool MHD, int CPT, int V>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_kernel(const __grid_constant__ FluidArgs a) {
-    fluid_sweep_body<T, MHD, CPT, FADE, CG>(a, blockIdx.x);
+    fluid_sweep_body<T, MHD, CPT, V>(a, blockIdx.x);
 }
 
 // The same sweep over many grids in one launch (BlockMap per CTA, arguments per member).
-template <typename T, bool MHD, int CPT, bool FADE, bool CG>
+template <typename T, bool MHD, int CPT, int V>
 __global__ void __launch_bounds__(512, CPT == 1 ? 2 : 1) fluid_sweep_batch_kernel(const FluidArgs* __restrict__ args,
                                                                                   const BlockMap* __restrict__ map) {
     __shared__ FluidArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    fluid_sweep_body<T, MHD, CPT, FADE, CG>(sa, (unsigned)bm.block);
+    fluid_sweep_body<T, MHD, CPT, V>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

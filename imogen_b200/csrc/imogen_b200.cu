@@ -432,6 +432,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
             const int m = a.mode[k][side];
             if ((m != IMG_BC_CIRC && m != IMG_BC_CONST) || m != a.mode[CLS_MASS][side]) L.cg = false;
         }
+    L.init = a.init_store || a.init_flux;   // first sweeps: the stored-edge capturing kernel
     if (ctx->rec) {
         OpRec r{};
         r.kind = OP_FLUID;
@@ -507,6 +508,7 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     // copy ghosts: single-CTA pencils with circ or const mag-class shifts along X
     L.cg = Lc.cg = pcf.CL == 1 && (a.modeX[0] == IMG_BC_CIRC || a.modeX[0] == IMG_BC_CONST) &&
                    (a.modeX[1] == IMG_BC_CIRC || a.modeX[1] == IMG_BC_CONST);
+    L.init = a.init_mag[0] || a.init_mag[1];   // first sweep of (I, X): the stored-edge capturing chain
     if (ctx->rec) {
         OpRec r{};
         r.elem = sizeof(T);
@@ -1356,7 +1358,7 @@ size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
 
 bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
     return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
-           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg;
+           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg && x.init == y.init;
 }
 
 // Turn the members' records into batched launch items and the arena image.

@@ -167,7 +167,9 @@ struct ChainComp {
 // FADE: a mag-class BC along X is fade (compiles the damping in).  CG (copy ghosts): single-CTA
 // pencils with circ or const mag-class shifts along X; the reader of a row next to a pencil end
 // indexes the row its ghost copies, so no stage needs halo jobs or the barrier after them.
-template <typename T, int CPT, bool FADE, int NQC, bool CG>
+// INIT: this launch may capture stored edges of first-assigned objects (compiled out otherwise; the
+// host never combines it with CG).
+template <typename T, int CPT, bool FADE, int NQC, bool CG, bool INIT>
 __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     if (a.tm->done || a.tm->error) return;
@@ -252,7 +254,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
                 if constexpr (sizeof(T) == 4) vgr[q][k] = (pm + pX[o]) * rcp_approx(rm + rho[o]);
                 else vgr[q][k] = (pm + pX[o]) / (rm + rho[o]);
                 bI[q][k] = c.BI[o];
-                if (c.init_mag && on_face(g, x, y, z))
+                if (INIT && c.init_mag && on_face(g, x, y, z))
                     init_edges_cell(g, et, mag_obj(c.e, d, MO_VELGRID), x, y, z, (double)vgr[q][k]);
             }
             S(q, 0)[tl.idx(k)] = vgr[q][k];
@@ -291,7 +293,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             vf[q][k] = (vg[q][k] + p1) < T(0) ? T(1) : T(0);
             const T F = bI[q][k] * vg[q][k];
             S(q, 2)[tl.idx(k)] = F;
-            if (cp[q].init_mag && tl.ok(k)) {
+            if (INIT && cp[q].init_mag && tl.ok(k)) {
                 int x, y, z;
                 tl.coords(k, x, y, z);
                 if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_STORE_R), x, y, z, (double)F);
@@ -328,7 +330,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             const T st = bI[q][k] - ff * (Fu - sh((const T*)S(q, 3), GS(q), k, -1, mlo));
             W[q][k] = st * vg[q][k];
             S(q, 0)[tl.idx(k)] = W[q][k];
-            if (cp[q].init_mag && tl.ok(k)) {
+            if (INIT && cp[q].init_mag && tl.ok(k)) {
                 int x, y, z;
                 tl.coords(k, x, y, z);
                 if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_WMAG), x, y, z, (double)W[q][k]);
@@ -397,7 +399,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             const T dFluxL = w - (v * p1d + (T(1) - v) * m1);
             Fl[q][k] = fx + limiter_corr<T>(a.limiter, dFluxL, dFluxR);
             S(q, 1)[ix] = Fl[q][k];
-            if (cp[q].init_mag && tl.ok(k)) {
+            if (INIT && cp[q].init_mag && tl.ok(k)) {
                 int x, y, z;
                 tl.coords(k, x, y, z);
                 if (on_face(g, x, y, z)) init_edges_cell(g, et, mag_obj(cp[q].e, d, MO_FLUX), x, y, z, (double)fx);
@@ -572,9 +574,9 @@ __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, 
     y = (int)(r - (unsigned)z * n1);
 }
 
-template <typename T, int CPT, bool FADE, int NQC, bool CG>
+template <typename T, int CPT, int NQC, int V>
 __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_kernel(const __grid_constant__ MagArgs a) {
-    mag_chain_body<T, CPT, FADE, NQC, CG>(a, blockIdx.x);
+    mag_chain_body<T, CPT, kv_fade<V>, NQC, kv_cg<V>, kv_init<V>>(a, blockIdx.x);
 }
 
 template <typename T, int CPT, bool FADE, bool CG>
@@ -583,14 +585,14 @@ __global__ void __launch_bounds__(512, 2) mag_ctcell_kernel(const __grid_constan
 }
 
 // The same passes over many grids in one launch (BlockMap per CTA, arguments per member).
-template <typename T, int CPT, bool FADE, int NQC, bool CG>
+template <typename T, int CPT, int NQC, int V>
 __global__ void __launch_bounds__(512, CPT == 1 && NQC == 1 ? 2 : 1) mag_chain_batch_kernel(const MagArgs* __restrict__ args,
                                                                                 const BlockMap* __restrict__ map) {
     __shared__ MagArgs sa;
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    mag_chain_body<T, CPT, FADE, NQC, CG>(sa, (unsigned)bm.block);
+    mag_chain_body<T, CPT, kv_fade<V>, NQC, kv_cg<V>, kv_init<V>>(sa, (unsigned)bm.block);
 }
 
 template <typename T, int CPT, bool FADE, bool CG>

@@ -46,76 +46,116 @@ cudaError_t launch_pencil(void (*kern)(const Args), const Args& a, const PencilL
     return cudaLaunchKernelEx(&lc, kern, a);
 }
 
-template <typename T, bool MHD, bool FADE, bool CG>
-void (*fluid_kernel(int cpt))(const FluidArgs) {
+// Kernel variant of a pencil launch (see kv_fade/kv_cg/kv_init): halo jobs (0), with fade (1), copy
+// ghosts (2), and the stored-edge capturing forms of 0 and 1 (3, 4), which first sweeps use.
+inline int kernel_variant(bool fade, bool cg, bool init) {
+    if (init) return fade ? 4 : 3;
+    return fade ? 1 : (cg ? 2 : 0);
+}
+
+template <typename T, bool MHD, int V>
+void (*fluid_kernel_v(int cpt))(const FluidArgs) {
     switch (cpt) {
-        case 1: return fluid_sweep_kernel<T, MHD, 1, FADE, CG>;
-        case 2: return fluid_sweep_kernel<T, MHD, 2, FADE, CG>;
-        default: return fluid_sweep_kernel<T, MHD, 4, FADE, CG>;
+        case 1: return fluid_sweep_kernel<T, MHD, 1, V>;
+        case 2: return fluid_sweep_kernel<T, MHD, 2, V>;
+        default: return fluid_sweep_kernel<T, MHD, 4, V>;
     }
 }
 
-template <typename T, bool FADE, bool CG>
-void (*chain_kernel(int cpt, int nqc))(const MagArgs) {
-    if (nqc == 2) return cpt == 1 ? mag_chain_kernel<T, 1, FADE, 2, CG> : mag_chain_kernel<T, 2, FADE, 2, CG>;
+template <typename T, bool MHD, int V>
+void (*fluid_batch_kernel_v(int cpt))(const FluidArgs*, const BlockMap*) {
     switch (cpt) {
-        case 1: return mag_chain_kernel<T, 1, FADE, 1, CG>;
-        case 2: return mag_chain_kernel<T, 2, FADE, 1, CG>;
-        default: return mag_chain_kernel<T, 4, FADE, 1, CG>;
+        case 1: return fluid_sweep_batch_kernel<T, MHD, 1, V>;
+        case 2: return fluid_sweep_batch_kernel<T, MHD, 2, V>;
+        default: return fluid_sweep_batch_kernel<T, MHD, 4, V>;
     }
 }
 
-// Ghost variant: 0 halo jobs, 1 halo jobs with fade damping, 2 copy ghosts.
-inline int ghost_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
+template <typename T, int V>
+void (*chain_kernel_v(int cpt, int nqc))(const MagArgs) {
+    if (nqc == 2) return cpt == 1 ? mag_chain_kernel<T, 1, 2, V> : mag_chain_kernel<T, 2, 2, V>;
+    switch (cpt) {
+        case 1: return mag_chain_kernel<T, 1, 1, V>;
+        case 2: return mag_chain_kernel<T, 2, 1, V>;
+        default: return mag_chain_kernel<T, 4, 1, V>;
+    }
+}
+
+template <typename T, int V>
+void (*chain_batch_kernel_v(int cpt, int nqc))(const MagArgs*, const BlockMap*) {
+    if (nqc == 2) return cpt == 1 ? mag_chain_batch_kernel<T, 1, 2, V> : mag_chain_batch_kernel<T, 2, 2, V>;
+    switch (cpt) {
+        case 1: return mag_chain_batch_kernel<T, 1, 1, V>;
+        case 2: return mag_chain_batch_kernel<T, 2, 1, V>;
+        default: return mag_chain_batch_kernel<T, 4, 1, V>;
+    }
+}
+
+template <typename T, bool MHD>
+void (*fluid_kernel_m(int cpt, int v))(const FluidArgs) {
+    switch (v) {
+        case 1: return fluid_kernel_v<T, MHD, 1>(cpt);
+        case 2: return fluid_kernel_v<T, MHD, 2>(cpt);
+        case 3: return fluid_kernel_v<T, MHD, 3>(cpt);
+        case 4: return fluid_kernel_v<T, MHD, 4>(cpt);
+        default: return fluid_kernel_v<T, MHD, 0>(cpt);
+    }
+}
+
+template <typename T, bool MHD>
+void (*fluid_batch_kernel_m(int cpt, int v))(const FluidArgs*, const BlockMap*) {
+    switch (v) {
+        case 1: return fluid_batch_kernel_v<T, MHD, 1>(cpt);
+        case 2: return fluid_batch_kernel_v<T, MHD, 2>(cpt);
+        case 3: return fluid_batch_kernel_v<T, MHD, 3>(cpt);
+        case 4: return fluid_batch_kernel_v<T, MHD, 4>(cpt);
+        default: return fluid_batch_kernel_v<T, MHD, 0>(cpt);
+    }
+}
 
 template <typename T>
-void (*chain_kernel(int cpt, int nqc, int gv))(const MagArgs) {
-    return gv == 1 ? chain_kernel<T, true, false>(cpt, nqc)
-                   : (gv == 2 ? chain_kernel<T, false, true>(cpt, nqc) : chain_kernel<T, false, false>(cpt, nqc));
+void (*fluid_kernel(int cpt, bool mhd, int v))(const FluidArgs) {
+    return mhd ? fluid_kernel_m<T, true>(cpt, v) : fluid_kernel_m<T, false>(cpt, v);
 }
 
-template <typename T, bool MHD, bool FADE, bool CG>
-void (*fluid_batch_kernel(int cpt))(const FluidArgs*, const BlockMap*) {
-    switch (cpt) {
-        case 1: return fluid_sweep_batch_kernel<T, MHD, 1, FADE, CG>;
-        case 2: return fluid_sweep_batch_kernel<T, MHD, 2, FADE, CG>;
-        default: return fluid_sweep_batch_kernel<T, MHD, 4, FADE, CG>;
-    }
+template <typename T>
+void (*fluid_batch_kernel(int cpt, bool mhd, int v))(const FluidArgs*, const BlockMap*) {
+    return mhd ? fluid_batch_kernel_m<T, true>(cpt, v) : fluid_batch_kernel_m<T, false>(cpt, v);
 }
 
-template <typename T, bool FADE, bool CG>
-void (*chain_batch_kernel(int cpt, int nqc))(const MagArgs*, const BlockMap*) {
-    if (nqc == 2) return cpt == 1 ? mag_chain_batch_kernel<T, 1, FADE, 2, CG> : mag_chain_batch_kernel<T, 2, FADE, 2, CG>;
-    switch (cpt) {
-        case 1: return mag_chain_batch_kernel<T, 1, FADE, 1, CG>;
-        case 2: return mag_chain_batch_kernel<T, 2, FADE, 1, CG>;
-        default: return mag_chain_batch_kernel<T, 4, FADE, 1, CG>;
+template <typename T>
+void (*chain_kernel(int cpt, int nqc, int v))(const MagArgs) {
+    switch (v) {
+        case 1: return chain_kernel_v<T, 1>(cpt, nqc);
+        case 2: return chain_kernel_v<T, 2>(cpt, nqc);
+        case 3: return chain_kernel_v<T, 3>(cpt, nqc);
+        case 4: return chain_kernel_v<T, 4>(cpt, nqc);
+        default: return chain_kernel_v<T, 0>(cpt, nqc);
     }
 }
 
 template <typename T>
-void (*chain_batch_kernel(int cpt, int nqc, int gv))(const MagArgs*, const BlockMap*) {
-    return gv == 1 ? chain_batch_kernel<T, true, false>(cpt, nqc)
-                   : (gv == 2 ? chain_batch_kernel<T, false, true>(cpt, nqc) : chain_batch_kernel<T, false, false>(cpt, nqc));
+void (*chain_batch_kernel(int cpt, int nqc, int v))(const MagArgs*, const BlockMap*) {
+    switch (v) {
+        case 1: return chain_batch_kernel_v<T, 1>(cpt, nqc);
+        case 2: return chain_batch_kernel_v<T, 2>(cpt, nqc);
+        case 3: return chain_batch_kernel_v<T, 3>(cpt, nqc);
+        case 4: return chain_batch_kernel_v<T, 4>(cpt, nqc);
+        default: return chain_batch_kernel_v<T, 0>(cpt, nqc);
+    }
 }
 
-template <typename T>
-void (*fluid_batch_kernel(int cpt, bool mhd, int gv))(const FluidArgs*, const BlockMap*) {
-    if (mhd)
-        return gv == 1 ? fluid_batch_kernel<T, true, true, false>(cpt)
-                       : (gv == 2 ? fluid_batch_kernel<T, true, false, true>(cpt) : fluid_batch_kernel<T, true, false, false>(cpt));
-    return gv == 1 ? fluid_batch_kernel<T, false, true, false>(cpt)
-                   : (gv == 2 ? fluid_batch_kernel<T, false, false, true>(cpt) : fluid_batch_kernel<T, false, false, false>(cpt));
-}
+// The CT kernel captures no stored edges: its variant ignores `init`.
+inline int ct_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
 
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
-    return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, ghost_variant(L.fade, L.cg)), args, map, L);
+    return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
-    return launch_pencil_batch(chain_batch_kernel<T>(L.cpt, L.nqc, ghost_variant(L.fade, L.cg)), args, map, L);
+    return launch_pencil_batch(chain_batch_kernel<T>(L.cpt, L.nqc, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 
 template <typename T, bool FADE, bool CG>
@@ -150,31 +190,22 @@ void (*ctcell_batch_kernel(int cpt, int gv))(const MagArgs*, const BlockMap*) {
 
 template <typename T>
 cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
-    return launch_pencil_batch(ctcell_batch_kernel<T>(L.cpt, ghost_variant(L.fade, L.cg)), args, map, L);
-}
-
-template <typename T>
-void (*fluid_kernel(int cpt, bool mhd, int gv))(const FluidArgs) {
-    if (mhd)
-        return gv == 1 ? fluid_kernel<T, true, true, false>(cpt)
-                       : (gv == 2 ? fluid_kernel<T, true, false, true>(cpt) : fluid_kernel<T, true, false, false>(cpt));
-    return gv == 1 ? fluid_kernel<T, false, true, false>(cpt)
-                   : (gv == 2 ? fluid_kernel<T, false, false, true>(cpt) : fluid_kernel<T, false, false, false>(cpt));
+    return launch_pencil_batch(ctcell_batch_kernel<T>(L.cpt, ct_variant(L.fade, L.cg)), args, map, L);
 }
 
 template <typename T>
 cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd) {
-    return launch_pencil(fluid_kernel<T>(L.cpt, mhd, ghost_variant(L.fade, L.cg)), a, L);
+    return launch_pencil(fluid_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L) {
-    return launch_pencil(chain_kernel<T>(L.cpt, L.nqc, ghost_variant(L.fade, L.cg)), a, L);
+    return launch_pencil(chain_kernel<T>(L.cpt, L.nqc, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_ctcell(const MagArgs& a, const PencilLaunch& L) {
-    return launch_pencil(ctcell_kernel<T>(L.cpt, ghost_variant(L.fade, L.cg)), a, L);
+    return launch_pencil(ctcell_kernel<T>(L.cpt, ct_variant(L.fade, L.cg)), a, L);
 }
 
 // Allow a kernel the device's whole opt-in shared memory per block (minus its static shared
@@ -190,7 +221,7 @@ cudaError_t allow_max_smem(K kern, int optin) {
 
 template <typename T>
 cudaError_t fluid_attributes(int cpt, int optin) {
-    for (int v = 0; v < 6; ++v) {
+    for (int v = 0; v < 10; ++v) {
         cudaError_t e = allow_max_smem(fluid_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e == cudaSuccess) e = allow_max_smem(fluid_batch_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e != cudaSuccess) return e;
@@ -200,14 +231,16 @@ cudaError_t fluid_attributes(int cpt, int optin) {
 
 template <typename T>
 cudaError_t chain_attributes(int cpt, int optin) {
-    for (int gv = 0; gv < 3; ++gv) {
+    for (int v = 0; v < 5; ++v) {
         for (int nqc = 1; nqc <= (cpt <= 2 ? 2 : 1); ++nqc) {
-            cudaError_t e = allow_max_smem(chain_kernel<T>(cpt, nqc, gv), optin);
-            if (e == cudaSuccess) e = allow_max_smem(chain_batch_kernel<T>(cpt, nqc, gv), optin);
+            cudaError_t e = allow_max_smem(chain_kernel<T>(cpt, nqc, v), optin);
+            if (e == cudaSuccess) e = allow_max_smem(chain_batch_kernel<T>(cpt, nqc, v), optin);
             if (e != cudaSuccess) return e;
         }
-        cudaError_t e = allow_max_smem(ctcell_kernel<T>(cpt, gv), optin);
-        if (e == cudaSuccess) e = allow_max_smem(ctcell_batch_kernel<T>(cpt, gv), optin);
+    }
+    for (int v = 0; v < 3; ++v) {
+        cudaError_t e = allow_max_smem(ctcell_kernel<T>(cpt, v), optin);
+        if (e == cudaSuccess) e = allow_max_smem(ctcell_batch_kernel<T>(cpt, v), optin);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -226,7 +259,7 @@ cudaError_t fluid_max_clusters(const PencilLaunch& L, int* n) {
     attr[0].val.clusterDim.z = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
-    return cudaOccupancyMaxActiveClusters(n, fluid_kernel<T>(L.cpt, true, ghost_variant(L.fade, L.cg)), &lc);
+    return cudaOccupancyMaxActiveClusters(n, fluid_kernel<T>(L.cpt, true, kernel_variant(L.fade, L.cg, L.init)), &lc);
 }
 
 }  // namespace img
