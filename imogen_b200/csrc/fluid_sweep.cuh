@@ -271,12 +271,13 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
     }
 }
 
-// Mixed form with copy ghosts (single-CTA pencils, circ/const shifts): the predictor and corrector
+// Mixed form with copy ghosts (single-CTA pencils, circ/const/fade shifts): the predictor and corrector
 // stages store the flux numerators F beside the state they come from, so a stage is written before
 // the pencil's freezing speed c_f is known and the two pencil maxima share the stage barriers.
 // Readers form R = (u + F/c_f)/2 and L = (u - F/c_f)/2 (relaxingFluid.m:30-31, 52-56) at the rows
 // they need, with the reciprocal of c_f the flux stage itself would use.  Three barriers per sweep.
-template <bool MHD, int CPT>
+// FADE: some side of this sweep is fade (copy of the near end row plus the damping of cg_fade).
+template <bool MHD, int CPT, bool FADE>
 __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, unsigned vblock) {
     using T = float;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -301,6 +302,20 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     auto nix = [&](int k, int n) -> int {
         const int r = tl.grow(k);
         return n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs);
+    };
+    // fade damping of value v, the shift by n of an array whose row j is val(j), at own row k
+    const bool fade_lo = FADE && a.mode[CLS_MASS][0] == BC_FADE, fade_hi = FADE && a.mode[CLS_MASS][1] == BC_FADE;
+    const int fw = a.fade_f;
+    auto fade = [&](T v, int k, int n, auto&& val) -> T {
+        if constexpr (FADE) {
+            const int r = tl.grow(k);
+            if (!(n < 0 ? fade_lo : fade_hi) || r >= N || (r >= fw && r < N - fw)) return v;
+            const T s0 = n < 0 ? val(0) : val(N > 1 ? 1 : 0);
+            const T sN1 = n < 0 ? val(N >= 2 ? N - 2 : 0) : val(N - 1);
+            return fade_apply(v, r, N, a.fade, fw, s0, sN1);
+        } else {
+            return v;
+        }
     };
     const double G = a.gamma;
     const double dt = a.tm->dt;
@@ -355,8 +370,12 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
 #pragma unroll
         for (int v = 0; v < 5; ++v) {
             const T w = c0[5 + v] * ic;
-            const T Rm = T(0.5) * (cm[v] + cm[5 + v] * ic);
-            const T Lp = T(0.5) * (cp[v] - cp[5 + v] * ic);
+            T Rm = T(0.5) * (cm[v] + cm[5 + v] * ic);
+            T Lp = T(0.5) * (cp[v] - cp[5 + v] * ic);
+            if constexpr (FADE) {
+                Rm = fade(Rm, k, -1, [&](int j) { const T* c = SA + tl.ridx(j) * CS; return T(0.5) * (c[v] + c[5 + v] * ic); });
+                Lp = fade(Lp, k, +1, [&](int j) { const T* c = SA + tl.ridx(j) * CS; return T(0.5) * (c[v] - c[5 + v] * ic); });
+            }
             us[v] = u[v][k] - half_ffx * cf * (T(0.5) * (u[v][k] + w) - Rm + T(0.5) * (u[v][k] - w) - Lp);
         }
         us[0] = us[0] > (T)a.minmass ? us[0] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
@@ -391,8 +410,16 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
         for (int v = 0; v < 5; ++v) {
             const T wm = bm[5 + v] * ics, w0 = b0[5 + v] * ics, wp = bp[5 + v] * ics;
             const T um = bm[v], u0 = b0[v], up = bp[v];
-            const T Rm = T(0.5) * (um + wm), r = T(0.5) * (u0 + w0), Rp = T(0.5) * (up + wp);
-            const T Lm = T(0.5) * (um - wm), l = T(0.5) * (u0 - w0), Lp = T(0.5) * (up - wp);
+            T Rm = T(0.5) * (um + wm), Rp = T(0.5) * (up + wp), Lm = T(0.5) * (um - wm), Lp = T(0.5) * (up - wp);
+            const T r = T(0.5) * (u0 + w0), l = T(0.5) * (u0 - w0);
+            if constexpr (FADE) {
+                auto Rs = [&](int j) { const T* c = SB + tl.ridx(j) * CS; return T(0.5) * (c[v] + c[5 + v] * ics); };
+                auto Ls = [&](int j) { const T* c = SB + tl.ridx(j) * CS; return T(0.5) * (c[v] - c[5 + v] * ics); };
+                Rm = fade(Rm, k, -1, Rs);
+                Rp = fade(Rp, k, +1, Rs);
+                Lm = fade(Lm, k, -1, Ls);
+                Lp = fade(Lp, k, +1, Ls);
+            }
             a0[v] = r + limiter_corr<T>(a.limiter, r - Rm, Rp - r);
             a0[5 + v] = l + limiter_corr<T>(a.limiter, Lm - l, l - Lp);
         }
@@ -408,7 +435,14 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
         const T* ap = SA + nix(k, +1) * CS;
         T unew[5];
 #pragma unroll
-        for (int v = 0; v < 5; ++v) unew[v] = u[v][k] - ff * cfs * (a0[v] - am[v] + a0[5 + v] - ap[5 + v]);
+        for (int v = 0; v < 5; ++v) {
+            T Rm = am[v], Lp = ap[5 + v];
+            if constexpr (FADE) {
+                Rm = fade(Rm, k, -1, [&](int j) { return SA[tl.ridx(j) * CS + v]; });
+                Lp = fade(Lp, k, +1, [&](int j) { return SA[tl.ridx(j) * CS + 5 + v]; });
+            }
+            unew[v] = u[v][k] - ff * cfs * (a0[v] - Rm + a0[5 + v] - Lp);
+        }
         unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
@@ -440,9 +474,10 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
 
 // One fluid sweep of one grid, run by CTA `vblock` of that grid's launch.
 // FADE: some BC of this sweep direction is fade (compiles the damping in).
-// CG (copy ghosts): single-CTA pencils whose three fluid classes share one circ or const mode per
-// side.  Those ghosts copy an own row (circ: the far end, const: the near end), so the reader of
-// row 0 or N-1 indexes that row directly: no halo jobs and no barrier after them.
+// CG (copy ghosts): single-CTA pencils whose three fluid classes share one circ, const or fade mode
+// per side.  Those ghosts copy an own row (circ: the far end, const and fade: the near end, fade then
+// damped by cg_fade), so the reader of row 0 or N-1 indexes that row directly: no halo jobs and no
+// barrier after them.
 // INIT: this launch may capture stored edges of first-assigned objects (compiled out otherwise).
 template <typename T, bool MHD, int CPT, bool FADE, bool CG, bool INIT>
 __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, unsigned vblock) {
@@ -471,6 +506,9 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
         if constexpr (CG) {
             const int r = tl.grow(k);
             const int ix = n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs);
+            if constexpr (FADE) {
+                if (mode == BC_FADE) return cg_fade(tl, A, r, n, A[ix], a.fade, a.fade_f);
+            }
             return A[ix];
         } else {
             return shifted<FADE>(tl, A, an, k, n, mode, a.fade, a.fade_f);
@@ -667,14 +705,14 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
 }
 
 // Kernel variant V: 0 halo jobs, 1 halo jobs with fade, 2 copy ghosts, 3 and 4 as 0 and 1 with the
-// capture of stored edges (a run's first sweeps).
-template <int V> constexpr bool kv_fade = V == 1 || V == 4;
-template <int V> constexpr bool kv_cg = V == 2;
-template <int V> constexpr bool kv_init = V >= 3;
+// capture of stored edges (a run's first sweeps), 5 copy ghosts with fade.
+template <int V> constexpr bool kv_fade = V == 1 || V == 4 || V == 5;
+template <int V> constexpr bool kv_cg = V == 2 || V == 5;
+template <int V> constexpr bool kv_init = V == 3 || V == 4;
 
 template <typename T, bool MHD, int CPT, int V>
 __device__ __forceinline__ void fluid_sweep_body(const FluidArgs& a, unsigned vblock) {
-    if constexpr (kv_cg<V> && sizeof(T) == 4) fluid_sweep_body_mixed_cg<MHD, CPT>(a, vblock);
+    if constexpr (kv_cg<V> && sizeof(T) == 4) fluid_sweep_body_mixed_cg<MHD, CPT, kv_fade<V>>(a, vblock);
     else fluid_sweep_body_general<T, MHD, CPT, kv_fade<V>, kv_cg<V>, kv_init<V>>(a, vblock);
 }
 

@@ -380,6 +380,9 @@ bool fade_on(const img_config& c, int d, int cls_lo, int cls_hi) {
     return false;
 }
 
+// Boundary modes whose ghosts copy an own row of the pencil (fade: the near end row, damped).
+bool copy_ghost_mode(int m) { return m == IMG_BC_CIRC || m == IMG_BC_CONST || m == IMG_BC_FADE; }
+
 template <typename T>
 PencilLaunch pencil_launch(const img_ctx* ctx, const PencilCfg& pcf, int d, size_t smem, unsigned grid_y, bool fade) {
     const long long ncol = ctx->g.ncell / ctx->g.n[d];
@@ -425,12 +428,12 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.cfl = cfl;
     PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
                                       fade_on(c, d, CLS_MASS, CLS_ENER));
-    // copy ghosts: single-CTA pencils, one circ or const mode per side shared by the fluid classes
+    // copy ghosts: single-CTA pencils, one circ, const or fade mode per side shared by the fluid classes
     L.cg = pcf.CL == 1;
     for (int k = 0; k < 3; ++k)
         for (int side = 0; side < 2; ++side) {
             const int m = a.mode[k][side];
-            if ((m != IMG_BC_CIRC && m != IMG_BC_CONST) || m != a.mode[CLS_MASS][side]) L.cg = false;
+            if (!copy_ghost_mode(m) || m != a.mode[CLS_MASS][side]) L.cg = false;
         }
     L.init = a.init_store || a.init_flux;   // first sweeps: the stored-edge capturing kernel
     if (ctx->rec) {
@@ -505,9 +508,8 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
                                       2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
     PencilLaunch Lc = pencil_launch<T>(ctx, pcf, d, ctcell_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
                                        fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
-    // copy ghosts: single-CTA pencils with circ or const mag-class shifts along X
-    L.cg = Lc.cg = pcf.CL == 1 && (a.modeX[0] == IMG_BC_CIRC || a.modeX[0] == IMG_BC_CONST) &&
-                   (a.modeX[1] == IMG_BC_CIRC || a.modeX[1] == IMG_BC_CONST);
+    // copy ghosts: single-CTA pencils with circ, const or fade mag-class shifts along X
+    L.cg = Lc.cg = pcf.CL == 1 && copy_ghost_mode(a.modeX[0]) && copy_ghost_mode(a.modeX[1]);
     L.init = a.init_mag[0] || a.init_mag[1];   // first sweep of (I, X): the stored-edge capturing chain
     if (ctx->rec) {
         OpRec r{};

@@ -165,7 +165,7 @@ struct ChainComp {
 // component blockIdx.y, NQC = 2 both transverse components, interleaved stage by stage so that
 // every barrier serves twice the work.
 // FADE: a mag-class BC along X is fade (compiles the damping in).  CG (copy ghosts): single-CTA
-// pencils with circ or const mag-class shifts along X; the reader of a row next to a pencil end
+// pencils with circ, const or fade mag-class shifts along X; the reader of a row next to a pencil end
 // indexes the row its ghost copies, so no stage needs halo jobs or the barrier after them.
 // INIT: this launch may capture stored edges of first-assigned objects (compiled out otherwise; the
 // host never combines it with CG).
@@ -204,7 +204,11 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     auto sh = [&](const T* A, const Ghost<T>* an, int k, int n, int mode) -> T {
         if constexpr (CG) {
             const int r = tl.grow(k);
-            return A[n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs)];
+            const T v = A[n < 0 ? (r == 0 ? dn_src : tl.idx(k) - tl.rs) : (r == N - 1 ? up_src : tl.idx(k) + tl.rs)];
+            if constexpr (FADE) {
+                if (mode == BC_FADE) return cg_fade(tl, A, r, n, v, fc, f);
+            }
+            return v;
         } else {
             return shifted<FADE>(tl, A, an, k, n, mode, fc, f);
         }
@@ -375,6 +379,13 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             if constexpr (CG) {   // the four upper calls share their ghosts
                 p1a = p1b = p1d = A[r == N - 1 ? up_src : ix + tl.rs];
                 p2 = A[r == N - 2 ? up_src : (r == N - 1 ? up2_src : ix + 2 * tl.rs)];
+                if constexpr (FADE) {
+                    if (mhi == BC_FADE && r < N && (r < f || r >= N - f)) {   // anchors of the +1 and +2 shifts
+                        const T a1 = A[tl.ridx(N > 1 ? 1 : 0)], aN = A[tl.ridx(N - 1)], a2 = A[tl.ridx(N > 2 ? 2 : N - 1)];
+                        p1a = p1b = p1d = fade_apply(p1a, r, N, fc, f, a1, aN);
+                        p2 = fade_apply(p2, r, N, fc, f, a2, aN);
+                    }
+                }
             } else if (r >= N - 2 && r < N) {   // rows next to the upper end: ghosts of the four calls
                 if (r == N - 1) {
                     p1a = gs[1 * Wb + b].g;
@@ -385,7 +396,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
                     p2 = gs[3 * Wb + b].g;
                 }
             }
-            if (FADE && mhi == BC_FADE) {
+            if (!CG && FADE && mhi == BC_FADE) {
                 const Ghost<T>& u1 = gs[1 * Wb + b];
                 const Ghost<T>& u2 = gs[3 * Wb + b];
                 p1a = fade_apply(p1a, r, N, fc, f, u1.s0, u1.sN1);
@@ -519,6 +530,12 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
             const int ix = tl.grow(k) == 0 ? dn_src : tl.idx(k) - tl.rs;
             D0 = S[ix];
             D1 = S[AS + ix];
+            if constexpr (FADE) {
+                if (mlo == BC_FADE) {
+                    D0 = cg_fade(tl, (const T*)S, tl.grow(k), -1, D0, fc, f);
+                    D1 = cg_fade(tl, (const T*)(S + AS), tl.grow(k), -1, D1, fc, f);
+                }
+            }
         } else {
             D0 = shifted<FADE>(tl, (const T*)S, GS, k, -1, mlo, fc, f);
             D1 = shifted<FADE>(tl, (const T*)(S + AS), GS + Wb, k, -1, mlo, fc, f);
@@ -546,8 +563,14 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         T up;
-        if constexpr (CG) up = S[2 * AS + (tl.grow(k) == N - 1 ? up_src : tl.idx(k) + tl.rs)];
-        else up = shifted<FADE>(tl, (const T*)(S + 2 * AS), GS + 2 * Wb, k, +1, mhi, fc, f);
+        if constexpr (CG) {
+            up = S[2 * AS + (tl.grow(k) == N - 1 ? up_src : tl.idx(k) + tl.rs)];
+            if constexpr (FADE) {
+                if (mhi == BC_FADE) up = cg_fade(tl, (const T*)(S + 2 * AS), tl.grow(k), +1, up, fc, f);
+            }
+        } else {
+            up = shifted<FADE>(tl, (const T*)(S + 2 * AS), GS + 2 * Wb, k, +1, mhi, fc, f);
+        }
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
         BX[o] = bx[k];

@@ -176,6 +176,18 @@ __device__ __forceinline__ T shifted(const Tile<T, CPT>& tl, const T* A, const G
     return v;
 }
 
+// Copy-ghost form of the fade damping: v is A.shift(d, n) at own row r (the ghost copies the near end
+// row, as a const shift); rows within f of either end are damped toward the shift's anchors, which
+// are the array's own rows 0 and N-2 (n = -1) or 1 and N-1 (n = +1) (fade_shift.m:31-44).
+template <typename T, int CPT>
+__device__ __forceinline__ T cg_fade(const Tile<T, CPT>& tl, const T* A, int r, int n, T v, const double* fc, int f) {
+    const int N = tl.N;
+    if (r >= N || (r >= f && r < N - f)) return v;
+    const T s0 = n < 0 ? A[tl.ridx(0)] : A[tl.ridx(N > 1 ? 1 : 0)];
+    const T sN1 = n < 0 ? A[tl.ridx(N >= 2 ? N - 2 : 0)] : A[tl.ridx(N - 1)];
+    return fade_apply(v, r, N, fc, f, s0, sN1);
+}
+
 // "No stored-edge value supplied" marker (stored edges are finite physical values).
 constexpr double NO_EV = -1.0e300;
 

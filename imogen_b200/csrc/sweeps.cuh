@@ -15,7 +15,7 @@ struct PencilLaunch {
     int cpt;                   // cells per thread (1, 2 or 4)
     int nqc;                   // magnet chain: transverse components per CTA (1, or 2 with cpt <= 2)
     bool fade;                 // a fade BC on this sweep direction
-    bool cg;                   // copy ghosts (single-CTA pencils, circ/const shifts)
+    bool cg;                   // copy ghosts (single-CTA pencils, circ/const/fade shifts)
     bool init;                 // fluid sweep / chain: captures stored edges (overrides cg)
     cudaStream_t stream;
 };

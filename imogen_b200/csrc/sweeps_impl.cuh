@@ -47,10 +47,12 @@ cudaError_t launch_pencil(void (*kern)(const Args), const Args& a, const PencilL
 }
 
 // Kernel variant of a pencil launch (see kv_fade/kv_cg/kv_init): halo jobs (0), with fade (1), copy
-// ghosts (2), and the stored-edge capturing forms of 0 and 1 (3, 4), which first sweeps use.
+// ghosts (2), the stored-edge capturing forms of 0 and 1 (3, 4), which first sweeps use, and copy
+// ghosts with fade (5).
 inline int kernel_variant(bool fade, bool cg, bool init) {
     if (init) return fade ? 4 : 3;
-    return fade ? 1 : (cg ? 2 : 0);
+    if (cg) return fade ? 5 : 2;
+    return fade ? 1 : 0;
 }
 
 template <typename T, bool MHD, int V>
@@ -98,6 +100,7 @@ void (*fluid_kernel_m(int cpt, int v))(const FluidArgs) {
         case 2: return fluid_kernel_v<T, MHD, 2>(cpt);
         case 3: return fluid_kernel_v<T, MHD, 3>(cpt);
         case 4: return fluid_kernel_v<T, MHD, 4>(cpt);
+        case 5: return fluid_kernel_v<T, MHD, 5>(cpt);
         default: return fluid_kernel_v<T, MHD, 0>(cpt);
     }
 }
@@ -109,6 +112,7 @@ void (*fluid_batch_kernel_m(int cpt, int v))(const FluidArgs*, const BlockMap*) 
         case 2: return fluid_batch_kernel_v<T, MHD, 2>(cpt);
         case 3: return fluid_batch_kernel_v<T, MHD, 3>(cpt);
         case 4: return fluid_batch_kernel_v<T, MHD, 4>(cpt);
+        case 5: return fluid_batch_kernel_v<T, MHD, 5>(cpt);
         default: return fluid_batch_kernel_v<T, MHD, 0>(cpt);
     }
 }
@@ -130,6 +134,7 @@ void (*chain_kernel(int cpt, int nqc, int v))(const MagArgs) {
         case 2: return chain_kernel_v<T, 2>(cpt, nqc);
         case 3: return chain_kernel_v<T, 3>(cpt, nqc);
         case 4: return chain_kernel_v<T, 4>(cpt, nqc);
+        case 5: return chain_kernel_v<T, 5>(cpt, nqc);
         default: return chain_kernel_v<T, 0>(cpt, nqc);
     }
 }
@@ -141,12 +146,13 @@ void (*chain_batch_kernel(int cpt, int nqc, int v))(const MagArgs*, const BlockM
         case 2: return chain_batch_kernel_v<T, 2>(cpt, nqc);
         case 3: return chain_batch_kernel_v<T, 3>(cpt, nqc);
         case 4: return chain_batch_kernel_v<T, 4>(cpt, nqc);
+        case 5: return chain_batch_kernel_v<T, 5>(cpt, nqc);
         default: return chain_batch_kernel_v<T, 0>(cpt, nqc);
     }
 }
 
-// The CT kernel captures no stored edges: its variant ignores `init`.
-inline int ct_variant(bool fade, bool cg) { return fade ? 1 : (cg ? 2 : 0); }
+// The CT kernel captures no stored edges: its variant ignores `init` (0 jobs, 1 fade, 2 cg, 3 both).
+inline int ct_variant(bool fade, bool cg) { return (fade ? 1 : 0) | (cg ? 2 : 0); }
 
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
@@ -178,14 +184,22 @@ void (*ctcell_batch_kernel(int cpt))(const MagArgs*, const BlockMap*) {
 
 template <typename T>
 void (*ctcell_kernel(int cpt, int gv))(const MagArgs) {
-    return gv == 1 ? ctcell_kernel<T, true, false>(cpt)
-                   : (gv == 2 ? ctcell_kernel<T, false, true>(cpt) : ctcell_kernel<T, false, false>(cpt));
+    switch (gv) {
+        case 1: return ctcell_kernel<T, true, false>(cpt);
+        case 2: return ctcell_kernel<T, false, true>(cpt);
+        case 3: return ctcell_kernel<T, true, true>(cpt);
+        default: return ctcell_kernel<T, false, false>(cpt);
+    }
 }
 
 template <typename T>
 void (*ctcell_batch_kernel(int cpt, int gv))(const MagArgs*, const BlockMap*) {
-    return gv == 1 ? ctcell_batch_kernel<T, true, false>(cpt)
-                   : (gv == 2 ? ctcell_batch_kernel<T, false, true>(cpt) : ctcell_batch_kernel<T, false, false>(cpt));
+    switch (gv) {
+        case 1: return ctcell_batch_kernel<T, true, false>(cpt);
+        case 2: return ctcell_batch_kernel<T, false, true>(cpt);
+        case 3: return ctcell_batch_kernel<T, true, true>(cpt);
+        default: return ctcell_batch_kernel<T, false, false>(cpt);
+    }
 }
 
 template <typename T>
@@ -221,7 +235,7 @@ cudaError_t allow_max_smem(K kern, int optin) {
 
 template <typename T>
 cudaError_t fluid_attributes(int cpt, int optin) {
-    for (int v = 0; v < 10; ++v) {
+    for (int v = 0; v < 12; ++v) {
         cudaError_t e = allow_max_smem(fluid_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e == cudaSuccess) e = allow_max_smem(fluid_batch_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e != cudaSuccess) return e;
@@ -231,14 +245,14 @@ cudaError_t fluid_attributes(int cpt, int optin) {
 
 template <typename T>
 cudaError_t chain_attributes(int cpt, int optin) {
-    for (int v = 0; v < 5; ++v) {
+    for (int v = 0; v < 6; ++v) {
         for (int nqc = 1; nqc <= (cpt <= 2 ? 2 : 1); ++nqc) {
             cudaError_t e = allow_max_smem(chain_kernel<T>(cpt, nqc, v), optin);
             if (e == cudaSuccess) e = allow_max_smem(chain_batch_kernel<T>(cpt, nqc, v), optin);
             if (e != cudaSuccess) return e;
         }
     }
-    for (int v = 0; v < 3; ++v) {
+    for (int v = 0; v < 4; ++v) {
         cudaError_t e = allow_max_smem(ctcell_kernel<T>(cpt, v), optin);
         if (e == cudaSuccess) e = allow_max_smem(ctcell_batch_kernel<T>(cpt, v), optin);
         if (e != cudaSuccess) return e;
