@@ -176,3 +176,16 @@ def test_long_pencils_along_y_and_z(grid, magnet, precision):
     o.run()
     g.run()
     _assert_close(o, g, tol, f"{grid} {precision}")
+
+
+@pytest.mark.parametrize("bc", BCS)
+@pytest.mark.parametrize("grid", [(24, 22, 1), (22, 21, 20)])
+def test_iterations_mixed_every_boundary(bc, grid):
+    """Mixed form (FP32 state; the copy-ghost kernels for circ/const/fade, halo jobs for the others)
+    against the FP64 oracle over 10 MHD iterations."""
+    s = _settings(grid, bc, magnet=True)
+    o, g = make_pair(s, smooth_state(grid, seed=5, mhd=True), precision="mixed")
+    o.run(10)
+    g.run(10)
+    assert abs(g.time.time - o.time) <= 1e-5 * max(1.0, o.time)
+    _assert_close(o, g, 2e-5, f"mixed, 10 iterations bc={bc}")
