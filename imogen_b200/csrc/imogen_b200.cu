@@ -99,6 +99,10 @@ struct img_ctx {
     DevTime* host_tm = nullptr;  // pinned mirror
     uint64_t launches = 0;       // kernels launched by this context
     cudaStream_t own_stream = nullptr;   // the context's stream (stream is the batch's while a member)
+    // mixed form: pipelined host transfers through the two halves of `stage` (copies on xfer_stream,
+    // FP64<->FP32 conversions on the context's stream); created at the first staged transfer
+    cudaStream_t xfer_stream = nullptr;
+    cudaEvent_t xfer_ev[5] = {};         // [0,1] half h converted, [2,3] half h copied, [4] fence
     img_batch* batch = nullptr;          // batch this context is a member of
     std::vector<OpRec>* rec = nullptr;   // set while the batch records this member's launches
 };
@@ -898,6 +902,9 @@ int img_destroy(img_ctx* ctx) {
     if (ctx->slab) cudaFree(ctx->slab);
     if (ctx->host_tm) cudaFreeHost(ctx->host_tm);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    for (cudaEvent_t e : ctx->xfer_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->xfer_stream) cudaStreamDestroy(ctx->xfer_stream);
     delete ctx;
     return IMG_OK;
 }
@@ -945,11 +952,80 @@ int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
     return IMG_OK;
 }
 
+// Mixed form, several arrays: each array moves in two parts through the two halves of the FP64
+// stage, the copies on a second stream and the conversions on the context's stream, so the copy of
+// one part overlaps the conversion of the previous one (the copy engine never waits for a kernel).
+// Part p of every array uses half p; events order a half's next copy after its last conversion (and
+// the reverse for downloads).  Halves split at a multiple of 4 values (16-byte vector access).
+static int staged_streams(img_ctx* ctx) {
+    if (ctx->xfer_stream) return IMG_OK;
+    CK(cudaStreamCreateWithFlags(&ctx->xfer_stream, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ctx->xfer_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return IMG_OK;
+}
+
+static int staged_transfer(img_ctx* ctx, int count, const int* vars, const double* const* up, double* const* down,
+                           size_t n) {
+    int rc = staged_streams(ctx);
+    if (rc != IMG_OK) return rc;
+    cudaStream_t ms = ctx->stream, xs = ctx->xfer_stream;
+    cudaEvent_t* ev = ctx->xfer_ev;
+    const size_t h = (n / 2) & ~(size_t)3;
+    const size_t off[2] = {0, h}, len[2] = {h, n - h};
+    CK(cudaEventRecord(ev[4], ms));        // the stream's earlier work (kernels reading or writing the state)
+    CK(cudaStreamWaitEvent(xs, ev[4], 0));
+    for (int i = 0; i < count; ++i) {
+        const int v = vars[i];
+        float* q = static_cast<float*>(ctx->q[v]);
+        for (int p = 0; p < 2; ++p) {
+            if (len[p] == 0) continue;
+            double* buf = ctx->stage + off[p];
+            const unsigned blocks = launch_blocks((long long)(len[p] + 3) / 4);
+            if (up) {
+                if (i > 0) CK(cudaStreamWaitEvent(xs, ev[p], 0));   // half p's last conversion is done
+                CK(cudaMemcpyAsync(buf, up[i] + off[p], len[p] * 8, cudaMemcpyHostToDevice, xs));
+                CK(cudaEventRecord(ev[2 + p], xs));
+                CK(cudaStreamWaitEvent(ms, ev[2 + p], 0));
+                f64_to_f32_kernel<<<blocks, 256, 0, ms>>>(buf, q + off[p], (long long)len[p]);
+                CK(cudaGetLastError());
+                CK(cudaEventRecord(ev[p], ms));
+            } else {
+                if (i > 0) CK(cudaStreamWaitEvent(ms, ev[2 + p], 0));   // half p's last copy is done
+                f32_to_f64_kernel<<<blocks, 256, 0, ms>>>(q + off[p], buf, (long long)len[p]);
+                CK(cudaGetLastError());
+                CK(cudaEventRecord(ev[p], ms));
+                CK(cudaStreamWaitEvent(xs, ev[p], 0));
+                CK(cudaMemcpyAsync(down[i] + off[p], buf, len[p] * 8, cudaMemcpyDeviceToHost, xs));
+                CK(cudaEventRecord(ev[2 + p], xs));
+            }
+            ctx->launches += 1;
+        }
+    }
+    CK(cudaEventRecord(ev[4], xs));        // the caller synchronises the context's stream
+    CK(cudaStreamWaitEvent(ms, ev[4], 0));
+    if (up) ctx->cfl_valid = false;
+    return IMG_OK;
+}
+
+static bool staged_ok(const img_ctx* ctx, int count, const int* var_ids, size_t n, int nvars) {
+    if (ctx->elem != 4 || n != (size_t)ctx->g.ncell || n < 64) return false;
+    for (int i = 0; i < count; ++i)
+        if (var_ids[i] < 0 || var_ids[i] >= nvars) return false;
+    return true;
+}
+
 int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* const* hosts, size_t n) {
     if (!ctx || count < 0 || (count && (!var_ids || !hosts))) return fail(ctx, IMG_ERR_ARG, "bad upload argument");
-    for (int i = 0; i < count; ++i) {
-        int rc = enqueue_upload(ctx, var_ids[i], hosts[i], n);
+    bool hosts_ok = true;
+    for (int i = 0; i < count; ++i) hosts_ok = hosts_ok && hosts[i];
+    if (hosts_ok && staged_ok(ctx, count, var_ids, n, IMG_VAR_MAGZ + 1)) {
+        int rc = staged_transfer(ctx, count, var_ids, hosts, nullptr, n);
         if (rc != IMG_OK) return rc;
+    } else {
+        for (int i = 0; i < count; ++i) {
+            int rc = enqueue_upload(ctx, var_ids[i], hosts[i], n);
+            if (rc != IMG_OK) return rc;
+        }
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
@@ -957,9 +1033,16 @@ int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* c
 
 int img_download_many(img_ctx* ctx, int count, const int* var_ids, double* const* hosts, size_t n) {
     if (!ctx || count < 0 || (count && (!var_ids || !hosts))) return fail(ctx, IMG_ERR_ARG, "bad download argument");
-    for (int i = 0; i < count; ++i) {
-        int rc = enqueue_download(ctx, var_ids[i], hosts[i], n);
+    bool hosts_ok = true;
+    for (int i = 0; i < count; ++i) hosts_ok = hosts_ok && hosts[i];
+    if (hosts_ok && staged_ok(ctx, count, var_ids, n, NQ)) {
+        int rc = staged_transfer(ctx, count, var_ids, nullptr, hosts, n);
         if (rc != IMG_OK) return rc;
+    } else {
+        for (int i = 0; i < count; ++i) {
+            int rc = enqueue_download(ctx, var_ids[i], hosts[i], n);
+            if (rc != IMG_OK) return rc;
+        }
     }
     CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
