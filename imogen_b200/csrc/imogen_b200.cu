@@ -7,7 +7,12 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
+#include <functional>
+#include <thread>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -43,6 +48,73 @@ int pow2ceil(long long v) {
     while (p < v) p <<= 1;
     return p;
 }
+
+// A small process-wide pool of host threads for the FP64 <-> FP32 conversions of the mixed form's
+// host transfers.  run(n, fn) calls fn(0..n-1) on the pool and the calling thread and returns when
+// all calls have returned.  Idle workers spin for a short while (transfers come in bursts of calls
+// tens of microseconds apart) and then sleep.  One run at a time (callers are serialised).
+class HostPool {
+  public:
+    static HostPool& get() {
+        static HostPool* pool = new HostPool();   // never destroyed: workers may sleep at exit
+        return *pool;
+    }
+    int threads() const { return (int)workers_.size() + 1; }
+    void run(int n, const std::function<void(int)>& fn) {
+        std::lock_guard<std::mutex> serial(run_mu_);
+        if (n <= 0) return;
+        {
+            std::lock_guard<std::mutex> lock(mu_);
+            job_.store(&fn);
+            total_.store(n);
+            next_.store(0);
+            finished_.store(0);
+            gen_.fetch_add(1);
+        }
+        cv_.notify_all();
+        work();
+        while (finished_.load() < n) std::this_thread::yield();
+        std::lock_guard<std::mutex> lock(mu_);
+        job_.store(nullptr);
+    }
+
+  private:
+    HostPool() {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nw = (int)std::min(7u, hw / 2);
+        for (int i = 0; i < nw; ++i) workers_.emplace_back([this] { loop(); });
+        for (auto& t : workers_) t.detach();
+    }
+    void work() {
+        for (int i; (i = next_.fetch_add(1)) < total_.load();) {
+            (*job_.load())(i);
+            finished_.fetch_add(1);
+        }
+    }
+    void loop() {
+        unsigned long long seen = 0;
+        for (;;) {
+            const auto t0 = std::chrono::steady_clock::now();
+            while (gen_.load() == seen && std::chrono::steady_clock::now() - t0 < std::chrono::microseconds(500))
+                std::this_thread::yield();
+            if (gen_.load() == seen) {
+                std::unique_lock<std::mutex> lock(mu_);
+                cv_.wait(lock, [&] { return gen_.load() != seen; });
+            }
+            std::unique_lock<std::mutex> lock(mu_);
+            seen = gen_.load();
+            if (!job_.load()) continue;
+            lock.unlock();
+            work();
+        }
+    }
+    std::vector<std::thread> workers_;
+    std::mutex mu_, run_mu_;
+    std::condition_variable cv_;
+    std::atomic<const std::function<void(int)>*> job_{nullptr};
+    std::atomic<int> total_{0}, next_{0}, finished_{0};
+    std::atomic<unsigned long long> gen_{0};
+};
 
 }  // namespace
 
@@ -99,10 +171,11 @@ struct img_ctx {
     DevTime* host_tm = nullptr;  // pinned mirror
     uint64_t launches = 0;       // kernels launched by this context
     cudaStream_t own_stream = nullptr;   // the context's stream (stream is the batch's while a member)
-    // mixed form: pipelined host transfers through the two halves of `stage` (copies on xfer_stream,
-    // FP64<->FP32 conversions on the context's stream); created at the first staged transfer
+    // mixed form: bulk host transfers in FP32 (copies on xfer_stream, FP64<->FP32 conversions on the
+    // host); created at the first bulk transfer
     cudaStream_t xfer_stream = nullptr;
-    cudaEvent_t xfer_ev[5] = {};         // [0,1] half h converted, [2,3] half h copied, [4] fence
+    cudaEvent_t xfer_ev[5] = {};         // [2,3] copy from / to host buffer b done, [4] stream fence
+    float* h32 = nullptr;                // two pinned FP32 host buffers of one array each
     img_batch* batch = nullptr;          // batch this context is a member of
     std::vector<OpRec>* rec = nullptr;   // set while the batch records this member's launches
 };
@@ -905,6 +978,7 @@ int img_destroy(img_ctx* ctx) {
     for (cudaEvent_t e : ctx->xfer_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->xfer_stream) cudaStreamDestroy(ctx->xfer_stream);
+    if (ctx->h32) cudaFreeHost(ctx->h32);
     delete ctx;
     return IMG_OK;
 }
@@ -952,11 +1026,11 @@ int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
     return IMG_OK;
 }
 
-// Mixed form, several arrays: each array moves in two parts through the two halves of the FP64
-// stage, the copies on a second stream and the conversions on the context's stream, so the copy of
-// one part overlaps the conversion of the previous one (the copy engine never waits for a kernel).
-// Part p of every array uses half p; events order a half's next copy after its last conversion (and
-// the reverse for downloads).  Halves split at a multiple of 4 values (16-byte vector access).
+// Mixed form, several arrays (img_upload_many / img_download_many): FP32 crosses PCIe.  The host
+// pool rounds each FP64 array to FP32 (or widens it after the copy) in chunks, into one of two pinned
+// FP32 buffers, and the copy of one array overlaps the conversion of the next.  The rounding is IEEE
+// round-to-nearest on the host as in the device conversion kernels, so the state holds the same bits
+// either way; the caller's arrays need not be pinned.
 static int staged_streams(img_ctx* ctx) {
     if (ctx->xfer_stream) return IMG_OK;
     CK(cudaStreamCreateWithFlags(&ctx->xfer_stream, cudaStreamNonBlocking));
@@ -964,51 +1038,63 @@ static int staged_streams(img_ctx* ctx) {
     return IMG_OK;
 }
 
+static void convert_chunks(size_t n, const std::function<void(size_t, size_t)>& f) {
+    HostPool& pool = HostPool::get();
+    const size_t chunk = std::max<size_t>(8192, (n + 2 * pool.threads() - 1) / (2 * pool.threads()));
+    const int nc = (int)((n + chunk - 1) / chunk);
+    pool.run(nc, [&](int c) {
+        const size_t a = (size_t)c * chunk;
+        f(a, std::min(n, a + chunk));
+    });
+}
+
 static int staged_transfer(img_ctx* ctx, int count, const int* vars, const double* const* up, double* const* down,
                            size_t n) {
     int rc = staged_streams(ctx);
     if (rc != IMG_OK) return rc;
+    if (!ctx->h32) CK(cudaHostAlloc(reinterpret_cast<void**>(&ctx->h32), 2 * n * sizeof(float), cudaHostAllocDefault));
     cudaStream_t ms = ctx->stream, xs = ctx->xfer_stream;
     cudaEvent_t* ev = ctx->xfer_ev;
-    const size_t h = (n / 2) & ~(size_t)3;
-    const size_t off[2] = {0, h}, len[2] = {h, n - h};
+    float* hb[2] = {ctx->h32, ctx->h32 + n};
     CK(cudaEventRecord(ev[4], ms));        // the stream's earlier work (kernels reading or writing the state)
     CK(cudaStreamWaitEvent(xs, ev[4], 0));
-    for (int i = 0; i < count; ++i) {
-        const int v = vars[i];
-        float* q = static_cast<float*>(ctx->q[v]);
-        for (int p = 0; p < 2; ++p) {
-            if (len[p] == 0) continue;
-            double* buf = ctx->stage + off[p];
-            const unsigned blocks = launch_blocks((long long)(len[p] + 3) / 4);
-            if (up) {
-                if (i > 0) CK(cudaStreamWaitEvent(xs, ev[p], 0));   // half p's last conversion is done
-                CK(cudaMemcpyAsync(buf, up[i] + off[p], len[p] * 8, cudaMemcpyHostToDevice, xs));
-                CK(cudaEventRecord(ev[2 + p], xs));
-                CK(cudaStreamWaitEvent(ms, ev[2 + p], 0));
-                f64_to_f32_kernel<<<blocks, 256, 0, ms>>>(buf, q + off[p], (long long)len[p]);
-                CK(cudaGetLastError());
-                CK(cudaEventRecord(ev[p], ms));
-            } else {
-                if (i > 0) CK(cudaStreamWaitEvent(ms, ev[2 + p], 0));   // half p's last copy is done
-                f32_to_f64_kernel<<<blocks, 256, 0, ms>>>(q + off[p], buf, (long long)len[p]);
-                CK(cudaGetLastError());
-                CK(cudaEventRecord(ev[p], ms));
-                CK(cudaStreamWaitEvent(xs, ev[p], 0));
-                CK(cudaMemcpyAsync(down[i] + off[p], buf, len[p] * 8, cudaMemcpyDeviceToHost, xs));
-                CK(cudaEventRecord(ev[2 + p], xs));
-            }
-            ctx->launches += 1;
+    if (up) {
+        for (int i = 0; i < count; ++i) {
+            const int b = i & 1;
+            if (i >= 2) CK(cudaEventSynchronize(ev[2 + b]));   // buffer b's previous copy is done
+            const double* src = up[i];
+            float* dst = hb[b];
+            convert_chunks(n, [&](size_t a, size_t e) {
+                for (size_t j = a; j < e; ++j) dst[j] = (float)src[j];
+            });
+            CK(cudaMemcpyAsync(ctx->q[vars[i]], dst, n * sizeof(float), cudaMemcpyHostToDevice, xs));
+            CK(cudaEventRecord(ev[2 + b], xs));
+        }
+        ctx->cfl_valid = false;
+    } else {
+        auto enqueue = [&](int i) -> cudaError_t {
+            cudaError_t e = cudaMemcpyAsync(hb[i & 1], ctx->q[vars[i]], n * sizeof(float), cudaMemcpyDeviceToHost, xs);
+            return e == cudaSuccess ? cudaEventRecord(ev[2 + (i & 1)], xs) : e;
+        };
+        for (int i = 0; i < count && i < 2; ++i) CK(enqueue(i));
+        for (int i = 0; i < count; ++i) {
+            const int b = i & 1;
+            CK(cudaEventSynchronize(ev[2 + b]));
+            const float* src = hb[b];
+            double* dst = down[i];
+            convert_chunks(n, [&](size_t a, size_t e) {
+                for (size_t j = a; j < e; ++j) dst[j] = (double)src[j];
+            });
+            if (i + 2 < count) CK(enqueue(i + 2));
         }
     }
     CK(cudaEventRecord(ev[4], xs));        // the caller synchronises the context's stream
     CK(cudaStreamWaitEvent(ms, ev[4], 0));
-    if (up) ctx->cfl_valid = false;
     return IMG_OK;
 }
 
 static bool staged_ok(const img_ctx* ctx, int count, const int* var_ids, size_t n, int nvars) {
-    if (ctx->elem != 4 || n != (size_t)ctx->g.ncell || n < 64) return false;
+    if (ctx->elem != 4 || n != (size_t)ctx->g.ncell) return false;
     for (int i = 0; i < count; ++i)
         if (var_ids[i] < 0 || var_ids[i] >= nvars) return false;
     return true;
