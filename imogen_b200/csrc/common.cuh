@@ -204,17 +204,15 @@ struct PressOut {
 };
 __device__ __forceinline__ PressOut pressure_totsnd(double G, double rho, double px, double py, double pz, double E,
                                                     double msq) {
-    double vsq = (px * px + py * py + pz * pz) / (rho * rho);
+    const double ir = 1.0 / rho;   // one division (a compiler CSE shares it with the flux terms)
+    double vsq = (px * px + py * py + pz * pz) * (ir * ir);
     double r = (G - 1.0) * (E - 0.5 * rho * vsq);
     PressOut o;
-    o.cs = sqrt(fabs((G * (r - (G - 1.0) * 0.5 * msq) + 2.0 * msq) / rho));
+    o.cs = sqrt(fabs((G * (r - (G - 1.0) * 0.5 * msq) + 2.0 * msq) * ir));
     r = r + 0.5 * (2.0 - G) * msq;
     o.p = r < 0 ? 0.0 : r;
     return o;
 }
-// Mixed form of 'totsnd' for FP32 state: the pressure recovery P0 = (G-1)(E - rho v^2/2) and the
-// magnetic terms are evaluated in FP64 (the reciprocal of rho is an FP32 estimate refined by one
-// FP64 Newton step, exact to ~1e-15), the sound speed is taken in FP32.
 // Hardware approximations for the FP32 arithmetic of the mixed form: the reciprocal within 1 ulp and
 // the square root within 2^-23 relative (PTX rcp.approx.f32 / sqrt.approx.f32), one instruction
 // each instead of the correctly rounded sequences.
@@ -229,6 +227,9 @@ __device__ __forceinline__ float sqrt_approx(float x) {
     return r;
 }
 
+// Mixed form of 'totsnd' for FP32 state: the pressure recovery P0 = (G-1)(E - rho v^2/2) and the
+// magnetic terms are evaluated in FP64 (the reciprocal of rho is an FP32 estimate refined by one
+// FP64 Newton step, exact to ~1e-15), the sound speed is taken in FP32.
 struct PressOutF {
     float p;
     float cs;

@@ -80,15 +80,17 @@ __device__ __forceinline__ void wflux(int d, const T u[5], const T bb[3], T pres
         flux_num(d, u, bb, press, w);
 #pragma unroll
         for (int v = 0; v < 5; ++v) w[v] = w[v] * ic;
-    } else {   // plain FP64: the operation order of wFluidFlux.m
-        T velocity = pX / u[0];
-        w[0] = pX / cf;
-        T we = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) / u[0];
-        w[4] = we / cf;
+    } else {   // plain FP64: wFluidFlux.m's terms, its divisions by rho and c_f as products with one
+               // reciprocal of each (a rounding-level difference)
+        const T ir = T(1) / u[0], ic = T(1) / cf;
+        T velocity = pX * ir;
+        w[0] = pX * ic;
+        T we = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
+        w[4] = we * ic;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             T dirv = c == d ? T(1) : T(0);
-            w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) / cf;
+            w[1 + c] = (velocity * u[1 + c] + press * dirv - bX * bb[c]) * ic;
         }
     }
 }
@@ -104,7 +106,7 @@ __device__ __forceinline__ T press_speed(double G, int d, const T u[5], double m
     } else {
         PressOut o = pressure_totsnd(G, u[0], u[1], u[2], u[3], u[4], msq);
         p = o.p + 0.0;   // + viscosity.solve ('empty' -> 0)
-        return fabs(pX / u[0]) + o.cs;
+        return fabs(pX * (1.0 / u[0])) + o.cs;
     }
 }
 
