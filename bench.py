@@ -306,10 +306,15 @@ def run_ours(args):
     ins = [pin(a) for a in src]
     outs = [pin(np.zeros(ncell)) for _ in range(8)]
     ke = max(3, args.steps // 2)
-    barrier()
-    t0 = time.perf_counter()
     up = dict(zip(names, ins))
     down = dict(zip(names, outs))
+    for _ in range(args.warmup):   # untimed: first transfers set up the transfer stream and host buffers
+        r.upload_many(up)
+        r.iterate()
+        r.download_many(down)
+    r.sync()
+    barrier()
+    t0 = time.perf_counter()
     for _ in range(ke):
         r.upload_many(up)
         r.iterate()

@@ -263,6 +263,14 @@ __device__ __forceinline__ void cfl_speeds(double G, double rho, double px, doub
     s[2] = fabs(pz * inv) + cs;
 }
 
+// Programmatic dependent launch: a pencil kernel launched with programmatic stream serialization may
+// be scheduled before the previous kernel of its stream has finished.  pdl_wait() blocks until that
+// kernel has completed and its memory is visible (a no-op for an ordinary launch); every read of data
+// another kernel wrote comes after it.  pdl_trigger() lets the next kernel be scheduled; a kernel
+// calls it at the start of its last stage, when every one of its CTAs is resident.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // Atomic max of a non-negative double through its bit pattern (NaN never reaches here).
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));

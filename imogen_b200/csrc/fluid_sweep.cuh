@@ -283,6 +283,7 @@ template <bool MHD, int CPT, bool FADE>
 __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, unsigned vblock) {
     using T = float;
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     if (a.tm->done || a.tm->error) return;
     __shared__ T part[2][MAX_WARPS][33];
     __shared__ double cflp[3][MAX_WARPS];
@@ -428,6 +429,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     }
     __syncthreads();
 
+    pdl_trigger();
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
     double m3[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -484,6 +486,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
 template <typename T, bool MHD, int CPT, bool FADE, bool CG, bool INIT>
 __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
     __shared__ T part[2][MAX_WARPS][33];   // per-warp column maxima (two freezing speeds; rows padded
                                            // so the lanes reading one column's warps hit distinct banks)
@@ -658,6 +661,7 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
         __syncthreads();
     }
 
+    pdl_trigger();
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
     double m3[3] = {0.0, 0.0, 0.0};
 #pragma unroll

@@ -172,6 +172,7 @@ struct ChainComp {
 template <typename T, int CPT, bool FADE, int NQC, bool CG, bool INIT>
 __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     if (a.tm->done || a.tm->error) return;
     Tile<T, CPT> tl;
     tl.init(a.sg, vblock);
@@ -429,6 +430,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
         }
         __syncthreads();
     }
+    pdl_trigger();
     // B_I = B_I - 2ff*(flux - flux.shift(X,-1))   (relaxingMagnet.m:49); F_I -> scratch for CT
 #pragma unroll
     for (int q = 0; q < NQC; ++q)
@@ -461,6 +463,7 @@ __host__ __device__ inline size_t ctcell_smem_bytes(int RC, int Wb) {
 template <typename T, int CPT, bool FADE, bool CG>
 __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
     if (a.tm->done || a.tm->error) return;
     Tile<T, CPT> tl;
     tl.init(a.sg, vblock);
@@ -551,6 +554,7 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
             halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, 1, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
         __syncthreads();
     }
+    pdl_trigger();
     T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
     const int e2 = a.I[1] - 1;
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);

@@ -6,6 +6,9 @@
 
 namespace img {
 
+// Launch configuration of a pencil kernel: the cluster shape, and for single-CTA pencils programmatic
+// stream serialization (the kernel may be scheduled while the previous kernel of the stream runs its
+// last stage; the kernel bodies wait for it with pdl_wait before reading anything it wrote).
 inline cudaLaunchConfig_t pencil_config(const PencilLaunch& L, cudaLaunchAttribute* attr) {
     cudaLaunchConfig_t lc{};
     lc.gridDim = dim3(L.grid_x, L.grid_y);
@@ -18,31 +21,26 @@ inline cudaLaunchConfig_t pencil_config(const PencilLaunch& L, cudaLaunchAttribu
     attr[0].val.clusterDim.z = 1;
     lc.attrs = attr;
     lc.numAttrs = 1;
+    if (L.cluster == 1) {
+        attr[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[1].val.programmaticStreamSerializationAllowed = 1;
+        lc.numAttrs = 2;
+    }
     return lc;
 }
 
 template <typename Args>
 cudaError_t launch_pencil_batch(void (*kern)(const Args*, const BlockMap*), const Args* args, const BlockMap* map,
                                 const PencilLaunch& L) {
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     cudaLaunchConfig_t lc = pencil_config(L, attr);
     return cudaLaunchKernelEx(&lc, kern, args, map);
 }
 
 template <typename Args>
 cudaError_t launch_pencil(void (*kern)(const Args), const Args& a, const PencilLaunch& L) {
-    cudaLaunchConfig_t lc{};
-    lc.gridDim = dim3(L.grid_x, L.grid_y);
-    lc.blockDim = dim3(L.block);
-    lc.dynamicSmemBytes = L.smem;
-    lc.stream = L.stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = L.cluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    lc.attrs = attr;
-    lc.numAttrs = 1;
+    cudaLaunchAttribute attr[2];
+    cudaLaunchConfig_t lc = pencil_config(L, attr);
     return cudaLaunchKernelEx(&lc, kern, a);
 }
 
