@@ -7,9 +7,12 @@
 // arrays of each variable are synthesised in the same pass.  The state is read once and written
 // once; the only other HBM traffic is the stored edges of stateful boundaries (trans, wall).
 //
-// Shared memory: two sets of ten halo'd flux arrays (R and L of the five variables) -- set A holds
-// the predictor fluxes and then the corrector fluxes, set B the half-step state and then the limited
-// corrector fluxes -- plus the fade anchors of the ten arrays of the current stage.
+// Two kernel bodies.  The general one (halo jobs, FP64 copy ghosts, first sweeps): shared memory holds
+// two sets of ten halo'd flux arrays (R and L of the five variables) -- set A the predictor fluxes
+// and then the corrector fluxes, set B the half-step state and then the limited corrector fluxes --
+// plus the fade anchors of the ten arrays of the current stage.  The mixed copy-ghost one
+// (fluid_sweep_body_mixed_cg): two cell-major sets of the state and its flux numerators, three
+// barriers per sweep (see there).
 #pragma once
 
 #include "pencil.cuh"

@@ -7,10 +7,12 @@
 // so global loads/stores are coalesced along x for every sweep direction.
 //
 // Stencil operands live in shared-memory arrays with HALO rows: local row 0 is the row below the
-// CTA's first row, local rows RC+1 and RC+2 the two rows above its last row (layout: Tile::rs/cs).  Between stages a few
-// threads fill the halos -- the neighbouring cluster rank's edge rows (read through DSMEM), or, at
-// the pencil ends, the boundary-condition ghost of the reference's shift (shifting/*_shift.m),
-// stateful edge drift included -- so every stencil read is one unconditional shared load.
+// CTA's first row, local rows RC+1 and RC+2 the two rows above its last row (layout: Tile::rs/cs).
+// Between stages a few threads fill the halos -- the neighbouring cluster rank's edge rows (read
+// through DSMEM), or, at the pencil ends, the boundary-condition ghost of the reference's shift
+// (shifting/*_shift.m), stateful edge drift included -- so every stencil read is one unconditional
+// shared load.  Single-CTA pencils with circ, const or fade shifts skip the halos: their ghosts copy
+// an own row, which the reader indexes directly (the copy-ghost kernel variants).
 #pragma once
 
 #include "common.cuh"
