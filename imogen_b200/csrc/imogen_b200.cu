@@ -163,7 +163,8 @@ struct img_ctx {
     bool cfl_valid = false;     // DevTime.maxbits hold the CFL maxima of the current state
     int iteration = 1;
     int iters_base = 0;
-    PencilCfg pcfg[2][3];        // pencil tiling per kernel family (0 fluid, 1 magnet) and direction
+    PencilCfg pcfg[3][3];        // pencil tiling per kernel (0 fluid sweep, 1 magnet chain, 2 magnet CT) and
+                                 // direction; the public magnet tiling sets 1 and 2, the autotuner tunes 2 alone
     // one captured iteration per (cfl_valid at its start, sweep-order row (iteration-1) % 6)
     cudaGraphExec_t graphs[2][6] = {};
     uint64_t graph_launches[2][6] = {};
@@ -581,12 +582,17 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     fill_mag_args<T>(ctx, X, I1, I2, a);
     const int d = X - 1;
     const PencilCfg& pcf = ctx->pcfg[1][d];
+    const PencilCfg& pcc = ctx->pcfg[2][d];   // the CT pass has a tiling of its own
+    MagArgs ac = a;
+    ac.sg = sweep_geom(ctx, d, pcc);
     PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
                                       2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
-    PencilLaunch Lc = pencil_launch<T>(ctx, pcf, d, ctcell_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
+    PencilLaunch Lc = pencil_launch<T>(ctx, pcc, d, ctcell_smem_bytes<T>(pcc.G * pcc.cpt, pcc.Wb), 1,
                                        fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
     // copy ghosts: single-CTA pencils with circ, const or fade mag-class shifts along X
-    L.cg = Lc.cg = pcf.CL == 1 && copy_ghost_mode(a.modeX[0]) && copy_ghost_mode(a.modeX[1]);
+    const bool cg_modes = copy_ghost_mode(a.modeX[0]) && copy_ghost_mode(a.modeX[1]);
+    L.cg = pcf.CL == 1 && cg_modes;
+    Lc.cg = pcc.CL == 1 && cg_modes;
     L.init = a.init_mag[0] || a.init_mag[1];   // first sweep of (I, X): the stored-edge capturing chain
     if (ctx->rec) {
         OpRec r{};
@@ -597,6 +603,7 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
         ctx->rec->push_back(r);
         r.kind = OP_CTCELL;
         r.L = Lc;
+        r.ma = ac;
         ctx->rec->push_back(r);
         ctx->init_mag[I1 - 1][d] = false;
         ctx->init_mag[I2 - 1][d] = false;
@@ -606,7 +613,7 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet chain launch (dim %d, grid %u x 2, block %u, smem %zu, cluster %d): %s", d,
                     L.grid_x, L.block, L.smem, L.cluster, cudaGetErrorString(le));
-    le = launch_mag_ctcell<T>(a, Lc);
+    le = launch_mag_ctcell<T>(ac, Lc);
     if (le != cudaSuccess)
         return fail(ctx, IMG_ERR_CUDA, "magnet CT launch (dim %d, grid %u, block %u, smem %zu, cluster %d): %s", d,
                     Lc.grid_x, Lc.block, Lc.smem, Lc.cluster, cudaGetErrorString(le));
@@ -661,7 +668,7 @@ int set_kernel_attributes(img_ctx* ctx) {
             dn = true;
         }
     }
-    for (int kind = 0; kind < 2; ++kind)
+    for (int kind = 0; kind < 3; ++kind)
         for (int d = 0; d < 3; ++d) {
             const PencilCfg& p = ctx->pcfg[kind][d];
             if (ctx->g.n[d] < 3) continue;
@@ -882,7 +889,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     g.s[1] = g.n[0];
     g.s[2] = (long long)g.n[0] * g.n[1];
     g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
-    for (int kind = 0; kind < 2; ++kind)
+    for (int kind = 0; kind < 3; ++kind)
         for (int d = 0; d < 3; ++d) {
             ctx->pcfg[kind][d] = choose_pencil(g, d, ctx->elem);
             std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -1956,9 +1963,10 @@ int img_autotune(img_ctx* ctx, int trials) {
     if (cudaMemcpyAsync(backup, ctx->slab, ctx->slab_bytes, cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
         cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
         rc = fail(ctx, IMG_ERR_CUDA, "autotune setup failed");
-    // each kernel family is tuned on its own sweeps: the fluid sweep for the fluid tiling, the
-    // magnet sweep (chain + CT) for the magnet tiling
-    for (int kind = 0; kind < 2 && rc == IMG_OK; ++kind) {
+    // each kernel is tuned on its own sweeps: the fluid sweep for the fluid tiling, the magnet sweep
+    // for the chain's tiling (the CT on its current one), then the magnet sweep for the CT's tiling
+    // with the chain's chosen
+    for (int kind = 0; kind < 3 && rc == IMG_OK; ++kind) {
         if (kind == 0 ? !ctx->cfg.fluid_active : !ctx->cfg.magnet_active) continue;
         for (int d = 0; d < 3 && rc == IMG_OK; ++d) {
             if (ctx->g.n[d] < 3) continue;
@@ -2040,6 +2048,7 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]) {
             return fail(ctx, IMG_ERR_UNSUPPORTED, "tiling cannot be scheduled on this device");
         }
         ctx->pcfg[kind][d] = c;
+        if (kind == 1) ctx->pcfg[2][d] = c;   // the public magnet tiling is the chain's and the CT's
         drop_graphs(ctx);
         return IMG_OK;
     }

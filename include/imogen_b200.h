@@ -153,16 +153,18 @@ size_t img_bytes_required(const img_config* cfg);
 int img_get_stream(img_ctx* ctx, void** stream);
 
 /* Autotuner: time every pencil tiling the kernels accept (cells per thread, CTA shape, cluster
- * size) for each swept direction and kernel family (fluid sweep; magnet chain) on this context's
- * own state, `trials` sweeps each, keep the fastest, and remember it for later contexts of the
- * same shape.  The state, stored edges and clock are restored afterwards.  Needs a temporary
- * device copy of the context.  No reference counterpart. */
+ * size) for each swept direction and kernel (fluid sweep; magnet chain; magnet CT pass) on this
+ * context's own state, `trials` sweeps each, keep the fastest, and remember it for later contexts
+ * of the same shape.  The state, stored edges and clock are restored afterwards.  Needs a
+ * temporary device copy of the context.  No reference counterpart. */
 int img_autotune(img_ctx* ctx, int trials);
-/* Tiling of slot dim: 1..3 the fluid sweeps along x, y, z, 4..6 the magnet sweeps along x, y, z;
+/* Tiling of slot dim: 1..3 the fluid sweeps along x, y, z, 4..6 the magnet chain along x, y, z
+ * (after img_autotune the magnet CT pass may run on a tiling of its own);
  * out = {pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread,
  * transverse components per CTA (magnet: 1 or 2; fluid: 1)}. */
 int img_get_tiling(const img_ctx* ctx, int dim, int out[6]);
-/* Set the tiling of slot dim to one of those the autotuner may pick (same field order). */
+/* Set the tiling of slot dim to one of those the autotuner may pick (same field order); a magnet
+ * slot sets the chain's and the CT pass's tiling. */
 int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]);
 
 /* Number of kernels the context has launched so far.  No reference counterpart. */
