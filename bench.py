@@ -323,6 +323,7 @@ def run_ours(args):
     el = time.perf_counter() - t0
     e2e = {"value": ncell * 2 * ke / el, "unit": "zone-updates/s",
            "h2d_bytes_per_step": 8 * ncell * 8, "d2h_bytes_per_step": 8 * ncell * 8,
+           "pcie_bytes_per_step_each_way": 8 * ncell * 4,   # FP32: the library converts on the host
            "form": "mixed", "steps": ke}
 
     kh = run_kh(args, timed_steps, measured_hbm_peak()[0]) if args.kh > 0 else None
