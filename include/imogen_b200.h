@@ -84,7 +84,9 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
 int img_upload(img_ctx* ctx, int var_id, const double* host, size_t n);
 int img_download(img_ctx* ctx, int var_id, double* host, size_t n);
 /* The same for several variables with one synchronisation at the end (hosts[i] holds n values of
- * variable var_ids[i]); the transfers are queued back to back on the context's stream. */
+ * variable var_ids[i]).  Mixed form: FP32 crosses PCIe; the values are rounded (IEEE
+ * round-to-nearest, as the single-array calls do on the device) or widened on a small pool of host
+ * threads, and the copy of one array overlaps the conversion of the next. */
 int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* const* hosts, size_t n);
 int img_download_many(img_ctx* ctx, int count, const int* var_ids, double* const* hosts, size_t n);
 
