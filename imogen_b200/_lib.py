@@ -25,7 +25,7 @@ SYMBOLS = (
     "img_time_update", "img_flux", "img_fluid_sweep", "img_magnet_sweep", "img_step", "img_run",
     "img_get_time", "img_set_time", "img_progress", "img_checkpoint_bytes", "img_checkpoint_save",
     "img_checkpoint_load", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
-    "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count",
+    "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count", "img_sweep_order",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -113,6 +113,8 @@ def lib():
     L.img_set_tiling.argtypes = [vp, ctypes.c_int, ip]
     L.img_set_tiling.restype = ctypes.c_int
     L.img_launch_count.restype = ctypes.c_int
+    L.img_sweep_order.argtypes = [ctypes.c_int, ctypes.c_int, ip]
+    L.img_sweep_order.restype = ctypes.c_int
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]
     L.img_batch_add.argtypes = [vp, vp]

@@ -29,8 +29,12 @@ using namespace img;
 
 namespace {
 
-// flux.m:17-27 -- perms([1 2 3]) in reverse-lexicographic order; backward rows are reversed.
-const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1, 2, 3}};
+// flux.m:17-27 -- sweep order rows: FWD = perms([1 2 3]), BWD = perms([3 2 1]) as MATLAB
+// R2009a-R2010b returns them.  That perms permutes positions and then indexes V (perms(V) = V(P)),
+// with P = perms(1:3) = 321, 312, 231, 213, 123, 132 (its recursive relabelling leaves the last two
+// rows out of reverse-lexicographic order); so BWD = 4 - FWD, row by row.
+const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 2, 3}, {1, 3, 2}};
+const int BWD[6][3] = {{1, 2, 3}, {1, 3, 2}, {2, 1, 3}, {2, 3, 1}, {3, 2, 1}, {3, 1, 2}};
 const int FWD_MI[3][2] = {{2, 3}, {1, 3}, {1, 2}};
 const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
 
@@ -698,11 +702,11 @@ int do_flux(img_ctx* ctx, int order, bool fuse_cfl) {
     int row = (ctx->iteration - 1) % 6;
     int last_fluid = -1;
     for (int q = 0; q < 3; ++q) {
-        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        int X = order > 0 ? FWD[row][q] : BWD[row][q];
         if (ctx->g.n[X - 1] >= 3) last_fluid = q;
     }
     for (int q = 0; q < 3; ++q) {
-        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        int X = order > 0 ? FWD[row][q] : BWD[row][q];
         if (ctx->g.n[X - 1] < 3) continue;
         bool cfl_here = fuse_cfl && order < 0 && q == last_fluid && c.fluid_active;
         int rc;
@@ -1864,10 +1868,10 @@ int img_batch_launch_count(const img_batch* b, uint64_t* count) {
 // ---- totals with static scratch -------------------------------------------------------------------
 // img_totals_static works in a file-scope device array instead of the context's slab: the 1023
 // per-block partial pairs (sum, compensation) of 8 variables, the 8 results and the 8-entry pointer
-// table, 128.2 KiB in all, whatever the grid size (the reduction is a grid-stride loop over a fixed
-// 1023 blocks).  Every call overwrites every slot it later reads, so nothing must start at zero.
-// All contexts of a device share the one array: calls that overlap in time (other threads, other
-// streams) race on it and must be serialised by the caller.
+// table: 2*8*1023 + 8 + 8 = 16384 doubles, 128 KiB exactly, whatever the grid size (the reduction is
+// a grid-stride loop over a fixed 1023 blocks).  Every call overwrites every slot it later reads, so
+// nothing must start at zero.  All contexts of a device share the one array: calls that overlap in
+// time (other threads, other streams) race on it and must be serialised by the caller.
 namespace {
 constexpr int kStaticTotalsBlocks = 1023;
 constexpr size_t kStaticTotalsPartial = 2 * 8 * kStaticTotalsBlocks;
@@ -1876,10 +1880,10 @@ constexpr int kMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) double g_static_totals[kStaticTotalsDoubles];
+static_assert(sizeof(g_static_totals) == 128 * 1024, "static totals scratch is 128 KiB");
 
-// Address of g_static_totals on device `dev` (the current device), looked up once per device.  The
-// first call on a device must come before any stream capture that includes this entry point: the
-// lookup may load the module.
+// Address of g_static_totals on the current device, looked up once per device.  The lookup may load
+// the module, so the first call on a device should come before any stream capture begins.
 static int static_totals_scratch(img_ctx* ctx, double** out) {
     static std::mutex mu;
     static double* addr[kMaxDevices] = {};
@@ -2064,6 +2068,13 @@ int img_get_tiling(const img_ctx* ctx, int dim, int out[6]) {
     out[3] = p.NT;
     out[4] = p.cpt;
     out[5] = p.nqc;
+    return IMG_OK;
+}
+
+int img_sweep_order(int order, int iteration, int out[3]) {
+    if (!out || (order != 1 && order != -1) || iteration < 1) return IMG_ERR_ARG;
+    const int row = (iteration - 1) % 6;
+    for (int q = 0; q < 3; ++q) out[q] = order > 0 ? FWD[row][q] : BWD[row][q];
     return IMG_OK;
 }
 

@@ -52,7 +52,7 @@ def orszag_tang(n=512, gamma=5 / 3, time_max=0.5, cfl=0.35):
     return settings, (r(rho), mom.reshape((3,) + grid), r(ener), mag.reshape((3,) + grid))
 
 
-def kelvin_helmholtz(n=256, gamma=5 / 3, seed=0, iter_max=100):
+def kelvin_helmholtz(n=256, gamma=5 / 3, seed=0, iter_max=200):
     """3-D MHD Kelvin-Helmholtz on [0,1)^3, periodic: rho=2, vx=+0.5 for |y|<0.25 else rho=1,
     vx=-0.5; P=2.5; Bx=0.1; vy = 0.01*U(-1,1) inside the layer (PCG64(seed))."""
     grid = (n, n, n)
@@ -72,7 +72,9 @@ def kelvin_helmholtz(n=256, gamma=5 / 3, seed=0, iter_max=100):
 
 def brio_wu_tube(n, rho_l, rho_r, p_l, p_r, gamma=2.0, time_max=0.1, width=3):
     """One Brio-Wu-type MHD tube on an n x width x width grid: Bx = 0.75, By = +1 | -1.
-    x: const BCs; y, z: periodic (uniform), so the Y/Z sweeps carry the v_y B_x induction."""
+    x: fade BCs, as the reference's magnetic shock tube sets them
+    (experiment/MagneticShockTube/MagneticShockTubeInitializer.m:52); y, z: periodic (uniform), so
+    the Y/Z sweeps carry the v_y B_x induction."""
     grid = (n, width, width)
     x = _centres(n)[:, None, None] * np.ones(grid)
     left = x < 0.5
@@ -81,7 +83,7 @@ def brio_wu_tube(n, rho_l, rho_r, p_l, p_r, gamma=2.0, time_max=0.1, width=3):
     mom = np.zeros((3,) + grid)
     mag = np.stack([np.full(grid, 0.75), np.where(left, 1.0, -1.0), np.zeros(grid)])
     ener = P / (gamma - 1) + 0.5 * (mag ** 2).sum(0)
-    bc = {"x": "const", "y": "circ", "z": "circ"}
+    bc = {"x": "fade", "y": "circ", "z": "circ"}
     settings = dict(grid=grid, dgrid=(1.0 / n, 1.0 / n, 1.0 / n), gamma=gamma, cfl=0.35, bc=bc,
                     limiter="vanleer", magnet=True, time_max=time_max, iter_max=10 ** 7)
     return settings, (rho, mom, ener, mag)

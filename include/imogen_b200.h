@@ -3,8 +3,7 @@
  *
  * Plain C: opaque context handles, host pointers and sizes, int status codes.  No exception or
  * C++/torch type crosses this boundary.  Every entry point replaces one piece of the reference's
- * MATLAB call surface (paths are relative to the reference project root); the MEX gateway that a
- * MATLAB caller binds is shown in INTEGRATION.md.
+ * MATLAB call surface (paths are relative to the reference project root).
  *
  * Threading: a context is used by one host thread at a time.  All work of a context is issued on
  * its own CUDA stream; state stays resident on the device between calls.
@@ -97,6 +96,11 @@ int img_time_update(img_ctx* ctx, int flux_direction, double* dt_out, int* dir_o
 /* flux(run, mass, mom, ener, mag, grav, order) (flux/flux.m:1-64) at the current iteration. */
 int img_flux(img_ctx* ctx, int order);
 
+/* directVec of flux.m:17-27: the three sweep dimensions (1-based, in sweep order) that img_flux uses
+ * at 1-based `iteration` for order +1 (perms([1 2 3])) or -1 (perms([3 2 1])), with MATLAB
+ * R2009a-R2010b's perms.  Host only; no device work. */
+int img_sweep_order(int order, int iteration, int out[3]);
+
 /* relaxingFluid(run, mass, mom, ener, mag, grav, X) (fluid/relaxingFluid.m:1) -- one sweep. */
 int img_fluid_sweep(img_ctx* ctx, int X);
 
@@ -132,13 +136,17 @@ int img_checkpoint_load(img_ctx* ctx, const void* host, size_t bytes);
 /* Compensated (Neumaier) FP64 totals of rho, px, py, pz, E, Bx, By, Bz over the grid. */
 int img_totals(img_ctx* ctx, double out[8]);
 
-/* The same totals as img_totals, bit for bit, computed without allocating anything: the scratch is a
- * file-scope device array of 128.2 KiB (1023 per-block partial pairs of 8 variables, the 8 results and
- * an 8-entry pointer table), looked up once per device with cudaGetSymbolAddress; grids of any size.
- * The first call on a device should come before any stream capture.  Every call overwrites all the
- * scratch it reads, so nothing needs to start at zero.  All contexts of a device share that scratch:
- * calls that overlap in time race on it and must be serialised by the caller.  The context's device
- * must be current.  No counterpart in the reference. */
+/* The same totals as img_totals, bit for bit, computed without allocating anything, for callers
+ * that may not call cudaMalloc (a MEX call whose device memory belongs to the MATLAB session's
+ * allocator, or a host that has fixed its device footprint up front).  The scratch is a file-scope
+ * device array of 128 KiB (16384 doubles: 1023 per-block partial pairs of 8 variables, the 8 results
+ * and an 8-entry pointer table), looked up once per device with cudaGetSymbolAddress; grids of any
+ * size.  The first call on a device does that lookup and should come before any stream capture
+ * begins.  Each call copies the pointer table from the host, synchronises the context's stream and
+ * copies the 8 results to `out` before it returns.  Every call overwrites all the scratch it reads,
+ * so nothing needs to start at zero.  All contexts of a device share that scratch: calls that
+ * overlap in time race on it and must be serialised by the caller.  The context's device must be
+ * current.  No counterpart in the reference. */
 int img_totals_static(img_ctx* ctx, double out[8]);
 
 /* Block until the context's stream is idle; returns a pending device error if any. */

@@ -50,6 +50,7 @@ def lib():
         L.orc_get_cfl.argtypes = [ctypes.c_void_p, dp, ip]
         L.orc_pchip.argtypes = [dp, ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_sweep_order.argtypes = [ctypes.c_int, ctypes.c_int, ip]
         L.orc_max_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -83,6 +84,13 @@ def pchip(x, y, xi):
     out = np.zeros((y.shape[0], xi.size))
     lib().orc_pchip(_dp(x), x.size, _dp(y), y.shape[0], _dp(xi), xi.size, _dp(out))
     return out
+
+
+def sweep_order(order, iteration):
+    """directVec of flux.m:17-27 as the C++ oracle's tables hold it."""
+    out = np.zeros(3, np.int32)
+    lib().orc_sweep_order(int(order), int(iteration), _ip(out))
+    return tuple(int(v) for v in out)
 
 
 def set_threads(n):

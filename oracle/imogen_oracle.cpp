@@ -11,8 +11,8 @@
 // depend on the thread count (no reductions other than max, which is exact).
 //
 // Parity against the MATLAB reference itself is unpinned (MATLAB/Octave are not available); the
-// MATLAB builtins it depends on are pinned separately (pchip vs SciPy, perms order by its
-// documented reverse-lexicographic order).
+// MATLAB builtins it depends on are pinned separately (pchip vs SciPy; the perms tables below
+// against oracle/np_oracle.py's restatement of the R2009-era perms algorithm).
 
 #include <algorithm>
 #include <cmath>
@@ -35,8 +35,13 @@ enum Cls { C_MASS = 0, C_MOM = 1, C_ENER = 2, C_MAG = 3 };
 
 using Vec = std::vector<double>;
 
-// flux.m:17-27 -- perms([1 2 3]) rows (reverse lexicographic) and the matching magnet indices.
-const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 3, 2}, {1, 2, 3}};
+// flux.m:17-27 -- the sweep order rows and the matching magnet indices.  FWD = perms([1 2 3]) and
+// BWD = perms([3 2 1]) as MATLAB R2009a-R2010b computes them: perms(V) = V(P) over the position
+// permutations P = perms(1:3) = 321, 312, 231, 213, 123, 132 (recursive construction with the
+// relabelling t(t == i) = n, which leaves the last two rows out of reverse-lexicographic order), so
+// BWD = 4 - FWD row by row.
+const int FWD[6][3] = {{3, 2, 1}, {3, 1, 2}, {2, 3, 1}, {2, 1, 3}, {1, 2, 3}, {1, 3, 2}};
+const int BWD[6][3] = {{1, 2, 3}, {1, 3, 2}, {2, 1, 3}, {2, 3, 1}, {3, 2, 1}, {3, 1, 2}};
 const int FWD_MI[3][2] = {{2, 3}, {1, 3}, {1, 2}};
 const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
 
@@ -578,7 +583,7 @@ void magnet_flux(Sim& s, int X, int I1, int I2) {
 void flux(Sim& s, int order) {
     int row = (s.iteration - 1) % 6;
     for (int q = 0; q < 3; ++q) {
-        int X = order > 0 ? FWD[row][q] : FWD[row][2 - q];
+        int X = order > 0 ? FWD[row][q] : BWD[row][q];
         if (s.n[X - 1] < 3) continue;
         if (order > 0) {
             if (s.fluid_active) relaxing_fluid(s, X);
@@ -749,6 +754,12 @@ void orc_set_time(void* p, double time, double dt, int iteration) {
 void orc_get_cfl(void* p, double* cmax, int* grid_index) {
     Sim& s = *static_cast<Sim*>(p);
     *cmax = s.last_cmax; *grid_index = s.last_grid_index;
+}
+
+// directVec of flux.m:17-27 for an iteration (1-based) and order (+1 forward, -1 backward).
+void orc_sweep_order(int order, int iteration, int out[3]) {
+    const int row = (iteration - 1) % 6;
+    for (int q = 0; q < 3; ++q) out[q] = order > 0 ? FWD[row][q] : BWD[row][q];
 }
 
 int orc_pchip(const double* x, int n, const double* y, int ncols, const double* xi, int m, double* out) {

@@ -19,7 +19,8 @@ statement can be read against the file it follows:
 
 Parity status: the reference is MATLAB and cannot run here, so this oracle is pinned only at
 the MATLAB-builtin boundary (``pchip`` against SciPy's PchipInterpolator, the ``perms`` row
-order by its documented reverse-lexicographic order) and by analytic / invariant checks
+order by a restatement of the R2009-era ``perms`` algorithm, ``matlab_perms``) and by analytic /
+invariant checks
 (exact Sod Riemann solution, conservation under periodic BCs, discrete div B under CT).
 Parity against the reference itself is therefore *unpinned*.
 
@@ -35,10 +36,34 @@ BC_MODES = (CIRC, CONST, FADE, MIRROR, TRANS, WALL)
 VANLEER, SUPERBEE, MINMOD = "vanleer", "superbee", "minmond"   # FluxLimiterEnum.m:10-13
 PER_STEP, PER_ITERATION = 0, 1                                  # enums/ENUM.m:33-34
 
-# perms([1 2 3]) in MATLAB's reverse-lexicographic order (flux.m:19); the backward table
-# perms([3 2 1]) is each row reversed (flux.m:25).
-FORWARD_ORDER = ((3, 2, 1), (3, 1, 2), (2, 3, 1), (2, 1, 3), (1, 3, 2), (1, 2, 3))
-BACKWARD_ORDER = tuple(tuple(reversed(r)) for r in FORWARD_ORDER)
+
+
+def perms_positions(n):
+    """Rows of ``perms(1:n)`` as MATLAB R2009a-R2010b builds them (the releases the reference
+    targets).  Recursive on n: the first m = (n-1)! rows are ``[n, perms(1:n-1)]``; then, for
+    i = n-1 down to 1, the next m rows are ``[i, q']`` where q' is ``perms(1:n-1)`` with the
+    value i relabelled to n (``t(t == i) = n``).  The relabelling is monotone only for
+    i = n-1, so the rows are not strictly reverse-lexicographic: for n = 3 they are
+    321, 312, 231, 213, 123, 132."""
+    if n <= 1:
+        return ((1,),) if n == 1 else ((),)
+    q = perms_positions(n - 1)
+    rows = [(n,) + r for r in q]
+    for i in range(n - 1, 0, -1):
+        rows += [(i,) + tuple(n if t == i else t for t in r) for r in q]
+    return tuple(rows)
+
+
+def matlab_perms(v):
+    """``perms(V)`` of that era: ``V(P)`` with P = ``perms_positions(numel(V))`` (the permutations
+    are of positions, then applied to V, so ``perms([3 2 1])`` is ``4 - perms(1:3)``)."""
+    return tuple(tuple(v[i - 1] for i in row) for row in perms_positions(len(v)))
+
+
+# flux.m:19 and flux.m:24: the forward rows are perms([1 2 3]), the backward rows perms([3 2 1]);
+# row mod(iteration-1, 6)+1 is used (flux.m:20,25).
+FORWARD_ORDER = matlab_perms((1, 2, 3))
+BACKWARD_ORDER = matlab_perms((3, 2, 1))
 FORWARD_MAGIDX = {1: (2, 3), 2: (1, 3), 3: (1, 2)}     # flux.m:21
 BACKWARD_MAGIDX = {1: (3, 2), 2: (3, 1), 3: (2, 1)}    # flux.m:27
 

@@ -27,6 +27,18 @@ def test_library_exports_every_declared_symbol():
     assert set(syms) == set(_lib.SYMBOLS)
 
 
+def test_sweep_order_table_matches_the_oracle():
+    """img_sweep_order (host only) returns the same directVec rows as both oracles (flux.m:17-27)."""
+    from oracle import np_oracle
+    L = _lib.lib()
+    out = (ctypes.c_int * 3)()
+    for it in range(1, 14):
+        for order, table in ((1, np_oracle.FORWARD_ORDER), (-1, np_oracle.BACKWARD_ORDER)):
+            assert L.img_sweep_order(order, it, out) == 0
+            assert tuple(out) == table[(it - 1) % 6]
+    assert L.img_sweep_order(0, 1, out) == -1
+
+
 def test_create_rejects_settings_the_reference_cannot_run():
     L = _lib.lib()
     for kw, code in [(dict(grid=(32, 1, 1), bc="mirror"), -4), (dict(grid=(19, 32, 1), bc="fade"), -4)]:

@@ -37,10 +37,45 @@ def test_fade_coefficients_match_scipy():
         assert np.allclose(np_oracle.fade_coefficients(f), ref, rtol=1e-12, atol=1e-15)
 
 
+# flux.m:19,24 under MATLAB R2009a-R2010b: perms(V) = V(P) with P = perms(1:3) built recursively by
+# relabelling (t(t == i) = n), written out by hand so the tables can be checked without MATLAB.
+FORWARD_ROWS = ((3, 2, 1), (3, 1, 2), (2, 3, 1), (2, 1, 3), (1, 2, 3), (1, 3, 2))
+BACKWARD_ROWS = ((1, 2, 3), (1, 3, 2), (2, 1, 3), (2, 3, 1), (3, 2, 1), (3, 1, 2))
+
+
 def test_perms_order():
-    # MATLAB perms returns rows in reverse lexicographic order (flux.m:19,25)
-    assert np_oracle.FORWARD_ORDER == tuple(sorted(itertools.permutations((1, 2, 3)), reverse=True))
-    assert all(b == tuple(reversed(f)) for f, b in zip(np_oracle.FORWARD_ORDER, np_oracle.BACKWARD_ORDER))
+    assert np_oracle.perms_positions(3) == FORWARD_ROWS
+    assert np_oracle.FORWARD_ORDER == FORWARD_ROWS
+    assert np_oracle.BACKWARD_ORDER == BACKWARD_ROWS
+    # perms([3 2 1]) indexes V = [3 2 1] with the position permutations: 4 - P row by row
+    for f, b in zip(np_oracle.FORWARD_ORDER, np_oracle.BACKWARD_ORDER):
+        assert b == tuple((3, 2, 1)[i - 1] for i in f) == tuple(4 - i for i in f)
+    # perms(1:2) = [2 1; 1 2]; every row of perms(1:4) is a permutation and all 24 appear once
+    assert np_oracle.perms_positions(2) == ((2, 1), (1, 2))
+    p4 = np_oracle.perms_positions(4)
+    assert len(set(p4)) == 24 and set(p4) == set(itertools.permutations((1, 2, 3, 4)))
+    # the C++ oracle's tables are the same rows, and row mod(iteration-1, 6)+1 is used
+    for it in range(1, 14):
+        assert cpp_oracle.sweep_order(1, it) == FORWARD_ROWS[(it - 1) % 6]
+        assert cpp_oracle.sweep_order(-1, it) == BACKWARD_ROWS[(it - 1) % 6]
+
+
+def test_sweep_order_changes_two_dimensional_results(monkeypatch):
+    """The order table is observable: on a 2-D Orszag-Tang grid, running the backward half-steps
+    with each forward row reversed (a wrong reading of perms([3 2 1])) moves the state far beyond
+    the 1e-10 parity bar within one cycle of the table.  The mistake is planted in the oracle."""
+    s, st = problems.orszag_tang(32, time_max=1.0)
+    kw = problems.oracle_kwargs(dict(s, iter_max=6))
+    good = np_oracle.Sim(**kw)
+    good.set_state(*st)
+    good.run()
+    monkeypatch.setattr(np_oracle, "BACKWARD_ORDER", tuple(tuple(reversed(r)) for r in FORWARD_ROWS))
+    bad = np_oracle.Sim(**kw)
+    bad.set_state(*st)
+    bad.run()
+    a, b = good.state(), bad.state()
+    rel = np.abs(a["mass"] - b["mass"]).sum() / np.abs(a["mass"]).sum()
+    assert rel > 1e-8, rel
 
 
 @pytest.mark.parametrize("bc", ["circ", "const", "mirror", "trans", "wall", "fade"])
@@ -49,7 +84,7 @@ def test_numpy_and_cpp_oracles_bitwise(bc, grid, mhd):
     spec = {f: (bc if not ((bc == "mirror" and grid[d] < 2) or (bc == "fade" and grid[d] < 20)) else "circ")
             for d, f in enumerate("xyz")}
     s = dict(grid=grid, dgrid=tuple(1 / g for g in grid), gamma=5 / 3, cfl=0.35, bc=spec,
-             limiter=("vanleer", "minmod", "superbee"), magnet=mhd, iter_max=3)
+             limiter=("vanleer", "minmod", "superbee"), magnet=mhd, iter_max=7)
     kw = problems.oracle_kwargs(s)
     st = smooth_state(grid, seed=5, mhd=mhd)
     a = np_oracle.Sim(**kw)

@@ -20,9 +20,12 @@ def _run(n, precision, iters):
     return g
 
 
+# 48^2 fits in one pass of the fixed 1023 x 256-thread grid; 528^2 = 278784 cells does not, so the
+# grid-stride loop and every block's partials carry data
+@pytest.mark.parametrize("n", [48, 528])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_static_totals_match_two_calls_in_a_row(precision):
-    g = _run(48, precision, 3)
+def test_static_totals_match_two_calls_in_a_row(precision, n):
+    g = _run(n, precision, 3)
     try:
         ref1, ref2 = g.totals(), g.totals()
         got1, got2 = g.totals_static(), g.totals_static()
