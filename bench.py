@@ -290,7 +290,8 @@ def run_ours(args):
         alg = ncell * (8 + 5) * w     # reads rho,p,E,cellB (8 words), writes rho,p,E (5 words)
         roof[prec] = {"bound": "hbm", "achieved": alg / per / 1e9, "peak": peak, "unit": "GB/s",
                       "frac": alg / per / 1e9 / peak, "traffic": traffic if prec == "mixed" else None,
-                      "traffic_source": "profiles/pencil_kernels_orszag_tang_512_mixed.md (ncu capture)"
+                      "traffic_source": "static figure from the ncu capture committed in "
+                                        "profiles/pencil_kernels_orszag_tang_512_mixed.md (not measured in this run)"
                       if prec == "mixed" and traffic else None, "kernel": "fluid_sweep_kernel X",
                       "launch_us": per * 1e6, "alg_bytes": alg, "peak_kind": peak_kind}
 
@@ -327,6 +328,7 @@ def run_ours(args):
            "form": "mixed", "steps": ke}
 
     kh = run_kh(args, timed_steps, measured_hbm_peak()[0]) if args.kh > 0 else None
+    accuracy = run_accuracy(args) if args.accuracy and rank == 0 else None
     serving = run_serving(args) if args.serve_jobs > 0 else None
     ensemble = run_ensemble(args, timed_steps) if args.ensemble > 0 else None
 
@@ -347,6 +349,8 @@ def run_ours(args):
             "mixed_over_fp64": v / v64,
             "l1_mixed_vs_fp64": l1,
             "l1_mixed_vs_fp64_max": max(l1.values()),
+            "l1_mixed_vs_fp64_after": f"{args.warmup + 1 + args.steps} iterations (plus autotuner trials)",
+            "accuracy_t_end": accuracy,
             "roofline": roof["mixed"],
             "roofline_fp64": roof["fp64"],
             "gpu_launches": launches["mixed"],
@@ -366,6 +370,51 @@ def run_ours(args):
         r.close()
     if ws > 1:
         torch.distributed.destroy_process_group()
+
+
+def div_b_rel(mag, dgrid):
+    """max |div B| * dx / max |B| of the face-centred field (B_d(i) on face i-1/2), periodic grid."""
+    div = np.zeros(mag.shape[1:])
+    for d in range(3):
+        if mag.shape[1 + d] > 1:
+            div += (np.roll(mag[d], -1, axis=d) - mag[d]) / dgrid[d]
+    bmax = float(np.abs(mag).max())
+    return float(np.abs(div).max() * min(dgrid[d] for d in range(3) if mag.shape[1 + d] > 1) / bmax) if bmax else 0.0
+
+
+def run_accuracy(args):
+    """The mixed form's acceptance point: Orszag-Tang 512^2 run to t = 0.5 in both forms (outside any
+    timed region); relative L1 of the mixed state against the FP64 state per variable (rho, E; momentum
+    and B per component and as vectors), the discrete div B of both, and their compensated totals."""
+    from imogen_b200 import ImogenRun, problems
+    s, st = problems.orszag_tang(512, time_max=0.5)
+    out = {"workload": "orszag_tang_512x512_mhd", "t_end": 0.5}
+    states, tots = {}, {}
+    for prec in ("fp64", "mixed"):
+        r = ImogenRun(precision=prec, **s)
+        r.set_state(*st)
+        n = r.run()
+        t, _, _ = r.progress()
+        states[prec] = r.state()
+        tots[prec] = [float(v) for v in r.totals()]
+        out[f"iterations_{prec}"] = n
+        out[f"time_{prec}"] = t
+        r.close()
+    a, b = states["mixed"], states["fp64"]
+    rel = lambda x, y: float(np.abs(x - y).sum() / np.abs(y).sum())
+    l1 = {"rho": rel(a["mass"], b["mass"]), "E": rel(a["ener"], b["ener"]),
+          "momentum": rel(a["mom"], b["mom"]), "B": rel(a["mag"], b["mag"])}
+    for c in range(2):
+        l1[f"mom{'xyz'[c]}"] = rel(a["mom"][c], b["mom"][c])
+        l1[f"B{'xyz'[c]}"] = rel(a["mag"][c], b["mag"][c])
+    out["l1_at_t_end"] = l1
+    out["l1_at_t_end_max"] = max(l1.values())
+    out["divb"] = {"fp64": div_b_rel(b["mag"], s["dgrid"]), "mixed": div_b_rel(a["mag"], s["dgrid"]),
+                   "measure": "max|div B| * dx / max|B|"}
+    out["totals"] = {"order": "rho, px, py, pz, E, Bx, By, Bz", "fp64": tots["fp64"], "mixed": tots["mixed"],
+                     "initial": [float(v) for v in (st[0].sum(), *st[1].reshape(3, -1).sum(1), st[2].sum(),
+                                                    *st[3].reshape(3, -1).sum(1))]}
+    return out
 
 
 def run_kh(args, timed_steps, peak):
@@ -479,6 +528,8 @@ def main():
     ap.add_argument("--kh", type=int, default=256, help="edge of the 3-D Kelvin-Helmholtz leg (0: skip)")
     ap.add_argument("--serve-budget-gb", type=int, default=64)
     ap.add_argument("--ensemble", type=int, default=512, help="members of the batched-ensemble leg (0: skip)")
+    ap.add_argument("--no-accuracy", dest="accuracy", action="store_false",
+                    help="skip the Orszag-Tang run to t = 0.5 (mixed vs FP64 L1, div B, totals)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

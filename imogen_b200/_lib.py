@@ -47,6 +47,7 @@ class ImgConfig(ctypes.Structure):
         ("iter_max", ctypes.c_int),
         ("update_mode", ctypes.c_int),
         ("precision", ctypes.c_int),
+        ("nonfinite_check", ctypes.c_int),
     ]
 
 

@@ -15,7 +15,9 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu"]
+UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu", "fluid_cluster.cu"]
+# per-unit ptxas options: the batched cluster fluid kernels are compiled at -O1 (fluid_cluster.cu says why)
+UNIT_FLAGS = {"fluid_cluster.cu": ["-Xptxas", "-O1"]}
 OUT = os.path.join(HERE, "libimogen_b200.so")
 HEADER = os.path.join(ROOT, "include", "imogen_b200.h")
 
@@ -50,8 +52,8 @@ def build(force=False, verbose=False, extra=()):
     try:
         def compile_unit(unit):
             obj = os.path.join(tmp, unit.replace(".cu", ".o"))
-            cmd = [cc, *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, unit),
-                   "-o", obj, *extra]
+            cmd = [cc, *ARCH, *FLAGS, *UNIT_FLAGS.get(unit, []), "-I", os.path.join(ROOT, "include"), "-c",
+                   os.path.join(CSRC, unit), "-o", obj, *extra]
             if verbose:
                 cmd += ["-Xptxas", "-v"]
             r = subprocess.run(cmd, capture_output=True, text=True)

@@ -18,6 +18,7 @@ struct CflArgs {
     double gamma;
     int mhd;
     int use_b[3];
+    int check_nonfinite;   // flag a non-finite speed candidate (DERR_NONFINITE_STATE)
 };
 
 // CFL maxima of one grid, run by block vblock of vgrid blocks of that grid's launch.
@@ -31,6 +32,7 @@ __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vbloc
     const T* cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
                       reinterpret_cast<const T*>(a.q[Q_CBZ])};
     double m3[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
     for (long long i = vblock * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
          i += (long long)vgrid * blockDim.x) {
         double r = rho[i], px = p[0][i], py = p[1][i], pz = p[2][i];
@@ -42,10 +44,12 @@ __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vbloc
         }
         double sp[3];
         cfl_speeds(a.gamma, r, px, py, pz, (double)E[i], msq, sp);
+        bad = bad || !isfinite(sp[0] + sp[1] + sp[2]);
         m3[0] = fmax(m3[0], sp[0]);
         m3[1] = fmax(m3[1], sp[1]);
         m3[2] = fmax(m3[2], sp[2]);
     }
+    if (a.check_nonfinite) flag_nonfinite(a.tm, bad);
     __shared__ double wp[3][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll

@@ -23,7 +23,7 @@ enum BcClass { CLS_MASS = 0, CLS_MOM = 1, CLS_ENER = 2, CLS_MAG = 3 };
 enum Var { Q_RHO = 0, Q_PX, Q_PY, Q_PZ, Q_E, Q_BX, Q_BY, Q_BZ, Q_CBX, Q_CBY, Q_CBZ, NQ };
 
 // Error bits written by kernels into DevTime::error (host reads them after a step).
-enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2 };
+enum DevError : int { DERR_NONFINITE_DT = 1, DERR_CFL = 2, DERR_NONFINITE_STATE = 4 };
 
 // ---- stored-edge objects ------------------------------------------------------------------------
 // Every array object of the reference that can be shifted under a stateful BC (trans, wall) owns a
@@ -263,6 +263,15 @@ __device__ __forceinline__ void cfl_speeds(double G, double rho, double px, doub
     s[2] = fabs(pz * inv) + cs;
 }
 
+// Barrier over every thread of the thread-block cluster, with release/acquire ordering of shared
+// memory (DSMEM) accesses across it.  The warp is reconverged first and the per-thread (non-aligned)
+// forms of barrier.cluster are used, so a warp that reaches the barrier after divergent work (halo
+// jobs, stored-edge captures done by a few lanes) arrives exactly once per thread.
+__device__ __forceinline__ void cluster_sync() {
+    __syncwarp();
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+
 // Programmatic dependent launch: a pencil kernel launched with programmatic stream serialization may
 // be scheduled before the previous kernel of its stream has finished.  pdl_wait() blocks until that
 // kernel has completed and its memory is visible (a no-op for an ordinary launch); every read of data
@@ -270,6 +279,12 @@ __device__ __forceinline__ void cfl_speeds(double G, double rho, double px, doub
 // calls it at the start of its last stage, when every one of its CTAs is resident.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Flag a non-finite CFL speed candidate (a non-finite rho, momentum, energy or B in the cell) of any
+// lane of the warp: one atomic per warp that saw one.
+__device__ __forceinline__ void flag_nonfinite(DevTime* tm, bool bad) {
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&tm->error, (int)DERR_NONFINITE_STATE);
+}
 
 // Atomic max of a non-negative double through its bit pattern (NaN never reaches here).
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {

@@ -37,8 +37,11 @@ struct FluidArgs {
     int init_flux;         // first assignment of fluxR/L
     int mhd;               // cell-centred B is nonzero / the magnet is active
     int use_b[3];          // pressure.m:28-33 skips components with isZero set
-    int cfl;               // accumulate the CFL maxima of the new state (fused TimeManager pass)
+    int cfl;               // accumulate the CFL maxima of the new state (fused TimeManager pass);
+                           // with CFL_CHECK_NONFINITE also flag a non-finite state
 };
+constexpr int CFL_ACCUMULATE = 1;
+constexpr int CFL_CHECK_NONFINITE = 2;
 
 constexpr int FLUID_NARR = 20;
 constexpr int MAX_WARPS = 16;
@@ -179,7 +182,7 @@ __device__ __forceinline__ T column_max(const Tile<T, CPT>& tl, int NT, T (*part
         for (int o = 16; o >= olo; o >>= 1) m = fmax(m, __shfl_xor_sync(mask, m, o));
     if (tl.CL == 1) return m;
     if (tl.g == 0) cpart[tl.b] = m;
-    cg::this_cluster().sync();
+    cluster_sync();
     T c = T(0);
     if (lig < tl.CL) c = tl.remote(cpart, lig)[tl.b];
     if (tl.d == 0) c = warp_max_nonneg(c);
@@ -435,6 +438,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
     pdl_trigger();
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
     double m3[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const T* am = SA + nix(k, -1) * CS;
@@ -459,11 +463,13 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             double sp[3];
             cfl_speeds(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3], (double)unew[4], msq[k],
                        sp);
+            bad = bad || !isfinite(sp[0] + sp[1] + sp[2]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp[c]);
         }
     }
     if (a.cfl) {
+        if (a.cfl & CFL_CHECK_NONFINITE) flag_nonfinite(a.tm, bad);
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
@@ -667,6 +673,7 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
     pdl_trigger();
     // ---- corrector update (relaxingFluid.m:64-71), stored cell by cell ----------------------------
     double m3[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
 #pragma unroll
     for (int k = 0; k < CPT; ++k) {
         const int ix = tl.idx(k);
@@ -689,15 +696,17 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
             double sp[3];
             cfl_speeds(G, (double)unew[0], (double)unew[1], (double)unew[2], (double)unew[3], (double)unew[4], msq[k],
                        sp);
+            bad = bad || !isfinite(sp[0] + sp[1] + sp[2]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp[c]);
         }
     }
 
     // peers of a cluster read this CTA's shared memory through DSMEM until their last stage ends
-    if (tl.CL > 1) cg::this_cluster().sync();
+    if (tl.CL > 1) cluster_sync();
 
     if (a.cfl) {
+        if (a.cfl & CFL_CHECK_NONFINITE) flag_nonfinite(a.tm, bad);
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {

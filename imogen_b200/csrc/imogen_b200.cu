@@ -507,7 +507,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.init_flux = ctx->init_flux;
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
-    a.cfl = cfl;
+    a.cfl = cfl ? (CFL_ACCUMULATE | (c.nonfinite_check ? CFL_CHECK_NONFINITE : 0)) : 0;
     PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
                                       fade_on(c, d, CLS_MASS, CLS_ENER));
     // copy ghosts: single-CTA pencils, one circ, const or fade mode per side shared by the fluid classes
@@ -636,6 +636,7 @@ int launch_cfl_reduce(img_ctx* ctx) {
     a.gamma = ctx->cfg.gamma;
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
+    a.check_nonfinite = ctx->cfg.nonfinite_check != 0;
     if (ctx->rec) {
         OpRec r{};
         r.kind = OP_CFL_REDUCE;
@@ -667,6 +668,7 @@ int set_kernel_attributes(img_ctx* ctx) {
             CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->dev));
             for (int cpt : {1, 2, 4}) {
                 CK(fluid_attributes<T>(cpt, optin));
+                CK(fluid_cluster_attributes<T>(cpt, optin));
                 CK(chain_attributes<T>(cpt, optin));
             }
             dn = true;
@@ -762,6 +764,8 @@ int check_dev_error(img_ctx* ctx) {
     int e = ctx->host_tm->error;
     if (e & DERR_CFL) return fail(ctx, IMG_ERR_CFL, "CFL error: no velocity exceeded the 1e-2 floor (cmax=%g)", ctx->host_tm->cmax);
     if (e & DERR_NONFINITE_DT) return fail(ctx, IMG_ERR_NONFINITE, "non-finite timestep");
+    if (e & DERR_NONFINITE_STATE)
+        return fail(ctx, IMG_ERR_NONFINITE, "non-finite value in the state (rho, momentum, energy or B)");
     return IMG_OK;
 }
 
@@ -872,6 +876,7 @@ void img_config_default(img_config* c) {
     c->iter_max = 10;
     c->update_mode = 1;
     c->precision = IMG_PREC_FP64;
+    c->nonfinite_check = 1;
 }
 
 size_t img_bytes_required(const img_config* cfg) { return cfg ? plan(*cfg).total : 0; }
@@ -970,8 +975,10 @@ int img_create(img_ctx** out, const img_config* cfg) {
         fail(ctx, IMG_ERR_CUDA, "device initialisation failed");
         return bail(IMG_ERR_CUDA);
     }
-    if ((ctx->elem == 8 ? set_kernel_attributes<double>(ctx) : set_kernel_attributes<float>(ctx)) != IMG_OK)
-        return bail(IMG_ERR_CUDA);
+    {
+        const int rc = ctx->elem == 8 ? set_kernel_attributes<double>(ctx) : set_kernel_attributes<float>(ctx);
+        if (rc != IMG_OK) return bail(rc);   // IMG_ERR_UNSUPPORTED: a pencil tiling that cannot be scheduled
+    }
     *out = ctx;
     return IMG_OK;
 }
@@ -1849,7 +1856,11 @@ int img_batch_run(img_batch* b, int max_iters, int check_every, int* iters_done)
     if ((rc = img_batch_status(b, flags.data(), (int)flags.size())) != IMG_OK) return rc;
     if (iters_done) *iters_done = n;
     for (size_t i = 0; i < flags.size(); ++i)
-        if (flags[i] & 2) return bfail(b, IMG_ERR_CFL, "member %zu stopped with a time-step error", i);
+        if (flags[i] & 2) {   // report the first failed member's own status (CFL or non-finite)
+            int mrc = check_dev_error(b->members[i]);
+            return bfail(b, mrc != IMG_OK ? mrc : IMG_ERR_CFL, "member %zu stopped with an error: %s", i,
+                         img_last_error(b->members[i]));
+        }
     return IMG_OK;
 }
 

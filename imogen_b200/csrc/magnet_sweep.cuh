@@ -442,7 +442,7 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
             cp[q].BI[o] = bI[q][k] - ff2 * (Fl[q][k] - fm);
             cp[q].Fout[o] = Fl[q][k];
         }
-    if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
+    if (tl.CL > 1) cluster_sync();   // keep shared memory alive for DSMEM readers
 }
 
 // ---- CT and cell-centring, fused along X-pencils --------------------------------------------------------
@@ -590,7 +590,7 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
         } else sh = b2;
         CB2[o] = T(0.5) * (b2 + sh);
     }
-    if (tl.CL > 1) cg::this_cluster().sync();   // keep shared memory alive for DSMEM readers
+    if (tl.CL > 1) cluster_sync();   // keep shared memory alive for DSMEM readers
 }
 
 __device__ __forceinline__ void cell_coords(const Geom& g, long long i, int& x, int& y, int& z) {

@@ -130,7 +130,7 @@ struct Tile {
         else { x = c1; y = c2; z = r; }
     }
     __device__ __forceinline__ void csync() const {
-        if (CL > 1) cg::this_cluster().sync();
+        if (CL > 1) cluster_sync();
         else __syncthreads();
     }
     template <typename U>
@@ -151,8 +151,11 @@ struct Tile {
 
 // Fade damping of fade_shift.m:31-44 applied to the constant-shifted value sv at row r of a line of
 // N cells: s0 and sN1 are the constant-shifted values at rows 0 and N-1 (the two anchors).
+// Rows past the pencil's end (idle rows of the last CTA) are returned unchanged: their values are
+// never read, and the coefficient index N-1-r would be negative there.
 template <typename T>
 __device__ __forceinline__ T fade_apply(T sv, int r, int N, const double* fc, int f, T s0, T sN1) {
+    if (r >= N) return sv;
     T lf = sv;
     if (r < f) lf = (T(1) - T(fc[r])) * sv + T(fc[r]) * s0;
     if (r >= N - f) {

@@ -27,6 +27,12 @@ template <typename T> cudaError_t launch_mag_ctcell(const MagArgs& a, const Penc
 // argument block per member, one BlockMap per CTA of the launch, L.grid_x CTAs).
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd);
+// The batched fluid sweep over pencils that span a thread-block cluster (L.cluster > 1), defined in
+// fluid_cluster.cu: that translation unit is compiled at ptxas -O1 (see there), and its kernels need
+// their own shared-memory attributes (fluid_cluster_attributes).
+template <typename T>
+cudaError_t launch_fluid_sweep_batch_cluster(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd);
+template <typename T> cudaError_t fluid_cluster_attributes(int cpt, int optin);
 template <typename T> cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L);
 template <typename T>
 cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L);

@@ -154,6 +154,7 @@ inline int ct_variant(bool fade, bool cg) { return (fade ? 1 : 0) | (cg ? 2 : 0)
 
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
+    if (L.cluster > 1) return launch_fluid_sweep_batch_cluster<T>(args, map, L, mhd);
     return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 

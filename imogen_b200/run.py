@@ -60,7 +60,7 @@ def bc_table(bc):
 
 def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ", bc_infinity=20,
                 limiter="vanleer", fluid=True, magnet=False, time_max=1e5, iter_max=10,
-                update_mode=1, precision="fp64"):
+                update_mode=1, precision="fp64", nonfinite_check=True):
     """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults)."""
     c = ImgConfig()
     lib().img_config_default(ctypes.byref(c))
@@ -90,6 +90,7 @@ def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ"
     c.iter_max = int(iter_max)
     c.update_mode = int(update_mode)
     c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    c.nonfinite_check = int(bool(nonfinite_check))
     return c
 
 

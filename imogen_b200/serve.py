@@ -21,6 +21,7 @@ from typing import Callable, Dict, List, Optional
 import numpy as np
 
 from . import problems
+from ._lib import ImogenError
 from .run import ImogenBatch, ImogenRun, bytes_required  # noqa: F401  (bytes_required is re-exported)
 
 
@@ -109,18 +110,25 @@ class Server:
 
     def _retire(self, batch: ImogenBatch):
         flags = batch.status()                           # synchronises the batch's stream
-        finished = [m for m, f in zip(list(batch.members), flags) if f & 3]
-        for run in finished:
+        finished = [(m, f) for m, f in zip(list(batch.members), flags) if f & 3]
+        for run, flag in finished:
             jid = next(k for k, v in self.running.items() if v[1] is run)
             job, _, need = self.running.pop(jid)
             batch.remove(run)
-            if callable(self.keep):
-                job.result = self.keep(run)
-            elif self.keep == "totals":
-                job.result = {"totals": run.totals()}
+            if flag & 2:                                 # the job's device error flag (CFL, non-finite)
+                try:
+                    run.progress()
+                    job.result = {"error": "device error flag set", "code": None}
+                except ImogenError as e:
+                    job.result = {"error": str(e), "code": e.code}
             else:
-                job.result = run.state()
-            job.result["time"], job.iterations, _ = run.progress()
+                if callable(self.keep):
+                    job.result = self.keep(run)
+                elif self.keep == "totals":
+                    job.result = {"totals": run.totals()}
+                else:
+                    job.result = run.state()
+                job.result["time"], job.iterations, _ = run.progress()
             job.completed = self.now()
             run.close()
             self.used -= need
@@ -164,8 +172,9 @@ class Server:
             return {"state": "running", "time": t, "iterations": n}
         for j in self.done:
             if j.id == job_id:
-                return {"state": "cancelled" if j.result and j.result.get("cancelled") else "done",
-                        "latency_s": j.latency}
+                r = j.result or {}
+                st = "cancelled" if r.get("cancelled") else ("failed" if "error" in r else "done")
+                return {"state": st, "latency_s": j.latency, **({"error": r["error"]} if "error" in r else {})}
         raise KeyError(job_id)
 
     def cancel(self, job_id: int) -> bool:

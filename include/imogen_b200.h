@@ -26,7 +26,7 @@ enum {
     IMG_ERR_NOMEM = -3,        /* device allocation failed / over the HBM budget */
     IMG_ERR_UNSUPPORTED = -4,  /* setting that the reference itself cannot run (index error) */
     IMG_ERR_CFL = -5,          /* TimeManager.m:79-86: no direction exceeded the 1e-2 floor */
-    IMG_ERR_NONFINITE = -6,    /* the timestep became non-finite */
+    IMG_ERR_NONFINITE = -6,    /* the timestep or (with nonfinite_check) the state became non-finite */
     IMG_ERR_STATE = -7         /* call out of order (e.g. step before state was set) */
 };
 
@@ -60,12 +60,18 @@ typedef struct img_config {
     int iter_max;             /* ini.iterMax */
     int update_mode;          /* ini.timeUpdateMode: 0 per step, 1 per iteration */
     int precision;            /* IMG_PREC_FP64 (plain) or IMG_PREC_MIXED (FP32 state, FP64 pressure/CFL) */
+    int nonfinite_check;      /* 1 (default): a CFL pass that meets a non-finite rho, momentum, energy or
+                                 B stops the run with IMG_ERR_NONFINITE.  0: the reference's behaviour
+                                 (its max ignores NaN, TimeManager.m:70-76; MINMASS replaces a NaN
+                                 density, relaxingFluid.m:39,71) and the run goes on.  No reference
+                                 counterpart. */
 } img_config;
 
 typedef struct img_ctx img_ctx;
 
 /* Default config: Initializer.m defaults (gamma 5/3, cfl 0.7, minMass 1e-5, circ BCs,
- * bcInfinity 20, vanleer, fluid on, magnet off, timeMax 1e5, iterMax 10, per-iteration dt). */
+ * bcInfinity 20, vanleer, fluid on, magnet off, timeMax 1e5, iterMax 10, per-iteration dt), plus
+ * nonfinite_check = 1. */
 void img_config_default(img_config* cfg);
 
 /* Create a context for one grid on the current CUDA device.  Replaces initialize.m:18-410 for

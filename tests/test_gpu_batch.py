@@ -122,3 +122,23 @@ def test_batch_rejects_members_with_another_launch_sequence():
     b.close()
     for r in (a, c, f):
         r.close()
+
+
+def test_long_cluster_members_with_fade_match_alone():
+    """Members whose x pencils span a 4-CTA cluster at 4 cells per thread (N > 4096), fade ends: the
+    batched launches run the same cluster barriers and DSMEM exchanges as the launches alone."""
+    tubes = [problems.brio_wu_ensemble()[i] for i in (4, 5, 9, 1)]      # N = 4288, 6054, 6541, 652
+    alone = [_make(dict(s, time_max=1e5), st, "mixed") for s, st in tubes]
+    together = [_make(dict(s, time_max=1e5), st, "mixed") for s, st in tubes]
+    b = ImogenBatch(together)
+    for _ in range(8):
+        b.step()
+        for r in alone:
+            r.iterate()
+    for r in alone:
+        r.sync()
+    for i, (x, y) in enumerate(zip(alone, together)):
+        _same(x, y, f"tube {i} (n={x.grid[0]})")
+    b.close()
+    for r in alone + together:
+        r.close()

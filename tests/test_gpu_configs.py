@@ -93,7 +93,9 @@ def test_kelvin_helmholtz_256_mixed_vs_fp64_200_iterations():
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 2e-5)])
 def test_brio_wu_ensemble_members_against_oracle(precision, tol):
-    tubes = problems.brio_wu_ensemble()[:16]
+    # the FP64 form holds pencils of up to about 5000 cells on one cluster of 4 CTAs (longer ones are
+    # rejected at img_create); the mixed form takes the ensemble's whole range (up to 8192)
+    tubes = [t for t in problems.brio_wu_ensemble() if precision == "mixed" or t[0]["grid"][0] <= 4096][:16]
     iters = 40
     runs = []
     for s, st in tubes:
