@@ -6,4 +6,5 @@ template cudaError_t launch_fluid_sweep<float>(const FluidArgs&, const PencilLau
 template cudaError_t launch_fluid_sweep_batch<float>(const FluidArgs*, const BlockMap*, const PencilLaunch&, bool);
 template cudaError_t fluid_attributes<float>(int, int);
 template cudaError_t fluid_max_clusters<float>(const PencilLaunch&, int*);
+template cudaError_t fluid_seg_attributes<float>(int);
 }  // namespace img

@@ -6,4 +6,5 @@ template cudaError_t launch_fluid_sweep<double>(const FluidArgs&, const PencilLa
 template cudaError_t launch_fluid_sweep_batch<double>(const FluidArgs*, const BlockMap*, const PencilLaunch&, bool);
 template cudaError_t fluid_attributes<double>(int, int);
 template cudaError_t fluid_max_clusters<double>(const PencilLaunch&, int*);
+template cudaError_t fluid_seg_attributes<double>(int);
 }  // namespace img

@@ -43,6 +43,7 @@ const int BWD_MI[3][2] = {{3, 2}, {3, 1}, {2, 1}};
 struct PencilCfg {
     int Wb = 1, G = 32, CL = 1, NT = 32, cpt = 2;
     int nqc = 1;   // magnet chain: transverse components per CTA
+    int seg = 0;   // fluid sweep: segment kernel with seg = cpt consecutive cells per thread (G = N / cpt)
 };
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -169,6 +170,9 @@ struct img_ctx {
     int iters_base = 0;
     PencilCfg pcfg[3][3];        // pencil tiling per kernel (0 fluid sweep, 1 magnet chain, 2 magnet CT) and
                                  // direction; the public magnet tiling sets 1 and 2, the autotuner tunes 2 alone
+    PencilCfg pcfg_tile[3];      // fluid sweep per direction: the tile-kernel tiling of the launches that the
+                                 // segment kernel does not take (stored-edge capture, fade, other ends)
+    PencilCfg pcfg_mtile[2][3];  // the same for the magnet chain [0] and CT pass [1] (window kernels)
     // one captured iteration per (cfl_valid at its start, sweep-order row (iteration-1) % 6)
     cudaGraphExec_t graphs[2][6] = {};
     uint64_t graph_launches[2][6] = {};
@@ -347,6 +351,93 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d, size_t elem) {
     return out;
 }
 
+// Segment tilings of the fluid sweep (seg_fluid.cuh): C consecutive cells per thread (2, 4 or 8; 2 or 4
+// in FP64), the whole pencil in one CTA of NT = Wb * S threads, 64 <= NT <= 512, S = N / C threads per
+// pencil.  Along x the S threads of a pencil are consecutive lanes: S is a power of two up to 32 or a
+// multiple of 32.  Along y and z Wb >= 4 pencils (a power of two) sit side by side.
+std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem) {
+    std::vector<PencilCfg> out;
+    const int N = g.n[d];
+    const long long ncol = g.ncell / N;
+    for (int C : {2, 4, 8}) {
+        if ((elem == 8 && C == 8) || N % C) continue;
+        const int S = N / C;
+        if (d == 0 && !(S % 32 == 0 || (S <= 32 && 32 % S == 0))) continue;
+        for (int Wb = d == 0 ? 1 : 4; Wb <= 32; Wb *= 2) {
+            const int NT = Wb * S;
+            if (NT > 512) break;
+            if (NT < 64 || NT % 32) continue;
+            if (Wb > 1 && (long long)Wb / 2 >= ncol) break;   // more pencil slots than pencils
+            const size_t smem = elem == 8 ? seg_fluid_smem_bytes<double>(NT) : seg_fluid_smem_bytes<float>(NT);
+            if (smem > kPencilSmemLimit) continue;
+            PencilCfg p;
+            p.Wb = Wb;
+            p.G = S;
+            p.CL = 1;
+            p.NT = NT;
+            p.cpt = C;
+            p.seg = C;
+            out.push_back(p);
+        }
+    }
+    return out;
+}
+
+// Window tilings of the magnet chain and CT pass (seg_magnet.cuh): C = 2, 4 or 8 consecutive cells per
+// thread with C dividing N, S = N / C threads per pencil, the whole pencil in one CTA of NT = Wb * S
+// threads (32 <= NT <= 512, a multiple of 32); along y and z Wb >= 4 pencils side by side.
+std::vector<PencilCfg> win_candidates(const Geom& g, int d) {
+    std::vector<PencilCfg> out;
+    const int N = g.n[d];
+    const long long ncol = g.ncell / N;
+    for (int C : {2, 4, 8}) {
+        if (N % C) continue;
+        const int S = N / C;
+        for (int Wb = d == 0 ? 1 : 4; Wb <= 64; Wb *= 2) {
+            const int NT = Wb * S;
+            if (NT > 512) break;
+            if (NT < 32 || NT % 32) continue;
+            if (Wb > 1 && (long long)Wb / 2 >= ncol) break;
+            PencilCfg p;
+            p.Wb = Wb;
+            p.G = S;
+            p.CL = 1;
+            p.NT = NT;
+            p.cpt = C;
+            p.seg = C;
+            out.push_back(p);
+        }
+    }
+    return out;
+}
+
+// Default magnet tiling: the window kernels where a window tiling exists (4 cells per thread, along y
+// and z at least 8 pencils side by side, the CTA nearest 256 threads), else the tile kernels' default.
+PencilCfg choose_window(const Geom& g, int d, const PencilCfg& tile) {
+    const PencilCfg* best = nullptr;
+    std::vector<PencilCfg> c = win_candidates(g, d);
+    for (const PencilCfg& p : c) {
+        if (p.seg != 4 || (d != 0 && p.Wb < 8)) continue;
+        if (!best || std::abs(p.NT - 256) < std::abs(best->NT - 256)) best = &p;
+    }
+    return best ? *best : tile;
+}
+
+// Default fluid tiling: in the mixed form the segment kernel where a segment tiling exists (4 cells per
+// thread, along y and z at least 8 pencils side by side, the CTA nearest 256 threads); in FP64, and where
+// no segment tiling exists, the tile kernels' default (the FP64 segment kernel needs more registers than
+// it has; the autotuner may still pick it).
+PencilCfg choose_fluid(const Geom& g, int d, size_t elem, const PencilCfg& tile) {
+    if (elem == 8) return tile;
+    const PencilCfg* best = nullptr;
+    std::vector<PencilCfg> c = seg_candidates(g, d, elem);
+    for (const PencilCfg& p : c) {
+        if (p.seg != 4 || (d != 0 && p.Wb < 8)) continue;
+        if (!best || std::abs(p.NT - 256) < std::abs(best->NT - 256)) best = &p;
+    }
+    return best ? *best : tile;
+}
+
 // Pencil tiling of one sweep direction: one cell per thread where the pencil fits a cluster of at
 // most 4 CTAs of 512 threads (2 or 4 cells per thread otherwise).  Along x a CTA holds whole pencil
 // segments of up to 512 rows; along y and z it holds 4 adjacent pencils, so each row of the tile is
@@ -486,7 +577,18 @@ template <typename T>
 int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     FluidArgs a{};
     const img_config& c = ctx->cfg;
-    const PencilCfg& pcf = ctx->pcfg[0][d];
+    // the segment kernel takes the steady sweeps of single-CTA pencils whose ends are circ or const for
+    // all fluid classes; stored-edge capture (a run's first sweeps), fade and other ends take the tile
+    // kernels
+    const bool fade = fade_on(c, d, CLS_MASS, CLS_ENER);
+    const bool init = ctx->init_store || ctx->init_flux;
+    bool seg_ok = ctx->pcfg[0][d].seg && !init && !fade;
+    for (int k = 0; k < 3; ++k)
+        for (int side = 0; side < 2; ++side) {
+            const int m = c.bc_modes[k][side][d];
+            if ((m != IMG_BC_CIRC && m != IMG_BC_CONST) || m != c.bc_modes[CLS_MASS][side][d]) seg_ok = false;
+        }
+    const PencilCfg& pcf = (seg_ok || !ctx->pcfg[0][d].seg) ? ctx->pcfg[0][d] : ctx->pcfg_tile[d];
     a.sg = sweep_geom(ctx, d, pcf);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
     a.tm = ctx->tm;
@@ -508,8 +610,10 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.cfl = cfl ? (CFL_ACCUMULATE | (c.nonfinite_check ? CFL_CHECK_NONFINITE : 0)) : 0;
-    PencilLaunch L = pencil_launch<T>(ctx, pcf, d, fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb), 1,
-                                      fade_on(c, d, CLS_MASS, CLS_ENER));
+    PencilLaunch L = pencil_launch<T>(ctx, pcf, d,
+                                      pcf.seg ? seg_fluid_smem_bytes<T>(pcf.NT) : fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb),
+                                      1, fade);
+    L.seg = pcf.seg;
     // copy ghosts: single-CTA pencils, one circ, const or fade mode per side shared by the fluid classes
     L.cg = pcf.CL == 1;
     for (int k = 0; k < 3; ++k)
@@ -518,6 +622,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
             if (!copy_ghost_mode(m) || m != a.mode[CLS_MASS][side]) L.cg = false;
         }
     L.init = a.init_store || a.init_flux;   // first sweeps: the stored-edge capturing kernel
+    if (L.seg) L.cg = true;                  // segment kernels index their ghosts directly
     if (ctx->rec) {
         OpRec r{};
         r.kind = OP_FLUID;
@@ -585,14 +690,23 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
     MagArgs a{};
     fill_mag_args<T>(ctx, X, I1, I2, a);
     const int d = X - 1;
-    const PencilCfg& pcf = ctx->pcfg[1][d];
-    const PencilCfg& pcc = ctx->pcfg[2][d];   // the CT pass has a tiling of its own
+    // the window kernels take the steady sweeps whose mag-class ends along X and transverse shifts (mass and
+    // mom classes below, mag class above, along both I) are circ or const; the rest take the tile kernels
+    auto stateless = [](int m) { return m == IMG_BC_CIRC || m == IMG_BC_CONST; };
+    bool win_ok = !(a.init_mag[0] || a.init_mag[1]) && stateless(a.modeX[0]) && stateless(a.modeX[1]);
+    for (int q = 0; q < 2; ++q)
+        win_ok = win_ok && stateless(a.modeI_mass[q][0]) && stateless(a.modeI_mom[q][0]) && stateless(a.modeI_mag[q][1]);
+    const PencilCfg& pcf = (win_ok || !ctx->pcfg[1][d].seg) ? ctx->pcfg[1][d] : ctx->pcfg_mtile[0][d];
+    const PencilCfg& pcc = (win_ok || !ctx->pcfg[2][d].seg) ? ctx->pcfg[2][d] : ctx->pcfg_mtile[1][d];   // CT: own tiling
+    a.sg = sweep_geom(ctx, d, pcf);
     MagArgs ac = a;
     ac.sg = sweep_geom(ctx, d, pcc);
-    PencilLaunch L = pencil_launch<T>(ctx, pcf, d, mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
-                                      2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
-    PencilLaunch Lc = pencil_launch<T>(ctx, pcc, d, ctcell_smem_bytes<T>(pcc.G * pcc.cpt, pcc.Wb), 1,
+    PencilLaunch L = pencil_launch<T>(ctx, pcf, d, pcf.seg ? 0 : mag_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb, pcf.nqc),
+                                      pcf.seg ? 1 : 2 / pcf.nqc, fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    PencilLaunch Lc = pencil_launch<T>(ctx, pcc, d, pcc.seg ? 0 : ctcell_smem_bytes<T>(pcc.G * pcc.cpt, pcc.Wb), 1,
                                        fade_on(ctx->cfg, d, CLS_MAG, CLS_MAG));
+    L.seg = pcf.seg;
+    Lc.seg = pcc.seg;
     // copy ghosts: single-CTA pencils with circ, const or fade mag-class shifts along X
     const bool cg_modes = copy_ghost_mode(a.modeX[0]) && copy_ghost_mode(a.modeX[1]);
     L.cg = pcf.CL == 1 && cg_modes;
@@ -671,13 +785,14 @@ int set_kernel_attributes(img_ctx* ctx) {
                 CK(fluid_cluster_attributes<T>(cpt, optin));
                 CK(chain_attributes<T>(cpt, optin));
             }
+            CK(fluid_seg_attributes<T>(optin));
             dn = true;
         }
     }
     for (int kind = 0; kind < 3; ++kind)
         for (int d = 0; d < 3; ++d) {
             const PencilCfg& p = ctx->pcfg[kind][d];
-            if (ctx->g.n[d] < 3) continue;
+            if (ctx->g.n[d] < 3 || p.seg) continue;   // segment tilings: one CTA, shared memory checked
             PencilLaunch L = pencil_launch<T>(ctx, p, d, fluid_smem_bytes<T>(p.G * p.cpt, p.Wb), 1, false);
             int nclusters = 0;
             cudaError_t e = fluid_max_clusters<T>(L, &nclusters);
@@ -898,9 +1013,22 @@ int img_create(img_ctx** out, const img_config* cfg) {
     g.s[1] = g.n[0];
     g.s[2] = (long long)g.n[0] * g.n[1];
     g.ncell = (long long)g.n[0] * g.n[1] * g.n[2];
+    // IMOGEN_B200_TILE_KERNELS=1 (read here, at creation): the pencil-tile kernels for every sweep, whatever
+    // the default or an earlier autotuning would pick (e.g. to check the segment and window kernels)
+    const char* tk = getenv("IMOGEN_B200_TILE_KERNELS");
+    const bool tile_only = tk && tk[0] == '1';
     for (int kind = 0; kind < 3; ++kind)
         for (int d = 0; d < 3; ++d) {
             ctx->pcfg[kind][d] = choose_pencil(g, d, ctx->elem);
+            if (kind == 0) {
+                ctx->pcfg_tile[d] = ctx->pcfg[0][d];
+                if (tile_only) continue;
+                ctx->pcfg[0][d] = choose_fluid(g, d, ctx->elem, ctx->pcfg_tile[d]);
+            } else {
+                ctx->pcfg_mtile[kind - 1][d] = ctx->pcfg[kind][d];
+                if (tile_only) continue;
+                ctx->pcfg[kind][d] = choose_window(g, d, ctx->pcfg_mtile[kind - 1][d]);
+            }
             std::lock_guard<std::mutex> lock(g_tune_mu);
             auto it = g_tuned.find(tune_key(kind, g, d, ctx->elem, *cfg));
             if (it != g_tuned.end()) ctx->pcfg[kind][d] = it->second;
@@ -1547,7 +1675,8 @@ size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
 
 bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
     return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
-           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg && x.init == y.init;
+           x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg && x.init == y.init &&
+           x.seg == y.seg;
 }
 
 // Turn the members' records into batched launch items and the arena image.
@@ -1988,7 +2117,9 @@ int img_autotune(img_ctx* ctx, int trials) {
             PencilCfg best = ctx->pcfg[kind][d];
             float best_ms = 1e30f;
             std::vector<PencilCfg> cands = pencil_candidates(ctx->g, d, ctx->elem);
-            if (kind == 1) {   // the chain may also take both transverse components per CTA
+            if (kind == 0)
+                for (const PencilCfg& sc : seg_candidates(ctx->g, d, ctx->elem)) cands.push_back(sc);
+            if (kind == 1) {   // (window tilings carry both components per thread: no nqc = 2 variant)   // the chain may also take both transverse components per CTA
                 const size_t n0 = cands.size();
                 for (size_t i = 0; i < n0; ++i)
                     if (cands[i].cpt <= 2) {
@@ -1997,17 +2128,21 @@ int img_autotune(img_ctx* ctx, int trials) {
                         cands.push_back(c2);
                     }
             }
+            if (kind != 0)
+                for (const PencilCfg& wc : win_candidates(ctx->g, d)) cands.push_back(wc);
             for (const PencilCfg& cand : cands) {
                 ctx->pcfg[kind][d] = cand;
-                int ncl = 0;
-                const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
-                                                 : fluid_smem_bytes<float>(cand.G * cand.cpt, cand.Wb);
-                PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, cand, d, fs, 1, false)
-                                                : pencil_launch<float>(ctx, cand, d, fs, 1, false);
-                cudaError_t ce = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
-                if (ce != cudaSuccess || ncl < 1) {
-                    cudaGetLastError();
-                    continue;
+                if (!cand.seg) {   // segment tilings are one CTA with checked shared memory
+                    int ncl = 0;
+                    const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(cand.G * cand.cpt, cand.Wb)
+                                                     : fluid_smem_bytes<float>(cand.G * cand.cpt, cand.Wb);
+                    PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, cand, d, fs, 1, false)
+                                                    : pencil_launch<float>(ctx, cand, d, fs, 1, false);
+                    cudaError_t ce = ctx->elem == 8 ? fluid_max_clusters<double>(L, &ncl) : fluid_max_clusters<float>(L, &ncl);
+                    if (ce != cudaSuccess || ncl < 1) {
+                        cudaGetLastError();
+                        continue;
+                    }
                 }
                 auto sweep = [&]() {
                     return kind == 0 ? fluid_sweep(ctx, d + 1, false)
@@ -2044,16 +2179,28 @@ int img_autotune(img_ctx* ctx, int trials) {
     return rc != IMG_OK ? rc : check_dev_error(ctx);
 }
 
-int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]) {
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[7]) {
     if (!ctx || !cfg || dim < 1 || dim > 6) return fail(ctx, IMG_ERR_ARG, "bad tiling argument");
     if (ctx->batch) return fail(ctx, IMG_ERR_STATE, "cannot retile a batch member");
     const int kind = (dim - 1) / 3, d = (dim - 1) % 3;
     const int nqc = cfg[5];
     if (nqc != 1 && !(nqc == 2 && kind == 1 && cfg[4] <= 2))
         return fail(ctx, IMG_ERR_UNSUPPORTED, "two components per CTA: magnet sweeps with at most 2 cells per thread");
-    for (PencilCfg c : pencil_candidates(ctx->g, d, ctx->elem)) {
-        if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4]) continue;
+    if (cfg[6] && nqc != 1) return fail(ctx, IMG_ERR_UNSUPPORTED, "window tilings carry both components per thread");
+    std::vector<PencilCfg> cands = pencil_candidates(ctx->g, d, ctx->elem);
+    for (const PencilCfg& sc : kind == 0 ? seg_candidates(ctx->g, d, ctx->elem) : win_candidates(ctx->g, d))
+        cands.push_back(sc);
+    for (PencilCfg c : cands) {
+        if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4] ||
+            (c.seg != 0) != (cfg[6] != 0))
+            continue;
         c.nqc = nqc;
+        if (c.seg) {
+            ctx->pcfg[kind][d] = c;
+            if (kind == 1) ctx->pcfg[2][d] = c;
+            drop_graphs(ctx);
+            return IMG_OK;
+        }
         int ncl = 0;
         const size_t fs = ctx->elem == 8 ? fluid_smem_bytes<double>(c.G * c.cpt, c.Wb) : fluid_smem_bytes<float>(c.G * c.cpt, c.Wb);
         PencilLaunch L = ctx->elem == 8 ? pencil_launch<double>(ctx, c, d, fs, 1, false) : pencil_launch<float>(ctx, c, d, fs, 1, false);
@@ -2070,7 +2217,7 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]) {
     return fail(ctx, IMG_ERR_UNSUPPORTED, "not a tiling the kernels accept for this direction");
 }
 
-int img_get_tiling(const img_ctx* ctx, int dim, int out[6]) {
+int img_get_tiling(const img_ctx* ctx, int dim, int out[7]) {
     if (!ctx || !out || dim < 1 || dim > 6) return IMG_ERR_ARG;
     const PencilCfg& p = ctx->pcfg[(dim - 1) / 3][(dim - 1) % 3];
     out[0] = p.Wb;
@@ -2079,6 +2226,7 @@ int img_get_tiling(const img_ctx* ctx, int dim, int out[6]) {
     out[3] = p.NT;
     out[4] = p.cpt;
     out[5] = p.nqc;
+    out[6] = p.seg ? 1 : 0;
     return IMG_OK;
 }
 

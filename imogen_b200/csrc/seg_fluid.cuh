@@ -1,0 +1,391 @@
+// Segment form of the fused fluid sweep (fluid/relaxingFluid.m:16-73, fluid/wFluidFlux.m:14-44,
+// pressure/pressure.m:23-64, flux/*Limiter.m) for pencils that fit one CTA with circ or const ends.
+//
+// Each thread owns C consecutive cells of a pencil (a "segment"), so every stencil neighbour inside a
+// segment is a register; only the cells at the two ends of a segment are exchanged, through shared
+// memory, and the exchanges ride on the two barriers that the pencil maxima need anyway:
+//   stage 1  load the segment (128-bit loads along x), 'totsnd' pressure, freezing-speed candidate and
+//            the flux numerators F (w = F / c_f) of every cell; publish (u, F) of the first and last
+//            cell; barrier; c_f = pencil max.
+//   stage 2  predictor half step with R = (u + F/c_f)/2, L = (u - F/c_f)/2 (relaxingFluid.m:30-39);
+//            pressure, speed and F of the half-step state; publish (u*, F*) of the first two and last
+//            two cells; barrier; c_f* = pencil max.
+//   stage 3  corrector fluxes R*, L* over the segment and the two neighbour cells each side, the TVD
+//            limiter (relaxingFluid.m:57-62) -- the limited values of the neighbour cells next to the
+//            segment are computed here as well, from the published cells -- and the update
+//            (relaxingFluid.m:64-71); store; fused CFL maxima on the last sweep of a step.
+// The arithmetic of every cell is the same sequence of operations as the pencil-tile kernels
+// (fluid_sweep.cuh), so both give the same bits.
+//
+// Thread placement (SweepGeom with G = S segments per pencil, RC = N): along x the S threads of a
+// pencil are consecutive (thread t = b*S + s), along y and z the Wb pencils of the CTA are (t = s*Wb +
+// b), so global loads and stores stay coalesced along x.  Pencil ends: a circ end's neighbour segment
+// is the pencil's other end; a const end's ghost is the end cell itself (constant_shift.m), applied to
+// every shifted array, the limited fluxes included.
+#pragma once
+
+#include <type_traits>
+
+#include "fluid_sweep.cuh"
+
+namespace img {
+
+// Words per thread of the two exchange sets and of the pencil maxima: (u, F) of 2 cells, (u*, F*) of
+// 4 cells, and 2 per-warp maxima slots of 32 columns.
+template <typename T>
+__host__ __device__ inline size_t seg_fluid_smem_bytes(int NT) {
+    return sizeof(T) * ((size_t)60 * NT + 2 * (size_t)(NT / 32) * 32);
+}
+
+// Placement of one thread in the segment layout.
+struct SegPos {
+    int b, s;            // pencil within the CTA, segment within the pencil
+    bool colok;          // the pencil exists (the last CTA may hold fewer than Wb)
+    long long base;      // offset of the pencil's row 0
+    __device__ __forceinline__ void init(const SweepGeom& g, unsigned vblock) {
+        const int t = threadIdx.x;
+        const unsigned q = g.div_lanes.div((unsigned)t);   // t / S (x) or t / Wb (y, z)
+        if (g.d == 0) { b = (int)q; s = t - b * g.G; }
+        else { s = (int)q; b = t - s * g.Wb; }
+        const int col = (int)(vblock * (unsigned)g.Wb + (unsigned)b);
+        colok = col < g.ncol;
+        const unsigned c = colok ? (unsigned)col : 0u;
+        const int c2 = (int)g.div_n1.div(c);
+        const int c1 = (int)(c - (unsigned)c2 * (unsigned)g.n1);
+        base = c1 * g.s1 + (long long)c2 * g.s2;
+    }
+};
+
+// C consecutive values of array p starting at offset o, stride sd (vector loads when sd == 1: the
+// offset is a multiple of C and arrays start 256-byte aligned).
+template <typename T, int C>
+__device__ __forceinline__ void seg_load(const void* p, long long o, long long sd, bool vec, T (&out)[C]) {
+    const T* a = reinterpret_cast<const T*>(p) + o;
+    if (vec) {
+        if constexpr (sizeof(T) == 4 && C % 4 == 0) {
+#pragma unroll
+            for (int k = 0; k < C; k += 4) {
+                const float4 v = *reinterpret_cast<const float4*>(a + k);
+                out[k] = v.x; out[k + 1] = v.y; out[k + 2] = v.z; out[k + 3] = v.w;
+            }
+            return;
+        } else if constexpr (C % 2 == 0) {
+            using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+#pragma unroll
+            for (int k = 0; k < C; k += 2) {
+                const V2 v = *reinterpret_cast<const V2*>(a + k);
+                out[k] = v.x; out[k + 1] = v.y;
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < C; ++k) out[k] = a[(long long)k * sd];
+}
+
+template <typename T, int C>
+__device__ __forceinline__ void seg_store(void* p, long long o, long long sd, bool vec, const T (&v)[C]) {
+    T* a = reinterpret_cast<T*>(p) + o;
+    if (vec) {
+        if constexpr (sizeof(T) == 4 && C % 4 == 0) {
+#pragma unroll
+            for (int k = 0; k < C; k += 4) *reinterpret_cast<float4*>(a + k) = make_float4(v[k], v[k + 1], v[k + 2], v[k + 3]);
+            return;
+        } else if constexpr (C % 2 == 0) {
+#pragma unroll
+            for (int k = 0; k < C; k += 2) {
+                if constexpr (sizeof(T) == 4) *reinterpret_cast<float2*>(a + k) = make_float2(v[k], v[k + 1]);
+                else *reinterpret_cast<double2*>(a + k) = make_double2(v[k], v[k + 1]);
+            }
+            return;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < C; ++k) a[(long long)k * sd] = v[k];
+}
+
+// The flux numerators F of wFluidFlux.m:31-44 (w = F * (1/c_f)) for one cell: the mixed form's
+// flux_num, and in FP64 the same terms with IEEE reciprocals (the operations of wflux<double>).
+template <typename T>
+__device__ __forceinline__ void flux_num_t(int d, const T u[5], const T bb[3], T press, T F[5]) {
+    if constexpr (sizeof(T) == 4) {
+        flux_num(d, u, bb, press, F);
+    } else {
+        const T pX = sel3(d, u[1], u[2], u[3]);
+        const T bX = sel3(d, bb[0], bb[1], bb[2]);
+        const T ir = T(1) / u[0];
+        const T velocity = pX * ir;
+        F[0] = pX;
+        F[4] = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) F[1 + c] = velocity * u[1 + c] + press * (c == d ? T(1) : T(0)) - bX * bb[c];
+    }
+}
+
+// Pencil maximum of non-negative speeds in the segment layout.  publish: reduce over the lanes of the
+// pencil inside the warp and leave the warp's value in pm where a pencil spans warps; collect, after
+// a barrier, reduces those.  Along x the S segments of a pencil are consecutive lanes (S a power of
+// two below 32, or a multiple of 32); along y and z the lanes of pencil b are b, b + Wb, ... (Wb a
+// power of two).
+template <typename T>
+__device__ __forceinline__ T seg_max_publish(const SweepGeom& g, T v, T* pm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
+    if (g.d == 0) {
+        if (g.G >= 32) {
+            v = warp_max_nonneg(v);
+            if (lane == 0) pm[warp * 32] = v;
+        } else {
+            for (int o = g.G / 2; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(full, v, o));
+        }
+        return v;
+    }
+    for (int o = 16; o >= g.Wb; o >>= 1) v = fmax(v, __shfl_xor_sync(full, v, o));
+    if (lane < g.Wb) pm[warp * 32 + lane] = v;
+    return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T seg_max_collect(const SweepGeom& g, int b, T wv, const T* pm) {
+    const int lane = threadIdx.x & 31;
+    if (g.d == 0) {
+        if (g.G < 32) return wv;
+        const int w0 = (b * g.G) >> 5, nw = g.G >> 5;
+        return warp_max_nonneg(lane < nw ? pm[(w0 + lane) * 32] : T(0));
+    }
+    T m = T(0);
+    const int nw = g.NT >> 5;
+    for (int w = 0; w < nw; ++w) m = fmax(m, pm[w * 32 + b]);
+    return m;
+}
+
+template <typename T, bool MHD, int C>
+__device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblock) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    pdl_wait();
+    if (a.tm->done || a.tm->error) return;
+    __shared__ double cflp[3][MAX_WARPS];
+    const SweepGeom& g = a.sg;
+    const int NT = g.NT, S = g.G, d = g.d;
+    const int t = threadIdx.x;
+    SegPos sp;
+    sp.init(g, vblock);
+    const int s = sp.s;
+    T* X1 = reinterpret_cast<T*>(smem);   // [20][NT]: (u, F) of the first cell, then of the last
+    T* X2 = X1 + 20 * NT;                 // [40][NT]: (u*, F*) of cells 0, 1, C-2, C-1
+    T* PM = X2 + 40 * NT;                 // [2][NT/32][32]: per-warp pencil maxima
+    const bool circ_lo = a.mode[CLS_MASS][0] == BC_CIRC, circ_hi = a.mode[CLS_MASS][1] == BC_CIRC;
+    const int ls = d == 0 ? 1 : g.Wb;     // thread distance between consecutive segments of a pencil
+    const bool lo_own = s == 0 && !circ_lo, hi_own = s == S - 1 && !circ_hi;
+    const int lt = s > 0 ? t - ls : (circ_lo ? t + (S - 1) * ls : t);
+    const int rt = s < S - 1 ? t + ls : (circ_hi ? t - (S - 1) * ls : t);
+    const double G = a.gamma;
+    const double dt = a.tm->dt;
+    const T ff = (T)(dt / a.dx);
+    const T half_ffx = (T)(0.5 * (dt / a.dx));
+    const bool vec = d == 0;
+    const long long o0 = sp.base + (long long)s * C * g.sd;
+
+    // ---- stage 1: load, pressure, speed, F -------------------------------------------------------
+    T u[5][C], bb[3][C], F[5][C];
+    double msq[C];
+    if (sp.colok) {
+#pragma unroll
+        for (int v = 0; v < 5; ++v) seg_load<T, C>(a.q[v], o0, g.sd, vec, u[v]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (MHD) seg_load<T, C>(a.q[Q_CBX + c], o0, g.sd, vec, bb[c]);
+            else
+#pragma unroll
+                for (int k = 0; k < C; ++k) bb[c][k] = T(0);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            u[0][k] = T(1);
+            u[1][k] = u[2][k] = u[3][k] = u[4][k] = T(0);
+            bb[0][k] = bb[1][k] = bb[2][k] = T(0);
+        }
+    }
+    T lmax = T(0);
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        double m = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (MHD && a.use_b[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+        msq[k] = m;
+        const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+        const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+        T p;
+        const T spd = press_speed<T>(G, d, uu, m, p);
+        if (sp.colok) lmax = fmax(lmax, spd);
+        T Fk[5];
+        flux_num_t<T>(d, uu, b3, p, Fk);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) F[v][k] = Fk[v];
+    }
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        X1[v * NT + t] = u[v][0];
+        X1[(5 + v) * NT + t] = F[v][0];
+        X1[(10 + v) * NT + t] = u[v][C - 1];
+        X1[(15 + v) * NT + t] = F[v][C - 1];
+    }
+    const T wv1 = seg_max_publish(g, lmax, PM);
+    __syncthreads();
+    const T cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22)
+    T ic;
+    if constexpr (sizeof(T) == 4) ic = __frcp_rn(cf);
+    else ic = T(1) / cf;
+
+    // ---- stage 2: predictor (relaxingFluid.m:30-39) and the half-step pressure, speed, F ----------
+    T us[5][C], Fs[5][C];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        const T uL = lo_own ? u[v][0] : X1[(10 + v) * NT + lt];
+        const T FL = lo_own ? F[v][0] : X1[(15 + v) * NT + lt];
+        const T uR = hi_own ? u[v][C - 1] : X1[v * NT + rt];
+        const T FR = hi_own ? F[v][C - 1] : X1[(5 + v) * NT + rt];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const T um = k > 0 ? u[v][k - 1] : uL, Fm = k > 0 ? F[v][k - 1] : FL;
+            const T up = k < C - 1 ? u[v][k + 1] : uR, Fp = k < C - 1 ? F[v][k + 1] : FR;
+            const T w = F[v][k] * ic;
+            const T Rm = T(0.5) * (um + Fm * ic);
+            const T Lp = T(0.5) * (up - Fp * ic);
+            us[v][k] = u[v][k] - half_ffx * cf * (T(0.5) * (u[v][k] + w) - Rm + T(0.5) * (u[v][k] - w) - Lp);
+        }
+    }
+    T lmax2 = T(0);
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        us[0][k] = us[0][k] > (T)a.minmass ? us[0][k] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
+        if (!sp.colok) { us[0][k] = T(1); us[1][k] = us[2][k] = us[3][k] = us[4][k] = T(0); }
+        const T uu[5] = {us[0][k], us[1][k], us[2][k], us[3][k], us[4][k]};
+        const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+        T p2;
+        const T spd = press_speed<T>(G, d, uu, msq[k], p2);   // relaxingFluid.m:47-50
+        if (sp.colok) lmax2 = fmax(lmax2, spd);
+        T Fk[5];
+        flux_num_t<T>(d, uu, b3, p2, Fk);
+#pragma unroll
+        for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
+    }
+    const int c1 = C > 1 ? 1 : 0;
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        X2[v * NT + t] = us[v][0];
+        X2[(5 + v) * NT + t] = Fs[v][0];
+        X2[(10 + v) * NT + t] = us[v][c1];
+        X2[(15 + v) * NT + t] = Fs[v][c1];
+        X2[(20 + v) * NT + t] = us[v][C - 1 - c1];
+        X2[(25 + v) * NT + t] = Fs[v][C - 1 - c1];
+        X2[(30 + v) * NT + t] = us[v][C - 1];
+        X2[(35 + v) * NT + t] = Fs[v][C - 1];
+    }
+    const T wv2 = seg_max_publish(g, lmax2, PM + (NT >> 5) * 32);
+    __syncthreads();
+    const T cfs = seg_max_collect(g, sp.b, wv2, PM + (NT >> 5) * 32);   // freezing speed of the half step
+    T ics;
+    if constexpr (sizeof(T) == 4) ics = __frcp_rn(cfs);
+    else ics = T(1) / cfs;
+
+    pdl_trigger();
+    // ---- stage 3: corrector fluxes, TVD limiter, update (relaxingFluid.m:52-71) -------------------
+    T unew[5][C];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+        // R* and L* at segment cells -2 .. C+1 (index j + 2)
+        T Rs[C + 4], Ls[C + 4];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const T w = Fs[v][k] * ics;
+            Rs[k + 2] = T(0.5) * (us[v][k] + w);
+            Ls[k + 2] = T(0.5) * (us[v][k] - w);
+        }
+        if (lo_own) {
+            Rs[1] = Rs[2]; Ls[1] = Ls[2];
+            Rs[0] = Rs[2]; Ls[0] = Ls[2];
+        } else {
+            const T u1 = X2[(30 + v) * NT + lt], w1 = X2[(35 + v) * NT + lt] * ics;   // left's last cell
+            const T u2 = X2[(20 + v) * NT + lt], w2 = X2[(25 + v) * NT + lt] * ics;   // left's cell C-2
+            Rs[1] = T(0.5) * (u1 + w1); Ls[1] = T(0.5) * (u1 - w1);
+            Rs[0] = T(0.5) * (u2 + w2); Ls[0] = T(0.5) * (u2 - w2);
+        }
+        if (hi_own) {
+            Rs[C + 2] = Rs[C + 1]; Ls[C + 2] = Ls[C + 1];
+            Rs[C + 3] = Rs[C + 1]; Ls[C + 3] = Ls[C + 1];
+        } else {
+            const T u1 = X2[v * NT + rt], w1 = X2[(5 + v) * NT + rt] * ics;           // right's first cell
+            const T u2 = X2[(10 + v) * NT + rt], w2 = X2[(15 + v) * NT + rt] * ics;   // right's cell 1
+            Rs[C + 2] = T(0.5) * (u1 + w1); Ls[C + 2] = T(0.5) * (u1 - w1);
+            Rs[C + 3] = T(0.5) * (u2 + w2); Ls[C + 3] = T(0.5) * (u2 - w2);
+        }
+        // limited R at cells -1 .. C-1 and limited L at cells 0 .. C (index j + 1)
+        T Rl[C + 1], Ll[C + 2];
+#pragma unroll
+        for (int j = -1; j < C; ++j) {
+            const T r = Rs[j + 2];
+            Rl[j + 1] = r + limiter_corr<T>(a.limiter, r - Rs[j + 1], Rs[j + 3] - r);
+        }
+#pragma unroll
+        for (int j = 0; j <= C; ++j) {
+            const T l = Ls[j + 2];
+            Ll[j + 1] = l + limiter_corr<T>(a.limiter, Ls[j + 1] - l, l - Ls[j + 3]);
+        }
+        if (lo_own) Rl[0] = Rl[1];           // the limited flux's own const ghost
+        if (hi_own) Ll[C + 1] = Ll[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) unew[v][k] = u[v][k] - ff * cfs * (Rl[k + 1] - Rl[k] + Ll[k + 1] - Ll[k + 2]);
+    }
+    double m3[3] = {0.0, 0.0, 0.0};
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        unew[0][k] = unew[0][k] > (T)a.minmass ? unew[0][k] : (T)a.minmass;
+        if (a.cfl && sp.colok) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
+            double sp3[3];
+            cfl_speeds(G, (double)unew[0][k], (double)unew[1][k], (double)unew[2][k], (double)unew[3][k],
+                       (double)unew[4][k], msq[k], sp3);
+            bad = bad || !isfinite(sp3[0] + sp3[1] + sp3[2]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp3[c]);
+        }
+    }
+    if (sp.colok)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) seg_store<T, C>(a.q[v], o0, g.sd, vec, unew[v]);
+    if (a.cfl) {
+        if (a.cfl & CFL_CHECK_NONFINITE) flag_nonfinite(a.tm, bad);
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            m3[c] = warp_max_nonneg(m3[c]);
+            if (lane == 0) cflp[c][warp] = m3[c];
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {   // one global atomic per CTA and direction
+            double m = 0.0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, cflp[threadIdx.x][w]);
+            atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
+        }
+    }
+}
+
+template <typename T, bool MHD, int C>
+__global__ void __launch_bounds__(512, 1) fluid_seg_kernel(const __grid_constant__ FluidArgs a) {
+    fluid_seg_body<T, MHD, C>(a, blockIdx.x);
+}
+
+template <typename T, bool MHD, int C>
+__global__ void __launch_bounds__(512, 1) fluid_seg_batch_kernel(const FluidArgs* __restrict__ args,
+                                                                  const BlockMap* __restrict__ map) {
+    __shared__ FluidArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    fluid_seg_body<T, MHD, C>(sa, (unsigned)bm.block);
+}
+
+}  // namespace img

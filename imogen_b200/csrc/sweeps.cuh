@@ -3,6 +3,8 @@
 #pragma once
 
 #include "magnet_sweep.cuh"
+#include "seg_fluid.cuh"
+#include "seg_magnet.cuh"
 
 namespace img {
 
@@ -17,6 +19,8 @@ struct PencilLaunch {
     bool fade;                 // a fade BC on this sweep direction
     bool cg;                   // copy ghosts (single-CTA pencils, circ/const/fade shifts)
     bool init;                 // fluid sweep / chain: captures stored edges (overrides cg)
+    int seg;                   // cells per thread of the segment fluid kernel (seg_fluid.cuh) or of the window
+                               // magnet kernels (seg_magnet.cuh); 0: the pencil-tile kernels
     cudaStream_t stream;
 };
 
@@ -42,5 +46,7 @@ template <typename T> cudaError_t fluid_attributes(int cpt, int optin);
 template <typename T> cudaError_t chain_attributes(int cpt, int optin);
 // Clusters of the MHD fluid kernel that can be co-resident for launch shape L (0: not schedulable).
 template <typename T> cudaError_t fluid_max_clusters(const PencilLaunch& L, int* n);
+// Shared-memory attributes of the segment fluid kernels (2, 4 and 8 cells per thread; 2 and 4 in FP64).
+template <typename T> cudaError_t fluid_seg_attributes(int optin);
 
 }  // namespace img

@@ -152,14 +152,61 @@ void (*chain_batch_kernel(int cpt, int nqc, int v))(const MagArgs*, const BlockM
 // The CT kernel captures no stored edges: its variant ignores `init` (0 jobs, 1 fade, 2 cg, 3 both).
 inline int ct_variant(bool fade, bool cg) { return (fade ? 1 : 0) | (cg ? 2 : 0); }
 
+// Segment fluid kernels by cells per thread (FP64: 2 and 4).
+template <typename T, bool MHD>
+void (*fluid_seg_kernel_c(int C))(const FluidArgs) {
+    if constexpr (sizeof(T) == 4) {
+        if (C == 8) return fluid_seg_kernel<T, MHD, 8>;
+    }
+    return C == 2 ? fluid_seg_kernel<T, MHD, 2> : fluid_seg_kernel<T, MHD, 4>;
+}
+
+template <typename T, bool MHD>
+void (*fluid_seg_batch_kernel_c(int C))(const FluidArgs*, const BlockMap*) {
+    if constexpr (sizeof(T) == 4) {
+        if (C == 8) return fluid_seg_batch_kernel<T, MHD, 8>;
+    }
+    return C == 2 ? fluid_seg_batch_kernel<T, MHD, 2> : fluid_seg_batch_kernel<T, MHD, 4>;
+}
+
+template <typename T>
+void (*fluid_seg_kernel_p(int C, bool mhd))(const FluidArgs) {
+    return mhd ? fluid_seg_kernel_c<T, true>(C) : fluid_seg_kernel_c<T, false>(C);
+}
+
+template <typename T>
+void (*fluid_seg_batch_kernel_p(int C, bool mhd))(const FluidArgs*, const BlockMap*) {
+    return mhd ? fluid_seg_batch_kernel_c<T, true>(C) : fluid_seg_batch_kernel_c<T, false>(C);
+}
+
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
+    if (L.seg) return launch_pencil_batch(fluid_seg_batch_kernel_p<T>(L.seg, mhd), args, map, L);
     if (L.cluster > 1) return launch_fluid_sweep_batch_cluster<T>(args, map, L, mhd);
     return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 
+// Window magnet kernels by cells per thread (2, 4, 8).
+template <typename T>
+void (*chain_win_kernel(int C))(const MagArgs) {
+    return C == 2 ? mag_chain_win_kernel<T, 2> : (C == 8 ? mag_chain_win_kernel<T, 8> : mag_chain_win_kernel<T, 4>);
+}
+template <typename T>
+void (*ct_win_kernel(int C))(const MagArgs) {
+    return C == 2 ? mag_ct_win_kernel<T, 2> : (C == 8 ? mag_ct_win_kernel<T, 8> : mag_ct_win_kernel<T, 4>);
+}
+template <typename T>
+void (*chain_win_batch_kernel(int C))(const MagArgs*, const BlockMap*) {
+    return C == 2 ? mag_chain_win_batch_kernel<T, 2> : (C == 8 ? mag_chain_win_batch_kernel<T, 8> : mag_chain_win_batch_kernel<T, 4>);
+}
+template <typename T>
+void (*ct_win_batch_kernel(int C))(const MagArgs*, const BlockMap*) {
+    return C == 2 ? mag_ct_win_batch_kernel<T, 2> : (C == 8 ? mag_ct_win_batch_kernel<T, 8> : mag_ct_win_batch_kernel<T, 4>);
+}
+
 template <typename T>
 cudaError_t launch_mag_chain_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
+    if (L.seg) return launch_pencil_batch(chain_win_batch_kernel<T>(L.seg), args, map, L);
     return launch_pencil_batch(chain_batch_kernel<T>(L.cpt, L.nqc, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 
@@ -203,21 +250,25 @@ void (*ctcell_batch_kernel(int cpt, int gv))(const MagArgs*, const BlockMap*) {
 
 template <typename T>
 cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, const PencilLaunch& L) {
+    if (L.seg) return launch_pencil_batch(ct_win_batch_kernel<T>(L.seg), args, map, L);
     return launch_pencil_batch(ctcell_batch_kernel<T>(L.cpt, ct_variant(L.fade, L.cg)), args, map, L);
 }
 
 template <typename T>
 cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd) {
+    if (L.seg) return launch_pencil(fluid_seg_kernel_p<T>(L.seg, mhd), a, L);
     return launch_pencil(fluid_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_chain(const MagArgs& a, const PencilLaunch& L) {
+    if (L.seg) return launch_pencil(chain_win_kernel<T>(L.seg), a, L);
     return launch_pencil(chain_kernel<T>(L.cpt, L.nqc, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
 
 template <typename T>
 cudaError_t launch_mag_ctcell(const MagArgs& a, const PencilLaunch& L) {
+    if (L.seg) return launch_pencil(ct_win_kernel<T>(L.seg), a, L);
     return launch_pencil(ctcell_kernel<T>(L.cpt, ct_variant(L.fade, L.cg)), a, L);
 }
 
@@ -238,6 +289,19 @@ cudaError_t fluid_attributes(int cpt, int optin) {
         cudaError_t e = allow_max_smem(fluid_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e == cudaSuccess) e = allow_max_smem(fluid_batch_kernel<T>(cpt, v & 1, v >> 1), optin);
         if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template <typename T>
+cudaError_t fluid_seg_attributes(int optin) {
+    for (int C : {2, 4, 8}) {
+        if (sizeof(T) == 8 && C == 8) continue;
+        for (int mhd = 0; mhd < 2; ++mhd) {
+            cudaError_t e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0), optin);
+            if (e == cudaSuccess) e = allow_max_smem(fluid_seg_batch_kernel_p<T>(C, mhd != 0), optin);
+            if (e != cudaSuccess) return e;
+        }
     }
     return cudaSuccess;
 }

@@ -277,19 +277,20 @@ class ImogenRun:
 
     def tiling(self, kind="fluid"):
         """{dim: (pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread,
-        transverse components per CTA)} of the fluid or the magnet sweeps."""
+        transverse components per CTA, segment layout)} of the fluid or the magnet sweeps."""
         out = {}
         base = 0 if kind == "fluid" else 3
         for d in (1, 2, 3):
-            t = (ctypes.c_int * 6)()
+            t = (ctypes.c_int * 7)()
             check(lib().img_get_tiling(self._h, base + d, t), self._h)
             out[d] = tuple(t)
         return out
 
     def set_tiling(self, dim, tiling, kind="fluid"):
         """Use one of the accepted tilings for direction dim (1..3) of the fluid or magnet sweeps."""
-        vals = [int(v) for v in tiling] + ([1] if len(tiling) == 5 else [])
-        t = (ctypes.c_int * 6)(*vals)
+        vals = [int(v) for v in tiling]
+        vals += [1, 0][len(vals) - 5:] if len(vals) < 7 else []
+        t = (ctypes.c_int * 7)(*vals)
         check(lib().img_set_tiling(self._h, int(dim) + (0 if kind == "fluid" else 3), t), self._h)
 
     def checkpoint(self):

@@ -177,11 +177,13 @@ int img_autotune(img_ctx* ctx, int trials);
 /* Tiling of slot dim: 1..3 the fluid sweeps along x, y, z, 4..6 the magnet chain along x, y, z
  * (after img_autotune the magnet CT pass may run on a tiling of its own);
  * out = {pencils per CTA, threads per pencil, CTAs per cluster, threads per CTA, cells per thread,
- * transverse components per CTA (magnet: 1 or 2; fluid: 1)}. */
-int img_get_tiling(const img_ctx* ctx, int dim, int out[6]);
+ * transverse components per CTA (magnet: 1 or 2; fluid: 1), segment layout: 1 when each thread owns
+ * consecutive cells -- the segment fluid kernel or the window magnet kernels, used for the steady sweeps
+ * of single-CTA pencils whose shifts are circ or const -- and 0 for the pencil-tile kernels}. */
+int img_get_tiling(const img_ctx* ctx, int dim, int out[7]);
 /* Set the tiling of slot dim to one of those the autotuner may pick (same field order); a magnet
  * slot sets the chain's and the CT pass's tiling. */
-int img_set_tiling(img_ctx* ctx, int dim, const int cfg[6]);
+int img_set_tiling(img_ctx* ctx, int dim, const int cfg[7]);
 
 /* Number of kernels the context has launched so far.  No reference counterpart. */
 int img_launch_count(const img_ctx* ctx, uint64_t* count);

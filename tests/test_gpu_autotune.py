@@ -1,5 +1,7 @@
 """Autotuner (img_autotune): it leaves the state untouched, every tiling it may pick gives the same
-results, and later contexts of the same shape start from the tuned tiling (GPU required)."""
+results (bit for bit within one kernel family; within round-off between the pencil-tile and the
+segment fluid kernels, whose compiled arithmetic may contract differently into FMAs), and later
+contexts of the same shape start from the tuned tiling (GPU required)."""
 import numpy as np
 import pytest
 
@@ -38,8 +40,11 @@ def test_autotune_keeps_state_and_results(precision, case):
         tuned.iterate()
         plain.iterate()
     a, b = tuned.state(), plain.state()
+    same_family = all(x[6] == y[6] for x, y in zip(tuned.tiling().values(), plain.tiling().values()))
+    tol = 0.0 if same_family else (1e-13 if precision == "fp64" else 1e-6)
     for k in a:
-        assert np.array_equal(a[k], b[k]), (k, tuned.tiling(), plain.tiling())
+        rel = float(np.abs(a[k] - b[k]).sum() / max(np.abs(b[k]).sum(), 1e-300))
+        assert rel <= tol, (k, rel, tuned.tiling(), plain.tiling())
     again = _run(s, st, precision)
     assert again.tiling("fluid") == tuned.tiling("fluid") and again.tiling("magnet") == tuned.tiling("magnet")
     for r in (tuned, plain, again):
