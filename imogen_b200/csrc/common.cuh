@@ -110,24 +110,34 @@ template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return a > b
 __device__ __forceinline__ double msign(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : (v == 0 ? 0.0 : v)); }
 __device__ __forceinline__ float msign(float v) { return v > 0 ? 1.f : (v < 0 ? -1.f : (v == 0 ? 0.f : v)); }
 
-// TVD limiter correction (flux/vanleerLimiter.m:9-11, minmodLimiter.m:9, superbeeLimiter.m:9-10).
-// The reference adds it to the flux in place: flux.array = flux.array + correction.
-template <typename T>
-__device__ __forceinline__ T limiter_corr(int lim, T dL, T dR) {
-    if (lim == LIM_VANLEER) {
+// TVD limiter correction (flux/vanleerLimiter.m:9-11, minmodLimiter.m:9, superbeeLimiter.m:9-10) for a
+// limiter known at compile time.  The reference adds it to the flux in place:
+// flux.array = flux.array + correction.
+template <int LIM, typename T>
+__device__ __forceinline__ T limiter_corr_t(T dL, T dR) {
+    if constexpr (LIM == LIM_VANLEER) {
         T p = dL * dR;
         T num = p > T(0) ? p : T(0);
         T st;
         if constexpr (sizeof(T) == 4) st = __fdividef(num, dL + dR);   // mixed form: fast divide
         else st = num / (dL + dR);
         return isnan(st) ? T(0) : st;
+    } else {
+        if constexpr (LIM == LIM_SUPERBEE) {
+            T c = fabs(dL) < fabs(dR) ? T(1) : T(0);
+            dL = (T(1) + c) * dL;
+            dR = (T(2) - c) * dR;
+        }
+        return T(0.125) * (msign(dL) + msign(dR)) * fmin(fabs(dL), fabs(dR));
     }
-    if (lim == LIM_SUPERBEE) {
-        T c = fabs(dL) < fabs(dR) ? T(1) : T(0);
-        dL = (T(1) + c) * dL;
-        dR = (T(2) - c) * dR;
-    }
-    return T(0.125) * (msign(dL) + msign(dR)) * fmin(fabs(dL), fabs(dR));
+}
+
+// The same for a limiter chosen at run time (uniform over a launch).
+template <typename T>
+__device__ __forceinline__ T limiter_corr(int lim, T dL, T dR) {
+    if (lim == LIM_VANLEER) return limiter_corr_t<LIM_VANLEER>(dL, dR);
+    if (lim == LIM_SUPERBEE) return limiter_corr_t<LIM_SUPERBEE>(dL, dR);
+    return limiter_corr_t<LIM_MINMOD>(dL, dR);
 }
 
 // Stored-edge drift of a transparent edge (Edges.m:121-136): move toward the current edge value

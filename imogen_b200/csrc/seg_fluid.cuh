@@ -14,8 +14,11 @@
 //            limiter (relaxingFluid.m:57-62) -- the limited values of the neighbour cells next to the
 //            segment are computed here as well, from the published cells -- and the update
 //            (relaxingFluid.m:64-71); store; fused CFL maxima on the last sweep of a step.
-// The arithmetic of every cell is the same sequence of operations as the pencil-tile kernels
-// (fluid_sweep.cuh), so both give the same bits.
+// Per cell the formulas are those of the pencil-tile kernels (fluid_sweep.cuh); the momentum and
+// cell-centred B are held in sweep-rotated order (the component along the sweep first), so sums over
+// components run in that order, and the compiler may contract differently into FMAs: the two kernel
+// families agree to round-off, not bit for bit.  The limiter is fixed per launch and compiled into the
+// corrector (seg_correct).
 //
 // Thread placement (SweepGeom with G = S segments per pencil, RC = N): along x the S threads of a
 // pencil are consecutive (thread t = b*S + s), along y and z the Wb pencils of the CTA are (t = s*Wb +
@@ -104,22 +107,84 @@ __device__ __forceinline__ void seg_store(void* p, long long o, long long sd, bo
     for (int k = 0; k < C; ++k) a[(long long)k * sd] = v[k];
 }
 
-// The flux numerators F of wFluidFlux.m:31-44 (w = F * (1/c_f)) for one cell: the mixed form's
-// flux_num, and in FP64 the same terms with IEEE reciprocals (the operations of wflux<double>).
+// The flux numerators F of wFluidFlux.m:31-44 (w = F * (1/c_f)) for one cell whose momentum and
+// cell-centred B are held in sweep-rotated order (component 0 along the sweep): the mixed form with the
+// one-instruction FP32 reciprocal of rho, FP64 with the IEEE reciprocal (the operations of wflux).
 template <typename T>
-__device__ __forceinline__ void flux_num_t(int d, const T u[5], const T bb[3], T press, T F[5]) {
+__device__ __forceinline__ void flux_num_rot(const T u[5], const T bb[3], T press, T F[5]) {
+    T ir;
+    if constexpr (sizeof(T) == 4) ir = rcp_approx(u[0]);
+    else ir = T(1) / u[0];
+    const T velocity = u[1] * ir;
+    F[0] = u[1];
+    F[4] = velocity * (u[4] + press) - bb[0] * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
+    F[1] = velocity * u[1] + press - bb[0] * bb[0];
+    F[2] = velocity * u[2] - bb[0] * bb[1];
+    F[3] = velocity * u[3] - bb[0] * bb[2];
+}
+
+// 'totsnd' pressure and the freezing-speed candidate |p_X / rho| + c_s of one cell (rotated order).
+template <typename T>
+__device__ __forceinline__ T press_speed_rot(double G, const T u[5], double msq, T& p) {
     if constexpr (sizeof(T) == 4) {
-        flux_num(d, u, bb, press, F);
+        PressOutF o = pressure_totsnd_mixed(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p;
+        return fabsf(u[1] * rcp_approx(u[0])) + o.cs;
     } else {
-        const T pX = sel3(d, u[1], u[2], u[3]);
-        const T bX = sel3(d, bb[0], bb[1], bb[2]);
-        const T ir = T(1) / u[0];
-        const T velocity = pX * ir;
-        F[0] = pX;
-        F[4] = velocity * (u[4] + press) - bX * (bb[0] * u[1] + bb[1] * u[2] + bb[2] * u[3]) * ir;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) F[1 + c] = velocity * u[1 + c] + press * (c == d ? T(1) : T(0)) - bX * bb[c];
+        PressOut o = pressure_totsnd(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p + 0.0;   // + viscosity.solve ('empty' -> 0)
+        return fabs(u[1] * (1.0 / u[0])) + o.cs;
     }
+}
+
+// Corrector (relaxingFluid.m:52-71) of one variable over a segment: R* = (u* + F*/c_f*)/2 and
+// L* = (u* - F*/c_f*)/2 at cells -2 .. C+1 (neighbour cells from the published exchange set X2), the
+// TVD limiter at cells -1 .. C (only those the update reads), and the update of the C own cells.
+// LIM: the launch's limiter (flux/*Limiter.m), fixed at compile time.
+template <typename T, int C, int LIM>
+__device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], const T (&Fs)[C], const T* X2v, int NT,
+                                            int lt, int rt, bool lo_own, bool hi_own, T ics, T ffc, T (&unew)[C]) {
+    T Rs[C + 4], Ls[C + 4];
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        const T w = Fs[k] * ics;
+        Rs[k + 2] = T(0.5) * (us[k] + w);
+        Ls[k + 2] = T(0.5) * (us[k] - w);
+    }
+    if (lo_own) {
+        Rs[1] = Rs[2]; Ls[1] = Ls[2];
+        Rs[0] = Rs[2]; Ls[0] = Ls[2];
+    } else {   // X2v holds [u*, F*] x [cell 0, cell 1, cell C-2, cell C-1] at strides of 5*NT
+        const T u1 = X2v[30 * NT + lt], w1 = X2v[35 * NT + lt] * ics;   // left's last cell
+        const T u2 = X2v[20 * NT + lt], w2 = X2v[25 * NT + lt] * ics;   // left's cell C-2
+        Rs[1] = T(0.5) * (u1 + w1); Ls[1] = T(0.5) * (u1 - w1);
+        Rs[0] = T(0.5) * (u2 + w2); Ls[0] = T(0.5) * (u2 - w2);
+    }
+    if (hi_own) {
+        Rs[C + 2] = Rs[C + 1]; Ls[C + 2] = Ls[C + 1];
+        Rs[C + 3] = Rs[C + 1]; Ls[C + 3] = Ls[C + 1];
+    } else {
+        const T u1 = X2v[rt], w1 = X2v[5 * NT + rt] * ics;                // right's first cell
+        const T u2 = X2v[10 * NT + rt], w2 = X2v[15 * NT + rt] * ics;      // right's cell 1
+        Rs[C + 2] = T(0.5) * (u1 + w1); Ls[C + 2] = T(0.5) * (u1 - w1);
+        Rs[C + 3] = T(0.5) * (u2 + w2); Ls[C + 3] = T(0.5) * (u2 - w2);
+    }
+    // limited R at cells -1 .. C-1 and limited L at cells 0 .. C (index j + 1)
+    T Rl[C + 1], Ll[C + 2];
+#pragma unroll
+    for (int j = -1; j < C; ++j) {
+        const T r = Rs[j + 2];
+        Rl[j + 1] = r + limiter_corr_t<LIM>(r - Rs[j + 1], Rs[j + 3] - r);
+    }
+#pragma unroll
+    for (int j = 0; j <= C; ++j) {
+        const T l = Ls[j + 2];
+        Ll[j + 1] = l + limiter_corr_t<LIM>(Ls[j + 1] - l, l - Ls[j + 3]);
+    }
+    if (lo_own) Rl[0] = Rl[1];   // the limited flux's own const ghost
+    if (hi_own) Ll[C + 1] = Ll[C];
+#pragma unroll
+    for (int k = 0; k < C; ++k) unew[k] = u[k] - ffc * (Rl[k + 1] - Rl[k] + Ll[k + 1] - Ll[k + 2]);
 }
 
 // Pencil maximum of non-negative speeds in the segment layout.  publish: reduce over the lanes of the
@@ -166,7 +231,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     if (a.tm->done || a.tm->error) return;
     __shared__ double cflp[3][MAX_WARPS];
     const SweepGeom& g = a.sg;
-    const int NT = g.NT, S = g.G, d = g.d;
+    const int NT = g.NT, S = g.G, d = g.d, d1 = g.d1, d2 = g.d2;
     const int t = threadIdx.x;
     SegPos sp;
     sp.init(g, vblock);
@@ -185,19 +250,23 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     const T half_ffx = (T)(0.5 * (dt / a.dx));
     const bool vec = d == 0;
     const long long o0 = sp.base + (long long)s * C * g.sd;
+    // momentum and cell-centred B in sweep-rotated order: component 0 along the sweep, then d1, d2
+    void* qv[5] = {a.q[Q_RHO], a.q[Q_PX + d], a.q[Q_PX + d1], a.q[Q_PX + d2], a.q[Q_E]};
+    const bool ub[3] = {a.use_b[d] != 0, a.use_b[d1] != 0, a.use_b[d2] != 0};
 
     // ---- stage 1: load, pressure, speed, F -------------------------------------------------------
     T u[5][C], bb[3][C], F[5][C];
     double msq[C];
     if (sp.colok) {
 #pragma unroll
-        for (int v = 0; v < 5; ++v) seg_load<T, C>(a.q[v], o0, g.sd, vec, u[v]);
+        for (int v = 0; v < 5; ++v) seg_load<T, C>(qv[v], o0, g.sd, vec, u[v]);
+        if (MHD) {
+            seg_load<T, C>(a.q[Q_CBX + d], o0, g.sd, vec, bb[0]);
+            seg_load<T, C>(a.q[Q_CBX + d1], o0, g.sd, vec, bb[1]);
+            seg_load<T, C>(a.q[Q_CBX + d2], o0, g.sd, vec, bb[2]);
+        } else {
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            if (MHD) seg_load<T, C>(a.q[Q_CBX + c], o0, g.sd, vec, bb[c]);
-            else
-#pragma unroll
-                for (int k = 0; k < C; ++k) bb[c][k] = T(0);
+            for (int k = 0; k < C; ++k) bb[0][k] = bb[1][k] = bb[2][k] = T(0);
         }
     } else {
 #pragma unroll
@@ -213,15 +282,15 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         double m = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            if (MHD && a.use_b[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+            if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
         msq[k] = m;
         const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
         const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
         T p;
-        const T spd = press_speed<T>(G, d, uu, m, p);
+        const T spd = press_speed_rot<T>(G, uu, m, p);
         if (sp.colok) lmax = fmax(lmax, spd);
         T Fk[5];
-        flux_num_t<T>(d, uu, b3, p, Fk);
+        flux_num_rot<T>(uu, b3, p, Fk);
 #pragma unroll
         for (int v = 0; v < 5; ++v) F[v][k] = Fk[v];
     }
@@ -241,21 +310,21 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
 
     // ---- stage 2: predictor (relaxingFluid.m:30-39) and the half-step pressure, speed, F ----------
     T us[5][C], Fs[5][C];
+    const T hfc = half_ffx * cf;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-        const T uL = lo_own ? u[v][0] : X1[(10 + v) * NT + lt];
-        const T FL = lo_own ? F[v][0] : X1[(15 + v) * NT + lt];
-        const T uR = hi_own ? u[v][C - 1] : X1[v * NT + rt];
-        const T FR = hi_own ? F[v][C - 1] : X1[(5 + v) * NT + rt];
+        // R = (u + F/c_f)/2 at cells -1 .. C-1 (index j + 1), L = (u - F/c_f)/2 at cells 0 .. C (index j)
+        T R[C + 1], L[C + 1];
 #pragma unroll
         for (int k = 0; k < C; ++k) {
-            const T um = k > 0 ? u[v][k - 1] : uL, Fm = k > 0 ? F[v][k - 1] : FL;
-            const T up = k < C - 1 ? u[v][k + 1] : uR, Fp = k < C - 1 ? F[v][k + 1] : FR;
             const T w = F[v][k] * ic;
-            const T Rm = T(0.5) * (um + Fm * ic);
-            const T Lp = T(0.5) * (up - Fp * ic);
-            us[v][k] = u[v][k] - half_ffx * cf * (T(0.5) * (u[v][k] + w) - Rm + T(0.5) * (u[v][k] - w) - Lp);
+            R[k + 1] = T(0.5) * (u[v][k] + w);
+            L[k] = T(0.5) * (u[v][k] - w);
         }
+        R[0] = lo_own ? R[1] : T(0.5) * (X1[(10 + v) * NT + lt] + X1[(15 + v) * NT + lt] * ic);
+        L[C] = hi_own ? L[C - 1] : T(0.5) * (X1[v * NT + rt] - X1[(5 + v) * NT + rt] * ic);
+#pragma unroll
+        for (int k = 0; k < C; ++k) us[v][k] = u[v][k] - hfc * (R[k + 1] - R[k] + L[k] - L[k + 1]);
     }
     T lmax2 = T(0);
 #pragma unroll
@@ -265,10 +334,10 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         const T uu[5] = {us[0][k], us[1][k], us[2][k], us[3][k], us[4][k]};
         const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
         T p2;
-        const T spd = press_speed<T>(G, d, uu, msq[k], p2);   // relaxingFluid.m:47-50
+        const T spd = press_speed_rot<T>(G, uu, msq[k], p2);   // relaxingFluid.m:47-50
         if (sp.colok) lmax2 = fmax(lmax2, spd);
         T Fk[5];
-        flux_num_t<T>(d, uu, b3, p2, Fk);
+        flux_num_rot<T>(uu, b3, p2, Fk);
 #pragma unroll
         for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
     }
@@ -294,52 +363,18 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     pdl_trigger();
     // ---- stage 3: corrector fluxes, TVD limiter, update (relaxingFluid.m:52-71) -------------------
     T unew[5][C];
+    const T ffc = ff * cfs;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-        // R* and L* at segment cells -2 .. C+1 (index j + 2)
-        T Rs[C + 4], Ls[C + 4];
-#pragma unroll
-        for (int k = 0; k < C; ++k) {
-            const T w = Fs[v][k] * ics;
-            Rs[k + 2] = T(0.5) * (us[v][k] + w);
-            Ls[k + 2] = T(0.5) * (us[v][k] - w);
-        }
-        if (lo_own) {
-            Rs[1] = Rs[2]; Ls[1] = Ls[2];
-            Rs[0] = Rs[2]; Ls[0] = Ls[2];
-        } else {
-            const T u1 = X2[(30 + v) * NT + lt], w1 = X2[(35 + v) * NT + lt] * ics;   // left's last cell
-            const T u2 = X2[(20 + v) * NT + lt], w2 = X2[(25 + v) * NT + lt] * ics;   // left's cell C-2
-            Rs[1] = T(0.5) * (u1 + w1); Ls[1] = T(0.5) * (u1 - w1);
-            Rs[0] = T(0.5) * (u2 + w2); Ls[0] = T(0.5) * (u2 - w2);
-        }
-        if (hi_own) {
-            Rs[C + 2] = Rs[C + 1]; Ls[C + 2] = Ls[C + 1];
-            Rs[C + 3] = Rs[C + 1]; Ls[C + 3] = Ls[C + 1];
-        } else {
-            const T u1 = X2[v * NT + rt], w1 = X2[(5 + v) * NT + rt] * ics;           // right's first cell
-            const T u2 = X2[(10 + v) * NT + rt], w2 = X2[(15 + v) * NT + rt] * ics;   // right's cell 1
-            Rs[C + 2] = T(0.5) * (u1 + w1); Ls[C + 2] = T(0.5) * (u1 - w1);
-            Rs[C + 3] = T(0.5) * (u2 + w2); Ls[C + 3] = T(0.5) * (u2 - w2);
-        }
-        // limited R at cells -1 .. C-1 and limited L at cells 0 .. C (index j + 1)
-        T Rl[C + 1], Ll[C + 2];
-#pragma unroll
-        for (int j = -1; j < C; ++j) {
-            const T r = Rs[j + 2];
-            Rl[j + 1] = r + limiter_corr<T>(a.limiter, r - Rs[j + 1], Rs[j + 3] - r);
-        }
-#pragma unroll
-        for (int j = 0; j <= C; ++j) {
-            const T l = Ls[j + 2];
-            Ll[j + 1] = l + limiter_corr<T>(a.limiter, Ls[j + 1] - l, l - Ls[j + 3]);
-        }
-        if (lo_own) Rl[0] = Rl[1];           // the limited flux's own const ghost
-        if (hi_own) Ll[C + 1] = Ll[C];
-#pragma unroll
-        for (int k = 0; k < C; ++k) unew[v][k] = u[v][k] - ff * cfs * (Rl[k + 1] - Rl[k] + Ll[k + 1] - Ll[k + 2]);
+        const T* X2v = X2 + v * NT;
+        if (a.limiter == LIM_VANLEER)
+            seg_correct<T, C, LIM_VANLEER>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
+        else if (a.limiter == LIM_SUPERBEE)
+            seg_correct<T, C, LIM_SUPERBEE>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
+        else
+            seg_correct<T, C, LIM_MINMOD>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
     }
-    double m3[3] = {0.0, 0.0, 0.0};
+    double m3[3] = {0.0, 0.0, 0.0};   // rotated order
     bool bad = false;
 #pragma unroll
     for (int k = 0; k < C; ++k) {
@@ -355,7 +390,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     }
     if (sp.colok)
 #pragma unroll
-        for (int v = 0; v < 5; ++v) seg_store<T, C>(a.q[v], o0, g.sd, vec, unew[v]);
+        for (int v = 0; v < 5; ++v) seg_store<T, C>(qv[v], o0, g.sd, vec, unew[v]);
     if (a.cfl) {
         if (a.cfl & CFL_CHECK_NONFINITE) flag_nonfinite(a.tm, bad);
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -365,9 +400,10 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
             if (lane == 0) cflp[c][warp] = m3[c];
         }
         __syncthreads();
-        if (threadIdx.x < 3) {   // one global atomic per CTA and direction
+        if (threadIdx.x < 3) {   // one global atomic per CTA and direction (rotated slot of direction t)
+            const int rc = threadIdx.x == d ? 0 : (threadIdx.x == d1 ? 1 : 2);
             double m = 0.0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, cflp[threadIdx.x][w]);
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, cflp[rc][w]);
             atomic_max_nonneg(&a.tm->maxbits[threadIdx.x], m);
         }
     }

@@ -13,12 +13,32 @@ from tests.parity import smooth_state
 pytestmark = pytest.mark.gpu
 
 
+def _segment_tiling(n, d):
+    """A segment fluid tiling for a pencil of n cells along dim d (the rules of the kernel's candidates)."""
+    for C in (4, 2):
+        if n % C:
+            continue
+        S = n // C
+        if d == 1 and not (S % 32 == 0 or (S <= 32 and 32 % S == 0)):
+            continue
+        for Wb in ((1, 2, 4, 8) if d == 1 else (8, 16, 32, 4)):
+            NT = Wb * S
+            if 64 <= NT <= 512 and NT % 32 == 0:
+                return (Wb, S, 1, NT, C, 1, 1)
+    return None
+
+
 def _run(settings, state, precision, tile, monkeypatch, iters=6):
     if tile:
         monkeypatch.setenv("IMOGEN_B200_TILE_KERNELS", "1")
     else:
         monkeypatch.delenv("IMOGEN_B200_TILE_KERNELS", raising=False)
     r = ImogenRun(precision=precision, **settings)
+    if not tile and precision == "fp64":   # the FP64 default is the tile kernel: pick segment tilings
+        for d, n in enumerate(settings["grid"], 1):
+            t = _segment_tiling(n, d) if n >= 3 else None
+            if t:
+                r.set_tiling(d, t)
     r.set_state(*state)
     r.run(iters)
     return r
