@@ -26,6 +26,7 @@ SYMBOLS = (
     "img_get_time", "img_set_time", "img_progress", "img_checkpoint_bytes", "img_checkpoint_save",
     "img_checkpoint_load", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count", "img_sweep_order",
+    "img_source", "img_radiation_strength",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -48,6 +49,12 @@ class ImgConfig(ctypes.Structure):
         ("update_mode", ctypes.c_int),
         ("precision", ctypes.c_int),
         ("nonfinite_check", ctypes.c_int),
+        ("viscosity_type", ctypes.c_int),
+        ("visc_linear", ctypes.c_double),
+        ("visc_quadratic", ctypes.c_double),
+        ("radiation_type", ctypes.c_int),
+        ("rad_exponent", ctypes.c_double),
+        ("rad_initial_maximum", ctypes.c_double),
     ]
 
 
@@ -116,6 +123,10 @@ def lib():
     L.img_launch_count.restype = ctypes.c_int
     L.img_sweep_order.argtypes = [ctypes.c_int, ctypes.c_int, ip]
     L.img_sweep_order.restype = ctypes.c_int
+    L.img_source.argtypes = [vp]
+    L.img_source.restype = ctypes.c_int
+    L.img_radiation_strength.argtypes = [vp, dp]
+    L.img_radiation_strength.restype = ctypes.c_int
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]
     L.img_batch_add.argtypes = [vp, vp]

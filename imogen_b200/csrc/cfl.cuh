@@ -13,42 +13,79 @@ namespace img {
 
 struct CflArgs {
     Geom g;
-    const void* q[NQ];
+    void* q[NQ];
     DevTime* tm;
     double gamma;
     int mhd;
     int use_b[3];
     int check_nonfinite;   // flag a non-finite speed candidate (DERR_NONFINITE_STATE)
+    int accumulate;        // accumulate the CFL maxima (0: the radiation sink alone)
+    int radiate;           // first apply the optically thin radiation sink to E (source.m:30)
+    double rad_exp;        // Radiation.exponent
 };
 
-// CFL maxima of one grid, run by block vblock of vgrid blocks of that grid's launch.
+// pressure(ENUM.PRESSURE_GAS, ...) of one cell (pressure.m:16-66): (G-1)(E - rho v^2/2) minus
+// (G-1) B^2/2 (msq: the components without isZero), floored at 0; the reference's operation order,
+// no FMA contraction.
+__device__ __forceinline__ double gas_pressure(double G, double rho, double px, double py, double pz, double E,
+                                               double msq) {
+    const double vel_sq = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz)) / __dmul_rn(rho, rho);
+    double r = __dmul_rn(G - 1.0, __dsub_rn(E, __dmul_rn(__dmul_rn(0.5, rho), vel_sq)));
+    r = __dsub_rn(r, __dmul_rn(__dmul_rn(G - 1.0, 0.5), msq));
+    return r < 0 ? 0.0 : r;
+}
+
+// Radiation.opticallyThinSolver (fluid/Radiation.m:86-88): (s rho^(2-a)) P_gas^a.
+__device__ __forceinline__ double thin_radiation(double s, double a, double rho, double gas) {
+    return __dmul_rn(__dmul_rn(s, pow(rho, 2.0 - a)), pow(gas, a));
+}
+
+// Sum of squares of the cell-centred B components without isZero, in component order.
+template <typename T>
+__device__ __forceinline__ double cell_msq(const CflArgs& a, const T* const cb[3], long long i) {
+    double msq = 0.0;
+    if (a.mhd) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (a.use_b[c]) { double b = cb[c][i]; msq = msq + b * b; }
+    }
+    return msq;
+}
+
+// CFL maxima of one grid, run by block vblock of vgrid blocks of that grid's launch; with `radiate`
+// the radiation sink E <- E - dt * radiation.solve (source.m:30) is applied to each cell first (its
+// CFL candidates are then those of the new E).
 template <typename T>
 __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vblock, unsigned vgrid) {
     if (a.tm->done || a.tm->error) return;
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
                      reinterpret_cast<const T*>(a.q[Q_PZ])};
-    const T* E = reinterpret_cast<const T*>(a.q[Q_E]);
-    const T* cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
-                      reinterpret_cast<const T*>(a.q[Q_CBZ])};
+    T* E = reinterpret_cast<T*>(a.q[Q_E]);
+    const T* const cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
+                            reinterpret_cast<const T*>(a.q[Q_CBZ])};
+    const double dt = a.tm->dt, rs = a.tm->rad_strength;
     double m3[3] = {0.0, 0.0, 0.0};
     bool bad = false;
     for (long long i = vblock * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
          i += (long long)vgrid * blockDim.x) {
         double r = rho[i], px = p[0][i], py = p[1][i], pz = p[2][i];
-        double msq = 0.0;
-        if (a.mhd) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (a.use_b[c]) { double b = cb[c][i]; msq = msq + b * b; }
+        const double msq = cell_msq<T>(a, cb, i);
+        double e = (double)E[i];
+        if (a.radiate) {
+            const double gas = gas_pressure(a.gamma, r, px, py, pz, e, msq);
+            E[i] = (T)__dsub_rn(e, __dmul_rn(dt, thin_radiation(rs, a.rad_exp, r, gas)));
+            e = (double)E[i];
         }
+        if (!a.accumulate) continue;
         double sp[3];
-        cfl_speeds(a.gamma, r, px, py, pz, (double)E[i], msq, sp);
+        cfl_speeds(a.gamma, r, px, py, pz, e, msq, sp);
         bad = bad || !isfinite(sp[0] + sp[1] + sp[2]);
         m3[0] = fmax(m3[0], sp[0]);
         m3[1] = fmax(m3[1], sp[1]);
         m3[2] = fmax(m3[2], sp[2]);
     }
+    if (!a.accumulate) return;   // uniform per launch
     if (a.check_nonfinite) flag_nonfinite(a.tm, bad);
     __shared__ double wp[3][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -78,6 +115,40 @@ __global__ void __launch_bounds__(256) cfl_reduce_batch_kernel(const CflArgs* __
     load_member_args(sa, args + bm.member);
     __syncthreads();
     cfl_reduce_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
+}
+
+// Radiation.initialize (fluid/Radiation.m:61-75), first part: the minimum over the cells of
+// (E - KE - ME) / unscaledRadiation, KE = (p.p)/(2 rho), ME = (B.B)/2 of the face-centred B, the
+// unscaled solver with strength 1 (NaN cells are skipped, as MATLAB's min does), into tm->rad_minbits
+// (which the host sets to the bits of +inf first).
+template <typename T>
+__global__ void __launch_bounds__(256) rad_init_kernel(const __grid_constant__ CflArgs a) {
+    const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
+    const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
+                     reinterpret_cast<const T*>(a.q[Q_PZ])};
+    const T* E = reinterpret_cast<const T*>(a.q[Q_E]);
+    const T* const cb[3] = {reinterpret_cast<const T*>(a.q[Q_CBX]), reinterpret_cast<const T*>(a.q[Q_CBY]),
+                            reinterpret_cast<const T*>(a.q[Q_CBZ])};
+    const T* B[3] = {reinterpret_cast<const T*>(a.q[Q_BX]), reinterpret_cast<const T*>(a.q[Q_BY]),
+                     reinterpret_cast<const T*>(a.q[Q_BZ])};
+    double m = __longlong_as_double(0x7ff0000000000000ll);   // +inf
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.g.ncell;
+         i += (long long)gridDim.x * blockDim.x) {
+        const double r = rho[i], px = p[0][i], py = p[1][i], pz = p[2][i], e = E[i];
+        const double bx = B[0][i], by = B[1][i], bz = B[2][i];
+        const double unscaled = thin_radiation(1.0, a.rad_exp, r, gas_pressure(a.gamma, r, px, py, pz, e, cell_msq<T>(a, cb, i)));
+        const double kinetic = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz))) / r;
+        const double magnetic = __dmul_rn(0.5, __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz)));
+        const double ratio = __dsub_rn(__dsub_rn(e, kinetic), magnetic) / unscaled;
+        if (ratio == ratio) m = fmin(m, ratio);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&a.tm->rad_minbits, ordered_bits(m));
+}
+
+// Radiation.initialize, second part: strength = initialMaximum / 100 * minimum.
+__global__ void rad_init_finalize_kernel(DevTime* tm, double scale) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) tm->rad_strength = scale * from_ordered_bits(tm->rad_minbits);
 }
 
 // check_running: evaluate TimeManager.running (time < TIMEMAX) first, as imogen.m:58 does at the

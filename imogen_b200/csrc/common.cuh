@@ -65,6 +65,8 @@ struct DevTime {
     unsigned long long maxbits[3];   // per-direction max of |v_i| + c_s (bit pattern, >= 0)
     unsigned int counter;            // CTAs finished in the current CFL reduction
     unsigned int pad2;
+    double rad_strength;             // Radiation.strength (set by Radiation.initialize at set_state)
+    unsigned long long rad_minbits;  // ordered bits of the running minimum of Radiation.initialize
 };
 
 // ---- batched launches -----------------------------------------------------------------------------
@@ -299,6 +301,16 @@ __device__ __forceinline__ void flag_nonfinite(DevTime* tm, bool bad) {
 // Atomic max of a non-negative double through its bit pattern (NaN never reaches here).
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// Doubles of either sign as unsigned integers of the same order (the callers exclude NaN).
+__device__ __forceinline__ unsigned long long ordered_bits(double v) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double from_ordered_bits(unsigned long long b) {
+    b = (b >> 63) ? (b & 0x7fffffffffffffffull) : ~b;
+    return __longlong_as_double((long long)b);
 }
 
 }  // namespace img

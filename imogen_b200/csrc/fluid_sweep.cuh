@@ -39,7 +39,14 @@ struct FluidArgs {
     int use_b[3];          // pressure.m:28-33 skips components with isZero set
     int cfl;               // accumulate the CFL maxima of the new state (fused TimeManager pass);
                            // with CFL_CHECK_NONFINITE also flag a non-finite state
+    // artificial viscosity (fluid/ArtificialViscosity.m; segment kernels only): VISC_* type, the
+    // linear and quadratic strengths c1, c2, and c2 (G+1), c2^2 ((G+1)/4)^2, c1^2 formed on the host
+    int visc;
+    double vc1, vc2, vk1, vk2, vc1sq;
 };
+constexpr int VISC_NONE = 0;
+constexpr int VISC_NR = 1;    // Neumann-Richtmyer (ArtificialViscosity.m:73-77)
+constexpr int VISC_CSW = 2;   // Caramana-Shashkov-Whalen (ArtificialViscosity.m:81-148)
 constexpr int CFL_ACCUMULATE = 1;
 constexpr int CFL_CHECK_NONFINITE = 2;
 

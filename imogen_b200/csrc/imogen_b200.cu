@@ -355,12 +355,12 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d, size_t elem) {
 // in FP64), the whole pencil in one CTA of NT = Wb * S threads, 64 <= NT <= 512, S = N / C threads per
 // pencil.  Along x the S threads of a pencil are consecutive lanes: S is a power of two up to 32 or a
 // multiple of 32.  Along y and z Wb >= 4 pencils (a power of two) sit side by side.
-std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem) {
+std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool visc = false) {
     std::vector<PencilCfg> out;
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
     for (int C : {2, 4, 8}) {
-        if ((elem == 8 && C == 8) || N % C) continue;
+        if ((elem == 8 && C == 8) || (visc && C == 8) || N % C) continue;
         const int S = N / C;
         if (d == 0 && !(S % 32 == 0 || (S <= 32 && 32 % S == 0))) continue;
         for (int Wb = d == 0 ? 1 : 4; Wb <= 32; Wb *= 2) {
@@ -368,7 +368,7 @@ std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem) {
             if (NT > 512) break;
             if (NT < 64 || NT % 32) continue;
             if (Wb > 1 && (long long)Wb / 2 >= ncol) break;   // more pencil slots than pencils
-            const size_t smem = elem == 8 ? seg_fluid_smem_bytes<double>(NT) : seg_fluid_smem_bytes<float>(NT);
+            const size_t smem = elem == 8 ? seg_fluid_smem_bytes<double>(NT, visc) : seg_fluid_smem_bytes<float>(NT, visc);
             if (smem > kPencilSmemLimit) continue;
             PencilCfg p;
             p.Wb = Wb;
@@ -438,6 +438,23 @@ PencilCfg choose_fluid(const Geom& g, int d, size_t elem, const PencilCfg& tile)
     return best ? *best : tile;
 }
 
+// Fluid tiling with artificial viscosity: the segment kernel is the only one with the viscous
+// exchanges; 4 cells per thread in the mixed form and 2 in FP64 (fewer registers), along y and z at
+// least 8 pencils side by side where possible, the CTA nearest 256 threads.  ok = false: no segment
+// tiling exists for this pencil length.
+PencilCfg choose_fluid_visc(const Geom& g, int d, size_t elem, bool& ok) {
+    const int want = elem == 8 ? 2 : 4;
+    const PencilCfg* best = nullptr;
+    std::vector<PencilCfg> c = seg_candidates(g, d, elem, true);
+    auto score = [&](const PencilCfg& p) {
+        return (p.seg == want ? 0 : 4096) + ((d != 0 && p.Wb < 8) ? 2048 : 0) + std::abs(p.NT - 256);
+    };
+    for (const PencilCfg& p : c)
+        if (!best || score(p) < score(*best)) best = &p;
+    ok = best != nullptr;
+    return ok ? *best : PencilCfg{};
+}
+
 // Pencil tiling of one sweep direction: one cell per thread where the pencil fits a cluster of at
 // most 4 CTAs of 512 threads (2 or 4 cells per thread otherwise).  Along x a CTA holds whole pencil
 // segments of up to 512 rows; along y and z it holds 4 adjacent pencils, so each row of the tile is
@@ -505,14 +522,14 @@ PencilCfg choose_pencil(const Geom& g, int d, size_t elem) {
 // Process-wide cache of autotuned tilings, keyed by what decides them: sweep direction, pencil
 // length, number of pencils (rounded up to a power of two), precision and physics.  Contexts
 // created later with the same key start from the tuned tiling.
-using TuneKey = std::tuple<int, int, int, int, int, int, int>;
+using TuneKey = std::tuple<int, int, int, int, int, int, int, int>;
 std::mutex g_tune_mu;
 std::map<TuneKey, PencilCfg> g_tuned;
 
 TuneKey tune_key(int kind, const Geom& g, int d, size_t elem, const img_config& c) {
     const long long ncol = g.ncell / g.n[d];
     return TuneKey(kind, d, g.n[d], pow2ceil((int)std::min<long long>(ncol, 1 << 30)), (int)elem, c.fluid_active,
-                   c.magnet_active);
+                   c.magnet_active, c.viscosity_type);
 }
 
 int launch_blocks(long long work, int bs = 256) {
@@ -588,6 +605,10 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
             const int m = c.bc_modes[k][side][d];
             if ((m != IMG_BC_CIRC && m != IMG_BC_CONST) || m != c.bc_modes[CLS_MASS][side][d]) seg_ok = false;
         }
+    // with artificial viscosity the tiling is always a segment one and every swept end circ or const
+    // (img_create and img_set_tiling see to it), so no stored edge is ever read: the first sweeps too
+    const bool visc = c.viscosity_type != IMG_VISC_NONE;
+    if (visc) seg_ok = true;
     const PencilCfg& pcf = (seg_ok || !ctx->pcfg[0][d].seg) ? ctx->pcfg[0][d] : ctx->pcfg_tile[d];
     a.sg = sweep_geom(ctx, d, pcf);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
@@ -610,8 +631,17 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.cfl = cfl ? (CFL_ACCUMULATE | (c.nonfinite_check ? CFL_CHECK_NONFINITE : 0)) : 0;
+    a.visc = c.viscosity_type;
+    if (visc) {   // ArtificialViscosity.m:73-77, 139-147
+        const double G = c.gamma, c1 = c.visc_linear, c2 = c.visc_quadratic, g4 = (G + 1) / 4;
+        a.vc1 = c1;
+        a.vc2 = c2;
+        a.vk1 = c2 * (G + 1);
+        a.vk2 = (c2 * c2) * (g4 * g4);
+        a.vc1sq = c1 * c1;
+    }
     PencilLaunch L = pencil_launch<T>(ctx, pcf, d,
-                                      pcf.seg ? seg_fluid_smem_bytes<T>(pcf.NT) : fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb),
+                                      pcf.seg ? seg_fluid_smem_bytes<T>(pcf.NT, visc) : fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb),
                                       1, fade);
     L.seg = pcf.seg;
     // copy ghosts: single-CTA pencils, one circ, const or fade mode per side shared by the fluid classes
@@ -742,7 +772,7 @@ int launch_magnet(img_ctx* ctx, int X, int I1, int I2) {
 }
 
 template <typename T>
-int launch_cfl_reduce(img_ctx* ctx) {
+CflArgs cfl_args(img_ctx* ctx) {
     CflArgs a{};
     a.g = ctx->g;
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
@@ -751,7 +781,20 @@ int launch_cfl_reduce(img_ctx* ctx) {
     a.mhd = ctx->mhd;
     for (int k = 0; k < 3; ++k) a.use_b[k] = ctx->use_b[k];
     a.check_nonfinite = ctx->cfg.nonfinite_check != 0;
+    a.accumulate = 1;
+    a.rad_exp = ctx->cfg.rad_exponent;
+    return a;
+}
+
+// The CFL maxima pass; with `radiate` the radiation sink first (source.m:30), and with accumulate =
+// false the sink alone.
+template <typename T>
+int launch_cfl_reduce(img_ctx* ctx, bool accumulate = true, bool radiate = false) {
+    CflArgs a = cfl_args<T>(ctx);
+    a.accumulate = accumulate ? 1 : 0;
+    a.radiate = radiate ? 1 : 0;
     if (ctx->rec) {
+        if (radiate) return fail(ctx, IMG_ERR_UNSUPPORTED, "radiation in a batched launch");
         OpRec r{};
         r.kind = OP_CFL_REDUCE;
         r.elem = sizeof(T);
@@ -813,6 +856,27 @@ int magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
 }
 int cfl_reduce(img_ctx* ctx) { return ctx->elem == 8 ? launch_cfl_reduce<double>(ctx) : launch_cfl_reduce<float>(ctx); }
 
+// source(run, ...) of source.m:1-36 for this path: the radiation sink (source.m:30); nothing
+// without radiation.  accumulate: the same pass collects the CFL maxima of the new state for the
+// next TimeManager.update.
+int source_sink(img_ctx* ctx, bool accumulate) {
+    if (ctx->cfg.radiation_type == IMG_RAD_NONE) return IMG_OK;
+    return ctx->elem == 8 ? launch_cfl_reduce<double>(ctx, accumulate, true) : launch_cfl_reduce<float>(ctx, accumulate, true);
+}
+
+// Radiation.initialize (fluid/Radiation.m:61-75) from the state on the device; tm->rad_minbits holds
+// the bits of +inf between calls (set at creation, reset by the finalisation).
+template <typename T>
+int radiation_initialize(img_ctx* ctx) {
+    const CflArgs a = cfl_args<T>(ctx);
+    rad_init_kernel<T><<<launch_blocks(ctx->g.ncell), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    rad_init_finalize_kernel<<<1, 32, 0, ctx->stream>>>(ctx->tm, ctx->cfg.rad_initial_maximum / 100);
+    CK(cudaGetLastError());
+    ctx->launches += 2;
+    return IMG_OK;
+}
+
 // flux.m:17-62 for one half step.  `fuse_cfl`: the final fluid sweep accumulates the CFL maxima.
 int do_flux(img_ctx* ctx, int order, bool fuse_cfl) {
     const img_config& c = ctx->cfg;
@@ -862,14 +926,23 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
 }
 
 // One iteration (imogen.m:60-66): time.update(1), flux(+1), time.update(2), flux(-1).
+// With radiation each timestep ends with source.m's sink (imogen.m:63-67), whose pass also collects
+// the CFL maxima that the next TimeManager.update reads (instead of the last fluid sweep).
 int enqueue_iteration(img_ctx* ctx) {
     int rc;
-    bool per_iter = ctx->cfg.update_mode != 0;
+    const bool per_iter = ctx->cfg.update_mode != 0;
+    const bool rad = ctx->cfg.radiation_type != IMG_RAD_NONE;
+    const bool fl = ctx->cfg.fluid_active != 0;
     if ((rc = time_update_async(ctx, 1)) != IMG_OK) return rc;
     if ((rc = do_flux(ctx, 1, false)) != IMG_OK) return rc;
+    if (rad) {
+        if ((rc = source_sink(ctx, !per_iter && fl)) != IMG_OK) return rc;
+        ctx->cfl_valid = !per_iter && fl;
+    }
     if ((rc = time_update_async(ctx, 2)) != IMG_OK) return rc;
-    if ((rc = do_flux(ctx, -1, per_iter)) != IMG_OK) return rc;
-    ctx->cfl_valid = per_iter && ctx->cfg.fluid_active;
+    if ((rc = do_flux(ctx, -1, per_iter && !rad)) != IMG_OK) return rc;
+    if (rad && (rc = source_sink(ctx, per_iter && fl)) != IMG_OK) return rc;
+    ctx->cfl_valid = per_iter && fl;
     return IMG_OK;
 }
 
@@ -893,6 +966,24 @@ int validate(const img_config& c, std::string& why) {
     if (c.precision != IMG_PREC_FP64 && c.precision != IMG_PREC_MIXED) { why = "unknown precision"; return IMG_ERR_ARG; }
     if ((long long)c.grid[0] * c.grid[1] * c.grid[2] >= (1LL << 31)) { why = "grids are limited to < 2^31 cells"; return IMG_ERR_ARG; }
     if (c.bc_infinity < 4) { why = "bcInfinity must be >= 4"; return IMG_ERR_ARG; }
+    if (c.viscosity_type < IMG_VISC_NONE || c.viscosity_type > IMG_VISC_CARAMANA_SHASHKOV_WHALEN) {
+        why = "unknown artificial viscosity type";
+        return IMG_ERR_ARG;
+    }
+    if (c.radiation_type < IMG_RAD_NONE || c.radiation_type > IMG_RAD_OPTICALLY_THIN) { why = "unknown radiation type"; return IMG_ERR_ARG; }
+    if (c.viscosity_type != IMG_VISC_NONE)   // the segment kernel's ends (seg_fluid.cuh)
+        for (int d = 0; d < 3; ++d) {
+            if (c.grid[d] < 3) continue;
+            for (int s = 0; s < 2; ++s) {
+                const int m = c.bc_modes[CLS_MASS][s][d];
+                bool ok = m == IMG_BC_CIRC || m == IMG_BC_CONST;
+                for (int k = 1; k < 4; ++k) ok = ok && c.bc_modes[k][s][d] == m;
+                if (!ok) {
+                    why = "artificial viscosity needs circ or const ends, the same for mass, momentum, energy and B";
+                    return IMG_ERR_UNSUPPORTED;
+                }
+            }
+        }
     int ndims = c.grid[2] > 1 ? 3 : 2;
     for (int k = 0; k < 4; ++k)
         for (int s = 0; s < 2; ++s)
@@ -992,6 +1083,7 @@ void img_config_default(img_config* c) {
     c->update_mode = 1;
     c->precision = IMG_PREC_FP64;
     c->nonfinite_check = 1;
+    c->rad_exponent = 0.5;   // Radiation.m:34
 }
 
 size_t img_bytes_required(const img_config* cfg) { return cfg ? plan(*cfg).total : 0; }
@@ -1028,6 +1120,17 @@ int img_create(img_ctx** out, const img_config* cfg) {
                 ctx->pcfg_mtile[kind - 1][d] = ctx->pcfg[kind][d];
                 if (tile_only) continue;
                 ctx->pcfg[kind][d] = choose_window(g, d, ctx->pcfg_mtile[kind - 1][d]);
+            }
+            if (kind == 0 && cfg->viscosity_type != IMG_VISC_NONE && g.n[d] >= 3) {
+                bool ok = false;
+                ctx->pcfg[0][d] = choose_fluid_visc(g, d, ctx->elem, ok);
+                if (!ok) {
+                    fail(ctx, IMG_ERR_UNSUPPORTED, "artificial viscosity: no one-block segment tiling for dimension %d "
+                         "(N = %d)", d + 1, g.n[d]);
+                    g_create_err = ctx->err;
+                    delete ctx;
+                    return IMG_ERR_UNSUPPORTED;
+                }
             }
             std::lock_guard<std::mutex> lock(g_tune_mu);
             auto it = g_tuned.find(tune_key(kind, g, d, ctx->elem, *cfg));
@@ -1095,6 +1198,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     t.cfl = cfg->cfl;
     for (int d = 0; d < 3; ++d) t.dgrid[d] = cfg->dgrid[d];
     t.update_mode = cfg->update_mode;
+    t.rad_minbits = 0xfff0000000000000ull;   // ordered bits of +inf (rad_init_kernel)
     *ctx->host_tm = t;
     if (cudaMemcpyAsync(ctx->fade_dev, ctx->fade_host.data(), sizeof(double) * ctx->fade_host.size(), cudaMemcpyHostToDevice,
                         ctx->stream) != cudaSuccess ||
@@ -1322,6 +1426,10 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
         if (!isZero) ctx->mhd = 1;
     }
     if ((rc = ctx->elem == 8 ? cellmag_init<double>(ctx) : cellmag_init<float>(ctx)) != IMG_OK) return rc;
+    // Radiation.initialize after the arrays exist (imogen.m:46 -> ImogenManager.initialize)
+    if (ctx->cfg.radiation_type != IMG_RAD_NONE &&
+        (rc = ctx->elem == 8 ? radiation_initialize<double>(ctx) : radiation_initialize<float>(ctx)) != IMG_OK)
+        return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->state_set = true;
     ctx->cfl_valid = false;
@@ -1351,6 +1459,22 @@ int img_flux(img_ctx* ctx, int order) {
     if (order != 1 && order != -1) return fail(ctx, IMG_ERR_ARG, "%d is not a recognized direction", order);
     ctx->cfl_valid = false;
     return do_flux(ctx, order, false);
+}
+
+int img_source(img_ctx* ctx) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (ctx->cfg.radiation_type == IMG_RAD_NONE) return IMG_OK;
+    ctx->cfl_valid = false;
+    return source_sink(ctx, false);
+}
+
+int img_radiation_strength(img_ctx* ctx, double* strength) {
+    if (!ctx || !strength) return fail(ctx, IMG_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *strength = ctx->host_tm->rad_strength;
+    return IMG_OK;
 }
 
 int img_fluid_sweep(img_ctx* ctx, int X) {
@@ -1849,6 +1973,8 @@ int img_batch_add(img_batch* b, img_ctx* ctx) {
     if (!ctx->state_set) return bfail(b, IMG_ERR_STATE, "member state not set");
     if (ctx->batch) return bfail(b, IMG_ERR_STATE, "context is already a batch member");
     if (ctx->dev != b->dev) return bfail(b, IMG_ERR_ARG, "member is on device %d, batch on %d", ctx->dev, b->dev);
+    if (ctx->cfg.viscosity_type != IMG_VISC_NONE || ctx->cfg.radiation_type != IMG_RAD_NONE)
+        return bfail(b, IMG_ERR_UNSUPPORTED, "contexts with artificial viscosity or radiation do not join batches");
     if (!b->members.empty() && !same_signature(b->members[0], ctx))
         return bfail(b, IMG_ERR_ARG, "member differs from the batch in precision, physics, swept dimensions, "
                      "time update mode or iteration");
@@ -2116,9 +2242,10 @@ int img_autotune(img_ctx* ctx, int trials) {
             if (ctx->g.n[d] < 3) continue;
             PencilCfg best = ctx->pcfg[kind][d];
             float best_ms = 1e30f;
-            std::vector<PencilCfg> cands = pencil_candidates(ctx->g, d, ctx->elem);
+            const bool visc = kind == 0 && ctx->cfg.viscosity_type != IMG_VISC_NONE;   // segment tilings only
+            std::vector<PencilCfg> cands = visc ? std::vector<PencilCfg>() : pencil_candidates(ctx->g, d, ctx->elem);
             if (kind == 0)
-                for (const PencilCfg& sc : seg_candidates(ctx->g, d, ctx->elem)) cands.push_back(sc);
+                for (const PencilCfg& sc : seg_candidates(ctx->g, d, ctx->elem, visc)) cands.push_back(sc);
             if (kind == 1) {   // (window tilings carry both components per thread: no nqc = 2 variant)   // the chain may also take both transverse components per CTA
                 const size_t n0 = cands.size();
                 for (size_t i = 0; i < n0; ++i)
@@ -2187,8 +2314,9 @@ int img_set_tiling(img_ctx* ctx, int dim, const int cfg[7]) {
     if (nqc != 1 && !(nqc == 2 && kind == 1 && cfg[4] <= 2))
         return fail(ctx, IMG_ERR_UNSUPPORTED, "two components per CTA: magnet sweeps with at most 2 cells per thread");
     if (cfg[6] && nqc != 1) return fail(ctx, IMG_ERR_UNSUPPORTED, "window tilings carry both components per thread");
-    std::vector<PencilCfg> cands = pencil_candidates(ctx->g, d, ctx->elem);
-    for (const PencilCfg& sc : kind == 0 ? seg_candidates(ctx->g, d, ctx->elem) : win_candidates(ctx->g, d))
+    const bool visc = kind == 0 && ctx->cfg.viscosity_type != IMG_VISC_NONE;   // segment tilings only
+    std::vector<PencilCfg> cands = visc ? std::vector<PencilCfg>() : pencil_candidates(ctx->g, d, ctx->elem);
+    for (const PencilCfg& sc : kind == 0 ? seg_candidates(ctx->g, d, ctx->elem, visc) : win_candidates(ctx->g, d))
         cands.push_back(sc);
     for (PencilCfg c : cands) {
         if (c.Wb != cfg[0] || c.G != cfg[1] || c.CL != cfg[2] || c.NT != cfg[3] || c.cpt != cfg[4] ||

@@ -14,6 +14,9 @@
 //            limiter (relaxingFluid.m:57-62) -- the limited values of the neighbour cells next to the
 //            segment are computed here as well, from the published cells -- and the update
 //            (relaxingFluid.m:64-71); store; fused CFL maxima on the last sweep of a step.
+// With artificial viscosity (fluid/ArtificialViscosity.m) stages 1 and 2 each publish the viscosity
+// exchange set with the pencil maximum, then compute the viscous pressure and F and publish (u, F)
+// behind one more barrier: four barriers instead of two.
 // Per cell the formulas are those of the pencil-tile kernels (fluid_sweep.cuh); the momentum and
 // cell-centred B are held in sweep-rotated order (the component along the sweep first), so sums over
 // components run in that order, and the compiler may contract differently into FMAs: the two kernel
@@ -33,11 +36,15 @@
 
 namespace img {
 
+// FP64 words per thread of the artificial-viscosity exchange set (seg_visc_publish).
+constexpr int VISC_ROWS = 9;
+
 // Words per thread of the two exchange sets and of the pencil maxima: (u, F) of 2 cells, (u*, F*) of
-// 4 cells, and 2 per-warp maxima slots of 32 columns.
+// 4 cells, and 2 per-warp maxima slots of 32 columns; with artificial viscosity the FP64 viscosity
+// exchange set after them.
 template <typename T>
-__host__ __device__ inline size_t seg_fluid_smem_bytes(int NT) {
-    return sizeof(T) * ((size_t)60 * NT + 2 * (size_t)(NT / 32) * 32);
+__host__ __device__ inline size_t seg_fluid_smem_bytes(int NT, bool visc = false) {
+    return sizeof(T) * ((size_t)60 * NT + 2 * (size_t)(NT / 32) * 32) + (visc ? sizeof(double) * VISC_ROWS * NT : 0);
 }
 
 // Placement of one thread in the segment layout.
@@ -137,6 +144,133 @@ __device__ __forceinline__ T press_speed_rot(double G, const T u[5], double msq,
     }
 }
 
+// The same, also returning the 'totsnd' sound speed (the Neumann-Richtmyer viscosity reads it).
+template <typename T>
+__device__ __forceinline__ T press_speed_rot(double G, const T u[5], double msq, T& p, T& cs) {
+    if constexpr (sizeof(T) == 4) {
+        PressOutF o = pressure_totsnd_mixed(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p;
+        cs = o.cs;
+        return fabsf(u[1] * rcp_approx(u[0])) + o.cs;
+    } else {
+        PressOut o = pressure_totsnd(G, u[0], u[1], u[2], u[3], u[4], msq);
+        p = o.p;
+        cs = o.cs;
+        return fabs(u[1] * (1.0 / u[0])) + o.cs;
+    }
+}
+
+// ---- artificial viscosity (fluid/ArtificialViscosity.m) in the segment layout ---------------------
+// Computed in FP64 for both forms, with explicit round-to-nearest products and sums (no FMA
+// contraction), in the reference's operation order.  The stage's state is the one wFluidFlux.m
+// receives: the primaries for the predictor, the half-step stores for the corrector; the viscous term
+// is added to the 'totsnd' pressure after the freezing speed is taken (wFluidFlux.m:18-24).
+
+// cswSoundSpeed's per-cell sound speed (ArtificialViscosity.m:157-190) from the natural-order
+// momentum and cell-centred B of one cell.  As the reference writes it, only the z momentum of the
+// velocity-squared sum is divided by rho^2, and every B component counts (no isZero test).
+__device__ __forceinline__ double csw_cell_sound(double G, double rho, double px, double py, double pz, double E,
+                                                 double bx, double by, double bz) {
+    const double vel_sq = __dadd_rn(__dadd_rn(__dmul_rn(px, px), __dmul_rn(py, py)), __dmul_rn(pz, pz) / __dmul_rn(rho, rho));
+    const double mag_sq = __dadd_rn(__dadd_rn(__dmul_rn(bx, bx), __dmul_rn(by, by)), __dmul_rn(bz, bz));
+    double s = __dmul_rn(G - 1.0, __dsub_rn(E, __dmul_rn(__dmul_rn(0.5, rho), vel_sq)));
+    s = __dsub_rn(s, __dmul_rn(__dmul_rn(G - 1.0, 0.5), mag_sq));
+    return sqrt(fabs(__dadd_rn(__dmul_rn(G, s), __dmul_rn(2.0, mag_sq)) / rho));
+}
+
+// Per-cell viscosity inputs of one stage and their exchange set V ([VISC_ROWS][NT] FP64): v = p_X/rho
+// of cells 0, 1, C-2, C-1 (rows 0-3), rho of cells 0 and C-1 (rows 4-5), the CSW cell sound speed of
+// cells 0 and C-1 (rows 6-7) and p_X of cell 0 (row 8).  w holds the stage state in sweep-rotated order;
+// (nx, ny, nz) give the rotated slot (0-2) of the natural components.
+template <typename T, int C, int VT>
+__device__ __forceinline__ void seg_visc_publish(const T (&w)[5][C], const T (&bb)[3][C], double G, int nx, int ny, int nz,
+                                                 double* V, int NT, int t, double (&vel)[C], double (&snd)[C]) {
+    static_assert(C >= 2, "the viscosity stencil reaches 2 cells: at least 2 cells per thread");
+#pragma unroll
+    for (int k = 0; k < C; ++k) {
+        vel[k] = (double)w[1][k] / (double)w[0][k];
+        if constexpr (VT == VISC_CSW) {
+            const double p[3] = {(double)w[1][k], (double)w[2][k], (double)w[3][k]};
+            const double b[3] = {(double)bb[0][k], (double)bb[1][k], (double)bb[2][k]};
+            auto pick = [](const double (&a)[3], int s) { return s == 0 ? a[0] : (s == 1 ? a[1] : a[2]); };
+            snd[k] = csw_cell_sound(G, (double)w[0][k], pick(p, nx), pick(p, ny), pick(p, nz), (double)w[4][k],
+                                    pick(b, nx), pick(b, ny), pick(b, nz));
+        } else {
+            snd[k] = 0.0;
+        }
+    }
+    if constexpr (VT == VISC_CSW) {
+        V[0 * NT + t] = vel[0];
+        V[1 * NT + t] = vel[1];
+        V[2 * NT + t] = vel[C - 2];
+        V[3 * NT + t] = vel[C - 1];
+        V[4 * NT + t] = (double)w[0][0];
+        V[5 * NT + t] = (double)w[0][C - 1];
+        V[6 * NT + t] = snd[0];
+        V[7 * NT + t] = snd[C - 1];
+    } else {
+        V[8 * NT + t] = (double)w[1][0];
+    }
+}
+
+// The viscous pressure q of the C own cells (after the barrier that follows seg_visc_publish).  lt/rt:
+// the threads of the neighbour segments; lo_own/hi_own: a const pencil end (its ghosts are the end
+// cell, constant_shift.m); cs: the 'totsnd' sound speed of each cell (Neumann-Richtmyer).
+template <typename T, int C, int VT>
+__device__ __forceinline__ void seg_visc_terms(const FluidArgs& a, double G, const T (&w)[5][C], const T (&cs)[C],
+                                               const double (&vel)[C], const double (&snd)[C], const double* V, int NT,
+                                               int lt, int rt, bool lo_own, bool hi_own, double (&q)[C]) {
+    if constexpr (VT == VISC_NR) {
+        // viscousMagnitude = min(p_X.shift(X, 1) - p_X, 0); q = vm (c1 c_s + c2 vm / rho)
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const double pn = k + 1 < C ? (double)w[1][k + 1] : (hi_own ? (double)w[1][C - 1] : V[8 * NT + rt]);
+            const double vm = fmin(__dsub_rn(pn, (double)w[1][k]), 0.0);
+            q[k] = __dmul_rn(vm, __dadd_rn(__dmul_rn(a.vc1, (double)cs[k]), __dmul_rn(a.vc2, vm) / (double)w[0][k]));
+        }
+    } else {
+        double vv[C + 4], rr[C + 2], ss[C + 2];   // cells -2 .. C+1 and -1 .. C
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            vv[k + 2] = vel[k];
+            rr[k + 1] = (double)w[0][k];
+            ss[k + 1] = snd[k];
+        }
+        vv[1] = lo_own ? vel[0] : V[3 * NT + lt];
+        vv[0] = lo_own ? vel[0] : V[2 * NT + lt];
+        rr[0] = lo_own ? rr[1] : V[5 * NT + lt];
+        ss[0] = lo_own ? ss[1] : V[7 * NT + lt];
+        vv[C + 2] = hi_own ? vel[C - 1] : V[0 * NT + rt];
+        vv[C + 3] = hi_own ? vel[C - 1] : V[1 * NT + rt];
+        rr[C + 1] = hi_own ? rr[C] : V[4 * NT + rt];
+        ss[C + 1] = hi_own ? ss[C] : V[6 * NT + rt];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const double mb = rr[k], mc = rr[k + 2];
+            const double rho = __dmul_rn(__dmul_rn(2.0, mc), mb) / __dadd_rn(mc, mb);   // averaged density
+            const double c = fmax(fmin(ss[k], ss[k + 2]), 0.0);                           // cswSoundSpeed
+            const double v0 = vv[k], v1 = vv[k + 1], v2 = vv[k + 3], v3 = vv[k + 4];
+            const double dv = __dsub_rn(v2, v1);
+            const double rl = __dsub_rn(v3, v2) / __dmul_rn(2.0, dv);
+            const double rr_ = __dsub_rn(v1, v0) / __dmul_rn(2.0, dv);
+            const double lim = fmax(0.0, fmin(fmin(__dmul_rn(0.5, __dadd_rn(rl, rr_)),
+                                                   fmin(__dmul_rn(2.0, rl), __dmul_rn(2.0, rr_))), 1.0));
+            const double adv = fabs(dv);
+            const double root = sqrt(__dadd_rn(__dmul_rn(a.vk2, __dmul_rn(dv, dv)), __dmul_rn(a.vc1sq, __dmul_rn(c, c))));
+            const double mag = __dadd_rn(__dmul_rn(a.vk1, adv) / 4.0, root);
+            q[k] = __dmul_rn(__dmul_rn(__dmul_rn(__dmul_rn(dv < 0.0 ? 1.0 : 0.0, rho), mag), __dsub_rn(1.0, lim)), adv);
+        }
+    }
+}
+
+// press + viscosity.solve: in FP64 the reference's sum; in the mixed form the FP32 pressure plus the
+// rounded viscous term.
+template <typename T>
+__device__ __forceinline__ T visc_add(T p, double q) {
+    if constexpr (sizeof(T) == 4) return p + (float)q;
+    else return __dadd_rn(p, q);
+}
+
 // Corrector (relaxingFluid.m:52-71) of one variable over a segment: R* = (u* + F*/c_f*)/2 and
 // L* = (u* - F*/c_f*)/2 at cells -2 .. C+1 (neighbour cells from the published exchange set X2), the
 // TVD limiter at cells -1 .. C (only those the update reads), and the update of the C own cells.
@@ -224,7 +358,10 @@ __device__ __forceinline__ T seg_max_collect(const SweepGeom& g, int b, T wv, co
     return m;
 }
 
-template <typename T, bool MHD, int C>
+// VT: the artificial viscosity (VISC_*), fixed per kernel.  With viscosity each of the first two
+// stages takes one more barrier: the viscosity exchange set is published with the pencil maximum, and
+// the flux numerators (which include the viscous pressure) are published after it.
+template <typename T, bool MHD, int C, int VT>
 __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
@@ -239,6 +376,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     T* X1 = reinterpret_cast<T*>(smem);   // [20][NT]: (u, F) of the first cell, then of the last
     T* X2 = X1 + 20 * NT;                 // [40][NT]: (u*, F*) of cells 0, 1, C-2, C-1
     T* PM = X2 + 40 * NT;                 // [2][NT/32][32]: per-warp pencil maxima
+    double* V = reinterpret_cast<double*>(PM + 2 * (NT >> 5) * 32);   // [VISC_ROWS][NT] (viscosity only)
     const bool circ_lo = a.mode[CLS_MASS][0] == BC_CIRC, circ_hi = a.mode[CLS_MASS][1] == BC_CIRC;
     const int ls = d == 0 ? 1 : g.Wb;     // thread distance between consecutive segments of a pencil
     const bool lo_own = s == 0 && !circ_lo, hi_own = s == S - 1 && !circ_hi;
@@ -253,6 +391,9 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     // momentum and cell-centred B in sweep-rotated order: component 0 along the sweep, then d1, d2
     void* qv[5] = {a.q[Q_RHO], a.q[Q_PX + d], a.q[Q_PX + d1], a.q[Q_PX + d2], a.q[Q_E]};
     const bool ub[3] = {a.use_b[d] != 0, a.use_b[d1] != 0, a.use_b[d2] != 0};
+    // rotated slots of the natural x, y, z components (the CSW sound speed sums in natural order)
+    const int nx = d == 0 ? 0 : (d1 == 0 ? 1 : 2), ny = d == 1 ? 0 : (d1 == 1 ? 1 : 2), nz = d == 2 ? 0 : (d1 == 2 ? 1 : 2);
+    constexpr bool LOADB = MHD || VT == VISC_CSW;   // cswSoundSpeed reads every cell-centred component
 
     // ---- stage 1: load, pressure, speed, F -------------------------------------------------------
     T u[5][C], bb[3][C], F[5][C];
@@ -260,7 +401,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     if (sp.colok) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) seg_load<T, C>(qv[v], o0, g.sd, vec, u[v]);
-        if (MHD) {
+        if (LOADB) {
             seg_load<T, C>(a.q[Q_CBX + d], o0, g.sd, vec, bb[0]);
             seg_load<T, C>(a.q[Q_CBX + d1], o0, g.sd, vec, bb[1]);
             seg_load<T, C>(a.q[Q_CBX + d2], o0, g.sd, vec, bb[2]);
@@ -277,33 +418,72 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         }
     }
     T lmax = T(0);
+    T cf;
+    if constexpr (VT == VISC_NONE) {
 #pragma unroll
-    for (int k = 0; k < C; ++k) {
-        double m = 0.0;
+        for (int k = 0; k < C; ++k) {
+            double m = 0.0;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
-        msq[k] = m;
-        const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
-        const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
-        T p;
-        const T spd = press_speed_rot<T>(G, uu, m, p);
-        if (sp.colok) lmax = fmax(lmax, spd);
-        T Fk[5];
-        flux_num_rot<T>(uu, b3, p, Fk);
+            for (int c = 0; c < 3; ++c)
+                if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+            msq[k] = m;
+            const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+            const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+            T p;
+            const T spd = press_speed_rot<T>(G, uu, m, p);
+            if (sp.colok) lmax = fmax(lmax, spd);
+            T Fk[5];
+            flux_num_rot<T>(uu, b3, p, Fk);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) F[v][k] = Fk[v];
+            for (int v = 0; v < 5; ++v) F[v][k] = Fk[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            X1[v * NT + t] = u[v][0];
+            X1[(5 + v) * NT + t] = F[v][0];
+            X1[(10 + v) * NT + t] = u[v][C - 1];
+            X1[(15 + v) * NT + t] = F[v][C - 1];
+        }
+        const T wv1 = seg_max_publish(g, lmax, PM);
+        __syncthreads();
+        cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22)
+    } else {
+        T P[C], CS[C];
+        double vel[C], snd[C], q[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            double m = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
+            msq[k] = m;
+            const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+            const T spd = press_speed_rot<T>(G, uu, m, P[k], CS[k]);
+            if (sp.colok) lmax = fmax(lmax, spd);
+        }
+        seg_visc_publish<T, C, VT>(u, bb, G, nx, ny, nz, V, NT, t, vel, snd);
+        const T wv1 = seg_max_publish(g, lmax, PM);
+        __syncthreads();
+        cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22), before the viscosity
+        seg_visc_terms<T, C, VT>(a, G, u, CS, vel, snd, V, NT, lt, rt, lo_own, hi_own, q);
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
+            const T b3[3] = {MHD ? bb[0][k] : T(0), MHD ? bb[1][k] : T(0), MHD ? bb[2][k] : T(0)};
+            T Fk[5];
+            flux_num_rot<T>(uu, b3, visc_add<T>(P[k], q[k]), Fk);   // press + viscosity.solve (wFluidFlux.m:24)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) F[v][k] = Fk[v];
+        }
+#pragma unroll
+        for (int v = 0; v < 5; ++v) {
+            X1[v * NT + t] = u[v][0];
+            X1[(5 + v) * NT + t] = F[v][0];
+            X1[(10 + v) * NT + t] = u[v][C - 1];
+            X1[(15 + v) * NT + t] = F[v][C - 1];
+        }
+        __syncthreads();
     }
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-        X1[v * NT + t] = u[v][0];
-        X1[(5 + v) * NT + t] = F[v][0];
-        X1[(10 + v) * NT + t] = u[v][C - 1];
-        X1[(15 + v) * NT + t] = F[v][C - 1];
-    }
-    const T wv1 = seg_max_publish(g, lmax, PM);
-    __syncthreads();
-    const T cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22)
     T ic;
     if constexpr (sizeof(T) == 4) ic = __frcp_rn(cf);
     else ic = T(1) / cf;
@@ -327,19 +507,43 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         for (int k = 0; k < C; ++k) us[v][k] = u[v][k] - hfc * (R[k + 1] - R[k] + L[k] - L[k + 1]);
     }
     T lmax2 = T(0);
+    T P2[C], CS2[C];
 #pragma unroll
     for (int k = 0; k < C; ++k) {
         us[0][k] = us[0][k] > (T)a.minmass ? us[0][k] : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
         if (!sp.colok) { us[0][k] = T(1); us[1][k] = us[2][k] = us[3][k] = us[4][k] = T(0); }
         const T uu[5] = {us[0][k], us[1][k], us[2][k], us[3][k], us[4][k]};
-        const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
-        T p2;
-        const T spd = press_speed_rot<T>(G, uu, msq[k], p2);   // relaxingFluid.m:47-50
-        if (sp.colok) lmax2 = fmax(lmax2, spd);
-        T Fk[5];
-        flux_num_rot<T>(uu, b3, p2, Fk);
+        if constexpr (VT == VISC_NONE) {
+            const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
+            T p2;
+            const T spd = press_speed_rot<T>(G, uu, msq[k], p2);   // relaxingFluid.m:47-50
+            if (sp.colok) lmax2 = fmax(lmax2, spd);
+            T Fk[5];
+            flux_num_rot<T>(uu, b3, p2, Fk);
 #pragma unroll
-        for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
+            for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
+        } else {
+            const T spd = press_speed_rot<T>(G, uu, msq[k], P2[k], CS2[k]);
+            if (sp.colok) lmax2 = fmax(lmax2, spd);
+        }
+    }
+    if constexpr (VT != VISC_NONE) {
+        // the viscosity of the half-step state: one more barrier before its fluxes are published
+        double vel[C], snd[C], q[C];
+        seg_visc_publish<T, C, VT>(us, bb, G, nx, ny, nz, V, NT, t, vel, snd);
+        const T wv2 = seg_max_publish(g, lmax2, PM + (NT >> 5) * 32);
+        __syncthreads();
+        lmax2 = seg_max_collect(g, sp.b, wv2, PM + (NT >> 5) * 32);
+        seg_visc_terms<T, C, VT>(a, G, us, CS2, vel, snd, V, NT, lt, rt, lo_own, hi_own, q);
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const T uu[5] = {us[0][k], us[1][k], us[2][k], us[3][k], us[4][k]};
+            const T b3[3] = {MHD ? bb[0][k] : T(0), MHD ? bb[1][k] : T(0), MHD ? bb[2][k] : T(0)};
+            T Fk[5];
+            flux_num_rot<T>(uu, b3, visc_add<T>(P2[k], q[k]), Fk);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
+        }
     }
     const int c1 = C > 1 ? 1 : 0;
 #pragma unroll
@@ -353,9 +557,15 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         X2[(30 + v) * NT + t] = us[v][C - 1];
         X2[(35 + v) * NT + t] = Fs[v][C - 1];
     }
-    const T wv2 = seg_max_publish(g, lmax2, PM + (NT >> 5) * 32);
-    __syncthreads();
-    const T cfs = seg_max_collect(g, sp.b, wv2, PM + (NT >> 5) * 32);   // freezing speed of the half step
+    T cfs;   // freezing speed of the half step
+    if constexpr (VT == VISC_NONE) {
+        const T wv2 = seg_max_publish(g, lmax2, PM + (NT >> 5) * 32);
+        __syncthreads();
+        cfs = seg_max_collect(g, sp.b, wv2, PM + (NT >> 5) * 32);
+    } else {
+        __syncthreads();
+        cfs = lmax2;
+    }
     T ics;
     if constexpr (sizeof(T) == 4) ics = __frcp_rn(cfs);
     else ics = T(1) / cfs;
@@ -409,9 +619,9 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     }
 }
 
-template <typename T, bool MHD, int C>
+template <typename T, bool MHD, int C, int VT = VISC_NONE>
 __global__ void __launch_bounds__(512, 1) fluid_seg_kernel(const __grid_constant__ FluidArgs a) {
-    fluid_seg_body<T, MHD, C>(a, blockIdx.x);
+    fluid_seg_body<T, MHD, C, VT>(a, blockIdx.x);
 }
 
 template <typename T, bool MHD, int C>
@@ -421,7 +631,7 @@ __global__ void __launch_bounds__(512, 1) fluid_seg_batch_kernel(const FluidArgs
     const BlockMap bm = map[blockIdx.x];
     load_member_args(sa, args + bm.member);
     __syncthreads();
-    fluid_seg_body<T, MHD, C>(sa, (unsigned)bm.block);
+    fluid_seg_body<T, MHD, C, VISC_NONE>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

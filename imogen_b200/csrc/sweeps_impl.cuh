@@ -169,8 +169,16 @@ void (*fluid_seg_batch_kernel_c(int C))(const FluidArgs*, const BlockMap*) {
     return C == 2 ? fluid_seg_batch_kernel<T, MHD, 2> : fluid_seg_batch_kernel<T, MHD, 4>;
 }
 
+// With artificial viscosity: 2 and 4 cells per thread.
+template <typename T, bool MHD, int VT>
+void (*fluid_seg_visc_kernel_c(int C))(const FluidArgs) {
+    return C == 2 ? fluid_seg_kernel<T, MHD, 2, VT> : fluid_seg_kernel<T, MHD, 4, VT>;
+}
+
 template <typename T>
-void (*fluid_seg_kernel_p(int C, bool mhd))(const FluidArgs) {
+void (*fluid_seg_kernel_p(int C, bool mhd, int visc = VISC_NONE))(const FluidArgs) {
+    if (visc == VISC_NR) return mhd ? fluid_seg_visc_kernel_c<T, true, VISC_NR>(C) : fluid_seg_visc_kernel_c<T, false, VISC_NR>(C);
+    if (visc == VISC_CSW) return mhd ? fluid_seg_visc_kernel_c<T, true, VISC_CSW>(C) : fluid_seg_visc_kernel_c<T, false, VISC_CSW>(C);
     return mhd ? fluid_seg_kernel_c<T, true>(C) : fluid_seg_kernel_c<T, false>(C);
 }
 
@@ -256,7 +264,7 @@ cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, co
 
 template <typename T>
 cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd) {
-    if (L.seg) return launch_pencil(fluid_seg_kernel_p<T>(L.seg, mhd), a, L);
+    if (L.seg) return launch_pencil(fluid_seg_kernel_p<T>(L.seg, mhd, a.visc), a, L);
     return launch_pencil(fluid_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
 
@@ -300,6 +308,8 @@ cudaError_t fluid_seg_attributes(int optin) {
         for (int mhd = 0; mhd < 2; ++mhd) {
             cudaError_t e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0), optin);
             if (e == cudaSuccess) e = allow_max_smem(fluid_seg_batch_kernel_p<T>(C, mhd != 0), optin);
+            for (int vt : {VISC_NR, VISC_CSW})
+                if (e == cudaSuccess && C <= 4) e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0, vt), optin);
             if (e != cudaSuccess) return e;
         }
     }

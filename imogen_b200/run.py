@@ -20,6 +20,9 @@ BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall")      # enums/ENU
 LIMITERS = {"vanleer": 0, "superbee": 1, "minmond": 2, "minmod": 2}   # FluxLimiterEnum.m:10-13
 BC_CLASSES = ("mass", "mom", "ener", "mag")
 PRECISIONS = {"fp64": 0, "mixed": 1}
+# ENUM.ARTIFICIAL_VISCOSITY_* and ENUM.RADIATION_* (enums/ENUM.m)
+VISCOSITIES = {"empty": 0, "none": 0, "neumann_richtmyer": 1, "caramana_shashkov_whalen": 2}
+RADIATIONS = {"empty": 0, "none": 0, "optically_thin": 1}
 VAR = dict(mass=0, momx=1, momy=2, momz=3, ener=4, magx=5, magy=6, magz=7, cmagx=8, cmagy=9, cmagz=10)
 
 
@@ -60,8 +63,10 @@ def bc_table(bc):
 
 def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ", bc_infinity=20,
                 limiter="vanleer", fluid=True, magnet=False, time_max=1e5, iter_max=10,
-                update_mode=1, precision="fp64", nonfinite_check=True):
-    """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults)."""
+                update_mode=1, precision="fp64", nonfinite_check=True, viscosity="empty", visc_linear=0.0,
+                visc_quadratic=0.0, radiation="empty", rad_exponent=0.5, rad_initial_maximum=0.0):
+    """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults; run.viscosity
+    and run.radiation as fluid/ArtificialViscosity.m:31-37 and fluid/Radiation.m:32-37 hold them)."""
     c = ImgConfig()
     lib().img_config_default(ctypes.byref(c))
     grid = tuple(int(g) for g in grid) + (1,) * (3 - len(grid))
@@ -91,6 +96,12 @@ def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ"
     c.update_mode = int(update_mode)
     c.precision = PRECISIONS[precision] if isinstance(precision, str) else int(precision)
     c.nonfinite_check = int(bool(nonfinite_check))
+    c.viscosity_type = VISCOSITIES[viscosity] if isinstance(viscosity, str) else int(viscosity)
+    c.visc_linear = float(visc_linear)
+    c.visc_quadratic = float(visc_quadratic)
+    c.radiation_type = RADIATIONS[radiation] if isinstance(radiation, str) else int(radiation)
+    c.rad_exponent = float(rad_exponent)
+    c.rad_initial_maximum = float(rad_initial_maximum)
     return c
 
 
@@ -238,6 +249,17 @@ class ImogenRun:
 
     def relaxing_fluid(self, X):
         check(lib().img_fluid_sweep(self._h, int(X)), self._h)
+
+    def source(self):
+        """source.m for this path: the radiation sink E -= dTime * radiation.solve (source.m:30)."""
+        check(lib().img_source(self._h), self._h)
+
+    @property
+    def radiation_strength(self):
+        """Radiation.strength as Radiation.initialize set it from the state (0 without radiation)."""
+        v = ctypes.c_double()
+        check(lib().img_radiation_strength(self._h, ctypes.byref(v)), self._h)
+        return v.value
 
     def magnet_flux(self, X, mag_indices):
         check(lib().img_magnet_sweep(self._h, int(X), int(mag_indices[0]), int(mag_indices[1])), self._h)
@@ -402,6 +424,11 @@ class ImogenBatch:
 def flux(run, mass, mom, ener, mag, grav, order):
     """flux(run, mass, mom, ener, mag, grav, order) -- flux/flux.m:1."""
     run.flux(order)
+
+
+def source(run, mass, mom, ener, mag, grav):
+    """source(run, mass, mom, ener, mag, grav) -- source.m:1 (radiation sink; no gravity)."""
+    run.source()
 
 
 def relaxingFluid(run, mass, mom, ener, mag, grav, X):

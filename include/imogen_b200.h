@@ -35,6 +35,9 @@ enum { IMG_BC_CIRC = 0, IMG_BC_CONST = 1, IMG_BC_FADE = 2, IMG_BC_MIRROR = 3, IM
 enum { IMG_LIM_VANLEER = 0, IMG_LIM_SUPERBEE = 1, IMG_LIM_MINMOD = 2 };
 enum { IMG_CLS_MASS = 0, IMG_CLS_MOM = 1, IMG_CLS_ENER = 2, IMG_CLS_MAG = 3 };
 enum { IMG_PREC_FP64 = 0, IMG_PREC_MIXED = 1 };
+/* ArtificialViscosity.type (fluid/ArtificialViscosity.m:45-56) and Radiation.type (fluid/Radiation.m:43-55) */
+enum { IMG_VISC_NONE = 0, IMG_VISC_NEUMANN_RICHTMYER = 1, IMG_VISC_CARAMANA_SHASHKOV_WHALEN = 2 };
+enum { IMG_RAD_NONE = 0, IMG_RAD_OPTICALLY_THIN = 1 };
 /* variable ids for upload/download: rho, momentum x/y/z, energy, face-centred B x/y/z, and the
  * cell-centred B x/y/z (MagnetArray.cellMag, download only) */
 enum {
@@ -65,13 +68,28 @@ typedef struct img_config {
                                  (its max ignores NaN, TimeManager.m:70-76; MINMASS replaces a NaN
                                  density, relaxingFluid.m:39,71) and the run goes on.  No reference
                                  counterpart. */
+    /* run.viscosity (fluid/ArtificialViscosity.m:31-37): type, linear and quadratic strengths.  A
+     * viscosity other than IMG_VISC_NONE needs circ or const ends on every dimension (the same mode
+     * for mass, momentum, energy and B on each side) and pencils that fit one thread block (along x
+     * N / C threads with C = 2 or 4 cells per thread a power of two up to 32 or a multiple of 32;
+     * N / C <= 512 along every dimension); img_create returns IMG_ERR_UNSUPPORTED otherwise, and
+     * such contexts do not join batches. */
+    int viscosity_type;
+    double visc_linear;
+    double visc_quadratic;
+    /* run.radiation (fluid/Radiation.m:32-37): type, exponent and initialMaximum (percent); the
+     * strength is set from the state by img_set_state (Radiation.initialize).  Contexts with
+     * radiation do not join batches. */
+    int radiation_type;
+    double rad_exponent;
+    double rad_initial_maximum;
 } img_config;
 
 typedef struct img_ctx img_ctx;
 
 /* Default config: Initializer.m defaults (gamma 5/3, cfl 0.7, minMass 1e-5, circ BCs,
- * bcInfinity 20, vanleer, fluid on, magnet off, timeMax 1e5, iterMax 10, per-iteration dt), plus
- * nonfinite_check = 1. */
+ * bcInfinity 20, vanleer, fluid on, magnet off, timeMax 1e5, iterMax 10, per-iteration dt, no
+ * viscosity (strengths 0), no radiation (exponent 0.5, initialMaximum 0)), plus nonfinite_check = 1. */
 void img_config_default(img_config* cfg);
 
 /* Create a context for one grid on the current CUDA device.  Replaces initialize.m:18-410 for
@@ -107,13 +125,20 @@ int img_flux(img_ctx* ctx, int order);
  * R2009a-R2010b's perms.  Host only; no device work. */
 int img_sweep_order(int order, int iteration, int out[3]);
 
+/* source(run, mass, mom, ener, mag, grav) (source.m:1-36) for this path: the radiation sink
+ * E = E - dTime * radiation.solve (source.m:30), nothing without radiation.  Gravity is out of scope. */
+int img_source(img_ctx* ctx);
+
+/* Radiation.strength (fluid/Radiation.m:71-72; 0 without radiation), synchronises. */
+int img_radiation_strength(img_ctx* ctx, double* strength);
+
 /* relaxingFluid(run, mass, mom, ener, mag, grav, X) (fluid/relaxingFluid.m:1) -- one sweep. */
 int img_fluid_sweep(img_ctx* ctx, int X);
 
 /* magnetFlux(run, mass, mom, mag, X, magneticIndices) (magnet/magnetFlux.m:1) -- one sweep. */
 int img_magnet_sweep(img_ctx* ctx, int X, int I1, int I2);
 
-/* One pass of the imogen.m:58-72 loop body: two timesteps (CFL, flux +1, flux -1), iteration+1.
+/* One pass of the imogen.m:58-72 loop body: two timesteps (CFL, flux, source), iteration+1.
  * Asynchronous: returns after enqueueing. */
 int img_step(img_ctx* ctx);
 

@@ -10,7 +10,8 @@ import subprocess
 
 import numpy as np
 
-from .np_oracle import (BC_MODES, MINMOD, PER_ITERATION, SUPERBEE, VANLEER, CIRC)
+from .np_oracle import (BC_MODES, MINMOD, PER_ITERATION, SUPERBEE, VANLEER, CIRC, VISC_NONE, VISC_NR, VISC_CSW,
+                        RAD_NONE, RAD_THIN)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -45,12 +46,17 @@ def lib():
             getattr(L, name).restype = ctypes.c_int
         L.orc_magnet_flux.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_iterate.argtypes = [ctypes.c_void_p]
+        L.orc_source.argtypes = [ctypes.c_void_p]
+        L.orc_radiation_strength.argtypes = [ctypes.c_void_p]
+        L.orc_radiation_strength.restype = ctypes.c_double
         L.orc_get_time.argtypes = [ctypes.c_void_p, dp, dp, ip]
         L.orc_set_time.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.orc_get_cfl.argtypes = [ctypes.c_void_p, dp, ip]
         L.orc_pchip.argtypes = [dp, ctypes.c_int, dp, ctypes.c_int, dp, ctypes.c_int, dp]
         L.orc_set_threads.argtypes = [ctypes.c_int]
         L.orc_sweep_order.argtypes = [ctypes.c_int, ctypes.c_int, ip]
+        L.orc_set_physics.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double]
         L.orc_max_threads.restype = ctypes.c_int
         _LIB = L
     return _LIB
@@ -106,7 +112,9 @@ class Sim:
 
     def __init__(self, grid, dgrid, gamma=5 / 3, cfl=0.7, minmass=1e-5, bc=None,
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
-                 magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION):
+                 magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
+                 viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0):
         self.grid = tuple(int(g) for g in grid)
         g = np.array(self.grid, dtype=np.int32)
         dg = np.array(dgrid, dtype=float)
@@ -117,6 +125,9 @@ class Sim:
                                    int(iter_max), int(update_mode))
         if not self._h:
             raise ValueError("BC settings not defined for this grid (see np_oracle.validate_bc)")
+        lib().orc_set_physics(self._h, {VISC_NONE: 0, VISC_NR: 1, VISC_CSW: 2}[viscosity], float(visc_linear),
+                              float(visc_quadratic), {RAD_NONE: 0, RAD_THIN: 1}[radiation], float(rad_exponent),
+                              float(rad_initial_maximum))
         self.TIMEMAX = float(time_max)
         self.ITERMAX = int(iter_max)
 
@@ -156,6 +167,14 @@ class Sim:
 
     def magnet_flux(self, X, mag_indices):
         lib().orc_magnet_flux(self._h, int(X), int(mag_indices[0]), int(mag_indices[1]))
+
+    def source(self):
+        """source.m:30: the radiation sink with the current dTime."""
+        lib().orc_source(self._h)
+
+    @property
+    def rad_strength(self):
+        return lib().orc_radiation_strength(self._h)
 
     def iterate(self):
         if lib().orc_iterate(self._h) != 0:

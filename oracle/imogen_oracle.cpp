@@ -124,6 +124,12 @@ struct Sim {
     int iteration = 1;
     double last_cmax = 0;
     int last_grid_index = 0;
+    // ArtificialViscosity (0 empty, 1 neumann_richtmyer, 2 caramana_shashkov_whalen) and Radiation
+    // (0 empty, 1 optically_thin) settings (ArtificialViscosity.m:31-57, Radiation.m:32-57)
+    int visc_type = 0;
+    double visc_lin = 0, visc_quad = 0;
+    int rad_type = 0;
+    double rad_exp = 0.5, rad_initmax = 0, rad_strength = 1;
 
     struct FluidVar { IArr prim, store, store_fluxR, store_fluxL, fluxR, fluxL; };
     struct MagComp {
@@ -352,10 +358,125 @@ void pressure(Sim& s, bool sound_mode, const Vec& rho, const Vec& px, const Vec&
     }
 }
 
-// wFluidFlux.m:14-44
-void w_fluid_flux(Sim& s, const Vec* u[5], int X, Vec& freeze, Vec w[5]) {
+// pressure('gas') (pressure.m:23-64): (G-1)(E - rho v^2/2) - (G-1) B^2/2, clamped at 0.
+Vec gas_pressure(const Sim& s) {
+    const double G = s.gamma;
+    long long N = s.N;
+    Vec out(N);
+    const Vec &rho = s.fv[0].prim.a, &px = s.fv[1].prim.a, &py = s.fv[2].prim.a, &pz = s.fv[3].prim.a,
+              &E = s.fv[4].prim.a;
+    const Vec* cm[3] = {&s.mg[0].cellMag.a, &s.mg[1].cellMag.a, &s.mg[2].cellMag.a};
+    bool use[3] = {!s.mg[0].isZero, !s.mg[1].isZero, !s.mg[2].isZero};
+    for (long long i = 0; i < N; ++i) {
+        double vsq = (px[i] * px[i] + py[i] * py[i] + pz[i] * pz[i]) / (rho[i] * rho[i]);
+        double msq = 0.0;
+        for (int c = 0; c < 3; ++c)
+            if (use[c]) msq = msq + (*cm[c])[i] * (*cm[c])[i];
+        double r = (G - 1.0) * (E[i] - 0.5 * rho[i] * vsq);
+        r = r - (G - 1.0) * 0.5 * msq;
+        out[i] = r < 0 ? 0.0 : r;
+    }
+    return out;
+}
+
+// x^e as NumPy's power computes it (its fast path takes the square root for e = 0.5).
+inline double npow(double x, double e) { return e == 0.5 ? std::sqrt(x) : std::pow(x, e); }
+
+// Radiation.solve: opticallyThinSolver (Radiation.m:86-88): strength * rho^(2-exponent) * Pgas^exponent.
+Vec radiation_solve(const Sim& s) {
+    Vec gas = gas_pressure(s);
+    const Vec& rho = s.fv[0].prim.a;
+    Vec out(s.N);
+    for (long long i = 0; i < s.N; ++i) out[i] = s.rad_strength * npow(rho[i], 2 - s.rad_exp) * npow(gas[i], s.rad_exp);
+    return out;
+}
+
+// Radiation.initialize (Radiation.m:61-75): strength from the initial state (face-centred B).
+void radiation_initialize(Sim& s) {
+    if (s.rad_type != 1) {
+        s.rad_strength = 0;
+        return;
+    }
+    s.rad_strength = 1;
+    Vec un = radiation_solve(s);
+    const Vec &rho = s.fv[0].prim.a, &E = s.fv[4].prim.a;
+    const Vec *p[3] = {&s.fv[1].prim.a, &s.fv[2].prim.a, &s.fv[3].prim.a};
+    const Vec *b[3] = {&s.mg[0].prim.a, &s.mg[1].prim.a, &s.mg[2].prim.a};
+    double mn = std::numeric_limits<double>::quiet_NaN();
+    for (long long i = 0; i < s.N; ++i) {
+        double ke = 0.5 * ((*p[0])[i] * (*p[0])[i] + (*p[1])[i] * (*p[1])[i] + (*p[2])[i] * (*p[2])[i]) / rho[i];
+        double me = 0.5 * ((*b[0])[i] * (*b[0])[i] + (*b[1])[i] * (*b[1])[i] + (*b[2])[i] * (*b[2])[i]);
+        double r = (E[i] - ke - me) / un[i];
+        if (!std::isnan(r) && (std::isnan(mn) || r < mn)) mn = r;   // minFinderND ignores NaN
+    }
+    s.rad_strength = (s.rad_initmax / 100) * mn;
+}
+
+// ArtificialViscosity.cswSoundSpeed (ArtificialViscosity.m:157-190): as in the reference, only the z
+// momentum of the velocity-squared sum is divided by rho^2.
+Vec csw_sound_speed(Sim& s, IArr* o[5], int X) {
+    const double G = s.gamma;
+    long long N = s.N;
+    Vec snd[2];
+    for (int q = 0; q < 2; ++q) {
+        int n = q == 0 ? 1 : -1;
+        Vec m0 = o[1]->shift(X, n), m1 = o[2]->shift(X, n), m2 = o[3]->shift(X, n), ms = o[0]->shift(X, n);
+        Vec b0 = s.mg[0].cellMag.shift(X, n), b1 = s.mg[1].cellMag.shift(X, n), b2 = s.mg[2].cellMag.shift(X, n);
+        Vec e = o[4]->shift(X, n), ms2 = o[0]->shift(X, n), ms3 = o[0]->shift(X, n);
+        Vec out(N);
+        for (long long i = 0; i < N; ++i) {
+            double vsq = m0[i] * m0[i] + m1[i] * m1[i] + m2[i] * m2[i] / (ms[i] * ms[i]);
+            double msq = b0[i] * b0[i] + b1[i] * b1[i] + b2[i] * b2[i];
+            double r = (G - 1.0) * (e[i] - 0.5 * ms2[i] * vsq);
+            r = r - (G - 1.0) * 0.5 * msq;
+            out[i] = std::sqrt(std::fabs((G * r + 2.0 * msq) / ms3[i]));
+        }
+        snd[q] = std::move(out);
+    }
+    Vec res(N);
+    for (long long i = 0; i < N; ++i) res[i] = std::fmax(std::fmin(snd[1][i], snd[0][i]), 0.0);
+    return res;
+}
+
+// ArtificialViscosity.solve (ArtificialViscosity.m:66-148) for the stage objects o (mass, mom x3, ener).
+Vec viscosity_solve(Sim& s, IArr* o[5], const Vec& sound, int X) {
+    long long N = s.N;
+    const double c1 = s.visc_lin, c2 = s.visc_quad, G = s.gamma;
+    Vec out(N, 0.0);
+    if (s.visc_type == 1) {   // neumannRichtmyerViscosity (:73-77)
+        Vec p1 = o[X]->shift(X, 1);
+        const Vec &px = o[X]->a, &rho = o[0]->a;
+        for (long long i = 0; i < N; ++i) {
+            double vm = std::fmin(p1[i] - px[i], 0.0);
+            out[i] = vm * (c1 * sound[i] + c2 * vm / rho[i]);
+        }
+    } else if (s.visc_type == 2) {   // caramanaShashkovWhalenViscosity (:81-148)
+        Vec mB = o[0]->shift(X, -1), mC = o[0]->shift(X, 1);
+        Vec cs = csw_sound_speed(s, o, X);
+        Vec pm2 = o[X]->shift(X, -2), rm2 = o[0]->shift(X, -2);
+        Vec pm1 = o[X]->shift(X, -1), rm1 = o[0]->shift(X, -1);
+        Vec pp1 = o[X]->shift(X, 1), rp1 = o[0]->shift(X, 1);
+        Vec pp2 = o[X]->shift(X, 2), rp2 = o[0]->shift(X, 2);
+        const double k1 = c2 * (G + 1), g4 = (G + 1) / 4, k2 = (c2 * c2) * (g4 * g4), k3 = c1 * c1;
+        for (long long i = 0; i < N; ++i) {
+            double rho = 2 * mC[i] * mB[i] / (mC[i] + mB[i]);
+            double v0 = pm2[i] / rm2[i], v1 = pm1[i] / rm1[i], v2 = pp1[i] / rp1[i], v3 = pp2[i] / rp2[i];
+            double dv = v2 - v1;
+            double rL = (v3 - v2) / (2 * dv), rR = (v1 - v0) / (2 * dv);
+            double lim = std::fmax(0.0, std::fmin(std::fmin(0.5 * (rL + rR), std::fmin(2 * rL, 2 * rR)), 1.0));
+            double adv = std::fabs(dv);
+            out[i] = (dv < 0 ? 1.0 : 0.0) * rho * (k1 * adv / 4 + std::sqrt(k2 * (dv * dv) + k3 * (cs[i] * cs[i]))) *
+                     (1 - lim) * adv;
+        }
+    }
+    return out;
+}
+
+// wFluidFlux.m:14-44 for the stage objects o (mass, mom x3, ener: primaries or stores)
+void w_fluid_flux(Sim& s, IArr* o[5], int X, Vec& freeze, Vec w[5]) {
     int d = X - 1;
     long long N = s.N;
+    const Vec* u[5] = {&o[0]->a, &o[1]->a, &o[2]->a, &o[3]->a, &o[4]->a};
     Vec press, sound;
     pressure(s, false, *u[0], *u[1], *u[2], *u[3], *u[4], press, &sound);
     Vec spd_line(s.face(d));
@@ -383,11 +504,12 @@ void w_fluid_flux(Sim& s, const Vec* u[5], int X, Vec& freeze, Vec w[5]) {
     }
     const Vec* cm[3] = {&s.mg[0].cellMag.a, &s.mg[1].cellMag.a, &s.mg[2].cellMag.a};
     for (int k = 0; k < 5; ++k) w[k].assign(N, 0.0);
+    Vec visc = viscosity_solve(s, o, sound, X);   // wFluidFlux.m:24 (0 for the empty solver)
 #pragma omp parallel for schedule(static)
     for (long long i = 0; i < N; ++i) {
         double fz = freeze[i];
         double velocity = mom_d[i] / rho[i];
-        double press_i = press[i] + 0.0;   // viscosity.solve -> 0 ('empty')
+        double press_i = press[i] + visc[i];
         double cx = (*cm[d])[i];
         w[0][i] = (*u[1 + d])[i] / fz;
         double we = velocity * ((*u[4])[i] + press_i) -
@@ -405,7 +527,7 @@ void relaxing_fluid(Sim& s, int X) {
     long long N = s.N;
     double ff = s.dt / s.dgrid[X - 1];
     Vec freeze, w[5];
-    const Vec* u[5] = {&s.fv[0].prim.a, &s.fv[1].prim.a, &s.fv[2].prim.a, &s.fv[3].prim.a, &s.fv[4].prim.a};
+    IArr* u[5] = {&s.fv[0].prim, &s.fv[1].prim, &s.fv[2].prim, &s.fv[3].prim, &s.fv[4].prim};
     w_fluid_flux(s, u, X, freeze, w);
     for (int k = 0; k < 5; ++k) {
         auto& v = s.fv[k];
@@ -433,7 +555,7 @@ void relaxing_fluid(Sim& s, int X) {
         for (long long i = 0; i < N; ++i) m[i] = std::fmax(s.fv[0].store.a[i], s.minmass);   // max ignores NaN
         s.fv[0].store.set(std::move(m));
     }
-    const Vec* us[5] = {&s.fv[0].store.a, &s.fv[1].store.a, &s.fv[2].store.a, &s.fv[3].store.a, &s.fv[4].store.a};
+    IArr* us[5] = {&s.fv[0].store, &s.fv[1].store, &s.fv[2].store, &s.fv[3].store, &s.fv[4].store};
     w_fluid_flux(s, us, X, freeze, w);
     int lim = s.limiter[X - 1];
     for (int k = 0; k < 5; ++k) {
@@ -627,10 +749,20 @@ int time_update(Sim& s, int flux_direction) {
 
 bool running(const Sim& s) { return s.iteration <= s.iter_max && s.time < s.time_max; }
 
+// source.m:30 (the radiation sink; gravity is not part of this path)
+void source(Sim& s) {
+    if (s.rad_type != 1) return;   // the empty solver gives 0
+    Vec r = radiation_solve(s);
+    Vec e(s.N);
+    for (long long k = 0; k < s.N; ++k) e[k] = s.fv[4].prim.a[k] - s.dt * r[k];
+    s.fv[4].prim.set(std::move(e));
+}
+
 int iterate(Sim& s) {
     for (int i = 1; i <= 2; ++i) {
         if (time_update(s, i) != 0) return -1;
         flux(s, i == 1 ? 1 : -1);
+        source(s);
     }
     s.iteration += 1;
     return 0;
@@ -692,6 +824,18 @@ void* orc_create(const int grid[3], const double dgrid[3], double gamma, double 
 
 void orc_destroy(void* p) { delete static_cast<Sim*>(p); }
 
+// Artificial viscosity and radiation settings (before orc_set_state, which initialises the radiation).
+void orc_set_physics(void* p, int visc_type, double visc_lin, double visc_quad, int rad_type, double rad_exp,
+                     double rad_initmax) {
+    Sim& s = *static_cast<Sim*>(p);
+    s.visc_type = visc_type;
+    s.visc_lin = visc_lin;
+    s.visc_quad = visc_quad;
+    s.rad_type = rad_type;
+    s.rad_exp = rad_exp;
+    s.rad_initmax = rad_initmax;
+}
+
 int orc_set_state(void* p, const double* mass, const double* mom, const double* ener, const double* mag) {
     Sim& s = *static_cast<Sim*>(p);
     long long N = s.N;
@@ -707,6 +851,7 @@ int orc_set_state(void* p, const double* mass, const double* mom, const double* 
         for (long long i = 0; i < N; ++i) sum += s.mg[c].prim.a[i];
         s.mg[c].isZero = (sum == 0) && !s.magnet_active;
     }
+    radiation_initialize(s);   // ImogenManager.initialize (imogen.m:46)
     return 0;
 }
 
@@ -728,6 +873,8 @@ int orc_flux(void* p, int order) { flux(*static_cast<Sim*>(p), order); return 0;
 int orc_relaxing_fluid(void* p, int X) { relaxing_fluid(*static_cast<Sim*>(p), X); return 0; }
 int orc_magnet_flux(void* p, int X, int I1, int I2) { magnet_flux(*static_cast<Sim*>(p), X, I1, I2); return 0; }
 int orc_iterate(void* p) { return iterate(*static_cast<Sim*>(p)); }
+void orc_source(void* p) { source(*static_cast<Sim*>(p)); }
+double orc_radiation_strength(void* p) { return static_cast<Sim*>(p)->rad_strength; }
 
 int orc_run(void* p, int max_iterations) {
     Sim& s = *static_cast<Sim*>(p);

@@ -29,12 +29,16 @@ dimension number d (1-based) is axis d-1 here.
 """
 from __future__ import annotations
 
+import math
+
 import numpy as np
 
 CIRC, CONST, FADE, MIRROR, TRANS, WALL = "circ", "const", "fade", "mirror", "trans", "wall"
 BC_MODES = (CIRC, CONST, FADE, MIRROR, TRANS, WALL)
 VANLEER, SUPERBEE, MINMOD = "vanleer", "superbee", "minmond"   # FluxLimiterEnum.m:10-13
 PER_STEP, PER_ITERATION = 0, 1                                  # enums/ENUM.m:33-34
+VISC_NONE, VISC_NR, VISC_CSW = "empty", "neumann_richtmyer", "caramana_shashkov_whalen"   # ENUM.m:53-55
+RAD_NONE, RAD_THIN = "empty", "optically_thin"                  # ENUM.m:49-50
 
 
 
@@ -161,6 +165,21 @@ class Edges:
             self.store[side][dim] = result
             return result
         return self.store[side][dim]   # fade / wall
+
+
+def _lpow(x, e):
+    """x**e elementwise with the C library's pow (correctly rounded; NumPy's vectorised power may differ
+    in the last bit), and the square root for e = 0.5 as NumPy's power takes it."""
+    x = np.asarray(x, dtype=float)
+    if e == 0.5:
+        return np.sqrt(x)
+
+    def one(v):
+        try:
+            return math.pow(v, e)
+        except (ValueError, OverflowError):
+            return float("nan")
+    return np.frompyfunc(one, 1, 1)(x).astype(float)
 
 
 # --------------------------------------------------------------------------------------------
@@ -414,7 +433,9 @@ class Sim:
 
     def __init__(self, grid, dgrid, gamma=5 / 3, cfl=0.7, minmass=1e-5, bc=None,
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
-                 magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION):
+                 magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
+                 viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0):
         self.grid = tuple(int(g) for g in grid)
         self.ndims = 3 if self.grid[2] > 1 else 2
         self.dgrid = tuple(float(v) for v in dgrid)
@@ -439,6 +460,14 @@ class Sim:
         self.dTime = 0.0
         self.iteration = 1
         self.history = []
+        # ArtificialViscosity (ArtificialViscosity.m:31-57) and Radiation (Radiation.m:32-57) settings
+        self.visc_type = viscosity
+        self.visc_linear = float(visc_linear)
+        self.visc_quadratic = float(visc_quadratic)
+        self.rad_type = radiation
+        self.rad_exponent = float(rad_exponent)
+        self.rad_initial_maximum = float(rad_initial_maximum)
+        self.rad_strength = 1.0
 
     # imogen.m:30-42
     def set_state(self, mass, mom, ener, mag):
@@ -450,6 +479,78 @@ class Sim:
         self.mag = [MagComp(self, i + 1, f(mag[i])) for i in range(3)]
         for i in range(3):
             self.mag[i].isZero = (np.sum(self.mag[i].prim.a) == 0) and not self.magnet_active
+        self.radiation_initialize()
+
+    # ---------------------------------------------------------------------------------------
+    # Radiation (fluid/Radiation.m) and ArtificialViscosity (fluid/ArtificialViscosity.m)
+    def radiation_solve(self):
+        """Radiation.solve: opticallyThinSolver (Radiation.m:86-88) or the empty solver (0)."""
+        if self.rad_type != RAD_THIN:
+            return 0.0
+        gas, _ = self.pressure("gas", self.mass.prim.a, [m.prim.a for m in self.mom], self.ener.prim.a)
+        return self.rad_strength * _lpow(self.mass.prim.a, 2 - self.rad_exponent) * _lpow(gas, self.rad_exponent)
+
+    def radiation_initialize(self):
+        """Radiation.initialize (Radiation.m:61-75), called by ImogenManager.initialize after the arrays
+        are built (imogen.m:46): strength = initialMaximum/100 * min((E - KE - ME) / unscaled), with the
+        kinetic energy from the momenta and the magnetic energy from the face-centred B."""
+        if self.rad_type != RAD_THIN:
+            self.rad_strength = 0.0
+            return
+        self.rad_strength = 1.0
+        unscaled = self.radiation_solve()
+        p = [m.prim.a for m in self.mom]
+        b = [m.prim.a for m in self.mag]
+        kinetic = 0.5 * (p[0] * p[0] + p[1] * p[1] + p[2] * p[2]) / self.mass.prim.a
+        magnetic = 0.5 * (b[0] * b[0] + b[1] * b[1] + b[2] * b[2])
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = (self.ener.prim.a - kinetic - magnetic) / unscaled
+        self.rad_strength = (self.rad_initial_maximum / 100) * float(np.nanmin(ratio))   # minFinderND
+
+    def csw_sound_speed(self, mass, mom, ener, X):
+        """ArtificialViscosity.cswSoundSpeed (ArtificialViscosity.m:157-190).  As written in the
+        reference, only the z momentum of the velocity-squared sum is divided by rho^2."""
+        G = self.GAMMA
+        out = []
+        for n in (1, -1):
+            vel_sq = (mom[0].shift(X, n) ** 2 + mom[1].shift(X, n) ** 2
+                      + mom[2].shift(X, n) ** 2 / mass.shift(X, n) ** 2)
+            mag_sq = (self.mag[0].cellMag.shift(X, n) ** 2 + self.mag[1].cellMag.shift(X, n) ** 2
+                      + self.mag[2].cellMag.shift(X, n) ** 2)
+            s = (G - 1.0) * (ener.shift(X, n) - 0.5 * mass.shift(X, n) * vel_sq)
+            s = s - (G - 1.0) * 0.5 * mag_sq
+            with np.errstate(invalid="ignore"):
+                s = np.sqrt(np.abs((G * s + 2.0 * mag_sq) / mass.shift(X, n)))
+            out.append(s)
+        snd_c, snd_b = out
+        return np.fmax(np.fmin(snd_b, snd_c), 0)
+
+    def viscosity_solve(self, mass, mom, ener, sound, X):
+        """ArtificialViscosity.solve for the stage arrays (objects with .a and .shift)."""
+        d = X - 1
+        c1, c2 = self.visc_linear, self.visc_quadratic
+        if self.visc_type == VISC_NR:   # ArtificialViscosity.m:73-77
+            vm = np.fmin(mom[d].shift(X, 1) - mom[d].a, 0)
+            return vm * (c1 * sound + c2 * vm / mass.a)
+        if self.visc_type == VISC_CSW:  # ArtificialViscosity.m:81-148 (averaged densities)
+            mass_b = mass.shift(X, -1)
+            mass_c = mass.shift(X, 1)
+            rho = 2 * mass_c * mass_b / (mass_c + mass_b)
+            cs = self.csw_sound_speed(mass, mom, ener, X)
+            v0 = mom[d].shift(X, -2) / mass.shift(X, -2)
+            v1 = mom[d].shift(X, -1) / mass.shift(X, -1)
+            v2 = mom[d].shift(X, 1) / mass.shift(X, 1)
+            v3 = mom[d].shift(X, 2) / mass.shift(X, 2)
+            dv = v2 - v1
+            G = self.GAMMA
+            with np.errstate(divide="ignore", invalid="ignore"):
+                r_l = (v3 - v2) / (2 * dv)
+                r_r = (v1 - v0) / (2 * dv)
+                limiter = np.fmax(0, np.fmin(np.fmin(0.5 * (r_l + r_r), np.fmin(2 * r_l, 2 * r_r)), 1))
+                return ((dv < 0) * rho * (c2 * (G + 1) * np.abs(dv) / 4
+                                          + np.sqrt(c2 ** 2 * ((G + 1) / 4) ** 2 * dv ** 2 + c1 ** 2 * cs ** 2))
+                        * (1 - limiter) * np.abs(dv))
+        return 0.0
 
     def state(self):
         return dict(mass=self.mass.prim.a.copy(), ener=self.ener.prim.a.copy(),
@@ -485,14 +586,17 @@ class Sim:
         result = np.where(result < 0, 0.0, result)
         return result, aux
 
-    def w_fluid_flux(self, rho, mom, ener, X):
-        """wFluidFlux.m:14-44: freeze speed (per-pencil max, broadcast) and W arrays."""
+    def w_fluid_flux(self, objs, X):
+        """wFluidFlux.m:14-44: freeze speed (per-pencil max, broadcast) and W arrays; objs are the
+        stage's (mass, [mom x3], ener) array objects (primaries for the predictor, stores for the
+        corrector)."""
         d = X - 1
+        rho, mom, ener = objs[0].a, [m.a for m in objs[1]], objs[2].a
         press, sound = self.pressure("totsnd", rho, mom, ener)
         velocity = mom[d] / rho
         spd = np.nanmax(np.abs(velocity) + sound, axis=d, keepdims=True)
         freeze = np.broadcast_to(spd, rho.shape)
-        press = press + 0.0                               # viscosity.solve: 'empty' -> 0
+        press = press + self.viscosity_solve(objs[0], objs[1], objs[2], sound, X)   # wFluidFlux.m:24
         cm = [self.mag[i].cellMag.a for i in range(3)]
         w_mass = mom[d] / freeze
         w_ener = velocity * (ener + press) - cm[d] * (cm[0] * mom[0] + cm[1] * mom[1]
@@ -511,8 +615,7 @@ class Sim:
         """relaxingFluid.m:16-73."""
         flux_factor = self.dTime / self.dgrid[X - 1]
         v = self.fluid_vars()
-        freeze, w = self.w_fluid_flux(v[0].prim.a, [v[1].prim.a, v[2].prim.a, v[3].prim.a],
-                                      v[4].prim.a, X)
+        freeze, w = self.w_fluid_flux((v[0].prim, [v[1].prim, v[2].prim, v[3].prim], v[4].prim), X)
         for i in range(5):
             vi = v[i]
             vi.store_fluxR.set(0.5 * (vi.prim.a + w[i]))
@@ -524,8 +627,7 @@ class Sim:
             vi.store_fluxL.cleanup()
         self.mass.store.set(np.fmax(self.mass.store.a, self.MINMASS))   # MATLAB max ignores NaN
 
-        freeze, w = self.w_fluid_flux(v[0].store.a, [v[1].store.a, v[2].store.a, v[3].store.a],
-                                      v[4].store.a, X)
+        freeze, w = self.w_fluid_flux((v[0].store, [v[1].store, v[2].store, v[3].store], v[4].store), X)
         lim = LIMITERS[self.limiter[X - 1]]
         for i in range(5):
             vi = v[i]
@@ -637,12 +739,18 @@ class Sim:
     def running(self):
         return self.iteration <= self.ITERMAX and self.time < self.TIMEMAX
 
+    def source(self):
+        """source.m:30: ener.array = ener.array - dTime * radiation.solve (the empty solver gives 0;
+        gravity is not part of this path)."""
+        if self.rad_type == RAD_THIN:
+            self.ener.prim.set(self.ener.prim.a - self.dTime * self.radiation_solve())
+
     def iterate(self):
         """One pass of the imogen.m:58-72 loop body (two timesteps)."""
         for i, direction in ((1, 1), (2, -1)):
             self.time_update(i)
             self.flux(direction)
-            # source.m:30 -- radiation 'empty' returns 0, so ener - dt*0 leaves ener unchanged
+            self.source()
         self.iteration += 1
 
     def run(self, max_iterations=None):

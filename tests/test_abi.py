@@ -92,3 +92,30 @@ def test_mex_gateway_compiles_against_the_abi():
         assert r.returncode == 0, r.stderr
     called = set(re.findall(r"\b(img_[a-z_]+)\(", open(src).read()))
     assert called <= set(_lib.SYMBOLS), called - set(_lib.SYMBOLS)
+
+
+def test_create_rejects_viscosity_the_segment_kernel_cannot_take():
+    """Artificial viscosity runs in the one-block segment kernel: circ or const ends shared by all
+    classes, and a segment tiling for every swept pencil length (checked before any device call)."""
+    L = _lib.lib()
+    cases = [dict(grid=(64, 32, 1), bc="trans"), dict(grid=(64, 32, 1), bc="mirror"),
+             dict(grid=(64, 32, 1), bc={"mass": "circ", "mom": "const", "ener": "circ", "mag": "circ"}),
+             dict(grid=(100, 32, 1), bc="circ"),        # x: 100 / C threads is no power of two up to 32
+             dict(grid=(64, 4096, 1), bc="circ")]       # y: N / C > 512 threads
+    for kw in cases:
+        c = make_config(viscosity="neumann_richtmyer", **kw)
+        h = ctypes.c_void_p()
+        assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -4, kw
+        assert b"viscosity" in L.img_last_error(None), kw
+    for bad in (dict(viscosity=3), dict(radiation=2)):
+        c = make_config(grid=(64, 32, 1), **bad)
+        h = ctypes.c_void_p()
+        assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -1, bad
+
+
+def test_config_defaults_match_the_reference_constructors():
+    """ArtificialViscosity() (ArtificialViscosity.m:31-37) and Radiation() (Radiation.m:32-37)."""
+    c = _lib.ImgConfig()
+    _lib.lib().img_config_default(ctypes.byref(c))
+    assert (c.viscosity_type, c.visc_linear, c.visc_quadratic) == (0, 0.0, 0.0)
+    assert (c.radiation_type, c.rad_exponent, c.rad_initial_maximum) == (0, 0.5, 0.0)

@@ -127,7 +127,7 @@ def test_batch_rejects_members_with_another_launch_sequence():
 def test_long_cluster_members_with_fade_match_alone():
     """Members whose x pencils span a 4-CTA cluster at 4 cells per thread (N > 4096), fade ends: the
     batched launches run the same cluster barriers and DSMEM exchanges as the launches alone."""
-    tubes = [problems.brio_wu_ensemble()[i] for i in (4, 5, 9, 1)]      # N = 4288, 6054, 6541, 652
+    tubes = [problems.brio_wu_ensemble(xbc="fade")[i] for i in (4, 5, 9, 1)]      # N = 4288, 6054, 6541, 652
     alone = [_make(dict(s, time_max=1e5), st, "mixed") for s, st in tubes]
     together = [_make(dict(s, time_max=1e5), st, "mixed") for s, st in tubes]
     b = ImogenBatch(together)

@@ -168,7 +168,7 @@ def _side_fluxes(jump, gamma):
     ener = P[side] / (gamma - 1) + 0.5 * r * (v[:, side] ** 2).sum(0) + 0.5 * (mag ** 2).sum(0)
     sim = np_oracle.Sim(grid, (1.0 / n,) * 3, gamma=gamma, bc="const", magnet_active=True)
     sim.set_state(r.reshape(grid), [m.reshape(grid) for m in mom], ener.reshape(grid), [b.reshape(grid) for b in mag])
-    freeze, w = sim.w_fluid_flux(sim.mass.prim.a, [m.prim.a for m in sim.mom], sim.ener.prim.a, 1)
+    freeze, w = sim.w_fluid_flux((sim.mass.prim, [m.prim for m in sim.mom], sim.ener.prim), 1)
     f = np.stack([np.asarray(wi * freeze).reshape(n) for wi in w])          # [variable][cell]
     ind = np.stack([v[0][side] * B[c][side] - B[0][side] * v[c][side] for c in (1, 2)])
     cells = [1, n - 2]                        # away from the interface (cell-centred B exact there)
@@ -231,3 +231,53 @@ def test_stationary_shock_from_reference_jump_stays_put():
     mid = 0.5 * (rho[0] + rho[1])
     crossing = np.argmax(out > mid)
     assert abs(crossing - n // 2) <= 2, (crossing, out)
+
+
+# run_Debug.m's settings: Neumann-Richtmyer 0.1 / 0.25, optically thin radiation with exponent 0.5 and
+# initialMaximum 0.1 (per cent); the CSW case takes the same strengths.
+@pytest.mark.parametrize("bc", ["circ", "const", "trans", "wall"])
+@pytest.mark.parametrize("viscosity,radiation", [
+    ("neumann_richtmyer", "empty"), ("caramana_shashkov_whalen", "empty"), ("empty", "optically_thin"),
+    ("neumann_richtmyer", "optically_thin"), ("caramana_shashkov_whalen", "optically_thin")])
+def test_numpy_and_cpp_oracles_bitwise_viscosity_radiation(bc, viscosity, radiation):
+    grid = (24, 22, 1)
+    s = dict(grid=grid, dgrid=tuple(1 / g for g in grid), gamma=5 / 3, cfl=0.35, bc=bc, magnet=True, iter_max=5,
+             viscosity=viscosity, visc_linear=0.1, visc_quadratic=0.25, radiation=radiation,
+             rad_exponent=0.5, rad_initial_maximum=0.1)
+    kw = problems.oracle_kwargs(s)
+    st = smooth_state(grid, seed=11, mhd=True)
+    a = np_oracle.Sim(**kw)
+    a.set_state(*st)
+    b = cpp_oracle.Sim(**kw)
+    b.set_state(*st)
+    assert a.rad_strength == b.rad_strength
+    if radiation == "optically_thin":
+        assert a.rad_strength > 0
+    a.run()
+    b.run()
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    assert a.time == b.time
+
+
+def test_viscosity_and_radiation_change_the_result():
+    """Each physics option moves the state away from the inviscid, non-radiating run."""
+    grid = (24, 22, 1)
+    base = dict(grid=grid, dgrid=tuple(1 / g for g in grid), gamma=5 / 3, cfl=0.35, bc="circ", magnet=True,
+                iter_max=4, visc_linear=0.1, visc_quadratic=0.25, rad_initial_maximum=0.1)
+    st = smooth_state(grid, seed=3, mhd=True)
+    st = (st[0], st[1] * 4, st[2] + 0.5 * ((st[1] * 4) ** 2 - st[1] ** 2).sum(0) / st[0], st[3])   # compressive flow
+    out = {}
+    for key, extra in {"none": {}, "nr": dict(viscosity="neumann_richtmyer"),
+                       "csw": dict(viscosity="caramana_shashkov_whalen"),
+                       "rad": dict(radiation="optically_thin")}.items():
+        o = cpp_oracle.Sim(**problems.oracle_kwargs(dict(base, **extra)))
+        o.set_state(*st)
+        o.run()
+        out[key] = o.state()
+    for key in ("nr", "csw", "rad"):
+        d = np.abs(out[key]["ener"] - out["none"]["ener"]).sum() / np.abs(out["none"]["ener"]).sum()
+        assert d > 1e-8, (key, d)
+    # the radiation sink removes energy
+    assert out["rad"]["ener"].sum() < out["none"]["ener"].sum()
