@@ -17,7 +17,17 @@ namespace img {
 namespace cg = cooperative_groups;
 
 // ---- enumerations shared with the host (values match include/imogen_b200.h) --------------------
-enum BcMode { BC_CIRC = 0, BC_CONST = 1, BC_FADE = 2, BC_MIRROR = 3, BC_TRANS = 4, BC_WALL = 5 };
+enum BcMode { BC_CIRC = 0, BC_CONST = 1, BC_FADE = 2, BC_MIRROR = 3, BC_TRANS = 4, BC_WALL = 5, BC_FLIP = 6, BC_ZERO = 7,
+              BC_LINEAR = 8, BC_WORMHOLE = 9 };
+// Ghost flags of one array object: GF_NEG negates mirror/flip ghosts (the array's component is the
+// shift direction, mirror_shift.m / flip_shift.m); GF_ZLO / GF_ZHI make a zero-BC ghost 0 on the
+// lower / upper side (zero_shift.m: a FluxArray other than fluxl below and other than fluxr above).
+constexpr int GF_NEG = 1;
+constexpr int GF_ZLO = 2;
+constexpr int GF_ZHI = 4;
+constexpr int GF_FLUXR = GF_ZLO;             // fluxType 'fluxr'
+constexpr int GF_FLUXL = GF_ZHI;             // fluxType 'fluxl'
+constexpr int GF_FLUX = GF_ZLO | GF_ZHI;     // other flux types ('flux')
 enum Limiter { LIM_VANLEER = 0, LIM_SUPERBEE = 1, LIM_MINMOD = 2 };
 enum BcClass { CLS_MASS = 0, CLS_MOM = 1, CLS_ENER = 2, CLS_MAG = 3 };
 enum Var { Q_RHO = 0, Q_PX, Q_PY, Q_PZ, Q_E, Q_BX, Q_BY, Q_BZ, Q_CBX, Q_CBY, Q_CBZ, NQ };

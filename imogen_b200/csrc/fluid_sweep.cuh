@@ -282,7 +282,7 @@ __device__ __forceinline__ void fluid_halo_jobs(const Tile<T, CPT>& tl, const Fl
         const int cls = fluid_class(v);
         double* edge = a.edges->p[fluid_obj(v, isL ? kindL : kindR)][tl.d][side];
         halo_job(tl, base + arr * AS, an + (arr * 2 + side) * tl.Wb, side, shift, a.mode[cls][side], a.act[cls],
-                 v == 1 + tl.d, edge, a.bc_inf, 1);
+                 (v == 1 + tl.d ? GF_NEG : 0) | (isL ? GF_FLUXL : GF_FLUXR), edge, a.bc_inf, 1);
     }
 }
 

@@ -989,7 +989,18 @@ int validate(const img_config& c, std::string& why) {
         for (int s = 0; s < 2; ++s)
             for (int d = 0; d < ndims; ++d) {
                 int m = c.bc_modes[k][s][d];
-                if (m < 0 || m > 5) { why = "unknown BC mode"; return IMG_ERR_ARG; }
+                if (m < 0 || m > IMG_BC_WORMHOLE) { why = "unknown BC mode"; return IMG_ERR_ARG; }
+                if (m == IMG_BC_LINEAR) {   // linear_shift.m:20: `dim` is never defined
+                    why = "linear BC: linear_shift.m indexes with the undefined variable 'dim' (the reference stops "
+                          "at the first shift)";
+                    return IMG_ERR_UNSUPPORTED;
+                }
+                if (m == IMG_BC_WORMHOLE && s == 0) {   // wormhole_shift.m:16-61, lower side only
+                    why = ndims < 3 ? "wormhole BC on a 2-D grid (wormhole_shift.m indexes a third dimension)"
+                                    : "lower wormhole BC: the ghosts come from the pencil mirrored along nextDir, "
+                                      "which this path does not couple";
+                    return IMG_ERR_UNSUPPORTED;
+                }
                 // mirror_shift.m:31-33 / fade_shift.m:34-44 and Edges.m:80-93 index outside short
                 // dimensions: the reference stops with an index error there.
                 if (m == IMG_BC_MIRROR && c.grid[d] < 2) { why = "mirror BC on a dimension of extent 1"; return IMG_ERR_UNSUPPORTED; }

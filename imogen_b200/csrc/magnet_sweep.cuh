@@ -46,7 +46,7 @@ struct MagArgs {
 // mode/act/flip/edge describe the array object; the edge state of a trans edge is drifted and
 // written back when `own_update` (exactly one thread per face cell calls with own_update = true).
 template <typename T, typename At>
-__device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long fi, int n, int mode, int act, bool flip,
+__device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long fi, int n, int mode, int act, int flip,
                                         double* edge, const double* fc, int f, double bc_inf, bool own_update) {
     const bool upper = n > 0;
     const bool is_ghost = upper ? (i == Ne - 1) : (i == 0);
@@ -61,7 +61,9 @@ __device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long f
     }
     switch (mode) {
         case BC_CIRC: return at(upper ? 0 : Ne - 1);
-        case BC_MIRROR: { T v = upper ? at(Ne - 2) : at(1); return flip ? -v : v; }
+        case BC_MIRROR: { T v = upper ? at(Ne - 2) : at(1); return (flip & GF_NEG) ? -v : v; }
+        case BC_FLIP: { T v = upper ? at(Ne - 1) : at(0); return (flip & GF_NEG) ? -v : v; }
+        case BC_ZERO: return (flip & (upper ? GF_ZHI : GF_ZLO)) ? T(0) : at(upper ? Ne - 1 : 0);
         case BC_WALL: return (T)edge[fi];
         case BC_TRANS: {
             T a1, a2;
@@ -87,7 +89,7 @@ __device__ __forceinline__ T shift_line(const At& at, int i, int Ne, long long f
 // A.shift(dim e, n)[cell] for an array A in global memory.
 template <typename T>
 __device__ __forceinline__ T shift_along(const Geom& g, const T* A, long long cell, int x, int y, int z, int e, int n,
-                                         int mode, int act, bool flip, double* edge, const double* fc, int f,
+                                         int mode, int act, int flip, double* edge, const double* fc, int f,
                                          double bc_inf, bool own_update) {
     const int Ne = sel3(e, g.n[0], g.n[1], g.n[2]);
     const long long se = sel3(e, g.s[0], g.s[1], g.s[2]);
@@ -219,8 +221,10 @@ __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock
     // halo jobs: (component q, side) is done by thread g == (2q + side) mod G of the column
     auto job = [&](int q, int side) { return tl.colok && tl.g == (2 * q + side) % tl.G; };
     auto halo = [&](int q, T* A, int kind, bool lo_shift, bool hi_shift, int hi_rows) {
-        if (job(q, 0)) halo_job(tl, A, GS(q), 0, lo_shift, mlo, a.actX, 0, edge_of(q, kind, 0), binf, hi_rows);
-        if (job(q, 1)) halo_job(tl, A, GS(q) + Wb, 1, hi_shift, mhi, a.actX, 0, edge_of(q, kind, 1), binf, hi_rows);
+        // zero-BC flags by object: the store's fluxR and the flux are FluxArrays, velGrid/wMag are not
+        const int gf = kind == MO_STORE_R ? GF_FLUXR : (kind == MO_FLUX ? GF_FLUX : 0);
+        if (job(q, 0)) halo_job(tl, A, GS(q), 0, lo_shift, mlo, a.actX, gf, edge_of(q, kind, 0), binf, hi_rows);
+        if (job(q, 1)) halo_job(tl, A, GS(q) + Wb, 1, hi_shift, mhi, a.actX, gf, edge_of(q, kind, 1), binf, hi_rows);
     };
 
     // ---- corner velocity (magnetFlux.m:18-19): transverse average with mass/mom BCs along I ------
@@ -506,7 +510,7 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
                 else {
                     int x, y, z;
                     tl.coords(k, x, y, z);
-                    c = fv - shift_along<T>(g, F, o, x, y, z, e, +1, modeI, actI, true,
+                    c = fv - shift_along<T>(g, F, o, x, y, z, e, +1, modeI, actI, GF_NEG | GF_FLUX,
                                             et->p[mag_obj(e, d, MO_FLUX)][e][1], fc, f, binf, true);
                 }
             }
@@ -519,7 +523,7 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
 #pragma unroll
         for (int q = 0; q < 2; ++q)
             if (tl.colok && tl.g == q % tl.G)
-                halo_job(tl, S + q * AS, GS + q * Wb, 0, true, mlo, a.actX, 0,
+                halo_job(tl, S + q * AS, GS + q * Wb, 0, true, mlo, a.actX, GF_FLUX,
                          et->p[mag_obj((q ? a.I[1] : a.I[0]) - 1, d, MO_FLUX)][d][0], binf, 1);
         __syncthreads();
     }
@@ -551,7 +555,7 @@ __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vbloc
     if constexpr (!CG) {
         // upper ghost of the new B_X along X: mag(X).shift(X, +1) of the primary array (mirror flips B_X)
         if (tl.colok && tl.g == 2 % tl.G)
-            halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, 1, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
+            halo_job(tl, S + 2 * AS, GS + 2 * Wb, 1, true, mhi, a.actX, GF_NEG, et->p[OBJ_PRIM_MAG + d][d][1], binf, 1);
         __syncthreads();
     }
     pdl_trigger();

@@ -241,8 +241,15 @@ __device__ __forceinline__ T bc_ghost(const Tile<T, CPT>& tl, const T* A, int n,
         case BC_CIRC: return upper ? tl.row(A, mp - 1) : tl.row(A, N - 1);
         case BC_MIRROR: {
             T x = upper ? tl.row(A, N - 1 - mp) : tl.row(A, mp);
-            return flip ? -x : x;
+            return (flip & GF_NEG) ? -x : x;
         }
+        case BC_FLIP: {   // flip_shift.m:22-40
+            T x = upper ? tl.row(A, N - 1) : tl.row(A, 0);
+            return (flip & GF_NEG) ? -x : x;
+        }
+        case BC_ZERO:     // zero_shift.m:14-46
+            if (flip & (upper ? GF_ZHI : GF_ZLO)) return T(0);
+            return upper ? tl.row(A, N - 1) : tl.row(A, 0);
         case BC_WALL: return (T)(ev != NO_EV ? ev : edge[tl.col]);
         case BC_TRANS: return (T)trans_bc_ghost<T, CPT>(tl, A, n, mp, act, edge, bc_inf, ev);
         default: return upper ? tl.row(A, N - 1) : tl.row(A, 0);   // const and fade: constant shift

@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from ._lib import ImgConfig, ImogenError, check, lib
 
-BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall")      # enums/ENUM.m:22-31
+BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall", "flip", "zero", "linear", "wormhole")   # enums/ENUM.m:22-32
 LIMITERS = {"vanleer": 0, "superbee": 1, "minmond": 2, "minmod": 2}   # FluxLimiterEnum.m:10-13
 BC_CLASSES = ("mass", "mom", "ener", "mag")
 PRECISIONS = {"fp64": 0, "mixed": 1}

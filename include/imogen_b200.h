@@ -31,7 +31,12 @@ enum {
 };
 
 /* ---- enumerations (enums/ENUM.m, enums/FluxLimiterEnum.m) ----------------------------------- */
-enum { IMG_BC_CIRC = 0, IMG_BC_CONST = 1, IMG_BC_FADE = 2, IMG_BC_MIRROR = 3, IMG_BC_TRANS = 4, IMG_BC_WALL = 5 };
+enum { IMG_BC_CIRC = 0, IMG_BC_CONST = 1, IMG_BC_FADE = 2, IMG_BC_MIRROR = 3, IMG_BC_TRANS = 4, IMG_BC_WALL = 5,
+       IMG_BC_FLIP = 6, IMG_BC_ZERO = 7, IMG_BC_LINEAR = 8, IMG_BC_WORMHOLE = 9 };
+/* linear: rejected (IMG_ERR_UNSUPPORTED) -- linear_shift.m:20 indexes with an undefined variable, so the
+ * reference stops at the first shift.  wormhole: the upper side is the constant shift (as in
+ * wormhole_shift.m); a lower wormhole side couples pencils across the grid and is rejected
+ * (IMG_ERR_UNSUPPORTED), as it is in 2-D by the reference itself. */
 enum { IMG_LIM_VANLEER = 0, IMG_LIM_SUPERBEE = 1, IMG_LIM_MINMOD = 2 };
 enum { IMG_CLS_MASS = 0, IMG_CLS_MOM = 1, IMG_CLS_ENER = 2, IMG_CLS_MAG = 3 };
 enum { IMG_PREC_FP64 = 0, IMG_PREC_MIXED = 1 };

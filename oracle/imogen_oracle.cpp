@@ -29,7 +29,10 @@
 
 namespace {
 
-enum Mode { CIRC = 0, CONST = 1, FADE = 2, MIRROR = 3, TRANS = 4, WALL = 5 };
+enum Mode { CIRC = 0, CONST = 1, FADE = 2, MIRROR = 3, TRANS = 4, WALL = 5, FLIP = 6, ZERO = 7, LINEAR = 8, WORMHOLE = 9 };
+// FluxArray.fluxType (flux/FluxArray.m:28-35) as zero_shift.m reads it: not a FluxArray, 'fluxr',
+// 'fluxl', or another flux type ('flux' of MagnetArray.m:96)
+enum FluxType { FT_NONE = 0, FT_FLUXR = 1, FT_FLUXL = 2, FT_FLUX = 3 };
 enum Lim { VANLEER = 0, SUPERBEE = 1, MINMOD = 2 };
 enum Cls { C_MASS = 0, C_MOM = 1, C_ENER = 2, C_MAG = 3 };
 
@@ -97,6 +100,7 @@ struct IArr {
     Sim* sim = nullptr;
     int component = 0;   // 0 scalar, 1..3
     int cls = 0;         // BC class
+    int ftype = FT_NONE; // FluxArray type (zero_shift.m)
     Vec a;
     bool uninit = true;
     Edges edges;
@@ -233,13 +237,48 @@ Vec IArr::shift(int DIRECT, int n) {
         }
         return r;
     }
-    // constant shift underlies const / trans / wall / fade
+    // constant shift underlies const / trans / wall / fade / flip / zero / wormhole
 #pragma omp parallel for schedule(static)
     for (long long f = 0; f < nf; ++f) {
         long long b = base_of(f);
         for (int i = 0; i < Nd; ++i) r[b + i * sd] = a[b + (long long)cidx(i, n, Nd) * sd];
     }
     if (mode == CONST) return r;
+    if (mode == FLIP || mode == ZERO) {
+        // flip_shift.m:22-40: the ghosts of the constant shift, negated for the component along DIRECT.
+        // zero_shift.m:14-46: a FluxArray's ghosts are 0 except on the side where its type keeps the
+        // constant shift (fluxl for n < 0, fluxr for n > 0); other arrays take the constant shift.
+        bool zero = false;
+        if (mode == ZERO) zero = ftype != FT_NONE && !(n < 0 ? ftype == FT_FLUXL : ftype == FT_FLUXR);
+        if (mode == FLIP && component != DIRECT) return r;
+        if (mode == ZERO && !zero) return r;
+        for (long long f = 0; f < nf; ++f) {
+            long long b = base_of(f);
+            for (int k = 0; k < m; ++k) {
+                double& v = r[b + (long long)(n < 0 ? k : Nd - m + k) * sd];
+                v = mode == FLIP ? -v : 0.0;
+            }
+        }
+        return r;
+    }
+    if (mode == WORMHOLE) {
+        // wormhole_shift.m:16-61: for n < 0 the first |n| ghosts along DIRECT are the array's own
+        // first |n| cells in reverse order along DIRECT and along nextDir = [2 3 1](DIRECT), negated
+        // for the component along DIRECT; for n > 0 the constant shift.  (3-D only: in 2-D the
+        // reference indexes a third dimension the array does not have.)
+        if (n > 0) return r;
+        const int dn = (d + 1) % 3;
+        const double sg = component == DIRECT ? -1.0 : 1.0;
+        for (long long c = 0; c < s.N; ++c) {
+            int xyz[3] = {(int)(c % s.n[0]), (int)((c / s.n[0]) % s.n[1]), (int)(c / ((long long)s.n[0] * s.n[1]))};
+            if (xyz[d] >= m) continue;
+            int src[3] = {xyz[0], xyz[1], xyz[2]};
+            src[d] = m - 1 - xyz[d];
+            src[dn] = s.n[dn] - 1 - xyz[dn];
+            r[c] = sg * a[src[0] + src[1] * s.stride(1) + src[2] * s.stride(2)];
+        }
+        return r;
+    }
 
     if (mode == WALL) {   // wall_shift.m:12-33
         Vec e = transparent_edge(DIRECT, n > 0);
@@ -797,8 +836,12 @@ void* orc_create(const int grid[3], const double dgrid[3], double gamma, double 
         for (int side = 0; side < 2; ++side)
             for (int d = 0; d < s->ndims; ++d) {
                 int mode = s->bc[c][side][d];
-                bool bad = mode < 0 || mode > 5 || (mode == MIRROR && grid[d] < 2) ||
-                           (mode == FADE && grid[d] < std::max(20, bc_infinity));
+                // linear_shift.m:20 indexes with the undefined variable `dim` (the reference errors at the
+                // first shift); wormhole_shift.m:27-33 indexes a third dimension (2-D grids error at the
+                // first lower shift)
+                bool bad = mode < 0 || mode > 9 || (mode == MIRROR && grid[d] < 2) ||
+                           (mode == FADE && grid[d] < std::max(20, bc_infinity)) || mode == LINEAR ||
+                           (mode == WORMHOLE && side == 0 && s->ndims < 3);
                 if (bad) { delete s; return nullptr; }
             }
     s->fluid_active = fluid_active != 0;
@@ -810,14 +853,19 @@ void* orc_create(const int grid[3], const double dgrid[3], double gamma, double 
         auto& v = s->fv[k];
         for (IArr* A : {&v.prim, &v.store, &v.store_fluxR, &v.store_fluxL, &v.fluxR, &v.fluxL})
             s->init_arr(*A, comp[k], cls[k]);
+        v.store_fluxR.ftype = v.fluxR.ftype = FT_FLUXR;   // StorageArray.m:69-70, FluidArray.m:104-105
+        v.store_fluxL.ftype = v.fluxL.ftype = FT_FLUXL;
     }
     for (int c = 0; c < 3; ++c) {
         auto& m = s->mg[c];
         s->init_arr(m.prim, c + 1, C_MAG);
         s->init_arr(m.cellMag, c + 1, C_MAG);
-        for (int X = 1; X <= 3; ++X)
+        for (int X = 1; X <= 3; ++X) {
             for (IArr* A : {&m.velGrid[X], &m.store[X], &m.store_fluxR[X], &m.wMag[X], &m.flux[X]})
                 s->init_arr(*A, c + 1, C_MAG);
+            m.store_fluxR[X].ftype = FT_FLUXR;   // the store's fluxR (StorageArray.m:70)
+            m.flux[X].ftype = FT_FLUX;           // MagnetArray.m:96: fluxType 'flux'
+        }
     }
     return s;
 }

@@ -34,7 +34,10 @@ import math
 import numpy as np
 
 CIRC, CONST, FADE, MIRROR, TRANS, WALL = "circ", "const", "fade", "mirror", "trans", "wall"
-BC_MODES = (CIRC, CONST, FADE, MIRROR, TRANS, WALL)
+FLIP, ZERO, LINEAR, WORMHOLE = "flip", "zero", "linear", "wormhole"
+BC_MODES = (CIRC, CONST, FADE, MIRROR, TRANS, WALL, FLIP, ZERO, LINEAR, WORMHOLE)
+# FluxArray.fluxType (flux/FluxArray.m:28-35) as zero_shift.m reads it (None: not a FluxArray)
+FLUXR, FLUXL, FLUX = "fluxr", "fluxl", "flux"
 VANLEER, SUPERBEE, MINMOD = "vanleer", "superbee", "minmond"   # FluxLimiterEnum.m:10-13
 PER_STEP, PER_ITERATION = 0, 1                                  # enums/ENUM.m:33-34
 VISC_NONE, VISC_NR, VISC_CSW = "empty", "neumann_richtmyer", "caramana_shashkov_whalen"   # ENUM.m:53-55
@@ -192,9 +195,10 @@ class IArray:
     InitializedArray.m:43-47); ``True`` gives a primary array whose edges come from the IC.
     """
 
-    def __init__(self, sim, component, bc_class, data=None):
+    def __init__(self, sim, component, bc_class, data=None, flux_type=None):
         self.sim = sim
         self.component = component          # 0 scalar, 1..3 vector component
+        self.flux_type = flux_type          # FluxArray type, None for other arrays
         self.bc_modes = sim.bc[bc_class]    # [side][dim]
         self.a = None
         self.edges = None
@@ -222,7 +226,8 @@ class IArray:
             return self.a
         mode = self.bc_modes[1 if n > 0 else 0][d]
         fn = {CIRC: _circ_shift, CONST: _constant_shift, MIRROR: _mirror_shift,
-              TRANS: _transparent_shift, WALL: _wall_shift, FADE: _fade_shift}[mode]
+              TRANS: _transparent_shift, WALL: _wall_shift, FADE: _fade_shift, FLIP: _flip_shift,
+              ZERO: _zero_shift, LINEAR: _linear_shift, WORMHOLE: _wormhole_shift}[mode]
         return fn(self.a, DIRECT, n, self)
 
     def transparent_edge(self, dim, upper):
@@ -248,6 +253,55 @@ def _circ_shift(a, DIRECT, n, obj):
 def _constant_shift(a, DIRECT, n, obj):
     d = DIRECT - 1
     return _take(a, _const_index(a.shape[d], n), d)              # constant_shift.m:21-29
+
+
+def _ghost_slice(a, d, n):
+    sl = [slice(None)] * a.ndim
+    N, m = a.shape[d], abs(n)
+    sl[d] = slice(0, m) if n < 0 else slice(N - m, N)
+    return tuple(sl)
+
+
+def _flip_shift(a, DIRECT, n, obj):
+    """flip_shift.m:22-40: the constant shift with its ghosts negated for the component along DIRECT."""
+    result = _constant_shift(a, DIRECT, n, obj)
+    if obj.component == DIRECT:
+        g = _ghost_slice(result, DIRECT - 1, n)
+        result[g] = -result[g]
+    return result
+
+
+def _zero_shift(a, DIRECT, n, obj):
+    """zero_shift.m:14-46: a FluxArray's ghosts are 0, except that fluxl keeps the constant shift for
+    n < 0 and fluxr for n > 0; any other array takes the constant shift."""
+    result = _constant_shift(a, DIRECT, n, obj)
+    if obj.flux_type is None or obj.flux_type == (FLUXL if n < 0 else FLUXR):
+        return result
+    result[_ghost_slice(result, DIRECT - 1, n)] = 0.0
+    return result
+
+
+def _linear_shift(a, DIRECT, n, obj):
+    """linear_shift.m:20 indexes with the variable `dim`, which the function never defines: the
+    reference stops with an undefined-variable error at the first shift."""
+    raise NameError("linear_shift.m: undefined function or variable 'dim'")
+
+
+def _wormhole_shift(a, DIRECT, n, obj):
+    """wormhole_shift.m:16-61: for n < 0 the first |n| ghosts along DIRECT are the first |n| cells in
+    reverse order along DIRECT and along nextDir = [2 3 1](DIRECT), negated for the component along
+    DIRECT; for n > 0 the constant shift."""
+    result = _constant_shift(a, DIRECT, n, obj)
+    if n > 0:
+        return result
+    d, m = DIRECT - 1, abs(n)
+    dn = (d + 1) % 3                       # nextDir(DIRECT) - 1
+    sl = [slice(None)] * 3
+    sl[d] = slice(0, m)
+    temp = a[tuple(sl)]
+    temp = np.flip(np.flip(temp, axis=d), axis=dn)
+    result[tuple(sl)] = (-1.0 if obj.component == DIRECT else 1.0) * temp
+    return result
 
 
 def _mirror_shift(a, DIRECT, n, obj):
@@ -378,10 +432,10 @@ class FluidVar:
     def __init__(self, sim, component, bc_class, data):
         self.prim = IArray(sim, component, bc_class, data)
         self.store = IArray(sim, component, bc_class)
-        self.store_fluxR = IArray(sim, component, bc_class)
-        self.store_fluxL = IArray(sim, component, bc_class)
-        self.fluxR = IArray(sim, component, bc_class)
-        self.fluxL = IArray(sim, component, bc_class)
+        self.store_fluxR = IArray(sim, component, bc_class, flux_type=FLUXR)   # StorageArray.m:69-70
+        self.store_fluxL = IArray(sim, component, bc_class, flux_type=FLUXL)
+        self.fluxR = IArray(sim, component, bc_class, flux_type=FLUXR)         # FluidArray.m:104-105
+        self.fluxL = IArray(sim, component, bc_class, flux_type=FLUXL)
         self.w = None
         self.store_w = None
 
@@ -395,8 +449,10 @@ class MagComp:
         for X in (1, 2, 3):
             if X == component:
                 continue
-            for tab in (self.velGrid, self.store, self.store_fluxR, self.wMag, self.flux):
+            for tab in (self.velGrid, self.store, self.wMag):
                 tab[X] = IArray(sim, component, "mag")
+            self.store_fluxR[X] = IArray(sim, component, "mag", flux_type=FLUXR)   # StorageArray.m:70
+            self.flux[X] = IArray(sim, component, "mag", flux_type=FLUX)           # MagnetArray.m:96
         self.cellMag = IArray(sim, component, "mag")
         self.update_cell_centered()
 
@@ -423,6 +479,10 @@ def validate_bc(grid, ndims, bc, bc_infinity):
                     raise ValueError(f"mirror BC on dim {d + 1} of extent {grid[d]}")
                 if mode == FADE and grid[d] < max(20, bc_infinity):
                     raise ValueError(f"fade BC on dim {d + 1} of extent {grid[d]} < max(20, bcInfinity)")
+                if mode == LINEAR:
+                    raise ValueError("linear BC: linear_shift.m:20 uses the undefined variable 'dim'")
+                if mode == WORMHOLE and s == 0 and ndims < 3:
+                    raise ValueError("wormhole BC on a 2-D grid: wormhole_shift.m:27-33 indexes a third dimension")
 
 
 class Sim:

@@ -119,3 +119,16 @@ def test_config_defaults_match_the_reference_constructors():
     _lib.lib().img_config_default(ctypes.byref(c))
     assert (c.viscosity_type, c.visc_linear, c.visc_quadratic) == (0, 0.0, 0.0)
     assert (c.radiation_type, c.rad_exponent, c.rad_initial_maximum) == (0, 0.5, 0.0)
+
+
+def test_create_rejects_the_boundaries_the_reference_cannot_run():
+    """linear_shift.m uses an undefined variable; wormhole_shift.m needs a third dimension; a lower
+    wormhole side couples pencils across the grid and is not on this path."""
+    L = _lib.lib()
+    for kw, word in [(dict(grid=(32, 16, 1), bc="linear"), b"linear"),
+                     (dict(grid=(32, 16, 1), bc={"x": ("wormhole", "const"), "y": "circ"}), b"wormhole"),
+                     (dict(grid=(16, 16, 16), bc={"x": "circ", "y": ("wormhole", "const"), "z": "circ"}), b"wormhole")]:
+        c = make_config(**kw)
+        h = ctypes.c_void_p()
+        assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -4, kw
+        assert word in L.img_last_error(None), kw

@@ -12,7 +12,8 @@ from tests.parity import errors, errors_vector, make_pair, smooth_state
 
 pytestmark = pytest.mark.gpu
 
-BCS = ["circ", "const", "mirror", "trans", "wall", "fade"]
+# every mode the path takes; a (lower, upper) pair sets different modes on the two sides
+BCS = ["circ", "const", "mirror", "trans", "wall", "fade", "flip", "zero", ("const", "wormhole"), ("zero", "flip")]
 
 
 def _bc_settings(bc, grid):

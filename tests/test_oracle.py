@@ -78,7 +78,7 @@ def test_sweep_order_changes_two_dimensional_results(monkeypatch):
     assert rel > 1e-8, rel
 
 
-@pytest.mark.parametrize("bc", ["circ", "const", "mirror", "trans", "wall", "fade"])
+@pytest.mark.parametrize("bc", ["circ", "const", "mirror", "trans", "wall", "fade", "flip", "zero"])
 @pytest.mark.parametrize("grid,mhd", [((30, 1, 1), False), ((24, 22, 1), True), ((21, 20, 20), True)])
 def test_numpy_and_cpp_oracles_bitwise(bc, grid, mhd):
     spec = {f: (bc if not ((bc == "mirror" and grid[d] < 2) or (bc == "fade" and grid[d] < 20)) else "circ")
@@ -281,3 +281,48 @@ def test_viscosity_and_radiation_change_the_result():
         assert d > 1e-8, (key, d)
     # the radiation sink removes energy
     assert out["rad"]["ener"].sum() < out["none"]["ener"].sum()
+
+
+@pytest.mark.parametrize("bc", [("wormhole", "const"), ("const", "wormhole"), ("wormhole", "wormhole")])
+def test_wormhole_oracles_bitwise(bc):
+    """wormhole_shift.m: the lower ghosts come from the pencil mirrored along nextDir (3-D only)."""
+    grid = (12, 10, 8)
+    s = dict(grid=grid, dgrid=tuple(1 / g for g in grid), gamma=5 / 3, cfl=0.35, bc={f: bc for f in "xyz"},
+             magnet=True, iter_max=4)
+    kw = problems.oracle_kwargs(s)
+    st = smooth_state(grid, seed=4, mhd=True)
+    a = np_oracle.Sim(**kw)
+    a.set_state(*st)
+    b = cpp_oracle.Sim(**kw)
+    b.set_state(*st)
+    a.run()
+    b.run()
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+
+
+def test_flip_zero_wormhole_shift_semantics():
+    """The ghost rules of flip_shift.m, zero_shift.m and wormhole_shift.m on a small array."""
+    grid = (4, 3, 2)
+    sim = np_oracle.Sim(grid, (1.0,) * 3, bc="circ")
+    a = np.arange(24, dtype=float).reshape(grid) + 1
+    vec = np_oracle.IArray(sim, 1, "mom", a)
+    fr = np_oracle.IArray(sim, 1, "mom", a, flux_type=np_oracle.FLUXR)
+    fl = np_oracle.IArray(sim, 2, "mom", a, flux_type=np_oracle.FLUXL)
+    ff = np_oracle.IArray(sim, 2, "mom", a, flux_type=np_oracle.FLUX)
+    f = np_oracle._flip_shift(a, 1, -1, vec)
+    assert np.array_equal(f[0], -a[0]) and np.array_equal(f[1:], a[:-1])
+    assert np.array_equal(np_oracle._flip_shift(a, 2, 1, vec)[:, -1], a[:, -1])   # component 1 != 2: no flip
+    assert np.array_equal(np_oracle._zero_shift(a, 1, -1, fr)[0], np.zeros((3, 2)))
+    assert np.array_equal(np_oracle._zero_shift(a, 1, 1, fr)[-1], a[-1])           # fluxr keeps its upper ghost
+    assert np.array_equal(np_oracle._zero_shift(a, 1, -1, fl)[0], a[0])            # fluxl keeps its lower ghost
+    assert np.array_equal(np_oracle._zero_shift(a, 1, 1, fl)[-1], np.zeros((3, 2)))
+    assert np.array_equal(np_oracle._zero_shift(a, 1, 1, ff)[-1], np.zeros((3, 2)))
+    assert np.array_equal(np_oracle._zero_shift(a, 1, -1, vec)[0], a[0])           # not a FluxArray
+    w = np_oracle._wormhole_shift(a, 1, -1, vec)                                     # nextDir(1) = 2 (y)
+    assert np.array_equal(w[0], -a[0, ::-1, :]) and np.array_equal(w[1:], a[:-1])
+    w2 = np_oracle._wormhole_shift(a, 2, -2, fl)                                     # nextDir(2) = 3 (z); component 2
+    assert np.array_equal(w2[:, 0, :], -a[:, 1, ::-1]) and np.array_equal(w2[:, 1, :], -a[:, 0, ::-1])
+    with pytest.raises(NameError):
+        np_oracle._linear_shift(a, 1, 1, vec)
