@@ -26,7 +26,7 @@ SYMBOLS = (
     "img_get_time", "img_set_time", "img_progress", "img_checkpoint_bytes", "img_checkpoint_save",
     "img_checkpoint_load", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count", "img_sweep_order",
-    "img_source", "img_radiation_strength",
+    "img_source", "img_radiation_strength", "img_treadmill", "img_treadmill_history",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -55,6 +55,7 @@ class ImgConfig(ctypes.Structure):
         ("radiation_type", ctypes.c_int),
         ("rad_exponent", ctypes.c_double),
         ("rad_initial_maximum", ctypes.c_double),
+        ("treadmill", ctypes.c_int),
     ]
 
 
@@ -127,6 +128,10 @@ def lib():
     L.img_source.restype = ctypes.c_int
     L.img_radiation_strength.argtypes = [vp, dp]
     L.img_radiation_strength.restype = ctypes.c_int
+    L.img_treadmill.argtypes = [vp]
+    L.img_treadmill.restype = ctypes.c_int
+    L.img_treadmill_history.argtypes = [vp, ip, ctypes.c_int, ip, ip]
+    L.img_treadmill_history.restype = ctypes.c_int
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]
     L.img_batch_add.argtypes = [vp, vp]

@@ -47,7 +47,8 @@ constexpr int OBJ_PRIM_MASS = 20;
 constexpr int OBJ_PRIM_MOM = 21;
 constexpr int OBJ_PRIM_MAG = 24;
 constexpr int OBJ_MAG = 27;
-constexpr int NOBJ = 27 + 36;
+constexpr int OBJ_PRIM_ENER = 27 + 36;   // the energy primary: its edges serve only treadmillGrid's shift
+constexpr int NOBJ = 27 + 36 + 1;
 enum FluidObj { FO_STORE_R = 0, FO_STORE_L = 1, FO_R = 2, FO_L = 3 };
 enum MagObj { MO_VELGRID = 0, MO_STORE_R = 1, MO_WMAG = 2, MO_FLUX = 3 };
 __host__ __device__ constexpr int fluid_obj(int v, int k) { return OBJ_FLUID + v * 4 + k; }
@@ -77,6 +78,10 @@ struct DevTime {
     unsigned int pad2;
     double rad_strength;             // Radiation.strength (set by Radiation.initialize at set_state)
     unsigned long long rad_minbits;  // ordered bits of the running minimum of Radiation.initialize
+    int tread_last;                  // TreadmillManager.last (-1 until the first treadmillGrid call)
+    int tread_dc;                    // dCells of the current call
+    int tread_go;                    // the current call shifts the grid
+    int tread_count;                 // entries in TreadmillManager.history
 };
 
 // ---- batched launches -----------------------------------------------------------------------------

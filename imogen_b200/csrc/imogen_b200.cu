@@ -24,6 +24,7 @@
 
 #include "../../include/imogen_b200.h"
 #include "cfl.cuh"
+#include "treadmill.cuh"
 
 using namespace img;
 
@@ -158,6 +159,9 @@ struct img_ctx {
     EdgeTable edges_host{};
     double* fade_dev = nullptr;
     double* partial = nullptr;  // totals partials
+    int* tread_idx = nullptr;       // treadmill: per-pencil maximum index, first means, history
+    double* tread_means = nullptr;
+    int* tread_hist = nullptr;
     double* stage = nullptr;    // mixed form: FP64 staging buffer of one array for host transfers
     std::vector<double> fade_host;
     int use_b[3] = {1, 1, 1};
@@ -222,6 +226,7 @@ bool active_lin(const img_config& c, int ndims, int cls, int DIRECT) {
 bool stateful(int m) { return m == IMG_BC_TRANS || m == IMG_BC_WALL; }
 
 int obj_class(int o) {
+    if (o == OBJ_PRIM_ENER) return CLS_ENER;
     if (o < OBJ_PRIM_MASS) {
         const int cls_of[5] = {CLS_MASS, CLS_MOM, CLS_MOM, CLS_MOM, CLS_ENER};
         return cls_of[(o - OBJ_FLUID) / 4];
@@ -232,6 +237,7 @@ int obj_class(int o) {
 }
 
 bool obj_used(const img_config& c, int o) {
+    if (o == OBJ_PRIM_ENER) return c.treadmill > 0;   // only treadmillGrid shifts the energy primary
     if (o < OBJ_PRIM_MASS) return c.fluid_active != 0;
     if (o < OBJ_MAG) return true;
     int r = (o - OBJ_MAG) / 4;
@@ -276,6 +282,7 @@ std::vector<double> fade_coefficients(int f) {
 // Dynamic shared memory per CTA the pencil kernels may use (the opt-in 227 KB, less a margin for
 // their static shared memory).
 constexpr size_t kPencilSmemLimit = 210 * 1024;
+constexpr int kTreadHistCap = 1 << 16;   // treadmill history entries kept on the device
 
 bool tiling_fits(const PencilCfg& p, size_t elem) {
     return (elem == 8 ? fluid_smem_bytes<double>(p.G * p.cpt, p.Wb) : fluid_smem_bytes<float>(p.G * p.cpt, p.Wb)) <=
@@ -829,6 +836,10 @@ int set_kernel_attributes(img_ctx* ctx) {
                 CK(chain_attributes<T>(cpt, optin));
             }
             CK(fluid_seg_attributes<T>(optin));
+            CK(cudaFuncSetAttribute(treadmill_detect_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kPencilSmemLimit));
+            CK(cudaFuncSetAttribute(treadmill_shift_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kPencilSmemLimit));
             dn = true;
         }
     }
@@ -855,6 +866,64 @@ int magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
     return ctx->elem == 8 ? launch_magnet<double>(ctx, X, I1, I2) : launch_magnet<float>(ctx, X, I1, I2);
 }
 int cfl_reduce(img_ctx* ctx) { return ctx->elem == 8 ? launch_cfl_reduce<double>(ctx) : launch_cfl_reduce<float>(ctx); }
+
+// treadmillGrid (treadmill/treadmillGrid.m:14-37): nothing when off or before iteration 10
+// (run.time.iteration, known to the host); otherwise the three treadmill kernels.
+template <typename T>
+int launch_treadmill(img_ctx* ctx) {
+    const img_config& c = ctx->cfg;
+    if (c.treadmill <= 0 || ctx->iteration < 10) return IMG_OK;
+    if (ctx->rec) return fail(ctx, IMG_ERR_UNSUPPORTED, "treadmill in a batched launch");
+    const int X = c.treadmill, d = X - 1;
+    const Geom& g = ctx->g;
+    TreadArgs a{};
+    a.g = g;
+    a.d = d;
+    a.d1 = d == 0 ? 1 : 0;
+    a.d2 = d == 2 ? 1 : 2;
+    a.n1 = g.n[a.d1];
+    a.n2 = g.n[a.d2];
+    a.sd = g.s[d];
+    a.s1 = g.s[a.d1];
+    a.s2 = g.s[a.d2];
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    a.tm = ctx->tm;
+    a.dx = c.dgrid[d];
+    const int cls[TREAD_ARRAYS] = {CLS_MASS, CLS_MOM, CLS_MOM, CLS_MOM, CLS_ENER, CLS_MAG, CLS_MAG, CLS_MAG};
+    const int comp[TREAD_ARRAYS] = {0, 1, 2, 3, 0, 1, 2, 3};
+    const int obj[TREAD_ARRAYS] = {OBJ_PRIM_MASS, OBJ_PRIM_MOM, OBJ_PRIM_MOM + 1, OBJ_PRIM_MOM + 2, OBJ_PRIM_ENER,
+                                   OBJ_PRIM_MAG, OBJ_PRIM_MAG + 1, OBJ_PRIM_MAG + 2};
+    for (int k = 0; k < TREAD_ARRAYS; ++k) {
+        for (int s = 0; s < 2; ++s) {
+            a.mode[k][s] = c.bc_modes[cls[k]][s][d];
+            a.edge[k][s] = d < g.ndims ? ctx->edges_host.p[obj[k]][d][s] : nullptr;
+        }
+        a.neg[k] = comp[k] == X;
+        a.act[k] = active_lin(c, g.ndims, cls[k], X);
+    }
+    a.fade = ctx->fade_dev;
+    a.fade_f = c.bc_infinity;
+    a.bc_inf = c.bc_infinity;
+    a.idx = ctx->tread_idx;
+    a.means = ctx->tread_means;
+    a.hist = ctx->tread_hist;
+    a.hist_cap = kTreadHistCap;
+    const long long ncol = g.ncell / g.n[d];
+    const size_t smem = tread_smem_bytes(g.n[d], sizeof(T));
+    if (d >= g.ndims) {   // ImogenArray.shift is not enabled along a third dimension of a 2-D grid
+        for (int k = 0; k < TREAD_ARRAYS; ++k) a.mode[k][0] = a.mode[k][1] = IMG_BC_CONST;
+    }
+    treadmill_detect_kernel<T><<<(unsigned)ncol, 256, smem, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    treadmill_finalize_kernel<<<1, 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    treadmill_shift_kernel<T><<<dim3((unsigned)ncol, TREAD_ARRAYS), 256, smem, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    ctx->launches += 3;
+    return IMG_OK;
+}
+
+int treadmill_grid(img_ctx* ctx) { return ctx->elem == 8 ? launch_treadmill<double>(ctx) : launch_treadmill<float>(ctx); }
 
 // source(run, ...) of source.m:1-36 for this path: the radiation sink (source.m:30); nothing
 // without radiation.  accumulate: the same pass collects the CFL maxima of the new state for the
@@ -928,21 +997,26 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
 // One iteration (imogen.m:60-66): time.update(1), flux(+1), time.update(2), flux(-1).
 // With radiation each timestep ends with source.m's sink (imogen.m:63-67), whose pass also collects
 // the CFL maxima that the next TimeManager.update reads (instead of the last fluid sweep).
+// The treadmill (imogen.m:64) moves the state after each flux, so with one the last fluid sweep
+// collects no CFL maxima either.
 int enqueue_iteration(img_ctx* ctx) {
     int rc;
     const bool per_iter = ctx->cfg.update_mode != 0;
     const bool rad = ctx->cfg.radiation_type != IMG_RAD_NONE;
+    const bool tread = ctx->cfg.treadmill > 0;
     const bool fl = ctx->cfg.fluid_active != 0;
     if ((rc = time_update_async(ctx, 1)) != IMG_OK) return rc;
     if ((rc = do_flux(ctx, 1, false)) != IMG_OK) return rc;
+    if ((rc = treadmill_grid(ctx)) != IMG_OK) return rc;
     if (rad) {
         if ((rc = source_sink(ctx, !per_iter && fl)) != IMG_OK) return rc;
         ctx->cfl_valid = !per_iter && fl;
     }
     if ((rc = time_update_async(ctx, 2)) != IMG_OK) return rc;
-    if ((rc = do_flux(ctx, -1, per_iter && !rad)) != IMG_OK) return rc;
+    if ((rc = do_flux(ctx, -1, per_iter && !rad && !tread)) != IMG_OK) return rc;
+    if ((rc = treadmill_grid(ctx)) != IMG_OK) return rc;
     if (rad && (rc = source_sink(ctx, per_iter && fl)) != IMG_OK) return rc;
-    ctx->cfl_valid = per_iter && fl;
+    ctx->cfl_valid = per_iter && fl && (rad || !tread);
     return IMG_OK;
 }
 
@@ -971,6 +1045,12 @@ int validate(const img_config& c, std::string& why) {
         return IMG_ERR_ARG;
     }
     if (c.radiation_type < IMG_RAD_NONE || c.radiation_type > IMG_RAD_OPTICALLY_THIN) { why = "unknown radiation type"; return IMG_ERR_ARG; }
+    if (c.treadmill < 0 || c.treadmill > 3) { why = "treadmill direction must be 0 (off) or 1-3"; return IMG_ERR_ARG; }
+    if (c.treadmill > 0 &&
+        tread_smem_bytes(c.grid[c.treadmill - 1], c.precision == IMG_PREC_FP64 ? 8 : 4) > kPencilSmemLimit) {
+        why = "treadmill: the pencils along its direction do not fit one thread block's shared memory";
+        return IMG_ERR_UNSUPPORTED;
+    }
     if (c.viscosity_type != IMG_VISC_NONE)   // the segment kernel's ends (seg_fluid.cuh)
         for (int d = 0; d < 3; ++d) {
             if (c.grid[d] < 3) continue;
@@ -1014,7 +1094,7 @@ int validate(const img_config& c, std::string& why) {
 
 // Device bytes: state + scratch + edges + tables.
 struct Layout {
-    size_t state, scratch, tm, table, fade, partial, stage, edges, total;
+    size_t state, scratch, tm, table, fade, partial, stage, tread, edges, total;
     size_t edge_off[NOBJ][3][2];
 };
 
@@ -1030,6 +1110,10 @@ Layout plan(const img_config& c) {
     L.fade = align256(sizeof(double) * std::max(1, c.bc_infinity));
     L.partial = align256(sizeof(double) * 2 * 8 * 1024);
     L.stage = elem == 4 ? align256(n * sizeof(double)) : 0;   // FP64 staging of host transfers (mixed)
+    if (c.treadmill > 0) {   // per-pencil indices, first means, history
+        const long long ncol = n / c.grid[c.treadmill - 1];
+        L.tread = align256(sizeof(int) * ncol) + align256(sizeof(double) * ncol) + align256(sizeof(int) * kTreadHistCap);
+    }
     int ndims = c.grid[2] > 1 ? 3 : 2;
     size_t off = 0;
     for (int o = 0; o < NOBJ; ++o)
@@ -1042,7 +1126,7 @@ Layout plan(const img_config& c) {
                 off += align256(sizeof(double) * (n / c.grid[e]));
             }
     L.edges = off;
-    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.edges;
+    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.tread + L.edges;
     return L;
 }
 
@@ -1190,6 +1274,13 @@ int img_create(img_ctx** out, const img_config* cfg) {
     p += L.partial;
     ctx->stage = L.stage ? reinterpret_cast<double*>(p) : nullptr;
     p += L.stage;
+    if (L.tread) {
+        const long long ncol = g.ncell / g.n[cfg->treadmill - 1];
+        ctx->tread_idx = reinterpret_cast<int*>(p);
+        ctx->tread_means = reinterpret_cast<double*>(p + align256(sizeof(int) * ncol));
+        ctx->tread_hist = reinterpret_cast<int*>(p + align256(sizeof(int) * ncol) + align256(sizeof(double) * ncol));
+    }
+    p += L.tread;
     char* edge_base = p;
     for (int o = 0; o < NOBJ; ++o)
         for (int e = 0; e < 3; ++e)
@@ -1210,6 +1301,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
     for (int d = 0; d < 3; ++d) t.dgrid[d] = cfg->dgrid[d];
     t.update_mode = cfg->update_mode;
     t.rad_minbits = 0xfff0000000000000ull;   // ordered bits of +inf (rad_init_kernel)
+    t.tread_last = -1;                       // TreadmillManager.last
     *ctx->host_tm = t;
     if (cudaMemcpyAsync(ctx->fade_dev, ctx->fade_host.data(), sizeof(double) * ctx->fade_host.size(), cudaMemcpyHostToDevice,
                         ctx->stream) != cudaSuccess ||
@@ -1415,15 +1507,15 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
         if ((rc = img_upload(ctx, IMG_VAR_MAGX + c, mag + c * n, n)) != IMG_OK) return rc;
     // primary stored edges from the initial condition (Edges.m:37-110 at FluidArray/MagnetArray creation)
     std::vector<double> face;
-    const double* prim[7] = {mass, mom, mom + n, mom + 2 * n, mag, mag + n, mag + 2 * n};
-    const int pobj[7] = {OBJ_PRIM_MASS, OBJ_PRIM_MOM, OBJ_PRIM_MOM + 1, OBJ_PRIM_MOM + 2, OBJ_PRIM_MAG, OBJ_PRIM_MAG + 1,
-                         OBJ_PRIM_MAG + 2};
-    for (int k = 0; k < 7; ++k)
+    const double* prim8[8] = {mass, mom, mom + n, mom + 2 * n, mag, mag + n, mag + 2 * n, ener};
+    const int pobj[8] = {OBJ_PRIM_MASS, OBJ_PRIM_MOM, OBJ_PRIM_MOM + 1, OBJ_PRIM_MOM + 2, OBJ_PRIM_MAG, OBJ_PRIM_MAG + 1,
+                         OBJ_PRIM_MAG + 2, OBJ_PRIM_ENER};
+    for (int k = 0; k < 8; ++k)
         for (int e = 0; e < ctx->g.ndims; ++e)
             for (int s = 0; s < 2; ++s) {
                 double* dst = ctx->edges_host.p[pobj[k]][e][s];
                 if (!dst) continue;
-                host_face(ctx->g, prim[k], e, s == 0 ? 0 : ctx->g.n[e] - 1, face);
+                host_face(ctx->g, prim8[k], e, s == 0 ? 0 : ctx->g.n[e] - 1, face);
                 CK(cudaMemcpyAsync(dst, face.data(), face.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
                 CK(cudaStreamSynchronize(ctx->stream));
             }
@@ -1480,6 +1572,29 @@ int img_source(img_ctx* ctx) {
     return source_sink(ctx, false);
 }
 
+int img_treadmill(img_ctx* ctx) {
+    if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    if (ctx->cfg.treadmill <= 0) return IMG_OK;
+    ctx->cfl_valid = false;
+    return treadmill_grid(ctx);
+}
+
+int img_treadmill_history(img_ctx* ctx, int* out, int cap, int* count, int* last) {
+    if (!ctx || (cap > 0 && !out)) return fail(ctx, IMG_ERR_ARG, "null argument");
+    CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const int n = ctx->host_tm->tread_count;
+    const int k = std::min(std::min(cap, n), kTreadHistCap);
+    if (k > 0) {
+        CK(cudaMemcpyAsync(out, ctx->tread_hist, sizeof(int) * k, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    if (count) *count = n;
+    if (last) *last = ctx->host_tm->tread_last;
+    return IMG_OK;
+}
+
 int img_radiation_strength(img_ctx* ctx, double* strength) {
     if (!ctx || !strength) return fail(ctx, IMG_ERR_ARG, "null argument");
     CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1508,6 +1623,7 @@ int img_magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
 // Whether the next iteration's launch sequence is the steady one a graph can replay: every
 // InitializedArray has had its first assignment (no edge-capture flags left in the arguments).
 static bool steady(const img_ctx* ctx) {
+    if (ctx->cfg.treadmill > 0) return false;   // treadmillGrid depends on the host iteration count
     if (ctx->init_store || ctx->init_flux) return !ctx->cfg.fluid_active;
     for (int c = 0; c < 3; ++c)
         for (int X = 0; X < 3; ++X)
@@ -1984,8 +2100,8 @@ int img_batch_add(img_batch* b, img_ctx* ctx) {
     if (!ctx->state_set) return bfail(b, IMG_ERR_STATE, "member state not set");
     if (ctx->batch) return bfail(b, IMG_ERR_STATE, "context is already a batch member");
     if (ctx->dev != b->dev) return bfail(b, IMG_ERR_ARG, "member is on device %d, batch on %d", ctx->dev, b->dev);
-    if (ctx->cfg.viscosity_type != IMG_VISC_NONE || ctx->cfg.radiation_type != IMG_RAD_NONE)
-        return bfail(b, IMG_ERR_UNSUPPORTED, "contexts with artificial viscosity or radiation do not join batches");
+    if (ctx->cfg.viscosity_type != IMG_VISC_NONE || ctx->cfg.radiation_type != IMG_RAD_NONE || ctx->cfg.treadmill > 0)
+        return bfail(b, IMG_ERR_UNSUPPORTED, "contexts with artificial viscosity, radiation or a treadmill do not join batches");
     if (!b->members.empty() && !same_signature(b->members[0], ctx))
         return bfail(b, IMG_ERR_ARG, "member differs from the batch in precision, physics, swept dimensions, "
                      "time update mode or iteration");

@@ -64,7 +64,7 @@ def bc_table(bc):
 def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ", bc_infinity=20,
                 limiter="vanleer", fluid=True, magnet=False, time_max=1e5, iter_max=10,
                 update_mode=1, precision="fp64", nonfinite_check=True, viscosity="empty", visc_linear=0.0,
-                visc_quadratic=0.0, radiation="empty", rad_exponent=0.5, rad_initial_maximum=0.0):
+                visc_quadratic=0.0, radiation="empty", rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
     """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults; run.viscosity
     and run.radiation as fluid/ArtificialViscosity.m:31-37 and fluid/Radiation.m:32-37 hold them)."""
     c = ImgConfig()
@@ -102,6 +102,7 @@ def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ"
     c.radiation_type = RADIATIONS[radiation] if isinstance(radiation, str) else int(radiation)
     c.rad_exponent = float(rad_exponent)
     c.rad_initial_maximum = float(rad_initial_maximum)
+    c.treadmill = int(treadmill)
     return c
 
 
@@ -253,6 +254,20 @@ class ImogenRun:
     def source(self):
         """source.m for this path: the radiation sink E -= dTime * radiation.solve (source.m:30)."""
         check(lib().img_source(self._h), self._h)
+
+    def treadmill(self):
+        """treadmillGrid (treadmill/treadmillGrid.m) at the current iteration (iterate calls it after
+        each flux)."""
+        check(lib().img_treadmill(self._h), self._h)
+
+    @property
+    def treadmill_history(self):
+        """(TreadmillManager.history as a list, TreadmillManager.last)."""
+        n, last = ctypes.c_int(), ctypes.c_int()
+        check(lib().img_treadmill_history(self._h, None, 0, ctypes.byref(n), ctypes.byref(last)), self._h)
+        out = (ctypes.c_int * max(n.value, 1))()
+        check(lib().img_treadmill_history(self._h, out, n.value, None, None), self._h)
+        return list(out[:min(n.value, 1 << 16)]), last.value
 
     @property
     def radiation_strength(self):

@@ -88,6 +88,11 @@ typedef struct img_config {
     int radiation_type;
     double rad_exponent;
     double rad_initial_maximum;
+    /* ini.treadmill (initialize.m:328-331): 0 off, else the direction (1-3) along which treadmillGrid
+     * keeps the steepest density rise in place (treadmill/treadmillGrid.m).  Pencils along it are
+     * staged whole in shared memory (2 N values must fit one block); contexts with a treadmill take no
+     * CUDA graph and do not join batches. */
+    int treadmill;
 } img_config;
 
 typedef struct img_ctx img_ctx;
@@ -133,6 +138,14 @@ int img_sweep_order(int order, int iteration, int out[3]);
 /* source(run, mass, mom, ener, mag, grav) (source.m:1-36) for this path: the radiation sink
  * E = E - dTime * radiation.solve (source.m:30), nothing without radiation.  Gravity is out of scope. */
 int img_source(img_ctx* ctx);
+
+/* treadmillGrid(run, mass, mom, ener, mag) (treadmill/treadmillGrid.m:1) at the current iteration;
+ * nothing when the treadmill is off or before iteration 10.  img_step calls it after each flux. */
+int img_treadmill(img_ctx* ctx);
+
+/* TreadmillManager.history (treadmill/TreadmillManager.m:50-56) and .last: copies min(cap, count)
+ * entries, *count = the number recorded (the device keeps the first 65536), synchronises. */
+int img_treadmill_history(img_ctx* ctx, int* out, int cap, int* count, int* last);
 
 /* Radiation.strength (fluid/Radiation.m:71-72; 0 without radiation), synchronises. */
 int img_radiation_strength(img_ctx* ctx, double* strength);

@@ -47,6 +47,12 @@ def lib():
         L.orc_magnet_flux.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_iterate.argtypes = [ctypes.c_void_p]
         L.orc_source.argtypes = [ctypes.c_void_p]
+        L.orc_treadmill.argtypes = [ctypes.c_void_p]
+        L.orc_set_treadmill.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_treadmill_history.argtypes = [ctypes.c_void_p, ip, ctypes.c_int]
+        L.orc_treadmill_history.restype = ctypes.c_int
+        L.orc_treadmill_last.argtypes = [ctypes.c_void_p]
+        L.orc_treadmill_last.restype = ctypes.c_int
         L.orc_radiation_strength.argtypes = [ctypes.c_void_p]
         L.orc_radiation_strength.restype = ctypes.c_double
         L.orc_get_time.argtypes = [ctypes.c_void_p, dp, dp, ip]
@@ -114,7 +120,7 @@ class Sim:
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
                  magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
                  viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
-                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0):
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
         self.grid = tuple(int(g) for g in grid)
         g = np.array(self.grid, dtype=np.int32)
         dg = np.array(dgrid, dtype=float)
@@ -128,6 +134,7 @@ class Sim:
         lib().orc_set_physics(self._h, {VISC_NONE: 0, VISC_NR: 1, VISC_CSW: 2}[viscosity], float(visc_linear),
                               float(visc_quadratic), {RAD_NONE: 0, RAD_THIN: 1}[radiation], float(rad_exponent),
                               float(rad_initial_maximum))
+        lib().orc_set_treadmill(self._h, int(treadmill))
         self.TIMEMAX = float(time_max)
         self.ITERMAX = int(iter_max)
 
@@ -171,6 +178,21 @@ class Sim:
     def source(self):
         """source.m:30: the radiation sink with the current dTime."""
         lib().orc_source(self._h)
+
+    def treadmill(self):
+        """treadmillGrid (treadmill/treadmillGrid.m:14-37)."""
+        lib().orc_treadmill(self._h)
+
+    @property
+    def treadmill_history(self):
+        n = lib().orc_treadmill_history(self._h, None, 0)
+        out = (ctypes.c_int * max(n, 1))()
+        lib().orc_treadmill_history(self._h, out, n)
+        return list(out[:n])
+
+    @property
+    def treadmill_last(self):
+        return lib().orc_treadmill_last(self._h)
 
     @property
     def rad_strength(self):

@@ -134,6 +134,10 @@ struct Sim {
     double visc_lin = 0, visc_quad = 0;
     int rad_type = 0;
     double rad_exp = 0.5, rad_initmax = 0, rad_strength = 1;
+    // TreadmillManager (treadmill/TreadmillManager.m): direction (0 inactive), last, history
+    int treadmill_dir = 0;
+    int treadmill_last = -1;
+    std::vector<int> treadmill_history;
 
     struct FluidVar { IArr prim, store, store_fluxR, store_fluxL, fluxR, fluxL; };
     struct MagComp {
@@ -281,7 +285,7 @@ Vec IArr::shift(int DIRECT, int n) {
     }
 
     if (mode == WALL) {   // wall_shift.m:12-33
-        Vec e = transparent_edge(DIRECT, n > 0);
+        Vec e = transparent_edge(DIRECT, n >= 0);   // n = 0: dir = -sign(0) takes the else (upper) branch
         for (long long f = 0; f < nf; ++f) {
             long long b = base_of(f);
             for (int k = 0; k < m; ++k) {
@@ -315,9 +319,9 @@ Vec IArr::shift(int DIRECT, int n) {
     // TRANS: transparent_shift.m:23-99
     bool act = edges.active[(DIRECT - 1) % 2][(DIRECT - 1) / 2];   // ACTIVE(DIRECT), linear index
     Vec e;
-    if (act) e = transparent_edge(DIRECT, n > 0);
+    if (act) e = transparent_edge(DIRECT, n >= 0);   // n = 0 takes transparent_shift.m's upper branch
     double xk[5] = {1, 2, 3, double(s.bc_inf), double(s.bc_inf + 1)};
-    double xe[2];
+    std::vector<double> xe(m), out(m);   // any shift distance (treadmillGrid shifts by many cells)
     for (int k = 0; k < m; ++k) xe[k] = n < 0 ? 3 + (m - k) : 3 + (k + 1);
     for (long long f = 0; f < nf; ++f) {
         long long b = base_of(f);
@@ -328,8 +332,7 @@ Vec IArr::shift(int DIRECT, int n) {
         }
         y[3] = act ? e[f] : 0.0;
         y[4] = y[3];
-        double out[2];
-        pchip_col(xk, 5, y, xe, m, out);
+        pchip_col(xk, 5, y, xe.data(), m, out.data());
         for (int k = 0; k < m; ++k) {
             int gi = n < 0 ? k : Nd - m + k;
             double orig = a[b + (long long)gi * sd];
@@ -797,10 +800,63 @@ void source(Sim& s) {
     s.fv[4].prim.set(std::move(e));
 }
 
+// treadmillGrid (treadmill/treadmillGrid.m:14-37): from iteration 10 on, newIndex = round(mean(mean(
+// first index of the largest forward difference of rho along DIRECTION, per pencil))); the first call
+// records it as `last`, later calls shift every primary by newIndex - last cells with its own BCs.
+void treadmill(Sim& s) {
+    const int X = s.treadmill_dir;
+    if (X <= 0 || s.iteration < 10) return;
+    const int d = X - 1;
+    IArr& mass = s.fv[0].prim;
+    const Vec sh = mass.shift(X, 1);   // calculate2PtDerivative (ImogenArray.m:190-192)
+    const int d1 = d == 0 ? 1 : 0, d2 = d == 2 ? 1 : 2;
+    const int n1 = s.n[d1], n2 = s.n[d2], Nd = s.n[d];
+    const long long sd = s.stride(d), s1 = s.stride(d1), s2 = s.stride(d2);
+    std::vector<double> idx((size_t)n1 * n2);
+    for (int c2 = 0; c2 < n2; ++c2)
+        for (int c1 = 0; c1 < n1; ++c1) {
+            const long long b = c1 * s1 + c2 * s2;
+            double best = -HUGE_VAL;
+            int bi = 0;
+            for (int i = 0; i < Nd; ++i) {   // max(..., [], X): first maximum, NaN skipped
+                const double v = (sh[b + i * sd] - mass.a[b + i * sd]) / s.dgrid[d];
+                if (v > best) { best = v; bi = i; }
+            }
+            idx[c1 + (size_t)n1 * c2] = bi + 1;
+        }
+    // mean(mean(.)): along the first non-singleton remaining dimension, then along the other
+    std::vector<double> first;
+    if (n1 > 1 && n2 > 1) {
+        for (int c2 = 0; c2 < n2; ++c2) {
+            double t = 0;
+            for (int c1 = 0; c1 < n1; ++c1) t += idx[c1 + (size_t)n1 * c2];
+            first.push_back(t / n1);
+        }
+    } else {
+        first = idx;
+    }
+    double t = 0;
+    for (double v : first) t += v;
+    const int new_index = (int)std::round(t / (double)first.size());
+    if (s.treadmill_last < 0) {
+        s.treadmill_last = new_index;
+        return;
+    }
+    const int dc = new_index - s.treadmill_last;
+    s.fv[0].prim.set(s.fv[0].prim.shift(X, dc));
+    s.fv[4].prim.set(s.fv[4].prim.shift(X, dc));
+    for (int i = 0; i < 3; ++i) {
+        s.fv[1 + i].prim.set(s.fv[1 + i].prim.shift(X, dc));
+        s.mg[i].prim.set(s.mg[i].prim.shift(X, dc));
+    }
+    s.treadmill_history.push_back(dc);
+}
+
 int iterate(Sim& s) {
     for (int i = 1; i <= 2; ++i) {
         if (time_update(s, i) != 0) return -1;
         flux(s, i == 1 ? 1 : -1);
+        treadmill(s);
         source(s);
     }
     s.iteration += 1;
@@ -922,6 +978,14 @@ int orc_relaxing_fluid(void* p, int X) { relaxing_fluid(*static_cast<Sim*>(p), X
 int orc_magnet_flux(void* p, int X, int I1, int I2) { magnet_flux(*static_cast<Sim*>(p), X, I1, I2); return 0; }
 int orc_iterate(void* p) { return iterate(*static_cast<Sim*>(p)); }
 void orc_source(void* p) { source(*static_cast<Sim*>(p)); }
+void orc_treadmill(void* p) { treadmill(*static_cast<Sim*>(p)); }
+void orc_set_treadmill(void* p, int direction) { static_cast<Sim*>(p)->treadmill_dir = direction; }
+int orc_treadmill_history(void* p, int* out, int cap) {
+    const auto& h = static_cast<Sim*>(p)->treadmill_history;
+    for (int i = 0; i < cap && i < (int)h.size(); ++i) out[i] = h[i];
+    return (int)h.size();
+}
+int orc_treadmill_last(void* p) { return static_cast<Sim*>(p)->treadmill_last; }
 double orc_radiation_strength(void* p) { return static_cast<Sim*>(p)->rad_strength; }
 
 int orc_run(void* p, int max_iterations) {

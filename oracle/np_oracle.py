@@ -255,6 +255,37 @@ def _constant_shift(a, DIRECT, n, obj):
     return _take(a, _const_index(a.shape[d], n), d)              # constant_shift.m:21-29
 
 
+def _mean_of_means(idx):
+    """mean(mean(A)) of treadmillGrid.m:22 for the index array of the non-swept dimensions (x
+    fastest): MATLAB's mean runs along the first non-singleton dimension, so the first mean averages
+    along the lower of the two remaining dimensions, the second along the other (each a sum in index
+    order divided by the count)."""
+    a = np.asarray(idx, dtype=float)
+    a = a.reshape([s for s in a.shape if s > 1] or [1])
+    if a.ndim == 2:
+        first = []
+        for k in range(a.shape[1]):
+            s = 0.0
+            for j in range(a.shape[0]):
+                s += a[j, k]
+            first.append(s / a.shape[0])
+        vals = first
+    else:
+        vals = list(a.reshape(-1))
+    s = 0.0
+    for v in vals:
+        s += v
+    return s / len(vals)
+
+
+def _matlab_round(x):
+    """MATLAB round: halves away from zero."""
+    r = math.floor(abs(x))
+    if abs(x) - r >= 0.5:
+        r += 1
+    return int(r) * (1 if x >= 0 else -1)
+
+
 def _ghost_slice(a, d, n):
     sl = [slice(None)] * a.ndim
     N, m = a.shape[d], abs(n)
@@ -495,7 +526,7 @@ class Sim:
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
                  magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
                  viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
-                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0):
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
         self.grid = tuple(int(g) for g in grid)
         self.ndims = 3 if self.grid[2] > 1 else 2
         self.dgrid = tuple(float(v) for v in dgrid)
@@ -528,6 +559,11 @@ class Sim:
         self.rad_exponent = float(rad_exponent)
         self.rad_initial_maximum = float(rad_initial_maximum)
         self.rad_strength = 1.0
+        # TreadmillManager (treadmill/TreadmillManager.m): ini.treadmill > 0 activates it along that
+        # direction (initialize.m:328-331); `last` starts at -1 and the history is kept
+        self.treadmill_dir = int(treadmill)
+        self.treadmill_last = -1
+        self.treadmill_history = []
 
     # imogen.m:30-42
     def set_state(self, mass, mom, ener, mag):
@@ -799,6 +835,30 @@ class Sim:
     def running(self):
         return self.iteration <= self.ITERMAX and self.time < self.TIMEMAX
 
+    def treadmill(self):
+        """treadmillGrid (treadmill/treadmillGrid.m:14-37): after iteration 10, the mean over the
+        pencils along DIRECTION of the (first) index of the largest forward difference of rho picks
+        newIndex; the first call only records it as `last`, later calls shift every primary array
+        by newIndex - last cells with its own boundary conditions."""
+        X = self.treadmill_dir
+        if X <= 0 or self.iteration < 10:
+            return
+        d = X - 1
+        deriv = (self.mass.prim.shift(X, 1) - self.mass.prim.a) / self.dgrid[d]   # calculate2PtDerivative
+        deriv = np.where(np.isnan(deriv), -np.inf, deriv)                         # max ignores NaN
+        idx = np.argmax(deriv, axis=d).astype(float) + 1                           # first maximum, 1-based
+        new_index = _matlab_round(_mean_of_means(idx))
+        if self.treadmill_last < 0:
+            self.treadmill_last = new_index
+            return
+        dc = new_index - self.treadmill_last
+        self.mass.prim.set(self.mass.prim.shift(X, dc))
+        self.ener.prim.set(self.ener.prim.shift(X, dc))
+        for i in range(3):
+            self.mom[i].prim.set(self.mom[i].prim.shift(X, dc))
+            self.mag[i].prim.set(self.mag[i].prim.shift(X, dc))
+        self.treadmill_history.append(dc)
+
     def source(self):
         """source.m:30: ener.array = ener.array - dTime * radiation.solve (the empty solver gives 0;
         gravity is not part of this path)."""
@@ -810,6 +870,7 @@ class Sim:
         for i, direction in ((1, 1), (2, -1)):
             self.time_update(i)
             self.flux(direction)
+            self.treadmill()
             self.source()
         self.iteration += 1
 

@@ -132,3 +132,13 @@ def test_create_rejects_the_boundaries_the_reference_cannot_run():
         h = ctypes.c_void_p()
         assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -4, kw
         assert word in L.img_last_error(None), kw
+
+
+def test_create_checks_the_treadmill_setting():
+    L = _lib.lib()
+    for kw, code in [(dict(grid=(32, 16, 1), treadmill=4), -1),
+                     (dict(grid=(40000, 2, 1), treadmill=1), -4)]:   # 2 x 40000 FP64 values exceed one block
+        c = make_config(**kw)
+        h = ctypes.c_void_p()
+        assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == code, kw
+        assert b"treadmill" in L.img_last_error(None), kw

@@ -326,3 +326,46 @@ def test_flip_zero_wormhole_shift_semantics():
     assert np.array_equal(w2[:, 0, :], -a[:, 1, ::-1]) and np.array_equal(w2[:, 1, :], -a[:, 0, ::-1])
     with pytest.raises(NameError):
         np_oracle._linear_shift(a, 1, 1, vec)
+
+
+def _shock_tube(grid):
+    """A density/pressure jump at x = 0.5 in a flow along x with a guide field (the shock the
+    treadmill follows)."""
+    x = (np.arange(grid[0]) + .5) / grid[0]
+    shape = (grid[0], 1, 1)
+    rho = np.where(x < 0.5, 1.0, 0.25).reshape(shape) * np.ones(grid)
+    mom = np.zeros((3,) + grid)
+    mom[0] = 0.3 * rho
+    P = np.where(x < 0.5, 1.0, 0.2).reshape(shape) * np.ones(grid)
+    mag = np.zeros((3,) + grid)
+    mag[0], mag[1] = 0.2, 0.1
+    ener = P / (2 / 3) + 0.5 * (mom ** 2).sum(0) / rho + 0.5 * (mag ** 2).sum(0)
+    return rho, mom, ener, mag
+
+
+@pytest.mark.parametrize("bc", ["fade", "circ", "const", "trans", "wall", "mirror", "flip"])
+def test_treadmill_oracles_bitwise(bc):
+    grid = (40, 6, 1)
+    s = dict(grid=grid, dgrid=(1 / 40, 1 / 40, 1.0), cfl=0.35, bc={"x": bc, "y": "circ", "z": "circ"}, magnet=True,
+             iter_max=25, treadmill=1)
+    kw = problems.oracle_kwargs(s)
+    a = np_oracle.Sim(**kw)
+    a.set_state(*_shock_tube(grid))
+    b = cpp_oracle.Sim(**kw)
+    b.set_state(*_shock_tube(grid))
+    a.run()
+    b.run()
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    assert a.treadmill_history == b.treadmill_history and a.treadmill_last == b.treadmill_last
+    assert len(a.treadmill_history) == 2 * (25 - 9) - 1      # from iteration 10, the first call sets `last`
+
+
+def test_treadmill_mean_and_round_follow_matlab():
+    # mean(mean(I)) along the first non-singleton dimension, then the other; round halves away from 0
+    idx = np.array([[1, 2], [4, 6], [3, 3]], dtype=float)    # n1 = 3 (fastest), n2 = 2
+    assert np_oracle._mean_of_means(idx) == ((1 + 4 + 3) / 3 + (2 + 6 + 3) / 3) / 2
+    assert np_oracle._mean_of_means(np.array([[5.0, 6.0]])) == 5.5
+    assert np_oracle._matlab_round(2.5) == 3 and np_oracle._matlab_round(-2.5) == -3
+    assert np_oracle._matlab_round(0.49999999999999994) == 0
