@@ -27,6 +27,7 @@ SYMBOLS = (
     "img_checkpoint_load", "img_totals", "img_totals_static", "img_sync", "img_last_error", "img_bytes_required",
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count", "img_sweep_order",
     "img_source", "img_radiation_strength", "img_treadmill", "img_treadmill_history",
+    "img_slice_write", "img_slice_read", "img_slice_last_error", "img_save_slice", "img_load_slice",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -56,6 +57,40 @@ class ImgConfig(ctypes.Structure):
         ("rad_exponent", ctypes.c_double),
         ("rad_initial_maximum", ctypes.c_double),
         ("treadmill", ctypes.c_int),
+    ]
+
+
+class ImgSliceMeta(ctypes.Structure):
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("index", ctypes.c_int * 3),
+        ("suffix", ctypes.c_char_p),
+        ("about", ctypes.c_char_p),
+        ("version", ctypes.c_double),
+        ("wall_max", ctypes.c_double),
+        ("started", ctypes.c_char_p),
+    ]
+
+
+class ImgSliceState(ctypes.Structure):
+    _fields_ = [
+        ("grid", ctypes.c_int * 3),
+        ("dgrid", ctypes.c_double * 3),
+        ("gamma", ctypes.c_double),
+        ("time", ctypes.c_double),
+        ("iteration", ctypes.c_int),
+        ("iter_max", ctypes.c_int),
+        ("time_max", ctypes.c_double),
+        ("dt_history", ctypes.POINTER(ctypes.c_double)),
+        ("n_history", ctypes.c_int),
+        ("magnet_active", ctypes.c_int),
+        ("mass", ctypes.POINTER(ctypes.c_double)),
+        ("mom", ctypes.POINTER(ctypes.c_double)),
+        ("ener", ctypes.POINTER(ctypes.c_double)),
+        ("mag", ctypes.POINTER(ctypes.c_double)),
+        ("treadmill", ctypes.c_int),
+        ("tread_history", ctypes.POINTER(ctypes.c_int)),
+        ("n_tread", ctypes.c_int),
     ]
 
 
@@ -132,6 +167,16 @@ def lib():
     L.img_treadmill.restype = ctypes.c_int
     L.img_treadmill_history.argtypes = [vp, ip, ctypes.c_int, ip, ip]
     L.img_treadmill_history.restype = ctypes.c_int
+    L.img_slice_write.argtypes = [ctypes.c_char_p, ctypes.POINTER(ImgSliceMeta), ctypes.POINTER(ImgSliceState)]
+    L.img_slice_write.restype = ctypes.c_int
+    L.img_slice_read.argtypes = [ctypes.c_char_p, ip, dp, dp, dp, dp, ip]
+    L.img_slice_read.restype = ctypes.c_int
+    L.img_slice_last_error.argtypes = []
+    L.img_slice_last_error.restype = ctypes.c_char_p
+    L.img_save_slice.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(ImgSliceMeta)]
+    L.img_save_slice.restype = ctypes.c_int
+    L.img_load_slice.argtypes = [vp, ctypes.c_char_p]
+    L.img_load_slice.restype = ctypes.c_int
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]
     L.img_batch_add.argtypes = [vp, vp]

@@ -1,8 +1,8 @@
 """Build the in-tree CUDA library libimogen_b200.so for sm_100a (nvcc, no JIT cache).
 
 The kernels are split over several translation units (host code; fluid and magnet sweeps per
-precision) that compile in parallel and link into one shared library with the CUDA runtime
-linked statically."""
+precision; the MAT-file slice reader/writer, host C++ linked with zlib) that compile in parallel and
+link into one shared library with the CUDA runtime linked statically."""
 from __future__ import annotations
 
 import concurrent.futures
@@ -15,7 +15,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
-UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu", "fluid_cluster.cu"]
+UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu", "fluid_cluster.cu",
+         "matfile.cpp"]
 # per-unit ptxas options: the batched cluster fluid kernels are compiled at -O1 (fluid_cluster.cu says why)
 UNIT_FLAGS = {"fluid_cluster.cu": ["-Xptxas", "-O1"]}
 OUT = os.path.join(HERE, "libimogen_b200.so")
@@ -51,7 +52,7 @@ def build(force=False, verbose=False, extra=()):
     tmp = tempfile.mkdtemp(prefix="imogen_b200_build_")
     try:
         def compile_unit(unit):
-            obj = os.path.join(tmp, unit.replace(".cu", ".o"))
+            obj = os.path.join(tmp, os.path.splitext(unit)[0] + ".o")
             cmd = [cc, *ARCH, *FLAGS, *UNIT_FLAGS.get(unit, []), "-I", os.path.join(ROOT, "include"), "-c",
                    os.path.join(CSRC, unit), "-o", obj, *extra]
             if verbose:
@@ -66,7 +67,7 @@ def build(force=False, verbose=False, extra=()):
                 sys.stderr.write(r.stdout + r.stderr)
             if r.returncode != 0:
                 raise RuntimeError(f"nvcc failed for {unit}")
-        link = [cc, *ARCH, "-shared", "-cudart", "static", *[o for _, o, _ in results], "-o", OUT + ".tmp"]
+        link = [cc, *ARCH, "-shared", "-cudart", "static", *[o for _, o, _ in results], "-lz", "-o", OUT + ".tmp"]
         r = subprocess.run(link, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)

@@ -159,7 +159,7 @@ __device__ __forceinline__ void cfl_finalize_body(DevTime* tm, int check_running
         tm->done = 1;
         return;
     }
-    if (check_running) tm->iters_run += 1;
+    if (check_running) tm->iters_run += 1;   // = run.time.iteration from here on
     double cmax = 1e-2;
     int gi = 0;
     for (int i = 0; i < 3; ++i) {
@@ -185,6 +185,10 @@ __device__ __forceinline__ void cfl_finalize_body(DevTime* tm, int check_running
     }
     tm->dt = dt;
     tm->time = nt;
+    // TimeManager.appendHistory: history(iteration) = dTime (the second update of a per-step
+    // iteration overwrites the first)
+    const int k = tm->iters_run - 1;
+    if (tm->dt_hist && k >= 0 && k < tm->dt_hist_cap) tm->dt_hist[k] = dt;
 }
 
 __global__ void cfl_finalize_kernel(DevTime* tm, int check_running) {

@@ -82,6 +82,9 @@ struct DevTime {
     int tread_dc;                    // dCells of the current call
     int tread_go;                    // the current call shifts the grid
     int tread_count;                 // entries in TreadmillManager.history
+    double* dt_hist;                 // TimeManager.history: dTime of iteration k at [k - 1] (k <= cap)
+    int dt_hist_cap;
+    int pad3;
 };
 
 // ---- batched launches -----------------------------------------------------------------------------

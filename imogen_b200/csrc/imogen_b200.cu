@@ -16,6 +16,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -162,6 +163,8 @@ struct img_ctx {
     int* tread_idx = nullptr;       // treadmill: per-pencil maximum index, first means, history
     double* tread_means = nullptr;
     int* tread_hist = nullptr;
+    double* dt_hist = nullptr;      // TimeManager.history (DevTime::dt_hist points here)
+    std::time_t created = 0;        // TimeManager.startTime
     double* stage = nullptr;    // mixed form: FP64 staging buffer of one array for host transfers
     std::vector<double> fade_host;
     int use_b[3] = {1, 1, 1};
@@ -283,6 +286,8 @@ std::vector<double> fade_coefficients(int f) {
 // their static shared memory).
 constexpr size_t kPencilSmemLimit = 210 * 1024;
 constexpr int kTreadHistCap = 1 << 16;   // treadmill history entries kept on the device
+constexpr int kDtHistCap = 1 << 16;      // TimeManager.history entries kept on the device
+int dt_hist_cap(const img_config& c) { return std::max(1, std::min(c.iter_max, kDtHistCap)); }
 
 bool tiling_fits(const PencilCfg& p, size_t elem) {
     return (elem == 8 ? fluid_smem_bytes<double>(p.G * p.cpt, p.Wb) : fluid_smem_bytes<float>(p.G * p.cpt, p.Wb)) <=
@@ -1094,7 +1099,7 @@ int validate(const img_config& c, std::string& why) {
 
 // Device bytes: state + scratch + edges + tables.
 struct Layout {
-    size_t state, scratch, tm, table, fade, partial, stage, tread, edges, total;
+    size_t state, scratch, tm, table, fade, partial, stage, tread, dthist, edges, total;
     size_t edge_off[NOBJ][3][2];
 };
 
@@ -1126,7 +1131,8 @@ Layout plan(const img_config& c) {
                 off += align256(sizeof(double) * (n / c.grid[e]));
             }
     L.edges = off;
-    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.tread + L.edges;
+    L.dthist = align256(sizeof(double) * dt_hist_cap(c));
+    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.tread + L.dthist + L.edges;
     return L;
 }
 
@@ -1246,6 +1252,7 @@ int img_create(img_ctx** out, const img_config* cfg) {
         return bail(IMG_ERR_CUDA);
     }
     ctx->own_stream = ctx->stream;
+    ctx->created = std::time(nullptr);
     Layout L = plan(*cfg);
     ctx->slab_bytes = L.total;
     if (cudaMalloc(&ctx->slab, L.total) != cudaSuccess) {
@@ -1281,6 +1288,8 @@ int img_create(img_ctx** out, const img_config* cfg) {
         ctx->tread_hist = reinterpret_cast<int*>(p + align256(sizeof(int) * ncol) + align256(sizeof(double) * ncol));
     }
     p += L.tread;
+    ctx->dt_hist = reinterpret_cast<double*>(p);
+    p += L.dthist;
     char* edge_base = p;
     for (int o = 0; o < NOBJ; ++o)
         for (int e = 0; e < 3; ++e)
@@ -1302,6 +1311,8 @@ int img_create(img_ctx** out, const img_config* cfg) {
     t.update_mode = cfg->update_mode;
     t.rad_minbits = 0xfff0000000000000ull;   // ordered bits of +inf (rad_init_kernel)
     t.tread_last = -1;                       // TreadmillManager.last
+    t.dt_hist = ctx->dt_hist;
+    t.dt_hist_cap = dt_hist_cap(*cfg);
     *ctx->host_tm = t;
     if (cudaMemcpyAsync(ctx->fade_dev, ctx->fade_host.data(), sizeof(double) * ctx->fade_host.size(), cudaMemcpyHostToDevice,
                         ctx->stream) != cudaSuccess ||
@@ -1595,6 +1606,81 @@ int img_treadmill_history(img_ctx* ctx, int* out, int cap, int* count, int* last
     return IMG_OK;
 }
 
+int img_save_slice(img_ctx* ctx, const char* path, const img_slice_meta* meta) {
+    if (!ctx || !path || !meta) return fail(ctx, IMG_ERR_ARG, "null argument");
+    if (!ctx->state_set) return fail(ctx, IMG_ERR_STATE, "state not set");
+    const long long n = ctx->g.ncell;
+    std::vector<double> mass(n), mom(3 * n), ener(n), mag(3 * n);
+    int ids[8] = {IMG_VAR_MASS, IMG_VAR_MOMX, IMG_VAR_MOMY, IMG_VAR_MOMZ, IMG_VAR_ENER, IMG_VAR_MAGX, IMG_VAR_MAGY,
+                  IMG_VAR_MAGZ};
+    double* hosts[8] = {mass.data(), mom.data(), mom.data() + n, mom.data() + 2 * n, ener.data(), mag.data(),
+                        mag.data() + n, mag.data() + 2 * n};
+    int rc = img_download_many(ctx, 8, ids, hosts, (size_t)n);
+    if (rc != IMG_OK) return rc;
+    CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const DevTime tm = *ctx->host_tm;
+    // the save follows the iteration it records: run.time.iteration = iterations completed
+    const int iter = ctx->iteration - 1;
+    const int nh = std::max(0, std::min(iter, tm.dt_hist_cap));
+    std::vector<double> hist(nh);
+    if (nh) {
+        CK(cudaMemcpyAsync(hist.data(), ctx->dt_hist, sizeof(double) * nh, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    std::vector<int> th(std::min(tm.tread_count, kTreadHistCap));
+    if (!th.empty()) {
+        CK(cudaMemcpyAsync(th.data(), ctx->tread_hist, sizeof(int) * th.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    img_slice_state st{};
+    for (int d = 0; d < 3; ++d) {
+        st.grid[d] = ctx->g.n[d];
+        st.dgrid[d] = ctx->cfg.dgrid[d];
+    }
+    st.gamma = ctx->cfg.gamma;
+    st.time = tm.time;
+    st.iteration = iter;
+    st.iter_max = ctx->cfg.iter_max;
+    st.time_max = ctx->cfg.time_max;
+    st.dt_history = hist.data();
+    st.n_history = nh;
+    st.magnet_active = ctx->cfg.magnet_active;
+    st.mass = mass.data();
+    st.mom = mom.data();
+    st.ener = ener.data();
+    st.mag = mag.data();
+    st.treadmill = ctx->cfg.treadmill;
+    st.tread_history = th.data();
+    st.n_tread = (int)th.size();
+    img_slice_meta m = *meta;
+    char started[32];
+    if (!m.started) {   // datestr(clock) default form, local time
+        std::tm lt{};
+        localtime_r(&ctx->created, &lt);
+        std::strftime(started, sizeof started, "%d-%b-%Y %H:%M:%S", &lt);
+        m.started = started;
+    }
+    rc = img_slice_write(path, &m, &st);
+    if (rc != IMG_OK) return fail(ctx, rc, "%s", img_slice_last_error());
+    return IMG_OK;
+}
+
+int img_load_slice(img_ctx* ctx, const char* path) {
+    if (!ctx || !path) return fail(ctx, IMG_ERR_ARG, "null argument");
+    int grid[3];
+    int rc = img_slice_read(path, grid, nullptr, nullptr, nullptr, nullptr, nullptr);
+    if (rc != IMG_OK) return fail(ctx, rc, "%s", img_slice_last_error());
+    if (grid[0] != ctx->g.n[0] || grid[1] != ctx->g.n[1] || grid[2] != ctx->g.n[2])
+        return fail(ctx, IMG_ERR_ARG, "slice of %dx%dx%d cells, context grid %dx%dx%d", grid[0], grid[1], grid[2],
+                    ctx->g.n[0], ctx->g.n[1], ctx->g.n[2]);
+    const long long n = ctx->g.ncell;
+    std::vector<double> mass(n), mom(3 * n), ener(n), mag(3 * n);
+    rc = img_slice_read(path, grid, mass.data(), mom.data(), ener.data(), mag.data(), nullptr);
+    if (rc != IMG_OK) return fail(ctx, rc, "%s", img_slice_last_error());
+    return img_set_state(ctx, mass.data(), mom.data(), ener.data(), mag.data());
+}
+
 int img_radiation_strength(img_ctx* ctx, double* strength) {
     if (!ctx || !strength) return fail(ctx, IMG_ERR_ARG, "null argument");
     CK(cudaMemcpyAsync(ctx->host_tm, ctx->tm, sizeof(DevTime), cudaMemcpyDeviceToHost, ctx->stream));
@@ -1778,8 +1864,9 @@ int img_checkpoint_load(img_ctx* ctx, const void* host, size_t bytes) {
     CK(cudaStreamSynchronize(ctx->stream));
     CK(cudaMemcpyAsync(ctx->slab, static_cast<const char*>(host) + sizeof h, ctx->slab_bytes, cudaMemcpyHostToDevice,
                        ctx->stream));
-    // the stored-edge table holds device addresses: this context's own, not the writer's
+    // the stored-edge table and the time record hold device addresses: this context's own, not the writer's
     CK(cudaMemcpyAsync(ctx->edges_dev, &ctx->edges_host, sizeof(EdgeTable), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(&ctx->tm->dt_hist, &ctx->dt_hist, sizeof(double*), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->state_set = h.state_set != 0;
     ctx->init_store = h.init_store != 0;

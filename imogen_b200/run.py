@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import ImgConfig, ImogenError, check, lib
+from ._lib import ImgConfig, ImgSliceMeta, ImgSliceState, ImogenError, check, lib
 
 BC_MODES = ("circ", "const", "fade", "mirror", "trans", "wall", "flip", "zero", "linear", "wormhole")   # enums/ENUM.m:22-32
 LIMITERS = {"vanleer": 0, "superbee": 1, "minmond": 2, "minmod": 2}   # FluxLimiterEnum.m:10-13
@@ -104,6 +104,73 @@ def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ"
     c.rad_initial_maximum = float(rad_initial_maximum)
     c.treadmill = int(treadmill)
     return c
+
+
+SLICE_TYPES = {"X": 1, "Y": 2, "Z": 3, "XY": 4, "XZ": 5, "YZ": 6, "XYZ": 7, "SP-XYZ": 8}   # SaveManager.SLICELABELS
+
+
+def slice_meta(slice="XYZ", index=(1, 1, 1), suffix="FINAL", about="", version=0.0, wall_max=1e5, started=None):
+    """img_slice_meta for one resultsHandler slice save (save/resultsHandler.m:26-113)."""
+    m = ImgSliceMeta()
+    m.type = SLICE_TYPES[slice] if isinstance(slice, str) else int(slice)
+    for d in range(3):
+        m.index[d] = int(index[d])
+    m.suffix = suffix.encode()
+    m.about = about.encode()
+    m.version = float(version)
+    m.wall_max = float(wall_max)
+    m.started = started.encode() if started is not None else None
+    return m
+
+
+def write_slice(path, state, grid, dgrid=(1.0, 1.0, 1.0), gamma=5 / 3, time=0.0, iteration=0, iter_max=10,
+                time_max=1e5, dt_history=(), magnet=True, treadmill=0, treadmill_history=(), **meta):
+    """img_slice_write of host arrays (mass, mom[3], ener, mag[3]; x fastest): no device involved."""
+    grid = tuple(int(g) for g in grid)
+    f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1, order="F"))
+    mass, ener = f(state[0]), f(state[2])
+    mom = np.concatenate([f(state[1][c]) for c in range(3)])
+    mag = np.concatenate([f(state[3][c]) for c in range(3)])
+    hist = np.ascontiguousarray(np.asarray(dt_history, dtype=np.float64))
+    th = np.ascontiguousarray(np.asarray(treadmill_history, dtype=np.int32))
+    st = ImgSliceState()
+    for d in range(3):
+        st.grid[d] = grid[d]
+        st.dgrid[d] = float(dgrid[d])
+    st.gamma, st.time, st.iteration, st.iter_max, st.time_max = gamma, time, iteration, iter_max, time_max
+    dp = ctypes.POINTER(ctypes.c_double)
+    st.dt_history = hist.ctypes.data_as(dp) if hist.size else None
+    st.n_history = int(hist.size)
+    st.magnet_active = int(bool(magnet))
+    st.mass, st.mom, st.ener, st.mag = (a.ctypes.data_as(dp) for a in (mass, mom, ener, mag))
+    st.treadmill = int(treadmill)
+    st.tread_history = th.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if th.size else None
+    st.n_tread = int(th.size)
+    m = slice_meta(**meta)
+    rc = lib().img_slice_write(str(path).encode(), ctypes.byref(m), ctypes.byref(st))
+    if rc != 0:
+        raise ImogenError(rc, lib().img_slice_last_error().decode())
+
+
+def read_slice(path):
+    """img_slice_read: (mass, mom[3], ener, mag[3]) as grid-shaped arrays, and whether B was stored."""
+    g = (ctypes.c_int * 3)()
+    rc = lib().img_slice_read(str(path).encode(), g, None, None, None, None, None)
+    if rc != 0:
+        raise ImogenError(rc, lib().img_slice_last_error().decode())
+    grid = tuple(g)
+    n = grid[0] * grid[1] * grid[2]
+    mass, ener = np.zeros(n), np.zeros(n)
+    mom, mag = np.zeros(3 * n), np.zeros(3 * n)
+    hm = ctypes.c_int()
+    dp = ctypes.POINTER(ctypes.c_double)
+    rc = lib().img_slice_read(str(path).encode(), g, mass.ctypes.data_as(dp), mom.ctypes.data_as(dp),
+                              ener.ctypes.data_as(dp), mag.ctypes.data_as(dp), ctypes.byref(hm))
+    if rc != 0:
+        raise ImogenError(rc, lib().img_slice_last_error().decode())
+    r = lambda a: a.reshape(grid, order="F")
+    r3 = lambda a: np.stack([r(a[c * n:(c + 1) * n]) for c in range(3)])
+    return (r(mass), r3(mom), r(ener), r3(mag)), bool(hm.value)
 
 
 def bytes_required(**kw):
@@ -254,6 +321,16 @@ class ImogenRun:
     def source(self):
         """source.m for this path: the radiation sink E -= dTime * radiation.solve (source.m:30)."""
         check(lib().img_source(self._h), self._h)
+
+    def save_slice(self, path, slice="XYZ", index=(1, 1, 1), suffix="FINAL", about="", version=0.0, wall_max=1e5,
+                   started=None):
+        """resultsHandler's save of one slice (save/resultsHandler.m:26-113) as a MAT-file (img_save_slice)."""
+        m = slice_meta(slice, index, suffix, about, version, wall_max, started)
+        check(lib().img_save_slice(self._h, str(path).encode(), ctypes.byref(m)), self._h)
+
+    def load_slice(self, path):
+        """Resume from a slice file as Initializer.loadDataFromFile does (img_load_slice)."""
+        check(lib().img_load_slice(self._h, str(path).encode()), self._h)
 
     def treadmill(self):
         """treadmillGrid (treadmill/treadmillGrid.m) at the current iteration (iterate calls it after

@@ -143,6 +143,56 @@ int img_source(img_ctx* ctx);
  * nothing when the treadmill is off or before iteration 10.  img_step calls it after each flux. */
 int img_treadmill(img_ctx* ctx);
 
+/* ---- slice files (save/resultsHandler.m:26-113) and resuming from them ------------------------ */
+/* One slice save: SaveManager's slice type (1-3: X, Y, Z lines; 4-6: XY, XZ, YZ planes; 7: XYZ;
+ * 8: SP-XYZ, SaveManager.SLICELABELS), SLICEINDEX (1-based cell of the cuts of types 1-6), the file
+ * suffix ('START', 'FINAL' or the iteration label; the variable is sx_<label>_<suffix>, made a valid
+ * name as genvarname does), and run.about / run.version / TimeManager.WALLMAX / the start date string
+ * (NULL: '' or, through a context, its creation time in datestr's default form). */
+typedef struct img_slice_meta {
+    int type;
+    int index[3];
+    const char* suffix;
+    const char* about;
+    double version;
+    double wall_max;
+    const char* started;
+} img_slice_meta;
+
+/* Host view of a run for img_slice_write: FP64 arrays, x fastest, mom and mag three components back
+ * to back; dt_history = TimeManager.history(1:n_history); tread_history = TreadmillManager.history. */
+typedef struct img_slice_state {
+    int grid[3];
+    double dgrid[3];
+    double gamma;
+    double time;
+    int iteration;
+    int iter_max;
+    double time_max;
+    const double* dt_history;
+    int n_history;
+    int magnet_active;
+    const double* mass;
+    const double* mom;
+    const double* ener;
+    const double* mag;
+    int treadmill;
+    const int* tread_history;
+    int n_tread;
+} img_slice_state;
+
+/* Write one slice file: a MAT-file Level 5 holding the struct resultsHandler saves (no device work). */
+int img_slice_write(const char* path, const img_slice_meta* meta, const img_slice_state* state);
+/* Read a slice file as Initializer.loadDataFromFile does (experiment/Initializer.m:269-292): the first
+ * variable's mass, ener, momX/Y/Z and magX/Y/Z (zeros when empty).  Any output pointer may be NULL
+ * (grid only: the extents of mass, trailing 1s added).  Uncompressed and zlib-compressed elements. */
+int img_slice_read(const char* path, int grid[3], double* mass, double* mom, double* ener, double* mag, int* has_mag);
+const char* img_slice_last_error(void);
+/* The same through a context: its state, clock, dt and treadmill history (synchronises); and a
+ * resume: img_set_state from a slice file whose arrays match the context's grid. */
+int img_save_slice(img_ctx* ctx, const char* path, const img_slice_meta* meta);
+int img_load_slice(img_ctx* ctx, const char* path);
+
 /* TreadmillManager.history (treadmill/TreadmillManager.m:50-56) and .last: copies min(cap, count)
  * entries, *count = the number recorded (the device keeps the first 65536), synchronises. */
 int img_treadmill_history(img_ctx* ctx, int* out, int cap, int* count, int* last);
