@@ -28,6 +28,8 @@ SYMBOLS = (
     "img_get_stream", "img_autotune", "img_get_tiling", "img_set_tiling", "img_launch_count", "img_sweep_order",
     "img_source", "img_radiation_strength", "img_treadmill", "img_treadmill_history",
     "img_slice_write", "img_slice_read", "img_slice_last_error", "img_save_slice", "img_load_slice",
+    "img_server_create", "img_server_destroy", "img_batch_submit", "img_batch_poll", "img_batch_cancel",
+    "img_batch_result", "img_server_stats", "img_monotonic_seconds",
     "img_batch_create", "img_batch_destroy", "img_batch_add", "img_batch_remove", "img_batch_size", "img_batch_step",
     "img_batch_run", "img_batch_status", "img_batch_get_stream", "img_batch_launch_count", "img_batch_last_error",
 )
@@ -91,6 +93,31 @@ class ImgSliceState(ctypes.Structure):
         ("treadmill", ctypes.c_int),
         ("tread_history", ctypes.POINTER(ctypes.c_int)),
         ("n_tread", ctypes.c_int),
+    ]
+
+
+class ImgJobInfo(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("time", ctypes.c_double),
+        ("iterations", ctypes.c_int),
+        ("submitted", ctypes.c_double),
+        ("admitted", ctypes.c_double),
+        ("completed", ctypes.c_double),
+        ("error_code", ctypes.c_int),
+        ("error", ctypes.c_char * 256),
+    ]
+
+
+class ImgServerInfo(ctypes.Structure):
+    _fields_ = [
+        ("budget", ctypes.c_size_t),
+        ("used", ctypes.c_size_t),
+        ("peak", ctypes.c_size_t),
+        ("queued", ctypes.c_int),
+        ("running", ctypes.c_int),
+        ("finished", ctypes.c_int),
+        ("rounds", ctypes.c_longlong),
     ]
 
 
@@ -177,6 +204,18 @@ def lib():
     L.img_save_slice.restype = ctypes.c_int
     L.img_load_slice.argtypes = [vp, ctypes.c_char_p]
     L.img_load_slice.restype = ctypes.c_int
+    L.img_server_create.argtypes = [ctypes.POINTER(vp), ctypes.c_size_t, ctypes.c_int, ctypes.c_int]
+    L.img_server_destroy.argtypes = [vp]
+    L.img_batch_submit.argtypes = [vp, cfgp, dp, dp, dp, dp, ip]
+    L.img_batch_poll.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ImgJobInfo)]
+    L.img_batch_cancel.argtypes = [vp, ctypes.c_int]
+    L.img_batch_result.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, ctypes.c_size_t]
+    L.img_server_stats.argtypes = [vp, ctypes.POINTER(ImgServerInfo)]
+    for name in ("img_server_create", "img_server_destroy", "img_batch_submit", "img_batch_poll", "img_batch_cancel",
+                 "img_batch_result", "img_server_stats"):
+        getattr(L, name).restype = ctypes.c_int
+    L.img_monotonic_seconds.argtypes = []
+    L.img_monotonic_seconds.restype = ctypes.c_double
     L.img_batch_create.argtypes = [ctypes.POINTER(vp)]
     L.img_batch_destroy.argtypes = [vp]
     L.img_batch_add.argtypes = [vp, vp]

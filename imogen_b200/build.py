@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 UNITS = ["imogen_b200.cu", "fluid_f32.cu", "fluid_f64.cu", "magnet_f32.cu", "magnet_f64.cu", "fluid_cluster.cu",
-         "matfile.cpp"]
+         "matfile.cpp", "server.cpp"]
 # per-unit ptxas options: the batched cluster fluid kernels are compiled at -O1 (fluid_cluster.cu says why)
 UNIT_FLAGS = {"fluid_cluster.cu": ["-Xptxas", "-O1"]}
 OUT = os.path.join(HERE, "libimogen_b200.so")

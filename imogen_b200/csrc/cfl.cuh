@@ -57,7 +57,7 @@ __device__ __forceinline__ double cell_msq(const CflArgs& a, const T* const cb[3
 // CFL candidates are then those of the new E).
 template <typename T>
 __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vblock, unsigned vgrid) {
-    if (a.tm->done || a.tm->error) return;
+    if (a.tm->done || a.tm->error || !(a.accumulate || a.radiate)) return;   // empty pass: nothing to do
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* p[3] = {reinterpret_cast<const T*>(a.q[Q_PX]), reinterpret_cast<const T*>(a.q[Q_PY]),
                      reinterpret_cast<const T*>(a.q[Q_PZ])};

@@ -173,6 +173,7 @@ struct img_ctx {
     bool init_store = true, init_flux = true;   // fluid objects not yet assigned
     bool init_mag[3][3] = {{true, true, true}, {true, true, true}, {true, true, true}};
     bool cfl_valid = false;     // DevTime.maxbits hold the CFL maxima of the current state
+    bool pad_cfl = false;       // batch recording: an empty CFL pass where another member needs one
     int iteration = 1;
     int iters_base = 0;
     PencilCfg pcfg[3][3];        // pencil tiling per kernel (0 fluid sweep, 1 magnet chain, 2 magnet CT) and
@@ -981,7 +982,11 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
     if (!ctx->cfl_valid) {
         int rc = cfl_reduce(ctx);
         if (rc != IMG_OK) return rc;
+    } else if (ctx->rec && ctx->pad_cfl) {   // a batch member with valid maxima beside one without
+        int rc = ctx->elem == 8 ? launch_cfl_reduce<double>(ctx, false) : launch_cfl_reduce<float>(ctx, false);
+        if (rc != IMG_OK) return rc;
     }
+    ctx->pad_cfl = false;
     if (ctx->rec) {
         OpRec r{};
         r.kind = OP_CFL_FINALIZE;
@@ -2222,6 +2227,11 @@ int img_batch_step(img_batch* b) {
     for (img_ctx* m : b->members)
         if (m->iteration > m->cfg.iter_max)
             BCK(cudaMemcpyAsync(&m->tm->done, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    // one launch sequence for all members: where some member's CFL maxima are not valid (a member that
+    // just joined), the others record an empty CFL pass in its place (their maxima are left as they are)
+    bool all_valid = true;
+    for (img_ctx* m : b->members) all_valid = all_valid && m->cfl_valid;
+    for (img_ctx* m : b->members) m->pad_cfl = !all_valid && m->cfl_valid;
     bool st = true;
     for (img_ctx* m : b->members) st = st && steady(m) && m->cfl_valid == b->members[0]->cfl_valid;
     const int phase = (int)(b->steps % 6);

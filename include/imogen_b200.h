@@ -143,6 +143,46 @@ int img_source(img_ctx* ctx);
  * nothing when the treadmill is off or before iteration 10.  img_step calls it after each flux. */
 int img_treadmill(img_ctx* ctx);
 
+/* ---- job server: img_batch_submit / poll / cancel ---------------------------------------------- */
+/* Jobs admitted by HBM budget (img_bytes_required), in submission order, into the running batch of
+ * their kind and advanced by one worker thread (see imogen_b200/csrc/server.cpp); a finished job's
+ * result (its whole state, or its eight totals) is kept in host memory until the server is destroyed.
+ * Every call returns at once and may come from any thread.  No reference counterpart: the reference
+ * runs one simulation per MATLAB session. */
+typedef struct img_server img_server;
+enum { IMG_JOB_QUEUED = 0, IMG_JOB_RUNNING = 1, IMG_JOB_DONE = 2, IMG_JOB_FAILED = 3, IMG_JOB_CANCELLED = 4 };
+enum { IMG_KEEP_STATE = 0, IMG_KEEP_TOTALS = 1 };
+enum { IMG_RESULT_TOTALS = -1 };   /* img_batch_result var_id of the totals (IMG_KEEP_TOTALS) */
+typedef struct img_job_info {
+    int status;                  /* IMG_JOB_* */
+    double time;                 /* simulated time reached (finished jobs) */
+    int iterations;              /* iterations that advanced the state (finished jobs) */
+    double submitted, admitted, completed;   /* img_monotonic_seconds() at those events (0: not yet) */
+    int error_code;              /* IMG_ERR_* of a failed job */
+    char error[256];
+} img_job_info;
+typedef struct img_server_info {
+    size_t budget, used, peak;   /* bytes: the budget, held now, most ever held */
+    int queued, running, finished;
+    long long rounds;            /* scheduling rounds (one iteration of every running job each) */
+} img_server_info;
+
+/* check_every: rounds between checks for finished jobs (a check synchronises); keep: IMG_KEEP_*. */
+int img_server_create(img_server** out, size_t hbm_budget, int check_every, int keep);
+int img_server_destroy(img_server* s);   /* stops the worker; jobs still running are dropped */
+/* Queue one job (settings + FP64 initial state as for img_set_state, copied).  IMG_ERR_NOMEM when
+ * the job alone exceeds the budget. */
+int img_batch_submit(img_server* s, const img_config* cfg, const double* mass, const double* mom, const double* ener,
+                     const double* mag, int* job_id);
+int img_batch_poll(img_server* s, int job_id, img_job_info* info);
+/* A queued job is dropped at once; a running one is stopped by the worker before its next round
+ * (poll until its status is IMG_JOB_CANCELLED).  IMG_ERR_STATE if the job already ended. */
+int img_batch_cancel(img_server* s, int job_id);
+/* The result of a finished job: variable var_id (IMG_VAR_*, n cells) or IMG_RESULT_TOTALS (8 values). */
+int img_batch_result(img_server* s, int job_id, int var_id, double* host, size_t n);
+int img_server_stats(img_server* s, img_server_info* info);
+double img_monotonic_seconds(void);   /* the clock of the job times above: CLOCK_MONOTONIC seconds */
+
 /* ---- slice files (save/resultsHandler.m:26-113) and resuming from them ------------------------ */
 /* One slice save: SaveManager's slice type (1-3: X, Y, Z lines; 4-6: XY, XZ, YZ planes; 7: XYZ;
  * 8: SP-XYZ, SaveManager.SLICELABELS), SLICEINDEX (1-based cell of the cuts of types 1-6), the file

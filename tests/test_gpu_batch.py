@@ -142,3 +142,32 @@ def test_long_cluster_members_with_fade_match_alone():
     b.close()
     for r in alone + together:
         r.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fresh_member_joins_a_running_batch(precision):
+    """A new member takes its first (edge-capturing, CFL-reducing) iteration inside a batch whose
+    members are mid-run (other sweep-order phases): everyone stays bitwise equal to running alone."""
+    s, st = _ot(40)
+    first = [_ot(32), _ot(48)]
+    alone = [_make(c, x, precision) for c, x in first] + [_make(s, st, precision)]
+    together = [_make(c, x, precision) for c, x in first]
+    b = ImogenBatch(together)
+    for _ in range(4):
+        b.step()
+        alone[0].iterate()
+        alone[1].iterate()
+    late = _make(s, st, precision)
+    b.add(late)
+    together.append(late)
+    for _ in range(9):
+        b.step()
+        for r in alone:
+            r.iterate()
+    for r in alone:
+        r.sync()
+    for i, (x, y) in enumerate(zip(alone, together)):
+        _same(x, y, f"member {i}")
+    b.close()
+    for r in alone + together:
+        r.close()

@@ -1,5 +1,6 @@
-"""Serving loop (imogen_b200.serve) on the GPU: results in the mix equal results alone, the HBM
-budget holds, and the mixed form stays within its tolerance of FP64 (GPU required)."""
+"""Serving (imogen_b200.serve over the native job server) on the GPU: results in the mix equal results
+alone, the HBM budget holds, the mixed form stays within its tolerance of FP64, jobs can be polled and
+cancelled, and the C ABI's img_batch_submit / poll / cancel work directly (GPU required)."""
 import numpy as np
 import pytest
 
@@ -41,18 +42,11 @@ def test_hbm_budget_bounds_the_jobs_on_the_device():
     need = [serve.bytes_required(**dict(j.settings, precision="mixed")) for j in jobs]
     budget = 2 * max(need)
     srv = serve.Server(hbm_budget=budget, check_every=1, keep="totals")
-    peak = [0]
-    admit = srv._admit
-
-    def watched():
-        admit()
-        peak[0] = max(peak[0], srv.used)
-        assert srv.used <= budget
-
-    srv._admit = watched
     done = srv.serve(jobs)
-    assert len(done) == len(jobs) and srv.used == 0
-    assert 0 < peak[0] <= budget
+    st = srv.stats()                                     # the native server's own accounting
+    assert len(done) == len(jobs) and st["used"] == 0 and st["finished"] == len(jobs)
+    assert max(need) <= st["peak"] <= budget
+    assert all("totals" in j.result for j in done)
 
 
 def test_mixed_form_within_tolerance_of_fp64():
@@ -108,3 +102,55 @@ def test_checkpoint_resumes_bit_for_bit(precision):
         assert a.time.time == b.time.time and a.time.iteration == b.time.iteration
         a.close()
         b.close()
+
+
+def test_job_api_through_the_c_abi():
+    """img_server_create / img_batch_submit / img_batch_poll / img_batch_cancel / img_batch_result as a
+    MEX gateway would call them (ctypes, no Python scheduler), including a job that fails at admission
+    (an unsupported boundary) next to jobs that finish."""
+    import ctypes
+    from imogen_b200 import _lib
+    from imogen_b200.run import make_config
+    L = _lib.lib()
+    h = ctypes.c_void_p()
+    assert L.img_server_create(ctypes.byref(h), 1 << 34, 2, 1) == 0
+    dp = ctypes.POINTER(ctypes.c_double)
+    ids = []
+    jobs = _stream("mixed", count=5, seed=21)
+    bad = dict(jobs[0].settings, bc="linear")
+    for settings in [j.settings for j in jobs] + [bad]:
+        st = [j for j in jobs if j.settings is settings] or [jobs[0]]
+        rho, mom, ener, mag = st[0].state
+        cfg = make_config(precision="mixed", **settings)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64).ravel(order="F"))
+        arrs = [f(rho), np.concatenate([f(m) for m in mom]), f(ener), np.concatenate([f(b) for b in mag])]
+        jid = ctypes.c_int()
+        assert L.img_batch_submit(h, ctypes.byref(cfg), *[a.ctypes.data_as(dp) for a in arrs], ctypes.byref(jid)) == 0
+        ids.append(jid.value)
+    victim = ids[2]
+    assert L.img_batch_cancel(h, victim) == 0
+    info = _lib.ImgJobInfo()
+    import time
+    t0 = time.time()
+    while True:
+        states = []
+        for j in ids:
+            assert L.img_batch_poll(h, j, ctypes.byref(info)) == 0
+            states.append(info.status)
+        if all(s >= 2 for s in states) or time.time() - t0 > 120:
+            break
+        time.sleep(0.01)
+    assert states[2] == 4                                # cancelled
+    assert states[-1] == 3                               # failed: the linear BC is rejected at creation
+    L.img_batch_poll(h, ids[-1], ctypes.byref(info))
+    assert b"linear" in info.error and info.error_code == -4
+    for j, s in zip(ids[:-1], states[:-1]):
+        if j == victim:
+            continue
+        assert s == 2
+        tot = np.zeros(8)
+        assert L.img_batch_result(h, j, -1, tot.ctypes.data_as(dp), 8) == 0 and tot[0] > 0
+    assert L.img_batch_cancel(h, ids[0]) != 0            # already done
+    srv_info = _lib.ImgServerInfo()
+    assert L.img_server_stats(h, ctypes.byref(srv_info)) == 0 and srv_info.used == 0
+    assert L.img_server_destroy(h) == 0
