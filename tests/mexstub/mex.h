@@ -21,5 +21,6 @@ int mxIsComplex(const mxArray*);
 mxArray* mxCreateNumericMatrix(mwSize, mwSize, mxClassID, mxComplexity);
 mxArray* mxCreateNumericArray(mwSize, const mwSize*, mxClassID, mxComplexity);
 mxArray* mxCreateDoubleScalar(double);
+mxArray* mxCreateString(const char*);
 void mexErrMsgIdAndTxt(const char*, const char*, ...);
 #endif
