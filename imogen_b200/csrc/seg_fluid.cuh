@@ -397,7 +397,15 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
 
     // ---- stage 1: load, pressure, speed, F -------------------------------------------------------
     T u[5][C], bb[3][C], F[5][C];
-    double msq[C];
+    // sum of squares of the cell-centred B components without isZero, in rotated order (recomputed
+    // where needed instead of kept: it would hold 2C registers for the whole kernel)
+    auto bsq = [&](const T (&b)[3][C], int k) {
+        double m = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            if (MHD && ub[c]) m = m + (double)b[c][k] * (double)b[c][k];
+        return m;
+    };
     if (sp.colok) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) seg_load<T, C>(qv[v], o0, g.sd, vec, u[v]);
@@ -422,11 +430,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     if constexpr (VT == VISC_NONE) {
 #pragma unroll
         for (int k = 0; k < C; ++k) {
-            double m = 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
-            msq[k] = m;
+            const double m = bsq(bb, k);
             const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
             const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
             T p;
@@ -452,11 +456,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         double vel[C], snd[C], q[C];
 #pragma unroll
         for (int k = 0; k < C; ++k) {
-            double m = 0.0;
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                if (MHD && ub[c]) m = m + (double)bb[c][k] * (double)bb[c][k];
-            msq[k] = m;
+            const double m = bsq(bb, k);
             const T uu[5] = {u[0][k], u[1][k], u[2][k], u[3][k], u[4][k]};
             const T spd = press_speed_rot<T>(G, uu, m, P[k], CS[k]);
             if (sp.colok) lmax = fmax(lmax, spd);
@@ -516,14 +516,14 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         if constexpr (VT == VISC_NONE) {
             const T b3[3] = {bb[0][k], bb[1][k], bb[2][k]};
             T p2;
-            const T spd = press_speed_rot<T>(G, uu, msq[k], p2);   // relaxingFluid.m:47-50
+            const T spd = press_speed_rot<T>(G, uu, bsq(bb, k), p2);   // relaxingFluid.m:47-50
             if (sp.colok) lmax2 = fmax(lmax2, spd);
             T Fk[5];
             flux_num_rot<T>(uu, b3, p2, Fk);
 #pragma unroll
             for (int v = 0; v < 5; ++v) Fs[v][k] = Fk[v];
         } else {
-            const T spd = press_speed_rot<T>(G, uu, msq[k], P2[k], CS2[k]);
+            const T spd = press_speed_rot<T>(G, uu, bsq(bb, k), P2[k], CS2[k]);
             if (sp.colok) lmax2 = fmax(lmax2, spd);
         }
     }
@@ -586,13 +586,19 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     }
     double m3[3] = {0.0, 0.0, 0.0};   // rotated order
     bool bad = false;
+    T cb[3][C];   // the CFL pass reloads the cell-centred B (cache hits; one sweep in six)
+    if (a.cfl && sp.colok && MHD) {
+        seg_load<T, C>(a.q[Q_CBX + d], o0, g.sd, vec, cb[0]);
+        seg_load<T, C>(a.q[Q_CBX + d1], o0, g.sd, vec, cb[1]);
+        seg_load<T, C>(a.q[Q_CBX + d2], o0, g.sd, vec, cb[2]);
+    }
 #pragma unroll
     for (int k = 0; k < C; ++k) {
         unew[0][k] = unew[0][k] > (T)a.minmass ? unew[0][k] : (T)a.minmass;
         if (a.cfl && sp.colok) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
             double sp3[3];
             cfl_speeds(G, (double)unew[0][k], (double)unew[1][k], (double)unew[2][k], (double)unew[3][k],
-                       (double)unew[4][k], msq[k], sp3);
+                       (double)unew[4][k], MHD ? bsq(cb, k) : 0.0, sp3);
             bad = bad || !isfinite(sp3[0] + sp3[1] + sp3[2]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp3[c]);
