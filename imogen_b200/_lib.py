@@ -59,6 +59,9 @@ class ImgConfig(ctypes.Structure):
         ("rad_exponent", ctypes.c_double),
         ("rad_initial_maximum", ctypes.c_double),
         ("treadmill", ctypes.c_int),
+        ("fade_active", ctypes.c_int),
+        ("fade_location", ctypes.c_int * 3),
+        ("fade_size", ctypes.c_double),
     ]
 
 

@@ -22,6 +22,8 @@ struct CflArgs {
     int accumulate;        // accumulate the CFL maxima (0: the radiation sink alone)
     int radiate;           // first apply the optically thin radiation sink to E (source.m:30)
     double rad_exp;        // Radiation.exponent
+    const void* fade_map;  // point-fade map (null: none); the sink's assignment to E fades it (fade_ener)
+    int fade_ener;
 };
 
 // pressure(ENUM.PRESSURE_GAS, ...) of one cell (pressure.m:16-66): (G-1)(E - rho v^2/2) minus
@@ -74,8 +76,10 @@ __device__ __forceinline__ void cfl_reduce_body(const CflArgs& a, unsigned vbloc
         double e = (double)E[i];
         if (a.radiate) {
             const double gas = gas_pressure(a.gamma, r, px, py, pz, e, msq);
-            E[i] = (T)__dsub_rn(e, __dmul_rn(dt, thin_radiation(rs, a.rad_exp, r, gas)));
-            e = (double)E[i];
+            T en = (T)__dsub_rn(e, __dmul_rn(dt, thin_radiation(rs, a.rad_exp, r, gas)));
+            if (a.fade_ener) en = point_fade(en, reinterpret_cast<const T*>(a.fade_map)[i]);
+            E[i] = en;
+            e = (double)en;
         }
         if (!a.accumulate) continue;
         double sp[3];
@@ -115,6 +119,50 @@ __global__ void __launch_bounds__(256) cfl_reduce_batch_kernel(const CflArgs* __
     load_member_args(sa, args + bm.member);
     __syncthreads();
     cfl_reduce_body<T>(sa, (unsigned)bm.block, (unsigned)bm.nblocks);
+}
+
+// Point-fade pass (classes/PointFade.m, ImogenArray.m:85-86).  var < 0: after a fluid sweep, whose
+// relaxingFluid.m:64-71 assigns the five primaries (each faded when in `mask`: bit 0 rho, 1 momentum,
+// 2 E) and then rho = max(rho, MINMASS) (faded again); the sweep itself left rho unclamped.  var >= 0:
+// one array assigned from the host (img_upload), faded once.
+struct FadeArgs {
+    long long n;
+    void* q[NQ];
+    const void* map;
+    int mask;
+    int var;   // -1: the post-sweep pass; else the Q_* index of the assigned array
+    double minmass;
+    DevTime* tm;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) point_fade_kernel(const __grid_constant__ FadeArgs a) {
+    if (a.var < 0 && (a.tm->done || a.tm->error)) return;
+    const T* A = reinterpret_cast<const T*>(a.map);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.n; i += (long long)gridDim.x * blockDim.x) {
+        const T f = A[i];
+        if (a.var >= 0) {
+            T* X = reinterpret_cast<T*>(a.q[a.var]);
+            X[i] = point_fade(X[i], f);
+            continue;
+        }
+        if (a.mask & 2)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                T* P = reinterpret_cast<T*>(a.q[Q_PX + c]);
+                P[i] = point_fade(P[i], f);
+            }
+        if (a.mask & 4) {
+            T* E = reinterpret_cast<T*>(a.q[Q_E]);
+            E[i] = point_fade(E[i], f);
+        }
+        T* R = reinterpret_cast<T*>(a.q[Q_RHO]);
+        T m = R[i];
+        if (a.mask & 1) m = point_fade(m, f);
+        m = m > (T)a.minmass ? m : (T)a.minmass;   // max(rho, MINMASS), NaN -> MINMASS
+        if (a.mask & 1) m = point_fade(m, f);
+        R[i] = m;
+    }
 }
 
 // Radiation.initialize (fluid/Radiation.m:61-75), first part: the minimum over the cells of

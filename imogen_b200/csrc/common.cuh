@@ -321,6 +321,15 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
     atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
 
+// PointFade.fadeArray (classes/PointFade.m:46-49): 0.95 u A + u (1 - A) in that order, without FMA
+// contraction.
+__device__ __forceinline__ float point_fade(float u, float A) {
+    return __fadd_rn(__fmul_rn(__fmul_rn(0.95f, u), A), __fmul_rn(u, __fsub_rn(1.0f, A)));
+}
+__device__ __forceinline__ double point_fade(double u, double A) {
+    return __dadd_rn(__dmul_rn(__dmul_rn(0.95, u), A), __dmul_rn(u, __dsub_rn(1.0, A)));
+}
+
 // Doubles of either sign as unsigned integers of the same order (the callers exclude NaN).
 __device__ __forceinline__ unsigned long long ordered_bits(double v) {
     const unsigned long long b = (unsigned long long)__double_as_longlong(v);

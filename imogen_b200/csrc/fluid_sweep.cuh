@@ -43,6 +43,8 @@ struct FluidArgs {
     // linear and quadratic strengths c1, c2, and c2 (G+1), c2^2 ((G+1)/4)^2, c1^2 formed on the host
     int visc;
     double vc1, vc2, vk1, vk2, vc1sq;
+    double minmass_out;    // the final max(rho, MINMASS) (relaxingFluid.m:71); -inf when a point-fade pass
+                           // follows the sweep (it fades, clamps and fades again, as the two sets do)
 };
 constexpr int VISC_NONE = 0;
 constexpr int VISC_NR = 1;    // Neumann-Richtmyer (ArtificialViscosity.m:73-77)
@@ -461,7 +463,7 @@ __device__ __forceinline__ void fluid_sweep_body_mixed_cg(const FluidArgs& a, un
             }
             unew[v] = u[v][k] - ff * cfs * (a0[v] - Rm + a0[5 + v] - Lp);
         }
-        unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
+        unew[0] = unew[0] > (T)a.minmass_out ? unew[0] : (T)a.minmass_out;
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
 #pragma unroll
@@ -694,7 +696,7 @@ __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, uns
             const T Lp = sh(L, AN + (2 * (5 + v) + 1) * Wb, k, +1, a.mode[cls][1]);
             unew[v] = u[v][k] - ff * cfs * (R[ix] - Rm + L[ix] - Lp);
         }
-        unew[0] = unew[0] > (T)a.minmass ? unew[0] : (T)a.minmass;
+        unew[0] = unew[0] > (T)a.minmass_out ? unew[0] : (T)a.minmass_out;
         if (!tl.ok(k)) continue;
         const long long o = tl.off(k);
 #pragma unroll

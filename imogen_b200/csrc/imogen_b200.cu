@@ -164,6 +164,9 @@ struct img_ctx {
     double* tread_means = nullptr;
     int* tread_hist = nullptr;
     double* dt_hist = nullptr;      // TimeManager.history (DevTime::dt_hist points here)
+    void* fade_map = nullptr;       // PointFade map (T per cell) when a point fade acts on a fluid primary
+    int fade_mask = 0;              // IMG_FADE_MASS | MOM | ENER bits in effect
+    bool constructing = false;      // img_set_state's uploads (the initial assignment is not faded)
     std::time_t created = 0;        // TimeManager.startTime
     double* stage = nullptr;    // mixed form: FP64 staging buffer of one array for host transfers
     std::vector<double> fade_host;
@@ -250,6 +253,53 @@ bool obj_used(const img_config& c, int o) {
 }
 
 // MATLAB pchip on 5 knots (host copy for the fade coefficients of fade_shift.m:31).
+// MATLAB pchip(xk, yk, x) (Moler's pchiptx: harmonic-mean interior slopes, one-sided end slopes)
+// for a few knots, evaluated at one point (host; the point-fade map).
+double pchip_host(const double* xk, const double* yk, int n, double x) {
+    std::vector<double> h(n - 1), del(n - 1), d(n);
+    auto sg = [](double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); };
+    for (int k = 0; k < n - 1; ++k) { h[k] = xk[k + 1] - xk[k]; del[k] = (yk[k + 1] - yk[k]) / h[k]; }
+    for (int k = 1; k < n - 1; ++k) {
+        double w1 = 2 * h[k] + h[k - 1], w2 = h[k] + 2 * h[k - 1];
+        d[k] = sg(del[k - 1]) * sg(del[k]) > 0 ? (w1 + w2) / (w1 / del[k - 1] + w2 / del[k]) : 0.0;
+    }
+    auto endslope = [&](double h0, double h1, double d0, double d1) {
+        double dd = ((2 * h0 + h1) * d0 - h0 * d1) / (h0 + h1);
+        if (sg(dd) != sg(d0)) dd = 0.0;
+        else if (sg(d0) != sg(d1) && std::fabs(dd) > std::fabs(3 * d0)) dd = 3 * d0;
+        return dd;
+    };
+    d[0] = endslope(h[0], h[1], del[0], del[1]);
+    d[n - 1] = endslope(h[n - 2], h[n - 3], del[n - 2], del[n - 3]);
+    int k = 0;
+    for (int q = 0; q < n; ++q)
+        if (xk[q] <= x) k = q;
+    k = std::min(k, n - 2);
+    const double s = x - xk[k];
+    const double c1 = (d[k] + d[k + 1] - 2 * del[k]) / (h[k] * h[k]);
+    const double c2 = (3 * del[k] - 2 * d[k] - d[k + 1]) / h[k];
+    return ((c1 * s + c2) * s + d[k]) * s + yk[k];
+}
+
+// PointFade(grid, location, fadeSize).array (classes/PointFade.m:29-38): with r the offset of a cell from
+// the 1-based location, dist = max(s^2 - |r|^2, 0), the map is pchip([-1 0 1 2], [1 1 0 0], 1 - dist/max).
+std::vector<double> point_fade_map(const img_config& c) {
+    const long long n = (long long)c.grid[0] * c.grid[1] * c.grid[2];
+    std::vector<double> d(n), out(n);
+    double mx = -HUGE_VAL;
+    const double s = c.fade_size;
+    for (long long i = 0; i < n; ++i) {
+        const double x = (double)(i % c.grid[0]) + 1 - c.fade_location[0];
+        const double y = (double)((i / c.grid[0]) % c.grid[1]) + 1 - c.fade_location[1];
+        const double z = (double)(i / ((long long)c.grid[0] * c.grid[1])) + 1 - c.fade_location[2];
+        d[i] = std::max(s * s - (x * x + y * y + z * z), 0.0);
+        mx = std::max(mx, d[i]);
+    }
+    const double xk[4] = {-1, 0, 1, 2}, yk[4] = {1, 1, 0, 0};
+    for (long long i = 0; i < n; ++i) out[i] = pchip_host(xk, yk, 4, 1 - d[i] / mx);
+    return out;
+}
+
 std::vector<double> fade_coefficients(int f) {
     double xk[5] = {0, std::ceil(f / 4.0), std::floor(f / 2.0 + 0.5), double(f - 1), double(f)};
     double yk[5] = {1, 1, 0.01, 0, 0};
@@ -628,6 +678,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     a.tm = ctx->tm;
     a.gamma = c.gamma;
     a.minmass = c.minmass;
+    a.minmass_out = ctx->fade_mask ? -HUGE_VAL : c.minmass;   // the point-fade pass clamps
     a.dx = c.dgrid[d];
     a.limiter = c.limiter[d];
     for (int k = 0; k < 4; ++k) {
@@ -796,6 +847,8 @@ CflArgs cfl_args(img_ctx* ctx) {
     a.check_nonfinite = ctx->cfg.nonfinite_check != 0;
     a.accumulate = 1;
     a.rad_exp = ctx->cfg.rad_exponent;
+    a.fade_map = ctx->fade_map;
+    a.fade_ener = (ctx->fade_mask & IMG_FADE_ENER) ? 1 : 0;
     return a;
 }
 
@@ -865,8 +918,33 @@ int set_kernel_attributes(img_ctx* ctx) {
     return IMG_OK;
 }
 
+// The point-fade pass of one array assignment (var >= 0: img_upload) or of a fluid sweep's assignments.
+template <typename T>
+int launch_point_fade(img_ctx* ctx, int var) {
+    if (ctx->rec) return fail(ctx, IMG_ERR_UNSUPPORTED, "point fades in a batched launch");
+    FadeArgs a{};
+    a.n = ctx->g.ncell;
+    for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
+    a.map = ctx->fade_map;
+    a.mask = ctx->fade_mask;
+    a.var = var;
+    a.minmass = ctx->cfg.minmass;
+    a.tm = ctx->tm;
+    point_fade_kernel<T><<<launch_blocks(ctx->g.ncell), 256, 0, ctx->stream>>>(a);
+    CK(cudaGetLastError());
+    ctx->launches += 1;
+    return IMG_OK;
+}
+int point_fade(img_ctx* ctx, int var) {
+    return ctx->elem == 8 ? launch_point_fade<double>(ctx, var) : launch_point_fade<float>(ctx, var);
+}
+
+// relaxingFluid (fluid/relaxingFluid.m:16-73): the sweep, then with a point fade the pass that fades
+// its assignments to the primaries (the sweep leaves rho unclamped for it).
 int fluid_sweep(img_ctx* ctx, int X, bool cfl) {
-    return ctx->elem == 8 ? launch_fluid<double>(ctx, X - 1, cfl) : launch_fluid<float>(ctx, X - 1, cfl);
+    int rc = ctx->elem == 8 ? launch_fluid<double>(ctx, X - 1, cfl) : launch_fluid<float>(ctx, X - 1, cfl);
+    if (rc == IMG_OK && ctx->fade_mask) rc = point_fade(ctx, -1);
+    return rc;
 }
 int magnet_sweep(img_ctx* ctx, int X, int I1, int I2) {
     return ctx->elem == 8 ? launch_magnet<double>(ctx, X, I1, I2) : launch_magnet<float>(ctx, X, I1, I2);
@@ -914,6 +992,8 @@ int launch_treadmill(img_ctx* ctx) {
     a.means = ctx->tread_means;
     a.hist = ctx->tread_hist;
     a.hist_cap = kTreadHistCap;
+    a.fade_map = ctx->fade_map;
+    a.fade_mask = ctx->fade_mask;
     const long long ncol = g.ncell / g.n[d];
     const size_t smem = tread_smem_bytes(g.n[d], sizeof(T));
     if (d >= g.ndims) {   // ImogenArray.shift is not enabled along a third dimension of a 2-D grid
@@ -1007,13 +1087,22 @@ int time_update_async(img_ctx* ctx, int flux_direction) {
 // One iteration (imogen.m:60-66): time.update(1), flux(+1), time.update(2), flux(-1).
 // With radiation each timestep ends with source.m's sink (imogen.m:63-67), whose pass also collects
 // the CFL maxima that the next TimeManager.update reads (instead of the last fluid sweep).
+// Whether DevTime holds the CFL maxima of the state an iteration leaves: with a per-iteration dt the
+// last fluid sweep collects them, or, with radiation, the sink's pass; a treadmill or a point fade changes
+// the state after the last sweep, so without radiation nothing collects them.
+bool cfl_valid_after_iteration(const img_ctx* ctx) {
+    const bool rad = ctx->cfg.radiation_type != IMG_RAD_NONE;
+    const bool late = ctx->cfg.treadmill > 0 || ctx->fade_mask;
+    return ctx->cfg.update_mode != 0 && ctx->cfg.fluid_active && (rad || !late);
+}
+
 // The treadmill (imogen.m:64) moves the state after each flux, so with one the last fluid sweep
 // collects no CFL maxima either.
 int enqueue_iteration(img_ctx* ctx) {
     int rc;
     const bool per_iter = ctx->cfg.update_mode != 0;
     const bool rad = ctx->cfg.radiation_type != IMG_RAD_NONE;
-    const bool tread = ctx->cfg.treadmill > 0;
+    const bool tread = ctx->cfg.treadmill > 0 || ctx->fade_mask;   // the state changes after the last sweep
     const bool fl = ctx->cfg.fluid_active != 0;
     if ((rc = time_update_async(ctx, 1)) != IMG_OK) return rc;
     if ((rc = do_flux(ctx, 1, false)) != IMG_OK) return rc;
@@ -1026,7 +1115,7 @@ int enqueue_iteration(img_ctx* ctx) {
     if ((rc = do_flux(ctx, -1, per_iter && !rad && !tread)) != IMG_OK) return rc;
     if ((rc = treadmill_grid(ctx)) != IMG_OK) return rc;
     if (rad && (rc = source_sink(ctx, per_iter && fl)) != IMG_OK) return rc;
-    ctx->cfl_valid = per_iter && fl && (rad || !tread);
+    ctx->cfl_valid = cfl_valid_after_iteration(ctx);
     return IMG_OK;
 }
 
@@ -1056,6 +1145,15 @@ int validate(const img_config& c, std::string& why) {
     }
     if (c.radiation_type < IMG_RAD_NONE || c.radiation_type > IMG_RAD_OPTICALLY_THIN) { why = "unknown radiation type"; return IMG_ERR_ARG; }
     if (c.treadmill < 0 || c.treadmill > 3) { why = "treadmill direction must be 0 (off) or 1-3"; return IMG_ERR_ARG; }
+    if (c.fade_active & ~31) { why = "unknown point-fade array in fade_active"; return IMG_ERR_ARG; }
+    if (c.fade_active) {
+        if (!(c.fade_size > 0)) { why = "point fade: fade_size must be > 0"; return IMG_ERR_ARG; }
+        for (int d = 0; d < 3; ++d)
+            if (c.fade_location[d] < 1 || c.fade_location[d] > c.grid[d]) {
+                why = "point fade: fade_location must be a cell of the grid (1-based)";
+                return IMG_ERR_ARG;
+            }
+    }
     if (c.treadmill > 0 &&
         tread_smem_bytes(c.grid[c.treadmill - 1], c.precision == IMG_PREC_FP64 ? 8 : 4) > kPencilSmemLimit) {
         why = "treadmill: the pencils along its direction do not fit one thread block's shared memory";
@@ -1104,7 +1202,7 @@ int validate(const img_config& c, std::string& why) {
 
 // Device bytes: state + scratch + edges + tables.
 struct Layout {
-    size_t state, scratch, tm, table, fade, partial, stage, tread, dthist, edges, total;
+    size_t state, scratch, tm, table, fade, partial, stage, tread, dthist, fademap, edges, total;
     size_t edge_off[NOBJ][3][2];
 };
 
@@ -1137,7 +1235,8 @@ Layout plan(const img_config& c) {
             }
     L.edges = off;
     L.dthist = align256(sizeof(double) * dt_hist_cap(c));
-    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.tread + L.dthist + L.edges;
+    L.fademap = (c.fade_active & (IMG_FADE_MASS | IMG_FADE_MOM | IMG_FADE_ENER)) ? arr : 0;
+    L.total = L.state + L.scratch + L.tm + L.table + L.fade + L.partial + L.stage + L.tread + L.dthist + L.fademap + L.edges;
     return L;
 }
 
@@ -1295,6 +1394,11 @@ int img_create(img_ctx** out, const img_config* cfg) {
     p += L.tread;
     ctx->dt_hist = reinterpret_cast<double*>(p);
     p += L.dthist;
+    if (L.fademap) {
+        ctx->fade_map = p;
+        ctx->fade_mask = cfg->fade_active & (IMG_FADE_MASS | IMG_FADE_MOM | IMG_FADE_ENER);
+    }
+    p += L.fademap;
     char* edge_base = p;
     for (int o = 0; o < NOBJ; ++o)
         for (int e = 0; e < 3; ++e)
@@ -1325,6 +1429,20 @@ int img_create(img_ctx** out, const img_config* cfg) {
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         fail(ctx, IMG_ERR_CUDA, "device initialisation failed");
         return bail(IMG_ERR_CUDA);
+    }
+    if (ctx->fade_map) {   // ImogenManager.addFades builds the map from the grid alone (ImogenManager.m:267)
+        const std::vector<double> m = point_fade_map(*cfg);
+        cudaError_t e;
+        if (ctx->elem == 8) {
+            e = cudaMemcpy(ctx->fade_map, m.data(), sizeof(double) * m.size(), cudaMemcpyHostToDevice);
+        } else {
+            const std::vector<float> f(m.begin(), m.end());
+            e = cudaMemcpy(ctx->fade_map, f.data(), sizeof(float) * f.size(), cudaMemcpyHostToDevice);
+        }
+        if (e != cudaSuccess) {
+            fail(ctx, IMG_ERR_CUDA, "point-fade map upload failed: %s", cudaGetErrorString(e));
+            return bail(IMG_ERR_CUDA);
+        }
     }
     {
         const int rc = ctx->elem == 8 ? set_kernel_attributes<double>(ctx) : set_kernel_attributes<float>(ctx);
@@ -1387,10 +1505,20 @@ static int enqueue_download(img_ctx* ctx, int var, double* host, size_t n) {
     return IMG_OK;
 }
 
+// X.array = value fades a primary the point fade acts on (ImogenArray.m:85), except the initial
+// assignment of img_set_state.
+static int fade_assigned(img_ctx* ctx, int var) {
+    if (!ctx->fade_mask || ctx->constructing) return IMG_OK;
+    const int bit = var == IMG_VAR_MASS ? IMG_FADE_MASS
+                    : (var >= IMG_VAR_MOMX && var <= IMG_VAR_MOMZ ? IMG_FADE_MOM : (var == IMG_VAR_ENER ? IMG_FADE_ENER : 0));
+    return (ctx->fade_mask & bit) ? point_fade(ctx, var) : IMG_OK;
+}
+
 int img_upload(img_ctx* ctx, int var, const double* host, size_t n) {
     if (!ctx) return fail(ctx, IMG_ERR_ARG, "null context");
     int rc = enqueue_upload(ctx, var, host, n);
     if (rc != IMG_OK) return rc;
+    if ((rc = fade_assigned(ctx, var)) != IMG_OK) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
 }
@@ -1482,6 +1610,10 @@ int img_upload_many(img_ctx* ctx, int count, const int* var_ids, const double* c
             if (rc != IMG_OK) return rc;
         }
     }
+    for (int i = 0; i < count; ++i) {
+        int rc = fade_assigned(ctx, var_ids[i]);
+        if (rc != IMG_OK) return rc;
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     return IMG_OK;
 }
@@ -1515,6 +1647,8 @@ int img_set_state(img_ctx* ctx, const double* mass, const double* mom, const dou
     if (!ctx || !mass || !mom || !ener || !mag) return fail(ctx, IMG_ERR_ARG, "null state array");
     long long n = ctx->g.ncell;
     int rc;
+    ctx->constructing = true;   // FluidArray/MagnetArray construction: no fades on the initial arrays
+    struct Done { img_ctx* c; ~Done() { c->constructing = false; } } done{ctx};
     if ((rc = img_upload(ctx, IMG_VAR_MASS, mass, n)) != IMG_OK) return rc;
     for (int c = 0; c < 3; ++c)
         if ((rc = img_upload(ctx, IMG_VAR_MOMX + c, mom + c * n, n)) != IMG_OK) return rc;
@@ -1749,7 +1883,7 @@ int img_step(img_ctx* ctx) {
         }
         CK(cudaGraphLaunch(ctx->graphs[cv][row], ctx->stream));
         ctx->launches += ctx->graph_launches[cv][row];
-        ctx->cfl_valid = ctx->cfg.update_mode != 0 && ctx->cfg.fluid_active;
+        ctx->cfl_valid = cfl_valid_after_iteration(ctx);
         ctx->iteration += 1;
         return IMG_OK;
     }
@@ -2192,8 +2326,10 @@ int img_batch_add(img_batch* b, img_ctx* ctx) {
     if (!ctx->state_set) return bfail(b, IMG_ERR_STATE, "member state not set");
     if (ctx->batch) return bfail(b, IMG_ERR_STATE, "context is already a batch member");
     if (ctx->dev != b->dev) return bfail(b, IMG_ERR_ARG, "member is on device %d, batch on %d", ctx->dev, b->dev);
-    if (ctx->cfg.viscosity_type != IMG_VISC_NONE || ctx->cfg.radiation_type != IMG_RAD_NONE || ctx->cfg.treadmill > 0)
-        return bfail(b, IMG_ERR_UNSUPPORTED, "contexts with artificial viscosity, radiation or a treadmill do not join batches");
+    if (ctx->cfg.viscosity_type != IMG_VISC_NONE || ctx->cfg.radiation_type != IMG_RAD_NONE || ctx->cfg.treadmill > 0 ||
+        ctx->fade_mask)
+        return bfail(b, IMG_ERR_UNSUPPORTED,
+                     "contexts with artificial viscosity, radiation, a treadmill or a point fade do not join batches");
     if (!b->members.empty() && !same_signature(b->members[0], ctx))
         return bfail(b, IMG_ERR_ARG, "member differs from the batch in precision, physics, swept dimensions, "
                      "time update mode or iteration");
@@ -2240,7 +2376,7 @@ int img_batch_step(img_batch* b) {
         BCK(cudaGraphLaunch(cp.graph, b->stream));
         b->launches += cp.items.size();
         for (img_ctx* m : b->members) {
-            m->cfl_valid = m->cfg.update_mode != 0 && m->cfg.fluid_active;
+            m->cfl_valid = cfl_valid_after_iteration(m);
             m->iteration += 1;
         }
         b->steps += 1;

@@ -594,7 +594,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     }
 #pragma unroll
     for (int k = 0; k < C; ++k) {
-        unew[0][k] = unew[0][k] > (T)a.minmass ? unew[0][k] : (T)a.minmass;
+        unew[0][k] = unew[0][k] > (T)a.minmass_out ? unew[0][k] : (T)a.minmass_out;
         if (a.cfl && sp.colok) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
             double sp3[3];
             cfl_speeds(G, (double)unew[0][k], (double)unew[1][k], (double)unew[2][k], (double)unew[3][k],

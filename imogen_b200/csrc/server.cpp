@@ -65,7 +65,8 @@ Kind kind_of(const img_config& c) {
 }
 
 bool batchable(const img_config& c) {
-    return c.viscosity_type == IMG_VISC_NONE && c.radiation_type == IMG_RAD_NONE && c.treadmill <= 0;
+    return c.viscosity_type == IMG_VISC_NONE && c.radiation_type == IMG_RAD_NONE && c.treadmill <= 0 &&
+           !(c.fade_active & (IMG_FADE_MASS | IMG_FADE_MOM | IMG_FADE_ENER));
 }
 
 }  // namespace

@@ -38,6 +38,8 @@ struct TreadArgs {
     double* means;                 // first means (n2 values)
     int* hist;                     // TreadmillManager.history
     int hist_cap;
+    const void* fade_map;          // point-fade map (null: none) and the arrays it acts on (bits of
+    int fade_mask;                 // IMG_FADE_*: 1 rho, 2 momentum, 4 E): the shift's assignment fades them
 };
 
 __host__ __device__ inline size_t tread_smem_bytes(int N, size_t elem) { return 2 * (size_t)N * elem; }
@@ -206,7 +208,13 @@ __global__ void __launch_bounds__(256) treadmill_shift_kernel(const __grid_const
     double* slot = a.edge[arr][n >= 0 ? 1 : 0];
     line_shift<T>(L, S, N, n, a.mode[arr][side], a.neg[arr] != 0, a.act[arr], slot ? slot + col : nullptr, a.fade,
                   a.fade_f, a.bc_inf);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) A[b + i * a.sd] = S[i];
+    const int fbit = arr == 0 ? 1 : (arr <= 3 ? 2 : (arr == 4 ? 4 : 0));
+    const T* F = reinterpret_cast<const T*>(a.fade_map);
+    const bool fade = F && (a.fade_mask & fbit);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        const long long o = b + i * a.sd;
+        A[o] = fade ? point_fade(S[i], F[o]) : S[i];
+    }
 }
 
 }  // namespace img

@@ -135,7 +135,9 @@ def oracle_kwargs(settings):
                 update_mode=s.get("update_mode", 1), viscosity=s.get("viscosity", "empty"),
                 visc_linear=s.get("visc_linear", 0.0), visc_quadratic=s.get("visc_quadratic", 0.0),
                 radiation=s.get("radiation", "empty"), rad_exponent=s.get("rad_exponent", 0.5),
-                rad_initial_maximum=s.get("rad_initial_maximum", 0.0), treadmill=s.get("treadmill", 0))
+                rad_initial_maximum=s.get("rad_initial_maximum", 0.0), treadmill=s.get("treadmill", 0),
+                fade_location=s.get("fade_location"), fade_size=s.get("fade_size", 0.0),
+                fade_active=s.get("fade_active", ()))
 
 
 WORKLOADS = {

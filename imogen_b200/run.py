@@ -23,6 +23,7 @@ PRECISIONS = {"fp64": 0, "mixed": 1}
 # ENUM.ARTIFICIAL_VISCOSITY_* and ENUM.RADIATION_* (enums/ENUM.m)
 VISCOSITIES = {"empty": 0, "none": 0, "neumann_richtmyer": 1, "caramana_shashkov_whalen": 2}
 RADIATIONS = {"empty": 0, "none": 0, "optically_thin": 1}
+FADE_IDS = {"mass": 1, "mom": 2, "ener": 4, "mag": 8, "grav": 16}   # ENUM.MASS .. ENUM.GRAV of a fade's activeList
 VAR = dict(mass=0, momx=1, momy=2, momz=3, ener=4, magx=5, magy=6, magz=7, cmagx=8, cmagy=9, cmagz=10)
 
 
@@ -64,7 +65,8 @@ def bc_table(bc):
 def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ", bc_infinity=20,
                 limiter="vanleer", fluid=True, magnet=False, time_max=1e5, iter_max=10,
                 update_mode=1, precision="fp64", nonfinite_check=True, viscosity="empty", visc_linear=0.0,
-                visc_quadratic=0.0, radiation="empty", rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
+                visc_quadratic=0.0, radiation="empty", rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0,
+                fade_location=None, fade_size=0.0, fade_active=()):
     """img_config from Initializer-style settings (experiment/Initializer.m:73-184 defaults; run.viscosity
     and run.radiation as fluid/ArtificialViscosity.m:31-37 and fluid/Radiation.m:32-37 hold them)."""
     c = ImgConfig()
@@ -103,6 +105,11 @@ def make_config(grid, dgrid=None, gamma=5 / 3, cfl=None, minmass=1e-5, bc="circ"
     c.rad_exponent = float(rad_exponent)
     c.rad_initial_maximum = float(rad_initial_maximum)
     c.treadmill = int(treadmill)
+    if fade_location is not None:   # one point fade (ini.fades): the arrays it acts on, location, radius
+        c.fade_active = sum(FADE_IDS[name] for name in fade_active)
+        for d in range(3):
+            c.fade_location[d] = int(fade_location[d])
+        c.fade_size = float(fade_size)
     return c
 
 

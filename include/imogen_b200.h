@@ -40,6 +40,9 @@ enum { IMG_BC_CIRC = 0, IMG_BC_CONST = 1, IMG_BC_FADE = 2, IMG_BC_MIRROR = 3, IM
 enum { IMG_LIM_VANLEER = 0, IMG_LIM_SUPERBEE = 1, IMG_LIM_MINMOD = 2 };
 enum { IMG_CLS_MASS = 0, IMG_CLS_MOM = 1, IMG_CLS_ENER = 2, IMG_CLS_MAG = 3 };
 enum { IMG_PREC_FP64 = 0, IMG_PREC_MIXED = 1 };
+/* PointFade activeList entries (ImogenManager.addFades, classes/ImogenManager.m:262-280): only the
+ * FluidArray primaries read fades (FluidArray.m:54), so MAG and GRAV are accepted and have no effect */
+enum { IMG_FADE_MASS = 1, IMG_FADE_MOM = 2, IMG_FADE_ENER = 4, IMG_FADE_MAG = 8, IMG_FADE_GRAV = 16 };
 /* ArtificialViscosity.type (fluid/ArtificialViscosity.m:45-56) and Radiation.type (fluid/Radiation.m:43-55) */
 enum { IMG_VISC_NONE = 0, IMG_VISC_NEUMANN_RICHTMYER = 1, IMG_VISC_CARAMANA_SHASHKOV_WHALEN = 2 };
 enum { IMG_RAD_NONE = 0, IMG_RAD_OPTICALLY_THIN = 1 };
@@ -93,6 +96,15 @@ typedef struct img_config {
      * staged whole in shared memory (2 N values must fit one block); contexts with a treadmill take no
      * CUDA graph and do not join batches. */
     int treadmill;
+    /* ini.fades (initialize.m:336-341) with one point fade (the reference's addFades takes one):
+     * IMG_FADE_* mask of the arrays it acts on (0: none), its 1-based cell location and its radius in
+     * cells.  Every assignment to a faded primary -- the sweeps' updates, relaxingFluid's MINMASS clamp,
+     * the radiation sink, the treadmill's shift, img_upload / img_upload_many -- multiplies it by
+     * 1 - 0.05 A, A the PointFade map (classes/PointFade.m:29-49).  Contexts with a fade do not join
+     * batches. */
+    int fade_active;
+    int fade_location[3];
+    double fade_size;
 } img_config;
 
 typedef struct img_ctx img_ctx;

@@ -47,6 +47,7 @@ def lib():
         L.orc_magnet_flux.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.orc_iterate.argtypes = [ctypes.c_void_p]
         L.orc_source.argtypes = [ctypes.c_void_p]
+        L.orc_set_fade.argtypes = [ctypes.c_void_p, ip, ctypes.c_double, ctypes.c_int]
         L.orc_treadmill.argtypes = [ctypes.c_void_p]
         L.orc_set_treadmill.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_treadmill_history.argtypes = [ctypes.c_void_p, ip, ctypes.c_int]
@@ -120,7 +121,8 @@ class Sim:
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
                  magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
                  viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
-                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0,
+                 fade_location=None, fade_size=0.0, fade_active=()):
         self.grid = tuple(int(g) for g in grid)
         g = np.array(self.grid, dtype=np.int32)
         dg = np.array(dgrid, dtype=float)
@@ -135,6 +137,10 @@ class Sim:
                               float(visc_quadratic), {RAD_NONE: 0, RAD_THIN: 1}[radiation], float(rad_exponent),
                               float(rad_initial_maximum))
         lib().orc_set_treadmill(self._h, int(treadmill))
+        if fade_location is not None:
+            mask = sum(b for name, b in (("mass", 1), ("mom", 2), ("ener", 4)) if name in fade_active)
+            loc = np.array([int(v) for v in fade_location], dtype=np.int32)
+            lib().orc_set_fade(self._h, _ip(loc), float(fade_size), mask)
         self.TIMEMAX = float(time_max)
         self.ITERMAX = int(iter_max)
 

@@ -101,6 +101,7 @@ struct IArr {
     int component = 0;   // 0 scalar, 1..3
     int cls = 0;         // BC class
     int ftype = FT_NONE; // FluxArray type (zero_shift.m)
+    const Vec* fades = nullptr;   // PointFade map applied at every assignment (readFades; primaries)
     Vec a;
     bool uninit = true;
     Edges edges;
@@ -136,6 +137,10 @@ struct Sim {
     double rad_exp = 0.5, rad_initmax = 0, rad_strength = 1;
     // TreadmillManager (treadmill/TreadmillManager.m): direction (0 inactive), last, history
     int treadmill_dir = 0;
+    // one PointFade (ImogenManager.addFades, PointFade.m:29-38): the map and the fluid variables it acts
+    // on (bit 0 mass, 1 mom, 2 ener)
+    Vec fade_arr;
+    int fade_mask = 0;
     int treadmill_last = -1;
     std::vector<int> treadmill_history;
 
@@ -166,6 +171,10 @@ Vec take_face(const Sim& s, const Vec& a, int d, int idx) {
 }
 
 void IArr::set(Vec v) {
+    if (fades) {   // ImogenArray.applyFades -> PointFade.fadeArray (PointFade.m:46-49), before the edges
+        const Vec& A = *fades;
+        for (size_t k = 0; k < v.size(); ++k) v[k] = 0.95 * v[k] * A[k] + v[k] * (1 - A[k]);
+    }
     a = std::move(v);
     if (uninit) {   // Edges(bcModes, array, 0.005) at first assignment (Edges.m:37-110)
         for (int side = 0; side < 2; ++side)
@@ -943,6 +952,7 @@ void orc_set_physics(void* p, int visc_type, double visc_lin, double visc_quad, 
 int orc_set_state(void* p, const double* mass, const double* mom, const double* ener, const double* mag) {
     Sim& s = *static_cast<Sim*>(p);
     long long N = s.N;
+    for (int k = 0; k < 5; ++k) s.fv[k].prim.fades = nullptr;   // the initial assignment is not faded
     s.fv[0].prim.set(Vec(mass, mass + N));
     for (int c = 0; c < 3; ++c) s.fv[1 + c].prim.set(Vec(mom + c * N, mom + (c + 1) * N));
     s.fv[4].prim.set(Vec(ener, ener + N));
@@ -955,8 +965,32 @@ int orc_set_state(void* p, const double* mass, const double* mom, const double* 
         for (long long i = 0; i < N; ++i) sum += s.mg[c].prim.a[i];
         s.mg[c].isZero = (sum == 0) && !s.magnet_active;
     }
+    if (!s.fade_arr.empty()) {   // FluidArray.readFades after the initial assignment (FluidArray.m:54)
+        const int bit[5] = {1, 2, 2, 2, 4};
+        for (int k = 0; k < 5; ++k)
+            if (s.fade_mask & bit[k]) s.fv[k].prim.fades = &s.fade_arr;
+    }
     radiation_initialize(s);   // ImogenManager.initialize (imogen.m:46)
     return 0;
+}
+
+// PointFade(grid, location, fadeSize).array (classes/PointFade.m:29-38) and the variables it acts on.
+void orc_set_fade(void* p, const int location[3], double fade_size, int mask) {
+    Sim& s = *static_cast<Sim*>(p);
+    s.fade_mask = mask;
+    s.fade_arr.assign(s.N, 0.0);
+    Vec d(s.N);
+    double mx = -HUGE_VAL;
+    for (long long c = 0; c < s.N; ++c) {
+        const double x = (double)(c % s.n[0]) + 1 - location[0];
+        const double y = (double)((c / s.n[0]) % s.n[1]) + 1 - location[1];
+        const double z = (double)(c / ((long long)s.n[0] * s.n[1])) + 1 - location[2];
+        d[c] = std::max(fade_size * fade_size - (x * x + y * y + z * z), 0.0);
+        mx = std::max(mx, d[c]);
+    }
+    for (long long c = 0; c < s.N; ++c) d[c] = 1 - d[c] / mx;
+    const double xk[4] = {-1, 0, 1, 2}, yk[4] = {1, 1, 0, 0};
+    pchip_col(xk, 4, yk, d.data(), (int)s.N, s.fade_arr.data());
 }
 
 int orc_get_state(void* p, double* mass, double* mom, double* ener, double* mag, double* cellmag) {

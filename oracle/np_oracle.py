@@ -206,8 +206,12 @@ class IArray:
         if data is not None:
             self.set(data)
 
-    # set.array (ImogenArray.m:82-89): fades/statics are empty for these runs
+    # set.array (ImogenArray.m:82-89): point fades of the array (readFades, primaries only), then the
+    # first-assignment edges; statics cannot occur (StaticsInitializer.m does not parse: one `end` short)
     def set(self, value):
+        if getattr(self, "fades", None) is not None:   # PointFade.fadeArray (PointFade.m:46-49)
+            A = self.fades
+            value = 0.95 * value * A + value * (1 - A)
         self.a = value
         if self.uninitialized:
             self.edges = Edges(self.bc_modes, value, self.sim.ndims, 0.005)
@@ -253,6 +257,20 @@ def _circ_shift(a, DIRECT, n, obj):
 def _constant_shift(a, DIRECT, n, obj):
     d = DIRECT - 1
     return _take(a, _const_index(a.shape[d], n), d)              # constant_shift.m:21-29
+
+
+def point_fade_array(grid, location, fade_size):
+    """PointFade(grid, location, fadeSize).array (classes/PointFade.m:29-38): with r the offset of a cell
+    from `location` (1-based), d = max(s^2 - |r|^2, 0), the map pchip([-1 0 1 2], [1 1 0 0], 1 - d/max d):
+    1 at the location, 0 beyond the radius s."""
+    g = [int(v) for v in grid]
+    loc = [float(v) for v in location]
+    ax = [np.arange(1 - loc[i], g[i] - loc[i] + 1) for i in range(3)]
+    x, y, z = np.meshgrid(*ax, indexing="ij")
+    s = float(fade_size)
+    d = np.maximum(s * s - (x * x + y * y + z * z), 0)
+    d = 1 - d / float(np.max(d))
+    return pchip([-1, 0, 1, 2], np.array([1.0, 1.0, 0.0, 0.0]), d.reshape(-1, order="F")).reshape(g, order="F")
 
 
 def _mean_of_means(idx):
@@ -526,7 +544,8 @@ class Sim:
                  bc_infinity=20, limiter=(VANLEER,) * 3, fluid_active=True,
                  magnet_active=False, time_max=1e5, iter_max=10, update_mode=PER_ITERATION,
                  viscosity=VISC_NONE, visc_linear=0.0, visc_quadratic=0.0,
-                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0):
+                 radiation=RAD_NONE, rad_exponent=0.5, rad_initial_maximum=0.0, treadmill=0,
+                 fade_location=None, fade_size=0.0, fade_active=()):
         self.grid = tuple(int(g) for g in grid)
         self.ndims = 3 if self.grid[2] > 1 else 2
         self.dgrid = tuple(float(v) for v in dgrid)
@@ -561,6 +580,11 @@ class Sim:
         self.rad_strength = 1.0
         # TreadmillManager (treadmill/TreadmillManager.m): ini.treadmill > 0 activates it along that
         # direction (initialize.m:328-331); `last` starts at -1 and the history is kept
+        # one PointFade (ImogenManager.addFades, ImogenManager.m:262-280; classes/PointFade.m:29-38): the
+        # damping map and the ids of the arrays it acts on ('mass', 'mom', 'ener'; 'mag' and 'grav' are
+        # accepted there but no MagnetArray reads fades)
+        self.fade_array = point_fade_array(self.grid, fade_location, fade_size) if fade_location is not None else None
+        self.fade_active = tuple(fade_active)
         self.treadmill_dir = int(treadmill)
         self.treadmill_last = -1
         self.treadmill_history = []
@@ -575,6 +599,11 @@ class Sim:
         self.mag = [MagComp(self, i + 1, f(mag[i])) for i in range(3)]
         for i in range(3):
             self.mag[i].isZero = (np.sum(self.mag[i].prim.a) == 0) and not self.magnet_active
+        if self.fade_array is not None:   # FluidArray.readFades after the initial assignment (FluidArray.m:54)
+            for name, vs in (("mass", [self.mass]), ("mom", self.mom), ("ener", [self.ener])):
+                if name in self.fade_active:
+                    for v in vs:
+                        v.prim.fades = self.fade_array
         self.radiation_initialize()
 
     # ---------------------------------------------------------------------------------------

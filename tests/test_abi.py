@@ -142,3 +142,17 @@ def test_create_checks_the_treadmill_setting():
         h = ctypes.c_void_p()
         assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == code, kw
         assert b"treadmill" in L.img_last_error(None), kw
+
+
+def test_create_checks_the_point_fade_setting():
+    L = _lib.lib()
+    for kw in (dict(fade_location=(3, 3, 1), fade_size=2.0, fade_active=("mass",)),):
+        for bad in (dict(fade_location=(0, 3, 1)), dict(fade_location=(3, 40, 1)), dict(fade_size=0.0)):
+            c = make_config(grid=(32, 16, 1), **dict(kw, **bad))
+            h = ctypes.c_void_p()
+            assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -1, bad
+            assert b"fade" in L.img_last_error(None), bad
+    c = make_config(grid=(32, 16, 1))
+    c.fade_active = 64
+    h = ctypes.c_void_p()
+    assert L.img_create(ctypes.byref(h), ctypes.byref(c)) == -1

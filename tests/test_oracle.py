@@ -369,3 +369,41 @@ def test_treadmill_mean_and_round_follow_matlab():
     assert np_oracle._mean_of_means(np.array([[5.0, 6.0]])) == 5.5
     assert np_oracle._matlab_round(2.5) == 3 and np_oracle._matlab_round(-2.5) == -3
     assert np_oracle._matlab_round(0.49999999999999994) == 0
+
+
+@pytest.mark.parametrize("grid,bc,active,extra", [
+    ((24, 20, 1), "circ", ("mass", "mom", "ener"), {}),
+    ((24, 20, 1), "trans", ("mass",), dict(radiation="optically_thin", rad_initial_maximum=0.1)),
+    ((14, 12, 10), "const", ("mom", "ener", "mag"), {}),
+    ((40, 6, 1), {"x": "fade", "y": "circ", "z": "circ"}, ("mass", "ener"), dict(treadmill=1, iter_max=14))])
+def test_point_fade_oracles_bitwise(grid, bc, active, extra):
+    """One PointFade (classes/PointFade.m) acting at every assignment of the chosen primaries."""
+    s = dict(grid=grid, dgrid=tuple(1 / g for g in grid), cfl=0.35, bc=bc, magnet=True, iter_max=5,
+             fade_location=(grid[0] // 2, grid[1] // 3, max(1, grid[2] // 2)), fade_size=5.0, fade_active=active)
+    s.update(extra)
+    kw = problems.oracle_kwargs(s)
+    st = _shock_tube(grid) if "treadmill" in extra else smooth_state(grid, seed=2, mhd=True)
+    a = np_oracle.Sim(**kw)
+    a.set_state(*st)
+    b = cpp_oracle.Sim(**kw)
+    b.set_state(*st)
+    assert np.array_equal(a.mass.prim.a, np.asarray(st[0], dtype=float))   # the initial arrays are not faded
+    a.run()
+    b.run()
+    sa, sb = a.state(), b.state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+    ref = np_oracle.Sim(**problems.oracle_kwargs(dict(s, fade_location=None)))
+    ref.set_state(*st)
+    ref.run()
+    assert np.abs(ref.state()["ener"] - sa["ener"]).max() > 1e-6       # the fade changes the run
+
+
+def test_point_fade_map():
+    """pchip([-1 0 1 2], [1 1 0 0], t) is 1 - 3t^2 + 2t^3 on [0, 1]: 1 at the location, 0 at and beyond
+    the radius."""
+    A = np_oracle.point_fade_array((20, 16, 1), (6, 9, 1), 4.0)
+    assert A[5, 8, 0] == 1.0 and A[5 + 4, 8, 0] == 0.0 and A[0, 0, 0] == 0.0
+    r2 = 2.0 ** 2 + 1.0 ** 2
+    t = 1 - (16 - r2) / 16
+    assert A[7, 9, 0] == pytest.approx(1 - 3 * t * t + 2 * t ** 3, rel=1e-14)
