@@ -6,7 +6,8 @@
  *
  *   h = imogen_b200_mex('create', grid, dgrid, gamma, cfl, minmass, bcinf, bcmodes, limiter,
  *                       fluid, magnet, timemax, itermax, updatemode, precision
- *                       [, visc, visclin, viscquad, rad, radexp, radmax, treadmill])
+ *                       [, visc, visclin, viscquad, rad, radexp, radmax, treadmill
+ *                        [, fademask, fadelocation, fadesize]])
  *   imogen_b200_mex('set_state', h, mass, mom, ener, mag)     % FluidArray/MagnetArray setup
  *   imogen_b200_mex('upload', h, varid, array)                % X.array = ...
  *   a = imogen_b200_mex('download', h, varid)                 % X.array
@@ -53,7 +54,8 @@ static void check(int rc, img_ctx* ctx) {
 
 static double scalar(const mxArray* a) { return mxGetScalar(a); }
 
-/* img_config from the create arguments prhs[0..n-1] (n = 14, or 21 with the physics settings). */
+/* img_config from the create arguments prhs[0..n-1] (n = 14, 21 with the physics settings, 24 with a
+ * point fade as well). */
 static void read_config(img_config* c, const mxArray* const* a, int n) {
     const double *grid, *dg, *bc, *lim;
     int i, k, s, d;
@@ -77,7 +79,7 @@ static void read_config(img_config* c, const mxArray* const* a, int n) {
     c->iter_max = (int)scalar(a[11]);
     c->update_mode = (int)scalar(a[12]);
     c->precision = (int)scalar(a[13]);
-    if (n == 21) {   /* run.viscosity, run.radiation, ini.treadmill */
+    if (n >= 21) {   /* run.viscosity, run.radiation, ini.treadmill */
         c->viscosity_type = (int)scalar(a[14]);
         c->visc_linear = scalar(a[15]);
         c->visc_quadratic = scalar(a[16]);
@@ -85,6 +87,12 @@ static void read_config(img_config* c, const mxArray* const* a, int n) {
         c->rad_exponent = scalar(a[18]);
         c->rad_initial_maximum = scalar(a[19]);
         c->treadmill = (int)scalar(a[20]);
+    }
+    if (n == 24) {   /* ini.fades with one point fade: IMG_FADE_* mask, 1-based location, radius */
+        const double* loc = mxGetPr(a[22]);
+        c->fade_active = (int)scalar(a[21]);
+        for (i = 0; i < 3; ++i) c->fade_location[i] = (int)loc[i];
+        c->fade_size = scalar(a[23]);
     }
 }
 
@@ -113,7 +121,7 @@ static int server_command(const char* cmd, int nlhs, mxArray* plhs[], int nrhs, 
     } else if (!strcmp(cmd, "submit")) {
         img_config c;
         int job = -1, ncfg = nrhs - 6;
-        if (ncfg != 14 && ncfg != 21) mexErrMsgIdAndTxt("imogen_b200:arg", "submit(s, <create arguments>, mass, mom, ener, mag)");
+        if (ncfg != 14 && ncfg != 21 && ncfg != 24) mexErrMsgIdAndTxt("imogen_b200:arg", "submit(s, <create arguments>, mass, mom, ener, mag)");
         read_config(&c, prhs + 2, ncfg);
         rc = img_batch_submit((img_server*)ptr(prhs[1]), &c, mxGetPr(prhs[nrhs - 4]), mxGetPr(prhs[nrhs - 3]),
                               mxGetPr(prhs[nrhs - 2]), mxGetPr(prhs[nrhs - 1]), &job);
@@ -165,7 +173,7 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     if (!strcmp(cmd, "create")) {
         img_config c;
         img_ctx* ctx = NULL;
-        if (nrhs != 15 && nrhs != 22) mexErrMsgIdAndTxt("imogen_b200:arg", "create takes 14 or 21 arguments");
+        if (nrhs != 15 && nrhs != 22 && nrhs != 25) mexErrMsgIdAndTxt("imogen_b200:arg", "create takes 14, 21 or 24 arguments");
         read_config(&c, prhs + 1, nrhs - 1);
         check(img_create(&ctx, &c), NULL);
         plhs[0] = handle_out(ctx);
