@@ -3,23 +3,28 @@ corrugation_jumps.json beside this script.
 
 Each file holds one stationary-shock solution of the reference's MHDJumpSolver (pre- and
 post-shock density, pressure, velocity and magnetic field, in the shock frame) for a sonic Mach
-number, Alfven Mach number, field angle and gamma; the values are copied as they are.  Run in a
-container where the reference tree is mounted (reads REFERENCE_ROOT, default /root/reference);
-the JSON is committed so the tests do not need the reference at run time."""
+number, Alfven Mach number, field angle and gamma; the values are copied as they are.  Usage:
+
+    python tests/golden/make_corrugation_fixture.py <root of the reference tree>
+
+The JSON is committed so the tests do not need the reference at run time."""
 import glob
 import json
 import os
+import sys
 
 import numpy as np
 import scipy.io
 
-ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
-def main():
+def main(root):
     out = []
-    for path in sorted(glob.glob(os.path.join(ROOT, "experiment", "CorrugationShock", "data", "ics-*.mat"))):
+    paths = sorted(glob.glob(os.path.join(root, "experiment", "CorrugationShock", "data", "ics-*.mat")))
+    if not paths:
+        raise SystemExit(f"no experiment/CorrugationShock/data/ics-*.mat under {root}")
+    for path in paths:
         r = scipy.io.loadmat(path)["result"][0, 0]
         names = r.dtype.names
         base = os.path.basename(path)
@@ -40,4 +45,6 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_corrugation_fixture.py <root of the reference tree>")
+    main(sys.argv[1])
