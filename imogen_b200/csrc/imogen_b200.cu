@@ -414,19 +414,20 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d, size_t elem) {
     return out;
 }
 
-// Segment tilings of the fluid sweep (seg_fluid.cuh): C consecutive cells per thread (2, 4 or 8; 2 or 4
-// in FP64), the whole pencil in one CTA of NT = Wb * S threads, 64 <= NT <= 512, S = N / C threads per
-// pencil.  Along x the S threads of a pencil are consecutive lanes: S is a power of two up to 32 or a
-// multiple of 32.  Along y and z Wb >= 4 pencils (a power of two) sit side by side.
+// Segment tilings of the fluid sweep (seg_fluid.cuh): C consecutive cells per thread (2, 3, 4 or 8; 2,
+// 3 or 4 in FP64; 2 or 4 with artificial viscosity), the whole pencil in one CTA of NT = Wb * S threads,
+// 64 <= NT <= 512, S = N / C threads per pencil.  Along x the S threads of a pencil are consecutive
+// lanes: S is a power of two up to 32 or a multiple of 32.  Along y and z Wb >= 4 pencils (a power of
+// two) sit side by side, at most 32 of them unless each pencil is one thread's (S = 1).
 std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool visc = false) {
     std::vector<PencilCfg> out;
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
-    for (int C : {2, 4, 8}) {
-        if ((elem == 8 && C == 8) || (visc && C == 8) || N % C) continue;
+    for (int C : {2, 3, 4, 8}) {
+        if ((elem == 8 && C == 8) || (visc && (C == 8 || C == 3)) || N % C) continue;
         const int S = N / C;
         if (d == 0 && !(S % 32 == 0 || (S <= 32 && 32 % S == 0))) continue;
-        for (int Wb = d == 0 ? 1 : 4; Wb <= 32; Wb *= 2) {
+        for (int Wb = d == 0 ? 1 : 4; Wb <= (d != 0 && S == 1 ? 512 : 32); Wb *= 2) {
             const int NT = Wb * S;
             if (NT > 512) break;
             if (NT < 64 || NT % 32) continue;
@@ -446,17 +447,18 @@ std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool vi
     return out;
 }
 
-// Window tilings of the magnet chain and CT pass (seg_magnet.cuh): C = 2, 4 or 8 consecutive cells per
+// Window tilings of the magnet chain and CT pass (seg_magnet.cuh): C = 2, 3, 4 or 8 consecutive cells per
 // thread with C dividing N, S = N / C threads per pencil, the whole pencil in one CTA of NT = Wb * S
-// threads (32 <= NT <= 512, a multiple of 32); along y and z Wb >= 4 pencils side by side.
+// threads (32 <= NT <= 512, a multiple of 32); along y and z Wb >= 4 pencils side by side (up to 64, or
+// to the CTA where each pencil is one thread's).
 std::vector<PencilCfg> win_candidates(const Geom& g, int d) {
     std::vector<PencilCfg> out;
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
-    for (int C : {2, 4, 8}) {
+    for (int C : {2, 3, 4, 8}) {
         if (N % C) continue;
         const int S = N / C;
-        for (int Wb = d == 0 ? 1 : 4; Wb <= 64; Wb *= 2) {
+        for (int Wb = d == 0 ? 1 : 4; Wb <= (d != 0 && S == 1 ? 512 : 64); Wb *= 2) {
             const int NT = Wb * S;
             if (NT > 512) break;
             if (NT < 32 || NT % 32) continue;
@@ -474,30 +476,38 @@ std::vector<PencilCfg> win_candidates(const Geom& g, int d) {
     return out;
 }
 
-// Default magnet tiling: the window kernels where a window tiling exists (4 cells per thread, along y
-// and z at least 8 pencils side by side, the CTA nearest 256 threads), else the tile kernels' default.
-PencilCfg choose_window(const Geom& g, int d, const PencilCfg& tile) {
+// Default segment or window tiling among candidates c: 4 cells per thread (along y and z at least 8
+// pencils side by side), else whole pencils of one thread each (pencils of 2 to 8 cells across y or z);
+// the CTA nearest 256 threads.  nullptr: none of these.
+const PencilCfg* default_segments(const std::vector<PencilCfg>& c, int d) {
     const PencilCfg* best = nullptr;
-    std::vector<PencilCfg> c = win_candidates(g, d);
     for (const PencilCfg& p : c) {
         if (p.seg != 4 || (d != 0 && p.Wb < 8)) continue;
         if (!best || std::abs(p.NT - 256) < std::abs(best->NT - 256)) best = &p;
     }
+    if (best || d == 0) return best;
+    for (const PencilCfg& p : c) {
+        if (p.G != 1) continue;
+        if (!best || std::abs(p.NT - 256) < std::abs(best->NT - 256)) best = &p;
+    }
+    return best;
+}
+
+// Default magnet tiling: the window kernels where a default window tiling exists, else the tile
+// kernels' default.
+PencilCfg choose_window(const Geom& g, int d, const PencilCfg& tile) {
+    std::vector<PencilCfg> c = win_candidates(g, d);
+    const PencilCfg* best = default_segments(c, d);
     return best ? *best : tile;
 }
 
-// Default fluid tiling: in the mixed form the segment kernel where a segment tiling exists (4 cells per
-// thread, along y and z at least 8 pencils side by side, the CTA nearest 256 threads); in FP64, and where
-// no segment tiling exists, the tile kernels' default (the FP64 segment kernel needs more registers than
-// it has; the autotuner may still pick it).
+// Default fluid tiling: in the mixed form the segment kernel where a default segment tiling exists
+// (default_segments); in FP64, and where none exists, the tile kernels' default (the FP64 segment kernel
+// needs more registers than it has; the autotuner may still pick it).
 PencilCfg choose_fluid(const Geom& g, int d, size_t elem, const PencilCfg& tile) {
     if (elem == 8) return tile;
-    const PencilCfg* best = nullptr;
     std::vector<PencilCfg> c = seg_candidates(g, d, elem);
-    for (const PencilCfg& p : c) {
-        if (p.seg != 4 || (d != 0 && p.Wb < 8)) continue;
-        if (!best || std::abs(p.NT - 256) < std::abs(best->NT - 256)) best = &p;
-    }
+    const PencilCfg* best = default_segments(c, d);
     return best ? *best : tile;
 }
 
@@ -2508,8 +2518,7 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) double g_static_totals[kStaticTotalsDoubles];
 static_assert(sizeof(g_static_totals) == 128 * 1024, "static totals scratch is 128 KiB");
 
-// Address of g_static_totals on the current device, looked up once per device.  The lookup may load
-// the module, so the first call on a device should come before any stream capture begins.
+// Address of g_static_totals on the current device, looked up once per device.
 static int static_totals_scratch(img_ctx* ctx, double** out) {
     static std::mutex mu;
     static double* addr[kMaxDevices] = {};
@@ -2532,6 +2541,11 @@ static int static_totals_scratch(img_ctx* ctx, double** out) {
 
 int img_totals_static(img_ctx* ctx, double out[8]) {
     if (!ctx || !out) return fail(ctx, IMG_ERR_ARG, "null argument");
+    // it copies from a host stack array and synchronises: neither may be captured into a graph
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone)
+        return fail(ctx, IMG_ERR_STATE, "img_totals_static cannot run while the context's stream is captured");
     double* scratch = nullptr;
     int rc = static_totals_scratch(ctx, &scratch);
     if (rc != IMG_OK) return rc;

@@ -325,11 +325,13 @@ __device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], c
 // pencil inside the warp and leave the warp's value in pm where a pencil spans warps; collect, after
 // a barrier, reduces those.  Along x the S segments of a pencil are consecutive lanes (S a power of
 // two below 32, or a multiple of 32); along y and z the lanes of pencil b are b, b + Wb, ... (Wb a
-// power of two).
+// power of two, at most 32 when S > 1).  With S = 1 (a short pencil held whole by one thread, Wb up to
+// the CTA) the thread's own maximum is the pencil's.
 template <typename T>
 __device__ __forceinline__ T seg_max_publish(const SweepGeom& g, T v, T* pm) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned full = 0xffffffffu;
+    if (g.G == 1) return v;
     if (g.d == 0) {
         if (g.G >= 32) {
             v = warp_max_nonneg(v);
@@ -347,6 +349,7 @@ __device__ __forceinline__ T seg_max_publish(const SweepGeom& g, T v, T* pm) {
 template <typename T>
 __device__ __forceinline__ T seg_max_collect(const SweepGeom& g, int b, T wv, const T* pm) {
     const int lane = threadIdx.x & 31;
+    if (g.G == 1) return wv;
     if (g.d == 0) {
         if (g.G < 32) return wv;
         const int w0 = (b * g.G) >> 5, nw = g.G >> 5;

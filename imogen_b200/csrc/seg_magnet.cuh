@@ -34,9 +34,19 @@ __device__ __forceinline__ long long trans_offset(int ie, int ne, long long se, 
 }
 
 // Global row of window cell j of segment s (rows r0 + j, wrapped for circ, clamped for const ends).
+// The window reaches at most 4 rows past a segment, so a pencil shorter than that wraps more than once
+// (r >= -4 and r < N + C + 4: the loops run at most a few times).
 __device__ __forceinline__ int win_row(int r, int N, bool circ_lo, bool circ_hi) {
-    if (r < 0) return circ_lo ? r + N : 0;
-    if (r >= N) return circ_hi ? r - N : N - 1;
+    if (r < 0) {
+        if (!circ_lo) return 0;
+        do r += N; while (r < 0);
+        return r;
+    }
+    if (r >= N) {
+        if (!circ_hi) return N - 1;
+        do r -= N; while (r >= N);
+        return r;
+    }
     return r;
 }
 

@@ -152,12 +152,14 @@ void (*chain_batch_kernel(int cpt, int nqc, int v))(const MagArgs*, const BlockM
 // The CT kernel captures no stored edges: its variant ignores `init` (0 jobs, 1 fade, 2 cg, 3 both).
 inline int ct_variant(bool fade, bool cg) { return (fade ? 1 : 0) | (cg ? 2 : 0); }
 
-// Segment fluid kernels by cells per thread (FP64: 2 and 4).
+// Segment fluid kernels by cells per thread (2, 3, 4 and 8; FP64: 2, 3 and 4).  3 serves pencils of
+// 3 cells held whole by one thread.
 template <typename T, bool MHD>
 void (*fluid_seg_kernel_c(int C))(const FluidArgs) {
     if constexpr (sizeof(T) == 4) {
         if (C == 8) return fluid_seg_kernel<T, MHD, 8>;
     }
+    if (C == 3) return fluid_seg_kernel<T, MHD, 3>;
     return C == 2 ? fluid_seg_kernel<T, MHD, 2> : fluid_seg_kernel<T, MHD, 4>;
 }
 
@@ -166,6 +168,7 @@ void (*fluid_seg_batch_kernel_c(int C))(const FluidArgs*, const BlockMap*) {
     if constexpr (sizeof(T) == 4) {
         if (C == 8) return fluid_seg_batch_kernel<T, MHD, 8>;
     }
+    if (C == 3) return fluid_seg_batch_kernel<T, MHD, 3>;
     return C == 2 ? fluid_seg_batch_kernel<T, MHD, 2> : fluid_seg_batch_kernel<T, MHD, 4>;
 }
 
@@ -194,21 +197,25 @@ cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map,
     return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
 }
 
-// Window magnet kernels by cells per thread (2, 4, 8).
+// Window magnet kernels by cells per thread (2, 3, 4, 8).
 template <typename T>
 void (*chain_win_kernel(int C))(const MagArgs) {
+    if (C == 3) return mag_chain_win_kernel<T, 3>;
     return C == 2 ? mag_chain_win_kernel<T, 2> : (C == 8 ? mag_chain_win_kernel<T, 8> : mag_chain_win_kernel<T, 4>);
 }
 template <typename T>
 void (*ct_win_kernel(int C))(const MagArgs) {
+    if (C == 3) return mag_ct_win_kernel<T, 3>;
     return C == 2 ? mag_ct_win_kernel<T, 2> : (C == 8 ? mag_ct_win_kernel<T, 8> : mag_ct_win_kernel<T, 4>);
 }
 template <typename T>
 void (*chain_win_batch_kernel(int C))(const MagArgs*, const BlockMap*) {
+    if (C == 3) return mag_chain_win_batch_kernel<T, 3>;
     return C == 2 ? mag_chain_win_batch_kernel<T, 2> : (C == 8 ? mag_chain_win_batch_kernel<T, 8> : mag_chain_win_batch_kernel<T, 4>);
 }
 template <typename T>
 void (*ct_win_batch_kernel(int C))(const MagArgs*, const BlockMap*) {
+    if (C == 3) return mag_ct_win_batch_kernel<T, 3>;
     return C == 2 ? mag_ct_win_batch_kernel<T, 2> : (C == 8 ? mag_ct_win_batch_kernel<T, 8> : mag_ct_win_batch_kernel<T, 4>);
 }
 
@@ -303,13 +310,13 @@ cudaError_t fluid_attributes(int cpt, int optin) {
 
 template <typename T>
 cudaError_t fluid_seg_attributes(int optin) {
-    for (int C : {2, 4, 8}) {
+    for (int C : {2, 3, 4, 8}) {
         if (sizeof(T) == 8 && C == 8) continue;
         for (int mhd = 0; mhd < 2; ++mhd) {
             cudaError_t e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0), optin);
             if (e == cudaSuccess) e = allow_max_smem(fluid_seg_batch_kernel_p<T>(C, mhd != 0), optin);
             for (int vt : {VISC_NR, VISC_CSW})
-                if (e == cudaSuccess && C <= 4) e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0, vt), optin);
+                if (e == cudaSuccess && (C == 2 || C == 4)) e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0, vt), optin);
             if (e != cudaSuccess) return e;
         }
     }

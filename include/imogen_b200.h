@@ -292,9 +292,9 @@ int img_totals(img_ctx* ctx, double out[8]);
  * allocator, or a host that has fixed its device footprint up front).  The scratch is a file-scope
  * device array of 128 KiB (16384 doubles: 1023 per-block partial pairs of 8 variables, the 8 results
  * and an 8-entry pointer table), looked up once per device with cudaGetSymbolAddress; grids of any
- * size.  The first call on a device does that lookup and should come before any stream capture
- * begins.  Each call copies the pointer table from the host, synchronises the context's stream and
- * copies the 8 results to `out` before it returns.  Every call overwrites all the scratch it reads,
+ * size.  Each call copies the pointer table from the host, synchronises the context's stream and
+ * copies the 8 results to `out` before it returns, so it cannot be captured into a graph: while the
+ * context's stream is capturing it returns IMG_ERR_STATE and does nothing.  Every call overwrites all the scratch it reads,
  * so nothing needs to start at zero.  All contexts of a device share that scratch: calls that
  * overlap in time race on it and must be serialised by the caller.  The context's device must be
  * current.  No counterpart in the reference. */

@@ -40,8 +40,11 @@ def test_autotune_keeps_state_and_results(precision, case):
         tuned.iterate()
         plain.iterate()
     a, b = tuned.state(), plain.state()
-    same_family = all(x[6] == y[6] for x, y in zip(tuned.tiling().values(), plain.tiling().values()))
-    tol = 0.0 if same_family else (1e-13 if precision == "fp64" else 1e-6)
+    # bit for bit where both runs use the same kernel instantiations (family and cells per thread, fluid
+    # and magnet); other instantiations may contract their sums into FMAs differently
+    same_kernels = all(x[4] == y[4] and x[6] == y[6] for kind in ("fluid", "magnet")
+                       for x, y in zip(tuned.tiling(kind).values(), plain.tiling(kind).values()))
+    tol = 0.0 if same_kernels else (1e-13 if precision == "fp64" else 1e-6)
     for k in a:
         rel = float(np.abs(a[k] - b[k]).sum() / max(np.abs(b[k]).sum(), 1e-300))
         assert rel <= tol, (k, rel, tuned.tiling(), plain.tiling())

@@ -53,3 +53,26 @@ def test_static_totals_alternating_contexts():
     finally:
         a.close()
         b.close()
+
+
+def test_static_totals_refuse_a_capturing_stream():
+    """The call copies from host memory and synchronises, which a graph capture cannot hold: while
+    the context's stream captures it fails with IMG_ERR_STATE and enqueues nothing."""
+    from cuda.bindings import runtime as rt
+    from imogen_b200 import ImogenError
+    g = _run(24, "fp64", 1)
+    try:
+        want = g.totals()
+        st = rt.cudaStream_t(g.stream)
+        err, = rt.cudaStreamBeginCapture(st, rt.cudaStreamCaptureMode.cudaStreamCaptureModeThreadLocal)
+        assert err == rt.cudaError_t.cudaSuccess
+        try:
+            with pytest.raises(ImogenError, match="captured"):
+                g.totals_static()
+        finally:
+            err, graph = rt.cudaStreamEndCapture(st)
+            assert err == rt.cudaError_t.cudaSuccess
+            rt.cudaGraphDestroy(graph)
+        np.testing.assert_array_equal(g.totals_static(), want)
+    finally:
+        g.close()
