@@ -450,27 +450,46 @@ std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool vi
 // Window tilings of the magnet chain and CT pass (seg_magnet.cuh): C = 2, 3, 4 or 8 consecutive cells per
 // thread with C dividing N, S = N / C threads per pencil, the whole pencil in one CTA of NT = Wb * S
 // threads (32 <= NT <= 512, a multiple of 32); along y and z Wb >= 4 pencils side by side (up to 64, or
-// to the CTA where each pencil is one thread's).
+// to the CTA where each pencil is one thread's).  Along x, for a C where no such tiling exists, the
+// padded ones: S = ceil(N / C) segments (the last one ragged), NT = Wb * S rounded up to a multiple of
+// 32 with the threads past the segments idle, and for S above 256 (512) segments one pencil over a
+// cluster of CL = ceil(S / 256) <= 8 CTAs (ceil(S / 512) <= 4) of NT = ceil(S / CL) rounded up.
 std::vector<PencilCfg> win_candidates(const Geom& g, int d) {
     std::vector<PencilCfg> out;
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
+    auto add = [&](int Wb, int S, int CL, int NT, int C) {
+        PencilCfg p;
+        p.Wb = Wb;
+        p.G = S;
+        p.CL = CL;
+        p.NT = NT;
+        p.cpt = C;
+        p.seg = C;
+        out.push_back(p);
+    };
     for (int C : {2, 3, 4, 8}) {
-        if (N % C) continue;
-        const int S = N / C;
-        for (int Wb = d == 0 ? 1 : 4; Wb <= (d != 0 && S == 1 ? 512 : 64); Wb *= 2) {
-            const int NT = Wb * S;
-            if (NT > 512) break;
-            if (NT < 32 || NT % 32) continue;
+        const size_t before = out.size();
+        if (N % C == 0) {
+            const int S = N / C;
+            for (int Wb = d == 0 ? 1 : 4; Wb <= (d != 0 && S == 1 ? 512 : 64); Wb *= 2) {
+                const int NT = Wb * S;
+                if (NT > 512) break;
+                if (NT < 32 || NT % 32) continue;
+                if (Wb > 1 && (long long)Wb / 2 >= ncol) break;
+                add(Wb, S, 1, NT, C);
+            }
+        }
+        if (d != 0 || out.size() > before || C == 3) continue;
+        const int S = (N + C - 1) / C;
+        for (int Wb = 1; Wb * S <= 512; Wb *= 2) {
             if (Wb > 1 && (long long)Wb / 2 >= ncol) break;
-            PencilCfg p;
-            p.Wb = Wb;
-            p.G = S;
-            p.CL = 1;
-            p.NT = NT;
-            p.cpt = C;
-            p.seg = C;
-            out.push_back(p);
+            add(Wb, S, 1, std::max(32, (Wb * S + 31) / 32 * 32), C);
+        }
+        for (int cap : {256, 512}) {
+            const int CL = (S + cap - 1) / cap;
+            if (CL < 2 || CL > (cap == 256 ? 8 : 4)) continue;
+            add(1, S, CL, ((S + CL - 1) / CL + 31) / 32 * 32, C);
         }
     }
     return out;

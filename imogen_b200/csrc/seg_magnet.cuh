@@ -16,8 +16,12 @@
 // Pencil ends along X (mag-class BC): circ wraps the window; const makes every shifted array take its
 // own end value (constant_shift.m), so after each stage the window cells beyond the pencil's end copy
 // the stage's value at the end cell.  Transverse shifts (along I) use circ or const too; other
-// boundaries, pencils longer than a CTA and a run's first sweeps (stored-edge capture) take the tile
-// kernels (magnet_sweep.cuh).  Per cell the arithmetic is that of the tile kernels.
+// boundaries and a run's first sweeps (stored-edge capture) take the tile kernels (magnet_sweep.cuh).
+// Per cell the arithmetic is that of the tile kernels.
+// Along x a pencil's length need not be a multiple of C (the last segment is ragged: S = ceil(N / C)
+// segments, threads past them idle), and a pencil longer than one CTA's segments spans the CTAs of a
+// thread-block cluster (one pencil per cluster; segment s = rank * NT + thread), whose barrier then
+// separates the reads from the in-place writes.
 #pragma once
 
 #include "seg_fluid.cuh"
@@ -64,24 +68,36 @@ __device__ __forceinline__ void const_fill(T* A, bool fill_lo, bool fill_hi) {
     }
 }
 
-// The segment placement of seg_fluid.cuh plus the pencil's coordinates along the transverse dims.
+// The segment placement of seg_fluid.cuh plus the pencil's coordinates along the transverse dims; G is
+// the pencil's segment count S, over the CL CTAs of a cluster where CL > 1.
 struct WinPos {
     int b, s, c1, c2;
     bool colok;
     long long base;
     __device__ __forceinline__ void init(const SweepGeom& g, unsigned vblock) {
-        const int t = threadIdx.x;
+        int t = threadIdx.x;
+        unsigned blk = vblock;
+        if (g.CL > 1) {   // cluster rank r holds segments r * NT .. r * NT + NT - 1 of the bundle's pencil
+            blk = g.div_cl.div(vblock);
+            t += (int)(vblock - blk * (unsigned)g.CL) * g.NT;
+        }
         const unsigned q = g.div_lanes.div((unsigned)t);
         if (g.d == 0) { b = (int)q; s = t - b * g.G; }
         else { s = (int)q; b = t - s * g.Wb; }
-        const int col = (int)(vblock * (unsigned)g.Wb + (unsigned)b);
-        colok = col < g.ncol;
+        const int col = (int)(blk * (unsigned)g.Wb + (unsigned)b);
+        colok = col < g.ncol && b < g.Wb && s < g.G;   // threads past the last segment idle
         const unsigned c = colok ? (unsigned)col : 0u;
         c2 = (int)g.div_n1.div(c);
         c1 = (int)(c - (unsigned)c2 * (unsigned)g.n1);
         base = c1 * g.s1 + (long long)c2 * g.s2;
     }
 };
+
+// Every read of the pencil's arrays before any in-place write: the CTA's barrier, or the cluster's.
+__device__ __forceinline__ void win_barrier(const SweepGeom& g) {
+    if (g.CL > 1) cluster_sync();
+    else __syncthreads();
+}
 
 template <typename T, int C>
 __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vblock) {
@@ -96,6 +112,9 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
     const int r0 = wp.s * C;
     const bool circ_lo = a.modeX[0] == BC_CIRC, circ_hi = a.modeX[1] == BC_CIRC;
     const bool fill_lo = !circ_lo && wp.s == 0, fill_hi = !circ_hi && r0 + C >= N;
+    // vector stores along x need every segment to start on a multiple of C: pencils (and the arrays,
+    // 256-byte aligned) start on one only where C divides N; ragged pencils store cell by cell
+    const bool vec = d == 0 && N % C == 0;
     const long long sd = g.sd;
     const T* rho = reinterpret_cast<const T*>(a.q[Q_RHO]);
     const T* pX = reinterpret_cast<const T*>(a.q[Q_PX + d]);
@@ -126,7 +145,7 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
             if (j >= 1 && j < W - 1) bI[q][j - 1] = BI[o];
         }
     }
-    __syncthreads();   // every thread has read B_I before any writes it
+    win_barrier(g);   // every thread has read B_I before any writes it
 
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
@@ -182,8 +201,8 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
             const long long o0 = wp.base + (long long)r0 * sd;
             const int nown = N - r0 < C ? N - r0 : C;
             if (nown == C) {
-                seg_store<T, C>(BI, o0, sd, d == 0, bnew);
-                seg_store<T, C>(Fo, o0, sd, d == 0, fo);
+                seg_store<T, C>(BI, o0, sd, vec, bnew);
+                seg_store<T, C>(Fo, o0, sd, vec, fo);
             } else {
 #pragma unroll
                 for (int k = 0; k < C; ++k)
@@ -206,6 +225,7 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     const int r0 = wp.s * C;
     const bool circ_lo = a.modeX[0] == BC_CIRC, circ_hi = a.modeX[1] == BC_CIRC;
     const bool fill_lo = !circ_lo && wp.s == 0, fill_hi = !circ_hi && r0 + C >= N;
+    const bool vec = d == 0 && N % C == 0;   // as in the chain
     const long long sd = g.sd;
     const double dt = a.tm->dt;
     // window cells -1 .. C (index j + 1)
@@ -236,7 +256,7 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     const T* BI2 = reinterpret_cast<const T*>(a.q[Q_BX + e2]);
     const long long nb2 = trans_offset(e2 == g.d1 ? wp.c1 : wp.c2, sel3(e2, gg.n[0], gg.n[1], gg.n[2]),
                                        sel3(e2, gg.s[0], gg.s[1], gg.s[2]), +1, a.modeI_mag[1][1], a.shiftI[1] != 0);
-    __syncthreads();   // every thread has read B_X before any writes it
+    win_barrier(g);   // every thread has read B_X before any writes it
     // D_q = C_q.shift(X,-1); B_X = (B_X - dt/dI1 D_1) - dt/dI2 D_2 at cells 0 .. C (index j)
     const T f0 = (T)(dt / a.dI[0]), f1 = (T)(dt / a.dI[1]);
     T bx[C + 1];
@@ -263,9 +283,9 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     }
     const int nown = N - r0 < C ? N - r0 : C;
     if (nown == C) {
-        seg_store<T, C>(BX, o0, sd, d == 0, bn);
-        seg_store<T, C>(CBX, o0, sd, d == 0, cbx);
-        seg_store<T, C>(CB2, o0, sd, d == 0, cb2);
+        seg_store<T, C>(BX, o0, sd, vec, bn);
+        seg_store<T, C>(CBX, o0, sd, vec, cbx);
+        seg_store<T, C>(CB2, o0, sd, vec, cb2);
     } else {
 #pragma unroll
         for (int k = 0; k < C; ++k)
