@@ -505,7 +505,11 @@ template <typename T, bool MHD, int CPT, bool FADE, bool CG, bool INIT>
 __device__ __forceinline__ void fluid_sweep_body_general(const FluidArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;   // uniform over the grid: a stopped or failed run does nothing
+    // A stopped or failed run does nothing.  Within a cluster every CTA must take the same branch before
+    // its cluster barriers, and the error word can be raised by another cluster of this very launch (the
+    // non-finite check of the fused CFL pass) while this one starts: cluster launches return on `done`
+    // only (set between launches), and a failed run's clusters compute on without consequence.
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;
     __shared__ T part[2][MAX_WARPS][33];   // per-warp column maxima (two freezing speeds; rows padded
                                            // so the lanes reading one column's warps hit distinct banks)
     __shared__ T cpart[2][32];             // per-CTA column maxima, read by the other cluster ranks

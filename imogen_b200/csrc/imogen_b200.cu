@@ -418,17 +418,39 @@ std::vector<PencilCfg> pencil_candidates(const Geom& g, int d, size_t elem) {
 // 3 or 4 in FP64; 2 or 4 with artificial viscosity), the whole pencil in one CTA of NT = Wb * S threads,
 // 64 <= NT <= 512, S = N / C threads per pencil.  Along x the S threads of a pencil are consecutive
 // lanes: S is a power of two up to 32 or a multiple of 32.  Along y and z Wb >= 4 pencils (a power of
-// two) sit side by side, at most 32 of them unless each pencil is one thread's (S = 1).
+// two) sit side by side, at most 32 of them unless each pencil is one thread's (S = 1).  Along x, for a
+// C (2, 4 or 8) with none of these and S = ceil(N / C) >= 64 segments, the cluster forms (seg_fluid.cuh's
+// CLU; no artificial viscosity): one pencil per CTA of NT = S rounded up to a multiple of 32 threads,
+// or over a cluster of CL = ceil(S / 256) <= 8 CTAs (ceil(S / 512) <= 4) of NT = ceil(S / CL) rounded
+// up; where C does not divide N the last segment is ragged (launch_fluid takes these for const ends
+// only).
+bool seg_cluster_form(const PencilCfg& p, int N) {
+    return p.seg && (p.CL > 1 || N % p.seg != 0 || p.NT != p.Wb * p.G);
+}
+
 std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool visc = false) {
     std::vector<PencilCfg> out;
     const int N = g.n[d];
     const long long ncol = g.ncell / N;
     for (int C : {2, 3, 4, 8}) {
-        if ((elem == 8 && C == 8) || (visc && (C == 8 || C == 3)) || N % C) continue;
-        const int S = N / C;
-        if (d == 0 && !(S % 32 == 0 || (S <= 32 && 32 % S == 0))) continue;
-        for (int Wb = d == 0 ? 1 : 4; Wb <= (d != 0 && S == 1 ? 512 : 32); Wb *= 2) {
-            const int NT = Wb * S;
+        if ((elem == 8 && C == 8) || (visc && (C == 8 || C == 3))) continue;
+        const size_t before = out.size();
+        auto add_cluster = [&](int S, int CL, int NT) {
+            const size_t smem = elem == 8 ? seg_fluid_smem_bytes<double>(NT) : seg_fluid_smem_bytes<float>(NT);
+            if (smem > kPencilSmemLimit) return;
+            PencilCfg p;
+            p.Wb = 1;
+            p.G = S;
+            p.CL = CL;
+            p.NT = NT;
+            p.cpt = C;
+            p.seg = C;
+            out.push_back(p);
+        };
+        const int Se = N / C;
+        const bool exact = N % C == 0 && (d != 0 || Se % 32 == 0 || (Se <= 32 && 32 % Se == 0));
+        for (int Wb = d == 0 ? 1 : 4; exact && Wb <= (d != 0 && Se == 1 ? 512 : 32); Wb *= 2) {
+            const int NT = Wb * Se;
             if (NT > 512) break;
             if (NT < 64 || NT % 32) continue;
             if (Wb > 1 && (long long)Wb / 2 >= ncol) break;   // more pencil slots than pencils
@@ -436,12 +458,20 @@ std::vector<PencilCfg> seg_candidates(const Geom& g, int d, size_t elem, bool vi
             if (smem > kPencilSmemLimit) continue;
             PencilCfg p;
             p.Wb = Wb;
-            p.G = S;
+            p.G = Se;
             p.CL = 1;
             p.NT = NT;
             p.cpt = C;
             p.seg = C;
             out.push_back(p);
+        }
+        if (d != 0 || visc || C == 3 || out.size() > before) continue;
+        const int S = (N + C - 1) / C;
+        if (S < 64) continue;
+        if (S <= 512) add_cluster(S, 1, (S + 31) / 32 * 32);
+        for (int cap : {256, 512}) {
+            const int CL = (S + cap - 1) / cap;
+            if (CL >= 2 && CL <= (cap == 256 ? 8 : 4)) add_cluster(S, CL, ((S + CL - 1) / CL + 31) / 32 * 32);
         }
     }
     return out;
@@ -701,6 +731,11 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
     // (img_create and img_set_tiling see to it), so no stored edge is ever read: the first sweeps too
     const bool visc = c.viscosity_type != IMG_VISC_NONE;
     if (visc) seg_ok = true;
+    // a ragged last segment (cluster forms) supports const ends only
+    const bool clu = seg_cluster_form(ctx->pcfg[0][d], ctx->g.n[d]);
+    if (clu && ctx->g.n[d] % ctx->pcfg[0][d].seg != 0)
+        for (int side = 0; side < 2; ++side)
+            if (c.bc_modes[CLS_MASS][side][d] != IMG_BC_CONST) seg_ok = false;
     const PencilCfg& pcf = (seg_ok || !ctx->pcfg[0][d].seg) ? ctx->pcfg[0][d] : ctx->pcfg_tile[d];
     a.sg = sweep_geom(ctx, d, pcf);
     for (int v = 0; v < NQ; ++v) a.q[v] = ctx->q[v];
@@ -737,6 +772,7 @@ int launch_fluid(img_ctx* ctx, int d, bool cfl) {
                                       pcf.seg ? seg_fluid_smem_bytes<T>(pcf.NT, visc) : fluid_smem_bytes<T>(pcf.G * pcf.cpt, pcf.Wb),
                                       1, fade);
     L.seg = pcf.seg;
+    L.clu = seg_cluster_form(pcf, ctx->g.n[d]);
     // copy ghosts: single-CTA pencils, one circ, const or fade mode per side shared by the fluid classes
     L.cg = pcf.CL == 1;
     for (int k = 0; k < 3; ++k)
@@ -2182,7 +2218,7 @@ size_t put(std::vector<unsigned char>& h, const V* v, size_t n) {
 bool same_shape(const PencilLaunch& x, const PencilLaunch& y) {
     return x.grid_y == y.grid_y && x.block == y.block && x.smem == y.smem && x.cluster == y.cluster &&
            x.cpt == y.cpt && x.nqc == y.nqc && x.fade == y.fade && x.cg == y.cg && x.init == y.init &&
-           x.seg == y.seg;
+           x.seg == y.seg && x.clu == y.clu;
 }
 
 // Turn the members' records into batched launch items and the arena image.

@@ -175,7 +175,7 @@ template <typename T, int CPT, bool FADE, int NQC, bool CG, bool INIT>
 __device__ __forceinline__ void mag_chain_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;   // clusters: as in the fluid sweeps
     Tile<T, CPT> tl;
     tl.init(a.sg, vblock);
     const int q0 = NQC == 2 ? 0 : (int)blockIdx.y;
@@ -468,7 +468,7 @@ template <typename T, int CPT, bool FADE, bool CG>
 __device__ __forceinline__ void mag_ctcell_body(const MagArgs& a, unsigned vblock) {
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;   // clusters: as in the fluid sweeps
     Tile<T, CPT> tl;
     tl.init(a.sg, vblock);
     const int d = a.X - 1;

@@ -50,8 +50,22 @@ __host__ __device__ inline size_t seg_fluid_smem_bytes(int NT, bool visc = false
 // Placement of one thread in the segment layout.
 struct SegPos {
     int b, s;            // pencil within the CTA, segment within the pencil
-    bool colok;          // the pencil exists (the last CTA may hold fewer than Wb)
+    int rank = 0;        // cluster rank (one pencil per cluster)
+    bool colok;          // the pencil exists (the last CTA may hold fewer than Wb) and so does the segment
     long long base;      // offset of the pencil's row 0
+    // One pencil along x over the CL CTAs of a cluster (CL = 1: one CTA), S = ceil(N / C) segments of
+    // which rank r holds r * NT .. r * NT + NT - 1; threads past the last segment idle.
+    __device__ __forceinline__ void init_cluster(const SweepGeom& g, unsigned vblock) {
+        const unsigned blk = g.div_cl.div(vblock);
+        rank = (int)(vblock - blk * (unsigned)g.CL);
+        b = 0;
+        s = rank * g.NT + (int)threadIdx.x;
+        colok = s < g.G && (long long)blk < g.ncol;
+        const unsigned c = colok ? blk : 0u;
+        const int c2 = (int)g.div_n1.div(c);
+        const int c1 = (int)(c - (unsigned)c2 * (unsigned)g.n1);
+        base = c1 * g.s1 + (long long)c2 * g.s2;
+    }
     __device__ __forceinline__ void init(const SweepGeom& g, unsigned vblock) {
         const int t = threadIdx.x;
         const unsigned q = g.div_lanes.div((unsigned)t);   // t / S (x) or t / Wb (y, z)
@@ -274,10 +288,15 @@ __device__ __forceinline__ T visc_add(T p, double q) {
 // Corrector (relaxingFluid.m:52-71) of one variable over a segment: R* = (u* + F*/c_f*)/2 and
 // L* = (u* - F*/c_f*)/2 at cells -2 .. C+1 (neighbour cells from the published exchange set X2), the
 // TVD limiter at cells -1 .. C (only those the update reads), and the update of the C own cells.
-// LIM: the launch's limiter (flux/*Limiter.m), fixed at compile time.
+// LIM: the launch's limiter (flux/*Limiter.m), fixed at compile time.  X2l/X2r: the exchange sets that
+// hold the left and right neighbour segments (another CTA's, through DSMEM, across a cluster).
+// nown < C: a ragged last segment with a const end after cell nown - 1 (its cells beyond hold copies of
+// that cell's state), whose limited L takes the end cell's value one cell past it.
 template <typename T, int C, int LIM>
-__device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], const T (&Fs)[C], const T* X2v, int NT,
-                                            int lt, int rt, bool lo_own, bool hi_own, T ics, T ffc, T (&unew)[C]) {
+__device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], const T (&Fs)[C], const T* X2l,
+                                            const T* X2r, int NT, int lt, int rt, bool lo_own, bool hi_own, T ics,
+                                            T ffc, T (&unew)[C], int nown = C) {
+    const T* X2v = X2l;
     T Rs[C + 4], Ls[C + 4];
 #pragma unroll
     for (int k = 0; k < C; ++k) {
@@ -298,8 +317,8 @@ __device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], c
         Rs[C + 2] = Rs[C + 1]; Ls[C + 2] = Ls[C + 1];
         Rs[C + 3] = Rs[C + 1]; Ls[C + 3] = Ls[C + 1];
     } else {
-        const T u1 = X2v[rt], w1 = X2v[5 * NT + rt] * ics;                // right's first cell
-        const T u2 = X2v[10 * NT + rt], w2 = X2v[15 * NT + rt] * ics;      // right's cell 1
+        const T u1 = X2r[rt], w1 = X2r[5 * NT + rt] * ics;                // right's first cell
+        const T u2 = X2r[10 * NT + rt], w2 = X2r[15 * NT + rt] * ics;      // right's cell 1
         Rs[C + 2] = T(0.5) * (u1 + w1); Ls[C + 2] = T(0.5) * (u1 - w1);
         Rs[C + 3] = T(0.5) * (u2 + w2); Ls[C + 3] = T(0.5) * (u2 - w2);
     }
@@ -317,6 +336,15 @@ __device__ __forceinline__ void seg_correct(const T (&u)[C], const T (&us)[C], c
     }
     if (lo_own) Rl[0] = Rl[1];   // the limited flux's own const ghost
     if (hi_own) Ll[C + 1] = Ll[C];
+    if (nown < C) {               // ragged end: the ghost one past cell nown - 1
+        T e = Ll[1];
+#pragma unroll
+        for (int j = 1; j < C; ++j)
+            if (j == nown) e = Ll[j];
+#pragma unroll
+        for (int j = 2; j <= C; ++j)
+            if (j == nown + 1) Ll[j] = e;
+    }
 #pragma unroll
     for (int k = 0; k < C; ++k) unew[k] = u[k] - ffc * (Rl[k + 1] - Rl[k] + Ll[k + 1] - Ll[k + 2]);
 }
@@ -361,20 +389,58 @@ __device__ __forceinline__ T seg_max_collect(const SweepGeom& g, int b, T wv, co
     return m;
 }
 
+// Stage barrier of the segment kernel: the cluster's where a pencil spans a cluster.
+template <bool CLU>
+__device__ __forceinline__ void sp_sync(const SweepGeom& g) {
+    if (CLU && g.CL > 1) cluster_sync();
+    else __syncthreads();
+}
+
+// Pencil maximum for one pencil over a cluster (init_cluster placement): publish leaves each warp's
+// maximum in pm; collect, after a barrier, reduces the CTA's warps and, with CL > 1, the CTAs' maxima
+// through DSMEM (slot `slot` of cm) behind one more cluster barrier.  All threads call both.
+template <typename T>
+__device__ __forceinline__ void clu_max_publish(T v, T* pm) {
+    v = warp_max_nonneg(v);
+    if ((threadIdx.x & 31) == 0) pm[(threadIdx.x >> 5) * 32] = v;
+}
+
+template <typename T>
+__device__ __forceinline__ T clu_max_collect(const SweepGeom& g, const T* pm, T* cm, int slot) {
+    const int lane = threadIdx.x & 31;
+    const T m = warp_max_nonneg(lane < (g.NT >> 5) ? pm[lane * 32] : T(0));
+    if (g.CL == 1) return m;
+    if (threadIdx.x == 0) cm[slot] = m;
+    cluster_sync();
+    T c = T(0);
+    if (lane < g.CL) c = cg::this_cluster().map_shared_rank(cm, lane)[slot];
+    return warp_max_nonneg(c);
+}
+
 // VT: the artificial viscosity (VISC_*), fixed per kernel.  With viscosity each of the first two
 // stages takes one more barrier: the viscosity exchange set is published with the pencil maximum, and
 // the flux numerators (which include the viscous pressure) are published after it.
-template <typename T, bool MHD, int C, int VT>
+// CLU: one pencil along x per cluster of CL CTAs (CL = 1: one CTA), placed by SegPos::init_cluster:
+// the exchanges with segments in another CTA read its shared memory through DSMEM, the barriers and the
+// pencil maxima span the cluster, and a length that C does not divide leaves the last segment ragged
+// (const ends only: its cells past the pencil's end load the end cell and, after the predictor, take the
+// end cell's half-step state, the const ghosts of every shifted array).
+template <typename T, bool MHD, int C, int VT, bool CLU = false>
 __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblock) {
+    static_assert(!CLU || VT == VISC_NONE, "cluster segments carry no viscosity");
     extern __shared__ __align__(16) unsigned char smem[];
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;
+    // cluster launches return on `done` only, as fluid_sweep_body_general's do
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;
     __shared__ double cflp[3][MAX_WARPS];
+    __shared__ T cmax[2];
     const SweepGeom& g = a.sg;
     const int NT = g.NT, S = g.G, d = g.d, d1 = g.d1, d2 = g.d2;
+    const int N = g.N;
     const int t = threadIdx.x;
     SegPos sp;
-    sp.init(g, vblock);
+    if constexpr (CLU) sp.init_cluster(g, vblock);
+    else sp.init(g, vblock);
     const int s = sp.s;
     T* X1 = reinterpret_cast<T*>(smem);   // [20][NT]: (u, F) of the first cell, then of the last
     T* X2 = X1 + 20 * NT;                 // [40][NT]: (u*, F*) of cells 0, 1, C-2, C-1
@@ -383,13 +449,38 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     const bool circ_lo = a.mode[CLS_MASS][0] == BC_CIRC, circ_hi = a.mode[CLS_MASS][1] == BC_CIRC;
     const int ls = d == 0 ? 1 : g.Wb;     // thread distance between consecutive segments of a pencil
     const bool lo_own = s == 0 && !circ_lo, hi_own = s == S - 1 && !circ_hi;
-    const int lt = s > 0 ? t - ls : (circ_lo ? t + (S - 1) * ls : t);
-    const int rt = s < S - 1 ? t + ls : (circ_hi ? t - (S - 1) * ls : t);
+    int lt = s > 0 ? t - ls : (circ_lo ? t + (S - 1) * ls : t);
+    int rt = s < S - 1 ? t + ls : (circ_hi ? t - (S - 1) * ls : t);
+    // the exchange sets holding the neighbour segments (another rank's across a cluster)
+    const T* X1l = X1;
+    const T* X1r = X1;
+    const T* X2l = X2;
+    const T* X2r = X2;
+    int nown = C;   // own cells inside the pencil (a ragged last segment: fewer; idle threads: none)
+    if constexpr (CLU) {
+        const int sc = s < S ? s : S - 1;   // idle threads read a real segment's neighbours
+        const int sl = sc > 0 ? sc - 1 : (circ_lo ? S - 1 : sc);
+        const int sr = sc < S - 1 ? sc + 1 : (circ_hi ? 0 : sc);
+        const int rl = sl / NT, rr = sr / NT;
+        lt = sl - rl * NT;
+        rt = sr - rr * NT;
+        if (rl != sp.rank) {
+            X1l = cg::this_cluster().map_shared_rank(X1, rl);
+            X2l = cg::this_cluster().map_shared_rank(X2, rl);
+        }
+        if (rr != sp.rank) {
+            X1r = cg::this_cluster().map_shared_rank(X1, rr);
+            X2r = cg::this_cluster().map_shared_rank(X2, rr);
+        }
+        nown = N - s * C < C ? N - s * C : C;
+    }
     const double G = a.gamma;
     const double dt = a.tm->dt;
     const T ff = (T)(dt / a.dx);
     const T half_ffx = (T)(0.5 * (dt / a.dx));
-    const bool vec = d == 0;
+    // vector accesses need segments on multiples of C: pencils start on one where C divides N
+    const bool vec = d == 0 && (!CLU || N % C == 0);
+    const bool ragged = CLU && nown < C;   // cells past the pencil's end: load (and later take) the end cell
     const long long o0 = sp.base + (long long)s * C * g.sd;
     // momentum and cell-centred B in sweep-rotated order: component 0 along the sweep, then d1, d2
     void* qv[5] = {a.q[Q_RHO], a.q[Q_PX + d], a.q[Q_PX + d1], a.q[Q_PX + d2], a.q[Q_E]};
@@ -409,7 +500,21 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
             if (MHD && ub[c]) m = m + (double)b[c][k] * (double)b[c][k];
         return m;
     };
-    if (sp.colok) {
+    if (sp.colok && ragged) {
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const long long o = sp.base + (long long)(k < nown ? s * C + k : N - 1) * g.sd;
+#pragma unroll
+            for (int v = 0; v < 5; ++v) u[v][k] = ldq<T>(qv[v], o);
+            if (LOADB) {
+                bb[0][k] = ldq<T>(a.q[Q_CBX + d], o);
+                bb[1][k] = ldq<T>(a.q[Q_CBX + d1], o);
+                bb[2][k] = ldq<T>(a.q[Q_CBX + d2], o);
+            } else {
+                bb[0][k] = bb[1][k] = bb[2][k] = T(0);
+            }
+        }
+    } else if (sp.colok) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) seg_load<T, C>(qv[v], o0, g.sd, vec, u[v]);
         if (LOADB) {
@@ -451,9 +556,15 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
             X1[(10 + v) * NT + t] = u[v][C - 1];
             X1[(15 + v) * NT + t] = F[v][C - 1];
         }
-        const T wv1 = seg_max_publish(g, lmax, PM);
-        __syncthreads();
-        cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22)
+        if constexpr (CLU) {
+            clu_max_publish(lmax, PM);
+            sp_sync<CLU>(g);
+            cf = clu_max_collect(g, PM, cmax, 0);   // freezing speed (wFluidFlux.m:18-22)
+        } else {
+            const T wv1 = seg_max_publish(g, lmax, PM);
+            __syncthreads();
+            cf = seg_max_collect(g, sp.b, wv1, PM);   // freezing speed (wFluidFlux.m:18-22)
+        }
     } else {
         T P[C], CS[C];
         double vel[C], snd[C], q[C];
@@ -504,10 +615,19 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
             R[k + 1] = T(0.5) * (u[v][k] + w);
             L[k] = T(0.5) * (u[v][k] - w);
         }
-        R[0] = lo_own ? R[1] : T(0.5) * (X1[(10 + v) * NT + lt] + X1[(15 + v) * NT + lt] * ic);
-        L[C] = hi_own ? L[C - 1] : T(0.5) * (X1[v * NT + rt] - X1[(5 + v) * NT + rt] * ic);
+        R[0] = lo_own ? R[1] : T(0.5) * (X1l[(10 + v) * NT + lt] + X1l[(15 + v) * NT + lt] * ic);
+        L[C] = hi_own ? L[C - 1] : T(0.5) * (X1r[v * NT + rt] - X1r[(5 + v) * NT + rt] * ic);
 #pragma unroll
         for (int k = 0; k < C; ++k) us[v][k] = u[v][k] - hfc * (R[k + 1] - R[k] + L[k] - L[k + 1]);
+        if (ragged && nown > 0) {   // cells past the end take the end cell's half-step state
+            T e = us[v][0];
+#pragma unroll
+            for (int k = 1; k < C; ++k)
+                if (k == nown - 1) e = us[v][k];
+#pragma unroll
+            for (int k = 1; k < C; ++k)
+                if (k >= nown) us[v][k] = e;
+        }
     }
     T lmax2 = T(0);
     T P2[C], CS2[C];
@@ -561,7 +681,11 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
         X2[(35 + v) * NT + t] = Fs[v][C - 1];
     }
     T cfs;   // freezing speed of the half step
-    if constexpr (VT == VISC_NONE) {
+    if constexpr (CLU) {
+        clu_max_publish(lmax2, PM + (NT >> 5) * 32);
+        sp_sync<CLU>(g);
+        cfs = clu_max_collect(g, PM + (NT >> 5) * 32, cmax, 1);
+    } else if constexpr (VT == VISC_NONE) {
         const T wv2 = seg_max_publish(g, lmax2, PM + (NT >> 5) * 32);
         __syncthreads();
         cfs = seg_max_collect(g, sp.b, wv2, PM + (NT >> 5) * 32);
@@ -579,18 +703,30 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
     const T ffc = ff * cfs;
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
-        const T* X2v = X2 + v * NT;
+        const T* Xl = X2l + v * NT;
+        const T* Xr = X2r + v * NT;
+        const int nc = CLU ? nown : C;
         if (a.limiter == LIM_VANLEER)
-            seg_correct<T, C, LIM_VANLEER>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
+            seg_correct<T, C, LIM_VANLEER>(u[v], us[v], Fs[v], Xl, Xr, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v], nc);
         else if (a.limiter == LIM_SUPERBEE)
-            seg_correct<T, C, LIM_SUPERBEE>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
+            seg_correct<T, C, LIM_SUPERBEE>(u[v], us[v], Fs[v], Xl, Xr, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v], nc);
         else
-            seg_correct<T, C, LIM_MINMOD>(u[v], us[v], Fs[v], X2v, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v]);
+            seg_correct<T, C, LIM_MINMOD>(u[v], us[v], Fs[v], Xl, Xr, NT, lt, rt, lo_own, hi_own, ics, ffc, unew[v], nc);
     }
+    // the other ranks have read this CTA's exchange sets before it moves on (and may exit)
+    if (CLU && g.CL > 1) cluster_sync();
     double m3[3] = {0.0, 0.0, 0.0};   // rotated order
     bool bad = false;
     T cb[3][C];   // the CFL pass reloads the cell-centred B (cache hits; one sweep in six)
-    if (a.cfl && sp.colok && MHD) {
+    if (a.cfl && sp.colok && MHD && ragged) {
+#pragma unroll
+        for (int k = 0; k < C; ++k) {
+            const long long o = sp.base + (long long)(k < nown ? s * C + k : N - 1) * g.sd;
+            cb[0][k] = ldq<T>(a.q[Q_CBX + d], o);
+            cb[1][k] = ldq<T>(a.q[Q_CBX + d1], o);
+            cb[2][k] = ldq<T>(a.q[Q_CBX + d2], o);
+        }
+    } else if (a.cfl && sp.colok && MHD) {
         seg_load<T, C>(a.q[Q_CBX + d], o0, g.sd, vec, cb[0]);
         seg_load<T, C>(a.q[Q_CBX + d1], o0, g.sd, vec, cb[1]);
         seg_load<T, C>(a.q[Q_CBX + d2], o0, g.sd, vec, cb[2]);
@@ -598,7 +734,7 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
 #pragma unroll
     for (int k = 0; k < C; ++k) {
         unew[0][k] = unew[0][k] > (T)a.minmass_out ? unew[0][k] : (T)a.minmass_out;
-        if (a.cfl && sp.colok) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
+        if (a.cfl && sp.colok && k < nown) {   // fused CFL maxima of the new state (TimeManager.m:65-77)
             double sp3[3];
             cfl_speeds(G, (double)unew[0][k], (double)unew[1][k], (double)unew[2][k], (double)unew[3][k],
                        (double)unew[4][k], MHD ? bsq(cb, k) : 0.0, sp3);
@@ -607,9 +743,16 @@ __device__ __forceinline__ void fluid_seg_body(const FluidArgs& a, unsigned vblo
             for (int c = 0; c < 3; ++c) m3[c] = fmax(m3[c], sp3[c]);
         }
     }
-    if (sp.colok)
+    if (sp.colok && ragged) {
+#pragma unroll
+        for (int k = 0; k < C; ++k)
+            if (k < nown)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) stq<T>(qv[v], o0 + (long long)k * g.sd, unew[v][k]);
+    } else if (sp.colok) {
 #pragma unroll
         for (int v = 0; v < 5; ++v) seg_store<T, C>(qv[v], o0, g.sd, vec, unew[v]);
+    }
     if (a.cfl) {
         if (a.cfl & CFL_CHECK_NONFINITE) flag_nonfinite(a.tm, bad);
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -641,6 +784,22 @@ __global__ void __launch_bounds__(512, 1) fluid_seg_batch_kernel(const FluidArgs
     load_member_args(sa, args + bm.member);
     __syncthreads();
     fluid_seg_body<T, MHD, C, VISC_NONE>(sa, (unsigned)bm.block);
+}
+
+// One pencil along x per cluster of CTAs, or per CTA with a ragged last segment (fluid_seg_body's CLU).
+template <typename T, bool MHD, int C>
+__global__ void __launch_bounds__(512, 1) fluid_seg_clu_kernel(const __grid_constant__ FluidArgs a) {
+    fluid_seg_body<T, MHD, C, VISC_NONE, true>(a, blockIdx.x);
+}
+
+template <typename T, bool MHD, int C>
+__global__ void __launch_bounds__(512, 1) fluid_seg_clu_batch_kernel(const FluidArgs* __restrict__ args,
+                                                                      const BlockMap* __restrict__ map) {
+    __shared__ FluidArgs sa;
+    const BlockMap bm = map[blockIdx.x];
+    load_member_args(sa, args + bm.member);
+    __syncthreads();
+    fluid_seg_body<T, MHD, C, VISC_NONE, true>(sa, (unsigned)bm.block);
 }
 
 }  // namespace img

@@ -102,7 +102,7 @@ __device__ __forceinline__ void win_barrier(const SweepGeom& g) {
 template <typename T, int C>
 __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vblock) {
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;   // clusters: as in the fluid sweeps
     constexpr int W = C + 8;   // window cells -4 .. C+3 (index j + 4)
     const SweepGeom& g = a.sg;
     const Geom& gg = g.g;
@@ -216,7 +216,7 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
 template <typename T, int C>
 __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vblock) {
     pdl_wait();
-    if (a.tm->done || a.tm->error) return;
+    if (a.tm->done || (a.sg.CL == 1 && a.tm->error)) return;   // clusters: as in the fluid sweeps
     const SweepGeom& g = a.sg;
     const Geom& gg = g.g;
     const int N = g.N, d = a.X - 1;

@@ -21,6 +21,8 @@ struct PencilLaunch {
     bool init;                 // fluid sweep / chain: captures stored edges (overrides cg)
     int seg;                   // cells per thread of the segment fluid kernel (seg_fluid.cuh) or of the window
                                // magnet kernels (seg_magnet.cuh); 0: the pencil-tile kernels
+    bool clu;                  // segment fluid kernel: one pencil along x per cluster (or per CTA with a
+                               // ragged last segment), seg_fluid.cuh's CLU form
     cudaStream_t stream;
 };
 
@@ -46,7 +48,8 @@ template <typename T> cudaError_t fluid_attributes(int cpt, int optin);
 template <typename T> cudaError_t chain_attributes(int cpt, int optin);
 // Clusters of the MHD fluid kernel that can be co-resident for launch shape L (0: not schedulable).
 template <typename T> cudaError_t fluid_max_clusters(const PencilLaunch& L, int* n);
-// Shared-memory attributes of the segment fluid kernels (2, 4 and 8 cells per thread; 2 and 4 in FP64).
+// Shared-memory attributes of the segment fluid kernels (2, 3, 4 and 8 cells per thread; 2, 3 and 4 in
+// FP64; the cluster forms with 2, 4 and 8, and 2 and 4).
 template <typename T> cudaError_t fluid_seg_attributes(int optin);
 
 }  // namespace img

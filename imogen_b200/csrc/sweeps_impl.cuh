@@ -190,8 +190,36 @@ void (*fluid_seg_batch_kernel_p(int C, bool mhd))(const FluidArgs*, const BlockM
     return mhd ? fluid_seg_batch_kernel_c<T, true>(C) : fluid_seg_batch_kernel_c<T, false>(C);
 }
 
+// Cluster (CLU) forms of the segment fluid kernel: 2, 4 and 8 cells per thread (FP64: 2 and 4).
+template <typename T, bool MHD>
+void (*fluid_seg_clu_kernel_c(int C))(const FluidArgs) {
+    if constexpr (sizeof(T) == 4) {
+        if (C == 8) return fluid_seg_clu_kernel<T, MHD, 8>;
+    }
+    return C == 2 ? fluid_seg_clu_kernel<T, MHD, 2> : fluid_seg_clu_kernel<T, MHD, 4>;
+}
+
+template <typename T, bool MHD>
+void (*fluid_seg_clu_batch_kernel_c(int C))(const FluidArgs*, const BlockMap*) {
+    if constexpr (sizeof(T) == 4) {
+        if (C == 8) return fluid_seg_clu_batch_kernel<T, MHD, 8>;
+    }
+    return C == 2 ? fluid_seg_clu_batch_kernel<T, MHD, 2> : fluid_seg_clu_batch_kernel<T, MHD, 4>;
+}
+
+template <typename T>
+void (*fluid_seg_clu_kernel_p(int C, bool mhd))(const FluidArgs) {
+    return mhd ? fluid_seg_clu_kernel_c<T, true>(C) : fluid_seg_clu_kernel_c<T, false>(C);
+}
+
+template <typename T>
+void (*fluid_seg_clu_batch_kernel_p(int C, bool mhd))(const FluidArgs*, const BlockMap*) {
+    return mhd ? fluid_seg_clu_batch_kernel_c<T, true>(C) : fluid_seg_clu_batch_kernel_c<T, false>(C);
+}
+
 template <typename T>
 cudaError_t launch_fluid_sweep_batch(const FluidArgs* args, const BlockMap* map, const PencilLaunch& L, bool mhd) {
+    if (L.seg && L.clu) return launch_pencil_batch(fluid_seg_clu_batch_kernel_p<T>(L.seg, mhd), args, map, L);
     if (L.seg) return launch_pencil_batch(fluid_seg_batch_kernel_p<T>(L.seg, mhd), args, map, L);
     if (L.cluster > 1) return launch_fluid_sweep_batch_cluster<T>(args, map, L, mhd);
     return launch_pencil_batch(fluid_batch_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), args, map, L);
@@ -271,6 +299,7 @@ cudaError_t launch_mag_ctcell_batch(const MagArgs* args, const BlockMap* map, co
 
 template <typename T>
 cudaError_t launch_fluid_sweep(const FluidArgs& a, const PencilLaunch& L, bool mhd) {
+    if (L.seg && L.clu) return launch_pencil(fluid_seg_clu_kernel_p<T>(L.seg, mhd), a, L);
     if (L.seg) return launch_pencil(fluid_seg_kernel_p<T>(L.seg, mhd, a.visc), a, L);
     return launch_pencil(fluid_kernel<T>(L.cpt, mhd, kernel_variant(L.fade, L.cg, L.init)), a, L);
 }
@@ -317,6 +346,8 @@ cudaError_t fluid_seg_attributes(int optin) {
             if (e == cudaSuccess) e = allow_max_smem(fluid_seg_batch_kernel_p<T>(C, mhd != 0), optin);
             for (int vt : {VISC_NR, VISC_CSW})
                 if (e == cudaSuccess && (C == 2 || C == 4)) e = allow_max_smem(fluid_seg_kernel_p<T>(C, mhd != 0, vt), optin);
+            if (e == cudaSuccess && C != 3) e = allow_max_smem(fluid_seg_clu_kernel_p<T>(C, mhd != 0), optin);
+            if (e == cudaSuccess && C != 3) e = allow_max_smem(fluid_seg_clu_batch_kernel_p<T>(C, mhd != 0), optin);
             if (e != cudaSuccess) return e;
         }
     }
