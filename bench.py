@@ -501,8 +501,8 @@ def run_ensemble(args, timed_steps):
         r.sync()
     seq = time.perf_counter() - t0
     b = ImogenBatch(members)
-    for _ in range(8):                         # into the graph-replay regime
-        b.step()
+    for _ in range(14):                        # into the graph-replay regime: the six sweep-order phases
+        b.step()                               # are captured at steps 7-12, then replayed
     l0 = b.launches
     el = timed_steps(b, k, per_launch=b.step)
     out = {"members": len(members), "cells": cells, "form": "mixed", "steps": k,

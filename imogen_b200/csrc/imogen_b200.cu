@@ -2126,6 +2126,7 @@ int img_totals(img_ctx* ctx, double out[8]) {
 
 struct BatchItem {            // one batched launch
     int kind = 0, elem = 0;
+    int op = 0;               // index of the members' launch it batches (the groups of one op run side by side)
     bool mhd = false;
     PencilLaunch L{};         // pencil kernels: the shared shape; grid_x = CTAs of all members
     unsigned blocks = 0;      // pointwise kernels: blocks of all members
@@ -2167,6 +2168,12 @@ struct img_batch {
     int* status_dev = nullptr;      // gathered done/error flags
     DevTime** tms_dev = nullptr;
     size_t status_cap = 0;
+    // The launch groups of one op touch disjoint members: all but the first go to side streams forked
+    // from and joined back into `stream` around the op, so their tails overlap (parallel graph branches).
+    static constexpr int kSide = 4;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork_ev = nullptr;
+    cudaEvent_t join_ev[kSide] = {};
 };
 
 namespace {
@@ -2255,6 +2262,7 @@ int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchP
         for (int h = 0; h < (int)heads.size(); ++h) {
             BatchItem it;
             const OpRec& r0 = recs[heads[h]][k];
+            it.op = (int)k;
             it.kind = kind;
             it.elem = r0.elem;
             it.mhd = r0.mhd;
@@ -2309,16 +2317,18 @@ int build_plan(img_batch* b, const std::vector<std::vector<OpRec>>& recs, BatchP
 
 template <typename T>
 cudaError_t launch_item(const BatchItem& it, const unsigned char* base, cudaStream_t st) {
+    PencilLaunch L = it.L;
+    L.stream = st;
     switch (it.kind) {
         case OP_FLUID:
             return launch_fluid_sweep_batch<T>(reinterpret_cast<const FluidArgs*>(base + it.args_off),
-                                               reinterpret_cast<const BlockMap*>(base + it.map_off), it.L, it.mhd);
+                                               reinterpret_cast<const BlockMap*>(base + it.map_off), L, it.mhd);
         case OP_CHAIN:
             return launch_mag_chain_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
-                                             reinterpret_cast<const BlockMap*>(base + it.map_off), it.L);
+                                             reinterpret_cast<const BlockMap*>(base + it.map_off), L);
         case OP_CTCELL:
             return launch_mag_ctcell_batch<T>(reinterpret_cast<const MagArgs*>(base + it.args_off),
-                                              reinterpret_cast<const BlockMap*>(base + it.map_off), it.L);
+                                              reinterpret_cast<const BlockMap*>(base + it.map_off), L);
         case OP_CFL_REDUCE:
             cfl_reduce_batch_kernel<T><<<it.blocks, 256, 0, st>>>(reinterpret_cast<const CflArgs*>(base + it.args_off),
                                                                  reinterpret_cast<const BlockMap*>(base + it.map_off));
@@ -2332,11 +2342,29 @@ cudaError_t launch_item(const BatchItem& it, const unsigned char* base, cudaStre
 
 int launch_plan(img_batch* b, const BatchPlan& plan) {
     const unsigned char* base = static_cast<const unsigned char*>(plan.dev);
-    for (const BatchItem& it : plan.items) {
-        cudaError_t e = it.elem == 8 ? launch_item<double>(it, base, b->stream) : launch_item<float>(it, base, b->stream);
-        if (e != cudaSuccess)
-            return bfail(b, IMG_ERR_CUDA, "batched launch (kind %d, %d members, grid %u): %s", it.kind, it.nmembers,
-                         pencil_kind(it.kind) ? it.L.grid_x : it.blocks, cudaGetErrorString(e));
+    const size_t n = plan.items.size();
+    for (size_t i0 = 0; i0 < n;) {
+        size_t i1 = i0 + 1;
+        while (i1 < n && plan.items[i1].op == plan.items[i0].op) ++i1;
+        const int groups = (int)(i1 - i0);
+        const int nside = std::min(groups - 1, img_batch::kSide);
+        if (nside > 0) {   // fork: the side streams start after everything before this op
+            BCK(cudaEventRecord(b->fork_ev, b->stream));
+            for (int j = 0; j < nside; ++j) BCK(cudaStreamWaitEvent(b->side[j], b->fork_ev, 0));
+        }
+        for (size_t i = i0; i < i1; ++i) {
+            const BatchItem& it = plan.items[i];
+            const cudaStream_t st = i == i0 ? b->stream : b->side[(i - i0 - 1) % img_batch::kSide];
+            cudaError_t e = it.elem == 8 ? launch_item<double>(it, base, st) : launch_item<float>(it, base, st);
+            if (e != cudaSuccess)
+                return bfail(b, IMG_ERR_CUDA, "batched launch (kind %d, %d members, grid %u): %s", it.kind, it.nmembers,
+                             pencil_kind(it.kind) ? it.L.grid_x : it.blocks, cudaGetErrorString(e));
+        }
+        for (int j = 0; j < nside; ++j) {   // join: the next op starts after every group of this one
+            BCK(cudaEventRecord(b->join_ev[j], b->side[j]));
+            BCK(cudaStreamWaitEvent(b->stream, b->join_ev[j], 0));
+        }
+        i0 = i1;
     }
     return IMG_OK;
 }
@@ -2354,8 +2382,14 @@ int img_batch_create(img_batch** out) {
     if (!out) return IMG_ERR_ARG;
     *out = nullptr;
     img_batch* b = new img_batch();
-    if (cudaGetDevice(&b->dev) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete b;
+    bool ok = cudaGetDevice(&b->dev) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int j = 0; ok && j < img_batch::kSide; ++j)
+        ok = cudaStreamCreateWithFlags(&b->side[j], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->join_ev[j], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        img_batch_destroy(b);
         return IMG_ERR_CUDA;
     }
     *out = b;
@@ -2379,7 +2413,12 @@ int img_batch_destroy(img_batch* b) {
     }
     if (b->status_dev) cudaFree(b->status_dev);
     if (b->tms_dev) cudaFree(b->tms_dev);
-    cudaStreamDestroy(b->stream);
+    for (int j = 0; j < img_batch::kSide; ++j) {
+        if (b->side[j]) cudaStreamDestroy(b->side[j]);
+        if (b->join_ev[j]) cudaEventDestroy(b->join_ev[j]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return IMG_OK;
 }
