@@ -54,17 +54,30 @@ __device__ __forceinline__ int win_row(int r, int N, bool circ_lo, bool circ_hi)
     return r;
 }
 
-// Const ends: window cells [lo, hi) of a stage array A (indices j + OFS) beyond the pencil's lower end
-// copy the end cell (local index 0), beyond its upper end the last cell (local index C - 1).
-template <typename T, int C, int OFS, int LO, int HI>
-__device__ __forceinline__ void const_fill(T* A, bool fill_lo, bool fill_hi) {
-    if (fill_lo) {
+// Const ends: the window cells of a stage array A (local cells LO .. HI-1 at A[j + OFS]) past the
+// pencil's lower end copy its row 0 (local cell lend = -r0), those past its upper end its last row
+// (local cell hend = N - 1 - r0): the const ghost of every shifted array (constant_shift.m).  A window
+// reaches 4 cells past its segment, so near an end several segments' windows cross it, and the end row
+// may be a window cell rather than an own one (short segments, a ragged last segment).
+template <typename T, int OFS, int LO, int HI>
+__device__ __forceinline__ void const_fill(T* A, bool circ_lo, bool circ_hi, int lend, int hend) {
+    if (!circ_lo && lend > LO) {
+        T e = A[LO + OFS];
 #pragma unroll
-        for (int j = LO; j < 0; ++j) A[j + OFS] = A[OFS];
+        for (int j = LO + 1; j < HI; ++j)
+            if (j == lend) e = A[j + OFS];
+#pragma unroll
+        for (int j = LO; j < HI; ++j)
+            if (j < lend) A[j + OFS] = e;
     }
-    if (fill_hi) {
+    if (!circ_hi && hend < HI - 1) {
+        T e = A[LO + OFS];
 #pragma unroll
-        for (int j = C; j < HI; ++j) A[j + OFS] = A[C - 1 + OFS];
+        for (int j = LO + 1; j < HI; ++j)
+            if (j == hend) e = A[j + OFS];
+#pragma unroll
+        for (int j = LO; j < HI; ++j)
+            if (j > hend) A[j + OFS] = e;
     }
 }
 
@@ -111,7 +124,9 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
     wp.init(g, vblock);
     const int r0 = wp.s * C;
     const bool circ_lo = a.modeX[0] == BC_CIRC, circ_hi = a.modeX[1] == BC_CIRC;
-    const bool fill_lo = !circ_lo && wp.s == 0, fill_hi = !circ_hi && r0 + C >= N;
+    const bool fill_lo = !circ_lo && wp.s == 0;
+    const int lend = -r0, hend = N - 1 - r0;    // local cells of the pencil's first and last rows
+    const int nown = N - r0 < C ? N - r0 : C;   // own cells inside the pencil (fewer in a ragged last segment)
     // vector stores along x need every segment to start on a multiple of C: pencils (and the arrays,
     // 256-byte aligned) start on one only where C divides N; ragged pencils store cell by cell
     const bool vec = d == 0 && N % C == 0;
@@ -154,20 +169,20 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
         T vg[W - 2];
 #pragma unroll
         for (int j = -3; j < C + 3; ++j) vg[j + 3] = T(0.25) * (vgr[q][j + 3] + vgr[q][j + 5] + T(2) * vgr[q][j + 4]);
-        const_fill<T, C, 3, -3, C + 3>(vg, fill_lo, fill_hi);
+        const_fill<T, 3, -3, C + 3>(vg, circ_lo, circ_hi, lend, hend);
         // velocityFlow = (vg + vg.shift(X,1)) < 0 and store.fluxR = F*(1-vf) + F.shift(X,1)*vf at cells
         // -3 .. C+1 (index j + 3), F = B_I * vg (relaxingMagnet.m:17-24)
         T Fr[W - 2], vf[W - 3], fR[W - 3];
 #pragma unroll
         for (int j = -3; j < C + 3; ++j) Fr[j + 3] = bI[q][j + 3] * vg[j + 3];
-        const_fill<T, C, 3, -3, C + 3>(Fr, fill_lo, fill_hi);
+        const_fill<T, 3, -3, C + 3>(Fr, circ_lo, circ_hi, lend, hend);
 #pragma unroll
         for (int j = -3; j < C + 2; ++j) {
             vf[j + 3] = (vg[j + 3] + vg[j + 4]) < T(0) ? T(1) : T(0);
             fR[j + 3] = Fr[j + 3] * (T(1) - vf[j + 3]) + Fr[j + 4] * vf[j + 3];
         }
-        const_fill<T, C, 3, -3, C + 2>(vf, fill_lo, fill_hi);
-        const_fill<T, C, 3, -3, C + 2>(fR, fill_lo, fill_hi);
+        const_fill<T, 3, -3, C + 2>(vf, circ_lo, circ_hi, lend, hend);
+        const_fill<T, 3, -3, C + 2>(fR, circ_lo, circ_hi, lend, hend);
         // store = B_I - ff*(fluxR - fluxR.shift(X,-1)); wMag = store.*velGrid at cells -2 .. C+1 (j + 2)
         T Wm[W - 4];
 #pragma unroll
@@ -175,7 +190,7 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
             const T st = bI[q][j + 3] - ff * (fR[j + 3] - fR[j + 2]);
             Wm[j + 2] = st * vg[j + 3];
         }
-        const_fill<T, C, 2, -2, C + 2>(Wm, fill_lo, fill_hi);
+        const_fill<T, 2, -2, C + 2>(Wm, circ_lo, circ_hi, lend, hend);
         // flux and its TVD correction (relaxingMagnet.m:32-51) at cells -1 .. C-1 (index j + 1)
         T Fl[C + 1];
 #pragma unroll
@@ -199,7 +214,6 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
                 fo[k] = Fl[k + 1];
             }
             const long long o0 = wp.base + (long long)r0 * sd;
-            const int nown = N - r0 < C ? N - r0 : C;
             if (nown == C) {
                 seg_store<T, C>(BI, o0, sd, vec, bnew);
                 seg_store<T, C>(Fo, o0, sd, vec, fo);
@@ -225,6 +239,7 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     const int r0 = wp.s * C;
     const bool circ_lo = a.modeX[0] == BC_CIRC, circ_hi = a.modeX[1] == BC_CIRC;
     const bool fill_lo = !circ_lo && wp.s == 0, fill_hi = !circ_hi && r0 + C >= N;
+    const int nown = N - r0 < C ? N - r0 : C;
     const bool vec = d == 0 && N % C == 0;   // as in the chain
     const long long sd = g.sd;
     const double dt = a.tm->dt;
@@ -266,7 +281,15 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
         if (j == 0 && fill_lo) { D0 = Cq[0][1]; D1 = Cq[1][1]; }
         bx[j] = (bxo[j] - f0 * D0) - f1 * D1;
     }
-    if (fill_hi) bx[C] = bx[C - 1];
+    if (fill_hi) {   // B_X.shift(X, +1) past the end cell nown - 1 is that cell's value (const)
+        T e = bx[0];
+#pragma unroll
+        for (int j = 1; j < C; ++j)
+            if (j == nown - 1) e = bx[j];
+#pragma unroll
+        for (int j = 1; j <= C; ++j)
+            if (j == nown) bx[j] = e;
+    }
     pdl_trigger();
     if (!wp.colok) return;
     T* CBX = reinterpret_cast<T*>(a.q[Q_CBX + d]);
@@ -277,11 +300,10 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     for (int k = 0; k < C; ++k) {
         bn[k] = bx[k];
         cbx[k] = T(0.5) * (bx[k] + bx[k + 1]);
-        const long long o = o0 + (long long)k * sd;
-        const T b2 = BI2[o];
-        cb2[k] = T(0.5) * (b2 + BI2[o + nb2]);
+        const long long o = o0 + (long long)k * sd;   // rows past a ragged end: not read (nor stored)
+        const T b2 = k < nown ? BI2[o] : T(0);
+        cb2[k] = k < nown ? T(0.5) * (b2 + BI2[o + nb2]) : T(0);
     }
-    const int nown = N - r0 < C ? N - r0 : C;
     if (nown == C) {
         seg_store<T, C>(BX, o0, sd, vec, bn);
         seg_store<T, C>(CBX, o0, sd, vec, cbx);

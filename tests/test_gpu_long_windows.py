@@ -82,3 +82,51 @@ def test_segment_fluid_cluster_periodic(precision, tol):
     g.run()
     _assert_close(o, g, tol, f"periodic 4800 {precision}")
     g.close()
+
+
+def _wavy_tube(n, width=3):
+    """An MHD tube with no uniform stretch anywhere (the const ends see every stage's own end value)."""
+    x = (np.arange(n) + 0.5)[:, None, None] / n * np.ones((n, width, width))
+    rho = 1 + 0.2 * np.sin(6 * np.pi * x + 0.3)
+    P = 1 + 0.1 * np.cos(4 * np.pi * x)
+    mom = np.stack([0.1 * np.sin(2 * np.pi * x), 0.05 * np.cos(2 * np.pi * x), 0 * x]) * rho
+    mag = np.stack([np.full(x.shape, 0.75), 0.5 + 0.1 * np.cos(2 * np.pi * x), 0.05 * np.sin(4 * np.pi * x)])
+    ener = P / (5 / 3 - 1) + 0.5 * (mom ** 2).sum(0) / rho + 0.5 * (mag ** 2).sum(0)
+    return rho, mom, ener, mag
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-11), ("mixed", 2e-5)])
+@pytest.mark.parametrize("n", [22, 1001, 2998])
+def test_ragged_const_ends_on_a_wavy_tube(n, precision, tol):
+    """Ragged last segments next to const ends, where the end cells' stage values differ from their
+    neighbours' (22 cells: windows of 6 segments, 32 pencils per CTA; 1001 and 2998: the segment fluid
+    kernel's cluster forms too, chosen for the mixed form and set for FP64)."""
+    grid = (n, 3, 3)
+    s = dict(grid=grid, dgrid=(1.0 / n,) * 3, gamma=5 / 3, cfl=0.35, bc={"x": "const", "y": "circ", "z": "circ"},
+             limiter=("vanleer", "minmod", "superbee"), magnet=True, time_max=1e5, iter_max=6)
+    o, g = make_pair(s, _wavy_tube(n), precision=precision)
+    if n > 64:
+        if precision == "fp64":
+            g.set_tiling(1, (1, -(-n // 4), -(-n // 1024), 256, 4, 1, 1))
+        assert g.tiling("fluid")[1][6] == 1 and g.tiling("fluid")[1][1] == -(-n // 4), g.tiling("fluid")
+    assert g.tiling("magnet")[1][6] == 1 and n % g.tiling("magnet")[1][4] != 0, g.tiling("magnet")
+    o.run()
+    g.run()
+    _assert_close(o, g, tol, f"wavy tube {n} {precision}")
+    g.close()
+
+
+@pytest.mark.parametrize("tiling", [(1, 32, 1, 32, 2, 1, 1), (4, 16, 1, 64, 4, 1, 1)])
+def test_window_segments_near_const_ends(tiling):
+    """Windows reach 4 cells past their segment: with 2 cells per thread the two segments next to each
+    const end see past it, and take that end's value at every stage as the last segment does."""
+    n = 64
+    grid = (n, 3, 3)
+    s = dict(grid=grid, dgrid=(1.0 / n,) * 3, gamma=5 / 3, cfl=0.35, bc={"x": "const", "y": "circ", "z": "circ"},
+             limiter=("vanleer", "minmod", "superbee"), magnet=True, time_max=1e5, iter_max=6)
+    o, g = make_pair(s, _wavy_tube(n))
+    g.set_tiling(1, tiling, kind="magnet")
+    o.run()
+    g.run()
+    _assert_close(o, g, 1e-11, f"window tiling {tiling}")
+    g.close()
