@@ -40,7 +40,7 @@ __device__ __forceinline__ long long trans_offset(int ie, int ne, long long se, 
 // Global row of window cell j of segment s (rows r0 + j, wrapped for circ, clamped for const ends).
 // The window reaches at most 4 rows past a segment, so a pencil shorter than that wraps more than once
 // (r >= -4 and r < N + C + 4: the loops run at most a few times).
-__device__ __forceinline__ int win_row(int r, int N, bool circ_lo, bool circ_hi) {
+__device__ __forceinline__ int win_row_multi(int r, int N, bool circ_lo, bool circ_hi) {
     if (r < 0) {
         if (!circ_lo) return 0;
         do r += N; while (r < 0);
@@ -52,6 +52,29 @@ __device__ __forceinline__ int win_row(int r, int N, bool circ_lo, bool circ_hi)
         return r;
     }
     return r;
+}
+
+// The same where one wrap suffices: rows r >= -N and r < 2N (a window that reaches H rows past its
+// segment, on a pencil of N >= C + H rows: the last segment starts at row N - 1 at most).  Selects
+// only, no loop.
+__device__ __forceinline__ int win_row_once(int r, int N, bool circ_lo, bool circ_hi) {
+    const int lo = circ_lo ? r + N : 0, hi = circ_hi ? r - N : N - 1;
+    return r < 0 ? lo : (r >= N ? hi : r);
+}
+
+// Global offsets of the W window rows r0 - H .. r0 - H + W - 1 (H rows of halo below the segment,
+// W - C - H above).  The choice between the two row functions is uniform over the launch (N is).
+template <int C, int W, int H>
+__device__ __forceinline__ void win_rows(long long (&orow)[W], long long base, int r0, int N, long long sd,
+                                         bool circ_lo, bool circ_hi) {
+    constexpr int REACH = (H > W - C - H ? H : W - C - H);
+    if (N >= C + REACH) {
+#pragma unroll
+        for (int j = 0; j < W; ++j) orow[j] = base + (long long)win_row_once(r0 + j - H, N, circ_lo, circ_hi) * sd;
+    } else {
+#pragma unroll
+        for (int j = 0; j < W; ++j) orow[j] = base + (long long)win_row_multi(r0 + j - H, N, circ_lo, circ_hi) * sd;
+    }
 }
 
 // Const ends: the window cells of a stage array A (local cells LO .. HI-1 at A[j + OFS]) past the
@@ -139,8 +162,8 @@ __device__ __forceinline__ void mag_chain_win_body(const MagArgs& a, unsigned vb
 
     // ---- loads: the corner velocity (magnetFlux.m:18-19) over the window, B_I over cells -3 .. C+2 ----
     long long orow[W];
-#pragma unroll
-    for (int j = 0; j < W; ++j) orow[j] = wp.base + (long long)win_row(r0 + j - 4, N, circ_lo, circ_hi) * sd;
+    // idle threads (past the last segment) read rows of segment 0 and store nothing
+    win_rows<C, W, 4>(orow, wp.base, wp.colok ? r0 : 0, N, sd, circ_lo, circ_hi);
     T vgr[2][W], bI[2][W - 2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
@@ -245,8 +268,7 @@ __device__ __forceinline__ void mag_ct_win_body(const MagArgs& a, unsigned vbloc
     const double dt = a.tm->dt;
     // window cells -1 .. C (index j + 1)
     long long orow[C + 2];
-#pragma unroll
-    for (int j = 0; j < C + 2; ++j) orow[j] = wp.base + (long long)win_row(r0 + j - 1, N, circ_lo, circ_hi) * sd;
+    win_rows<C, C + 2, 1>(orow, wp.base, wp.colok ? r0 : 0, N, sd, circ_lo, circ_hi);
     // C_q = F_q - F_q.shift(I_q, +1) over the window (relaxingMagnet.m:56)
     T Cq[2][C + 2];
 #pragma unroll
