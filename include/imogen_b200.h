@@ -291,8 +291,9 @@ int img_totals(img_ctx* ctx, double out[8]);
  * that may not call cudaMalloc (a MEX call whose device memory belongs to the MATLAB session's
  * allocator, or a host that has fixed its device footprint up front).  The scratch is a file-scope
  * device array of 128 KiB (16384 doubles: 1023 per-block partial pairs of 8 variables, the 8 results
- * and an 8-entry pointer table), looked up once per device with cudaGetSymbolAddress; grids of any
- * size.  Each call copies the pointer table from the host, synchronises the context's stream and
+ * and an 8-entry pointer table), whose device address the first call on each device looks up with
+ * cudaGetSymbolAddress (make that first call before any stream capture on the device); grids of any
+ * size. Each call copies the pointer table from the host, synchronises the context's stream and
  * copies the 8 results to `out` before it returns, so it cannot be captured into a graph: while the
  * context's stream is capturing it returns IMG_ERR_STATE and does nothing.  Every call overwrites all the scratch it reads,
  * so nothing needs to start at zero.  All contexts of a device share that scratch: calls that
