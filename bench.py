@@ -277,22 +277,31 @@ def run_ours(args):
             if den > 0:
                 l1[f"{k}{'xyz'[c]}"] = float(np.abs(sm[k][c] - sf[k][c]).sum() / den)
 
-    # per-kernel roofline: the fused fluid sweep timed alone, L2 flushed before each launch
+    # per-kernel roofline: the fused fluid sweep of each swept direction timed alone, L2 flushed before
+    # each launch; the slower direction (the dominant fluid kernel of the step) is the line's roofline
     peak, peak_kind = measured_hbm_peak()
     traffic = profiled_traffic("fluid_sweep_x_mixed") if args.workload == "ot512" else None
-    roof = {}
+    roof, sweeps = {}, {}
+    dims = [d for d in (1, 2, 3) if s["grid"][d - 1] >= 3]
     for prec in ("mixed", "fp64"):
         r = runs[prec]
         w = 4 if prec == "mixed" else 8
-        r.time.set(r.time.time, 1e-4, r.time.iteration)
-        el = timed_steps(r, max(5, args.steps), per_launch=lambda r=r: r.relaxing_fluid(1))
-        per = el / max(5, args.steps)
         alg = ncell * (8 + 5) * w     # reads rho,p,E,cellB (8 words), writes rho,p,E (5 words)
+        sweeps[prec] = {}
+        for X in dims:
+            r.time.set(r.time.time, 1e-4, r.time.iteration)
+            el = timed_steps(r, max(5, args.steps), per_launch=lambda r=r, X=X: r.relaxing_fluid(X))
+            per = el / max(5, args.steps)
+            sweeps[prec]["xyz"[X - 1]] = {"launch_us": per * 1e6, "achieved": alg / per / 1e9,
+                                          "frac": alg / per / 1e9 / peak}
+        dom = max(sweeps[prec], key=lambda k: sweeps[prec][k]["launch_us"])
+        per = sweeps[prec][dom]["launch_us"] * 1e-6
+        tr = traffic if (prec == "mixed" and dom == "x") else None
         roof[prec] = {"bound": "hbm", "achieved": alg / per / 1e9, "peak": peak, "unit": "GB/s",
-                      "frac": alg / per / 1e9 / peak, "traffic": traffic if prec == "mixed" else None,
+                      "frac": alg / per / 1e9 / peak, "traffic": tr,
                       "traffic_source": "static figure from the ncu capture committed in "
                                         "profiles/pencil_kernels_orszag_tang_512_mixed.md (not measured in this run)"
-                      if prec == "mixed" and traffic else None, "kernel": "fluid_sweep_kernel X",
+                      if tr else None, "kernel": f"fluid sweep along {dom} (the slower swept direction)",
                       "launch_us": per * 1e6, "alg_bytes": alg, "peak_kind": peak_kind}
 
     # end to end through the C ABI: the step's state comes from pinned host memory (X.array = ...
@@ -354,6 +363,7 @@ def run_ours(args):
             "accuracy_t_end": accuracy,
             "roofline": roof["mixed"],
             "roofline_fp64": roof["fp64"],
+            "roofline_sweeps": sweeps,
             "gpu_launches": launches["mixed"],
             "clocks": clk,
             "e2e": e2e,
@@ -439,12 +449,15 @@ def run_kh(args, timed_steps, peak):
             r.iterate()
         k = 5
         el = timed_steps(r, k)
-        r.time.set(r.time.time, 1e-5, r.time.iteration)
-        per = timed_steps(r, k, per_launch=lambda r=r: r.relaxing_fluid(1)) / k
         alg = cells * (8 + 5) * w
+        fl = {}
+        for X in (1, 2, 3):   # each direction's fluid sweep alone (the inputs are larger than L2)
+            r.time.set(r.time.time, 1e-5, r.time.iteration)
+            per = timed_steps(r, k, per_launch=lambda r=r, X=X: r.relaxing_fluid(X)) / k
+            fl["xyz"[X - 1]] = {"launch_us": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
+                                "frac_of_measured_hbm": alg / per / 1e9 / peak}
         out[prec] = {"zone_updates_per_s": cells * 2 * k / el, "ms_per_step": 1e3 * el / k,
-                     "fluid_x": {"launch_us": per * 1e6, "alg_bytes": alg, "achieved_gbs": alg / per / 1e9,
-                                 "frac_of_measured_hbm": alg / per / 1e9 / peak},
+                     "fluid_x": fl["x"], "fluid_sweeps": fl,
                      "tiling": {kind: {"xyz"[d - 1]: t for d, t in tl.items()} for kind, tl in tiling.items()}}
         r.close()
     return out
@@ -466,12 +479,16 @@ def run_serving(args, small=False):
     # every kernel variant and batch shape they meet loads its code; launch plans are set up); the
     # one-at-a-time baseline warms on its first 20 jobs
     warm_n = args.serve_jobs if small else min(args.serve_jobs, 40)
+    # rounds between checks for finished jobs (a check synchronises every batch): the stated stream's
+    # rounds carry many large jobs and take tens of milliseconds, so it checks less often; the
+    # unsaturated stream's rounds are short and a finished job should leave within a few of them
+    ce = 4 if small else 32
     warm = serve.sedov_stream(warm_n, rate=1e6, seed=0, precision="mixed", **sizes)
-    serve.Server(hbm_budget=args.serve_budget_gb << 30, check_every=4, keep="totals").serve(warm)
+    serve.Server(hbm_budget=args.serve_budget_gb << 30, check_every=ce, keep="totals").serve(warm)
     serve.one_at_a_time(serve.sedov_stream(20, rate=1e6, seed=0, precision="fp64", **sizes), precision="fp64")
     jobs = serve.sedov_stream(args.serve_jobs, rate=50.0, seed=0, precision="mixed", **sizes)
     t0 = time.perf_counter()
-    done = serve.Server(hbm_budget=args.serve_budget_gb << 30, check_every=4, keep="totals").serve(jobs)
+    done = serve.Server(hbm_budget=args.serve_budget_gb << 30, check_every=ce, keep="totals").serve(jobs)
     el = time.perf_counter() - t0
     a = serve.latency_summary(done)
     a.update(wall_s=el, zone_updates_per_s=a["zone_updates"] / el)
@@ -486,7 +503,7 @@ def run_serving(args, small=False):
                         f"3-D {lo3}^3..{hi3}^3 log-uniform, t=0.05, HBM budget {args.serve_budget_gb} GB",
             "server": "native job server (img_server_create / img_batch_submit / img_batch_poll)",
             "arrival_span_s": arrivals,
-            "offered_load": a["zone_updates"] / arrivals / a["zone_updates_per_s"],
+            "offered_load": a["zone_updates"] / arrivals / a["zone_updates_per_s"], "check_every": ce,
             "served_mixed": a, "one_at_a_time_fp64": b}
 
 

@@ -130,3 +130,22 @@ def test_window_segments_near_const_ends(tiling):
     g.run()
     _assert_close(o, g, 1e-11, f"window tiling {tiling}")
     g.close()
+
+
+@pytest.mark.parametrize("bc", ["circ", "const"])
+@pytest.mark.parametrize("n", [5, 7, 8, 13])
+def test_window_rows_at_the_one_wrap_threshold(n, bc):
+    """The window kernels wrap (circ) or clamp (const) their rows with selects where one wrap reaches
+    every row -- N >= C + 4 for the chain, N >= C + 1 for CT -- and with loops below that.  With C = 4:
+    n = 5 and 7 take the loops in the chain (5 takes the selects in CT), 8 sits at the chain's threshold,
+    13 leaves a ragged one-cell last segment; 16 pencils per CTA on 9 pencils leave idle threads."""
+    grid = (n, 3, 3)
+    s = dict(grid=grid, dgrid=(1.0 / n,) * 3, gamma=5 / 3, cfl=0.35, bc={"x": bc, "y": "circ", "z": "circ"},
+             limiter=("vanleer", "minmod", "superbee"), magnet=True, time_max=1e5, iter_max=6)
+    o, g = make_pair(s, _wavy_tube(n))
+    seg = -(-n // 4)
+    g.set_tiling(1, (32 // seg, seg, 1, 32, 4, 1, 1), kind="magnet")
+    o.run()
+    g.run()
+    _assert_close(o, g, 1e-11, f"n={n} {bc}")
+    g.close()
