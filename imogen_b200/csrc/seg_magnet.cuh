@@ -40,7 +40,7 @@ __device__ __forceinline__ long long trans_offset(int ie, int ne, long long se, 
 // Global row of window cell j of segment s (rows r0 + j, wrapped for circ, clamped for const ends).
 // The window reaches at most 4 rows past a segment, so a pencil shorter than that wraps more than once
 // (r >= -4 and r < N + C + 4: the loops run at most a few times).
-__device__ __forceinline__ int win_row_multi(int r, int N, bool circ_lo, bool circ_hi) {
+__host__ __device__ __forceinline__ int win_row_multi(int r, int N, bool circ_lo, bool circ_hi) {
     if (r < 0) {
         if (!circ_lo) return 0;
         do r += N; while (r < 0);
@@ -57,7 +57,7 @@ __device__ __forceinline__ int win_row_multi(int r, int N, bool circ_lo, bool ci
 // The same where one wrap suffices: rows r >= -N and r < 2N (a window that reaches H rows past its
 // segment, on a pencil of N >= C + H rows: the last segment starts at row N - 1 at most).  Selects
 // only, no loop.
-__device__ __forceinline__ int win_row_once(int r, int N, bool circ_lo, bool circ_hi) {
+__host__ __device__ __forceinline__ int win_row_once(int r, int N, bool circ_lo, bool circ_hi) {
     const int lo = circ_lo ? r + N : 0, hi = circ_hi ? r - N : N - 1;
     return r < 0 ? lo : (r >= N ? hi : r);
 }
