@@ -117,6 +117,18 @@ def profiled_traffic(key):
         return None
 
 
+def max_over_ranks(x, device):
+    """The largest of x over the ranks of the default process group (x itself with one rank): the job's
+    time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -259,11 +271,7 @@ def run_ours(args):
             l0 = r.launches
             el = timed_steps(r, args.steps)
             launches[prec] = r.launches - l0
-            if ws > 1:
-                t = torch.tensor([el], device=dev, dtype=torch.float64)
-                torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-                el = float(t.item())
-            results[prec] = el
+            results[prec] = max_over_ranks(el, dev)
     clk = clocks.summary()
 
     # relative L1 of mixed vs FP64 after the same iterations
